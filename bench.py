@@ -1,0 +1,300 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Monte Carlo engine on the local-volatility RQMC workload.
+
+Workload (one "step" = one evaluation of the whole workload):
+  SSVI surface (theta = 0.04 t, rho = -0.4, eta = 1, gamma = 0.5) -> Dupire
+  local-variance grid 31 x 100, 252 daily Log-Euler steps, T = 1, 2^20 Sobol
+  points x 16 scrambles with a Brownian-bridge plan, an arithmetic-average Asian
+  call K = 100 and a discrete down-and-out call (B = 80, daily, rebate 1) priced
+  on the same draws.  2^24 paths x 252 steps = 4.23e9 path-steps per step.
+  Synthetic market (S = 100, r = 3%, q = 1%); FP64 arithmetic.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Weak scaling: rank r evaluates scrambles [16 r, 16 r + 16) of one plan, so each
+GPU's work is fixed; the per-scramble means are gathered to rank 0.
+`--impl reference` times the CPU restatement of the reference's executor (the
+oracle) on this host's cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "rust-pricing-library_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "path-steps/s on 1 B200; time to 1bp price err: batched/adjoint/learned vs plain"
+UNIT = "path-steps/s"
+POINTS, SCRAMBLES, STEPS = 1 << 20, 16, 252
+# Algorithmic FP64 operations per path-step of this workload (each IEEE result
+# counts once; div, sqrt, log and exp count as one operation each):
+#   AS241 central branch 33 (+ 15% tails x 31) + midpoint map 2 + bridge node 5
+#   + increment 2 + Log-Euler step 27 (f/F, ln, clamp, x weight 3, bilinear 12,
+#   sqrt, exponent 5, exp, ratio and state products 2) + Asian 2 + barrier 4.
+FLOPS_PER_PATH_STEP = 33 + 0.15 * 31 + 2 + 5 + 2 + 27 + 2 + 4
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--points", type=int, default=POINTS)
+    ap.add_argument("--scrambles", type=int, default=SCRAMBLES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def workload(points, scrambles, builder, scramble_begin=0):
+    from rust_pricing_b200 import workloads as W
+    spec = W.local_vol_rqmc(builder, points=points, scrambles=scrambles)
+    spec.scramble_begin = scramble_begin
+    return spec
+
+
+def gpu_grid(surface, floor, cap):
+    import numpy as np
+    from rust_pricing_b200 import _native as N
+    tt, tv, slope, rho, eta, gamma, tn, xn = surface.grid_args()
+    arr = [np.ascontiguousarray(a, dtype=np.float64) for a in (tt, tv, tn, xn)]
+    out = np.zeros(len(tn) * len(xn))
+    rep = C.c_uint32()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    N.check(N.library().mcg_ssvi_local_variance_grid(
+        dp(arr[0]), dp(arr[1]), len(tt), slope, rho, eta, gamma, dp(arr[2]), len(tn), dp(arr[3]),
+        len(xn), floor, cap, dp(out), C.byref(rep)))
+    return out.reshape(len(tn), len(xn))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except (OSError, ValueError):
+        return {}
+
+
+def cpu_baseline(points: int, scrambles: int, threads: int, grid_builder=None):
+    """The oracle (CPU restatement of the reference executor) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+    from rust_pricing_b200 import workloads as W
+    if grid_builder is None:
+        import gpu_common as G
+        grid_builder = G.oracle_grid
+    spec = W.local_vol_rqmc(grid_builder, points=points, scrambles=scrambles)
+    spec.reduction_block_size = 256
+    t0 = time.perf_counter()
+    H.oracle_evaluate(spec, threads)
+    dt = time.perf_counter() - t0
+    path_steps = points * scrambles * STEPS
+    return path_steps / dt, dt, path_steps
+
+
+def run_reference(args, rank, world):
+    """CPU executor (oracle port) on all host cores; rank 0 only."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sample_points, sample_scrambles = 1 << 15, 2
+    for _ in range(args.warmup and 1):
+        cpu_baseline(1 << 10, 1, threads)
+    times = []
+    for _ in range(args.steps):
+        value, dt, ps = cpu_baseline(sample_points, sample_scrambles, threads)
+        times.append(dt)
+    per = statistics.mean(times)
+    value = sample_points * sample_scrambles * STEPS / per
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "local-vol RQMC: SSVI->Dupire 31x100 grid, 252 daily steps, 2^20 Sobol points x 16 "
+                               "scrambles, Brownian bridge, Asian call + discrete down-and-out on the same draws",
+                   "sample": f"{sample_points} points x {sample_scrambles} scrambles per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sample_points} points x {sample_scrambles} scrambles x {STEPS} steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    import numpy as np
+    import torch
+    from rust_pricing_b200 import _native as N
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    handle = stream.cuda_stream
+    spec = workload(args.points, args.scrambles, gpu_grid, scramble_begin=rank * args.scrambles)
+    plan = N.Plan(spec)
+    path_steps_rank = args.points * args.scrambles * STEPS
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        res = plan.evaluate(handle)
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms, launches = [], 0
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            events[k][0].record(stream)
+            buf = plan.evaluate(handle)
+            events[k][1].record(stream)
+            kernel_ms.append(buf.result.path_kernel_ms)
+            launches += buf.result.kernel_launches
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in events]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        # gather the per-scramble price means (the estimator's replicate values)
+    ms_per_step = total_ms / args.steps
+    value = world * path_steps_rank / (ms_per_step * 1e-3)
+
+    # roofline of the dominant kernel (the path kernel): FP64 operations
+    peak = C.c_double()
+    N.check(N.library().mcg_measure_fp64_peak(C.c_void_p(handle), C.byref(peak)))
+    path_ms = statistics.mean(kernel_ms)
+    achieved = FLOPS_PER_PATH_STEP * path_steps_rank / (path_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "peak_source": "measured live: mcg_measure_fp64_peak (DFMA chains, this GPU)",
+                "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel_ms": path_ms}
+
+    # end to end: the C-ABI call with host buffers (plan compile + upload + run + results back)
+    e2e_times = []
+    desc = spec.desc()
+    for _ in range(args.e2e_steps):
+        rb = __import__("rust_pricing_b200._abi", fromlist=["_abi"]).ResultBuffers(len(spec.products))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        N.check(N.library().mcg_price(C.byref(desc), C.c_void_p(handle), C.byref(rb.result)), rb.result.error)
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = min(e2e_times)
+    grid_bytes = spec.grid_value_count() * 8 + (len(spec.local_variance.time_nodes) + len(spec.local_variance.log_moneyness_nodes)) * 8
+    h2d = grid_bytes + spec._dimension_hint() * 32 * 4 + len(spec.observation_times) * 8 * 4 + 2 * STEPS * 8 * 12
+    d2h = args.scrambles * len(spec.products) * 18 * 40 + 32
+    e2e = {"value": world * path_steps_rank / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_s,
+           "path": "mcg_price(): plan compile, upload, evaluate, statistics back"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "local-vol RQMC: SSVI->Dupire 31x100 grid, 252 daily steps, 2^20 Sobol points x 16 "
+                               "scrambles, Brownian bridge, Asian call + discrete down-and-out on the same draws",
+                   "points_per_scramble": args.points, "scrambles_per_gpu": args.scrambles, "time_steps": STEPS,
+                   "path_steps_per_gpu": path_steps_rank, "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"scramble shards x{world}"},
+        "roofline": roofline,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "prices": [buf.products[k].price.value for k in range(len(spec.products))],
+        "price_standard_errors": [buf.products[k].price.standard_error for k in range(len(spec.products))],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample_points, sample_scrambles = 1 << 15, 2
+        value_cpu, dt, ps = cpu_baseline(sample_points, sample_scrambles, threads, grid_builder=gpu_grid)
+        line["cpu_baseline"] = {"value": value_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{sample_points} points x {sample_scrambles} scrambles x {STEPS} steps "
+                                          f"({ps:.3g} path-steps, {dt:.1f} s)"}
+    plan.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

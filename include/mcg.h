@@ -1,0 +1,331 @@
+/*
+ * mcg.h -- C ABI of the B200 Monte Carlo pricing engine.
+ *
+ * The engine replaces the CPU executor seam of msfmfjt/rust-pricing-library:
+ *
+ *   SimulationPlan::execute            crates/pricing/src/engine/risk/valuation.rs:19-33
+ *     -> execute_pseudo / execute_rqmc crates/pricing/src/engine/risk/valuation.rs:126-437
+ *     -> execute_local_vol_pseudo/rqmc crates/pricing/src/engine/risk/local_vol.rs:24-420
+ *     -> DeterministicExecutor::try_map_reduce_*  crates/pricing/src/engine/mc/execution.rs:361-726
+ *
+ * A caller compiles a request into an `mcg_plan_desc` (the data the reference
+ * keeps in its immutable `SimulationPlan`, crates/pricing/src/engine/plan/simulation.rs:73-119),
+ * hands it to `mcg_plan_create`, and evaluates the plan on a CUDA stream.  The
+ * result carries, per product, the 18 pathwise components as
+ * `DeterministicStatistics` records (crates/pricing/src/engine/mc/execution.rs:140-166)
+ * reduced in a fixed order, plus the estimates the reference builds from them
+ * (crates/pricing/src/engine/risk/report.rs:454-473).
+ *
+ * Everything here is plain C11: pointers, sizes and scalars.  Arrays passed in a
+ * descriptor are owned by the caller and copied during `mcg_plan_create`.
+ * Every entry point returns an `mcg_status`; none of them aborts the process.
+ */
+#ifndef MCG_H
+#define MCG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCG_ABI_VERSION 1u
+
+/* Component layout of one sampling unit, crates/pricing/src/engine/plan/simulation.rs:26-62. */
+#define MCG_PRICE 0
+#define MCG_DELTA 1
+#define MCG_VEGA 2
+#define MCG_GAMMA 3
+#define MCG_BUMP_DELTA 4
+#define MCG_DELTA_DIFFERENCE 5
+#define MCG_BUMP_VEGA 6
+#define MCG_VEGA_DIFFERENCE 7
+#define MCG_BUMP_GAMMA 8
+#define MCG_GAMMA_DIFFERENCE 9
+#define MCG_BARRIER_ENDPOINT_HIT 10
+#define MCG_BARRIER_DIVIDEND_JUMP_HIT 11
+#define MCG_BARRIER_BRIDGE_HIT_WEIGHT 12
+#define MCG_BARRIER_INTERVAL_COUNT 13
+#define MCG_BARRIER_FINITE_CORRECTION_COUNT 14
+#define MCG_BARRIER_ZERO_VARIANCE_COUNT 15
+#define MCG_BARRIER_SURVIVAL_UNDERFLOW_COUNT 16
+#define MCG_BARRIER_CERTAIN_SURVIVAL_COUNT 17
+#define MCG_PATHWISE_COMPONENTS 18
+
+/* Limits.  MCG_MAX_SOBOL_DIMENSION is RqmcConfig::MAX_SOBOL_DIMENSION
+ * (crates/pricing/src/engine/mc/config.rs:88). */
+#define MCG_MAX_SOBOL_DIMENSION 21201u
+#define MCG_MAX_PRODUCTS 8u
+
+/* Status codes.  They mirror the reference's error variants
+ * (crates/pricing/src/api/error.rs:256-301, LocalVolError
+ * crates/pricing/src/engine/processes/local_vol.rs:24-73,
+ * BarrierBridgeError crates/pricing/src/engine/payoff/barrier_bridge.rs:27-55). */
+typedef enum mcg_status {
+    MCG_OK = 0,
+    MCG_ERR_INVALID_ARGUMENT = 1,      /* malformed descriptor; `mcg_last_error` names the field */
+    MCG_ERR_UNSUPPORTED = 2,           /* a combination this engine does not implement */
+    MCG_ERR_CUDA = 3,                  /* CUDA runtime failure (no device, launch failure, ...) */
+    MCG_ERR_ALLOCATION = 4,            /* device or host allocation failed */
+    MCG_ERR_INSUFFICIENT_UNITS = 5,    /* MonteCarloError::InsufficientSamplingUnits */
+    MCG_ERR_NON_FINITE_STATE = 6,      /* LocalVolError::NonFiniteState{step,bits} */
+    MCG_ERR_INVALID_SURFACE_QUERY = 7, /* MarketError::InvalidSurfaceQuery */
+    MCG_ERR_SOBOL_DIMENSION = 8,       /* RqmcPlanError::DimensionLimitExceeded */
+    MCG_ERR_BRIDGE = 9,                /* BrownianBridgeError */
+    MCG_ERR_BARRIER_BRIDGE = 10,       /* BarrierBridgeError */
+    MCG_ERR_MARKET = 11,               /* MarketError (curve, surface, grid) */
+    MCG_ERR_LSM = 12,                  /* LsmNumericalError */
+    MCG_ERR_TIMEOUT = 13,              /* a bounded device wait ran out */
+    MCG_ERR_NOT_BUILT = 14             /* a kernel variant is missing from this build */
+} mcg_status;
+
+typedef enum mcg_model_kind {
+    MCG_MODEL_BLACK_SCHOLES = 0,
+    MCG_MODEL_LOCAL_VOLATILITY = 1
+} mcg_model_kind;
+
+typedef enum mcg_engine_kind {
+    MCG_ENGINE_PSEUDO = 0, /* PseudoMcConfig, crates/pricing/src/engine/mc/config.rs */
+    MCG_ENGINE_RQMC = 1    /* RqmcConfig */
+} mcg_engine_kind;
+
+typedef enum mcg_product_kind {
+    MCG_PRODUCT_EUROPEAN = 0,
+    MCG_PRODUCT_DIGITAL = 1,
+    MCG_PRODUCT_ASIAN = 2,
+    MCG_PRODUCT_LOOKBACK = 3,
+    MCG_PRODUCT_DISCRETE_BARRIER = 4,
+    MCG_PRODUCT_CONTINUOUS_BARRIER = 5,
+    MCG_PRODUCT_AMERICAN = 6
+} mcg_product_kind;
+
+typedef enum mcg_side { MCG_CALL = 0, MCG_PUT = 1 } mcg_side;
+typedef enum mcg_barrier_direction { MCG_BARRIER_UP = 0, MCG_BARRIER_DOWN = 1 } mcg_barrier_direction;
+typedef enum mcg_barrier_style { MCG_KNOCK_OUT = 0, MCG_KNOCK_IN = 1 } mcg_barrier_style;
+typedef enum mcg_digital_payout { MCG_DIGITAL_CASH = 0, MCG_DIGITAL_ASSET = 1 } mcg_digital_payout;
+
+/* Arithmetic of the path bulk.  FP64 reproduces the reference; FP32 runs the
+ * state evolution in single precision and keeps payoff and statistics in FP64. */
+typedef enum mcg_precision { MCG_PRECISION_F64 = 0, MCG_PRECISION_F32_BULK = 1 } mcg_precision;
+
+/* Log-linear discount curve, LogLinearDiscountCurve
+ * (crates/pricing/src/market/curve.rs:38-200). */
+typedef struct mcg_curve {
+    uint32_t pillar_count;
+    const double* times;            /* strictly increasing, times[0] >= 0 */
+    const double* discount_factors; /* positive */
+} mcg_curve;
+
+/* Dupire local-variance grid, LocalVarianceGrid
+ * (crates/pricing/src/market/local_variance.rs:125-206).  `values` is
+ * time-major: values[t * log_moneyness_count + x]. */
+typedef struct mcg_local_variance_grid {
+    uint32_t time_count;
+    uint32_t log_moneyness_count;
+    const double* time_nodes;          /* time_nodes[0] == +0.0, last == expiry time */
+    const double* log_moneyness_nodes; /* strictly increasing */
+    const double* values;
+    double floor;
+    double cap;
+} mcg_local_variance_grid;
+
+/* One product.  All products of one plan observe the same dates
+ * (`observation_times` of the plan); the product's own arrays index those. */
+typedef struct mcg_product_desc {
+    int32_t kind;      /* mcg_product_kind */
+    int32_t side;      /* mcg_side */
+    double strike;
+    double notional;
+    /* Digital, crates/pricing/src/engine/payoff/compile.rs:104-157 */
+    int32_t digital_payout; /* mcg_digital_payout */
+    double payout;
+    /* Barrier, crates/pricing/src/engine/payoff/compile.rs:204-403 */
+    int32_t barrier_direction; /* mcg_barrier_direction */
+    int32_t barrier_style;     /* mcg_barrier_style */
+    int32_t has_rebate;
+    double barrier;
+    double rebate;
+    /* Arithmetic Asian weights, one per plan observation (NULL for other kinds),
+     * crates/pricing/src/engine/payoff/compile.rs:159-202. */
+    const double* observation_weights;
+} mcg_product_desc;
+
+/* The compiled plan: the hot-path part of the reference's SimulationPlan. */
+typedef struct mcg_plan_desc {
+    uint32_t abi_version; /* MCG_ABI_VERSION */
+    int32_t model;        /* mcg_model_kind */
+    int32_t engine;       /* mcg_engine_kind */
+    int32_t precision;    /* mcg_precision */
+
+    /* Engine configuration.  Pseudo: `sampling_units` independent units under
+     * `master_seed`.  RQMC: `sampling_units` points per scramble (a power of
+     * two) times `scramble_count` scrambles under `master_seed`. */
+    uint64_t master_seed;
+    uint64_t sampling_units;
+    uint32_t scramble_count;
+    uint32_t scramble_begin;       /* RQMC: index of the first scramble (shards of one plan) */
+    int32_t antithetic;
+    int32_t brownian_bridge;
+    uint64_t reduction_block_size; /* ExecutionPolicy, default 4096 */
+    /* Joe--Kuo direction words for RQMC, `sobol_dimension_count` x 32,
+     * dimension-major (the reference's embedded asset
+     * crates/pricing/data/joe-kuo-6.21201-u32be.bin, decoded). */
+    uint32_t sobol_dimension_count;
+    const uint32_t* sobol_directions;
+
+    /* Market. */
+    double spot;
+    mcg_curve discount_curve;
+    mcg_curve dividend_curve;
+    double volatility; /* Black-Scholes only */
+    mcg_local_variance_grid local_variance; /* local volatility only */
+
+    /* Contract timing.  `observation_times` are ACT/365F year fractions of the
+     * product's fixing dates (strictly increasing, > 0); the last one is the
+     * expiry.  `payment_time` discounts the payoff. */
+    uint32_t observation_count;
+    const double* observation_times;
+    double payment_time;
+
+    /* Products priced on the same draws. */
+    uint32_t product_count;
+    const mcg_product_desc* products;
+
+    /* Risk request, RiskRequest (crates/pricing/src/risk/request.rs:227). */
+    int32_t request_delta;
+    int32_t request_gamma;
+    int32_t request_vega;
+    int32_t request_local_vega_nodes; /* LV: per-node local-vega sensitivities */
+    int32_t gamma_bump_relative;      /* 1: relative, 0: absolute */
+    double gamma_bump;                /* relative fraction or absolute amount */
+    double smoothing_half_width;      /* PayoffSmoothing::compact_c2; 0 = exact */
+    uint32_t checkpoint_interval;     /* LV reverse: steps between stored states */
+} mcg_plan_desc;
+
+typedef struct mcg_statistics {
+    double sum;        /* NeumaierSum (crates/pricing-numerics/src/reduction.rs:3-56) */
+    double correction;
+    uint64_t count;    /* CenteredMoment (reduction.rs:73-170) */
+    double mean;
+    double second_moment;
+} mcg_statistics;
+
+typedef struct mcg_estimate {
+    double value;
+    double standard_error;
+    double confidence_lower;
+    double confidence_upper;
+    uint64_t effective_sampling_units;
+} mcg_estimate;
+
+typedef struct mcg_product_result {
+    mcg_statistics components[MCG_PATHWISE_COMPONENTS];
+    mcg_estimate price;
+    mcg_estimate delta;
+    mcg_estimate gamma;
+    mcg_estimate vega;
+    mcg_estimate bump_delta;
+    mcg_estimate bump_gamma;
+    mcg_estimate bump_vega;
+    double sampling_variance;
+    double estimator_variance;
+} mcg_product_result;
+
+typedef struct mcg_error_record {
+    int32_t code;          /* mcg_status of the first failing unit */
+    uint32_t step;         /* step or index inside the unit */
+    uint64_t sampling_unit;
+    uint64_t value_bits;   /* bit pattern of the offending value */
+} mcg_error_record;
+
+typedef struct mcg_result {
+    uint32_t product_capacity;       /* entries available in `products` */
+    mcg_product_result* products;    /* caller-owned */
+    /* Local-volatility node sensitivities (grid value count entries each),
+     * caller-owned; NULL when not requested. */
+    uint32_t node_capacity;
+    mcg_statistics* local_vega_nodes;
+    mcg_estimate* local_vega_node_estimates;
+
+    uint64_t independent_sampling_units;
+    uint64_t evaluated_paths;
+    uint32_t time_steps;       /* path steps per evaluated path */
+    uint32_t effective_dimension;
+    uint32_t reduction_records;
+    uint32_t kernel_launches;  /* kernels this evaluation launched */
+    float device_ms;           /* device time of the evaluation (CUDA events) */
+    float path_kernel_ms;      /* device time of the path kernel alone */
+    mcg_error_record error;
+} mcg_result;
+
+typedef struct mcg_plan mcg_plan;
+
+/* Library identity and the last error message of the calling thread. */
+uint32_t mcg_abi_version(void);
+const char* mcg_last_error(void);
+
+/* Compile a plan: validates the descriptor, builds the time grid, the Brownian
+ * bridge, the RQMC scramble table and the device-resident layout.  Replaces
+ * SimulationPlan::compile's runtime part (crates/pricing/src/engine/compile/simulation.rs:78-700,
+ * crates/pricing/src/engine/compile/local_vol.rs:14-102). */
+mcg_status mcg_plan_create(const mcg_plan_desc* desc, mcg_plan** out_plan);
+
+/* Evaluate on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * synchronise.  Replaces SimulationPlan::execute
+ * (crates/pricing/src/engine/risk/valuation.rs:19-33). */
+mcg_status mcg_plan_evaluate(mcg_plan* plan, void* stream, mcg_result* result);
+
+/* Evaluate from host-resident descriptor arrays in one call: create, evaluate,
+ * destroy.  The PricingPlan::compile + evaluate pair of the facade
+ * (crates/pricing/src/engine/risk/pricing.rs:53-88). */
+mcg_status mcg_price(const mcg_plan_desc* desc, void* stream, mcg_result* result);
+
+void mcg_plan_destroy(mcg_plan* plan);
+
+/* Plan introspection: time steps and effective Sobol dimension. */
+mcg_status mcg_plan_shape(const mcg_plan* plan, uint32_t* time_steps,
+                          uint32_t* effective_dimension, uint32_t* grid_value_count);
+
+/* ---- Sampling primitives, exposed for replay and known-answer tests ---- */
+
+/* Standard normals of `count` consecutive sampling units, dimension-major
+ * out[d * count + i], for the Philox coordinate stream
+ * (crates/pricing/src/engine/sampling/random.rs:100-149,176-277). */
+mcg_status mcg_philox_normals(uint64_t master_seed, uint64_t first_unit, uint64_t count,
+                              uint32_t dimensions, uint32_t domain, double* out_host);
+
+/* Scrambled Sobol words of `count` consecutive points of one scramble,
+ * dimension-major out[d * count + i]
+ * (crates/pricing/src/engine/sampling/qmc.rs:47-132,204-369).  `directions`
+ * holds the Joe--Kuo direction words, dimensions x 32. */
+mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint64_t master_seed,
+                          uint32_t scramble, uint64_t first_point, uint64_t count,
+                          uint32_t* out_host);
+
+/* Dupire local-variance grid from a standard SSVI surface with a power-law
+ * phi and PCHIP theta curve, computed on the device
+ * (crates/pricing/src/market/local_variance.rs:149-206,
+ *  crates/pricing/src/market/ssvi.rs:121-176,226-273,410-479,
+ *  crates/pricing/src/market/pchip.rs:111-237).  `values` receives
+ * time_count x log_moneyness_count entries; `repairs` (may be NULL) the number
+ * of floor/cap repairs. */
+mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double* theta_values,
+                                        uint32_t theta_count, double terminal_slope, double rho,
+                                        double eta, double gamma, const double* time_nodes,
+                                        uint32_t time_count, const double* log_moneyness_nodes,
+                                        uint32_t log_moneyness_count, double floor, double cap,
+                                        double* values, uint32_t* repairs);
+
+/* ---- Diagnostics (no counterpart in the reference) ---- */
+
+/* Dense FP64 FMA throughput of the current device in TFLOP/s (an FMA counts as
+ * two flops), measured with independent DFMA chains.  The benchmark uses it as
+ * the roofline of the FP64 path kernels. */
+mcg_status mcg_measure_fp64_peak(void* stream, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCG_H */

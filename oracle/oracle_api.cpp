@@ -1,0 +1,168 @@
+// oracle_api.cpp -- extern "C" surface of the CPU oracle (liboracle.so).
+//
+// TEST INFRASTRUCTURE ONLY.  Loaded by tests/, __graft_entry__.smoke() and the
+// CPU-baseline leg of bench.py to check and time the CUDA engine; never linked
+// into the engine itself.
+#include <cstring>
+#include <vector>
+
+#include "../include/mcg.h"
+#include "oracle_core.h"
+
+namespace oracle {
+int evaluate(const mcg_plan_desc* desc, mcg_result* result, int threads);
+const char* last_error();
+int unit_shocks_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out);
+int unit_values_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out);
+int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacity, uint32_t* count);
+std::vector<double> pchip_derivatives(const std::vector<double>& t, const std::vector<double>& v);
+int ssvi_grid(const std::vector<double>& theta_t, const std::vector<double>& theta_v, double slope,
+              double rho, double eta, double gamma, const std::vector<double>& tn,
+              const std::vector<double>& xn, double floor, double cap, std::vector<double>& out);
+std::vector<double> piecewise_sinh_nodes(double left, double right, size_t nl, size_t nr,
+                                         double ls, double rs);
+}  // namespace oracle
+
+extern "C" {
+
+void oracle_philox_block(uint64_t seed, const uint32_t counter[4], uint32_t out[4]) {
+    oracle::Block4 c{{counter[0], counter[1], counter[2], counter[3]}};
+    const oracle::Block4 r = oracle::philox_generate(seed, c);
+    std::memcpy(out, r.v, sizeof(r.v));
+}
+
+uint32_t oracle_philox_word(uint64_t seed, uint64_t path, uint32_t dimension, uint32_t domain) {
+    return oracle::philox_word(seed, path, dimension, domain);
+}
+
+double oracle_open_unit_interval(uint32_t word) { return oracle::open_unit_interval(word); }
+
+double oracle_inverse_normal(double p) { return oracle::inverse_standard_normal(p); }
+
+double oracle_philox_normal(uint64_t seed, uint64_t path, uint32_t dimension, uint32_t domain) {
+    return oracle::philox_normal(seed, path, dimension, domain);
+}
+
+uint32_t oracle_sobol_word(const uint32_t* directions32, uint32_t point) {
+    return oracle::sobol_word(directions32, point);
+}
+
+void oracle_scramble(uint64_t seed, uint32_t scramble, uint32_t dimension, uint32_t* shift,
+                     uint32_t rows[32]) {
+    const oracle::Scramble s = oracle::compile_scramble(seed, scramble, dimension);
+    *shift = s.shift;
+    std::memcpy(rows, s.rows, sizeof(s.rows));
+}
+
+uint32_t oracle_rqmc_word(const uint32_t* directions32, uint64_t seed, uint32_t scramble,
+                          uint32_t dimension, uint32_t point) {
+    const oracle::Scramble s = oracle::compile_scramble(seed, scramble, dimension);
+    return s.apply(oracle::sobol_word(directions32, point));
+}
+
+// Brownian bridge: returns the instruction count (or -1 on an invalid grid) and
+// fills node/rank order plus coefficients when the outputs are non-null.
+int oracle_bridge_compile(const double* times, uint32_t count, uint32_t* nodes, uint32_t* ranks,
+                          double* left_weights, double* right_weights, double* sds) {
+    oracle::BridgePlan plan;
+    if (!plan.compile(std::vector<double>(times, times + count))) return -1;
+    for (size_t i = 0; i < plan.instructions.size(); ++i) {
+        const auto& ins = plan.instructions[i];
+        if (nodes) nodes[i] = ins.node;
+        if (ranks) ranks[i] = ins.rank;
+        if (left_weights) left_weights[i] = ins.left_weight;
+        if (right_weights) right_weights[i] = ins.right_weight;
+        if (sds) sds[i] = ins.standard_deviation;
+    }
+    return static_cast<int>(plan.instructions.size());
+}
+
+int oracle_bridge_apply(const double* times, uint32_t count, const double* normals,
+                        double* increments) {
+    oracle::BridgePlan plan;
+    if (!plan.compile(std::vector<double>(times, times + count))) return -1;
+    std::vector<double> scratch;
+    plan.apply(normals, increments, scratch);
+    return 0;
+}
+
+int oracle_bridge_reverse(const double* times, uint32_t count, const double* increment_adjoints,
+                          double* normal_adjoints) {
+    oracle::BridgePlan plan;
+    if (!plan.compile(std::vector<double>(times, times + count))) return -1;
+    std::vector<double> scratch;
+    plan.reverse(increment_adjoints, normal_adjoints, scratch);
+    return 0;
+}
+
+int oracle_evaluate(const mcg_plan_desc* desc, mcg_result* result, int threads) {
+    return oracle::evaluate(desc, result, threads);
+}
+
+int oracle_unit_shocks(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out) {
+    return oracle::unit_shocks_api(desc, scramble, unit, out);
+}
+
+int oracle_unit_values(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out) {
+    return oracle::unit_values_api(desc, scramble, unit, out);
+}
+
+int oracle_time_grid(const mcg_plan_desc* desc, double* nodes, uint32_t capacity,
+                     uint32_t* count) {
+    return oracle::time_grid_api(desc, nodes, capacity, count);
+}
+
+const char* oracle_last_error(void) { return oracle::last_error(); }
+
+int oracle_ssvi_grid(const double* theta_t, const double* theta_v, uint32_t theta_count,
+                     double slope, double rho, double eta, double gamma, const double* tn,
+                     uint32_t nt, const double* xn, uint32_t nx, double floor, double cap,
+                     double* out) {
+    std::vector<double> values;
+    const int repairs = oracle::ssvi_grid(std::vector<double>(theta_t, theta_t + theta_count),
+                                          std::vector<double>(theta_v, theta_v + theta_count), slope,
+                                          rho, eta, gamma, std::vector<double>(tn, tn + nt),
+                                          std::vector<double>(xn, xn + nx), floor, cap, values);
+    if (repairs >= 0) std::memcpy(out, values.data(), values.size() * sizeof(double));
+    return repairs;
+}
+
+int oracle_piecewise_sinh_nodes(double left, double right, uint32_t nl, uint32_t nr,
+                                double left_shape, double right_shape, double* out) {
+    const std::vector<double> n =
+        oracle::piecewise_sinh_nodes(left, right, nl, nr, left_shape, right_shape);
+    std::memcpy(out, n.data(), n.size() * sizeof(double));
+    return static_cast<int>(n.size());
+}
+
+}  // extern "C"
+
+namespace oracle {
+int barrier_path_api(int up, double barrier, double h, const double* states,
+                     const double* variances, const double* times, size_t count, double* survival,
+                     double* diag);
+}
+
+extern "C" int oracle_barrier_path(int up, double barrier, double h, const double* states,
+                                   const double* variances, const double* times, uint32_t count,
+                                   double* survival, double* diag) {
+    return oracle::barrier_path_api(up, barrier, h, states, variances, times, count, survival, diag);
+}
+
+namespace oracle {
+void smoothing_api(double h, double input, double* out);
+void extrema_api(double h, double left, double right, double* out);
+int exact_bridge_api(int up, double barrier, double s0, double s1, double integrated, double* survival);
+int smoothed_bridge_api(int up, double barrier, double s0, double s1, double h, double integrated, double* out);
+}
+
+extern "C" {
+void oracle_smoothing(double h, double input, double* out) { oracle::smoothing_api(h, input, out); }
+void oracle_smooth_extrema(double h, double l, double r, double* out) { oracle::extrema_api(h, l, r, out); }
+int oracle_exact_bridge(int up, double barrier, double s0, double s1, double iv, double* survival) {
+    return oracle::exact_bridge_api(up, barrier, s0, s1, iv, survival);
+}
+int oracle_smoothed_bridge(int up, double barrier, double s0, double s1, double h, double iv, double* out) {
+    return oracle::smoothed_bridge_api(up, barrier, s0, s1, h, iv, out);
+}
+}

@@ -1,0 +1,1067 @@
+// mcg_host.cu -- plan compiler and C ABI of the B200 Monte Carlo engine.
+//
+// mcg_plan_create turns an mcg_plan_desc into device-resident plan data:
+//   * the local-volatility time grid (LocalVolTimeGrid::compile,
+//     crates/pricing/src/engine/processes/local_vol.rs:167-237) and forward
+//     normalisers for the base and the two bumped spots
+//     (crates/pricing/src/engine/compile/local_vol.rs:14-102,
+//      crates/pricing/src/engine/processes/local_vol_valuation.rs:24-68),
+//   * the Brownian-bridge plan (crates/pricing/src/engine/sampling/bridge.rs:177-208,395-467)
+//     recompiled into a time-ordered program with a handful of live slots,
+//   * the RQMC scramble table, pre-applied to the Joe--Kuo directions on the device,
+//   * per-step constants (dt, sqrt(dt), grid time cell and weight, forward ratios).
+// mcg_plan_evaluate launches the path kernel and the tile reduction, merges
+// the per-scramble records and builds the estimates of
+// crates/pricing/src/engine/risk/report.rs:454-473.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <queue>
+#include <string>
+#include <vector>
+
+#include "mcg_kernels.cuh"
+
+namespace mcg {
+cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
+                           StatRecord* partials, uint32_t mask, ErrorWord* err, int detail,
+                           cudaStream_t stream, int& evolutions_out);
+cudaError_t launch_bs_path(const DevicePlan& P, bool single_terminal, uint64_t unit_begin, uint64_t units,
+                           uint32_t scrambles, StatRecord* partials, uint32_t mask, ErrorWord* err,
+                           int detail, cudaStream_t stream);
+__global__ void scramble_table_kernel(const uint32_t*, uint32_t, uint32_t, uint32_t, uint64_t, uint32_t*,
+                                      uint32_t*);
+__global__ void reduce_tiles_kernel(const StatRecord*, uint32_t, uint32_t, StatRecord*);
+__global__ void philox_normals_kernel(uint64_t, uint64_t, uint64_t, uint32_t, uint32_t, double*);
+__global__ void rqmc_words_kernel(const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint64_t,
+                                  uint64_t, uint32_t*);
+struct Pchip {
+    const double* t;
+    const double* v;
+    const double* d;
+    uint32_t n;
+    double slope;
+};
+__global__ void fp64_peak_kernel(double*, int);
+__global__ void ssvi_grid_kernel(Pchip, double, double, double, const double*, uint32_t,
+                                 const double*, uint32_t, double, double, double*, uint32_t*,
+                                 uint32_t*);
+}  // namespace mcg
+
+using namespace mcg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+mcg_status fail(mcg_status code, const std::string& message) {
+    g_last_error = message;
+    return code;
+}
+
+uint64_t bits_of(double v) {
+    uint64_t b;
+    std::memcpy(&b, &v, 8);
+    return b;
+}
+
+int64_t host_total_key(double x) {
+    int64_t b;
+    std::memcpy(&b, &x, 8);
+    return b ^ static_cast<int64_t>(static_cast<uint64_t>(b >> 63) >> 1);
+}
+
+// Index of the first element whose total-order key is >= key.
+size_t lower_bound_key(const std::vector<double>& v, int64_t key) {
+    size_t lo = 0, hi = v.size();
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (host_total_key(v[mid]) < key) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Log-linear discount curve (crates/pricing/src/market/curve.rs:156-205).
+struct HostCurve {
+    std::vector<double> t, logs;
+    double log_discount(double time) const {
+        if (time == 0.0) time = 0.0;
+        const int64_t key = host_total_key(time);
+        const size_t lo = lower_bound_key(t, key);
+        if (lo < t.size() && host_total_key(t[lo]) == key) return logs[lo];
+        const size_t right = lo < t.size() ? lo : t.size() - 1;
+        const size_t left = right - 1;
+        const double w = (time - t[left]) / (t[right] - t[left]);
+        return logs[left] + w * (logs[right] - logs[left]);
+    }
+};
+
+bool load_curve(const mcg_curve& c, HostCurve& out, const char* name, std::string& why) {
+    if (c.pillar_count < 2 || !c.times || !c.discount_factors) {
+        why = std::string(name) + ": needs at least two pillars";
+        return false;
+    }
+    if (c.times[0] != 0.0 || c.discount_factors[0] != 1.0) {
+        why = std::string(name) + ": the first pillar must be time 0 with discount 1";
+        return false;
+    }
+    for (uint32_t i = 0; i < c.pillar_count; ++i) {
+        if (!std::isfinite(c.times[i]) || !std::isfinite(c.discount_factors[i]) ||
+            c.discount_factors[i] <= 0.0 || (i > 0 && !(c.times[i] > c.times[i - 1]))) {
+            why = std::string(name) + ": pillar " + std::to_string(i) + " is invalid";
+            return false;
+        }
+    }
+    out.t.assign(c.times, c.times + c.pillar_count);
+    out.t[0] = 0.0;
+    out.logs.resize(c.pillar_count);
+    for (uint32_t i = 0; i < c.pillar_count; ++i) out.logs[i] = std::log(c.discount_factors[i]);
+    return true;
+}
+
+// ---------------------------------------------------------- bridge plan
+
+struct BridgeInstr {
+    bool terminal;
+    uint32_t node, left, right, rank;
+    double wl, wr, sd;
+};
+
+struct Candidate {
+    double variance, time;
+    uint32_t node, left, right;
+};
+
+// IntervalCandidate's order (bridge.rs:149-160): variance, then the earlier
+// time, then the smaller node wins.
+bool candidate_less(const Candidate& a, const Candidate& b) {
+    const int64_t va = host_total_key(a.variance), vb = host_total_key(b.variance);
+    if (va != vb) return va < vb;
+    const int64_t ta = host_total_key(a.time), tb = host_total_key(b.time);
+    if (ta != tb) return ta > tb;
+    return a.node > b.node;
+}
+
+bool best_candidate(const std::vector<double>& t, uint32_t left, uint32_t right, Candidate& best,
+                    bool& any) {
+    any = false;
+    if (right <= left + 1) return true;
+    const double den = t[right] - t[left];
+    for (uint32_t node = left + 1; node < right; ++node) {
+        const double variance = ((t[node] - t[left]) * (t[right] - t[node])) / den;
+        if (!std::isfinite(variance) || variance <= 0.0) return false;
+        const Candidate c{variance, t[node], node, left, right};
+        if (!any || candidate_less(best, c)) best = c;
+        any = true;
+    }
+    return true;
+}
+
+bool compile_bridge(const std::vector<double>& t, std::vector<BridgeInstr>& out) {
+    out.clear();
+    const uint32_t terminal = static_cast<uint32_t>(t.size() - 1);
+    out.push_back({true, terminal, 0, 0, 0, 0.0, 0.0, std::sqrt(t[terminal])});
+    auto cmp = [](const Candidate& a, const Candidate& b) { return candidate_less(a, b); };
+    std::priority_queue<Candidate, std::vector<Candidate>, decltype(cmp)> heap(cmp);
+    Candidate c;
+    bool any;
+    if (!best_candidate(t, 0, terminal, c, any)) return false;
+    if (any) heap.push(c);
+    uint32_t rank = 1;
+    while (!heap.empty()) {
+        const Candidate top = heap.top();
+        heap.pop();
+        const double den = t[top.right] - t[top.left];
+        out.push_back({false, top.node, top.left, top.right, rank++,
+                       (t[top.right] - t[top.node]) / den, (t[top.node] - t[top.left]) / den,
+                       std::sqrt(top.variance)});
+        if (!best_candidate(t, top.left, top.node, c, any)) return false;
+        if (any) heap.push(c);
+        if (!best_candidate(t, top.node, top.right, c, any)) return false;
+        if (any) heap.push(c);
+    }
+    return true;
+}
+
+// Time-ordered program of a bridge: node values are produced on demand (the
+// right bracketing node first), each value lives in a slot from its
+// computation to its last read.  Returns false when more than kMaxBridgeSlots
+// values would be live at once.
+bool bridge_program(const std::vector<double>& t, const std::vector<BridgeInstr>& instrs,
+                    std::vector<Op>& ops, uint32_t& slot_count) {
+    const uint32_t n = static_cast<uint32_t>(t.size());  // nodes 0..n-1
+    std::vector<int> by_node(n, -1);
+    for (size_t i = 0; i < instrs.size(); ++i) by_node[instrs[i].node] = static_cast<int>(i);
+    std::vector<char> done(n, 0);
+    done[0] = 1;
+    // (kind, node or step) in execution order
+    struct Raw {
+        int kind;
+        uint32_t a;
+    };
+    std::vector<Raw> order;
+    std::vector<uint32_t> stack;
+    for (uint32_t s = 0; s + 1 < n; ++s) {
+        // ensure(s + 1): walk up the right brackets until a computed node.
+        stack.clear();
+        uint32_t m = s + 1;
+        while (!done[m]) {
+            stack.push_back(m);
+            const BridgeInstr& in = instrs[by_node[m]];
+            if (in.terminal) break;
+            m = in.right;
+        }
+        while (!stack.empty()) {
+            const uint32_t node = stack.back();
+            stack.pop_back();
+            order.push_back({0, node});
+            done[node] = 1;
+        }
+        order.push_back({1, s});
+    }
+    // last use of every node value
+    std::vector<int> last(n, -1);
+    for (size_t i = 0; i < order.size(); ++i) {
+        if (order[i].kind == 0) {
+            const BridgeInstr& in = instrs[by_node[order[i].a]];
+            if (!in.terminal) {
+                last[in.left] = static_cast<int>(i);
+                last[in.right] = static_cast<int>(i);
+            }
+        } else {
+            last[order[i].a] = static_cast<int>(i);
+            last[order[i].a + 1] = static_cast<int>(i);
+        }
+    }
+    std::vector<int> slot_of(n, -1);
+    std::vector<int> free_slots;
+    uint32_t used = 0;
+    auto take = [&]() -> int {
+        if (!free_slots.empty()) {
+            const int sl = free_slots.back();
+            free_slots.pop_back();
+            return sl;
+        }
+        return static_cast<int>(used++);
+    };
+    slot_of[0] = take();  // W(0) = 0
+    ops.clear();
+    ops.push_back({kOpZero, slot_of[0], 0, 0, 0, 0, 0.0, 0.0, 0.0});  // W(0) = 0
+    for (size_t i = 0; i < order.size(); ++i) {
+        if (order[i].kind == 0) {
+            const uint32_t node = order[i].a;
+            const BridgeInstr& in = instrs[by_node[node]];
+            const int out = take();
+            slot_of[node] = out;
+            Op op{};
+            op.kind = in.terminal ? kOpTerminal : kOpInterior;
+            op.out = out;
+            op.left = in.terminal ? 0 : slot_of[in.left];
+            op.right = in.terminal ? 0 : slot_of[in.right];
+            op.rank = static_cast<int32_t>(in.rank);
+            op.wl = in.wl;
+            op.wr = in.wr;
+            op.sd = in.sd;
+            ops.push_back(op);
+        } else {
+            const uint32_t s = order[i].a;
+            Op op{};
+            op.kind = kOpStep;
+            op.left = slot_of[s];
+            op.right = slot_of[s + 1];
+            op.step = static_cast<int32_t>(s);
+            ops.push_back(op);
+        }
+        // release values whose last read was this op
+        auto release = [&](uint32_t node) {
+            if (last[node] == static_cast<int>(i) && slot_of[node] >= 0) {
+                free_slots.push_back(slot_of[node]);
+                slot_of[node] = -1;
+            }
+        };
+        if (order[i].kind == 0) {
+            const BridgeInstr& in = instrs[by_node[order[i].a]];
+            if (!in.terminal) {
+                release(in.left);
+                release(in.right);
+            }
+        } else {
+            release(order[i].a);
+            release(order[i].a + 1);
+        }
+    }
+    slot_count = used;
+    return used <= static_cast<uint32_t>(kMaxBridgeSlots);
+}
+
+template <class T>
+struct DeviceArray {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaError_t upload(const std::vector<T>& v) {
+        count = v.size();
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&ptr, count * sizeof(T));
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(ptr, v.data(), count * sizeof(T), cudaMemcpyHostToDevice);
+    }
+    cudaError_t alloc(size_t n) {
+        count = n;
+        return n ? cudaMalloc(&ptr, n * sizeof(T)) : cudaSuccess;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+    }
+};
+
+}  // namespace
+
+struct mcg_plan {
+    DevicePlan dp{};
+    bool single_terminal = false;
+    uint32_t product_count = 0;
+    uint32_t mask = 1u;  // components reduced on the device
+    uint32_t slots = 1;  // popcount(mask)
+    double total_variance = 0.0;
+    uint32_t grid_values = 0;
+    std::vector<ProductParams> products;
+    // device storage
+    DeviceArray<Op> ops;
+    DeviceArray<double> node_time, dt, sqrt_dt, inv_sqrt_dt, time_weight, fwd, ratio, obs_time,
+        obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, weights;
+    DeviceArray<int32_t> obs_of_node, time_cell;
+    DeviceArray<uint32_t> scr_dirs, scr_shift, directions;
+    DeviceArray<StatRecord> partials, records;
+    DeviceArray<ErrorWord> error;
+    uint32_t tiles = 0;
+
+    ~mcg_plan() {
+        ops.release();
+        node_time.release();
+        dt.release();
+        sqrt_dt.release();
+        inv_sqrt_dt.release();
+        time_weight.release();
+        fwd.release();
+        ratio.release();
+        obs_time.release();
+        obs_fwd.release();
+        obs_sqrt_step.release();
+        grid_t.release();
+        grid_x.release();
+        grid_v.release();
+        weights.release();
+        obs_of_node.release();
+        time_cell.release();
+        scr_dirs.release();
+        scr_shift.release();
+        directions.release();
+        partials.release();
+        records.release();
+        error.release();
+    }
+};
+
+namespace {
+
+#define MCG_CUDA(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? MCG_ERR_ALLOCATION : MCG_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+// LocalVolTimeGrid::compile, local_vol.rs:167-237.
+void compile_time_grid(std::vector<double> events, double maximum_step, std::vector<double>& nodes) {
+    std::sort(events.begin(), events.end(),
+              [](double a, double b) { return host_total_key(a) < host_total_key(b); });
+    events.erase(std::unique(events.begin(), events.end(),
+                             [](double a, double b) { return bits_of(a) == bits_of(b); }),
+                 events.end());
+    if (bits_of(events[0]) != 0) events.insert(events.begin(), 0.0);
+    nodes.assign(1, 0.0);
+    for (size_t i = 0; i + 1 < events.size(); ++i) {
+        const double left = events[i], right = events[i + 1];
+        if (right <= left) continue;
+        const double interval = right - left;
+        const double steps_f = std::ceil(interval / maximum_step);
+        const size_t steps = steps_f < 1.0 ? 1 : static_cast<size_t>(steps_f);
+        const double sub = interval / static_cast<double>(steps);
+        for (size_t k = 1; k < steps; ++k) nodes.push_back(left + sub * static_cast<double>(k));
+        nodes.push_back(right);
+    }
+}
+
+mcg_status validate_products(const mcg_plan_desc* d, std::vector<ProductParams>& out, bool& single) {
+    if (d->product_count == 0 || d->product_count > MCG_MAX_PRODUCTS || !d->products)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "product_count must be 1..8");
+    single = d->observation_count == 1;
+    for (uint32_t i = 0; i < d->product_count; ++i) {
+        const mcg_product_desc& p = d->products[i];
+        ProductParams q{};
+        q.kind = p.kind;
+        q.side = p.side;
+        q.strike = p.strike;
+        q.notional = p.notional;
+        q.digital_payout = p.digital_payout;
+        q.payout = p.payout;
+        q.barrier_direction = p.barrier_direction;
+        q.barrier_style = p.barrier_style;
+        q.has_rebate = p.has_rebate;
+        q.barrier = p.barrier;
+        q.rebate = p.rebate;
+        if (p.kind < MCG_PRODUCT_EUROPEAN || p.kind > MCG_PRODUCT_CONTINUOUS_BARRIER)
+            return fail(MCG_ERR_UNSUPPORTED, "product kind " + std::to_string(p.kind));
+        if (!(p.notional > 0.0) || !std::isfinite(p.strike) || p.strike <= 0.0)
+            return fail(MCG_ERR_INVALID_ARGUMENT, "product strike/notional must be positive");
+        if ((p.kind == MCG_PRODUCT_DISCRETE_BARRIER || p.kind == MCG_PRODUCT_CONTINUOUS_BARRIER) &&
+            !(p.barrier > 0.0))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "barrier level must be positive");
+        if (p.kind == MCG_PRODUCT_ASIAN && !p.observation_weights)
+            return fail(MCG_ERR_INVALID_ARGUMENT, "Asian product needs observation weights");
+        if (p.kind != MCG_PRODUCT_EUROPEAN && p.kind != MCG_PRODUCT_DIGITAL) single = false;
+        out.push_back(q);
+    }
+    return MCG_OK;
+}
+
+double resolve_gamma_bump(const mcg_plan_desc* d) {
+    return d->gamma_bump_relative ? d->spot * d->gamma_bump : d->gamma_bump;
+}
+
+mcg_status build(const mcg_plan_desc* d, mcg_plan& plan) {
+    if (!d) return fail(MCG_ERR_INVALID_ARGUMENT, "null descriptor");
+    if (d->abi_version != MCG_ABI_VERSION) return fail(MCG_ERR_INVALID_ARGUMENT, "abi_version mismatch");
+    if (d->model != MCG_MODEL_BLACK_SCHOLES && d->model != MCG_MODEL_LOCAL_VOLATILITY)
+        return fail(MCG_ERR_UNSUPPORTED, "model");
+    if (d->engine != MCG_ENGINE_PSEUDO && d->engine != MCG_ENGINE_RQMC)
+        return fail(MCG_ERR_UNSUPPORTED, "engine");
+    if (d->precision != MCG_PRECISION_F64)
+        return fail(MCG_ERR_UNSUPPORTED, "precision: this entry point evaluates FP64 plans");
+    if (!(d->spot > 0.0) || !std::isfinite(d->spot)) return fail(MCG_ERR_INVALID_ARGUMENT, "spot");
+    if (d->observation_count == 0 || !d->observation_times)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "observation_times");
+    for (uint32_t i = 0; i < d->observation_count; ++i) {
+        const double t = d->observation_times[i];
+        if (!std::isfinite(t) || t <= 0.0 || (i && !(t > d->observation_times[i - 1])))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "observation_times must be positive and increasing");
+    }
+    if (d->sampling_units == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "sampling_units");
+    if (d->engine == MCG_ENGINE_RQMC) {
+        if (d->scramble_count == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "scramble_count");
+        if ((d->sampling_units & (d->sampling_units - 1)) != 0 || d->sampling_units > (1ull << 32))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "points_per_scramble must be a power of two <= 2^32");
+    }
+    HostCurve rc, qc;
+    std::string why;
+    if (!load_curve(d->discount_curve, rc, "discount_curve", why)) return fail(MCG_ERR_MARKET, why);
+    if (!load_curve(d->dividend_curve, qc, "dividend_curve", why)) return fail(MCG_ERR_MARKET, why);
+    auto forward = [&](double spot, double t) {
+        return spot * std::exp(qc.log_discount(t) - rc.log_discount(t));
+    };
+    bool single;
+    mcg_status st = validate_products(d, plan.products, single);
+    if (st != MCG_OK) return st;
+    const uint32_t n = d->observation_count;
+    const double expiry = d->observation_times[n - 1];
+    const bool lv = d->model == MCG_MODEL_LOCAL_VOLATILITY;
+
+    DevicePlan& P = plan.dp;
+    P.model = d->model;
+    P.engine = d->engine;
+    P.precision = d->precision;
+    P.antithetic = d->antithetic != 0;
+    P.seed = d->master_seed;
+    P.units = d->sampling_units;
+    P.scramble_count = d->engine == MCG_ENGINE_RQMC ? d->scramble_count : 1;
+    P.observation_count = n;
+    P.product_count = d->product_count;
+    P.spot = d->spot;
+    P.vol = d->volatility;
+    P.expiry = expiry;
+    P.discount = std::exp(rc.log_discount(d->payment_time));
+    P.smoothing = d->smoothing_half_width;
+    if (!(P.smoothing >= 0.0) || !std::isfinite(P.smoothing))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "smoothing_half_width");
+    const bool risk = d->request_delta || d->request_gamma || d->request_vega;
+    // Bumps, crates/pricing/src/engine/compile/simulation.rs:481-502.
+    P.req_gamma = d->request_gamma != 0;
+    P.gamma_bump = resolve_gamma_bump(d);
+    if (d->request_gamma && (!std::isfinite(P.gamma_bump) || P.gamma_bump >= d->spot || P.gamma_bump <= 0.0))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "gamma bump must be positive and below spot");
+    P.spot_bump = d->request_gamma ? P.gamma_bump : std::min(d->spot * 1.0e-4, 0.5 * d->spot);
+    P.spot_variant[0] = d->spot;
+    P.spot_variant[1] = d->spot - P.spot_bump;
+    P.spot_variant[2] = d->spot + P.spot_bump;
+    bool has_continuous = false;
+    for (auto& q : plan.products) has_continuous |= q.kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+
+    uint32_t steps;
+    if (!lv) {
+        if (!(d->volatility >= 0.0) || !std::isfinite(d->volatility))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "volatility");
+        P.vol_bump = d->volatility == 0.0 ? 0.0 : std::min(1.0e-4, d->volatility * 0.5);
+        plan.total_variance = d->volatility * d->volatility * expiry;
+        P.zero_variance = plan.total_variance == 0.0;
+        P.risk = risk;
+        if (risk && !single) return fail(MCG_ERR_UNSUPPORTED, "Black-Scholes risk for path-dependent products");
+        std::vector<double> of(n), ot(n), sq(n);
+        double prev = 0.0;
+        for (uint32_t i = 0; i < n; ++i) {
+            ot[i] = d->observation_times[i];
+            of[i] = forward(d->spot, ot[i]);
+            sq[i] = std::sqrt(std::max(ot[i] - prev, 0.0));
+            prev = ot[i];
+        }
+        MCG_CUDA(plan.obs_time.upload(ot));
+        MCG_CUDA(plan.obs_fwd.upload(of));
+        MCG_CUDA(plan.obs_sqrt_step.upload(sq));
+        P.obs_time = plan.obs_time.ptr;
+        P.obs_fwd = plan.obs_fwd.ptr;
+        P.obs_sqrt_step = plan.obs_sqrt_step.ptr;
+        steps = n;
+        P.steps = n;
+        P.dimension = n;
+        plan.single_terminal = single;
+        plan.mask = 1u;
+        if (risk && single) plan.mask = 0x3ffu;
+        if (has_continuous) plan.mask |= 0xffu << 10;
+    } else {
+        if (d->request_vega || d->request_local_vega_nodes)
+            return fail(MCG_ERR_UNSUPPORTED, "local-volatility Vega runs in the adjoint entry point");
+        const mcg_local_variance_grid& g = d->local_variance;
+        if (g.time_count < 2 || g.log_moneyness_count < 2 || !g.time_nodes || !g.log_moneyness_nodes || !g.values)
+            return fail(MCG_ERR_MARKET, "local variance grid needs at least 2x2 nodes");
+        std::vector<double> gt(g.time_nodes, g.time_nodes + g.time_count);
+        std::vector<double> gx(g.log_moneyness_nodes, g.log_moneyness_nodes + g.log_moneyness_count);
+        std::vector<double> gv(g.values, g.values + static_cast<size_t>(g.time_count) * g.log_moneyness_count);
+        for (size_t i = 0; i < gt.size(); ++i)
+            if (!std::isfinite(gt[i]) || gt[i] < 0.0 || (i && !(gt[i] > gt[i - 1])))
+                return fail(MCG_ERR_MARKET, "grid time nodes must be finite, non-negative and increasing");
+        for (size_t i = 0; i < gx.size(); ++i)
+            if (!std::isfinite(gx[i]) || (i && !(gx[i] > gx[i - 1])))
+                return fail(MCG_ERR_MARKET, "grid log-moneyness nodes must be finite and increasing");
+        for (size_t i = 0; i < gv.size(); ++i)
+            if (!std::isfinite(gv[i]) || gv[i] < g.floor || gv[i] > g.cap)
+                return fail(MCG_ERR_MARKET, "grid value " + std::to_string(i) + " outside [floor, cap]");
+        if (bits_of(gt[0]) != 0 || bits_of(gt.back()) != bits_of(expiry))
+            return fail(MCG_ERR_MARKET, "grid time nodes must start at +0.0 and end at the expiry time");
+        double maximum_step = 0.0;
+        for (size_t i = 0; i + 1 < gt.size(); ++i) maximum_step = std::max(maximum_step, gt[i + 1] - gt[i]);
+        std::vector<double> events = gt;
+        events.insert(events.end(), d->observation_times, d->observation_times + n);
+        std::vector<double> nodes;
+        compile_time_grid(events, maximum_step, nodes);
+        steps = static_cast<uint32_t>(nodes.size() - 1);
+        P.steps = steps;
+        P.dimension = steps;
+        plan.total_variance = nodes.back() * g.cap;
+        std::vector<double> dtv(steps), sq(steps), isq(steps), tw(steps), fw(3 * (steps + 1)), ra(3 * steps);
+        std::vector<int32_t> tc(steps), oon(steps + 1, -1);
+        for (uint32_t s = 0; s < steps; ++s) {
+            dtv[s] = nodes[s + 1] - nodes[s];
+            sq[s] = std::sqrt(dtv[s]);
+            isq[s] = 1.0 / std::sqrt(dtv[s]);
+            // lower_cell under total_cmp, local_variance.rs:629-634
+            const int64_t key = host_total_key(nodes[s]);
+            const size_t lo = lower_bound_key(gt, key);
+            size_t c = (lo < gt.size() && host_total_key(gt[lo]) == key) ? lo : (lo == 0 ? 0 : lo - 1);
+            c = std::min(c, gt.size() - 2);
+            tc[s] = static_cast<int32_t>(c);
+            tw[s] = (nodes[s] - gt[c]) / (gt[c + 1] - gt[c]);
+        }
+        for (int k = 0; k < 3; ++k)
+            for (uint32_t i = 0; i <= steps; ++i) {
+                fw[k * (steps + 1) + i] = forward(P.spot_variant[k], nodes[i]);
+                if (!std::isfinite(fw[k * (steps + 1) + i]) || fw[k * (steps + 1) + i] <= 0.0)
+                    return fail(MCG_ERR_MARKET, "non-finite forward normaliser");
+            }
+        for (int k = 0; k < 3; ++k)
+            for (uint32_t s = 0; s < steps; ++s)
+                ra[k * steps + s] = fw[k * (steps + 1) + s + 1] / fw[k * (steps + 1) + s];
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint64_t b = bits_of(d->observation_times[i]);
+            uint32_t k = 0;
+            while (k <= steps && bits_of(nodes[k]) != b) ++k;
+            if (k > steps) return fail(MCG_ERR_MARKET, "observation time missing from the time grid");
+            oon[k] = static_cast<int32_t>(i);
+        }
+        MCG_CUDA(plan.node_time.upload(nodes));
+        MCG_CUDA(plan.dt.upload(dtv));
+        MCG_CUDA(plan.sqrt_dt.upload(sq));
+        MCG_CUDA(plan.inv_sqrt_dt.upload(isq));
+        MCG_CUDA(plan.time_weight.upload(tw));
+        MCG_CUDA(plan.time_cell.upload(tc));
+        MCG_CUDA(plan.fwd.upload(fw));
+        MCG_CUDA(plan.ratio.upload(ra));
+        MCG_CUDA(plan.obs_of_node.upload(oon));
+        MCG_CUDA(plan.grid_t.upload(gt));
+        MCG_CUDA(plan.grid_x.upload(gx));
+        MCG_CUDA(plan.grid_v.upload(gv));
+        P.node_time = plan.node_time.ptr;
+        P.dt = plan.dt.ptr;
+        P.sqrt_dt = plan.sqrt_dt.ptr;
+        P.inv_sqrt_dt = plan.inv_sqrt_dt.ptr;
+        P.time_weight = plan.time_weight.ptr;
+        P.time_cell = plan.time_cell.ptr;
+        P.fwd = plan.fwd.ptr;
+        P.ratio = plan.ratio.ptr;
+        P.obs_of_node = plan.obs_of_node.ptr;
+        P.grid_t = plan.grid_t.ptr;
+        P.grid_x = plan.grid_x.ptr;
+        P.grid_v = plan.grid_v.ptr;
+        P.nt = g.time_count;
+        P.nx = g.log_moneyness_count;
+        plan.grid_values = static_cast<uint32_t>(gv.size());
+        P.lv_bumps = d->request_delta || d->request_gamma;
+        plan.mask = 1u;
+        if (P.lv_bumps) plan.mask |= (1u << MCG_DELTA) | (1u << MCG_BUMP_DELTA);
+        if (d->request_gamma) plan.mask |= (1u << MCG_GAMMA) | (1u << MCG_BUMP_GAMMA);
+        if (has_continuous) plan.mask |= 0xffu << 10;
+        // Program: Brownian bridge on the time grid, or steps in order.
+        std::vector<Op> ops;
+        uint32_t slots = 1;
+        if (d->brownian_bridge) {
+            std::vector<BridgeInstr> instrs;
+            if (!compile_bridge(nodes, instrs)) return fail(MCG_ERR_BRIDGE, "invalid bridge grid");
+            if (!bridge_program(nodes, instrs, ops, slots))
+                return fail(MCG_ERR_UNSUPPORTED, "bridge needs more than 32 live values");
+        } else {
+            for (uint32_t s = 0; s < steps; ++s) {
+                Op op{};
+                op.kind = kOpStepDirect;
+                op.rank = static_cast<int32_t>(s);
+                op.step = static_cast<int32_t>(s);
+                ops.push_back(op);
+            }
+        }
+        // Every index a kernel reads from the program stays inside its buffer.
+        for (const Op& op : ops) {
+            const bool slots_ok = op.out >= 0 && op.out < static_cast<int32_t>(slots) && op.left >= 0 &&
+                                  op.left < static_cast<int32_t>(slots) && op.right >= 0 &&
+                                  op.right < static_cast<int32_t>(slots);
+            const bool rank_ok = op.rank >= 0 && op.rank < static_cast<int32_t>(steps);
+            const bool step_ok = op.step >= 0 && op.step < static_cast<int32_t>(steps);
+            if (!slots_ok || !rank_ok || !step_ok)
+                return fail(MCG_ERR_BRIDGE, "internal: path program index out of range");
+        }
+        MCG_CUDA(plan.ops.upload(ops));
+        P.ops = plan.ops.ptr;
+        P.op_count = static_cast<uint32_t>(ops.size());
+        P.slot_count = slots;
+        const size_t smem = (gv.size() + 2 * gx.size()) * sizeof(double) +
+                            static_cast<size_t>(slots) * kThreads * sizeof(double) +
+                            4 * kComponents * sizeof(Stat);
+        if (smem > 200 * 1024) return fail(MCG_ERR_UNSUPPORTED, "local-variance grid too large for shared memory");
+    }
+    // Asian weights: one device array per product, concatenated.
+    {
+        std::vector<double> w;
+        std::vector<size_t> offsets;
+        for (uint32_t i = 0; i < d->product_count; ++i) {
+            offsets.push_back(w.size());
+            if (d->products[i].observation_weights)
+                w.insert(w.end(), d->products[i].observation_weights, d->products[i].observation_weights + n);
+        }
+        MCG_CUDA(plan.weights.upload(w));
+        for (uint32_t i = 0; i < d->product_count; ++i) {
+            plan.products[i].weights = d->products[i].observation_weights ? plan.weights.ptr + offsets[i] : nullptr;
+            P.products[i] = plan.products[i];
+        }
+    }
+    plan.product_count = d->product_count;
+    plan.slots = static_cast<uint32_t>(__builtin_popcount(plan.mask));
+    // RQMC scramble table.
+    if (d->engine == MCG_ENGINE_RQMC) {
+        if (P.dimension > MCG_MAX_SOBOL_DIMENSION)
+            return fail(MCG_ERR_SOBOL_DIMENSION, "effective Sobol dimension exceeds 21201");
+        if (!d->sobol_directions || d->sobol_dimension_count < P.dimension)
+            return fail(MCG_ERR_SOBOL_DIMENSION, "sobol_directions cover fewer dimensions than the plan needs");
+        std::vector<uint32_t> dirs(d->sobol_directions, d->sobol_directions + static_cast<size_t>(P.dimension) * 32u);
+        MCG_CUDA(plan.directions.upload(dirs));
+        MCG_CUDA(plan.scr_dirs.alloc(static_cast<size_t>(P.scramble_count) * P.dimension * 32u));
+        MCG_CUDA(plan.scr_shift.alloc(static_cast<size_t>(P.scramble_count) * P.dimension));
+        const uint32_t total = P.scramble_count * P.dimension;
+        scramble_table_kernel<<<(total + 127) / 128, 128>>>(plan.directions.ptr, P.dimension, P.scramble_count,
+                                                           d->scramble_begin, P.seed, plan.scr_dirs.ptr,
+                                                           plan.scr_shift.ptr);
+        MCG_CUDA(cudaGetLastError());
+        MCG_CUDA(cudaDeviceSynchronize());
+        P.scr_dirs = plan.scr_dirs.ptr;
+        P.scr_shift = plan.scr_shift.ptr;
+    }
+    (void)steps;
+    // Reduction buffers.
+    plan.tiles = static_cast<uint32_t>((P.units + kThreads - 1) / kThreads);
+    MCG_CUDA(plan.partials.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * plan.product_count * kComponents));
+    MCG_CUDA(plan.records.alloc(static_cast<size_t>(P.scramble_count) * plan.product_count * kComponents));
+    MCG_CUDA(plan.error.alloc(1));
+    return MCG_OK;
+}
+
+// Statistics over ordered values, two passes
+// (CenteredMoment::from_ordered_values_two_pass, reduction.rs:99-122).
+struct HostStat {
+    double sum = 0.0, corr = 0.0;
+    uint64_t count = 0;
+    double mean = 0.0, m2 = 0.0;
+    double total() const { return sum + corr; }
+};
+
+void neumaier(double& s, double& c, double v) {
+    const double u = s + v;
+    if (std::fabs(s) >= std::fabs(v)) c += (s - u) + v;
+    else c += (v - u) + s;
+    s = u;
+}
+
+HostStat two_pass(const std::vector<double>& values) {
+    HostStat h;
+    if (values.empty()) return h;
+    double s = 0.0, c = 0.0;
+    for (double v : values) neumaier(s, c, v);
+    h.sum = s;
+    h.corr = c;
+    const double mean = (s + c) / static_cast<double>(values.size());
+    double qs = 0.0, qc = 0.0;
+    for (double v : values) {
+        const double dv = v - mean;
+        neumaier(qs, qc, dv * dv);
+    }
+    h.count = values.size();
+    h.mean = mean;
+    h.m2 = qs + qc;
+    return h;
+}
+
+mcg_estimate make_estimate(const HostStat& s, uint64_t units, double scale) {
+    const double inv = 1.0 / static_cast<double>(units);
+    const double value = s.total() * inv * scale;
+    const double var = s.count > 1 ? s.m2 / static_cast<double>(s.count - 1) : 0.0;
+    const double se = std::sqrt(var * inv) * std::fabs(scale);
+    const double hw = 1.959963984540054 * se;
+    return {value, se, value - hw, value + hw, units};
+}
+
+mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
+    if (!plan || !result) return fail(MCG_ERR_INVALID_ARGUMENT, "null plan or result");
+    if (result->product_capacity < plan->product_count || !result->products)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "result has too few product slots");
+    std::memset(&result->error, 0, sizeof(result->error));
+    DevicePlan& P = plan->dp;
+    const uint32_t slots = plan->slots;
+    ErrorWord init{~0ull, 0, 0, 0, 0};
+    MCG_CUDA(cudaMemcpyAsync(plan->error.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    cudaEvent_t t0, t1, tp;
+    MCG_CUDA(cudaEventCreate(&t0));
+    MCG_CUDA(cudaEventCreate(&t1));
+    MCG_CUDA(cudaEventCreate(&tp));
+    MCG_CUDA(cudaEventRecord(t0, stream));
+    // Kernels write records in compact (slot) order: remap through the mask.
+    uint32_t launches = 0;
+    cudaError_t e;
+    // Per-product partials use kComponents stride; reduce only masked slots below.
+    if (P.model == MCG_MODEL_LOCAL_VOLATILITY) {
+        int evolutions;
+        e = launch_lv_path(P, 0, P.units, P.scramble_count, plan->partials.ptr, plan->mask, plan->error.ptr, 0,
+                           stream, evolutions);
+    } else {
+        e = launch_bs_path(P, plan->single_terminal, 0, P.units, P.scramble_count, plan->partials.ptr,
+                           plan->mask, plan->error.ptr, 0, stream);
+    }
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("path kernel: ") + cudaGetErrorString(e));
+    ++launches;
+    MCG_CUDA(cudaEventRecord(tp, stream));
+    const uint32_t width = plan->product_count * kComponents;
+    reduce_tiles_kernel<<<dim3(width, P.scramble_count), 256, 0, stream>>>(plan->partials.ptr, plan->tiles,
+                                                                           width, plan->records.ptr);
+    MCG_CUDA(cudaGetLastError());
+    ++launches;
+    MCG_CUDA(cudaEventRecord(t1, stream));
+    std::vector<StatRecord> rec(static_cast<size_t>(P.scramble_count) * width);
+    ErrorWord ew;
+    MCG_CUDA(cudaMemcpyAsync(rec.data(), plan->records.ptr, rec.size() * sizeof(StatRecord),
+                             cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaMemcpyAsync(&ew, plan->error.ptr, sizeof(ew), cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0.0f, path_ms = 0.0f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventElapsedTime(&path_ms, t0, tp);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaEventDestroy(tp);
+    result->device_ms = ms;
+    result->path_kernel_ms = path_ms;
+    result->kernel_launches = launches;
+    if (ew.key != ~0ull) {
+        // Re-run the first failing unit alone to recover step and value bits.
+        const uint64_t unit = ew.key >> 8;
+        const uint32_t scrambles_for_detail = 1;
+        (void)scrambles_for_detail;
+        MCG_CUDA(cudaMemcpyAsync(plan->error.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        if (P.model == MCG_MODEL_LOCAL_VOLATILITY) {
+            int ev;
+            e = launch_lv_path(P, unit, 1, P.scramble_count, plan->partials.ptr, plan->mask, plan->error.ptr, 1,
+                               stream, ev);
+        } else {
+            e = launch_bs_path(P, plan->single_terminal, unit, 1, P.scramble_count, plan->partials.ptr,
+                               plan->mask, plan->error.ptr, 1, stream);
+        }
+        MCG_CUDA(cudaMemcpyAsync(&ew, plan->error.ptr, sizeof(ew), cudaMemcpyDeviceToHost, stream));
+        MCG_CUDA(cudaStreamSynchronize(stream));
+        result->error.code = static_cast<int32_t>(ew.key & 0xff);
+        result->error.sampling_unit = ew.key >> 8;
+        result->error.step = ew.step;
+        result->error.value_bits = ew.value_bits;
+        return fail(static_cast<mcg_status>(result->error.code),
+                    "sampling unit " + std::to_string(result->error.sampling_unit) + " failed");
+    }
+    const bool rqmc = P.engine == MCG_ENGINE_RQMC;
+    const uint64_t independent = rqmc ? P.scramble_count : P.units;
+    result->independent_sampling_units = independent;
+    result->evaluated_paths = P.units * (rqmc ? P.scramble_count : 1) * (P.antithetic ? 2 : 1);
+    result->time_steps = P.steps;
+    result->effective_dimension = P.dimension;
+    result->reduction_records = plan->tiles * P.scramble_count;
+    for (uint32_t k = 0; k < plan->product_count; ++k) {
+        mcg_product_result& r = result->products[k];
+        HostStat stats[kComponents];
+        for (int c = 0; c < kComponents; ++c) {
+            const bool active = plan->mask & (1u << c);
+            HostStat h;
+            if (!rqmc) {
+                if (active) {
+                    const StatRecord& s = rec[static_cast<size_t>(k) * kComponents + c];
+                    h = {s.sum, s.corr, static_cast<uint64_t>(s.count), s.mean, s.m2};
+                } else {
+                    h.count = P.units;
+                }
+            } else {
+                std::vector<double> reps(P.scramble_count, 0.0);
+                if (active)
+                    for (uint32_t s = 0; s < P.scramble_count; ++s) {
+                        const StatRecord& x = rec[(static_cast<size_t>(s) * plan->product_count + k) * kComponents + c];
+                        reps[s] = (x.sum + x.corr) / static_cast<double>(P.units);
+                    }
+                h = two_pass(reps);
+            }
+            stats[c] = h;
+            r.components[c] = {h.sum, h.corr, h.count, h.mean, h.m2};
+        }
+        r.price = make_estimate(stats[MCG_PRICE], independent, 1.0);
+        r.delta = make_estimate(stats[MCG_DELTA], independent, 1.0);
+        r.gamma = make_estimate(stats[MCG_GAMMA], independent, 1.0);
+        r.vega = make_estimate(stats[MCG_VEGA], independent, 1.0);
+        r.bump_delta = make_estimate(stats[MCG_BUMP_DELTA], independent, 1.0);
+        r.bump_gamma = make_estimate(stats[MCG_BUMP_GAMMA], independent, 1.0);
+        r.bump_vega = make_estimate(stats[MCG_BUMP_VEGA], independent, 1.0);
+        const HostStat& pr = stats[MCG_PRICE];
+        const double sv = pr.count > 1 ? pr.m2 / static_cast<double>(pr.count - 1) : 0.0;
+        r.sampling_variance = plan->total_variance == 0.0 ? 0.0 : sv;
+        r.estimator_variance = r.sampling_variance / static_cast<double>(independent);
+    }
+    if (plan->total_variance > 0.0 && independent < 2)
+        return fail(MCG_ERR_INSUFFICIENT_UNITS, "at least two independent sampling units are required");
+    return MCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t mcg_abi_version(void) { return MCG_ABI_VERSION; }
+
+const char* mcg_last_error(void) { return g_last_error.c_str(); }
+
+mcg_status mcg_plan_create(const mcg_plan_desc* desc, mcg_plan** out_plan) {
+    if (!out_plan) return fail(MCG_ERR_INVALID_ARGUMENT, "null out_plan");
+    *out_plan = nullptr;
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+        return fail(MCG_ERR_CUDA, "no CUDA device is visible");
+    auto* plan = new (std::nothrow) mcg_plan();
+    if (!plan) return fail(MCG_ERR_ALLOCATION, "plan allocation");
+    const mcg_status st = build(desc, *plan);
+    if (st != MCG_OK) {
+        delete plan;
+        return st;
+    }
+    *out_plan = plan;
+    return MCG_OK;
+}
+
+mcg_status mcg_plan_evaluate(mcg_plan* plan, void* stream, mcg_result* result) {
+    return evaluate(plan, static_cast<cudaStream_t>(stream), result);
+}
+
+void mcg_plan_destroy(mcg_plan* plan) { delete plan; }
+
+mcg_status mcg_price(const mcg_plan_desc* desc, void* stream, mcg_result* result) {
+    mcg_plan* plan = nullptr;
+    mcg_status st = mcg_plan_create(desc, &plan);
+    if (st != MCG_OK) return st;
+    st = mcg_plan_evaluate(plan, stream, result);
+    mcg_plan_destroy(plan);
+    return st;
+}
+
+mcg_status mcg_plan_shape(const mcg_plan* plan, uint32_t* time_steps, uint32_t* effective_dimension,
+                          uint32_t* grid_value_count) {
+    if (!plan) return fail(MCG_ERR_INVALID_ARGUMENT, "null plan");
+    if (time_steps) *time_steps = plan->dp.steps;
+    if (effective_dimension) *effective_dimension = plan->dp.dimension;
+    if (grid_value_count) *grid_value_count = plan->grid_values;
+    return MCG_OK;
+}
+
+mcg_status mcg_philox_normals(uint64_t master_seed, uint64_t first_unit, uint64_t count, uint32_t dimensions,
+                              uint32_t domain, double* out_host) {
+    if (!out_host || count == 0 || dimensions == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "empty request");
+    double* dev = nullptr;
+    MCG_CUDA(cudaMalloc(&dev, count * dimensions * sizeof(double)));
+    philox_normals_kernel<<<static_cast<unsigned>((count + 127) / 128), 128>>>(master_seed, first_unit, count,
+                                                                              dimensions, domain, dev);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out_host, dev, count * dimensions * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dev);
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+    return MCG_OK;
+}
+
+mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint64_t master_seed, uint32_t scramble,
+                          uint64_t first_point, uint64_t count, uint32_t* out_host) {
+    if (!directions || !out_host || count == 0 || dimensions == 0)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "empty request");
+    uint32_t *dirs = nullptr, *table = nullptr, *shifts = nullptr, *out = nullptr;
+    const uint32_t scrambles = scramble + 1;
+    MCG_CUDA(cudaMalloc(&dirs, static_cast<size_t>(dimensions) * 32 * 4));
+    MCG_CUDA(cudaMalloc(&table, static_cast<size_t>(scrambles) * dimensions * 32 * 4));
+    MCG_CUDA(cudaMalloc(&shifts, static_cast<size_t>(scrambles) * dimensions * 4));
+    MCG_CUDA(cudaMalloc(&out, count * dimensions * 4));
+    cudaError_t e = cudaMemcpy(dirs, directions, static_cast<size_t>(dimensions) * 32 * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const uint32_t total = scrambles * dimensions;
+        scramble_table_kernel<<<(total + 127) / 128, 128>>>(dirs, dimensions, scrambles, 0u, master_seed, table,
+                                                           shifts);
+        rqmc_words_kernel<<<static_cast<unsigned>((count + 127) / 128), 128>>>(table, shifts, dimensions, scramble,
+                                                                              first_point, count, out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out_host, out, count * dimensions * 4, cudaMemcpyDeviceToHost);
+    cudaFree(dirs);
+    cudaFree(table);
+    cudaFree(shifts);
+    cudaFree(out);
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+    return MCG_OK;
+}
+
+mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double* theta_values, uint32_t theta_count,
+                                        double terminal_slope, double rho, double eta, double gamma,
+                                        const double* time_nodes, uint32_t time_count,
+                                        const double* log_moneyness_nodes, uint32_t log_moneyness_count,
+                                        double floor, double cap, double* values, uint32_t* repairs) {
+    if (!theta_times || !theta_values || theta_count < 2 || !time_nodes || time_count < 2 ||
+        !log_moneyness_nodes || log_moneyness_count < 2 || !values)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "ssvi grid inputs");
+    if (!(gamma > 0.0 && gamma < 1.0) || !(eta > 0.0) || !(rho > -1.0 && rho < 1.0))
+        return fail(MCG_ERR_MARKET, "SSVI parameters outside their domain");
+    // PCHIP derivatives on the host (pchip.rs:178-237); one-off knot data.
+    const uint32_t n = theta_count;
+    std::vector<double> h(n - 1), s(n - 1), dv(n, 0.0);
+    for (uint32_t i = 0; i + 1 < n; ++i) {
+        h[i] = theta_times[i + 1] - theta_times[i];
+        s[i] = (theta_values[i + 1] - theta_values[i]) / h[i];
+    }
+    auto sg = [](double x) { return std::signbit(x) ? -1.0 : 1.0; };
+    auto endpoint = [&](double aw, double nw, double as, double ns) {
+        double dd = ((2.0 * aw + nw) * as - aw * ns) / (aw + nw);
+        if (sg(dd) != sg(as)) dd = 0.0;
+        else if (sg(as) != sg(ns) && std::fabs(dd) > 3.0 * std::fabs(as)) dd = 3.0 * as;
+        return dd;
+    };
+    if (n == 2) {
+        dv[0] = dv[1] = s[0];
+    } else {
+        dv[0] = endpoint(h[0], h[1], s[0], s[1]);
+        for (uint32_t i = 1; i + 1 < n; ++i) {
+            const double l = s[i - 1], r = s[i];
+            if (l == 0.0 || r == 0.0 || sg(l) != sg(r)) {
+                dv[i] = 0.0;
+            } else {
+                const double w1 = 2.0 * h[i] + h[i - 1];
+                const double w2 = h[i] + 2.0 * h[i - 1];
+                dv[i] = (w1 + w2) / (w1 / l + w2 / r);
+            }
+        }
+        dv[n - 1] = endpoint(h[n - 2], h[n - 3], s[n - 2], s[n - 3]);
+    }
+    double *dt = nullptr, *dvv = nullptr, *dd = nullptr, *tn = nullptr, *xn = nullptr, *out = nullptr;
+    uint32_t* counters = nullptr;
+    const size_t nv = static_cast<size_t>(time_count) * log_moneyness_count;
+    MCG_CUDA(cudaMalloc(&dt, n * 8));
+    MCG_CUDA(cudaMalloc(&dvv, n * 8));
+    MCG_CUDA(cudaMalloc(&dd, n * 8));
+    MCG_CUDA(cudaMalloc(&tn, time_count * 8));
+    MCG_CUDA(cudaMalloc(&xn, log_moneyness_count * 8));
+    MCG_CUDA(cudaMalloc(&out, nv * 8));
+    MCG_CUDA(cudaMalloc(&counters, 2 * 4));
+    cudaMemcpy(dt, theta_times, n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dvv, theta_values, n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dd, dv.data(), n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(tn, time_nodes, time_count * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(xn, log_moneyness_nodes, log_moneyness_count * 8, cudaMemcpyHostToDevice);
+    cudaMemset(counters, 0, 8);
+    Pchip pc{dt, dvv, dd, n, terminal_slope};
+    ssvi_grid_kernel<<<static_cast<unsigned>((nv + 127) / 128), 128>>>(pc, rho, eta, gamma, tn, time_count, xn,
+                                                                      log_moneyness_count, floor, cap, out,
+                                                                      counters, counters + 1);
+    cudaError_t e = cudaGetLastError();
+    uint32_t host_counters[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(values, out, nv * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(host_counters, counters, 8, cudaMemcpyDeviceToHost);
+    cudaFree(dt);
+    cudaFree(dvv);
+    cudaFree(dd);
+    cudaFree(tn);
+    cudaFree(xn);
+    cudaFree(out);
+    cudaFree(counters);
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+    if (repairs) *repairs = host_counters[0];
+    if (host_counters[1]) return fail(MCG_ERR_MARKET, "SSVI surface has a non-positive variance or density");
+    return MCG_OK;
+}
+
+mcg_status mcg_measure_fp64_peak(void* stream, double* tflops) {
+    if (!tflops) return fail(MCG_ERR_INVALID_ARGUMENT, "null output");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int device = 0, sms = 0;
+    MCG_CUDA(cudaGetDevice(&device));
+    MCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    double* sink = nullptr;
+    MCG_CUDA(cudaMalloc(&sink, 1024 * sizeof(double)));
+    const int iterations = 4096, threads = 256, blocks = sms * 8;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    fp64_peak_kernel<<<blocks, threads, 0, st>>>(sink, 16);  // warm-up
+    cudaEventRecord(a, st);
+    fp64_peak_kernel<<<blocks, threads, 0, st>>>(sink, iterations);
+    cudaEventRecord(b, st);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+    const double flops = 2.0 * 8.0 * 16.0 * iterations * static_cast<double>(threads) * blocks;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return MCG_OK;
+}
+
+}  // extern "C"

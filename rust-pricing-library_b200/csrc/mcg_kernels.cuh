@@ -1,0 +1,139 @@
+// mcg_kernels.cuh -- path kernels of the B200 Monte Carlo engine.
+//
+// One thread evaluates one sampling unit (a pseudo-random path or one Sobol
+// point of one scramble) from its normals to its 18 pathwise components, in
+// registers; a CTA reduces its units into one statistics record per component
+// with a fixed-shape tree.  This replaces the per-unit closures that
+// DeterministicExecutor runs on a Rayon pool
+// (crates/pricing/src/engine/mc/execution.rs:550-726) and the closures of
+// crates/pricing/src/engine/risk/valuation.rs:126-437 and
+// crates/pricing/src/engine/risk/local_vol.rs:24-420.
+#pragma once
+
+#include "mcg_device.cuh"
+#include "mcg_payoff.cuh"
+
+namespace mcg {
+
+constexpr int kThreads = 128;
+
+struct ErrorWord {
+    unsigned long long key;  // (unit << 8) | code, atomicMin over failing units
+    int32_t code;
+    uint32_t step;
+    unsigned long long unit;
+    unsigned long long value_bits;
+};
+
+__device__ __forceinline__ void report_error(ErrorWord* err, uint64_t unit, int code, uint32_t step,
+                                             double value, bool detail) {
+    atomicMin(&err->key, (static_cast<unsigned long long>(unit) << 8) | static_cast<unsigned>(code));
+    if (detail) {
+        err->code = code;
+        err->step = step;
+        err->unit = unit;
+        err->value_bits = static_cast<unsigned long long>(__double_as_longlong(value));
+    }
+}
+
+// ----------------------------------------------------------------- normals
+
+// Normal for dimension `dim` of one unit.  RQMC: scrambled Sobol word as
+// shift XOR the pre-applied scrambled directions of the set Gray-code bits
+// (qmc.rs:71-84,125-132: apply is GF(2)-linear, so apply(XOR v_k) =
+// XOR M v_k ^ shift); pseudo: Philox coordinate (unit, dim, Valuation).
+struct NormalSource {
+    int32_t rqmc;
+    uint64_t seed;
+    uint64_t unit;        // pseudo: sampling unit
+    uint32_t gray;        // rqmc: Gray code of the point
+    const uint32_t* dirs; // rqmc: this scramble's [dim][32] table
+    const uint32_t* shift;
+    uint32_t cached_block;
+    uint4 block;
+
+    __device__ __forceinline__ uint32_t word(uint32_t dim) {
+        if (rqmc) {
+            const uint32_t* d = dirs + static_cast<size_t>(dim) * 32u;
+            uint32_t x = __ldg(shift + dim);
+            uint32_t g = gray;
+            while (g) {
+                const int b = __ffs(g) - 1;
+                x ^= __ldg(d + b);
+                g &= g - 1u;
+            }
+            return x;
+        }
+        const uint32_t blk = dim >> 2;
+        if (blk != cached_block) {
+            block = philox_block(seed, unit, blk, 0u);
+            cached_block = blk;
+        }
+        return lane_of(block, dim & 3u);
+    }
+
+    __device__ __forceinline__ double normal(uint32_t dim) { return as241(open_unit(word(dim))); }
+};
+
+// ------------------------------------------------------- grid interpolation
+
+// LocalVarianceGrid::interpolate_with_hints, local_variance.rs:303-414: the
+// x cell is found by walking from the previous cell (the same answer as the
+// binary search under total_cmp), the time cell and weight of each step are
+// plan constants.
+struct GridView {
+    const double* v;        // nt x nx values (shared memory when they fit)
+    const double* x;        // nx nodes
+    const long long* xkey;  // total-order keys of the nodes
+    int nx;
+};
+
+__device__ __forceinline__ double interp_variance(const GridView& g, int tc, double tw, double xq,
+                                                  int& hint) {
+    double xv = xq;
+    if (xq < g.x[0]) xv = g.x[0];
+    else if (xq > g.x[g.nx - 1]) xv = g.x[g.nx - 1];
+    const long long k = total_key(xv);
+    int count = min(hint + 1, g.nx);
+    while (count < g.nx && g.xkey[count] <= k) ++count;
+    while (count > 0 && g.xkey[count - 1] > k) --count;
+    const int c = min(max(count - 1, 0), g.nx - 2);
+    hint = c;
+    const double xw = (xv - g.x[c]) / (g.x[c + 1] - g.x[c]);
+    const double* row = g.v + static_cast<size_t>(tc) * g.nx;
+    const double* next = row + g.nx;
+    const double lower = row[c] * (1.0 - xw) + row[c + 1] * xw;
+    const double upper = next[c] * (1.0 - xw) + next[c + 1] * xw;
+    return lower * (1.0 - tw) + upper * tw;
+}
+
+// ------------------------------------------------------- CTA reduction
+
+// Reduce NC component values of every thread into one record per component.
+// Fixed tree: warp butterfly with the lower lane on the left, then the warps
+// in index order -- deterministic for a given launch shape.
+template <int NC>
+__device__ __forceinline__ void cta_reduce_write(const double (&vals)[NC], bool valid,
+                                                 uint32_t mask, StatRecord* out, Stat* scratch) {
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    constexpr int kWarps = kThreads / 32;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        if (!(mask & (1u << (c % 32)))) continue;
+        const Stat s = warp_reduce_stat(stat_of(vals[c], valid));
+        if (lane == 0) scratch[warp * NC + c] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < NC && (mask & (1u << (threadIdx.x % 32)))) {
+        const int c = threadIdx.x;
+        Stat a = stat_merge(scratch[0 * NC + c], scratch[1 * NC + c]);
+        Stat b = stat_merge(scratch[2 * NC + c], scratch[3 * NC + c]);
+        static_assert(kWarps == 4, "tree below assumes four warps");
+        const Stat m = stat_merge(a, b);
+        out[c] = {m.sum, m.corr, m.count, m.mean, m.m2};
+    }
+    __syncthreads();
+}
+
+}  // namespace mcg

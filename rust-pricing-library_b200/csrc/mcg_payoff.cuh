@@ -1,0 +1,315 @@
+// mcg_payoff.cuh -- streaming payoff accumulators and the continuous-barrier
+// bridge of the path kernels.
+//
+// The reference evaluates each product as an opcode tape over stored
+// observations (crates/pricing/src/engine/payoff/tape.rs:953-1088, graphs from
+// crates/pricing/src/engine/payoff/compile.rs:35-474).  Here each product keeps
+// a few registers that are updated as the path reaches an observation, with
+// the same arithmetic in the same order, so no observation vector is stored.
+#pragma once
+
+#include "mcg_device.cuh"
+
+namespace mcg {
+
+constexpr double kLogMaxExpArgument = 6.564958884017094;  // barrier_bridge.rs:9
+constexpr double kLogMinPositive = -744.4400719213812;    // barrier_bridge.rs:10
+constexpr double kLn2 = 0.6931471805599453;
+
+// Streaming state of one product on one path.
+struct ProductAcc {
+    double a;        // Asian weighted sum, lookback extremum, barrier hit state
+    double log_sum;  // continuous barrier: sum of interval log survivals
+    double hit_log;  // smoothed continuous barrier: sum of log safety weights
+    double hit_prod; // smoothed continuous barrier: product of safety weights
+    double terminal; // last observed spot
+    uint32_t counts; // continuous barrier status counts: finite | zero<<8 | under<<16 | certain<<24 (saturating per byte is avoided by 10-bit fields below)
+    uint32_t counts2;
+    int32_t touched; // exact continuous barrier: an endpoint touched
+    int32_t initial_touched;
+};
+
+MCG_HD void acc_init(ProductAcc& s) {
+    s.a = 0.0;
+    s.log_sum = 0.0;
+    s.hit_log = 0.0;
+    s.hit_prod = 1.0;
+    s.terminal = 0.0;
+    s.counts = 0;
+    s.counts2 = 0;
+    s.touched = 0;
+    s.initial_touched = 0;
+}
+
+// Observation update: discrete products (compile.rs:159-202 Asian, :204-403
+// discrete barrier, :405-474 lookback, tape.rs:1038-1080 opcode semantics).
+MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
+                                           double spot, double smoothing, bool& failed) {
+    (void)failed;
+    s.terminal = spot;
+    switch (p.kind) {
+    case MCG_PRODUCT_ASIAN:
+        s.a = s.a + spot * p.weights[obs];
+        break;
+    case MCG_PRODUCT_LOOKBACK:
+        if (obs == 0) {
+            s.a = spot;
+        } else if (p.side == MCG_CALL) {
+            if (!(s.a >= spot)) s.a = spot;
+        } else {
+            if (!(s.a <= spot)) s.a = spot;
+        }
+        break;
+    case MCG_PRODUCT_DISCRETE_BARRIER: {
+        const double dist =
+            p.barrier_direction == MCG_BARRIER_UP ? spot - p.barrier : p.barrier - spot;
+        double w;
+        if (smoothing > 0.0) {
+            double comp;
+            w = smooth_indicator(smoothing, dist, comp).value;
+        } else {
+            w = dist >= 0.0 ? 1.0 : 0.0;
+        }
+        s.a = s.a + (1.0 - s.a) * w;
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// ---------------------------------------------- continuous barrier bridge
+
+// BarrierBridgeInterval::evaluate (exact), barrier_bridge.rs:446-528, with a
+// constant barrier; returns the status and log survival only.
+MCG_HD int exact_interval(bool up, double ls, double rs, double barrier,
+                                              double lv, double rv, double dt, double& log_surv,
+                                              bool& failed) {
+    if (!(ls > 0.0) || !isfinite(ls) || !(rs > 0.0) || !isfinite(rs) || !(lv >= 0.0) ||
+        !isfinite(lv) || !(rv >= 0.0) || !isfinite(rv)) {
+        failed = true;
+        log_surv = 0.0;
+        return 1;
+    }
+    const double lb = log(barrier);
+    const double ld = up ? lb - log(ls) : log(ls) - lb;
+    const double rd = up ? lb - log(rs) : log(rs) - lb;
+    if (ld <= 0.0 || rd <= 0.0) {
+        log_surv = -INFINITY;
+        return 1;  // touched
+    }
+    const double integrated = (0.5 * lv + 0.5 * rv) * dt;
+    if (!isfinite(integrated)) {
+        failed = true;
+        log_surv = 0.0;
+        return 1;
+    }
+    if (integrated == 0.0) {
+        log_surv = 0.0;
+        return 2;
+    }
+    const double le = kLn2 + log(ld) + log(rd) - log(integrated);
+    if (le >= kLogMaxExpArgument) {
+        log_surv = 0.0;
+        return 4;
+    }
+    if (le <= kLogMinPositive) {
+        log_surv = le;
+        return 3;
+    }
+    const double e = exp(le);
+    log_surv = log(-expm1(-e));
+    return 0;
+}
+
+// SmoothedBarrierBridgeEndpoint::evaluate, barrier_bridge.rs:160-215: the
+// safety weight and effective log distance of one endpoint (affine scale 1).
+MCG_HD void smooth_endpoint(bool up, double state, double barrier, double h,
+                                                double& safety, double& eld, bool& failed) {
+    if (!(state > 0.0) || !isfinite(state)) {
+        failed = true;
+        safety = 1.0;
+        eld = 1.0;
+        return;
+    }
+    const double sign = up ? 1.0 : -1.0;
+    const double signed_hit = 1.0 * sign * (state - barrier);
+    smooth_indicator(h, signed_hit, safety);
+    const SmoothD safe = smooth_positive_part(h, -signed_hit);
+    const double spot_barrier = 1.0 * barrier;
+    const double denominator = up ? spot_barrier - safe.value : spot_barrier + safe.value;
+    if (!isfinite(denominator) || denominator <= 0.0) {
+        failed = true;
+        eld = 1.0;
+        return;
+    }
+    eld = up ? -log1p(-safe.value / spot_barrier) : log1p(safe.value / spot_barrier);
+}
+
+// SmoothedBarrierBridgeInterval::evaluate, barrier_bridge.rs:276-357.
+MCG_HD int smooth_interval(double ld, double rd, double lv, double rv,
+                                               double dt, double& log_surv, bool& failed) {
+    if (!(lv >= 0.0) || !isfinite(lv) || !(rv >= 0.0) || !isfinite(rv)) {
+        failed = true;
+        log_surv = 0.0;
+        return 1;
+    }
+    if (ld == 0.0 || rd == 0.0) {
+        log_surv = -INFINITY;
+        return 1;
+    }
+    const double integrated = (0.5 * lv + 0.5 * rv) * dt;
+    if (!isfinite(integrated)) {
+        failed = true;
+        log_surv = 0.0;
+        return 1;
+    }
+    if (integrated == 0.0) {
+        log_surv = 0.0;
+        return 2;
+    }
+    const double le = kLn2 + log(ld) + log(rd) - log(integrated);
+    if (le >= kLogMaxExpArgument) {
+        log_surv = 0.0;
+        return 4;
+    }
+    if (le <= kLogMinPositive) {
+        log_surv = le;
+        return 3;
+    }
+    const double e = exp(le);
+    log_surv = log(-expm1(-e));
+    return 0;
+}
+
+MCG_HD void count_status(ProductAcc& s, int status) {
+    // 16-bit fields: counts = finite | zero << 16, counts2 = underflow | certain << 16.
+    if (status == 0) s.counts += 1u;
+    else if (status == 2) s.counts += 1u << 16;
+    else if (status == 3) s.counts2 += 1u;
+    else if (status == 4) s.counts2 += 1u << 16;
+}
+
+// One bridge interval of a continuous barrier (exact or smoothed).  Smoothed
+// endpoints are recomputed for each interval, as the reference does; the
+// smoothed right endpoint's safety weight is a hit factor.
+MCG_HD void barrier_interval(const ProductParams& p, ProductAcc& s,
+                                                 double h, double ls, double rs, double lv,
+                                                 double rv, double dt, bool& failed) {
+    const bool up = p.barrier_direction == MCG_BARRIER_UP;
+    if (!(dt > 0.0)) return;
+    double log_surv;
+    int status;
+    if (h > 0.0) {
+        double lsafe, rsafe, ld, rd;
+        smooth_endpoint(up, ls, p.barrier, h, lsafe, ld, failed);
+        smooth_endpoint(up, rs, p.barrier, h, rsafe, rd, failed);
+        status = smooth_interval(ld, rd, lv, rv, dt, log_surv, failed);
+        s.hit_log = s.hit_log + log(rsafe);
+        s.hit_prod = s.hit_prod * rsafe;
+    } else {
+        if (s.initial_touched) return;
+        status = exact_interval(up, ls, rs, p.barrier, lv, rv, dt, log_surv, failed);
+        if (status == 1) s.touched = 1;
+    }
+    s.log_sum += log_surv;
+    count_status(s, status);
+}
+
+// Start of a continuous-barrier path at the initial state (the spot).
+MCG_HD void barrier_begin(const ProductParams& p, ProductAcc& s, double h,
+                                              double spot, bool& failed) {
+    const bool up = p.barrier_direction == MCG_BARRIER_UP;
+    if (h > 0.0) {
+        double safety, eld;
+        smooth_endpoint(up, spot, p.barrier, h, safety, eld, failed);
+        s.hit_log = 0.0 + log(safety);
+        s.hit_prod = 1.0 * safety;
+    } else {
+        s.initial_touched = up ? spot >= p.barrier : spot <= p.barrier;
+    }
+}
+
+// Final survival and component 10..17 diagnostics,
+// crates/pricing/src/engine/payoff/barrier.rs:40-153,204-226.
+MCG_HD double barrier_finish(ProductAcc& s, double h, uint32_t intervals,
+                                                 double* diag) {
+    const double finite = static_cast<double>(s.counts & 0xffffu);
+    const double zero = static_cast<double>(s.counts >> 16);
+    const double under = static_cast<double>(s.counts2 & 0xffffu);
+    const double certain = static_cast<double>(s.counts2 >> 16);
+    if (h > 0.0) {
+        diag[0] = 1.0 - s.hit_prod;
+        diag[1] = 1.0 - 1.0;
+        diag[2] = 1.0 - exp(s.log_sum);
+        diag[3] = static_cast<double>(intervals);
+        diag[4] = finite;
+        diag[5] = zero;
+        diag[6] = under;
+        diag[7] = certain;
+        return exp(s.log_sum + s.hit_log);
+    }
+    const bool endpoint_touched = s.initial_touched || s.touched;
+    const double surv = exp(s.log_sum);
+    diag[0] = endpoint_touched ? 1.0 : 0.0;
+    diag[1] = 0.0;
+    diag[2] = endpoint_touched ? 0.0 : 1.0 - surv;
+    diag[3] = s.initial_touched ? 0.0 : static_cast<double>(intervals);
+    diag[4] = finite;
+    diag[5] = zero;
+    diag[6] = under;
+    diag[7] = certain;
+    return endpoint_touched ? 0.0 : surv;
+}
+
+// continuous_barrier_payoff_terms, barrier.rs:307-355 (value only).
+MCG_HD double barrier_value(const ProductParams& p, double terminal,
+                                                double survival) {
+    const bool call = p.side == MCG_CALL;
+    const double in = call ? terminal - p.strike : p.strike - terminal;
+    const double vanilla = fmax(in, 0.0) * p.notional;
+    const double rebate = p.has_rebate ? p.rebate : 0.0;
+    if (p.barrier_style == MCG_KNOCK_OUT) return rebate + survival * (vanilla - rebate);
+    return vanilla + survival * (rebate - vanilla);
+}
+
+// Undiscounted payoff of a discrete product from its accumulator.
+MCG_HD double acc_payoff(const ProductParams& p, const ProductAcc& s,
+                                             double smoothing) {
+    const bool call = p.side == MCG_CALL;
+    switch (p.kind) {
+    case MCG_PRODUCT_EUROPEAN: {
+        const double in = call ? s.terminal - p.strike : p.strike - s.terminal;
+        return (in >= 0.0 ? in : 0.0) * p.notional;
+    }
+    case MCG_PRODUCT_DIGITAL: {
+        const double dist = call ? s.terminal - p.strike : p.strike - s.terminal;
+        double ind;
+        if (smoothing > 0.0) {
+            double comp;
+            ind = smooth_indicator(smoothing, dist, comp).value;
+        } else {
+            ind = dist >= 0.0 ? 1.0 : 0.0;
+        }
+        const double base = p.digital_payout == MCG_DIGITAL_ASSET ? s.terminal * p.payout : p.payout;
+        return ind * base;
+    }
+    case MCG_PRODUCT_ASIAN:
+    case MCG_PRODUCT_LOOKBACK: {
+        const double in = call ? s.a - p.strike : p.strike - s.a;
+        return (in >= 0.0 ? in : 0.0) * p.notional;
+    }
+    case MCG_PRODUCT_DISCRETE_BARRIER: {
+        const double in = call ? s.terminal - p.strike : p.strike - s.terminal;
+        const double vanilla = (in >= 0.0 ? in : 0.0) * p.notional;
+        const double active = p.barrier_style == MCG_KNOCK_OUT ? 1.0 - s.a : s.a;
+        double value = vanilla * active;
+        if (p.has_rebate) value = value + (1.0 - active) * p.rebate;
+        return value;
+    }
+    default:
+        return 0.0;
+    }
+}
+
+}  // namespace mcg

@@ -1,0 +1,117 @@
+// mcg_plan.h -- device-resident plan layout shared by the host compiler
+// (mcg_host.cu) and the path kernels.
+//
+// A compiled plan is a set of flat device arrays plus this POD header, passed
+// to every kernel by value.  The layout follows the reference's immutable
+// SimulationPlan (crates/pricing/src/engine/plan/simulation.rs:73-119) and
+// LocalVolRuntime (:129-140), re-laid out for one-thread-per-path kernels:
+// per-step constants are structure-of-arrays in global memory (read uniformly
+// by a warp), the local-variance grid is staged in shared memory.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/mcg.h"
+
+namespace mcg {
+
+constexpr int kMaxProducts = MCG_MAX_PRODUCTS;
+constexpr int kComponents = MCG_PATHWISE_COMPONENTS;
+constexpr int kMaxBridgeSlots = 32;
+
+// Path program opcodes.  A Brownian-bridge plan is compiled into a
+// time-ordered program: node values are produced just before the step that
+// needs them and live in a few shared-memory slots (crates/pricing/src/engine/sampling/bridge.rs:272-311
+// evaluates the same linear map in heap order over a full array).
+enum OpKind : int32_t {
+    kOpTerminal = 0,  // W[out] = sd * z[rank]
+    kOpInterior = 1,  // W[out] = wl * W[left] + wr * W[right] + sd * z[rank]
+    kOpStep = 2,      // shock = (W[right] - W[left]) * inv_sqrt_dt[step]; evolve one step
+    kOpStepDirect = 3, // shock = z[rank]; evolve one step
+    kOpZero = 4        // W[out] = 0 (the bridge's time-zero node)
+};
+
+struct Op {
+    int32_t kind;
+    int32_t out;    // slot written (terminal/interior)
+    int32_t left;   // slot read
+    int32_t right;  // slot read
+    int32_t rank;   // normal dimension
+    int32_t step;   // step index (step ops)
+    double wl, wr, sd;
+};
+
+struct ProductParams {
+    int32_t kind, side;
+    double strike, notional;
+    int32_t digital_payout;
+    double payout;
+    int32_t barrier_direction, barrier_style, has_rebate;
+    double barrier, rebate;
+    const double* weights;  // device, one per observation (Asian)
+};
+
+struct DevicePlan {
+    int32_t model, engine, precision;
+    int32_t antithetic;
+    uint64_t seed;
+    uint64_t units;          // pseudo: units; rqmc: points per scramble
+    uint32_t scramble_count;
+    uint32_t steps;          // time steps of one path
+    uint32_t observation_count;
+    uint32_t product_count;
+    uint32_t dimension;      // Sobol / Philox dimensions per path
+    int32_t zero_variance;   // BS with total variance 0: normals are zero
+
+    // program
+    const Op* ops;
+    uint32_t op_count;
+    uint32_t slot_count;
+
+    // per-step constants (steps entries unless noted)
+    const double* node_time;     // steps + 1
+    const double* dt;
+    const double* sqrt_dt;
+    const double* inv_sqrt_dt;
+    const int32_t* obs_of_node;  // steps + 1: observation index or -1
+    const int32_t* time_cell;    // LV: grid time cell per step
+    const double* time_weight;   // LV: grid time weight per step
+    const double* fwd;           // LV: 3 x (steps + 1) forward normalizers (base, down, up)
+    const double* ratio;         // LV: 3 x steps forward ratios F[i+1]/F[i]
+    const float* fwd_f;          // FP32 copies for the bulk path
+    const float* ratio_f;
+
+    // Black--Scholes observation data (observation_count entries)
+    const double* obs_time;
+    const double* obs_fwd;
+    const double* obs_sqrt_step;
+    double spot, vol, discount, expiry;
+    double spot_variant[3];      // base, down, up spots
+
+    // local-variance grid
+    const double* grid_t;
+    const double* grid_x;
+    const double* grid_v;
+    const float* grid_v_f;
+    uint32_t nt, nx;
+
+    // RQMC: scrambled direction table [scramble][dim][32] and shifts [scramble][dim]
+    const uint32_t* scr_dirs;
+    const uint32_t* scr_shift;
+
+    // risk
+    int32_t risk;          // BS: pathwise values with bumps
+    int32_t req_gamma;
+    int32_t lv_bumps;      // LV: CRN delta/gamma evolutions
+    double gamma_bump, spot_bump, vol_bump;
+    double smoothing;
+
+    ProductParams products[kMaxProducts];
+};
+
+// Per-CTA statistics record of one component.
+struct StatRecord {
+    double sum, corr, count, mean, m2;
+};
+
+}  // namespace mcg

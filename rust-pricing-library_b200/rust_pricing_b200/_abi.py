@@ -1,0 +1,137 @@
+"""ctypes mirror of include/mcg.h (the engine's C ABI).
+
+The structures here must match the header field for field; the layout test in
+tests/test_abi.py compares their sizes with the C compiler's.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+ABI_VERSION = 1
+PATHWISE_COMPONENTS = 18
+
+PRICE, DELTA, VEGA, GAMMA = 0, 1, 2, 3
+BUMP_DELTA, DELTA_DIFFERENCE, BUMP_VEGA, VEGA_DIFFERENCE = 4, 5, 6, 7
+BUMP_GAMMA, GAMMA_DIFFERENCE = 8, 9
+BARRIER_ENDPOINT_HIT, BARRIER_DIVIDEND_JUMP_HIT, BARRIER_BRIDGE_HIT_WEIGHT = 10, 11, 12
+BARRIER_INTERVAL_COUNT, BARRIER_FINITE_CORRECTION_COUNT = 13, 14
+BARRIER_ZERO_VARIANCE_COUNT, BARRIER_SURVIVAL_UNDERFLOW_COUNT = 15, 16
+BARRIER_CERTAIN_SURVIVAL_COUNT = 17
+
+MODEL_BLACK_SCHOLES, MODEL_LOCAL_VOLATILITY = 0, 1
+ENGINE_PSEUDO, ENGINE_RQMC = 0, 1
+PRECISION_F64, PRECISION_F32_BULK = 0, 1
+(PRODUCT_EUROPEAN, PRODUCT_DIGITAL, PRODUCT_ASIAN, PRODUCT_LOOKBACK,
+ PRODUCT_DISCRETE_BARRIER, PRODUCT_CONTINUOUS_BARRIER, PRODUCT_AMERICAN) = range(7)
+CALL, PUT = 0, 1
+BARRIER_UP, BARRIER_DOWN = 0, 1
+KNOCK_OUT, KNOCK_IN = 0, 1
+DIGITAL_CASH, DIGITAL_ASSET = 0, 1
+
+STATUS_NAMES = {
+    0: "ok", 1: "invalid_argument", 2: "unsupported", 3: "cuda", 4: "allocation",
+    5: "insufficient_sampling_units", 6: "non_finite_state", 7: "invalid_surface_query",
+    8: "sobol_dimension", 9: "brownian_bridge", 10: "barrier_bridge", 11: "market",
+    12: "lsm", 13: "timeout", 14: "not_built",
+}
+
+_dp = C.POINTER(C.c_double)
+_up = C.POINTER(C.c_uint32)
+
+
+class Curve(C.Structure):
+    _fields_ = [("pillar_count", C.c_uint32), ("times", _dp), ("discount_factors", _dp)]
+
+
+class LocalVarianceGrid(C.Structure):
+    _fields_ = [
+        ("time_count", C.c_uint32), ("log_moneyness_count", C.c_uint32),
+        ("time_nodes", _dp), ("log_moneyness_nodes", _dp), ("values", _dp),
+        ("floor", C.c_double), ("cap", C.c_double),
+    ]
+
+
+class ProductDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("side", C.c_int32), ("strike", C.c_double), ("notional", C.c_double),
+        ("digital_payout", C.c_int32), ("payout", C.c_double),
+        ("barrier_direction", C.c_int32), ("barrier_style", C.c_int32), ("has_rebate", C.c_int32),
+        ("barrier", C.c_double), ("rebate", C.c_double),
+        ("observation_weights", _dp),
+    ]
+
+
+class PlanDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_uint32), ("model", C.c_int32), ("engine", C.c_int32),
+        ("precision", C.c_int32),
+        ("master_seed", C.c_uint64), ("sampling_units", C.c_uint64),
+        ("scramble_count", C.c_uint32), ("scramble_begin", C.c_uint32), ("antithetic", C.c_int32),
+        ("brownian_bridge", C.c_int32),
+        ("reduction_block_size", C.c_uint64),
+        ("sobol_dimension_count", C.c_uint32), ("sobol_directions", _up),
+        ("spot", C.c_double), ("discount_curve", Curve), ("dividend_curve", Curve),
+        ("volatility", C.c_double), ("local_variance", LocalVarianceGrid),
+        ("observation_count", C.c_uint32), ("observation_times", _dp), ("payment_time", C.c_double),
+        ("product_count", C.c_uint32), ("products", C.POINTER(ProductDesc)),
+        ("request_delta", C.c_int32), ("request_gamma", C.c_int32), ("request_vega", C.c_int32),
+        ("request_local_vega_nodes", C.c_int32), ("gamma_bump_relative", C.c_int32),
+        ("gamma_bump", C.c_double), ("smoothing_half_width", C.c_double),
+        ("checkpoint_interval", C.c_uint32),
+    ]
+
+
+class Statistics(C.Structure):
+    _fields_ = [("sum", C.c_double), ("correction", C.c_double), ("count", C.c_uint64),
+                ("mean", C.c_double), ("second_moment", C.c_double)]
+
+    def total(self) -> float:
+        return self.sum + self.correction
+
+
+class Estimate(C.Structure):
+    _fields_ = [("value", C.c_double), ("standard_error", C.c_double),
+                ("confidence_lower", C.c_double), ("confidence_upper", C.c_double),
+                ("effective_sampling_units", C.c_uint64)]
+
+
+class ProductResult(C.Structure):
+    _fields_ = [
+        ("components", Statistics * PATHWISE_COMPONENTS),
+        ("price", Estimate), ("delta", Estimate), ("gamma", Estimate), ("vega", Estimate),
+        ("bump_delta", Estimate), ("bump_gamma", Estimate), ("bump_vega", Estimate),
+        ("sampling_variance", C.c_double), ("estimator_variance", C.c_double),
+    ]
+
+
+class ErrorRecord(C.Structure):
+    _fields_ = [("code", C.c_int32), ("step", C.c_uint32), ("sampling_unit", C.c_uint64),
+                ("value_bits", C.c_uint64)]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("product_capacity", C.c_uint32), ("products", C.POINTER(ProductResult)),
+        ("node_capacity", C.c_uint32), ("local_vega_nodes", C.POINTER(Statistics)),
+        ("local_vega_node_estimates", C.POINTER(Estimate)),
+        ("independent_sampling_units", C.c_uint64), ("evaluated_paths", C.c_uint64),
+        ("time_steps", C.c_uint32), ("effective_dimension", C.c_uint32),
+        ("reduction_records", C.c_uint32), ("kernel_launches", C.c_uint32),
+        ("device_ms", C.c_float), ("path_kernel_ms", C.c_float), ("error", ErrorRecord),
+    ]
+
+
+class ResultBuffers:
+    """Caller-owned result storage for `products` products and `nodes` node entries."""
+
+    def __init__(self, products: int, nodes: int = 0):
+        self.products = (ProductResult * max(products, 1))()
+        self.node_stats = (Statistics * nodes)() if nodes else None
+        self.node_estimates = (Estimate * nodes)() if nodes else None
+        self.result = Result()
+        self.result.product_capacity = products
+        self.result.products = C.cast(self.products, C.POINTER(ProductResult))
+        self.result.node_capacity = nodes
+        if nodes:
+            self.result.local_vega_nodes = C.cast(self.node_stats, C.POINTER(Statistics))
+            self.result.local_vega_node_estimates = C.cast(self.node_estimates, C.POINTER(Estimate))

@@ -1,0 +1,116 @@
+"""Loader of the engine library (libmcg.so, include/mcg.h).
+
+The engine has no CPU fallback: if the library is missing or cannot be loaded,
+every entry point raises.  `build()` (rust-pricing-library_b200/build.py)
+compiles it in place for sm_100a.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import _abi as A
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(HERE, "libmcg.so")
+
+EXPORTS = (
+    "mcg_abi_version", "mcg_last_error", "mcg_plan_create", "mcg_plan_evaluate", "mcg_price",
+    "mcg_plan_destroy", "mcg_plan_shape", "mcg_philox_normals", "mcg_rqmc_words",
+    "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak",
+)
+
+_lib = None
+
+
+class EngineError(RuntimeError):
+    """An mcg_status other than MCG_OK, with the library's message."""
+
+    def __init__(self, status: int, message: str, error: A.ErrorRecord | None = None):
+        self.status = status
+        self.name = A.STATUS_NAMES.get(status, str(status))
+        self.error = error
+        detail = ""
+        if error is not None and error.code:
+            detail = (f" (sampling unit {error.sampling_unit}, step {error.step}, "
+                      f"value bits 0x{error.value_bits:016x})")
+        super().__init__(f"{self.name}: {message}{detail}")
+
+
+def library() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBRARY_PATH):
+        raise EngineError(14, f"engine library {LIBRARY_PATH} is not built; run build()")
+    lib = C.CDLL(LIBRARY_PATH)
+    u32, u64, dbl, vp = C.c_uint32, C.c_uint64, C.c_double, C.c_void_p
+    lib.mcg_abi_version.restype = u32
+    lib.mcg_last_error.restype = C.c_char_p
+    lib.mcg_plan_create.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(vp)]
+    lib.mcg_plan_create.restype = C.c_int
+    lib.mcg_plan_evaluate.argtypes = [vp, vp, C.POINTER(A.Result)]
+    lib.mcg_plan_evaluate.restype = C.c_int
+    lib.mcg_price.argtypes = [C.POINTER(A.PlanDesc), vp, C.POINTER(A.Result)]
+    lib.mcg_price.restype = C.c_int
+    lib.mcg_plan_destroy.argtypes = [vp]
+    lib.mcg_plan_shape.argtypes = [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
+    lib.mcg_plan_shape.restype = C.c_int
+    lib.mcg_philox_normals.argtypes = [u64, u64, u64, u32, u32, C.POINTER(dbl)]
+    lib.mcg_philox_normals.restype = C.c_int
+    lib.mcg_rqmc_words.argtypes = [C.POINTER(u32), u32, u64, u32, u64, u64, C.POINTER(u32)]
+    lib.mcg_rqmc_words.restype = C.c_int
+    dp = C.POINTER(dbl)
+    lib.mcg_ssvi_local_variance_grid.argtypes = [dp, dp, u32, dbl, dbl, dbl, dbl, dp, u32, dp, u32,
+                                                 dbl, dbl, dp, C.POINTER(u32)]
+    lib.mcg_ssvi_local_variance_grid.restype = C.c_int
+    lib.mcg_measure_fp64_peak.argtypes = [vp, C.POINTER(dbl)]
+    lib.mcg_measure_fp64_peak.restype = C.c_int
+    if lib.mcg_abi_version() != A.ABI_VERSION:
+        raise EngineError(1, "engine library ABI version mismatch")
+    _lib = lib
+    return lib
+
+
+def check(status: int, error: A.ErrorRecord | None = None) -> None:
+    if status != 0:
+        raise EngineError(status, library().mcg_last_error().decode(), error)
+
+
+class Plan:
+    """An mcg_plan handle: compile once, evaluate many times."""
+
+    def __init__(self, spec):
+        self.spec = spec
+        self.desc = spec.desc()
+        self.handle = C.c_void_p()
+        check(library().mcg_plan_create(C.byref(self.desc), C.byref(self.handle)))
+        self.nodes = spec.grid_value_count() * len(spec.products) if spec.request_local_vega_nodes else 0
+
+    def evaluate(self, stream: int = 0) -> A.ResultBuffers:
+        buf = A.ResultBuffers(len(self.spec.products), self.nodes)
+        status = library().mcg_plan_evaluate(self.handle, C.c_void_p(stream), C.byref(buf.result))
+        check(status, buf.result.error)
+        return buf
+
+    def shape(self):
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(library().mcg_plan_shape(self.handle, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def close(self) -> None:
+        if self.handle:
+            library().mcg_plan_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,170 @@
+"""Builds `mcg_plan_desc` descriptors (include/mcg.h) from Python values.
+
+A `PlanSpec` owns every array the descriptor points at, so the descriptor stays
+valid for as long as the spec lives.  This is the data the reference keeps in
+its compiled `SimulationPlan` (crates/pricing/src/engine/plan/simulation.rs:73-119):
+market curves, model, observation times, products and the risk request.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi as A
+from . import sobol
+
+
+def _f64(values) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.float64))
+
+
+def _ptr(array: Optional[np.ndarray], ctype=C.c_double):
+    if array is None:
+        return C.POINTER(ctype)()
+    return array.ctypes.data_as(C.POINTER(ctype))
+
+
+@dataclass
+class ProductSpec:
+    kind: int
+    side: int = A.CALL
+    strike: float = 100.0
+    notional: float = 1.0
+    digital_payout: int = A.DIGITAL_CASH
+    payout: float = 1.0
+    barrier_direction: int = A.BARRIER_DOWN
+    barrier_style: int = A.KNOCK_OUT
+    barrier: float = 0.0
+    rebate: Optional[float] = None
+    weights: Optional[Sequence[float]] = None
+
+
+@dataclass
+class LocalVarianceSpec:
+    time_nodes: Sequence[float]
+    log_moneyness_nodes: Sequence[float]
+    values: np.ndarray
+    floor: float = 1e-8
+    cap: float = 4.0
+
+
+@dataclass
+class PlanSpec:
+    observation_times: Sequence[float]
+    products: Sequence[ProductSpec]
+    model: int = A.MODEL_BLACK_SCHOLES
+    engine: int = A.ENGINE_PSEUDO
+    precision: int = A.PRECISION_F64
+    master_seed: int = 0x0123456789ABCDEF
+    sampling_units: int = 1 << 14
+    scramble_count: int = 16
+    scramble_begin: int = 0
+    antithetic: bool = False
+    brownian_bridge: bool = False
+    reduction_block_size: int = 4096
+    spot: float = 100.0
+    discount_times: Sequence[float] = (0.0, 1.0)
+    discount_factors: Sequence[float] = (1.0, float(np.exp(-0.03)))
+    dividend_times: Sequence[float] = (0.0, 1.0)
+    dividend_factors: Sequence[float] = (1.0, float(np.exp(-0.01)))
+    volatility: float = 0.2
+    local_variance: Optional[LocalVarianceSpec] = None
+    payment_time: Optional[float] = None
+    request_delta: bool = False
+    request_gamma: bool = False
+    request_vega: bool = False
+    request_local_vega_nodes: bool = False
+    gamma_bump_relative: bool = True
+    gamma_bump: float = 0.01
+    smoothing_half_width: float = 0.0
+    checkpoint_interval: int = 16
+    _keep: list = field(default_factory=list, repr=False)
+
+    def steps(self) -> int:
+        return len(self.observation_times)
+
+    def desc(self) -> A.PlanDesc:
+        keep = self._keep
+        keep.clear()
+        d = A.PlanDesc()
+        d.abi_version = A.ABI_VERSION
+        d.model = self.model
+        d.engine = self.engine
+        d.precision = self.precision
+        d.master_seed = self.master_seed & 0xFFFFFFFFFFFFFFFF
+        d.sampling_units = self.sampling_units
+        d.scramble_count = self.scramble_count
+        d.scramble_begin = self.scramble_begin
+        d.antithetic = int(self.antithetic)
+        d.brownian_bridge = int(self.brownian_bridge)
+        d.reduction_block_size = self.reduction_block_size
+        if self.engine == A.ENGINE_RQMC:
+            dims = self._dimension_hint()
+            words = np.ascontiguousarray(sobol.direction_words(dims))
+            keep.append(words)
+            d.sobol_dimension_count = dims
+            d.sobol_directions = _ptr(words, C.c_uint32)
+        d.spot = self.spot
+        for name, times, factors in (("discount_curve", self.discount_times, self.discount_factors),
+                                     ("dividend_curve", self.dividend_times, self.dividend_factors)):
+            t, f = _f64(times), _f64(factors)
+            keep += [t, f]
+            curve = A.Curve(len(t), _ptr(t), _ptr(f))
+            setattr(d, name, curve)
+        d.volatility = self.volatility
+        if self.local_variance is not None:
+            g = self.local_variance
+            t, x, v = _f64(g.time_nodes), _f64(g.log_moneyness_nodes), _f64(g.values).ravel()
+            keep += [t, x, v]
+            d.local_variance = A.LocalVarianceGrid(len(t), len(x), _ptr(t), _ptr(x), _ptr(v),
+                                                   g.floor, g.cap)
+        obs = _f64(self.observation_times)
+        keep.append(obs)
+        d.observation_count = len(obs)
+        d.observation_times = _ptr(obs)
+        d.payment_time = float(obs[-1] if self.payment_time is None else self.payment_time)
+        products = (A.ProductDesc * len(self.products))()
+        for i, p in enumerate(self.products):
+            q = products[i]
+            q.kind, q.side, q.strike, q.notional = p.kind, p.side, p.strike, p.notional
+            q.digital_payout, q.payout = p.digital_payout, p.payout
+            q.barrier_direction, q.barrier_style = p.barrier_direction, p.barrier_style
+            q.barrier = p.barrier
+            q.has_rebate = int(p.rebate is not None)
+            q.rebate = 0.0 if p.rebate is None else p.rebate
+            if p.weights is not None:
+                w = _f64(p.weights)
+                keep.append(w)
+                q.observation_weights = _ptr(w)
+        keep.append(products)
+        d.product_count = len(self.products)
+        d.products = C.cast(products, C.POINTER(A.ProductDesc))
+        d.request_delta = int(self.request_delta)
+        d.request_gamma = int(self.request_gamma)
+        d.request_vega = int(self.request_vega)
+        d.request_local_vega_nodes = int(self.request_local_vega_nodes)
+        d.gamma_bump_relative = int(self.gamma_bump_relative)
+        d.gamma_bump = self.gamma_bump
+        d.smoothing_half_width = self.smoothing_half_width
+        d.checkpoint_interval = self.checkpoint_interval
+        keep.append(d)
+        return d
+
+    def _dimension_hint(self) -> int:
+        """Sobol dimensions the plan may need (time steps, including substeps)."""
+        if self.model == A.MODEL_LOCAL_VOLATILITY and self.local_variance is not None:
+            union = np.union1d(np.asarray(self.local_variance.time_nodes, dtype=np.float64),
+                               np.asarray(self.observation_times, dtype=np.float64))
+            gaps = np.diff(np.asarray(self.local_variance.time_nodes, dtype=np.float64))
+            step = float(gaps.max())
+            count = int(np.sum(np.maximum(1, np.ceil(np.diff(np.concatenate([[0.0], union])) / step))))
+            return min(max(count + 8, 1), sobol.DIMENSIONS)
+        return min(len(self.observation_times), sobol.DIMENSIONS)
+
+    def grid_value_count(self) -> int:
+        if self.local_variance is None:
+            return 0
+        return len(self.local_variance.time_nodes) * len(self.local_variance.log_moneyness_nodes)

@@ -1,0 +1,88 @@
+"""Extracts golden vectors from the reference's fixtures into tests/golden/.
+
+Run in the build container, where the reference checkout is mounted at
+/root/reference (it is not present on GPU machines).  The extracted JSON files
+are committed; the tests only read them.
+
+* replay_european_bs.json  -- fixtures/replay/european_bs-windows-x86_64.json:
+  request parameters and result values of the pseudo and RQMC full-risk cases.
+* bs_analytical.json       -- fixtures/acceptance/european_bs_analytical.csv.
+* path_dependence.json     -- fixtures/path-dependence/reference-cases-v0.1.json
+  (smoothing, extrema, exact and smoothed bridge cases; decimal strings).
+"""
+import csv
+import json
+import os
+import sys
+
+REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def replay():
+    src = os.path.join(REF, "fixtures/replay/european_bs-windows-x86_64.json")
+    d = json.load(open(src))
+    cases = []
+    for c in d["cases"]:
+        req, res = c["request"], c["result"]
+        eng = req["engine"]
+        case = {
+            "name": c["name"],
+            "engine": eng["type"],
+            "master_seed": eng.get("master_seed", eng.get("master_scramble_seed")),
+            "sampling_units": eng.get("independent_sampling_units", eng.get("points_per_scramble")),
+            "scramble_count": eng.get("scramble_count"),
+            "antithetic": eng["variance_reduction"]["antithetic"],
+            "brownian_bridge": eng["variance_reduction"]["brownian_bridge"],
+            "reduction_block_size": c["execution"]["monte_carlo"]["reduction_block_size"],
+            "spot": req["market"]["spot"],
+            "discount_curve": req["market"]["discount_curve"],
+            "dividend_curve": req["market"]["dividend_curve"],
+            "volatility": req["model"]["volatility"],
+            "strike": req["product"]["strike"],
+            "valuation_date": req["valuation_date"],
+            "expiry": req["product"]["expiry"],
+            "gamma_bump_relative": req["risk"]["gamma"]["bump"]["value"],
+            "expected": {
+                "price": res["value"]["value"],
+                "price_standard_error": res["value"]["standard_error"],
+                "delta": res["risks"]["delta"]["raw"]["value"],
+                "delta_standard_error": res["risks"]["delta"]["raw"]["standard_error"],
+                "gamma": res["risks"]["gamma"]["raw"]["value"],
+                "gamma_standard_error": res["risks"]["gamma"]["raw"]["standard_error"],
+                "vega": res["risks"]["vega"]["raw"]["value"],
+                "vega_standard_error": res["risks"]["vega"]["raw"]["standard_error"],
+                "sampling_variance_bits": c["execution"]["sampling_variance_bits"],
+                "estimator_variance_bits": c["execution"]["estimator_variance_bits"],
+                "bump_delta_value_bits": c["execution"]["risk_validation"]["delta"]["bump_and_revalue"]["value_bits"],
+                "bump_gamma_value_bits": c["execution"]["risk_validation"]["gamma"]["bump_and_revalue"]["value_bits"],
+                "bump_vega_value_bits": c["execution"]["risk_validation"]["vega"]["bump_and_revalue"]["value_bits"],
+            },
+        }
+        cases.append(case)
+    json.dump({"source": "fixtures/replay/european_bs-windows-x86_64.json", "cases": cases},
+              open(os.path.join(OUT, "replay_european_bs.json"), "w"), indent=1)
+
+
+def analytical():
+    src = os.path.join(REF, "fixtures/acceptance/european_bs_analytical.csv")
+    rows = list(csv.DictReader(open(src)))
+    json.dump({"source": "fixtures/acceptance/european_bs_analytical.csv", "rows": rows},
+              open(os.path.join(OUT, "bs_analytical.json"), "w"), indent=1)
+
+
+def path_dependence():
+    src = os.path.join(REF, "fixtures/path-dependence/reference-cases-v0.1.json")
+    d = json.load(open(src))
+    keep = {k: d[k] for k in ("smoothing_cases", "extrema_cases", "bridge_cases", "smoothed_bridge_cases")}
+    keep["source"] = "fixtures/path-dependence/reference-cases-v0.1.json"
+    json.dump(keep, open(os.path.join(OUT, "path_dependence.json"), "w"), indent=1)
+
+
+if __name__ == "__main__":
+    if not os.path.isdir(REF):
+        sys.exit(f"reference checkout not found at {REF}")
+    replay()
+    analytical()
+    path_dependence()
+    print("golden fixtures written to", OUT)
