@@ -317,6 +317,25 @@ mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double*
                                         uint32_t log_moneyness_count, double floor, double cap,
                                         double* values, uint32_t* repairs);
 
+/* ---- Pricing without device allocation (no counterpart in the reference) ----
+ *
+ * For callers that must not allocate GPU memory while pricing (a service that
+ * gives the whole device to its own pool at start-up, a host held to a fixed
+ * device-memory budget, or a latency-bound caller that cannot take the
+ * device-wide synchronisation of cudaFree/cudaMalloc).  Prices one European or
+ * Digital Black--Scholes product observed once at expiry, pseudo-MC or RQMC,
+ * price-only or full risk, with the same kernels as mcg_plan_evaluate; the
+ * kernels' scratch lives in a static device array of MCG_NOALLOC_SCRATCH_BYTES
+ * per GPU that loads this library, held until the process exits.  Limits:
+ * sampling units x scrambles <= 2^20 and scramble_count <= 64; larger
+ * requests return MCG_ERR_INVALID_ARGUMENT.  All calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * first call on a device resolves the array's address; make it before any
+ * stream capture.  `result->products` needs one slot; device_ms is not timed;
+ * failures are described by mcg_last_error(). */
+#define MCG_NOALLOC_SCRATCH_BYTES 5953280u
+mcg_status mcg_price_european_noalloc(const mcg_plan_desc* desc, void* stream, mcg_result* result);
+
 /* ---- Diagnostics (no counterpart in the reference) ---- */
 
 /* Dense FP64 FMA throughput of the current device in TFLOP/s (an FMA counts as

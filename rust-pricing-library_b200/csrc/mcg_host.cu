@@ -870,6 +870,11 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
 
 }  // namespace
 
+namespace mcg {
+// Lets other translation units report through mcg_last_error().
+void set_last_error(const std::string& message) { g_last_error = message; }
+}  // namespace mcg
+
 extern "C" {
 
 uint32_t mcg_abi_version(void) { return MCG_ABI_VERSION; }

@@ -17,7 +17,7 @@ LIBRARY_PATH = os.path.join(HERE, "libmcg.so")
 EXPORTS = (
     "mcg_abi_version", "mcg_last_error", "mcg_plan_create", "mcg_plan_evaluate", "mcg_price",
     "mcg_plan_destroy", "mcg_plan_shape", "mcg_philox_normals", "mcg_rqmc_words",
-    "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak",
+    "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
 )
 
 _lib = None
@@ -64,6 +64,8 @@ def library() -> C.CDLL:
     lib.mcg_ssvi_local_variance_grid.argtypes = [dp, dp, u32, dbl, dbl, dbl, dbl, dp, u32, dp, u32,
                                                  dbl, dbl, dp, C.POINTER(u32)]
     lib.mcg_ssvi_local_variance_grid.restype = C.c_int
+    lib.mcg_price_european_noalloc.argtypes = [C.POINTER(A.PlanDesc), vp, C.POINTER(A.Result)]
+    lib.mcg_price_european_noalloc.restype = C.c_int
     lib.mcg_measure_fp64_peak.argtypes = [vp, C.POINTER(dbl)]
     lib.mcg_measure_fp64_peak.restype = C.c_int
     if lib.mcg_abi_version() != A.ABI_VERSION:
