@@ -230,6 +230,12 @@ typedef struct mcg_product_result {
     mcg_estimate bump_vega;
     double sampling_variance;
     double estimator_variance;
+    /* Local volatility with Vega and Delta requested: the adjoint sweep's spot
+     * Delta dP/dS0 and the central difference of adjoint Deltas at S +/- h
+     * (beyond the reference, which bumps Delta and Gamma for local vol). */
+    mcg_statistics adjoint_components[2];
+    mcg_estimate adjoint_delta;
+    mcg_estimate adjoint_gamma;
 } mcg_product_result;
 
 typedef struct mcg_error_record {

@@ -166,3 +166,12 @@ int oracle_smoothed_bridge(int up, double barrier, double s0, double s1, double 
     return oracle::smoothed_bridge_api(up, barrier, s0, s1, h, iv, out);
 }
 }
+
+namespace oracle {
+int interval_adjoint_api(int up, double barrier, double h, double lsa, double ls, double rs, double lv,
+                         double rv, double dt, double* out);
+}
+extern "C" int oracle_interval_adjoint(int up, double barrier, double h, double lsa, double ls, double rs,
+                                       double lv, double rv, double dt, double* out) {
+    return oracle::interval_adjoint_api(up, barrier, h, lsa, ls, rs, lv, rv, dt, out);
+}

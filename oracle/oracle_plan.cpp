@@ -22,6 +22,9 @@ namespace oracle {
 namespace {
 
 constexpr int kComponents = MCG_PATHWISE_COMPONENTS;
+// Per-unit values: the reference's 18 components plus the adjoint Delta and
+// the bumped-adjoint Gamma of the local-volatility adjoint.
+constexpr int kWidth = kComponents + 2;
 constexpr double kNormal95 = 1.959963984540054;  // plan/simulation.rs:24
 constexpr double kLogMaxExpArgument = 6.564958884017094;   // barrier_bridge.rs:9
 constexpr double kLogMinPositive = -744.4400719213812;     // barrier_bridge.rs:10
@@ -1024,22 +1027,27 @@ bool lv_payoff(const Plan& p, const Product& pr, int which, const LvPath& path, 
 }
 
 // reverse_path_with_variance_seeds and LocalVolPath::reverse_state_adjoints,
-// local_vol/direct_adjoints.rs:97-159 and local_vol.rs:723-803.  Returns the
-// combined grid-value adjoints.
-bool lv_reverse(const Plan& p, const LvPath& path, std::vector<double> seeds,
+// local_vol/direct_adjoints.rs:97-159 and local_vol.rs:723-803, for the spot
+// runtime `which`.  Returns the combined grid-value adjoints, the adjoint of the
+// initial state and x_sum = sum over nodes of dPayoff/dx_i, the sensitivity to
+// the forward normalisers (every F_i is proportional to the spot).
+bool lv_reverse(const Plan& p, int which, const LvPath& path, std::vector<double> seeds,
                 const std::vector<double>& var_seeds, std::vector<double>& grid_adj,
-                Failure& f) {
+                double& initial_adjoint, double& x_sum, Failure& f) {
     const size_t count = p.nodes.size();
     const size_t steps = count - 1;
     grid_adj.assign(p.grid.v.size(), 0.0);
+    x_sum = 0.0;
     for (size_t i = 0; i < count; ++i) {
         Interpolation in;
-        if (!p.grid.interpolate(p.nodes[i], std::log(path.state[i] / p.fwd[0][i]), in)) {
+        if (!p.grid.interpolate(p.nodes[i], std::log(path.state[i] / p.fwd[which][i]), in)) {
             f = {MCG_ERR_INVALID_SURFACE_QUERY, static_cast<uint32_t>(i), 0.0};
             return false;
         }
         const double seed = var_seeds[i];
-        seeds[i] += seed * p.grid.x_derivative(in) / path.state[i];
+        const double dvdx = p.grid.x_derivative(in);
+        seeds[i] += seed * dvdx / path.state[i];
+        x_sum += seed * dvdx;
         p.grid.transpose_accumulate(in, seed, grid_adj.data());
     }
     std::vector<double> trans(p.grid.v.size(), 0.0);
@@ -1052,8 +1060,9 @@ bool lv_reverse(const Plan& p, const LvPath& path, std::vector<double> seeds,
         const double sqdt = std::sqrt(dt);
         seeds[s] += nsa * path.expo[s];
         const double lva = lea * (-0.5 * dt + path.shock[s] * sqdt / (2.0 * lvol));
-        const double deriv = p.grid.x_derivative(path.interp[s]) / path.state[s];
-        seeds[s] += lva * deriv;
+        const double dvdx = p.grid.x_derivative(path.interp[s]);
+        seeds[s] += lva * (dvdx / path.state[s]);
+        x_sum += lva * dvdx;
         if (!std::isfinite(seeds[s]) || !std::isfinite(lva)) {
             f = {MCG_ERR_NON_FINITE_STATE, static_cast<uint32_t>(s), seeds[s]};
             return false;
@@ -1061,77 +1070,115 @@ bool lv_reverse(const Plan& p, const LvPath& path, std::vector<double> seeds,
         p.grid.transpose_accumulate(path.interp[s], lva, trans.data());
     }
     for (size_t k = 0; k < grid_adj.size(); ++k) grid_adj[k] += trans[k];
+    initial_adjoint = seeds[0];
     return true;
 }
 
-// local_vol_pathwise_values_and_buckets_inner,
-// crates/pricing/src/engine/risk/pathwise_local_vol.rs:127-361.
-bool lv_unit_product(const Plan& p, const Product& pr, const double* shocks, double* values,
-                     double* node_values, Failure& f) {
-    for (int c = 0; c < kComponents; ++c) values[c] = 0.0;
+// Payoff seeds of one LV path (pathwise_local_vol.rs:206-303) and the reverse
+// sweep: Vega = sum of 2 sqrt(v) x node adjoint (:310-321), node values, and
+// the adjoint spot Delta dP/dS0 = lambda_0 - x_sum / S0 (holding the dynamics
+// in forward-normalised log-moneyness, as the bumped runtimes do).
+bool lv_adjoint(const Plan& p, const Product& pr, int which, const double* shocks, double& price,
+                double& vega, double& adjoint_delta, double* node_values, double* diag, Failure& f) {
     LvPath path;
-    if (!lv_evolve(p, 0, shocks, path, f)) return false;
-    double price;
+    if (!lv_evolve(p, which, shocks, path, f)) return false;
     BarrierEval be;
     BarrierTerms terms{};
     std::vector<double> nv;
     const bool cb = pr.d.kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
-    if (!lv_payoff(p, pr, 0, path, price, cb ? &be : nullptr, cb ? &terms : nullptr, nv, f))
+    if (!lv_payoff(p, pr, which, path, price, cb ? &be : nullptr, cb ? &terms : nullptr, nv, f))
         return false;
-    values[MCG_PRICE] = price;
-    if (cb)
-        for (int k = 0; k < 8; ++k) values[10 + k] = be.diag[k];
-    if (p.req_vega || p.req_nodes) {
-        const size_t count = p.nodes.size();
-        const size_t n = p.obs_t.size();
-        std::vector<double> seeds(count, 0.0), vseeds(count, 0.0);
-        if (cb) {
-            const uint32_t tn = p.obs_node[n - 1];
-            seeds[tn] += p.discount * terms.terminal_derivative * 1.0;
-            if (p.smoothing > 0.0) {
-                const double lsa = (p.discount * terms.survival_derivative) * be.survival;
-                for (size_t k = 0; k < be.sm.size(); ++k) {
-                    const auto& si = be.sm[k];
-                    seeds[k] += 0.0 * si.left.hit_d_state + (lsa * si.d_left_distance) * si.left.eld_d_state;
-                    seeds[k + 1] += 0.0 * si.right.hit_d_state + (lsa * si.d_right_distance) * si.right.eld_d_state;
-                    vseeds[k] += lsa * si.d_left_var;
-                    vseeds[k + 1] += lsa * si.d_right_var;
-                }
-                for (size_t k = 0; k < be.hit_safety.size(); ++k) {
-                    const double der = be.hit_safety[k] == 0.0
-                                           ? 0.0
-                                           : -lsa * be.hit_dstate[k] / be.hit_safety[k];
-                    seeds[k] += der;
-                }
-            } else if (be.exact_active) {
-                const double lsa = p.discount * terms.survival_derivative * be.survival;
-                for (size_t k = 0; k < be.ex.size(); ++k) {
-                    seeds[k] += lsa * be.ex[k].d_left_state;
-                    seeds[k + 1] += lsa * be.ex[k].d_right_state;
-                    vseeds[k] += lsa * be.ex[k].d_left_var;
-                    vseeds[k + 1] += lsa * be.ex[k].d_right_var;
-                }
+    if (cb && diag)
+        for (int k = 0; k < 8; ++k) diag[k] = be.diag[k];
+    const size_t count = p.nodes.size();
+    const size_t n = p.obs_t.size();
+    std::vector<double> seeds(count, 0.0), vseeds(count, 0.0);
+    if (cb) {
+        const uint32_t tn = p.obs_node[n - 1];
+        seeds[tn] += p.discount * terms.terminal_derivative * 1.0;
+        if (p.smoothing > 0.0) {
+            const double lsa = (p.discount * terms.survival_derivative) * be.survival;
+            for (size_t k = 0; k < be.sm.size(); ++k) {
+                const auto& si = be.sm[k];
+                seeds[k] += 0.0 * si.left.hit_d_state + (lsa * si.d_left_distance) * si.left.eld_d_state;
+                seeds[k + 1] += 0.0 * si.right.hit_d_state + (lsa * si.d_right_distance) * si.right.eld_d_state;
+                vseeds[k] += lsa * si.d_left_var;
+                vseeds[k + 1] += lsa * si.d_right_var;
             }
-        } else {
-            std::vector<double> spots(n), adj(n);
-            for (size_t i = 0; i < n; ++i) spots[i] = path.state[p.obs_node[i]];
-            payoff_eval(pr, spots.data(), n, p.smoothing, adj.data());
-            for (size_t k = n; k-- > 0;)
-                if (adj[k] != 0.0) seeds[p.obs_node[k]] += p.discount * adj[k] * 1.0;
+            for (size_t k = 0; k < be.hit_safety.size(); ++k) {
+                const double der = be.hit_safety[k] == 0.0
+                                       ? 0.0
+                                       : -lsa * be.hit_dstate[k] / be.hit_safety[k];
+                seeds[k] += der;
+            }
+        } else if (be.exact_active) {
+            const double lsa = p.discount * terms.survival_derivative * be.survival;
+            for (size_t k = 0; k < be.ex.size(); ++k) {
+                seeds[k] += lsa * be.ex[k].d_left_state;
+                seeds[k + 1] += lsa * be.ex[k].d_right_state;
+                vseeds[k] += lsa * be.ex[k].d_left_var;
+                vseeds[k + 1] += lsa * be.ex[k].d_right_var;
+            }
         }
-        std::vector<double> grid_adj;
-        if (!lv_reverse(p, path, seeds, vseeds, grid_adj, f)) return false;
-        NeumaierSum vega;
-        for (size_t k = 0; k < grid_adj.size(); ++k) {
-            const double node = grid_adj[k] * 2.0 * std::sqrt(p.grid.v[k]);
-            vega.add(node);
-            if (node_values) node_values[k] = node;
-        }
-        values[MCG_VEGA] = vega.total();
+    } else {
+        std::vector<double> spots(n), adj(n);
+        for (size_t i = 0; i < n; ++i) spots[i] = path.state[p.obs_node[i]];
+        payoff_eval(pr, spots.data(), n, p.smoothing, adj.data());
+        for (size_t k = n; k-- > 0;)
+            if (adj[k] != 0.0) seeds[p.obs_node[k]] += p.discount * adj[k] * 1.0;
     }
+    std::vector<double> grid_adj;
+    double lambda0, x_sum;
+    if (!lv_reverse(p, which, path, seeds, vseeds, grid_adj, lambda0, x_sum, f)) return false;
+    NeumaierSum v;
+    for (size_t k = 0; k < grid_adj.size(); ++k) {
+        const double node = grid_adj[k] * 2.0 * std::sqrt(p.grid.v[k]);
+        v.add(node);
+        if (node_values) node_values[k] = node;
+    }
+    vega = v.total();
+    adjoint_delta = lambda0 - x_sum / p.bump_spot[which];
+    return true;
+}
+
+// local_vol_pathwise_values_and_buckets_inner,
+// crates/pricing/src/engine/risk/pathwise_local_vol.rs:127-361.  Values 18 and
+// 19 (beyond the reference's 18) hold the adjoint Delta and the bumped-adjoint
+// Gamma when Vega and Delta (and Gamma) are requested.
+bool lv_unit_product(const Plan& p, const Product& pr, const double* shocks, double* values,
+                     double* node_values, Failure& f) {
+    for (int c = 0; c < kComponents + 2; ++c) values[c] = 0.0;
+    double price;
+    if (p.req_vega || p.req_nodes) {
+        double vega, adelta, diag[8];
+        if (!lv_adjoint(p, pr, 0, shocks, price, vega, adelta, node_values, diag, f)) return false;
+        values[MCG_VEGA] = vega;
+        if (pr.d.kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
+            for (int k = 0; k < 8; ++k) values[10 + k] = diag[k];
+        if (p.req_delta) values[kComponents] = adelta;
+        if (p.req_delta && p.req_gamma) {
+            double pd, pu, vd, vu, dd, du;
+            if (!lv_adjoint(p, pr, 1, shocks, pd, vd, dd, nullptr, nullptr, f)) return false;
+            if (!lv_adjoint(p, pr, 2, shocks, pu, vu, du, nullptr, nullptr, f)) return false;
+            values[kComponents + 1] = (du - dd) / (2.0 * p.spot_bump);
+        }
+    } else {
+        LvPath path;
+        if (!lv_evolve(p, 0, shocks, path, f)) return false;
+        BarrierEval be;
+        BarrierTerms terms{};
+        std::vector<double> nv;
+        const bool cb = pr.d.kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+        if (!lv_payoff(p, pr, 0, path, price, cb ? &be : nullptr, cb ? &terms : nullptr, nv, f))
+            return false;
+        if (cb)
+            for (int k = 0; k < 8; ++k) values[10 + k] = be.diag[k];
+    }
+    values[MCG_PRICE] = price;
     if (p.req_delta || p.req_gamma) {
         double down, up;
         LvPath bumped;
+        std::vector<double> nv;
         if (!lv_evolve(p, 1, shocks, bumped, f)) return false;
         if (!lv_payoff(p, pr, 1, bumped, down, nullptr, nullptr, nv, f)) return false;
         if (!lv_evolve(p, 2, shocks, bumped, f)) return false;
@@ -1188,11 +1235,11 @@ bool unit_values(const Plan& p, uint32_t scramble, uint64_t unit, std::vector<do
     std::vector<double> z(dims), mate(dims), normals, scratch, tmp;
     std::vector<Obs> obs;
     unit_shocks(p, scramble, unit, z.data(), normals, scratch);
-    out.assign(P * kComponents, 0.0);
+    out.assign(P * kWidth, 0.0);
     const size_t gv = p.grid.v.size();
     const bool want_nodes = p.model == MCG_MODEL_LOCAL_VOLATILITY && p.req_nodes;
     if (want_nodes) nodes_out.assign(P * gv, 0.0);
-    std::vector<double> a(kComponents), b(kComponents), na(gv), nb(gv);
+    std::vector<double> a(kWidth, 0.0), b(kWidth, 0.0), na(gv), nb(gv);
     for (size_t k = 0; k < P; ++k) {
         const Product& pr = p.products[k];
         bool ok;
@@ -1208,11 +1255,11 @@ bool unit_values(const Plan& p, uint32_t scramble, uint64_t unit, std::vector<do
             else
                 ok = lv_unit_product(p, pr, mate.data(), b.data(), want_nodes ? nb.data() : nullptr, f);
             if (!ok) return false;
-            for (int c = 0; c < kComponents; ++c) a[c] = (a[c] + b[c]) * 0.5;
+            for (int c = 0; c < kWidth; ++c) a[c] = (a[c] + b[c]) * 0.5;
             if (want_nodes)
                 for (size_t g = 0; g < gv; ++g) na[g] = (na[g] + nb[g]) * 0.5;
         }
-        std::copy(a.begin(), a.end(), out.begin() + k * kComponents);
+        std::copy(a.begin(), a.end(), out.begin() + k * kWidth);
         if (want_nodes) std::copy(na.begin(), na.end(), nodes_out.begin() + k * gv);
     }
     return true;
@@ -1232,7 +1279,7 @@ bool map_reduce(const Plan& p, uint32_t scramble, uint64_t units, int threads,
                 std::vector<Statistics>& total, mcg_error_record& err) {
     const size_t P = p.products.size();
     const size_t gv = (p.model == MCG_MODEL_LOCAL_VOLATILITY && p.req_nodes) ? p.grid.v.size() : 0;
-    const size_t width = P * kComponents + P * gv;
+    const size_t width = P * kWidth + P * gv;
     const uint64_t block = p.block;
     const uint64_t nblocks = (units + block - 1) / block;
     std::vector<BlockResult> results(nblocks);
@@ -1250,8 +1297,8 @@ bool map_reduce(const Plan& p, uint32_t scramble, uint64_t units, int threads,
                     r.failed_unit = u;
                     break;
                 }
-                for (size_t i = 0; i < P * kComponents; ++i) r.stats[i].add(vals[i]);
-                for (size_t i = 0; i < P * gv; ++i) r.stats[P * kComponents + i].add(nodes[i]);
+                for (size_t i = 0; i < P * kWidth; ++i) r.stats[i].add(vals[i]);
+                for (size_t i = 0; i < P * gv; ++i) r.stats[P * kWidth + i].add(nodes[i]);
             }
         }
     };
@@ -1318,7 +1365,7 @@ int evaluate(const mcg_plan_desc* desc, mcg_result* result, int threads) {
         independent = p.units;
         result->evaluated_paths = p.units * (p.antithetic ? 2 : 1);
     } else {
-        const size_t width = P * kComponents + P * gv;
+        const size_t width = P * kWidth + P * gv;
         std::vector<std::vector<double>> replicate(width);
         for (uint32_t s = 0; s < p.scrambles; ++s) {
             std::vector<Statistics> within;
@@ -1339,15 +1386,18 @@ int evaluate(const mcg_plan_desc* desc, mcg_result* result, int threads) {
     result->effective_dimension = p.dimension;
     for (size_t k = 0; k < P; ++k) {
         mcg_product_result& r = result->products[k];
-        for (int c = 0; c < kComponents; ++c) r.components[c] = to_c(stats[k * kComponents + c]);
-        const Statistics& price = stats[k * kComponents + MCG_PRICE];
+        for (int c = 0; c < kComponents; ++c) r.components[c] = to_c(stats[k * kWidth + c]);
+        for (int c = 0; c < 2; ++c) r.adjoint_components[c] = to_c(stats[k * kWidth + kComponents + c]);
+        const Statistics& price = stats[k * kWidth + MCG_PRICE];
         r.price = estimate(price, independent, 1.0);
-        r.delta = estimate(stats[k * kComponents + MCG_DELTA], independent, 1.0);
-        r.gamma = estimate(stats[k * kComponents + MCG_GAMMA], independent, 1.0);
-        r.vega = estimate(stats[k * kComponents + MCG_VEGA], independent, 1.0);
-        r.bump_delta = estimate(stats[k * kComponents + MCG_BUMP_DELTA], independent, 1.0);
-        r.bump_gamma = estimate(stats[k * kComponents + MCG_BUMP_GAMMA], independent, 1.0);
-        r.bump_vega = estimate(stats[k * kComponents + MCG_BUMP_VEGA], independent, 1.0);
+        r.delta = estimate(stats[k * kWidth + MCG_DELTA], independent, 1.0);
+        r.gamma = estimate(stats[k * kWidth + MCG_GAMMA], independent, 1.0);
+        r.vega = estimate(stats[k * kWidth + MCG_VEGA], independent, 1.0);
+        r.bump_delta = estimate(stats[k * kWidth + MCG_BUMP_DELTA], independent, 1.0);
+        r.bump_gamma = estimate(stats[k * kWidth + MCG_BUMP_GAMMA], independent, 1.0);
+        r.bump_vega = estimate(stats[k * kWidth + MCG_BUMP_VEGA], independent, 1.0);
+        r.adjoint_delta = estimate(stats[k * kWidth + kComponents], independent, 1.0);
+        r.adjoint_gamma = estimate(stats[k * kWidth + kComponents + 1], independent, 1.0);
         const double sv = price.moments.count > 1
                               ? price.moments.second_moment /
                                     static_cast<double>(price.moments.count - 1)
@@ -1357,7 +1407,7 @@ int evaluate(const mcg_plan_desc* desc, mcg_result* result, int threads) {
     }
     if (gv && result->local_vega_nodes && result->node_capacity >= P * gv) {
         for (size_t i = 0; i < P * gv; ++i) {
-            const Statistics& s = stats[P * kComponents + i];
+            const Statistics& s = stats[P * kWidth + i];
             result->local_vega_nodes[i] = to_c(s);
             if (result->local_vega_node_estimates)
                 result->local_vega_node_estimates[i] = estimate(s, independent, 1.0);
@@ -1451,6 +1501,31 @@ int smoothed_bridge_api(int up, double barrier, double s0, double s1, double h, 
     out[3] = si.right.eld;
     out[4] = std::exp(si.log_survival);
     out[5] = si.left.safety_weight * si.right.safety_weight;
+    return 0;
+}
+}  // namespace oracle
+
+namespace oracle {
+// Adjoint of one continuous-barrier interval (test entry point): state and
+// direct-variance seeds of the two nodes for a log-survival adjoint lsa.
+int interval_adjoint_api(int up, double barrier, double h, double lsa, double ls, double rs, double lv,
+                         double rv, double dt, double* out) {
+    Failure f;
+    if (h > 0.0) {
+        SmoothInterval si;
+        if (!smooth_interval(up != 0, ls, rs, barrier, barrier, 1.0, 1.0, lv, rv, dt, h, si, f)) return f.code;
+        out[0] = 0.0 * si.left.hit_d_state + (lsa * si.d_left_distance) * si.left.eld_d_state;
+        out[1] = 0.0 * si.right.hit_d_state + (lsa * si.d_right_distance) * si.right.eld_d_state;
+        out[2] = lsa * si.d_left_var;
+        out[3] = lsa * si.d_right_var;
+        return 0;
+    }
+    ExactInterval iv;
+    if (!exact_interval(up != 0, ls, rs, barrier, barrier, lv, rv, dt, iv, f)) return f.code;
+    out[0] = lsa * iv.d_left_state;
+    out[1] = lsa * iv.d_right_state;
+    out[2] = lsa * iv.d_left_var;
+    out[3] = lsa * iv.d_right_var;
     return 0;
 }
 }  // namespace oracle

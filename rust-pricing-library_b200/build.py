@@ -24,6 +24,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-
 # (source, extra flags)
 UNITS = [
     ("mcg_lv.cu", ["-fmad=false"]),
+    ("mcg_lv_adjoint.cu", ["-fmad=false"]),
     ("mcg_bs.cu", ["-fmad=false"]),
     ("mcg_setup.cu", ["-fmad=false"]),
     ("mcg_host.cu", ["-fmad=false"]),

@@ -44,6 +44,28 @@ struct Pchip {
     double slope;
 };
 __global__ void fp64_peak_kernel(double*, int);
+struct AdjointArgs {
+    int32_t which;
+    double sign;
+    double node_weight;
+    int32_t node_add;
+    uint32_t scramble;
+    uint64_t unit_begin;
+    uint64_t units;
+    uint32_t tile_offset;
+    double* tape_f;
+    double* tape_z;
+    double* out_vega;
+    double* out_delta;
+    double* node_tiles;
+};
+size_t lv_adjoint_smem(const DevicePlan& P);
+cudaError_t launch_lv_adjoint(const DevicePlan& P, const AdjointArgs& A, ErrorWord* err, cudaStream_t stream);
+cudaError_t launch_lv_adjoint_combine(const double* vega, const double* delta, uint64_t units, int pairs,
+                                      int have_gamma, double h, uint32_t tile_offset, StatRecord* partials,
+                                      cudaStream_t stream);
+cudaError_t launch_lv_node_reduce(const double* node_tiles, uint32_t tiles_per_scramble, uint32_t scrambles,
+                                  uint32_t nv, StatRecord* out, cudaStream_t stream);
 __global__ void ssvi_grid_kernel(Pchip, double, double, double, const double*, uint32_t,
                                  const double*, uint32_t, double, double, double*, uint32_t*,
                                  uint32_t*);
@@ -336,6 +358,11 @@ struct mcg_plan {
     DeviceArray<StatRecord> partials, records;
     DeviceArray<ErrorWord> error;
     uint32_t tiles = 0;
+    // local-volatility adjoint (Vega, adjoint Delta/Gamma, node sensitivities)
+    bool adjoint = false, adjoint_nodes = false, adjoint_gamma = false;
+    uint64_t chunk_units = 0;
+    DeviceArray<double> tape, adj_vega, adj_delta, node_tiles;
+    DeviceArray<StatRecord> adj_partials, adj_records, node_records;
 
     ~mcg_plan() {
         ops.release();
@@ -361,6 +388,13 @@ struct mcg_plan {
         partials.release();
         records.release();
         error.release();
+        tape.release();
+        adj_vega.release();
+        adj_delta.release();
+        node_tiles.release();
+        adj_partials.release();
+        adj_records.release();
+        node_records.release();
     }
 };
 
@@ -530,8 +564,15 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan) {
         if (risk && single) plan.mask = 0x3ffu;
         if (has_continuous) plan.mask |= 0xffu << 10;
     } else {
-        if (d->request_vega || d->request_local_vega_nodes)
-            return fail(MCG_ERR_UNSUPPORTED, "local-volatility Vega runs in the adjoint entry point");
+        plan.adjoint = d->request_vega || d->request_local_vega_nodes;
+        plan.adjoint_nodes = d->request_local_vega_nodes != 0;
+        plan.adjoint_gamma = plan.adjoint && d->request_delta && d->request_gamma;
+        if (plan.adjoint) {
+            if (d->product_count != 1)
+                return fail(MCG_ERR_UNSUPPORTED, "local-volatility Vega prices one product per plan");
+            if (d->products[0].kind == MCG_PRODUCT_DISCRETE_BARRIER && d->smoothing_half_width > 0.0)
+                return fail(MCG_ERR_UNSUPPORTED, "local-volatility Vega of a smoothed discrete barrier");
+        }
         const mcg_local_variance_grid& g = d->local_variance;
         if (g.time_count < 2 || g.log_moneyness_count < 2 || !g.time_nodes || !g.log_moneyness_nodes || !g.values)
             return fail(MCG_ERR_MARKET, "local variance grid needs at least 2x2 nodes");
@@ -699,6 +740,21 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan) {
     MCG_CUDA(plan.partials.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * plan.product_count * kComponents));
     MCG_CUDA(plan.records.alloc(static_cast<size_t>(P.scramble_count) * plan.product_count * kComponents));
     MCG_CUDA(plan.error.alloc(1));
+    if (plan.adjoint) {
+        // Per-step checkpoints of one chunk of units: states (steps + 1) and shocks (steps).
+        plan.chunk_units = std::min<uint64_t>(P.units, 1ull << 20);
+        MCG_CUDA(plan.tape.alloc(static_cast<size_t>(2 * P.steps + 1) * plan.chunk_units));
+        MCG_CUDA(plan.adj_vega.alloc(6 * plan.chunk_units));
+        MCG_CUDA(plan.adj_delta.alloc(6 * plan.chunk_units));
+        MCG_CUDA(plan.adj_partials.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * 3));
+        MCG_CUDA(plan.adj_records.alloc(static_cast<size_t>(P.scramble_count) * 3));
+        if (plan.adjoint_nodes) {
+            MCG_CUDA(plan.node_tiles.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * plan.grid_values));
+            MCG_CUDA(plan.node_records.alloc(static_cast<size_t>(P.scramble_count) * plan.grid_values));
+        }
+        if (lv_adjoint_smem(P) > 200 * 1024)
+            return fail(MCG_ERR_UNSUPPORTED, "local-variance grid too large for the adjoint kernel's shared memory");
+    }
     return MCG_OK;
 }
 
@@ -780,7 +836,64 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
                                                                            width, plan->records.ptr);
     MCG_CUDA(cudaGetLastError());
     ++launches;
+    std::vector<StatRecord> adj_rec, node_rec;
+    if (plan->adjoint) {
+        const int pairs = P.antithetic ? 2 : 1;
+        const uint32_t tiles_chunk = static_cast<uint32_t>((plan->chunk_units + kThreads - 1) / kThreads);
+        for (uint32_t sc = 0; sc < P.scramble_count; ++sc) {
+            for (uint64_t begin = 0; begin < P.units; begin += plan->chunk_units) {
+                const uint64_t n = std::min<uint64_t>(plan->chunk_units, P.units - begin);
+                const uint32_t tile_offset = sc * plan->tiles + static_cast<uint32_t>(begin / kThreads);
+                for (int pr = 0; pr < pairs; ++pr) {
+                    for (int which : {1, 2, 0}) {
+                        if (which != 0 && !plan->adjoint_gamma) continue;
+                        AdjointArgs A{};
+                        A.which = which;
+                        A.sign = pr == 0 ? 1.0 : -1.0;
+                        A.node_weight = pairs == 2 ? 0.5 : 1.0;
+                        A.node_add = pr;
+                        A.scramble = sc;
+                        A.unit_begin = begin;
+                        A.units = n;
+                        A.tile_offset = tile_offset;
+                        A.tape_f = plan->tape.ptr;
+                        A.tape_z = plan->tape.ptr + static_cast<size_t>(P.steps + 1) * plan->chunk_units;
+                        A.out_vega = plan->adj_vega.ptr + static_cast<size_t>(pr * 3 + which) * n;
+                        A.out_delta = plan->adj_delta.ptr + static_cast<size_t>(pr * 3 + which) * n;
+                        A.node_tiles = (which == 0 && plan->adjoint_nodes) ? plan->node_tiles.ptr : nullptr;
+                        e = launch_lv_adjoint(P, A, plan->error.ptr, stream);
+                        if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("adjoint kernel: ") + cudaGetErrorString(e));
+                        ++launches;
+                    }
+                }
+                e = launch_lv_adjoint_combine(plan->adj_vega.ptr, plan->adj_delta.ptr, n, pairs,
+                                              plan->adjoint_gamma ? 1 : 0, P.spot_bump, tile_offset,
+                                              plan->adj_partials.ptr, stream);
+                if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+                ++launches;
+                (void)tiles_chunk;
+            }
+        }
+        reduce_tiles_kernel<<<dim3(3, P.scramble_count), 256, 0, stream>>>(plan->adj_partials.ptr, plan->tiles, 3,
+                                                                          plan->adj_records.ptr);
+        MCG_CUDA(cudaGetLastError());
+        ++launches;
+        adj_rec.resize(static_cast<size_t>(P.scramble_count) * 3);
+        if (plan->adjoint_nodes) {
+            e = launch_lv_node_reduce(plan->node_tiles.ptr, plan->tiles, P.scramble_count, plan->grid_values,
+                                      plan->node_records.ptr, stream);
+            if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+            ++launches;
+            node_rec.resize(static_cast<size_t>(P.scramble_count) * plan->grid_values);
+        }
+    }
     MCG_CUDA(cudaEventRecord(t1, stream));
+    if (!adj_rec.empty())
+        MCG_CUDA(cudaMemcpyAsync(adj_rec.data(), plan->adj_records.ptr, adj_rec.size() * sizeof(StatRecord),
+                                 cudaMemcpyDeviceToHost, stream));
+    if (!node_rec.empty())
+        MCG_CUDA(cudaMemcpyAsync(node_rec.data(), plan->node_records.ptr, node_rec.size() * sizeof(StatRecord),
+                                 cudaMemcpyDeviceToHost, stream));
     std::vector<StatRecord> rec(static_cast<size_t>(P.scramble_count) * width);
     ErrorWord ew;
     MCG_CUDA(cudaMemcpyAsync(rec.data(), plan->records.ptr, rec.size() * sizeof(StatRecord),
@@ -851,6 +964,28 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
             stats[c] = h;
             r.components[c] = {h.sum, h.corr, h.count, h.mean, h.m2};
         }
+        if (plan->adjoint) {
+            // Vega and the adjoint Delta/Gamma come from the reverse sweep.
+            HostStat adj[3];
+            for (int c = 0; c < 3; ++c) {
+                if (!rqmc) {
+                    const StatRecord& x = adj_rec[c];
+                    adj[c] = {x.sum, x.corr, static_cast<uint64_t>(x.count), x.mean, x.m2};
+                } else {
+                    std::vector<double> reps(P.scramble_count);
+                    for (uint32_t sc = 0; sc < P.scramble_count; ++sc)
+                        reps[sc] = (adj_rec[sc * 3 + c].sum + adj_rec[sc * 3 + c].corr) / static_cast<double>(P.units);
+                    adj[c] = two_pass(reps);
+                }
+            }
+            stats[MCG_VEGA] = adj[0];
+            r.components[MCG_VEGA] = {adj[0].sum, adj[0].corr, adj[0].count, adj[0].mean, adj[0].m2};
+            for (int c = 0; c < 2; ++c)
+                r.adjoint_components[c] = {adj[c + 1].sum, adj[c + 1].corr, adj[c + 1].count, adj[c + 1].mean,
+                                           adj[c + 1].m2};
+            r.adjoint_delta = make_estimate(adj[1], independent, 1.0);
+            r.adjoint_gamma = make_estimate(adj[2], independent, 1.0);
+        }
         r.price = make_estimate(stats[MCG_PRICE], independent, 1.0);
         r.delta = make_estimate(stats[MCG_DELTA], independent, 1.0);
         r.gamma = make_estimate(stats[MCG_GAMMA], independent, 1.0);
@@ -862,6 +997,36 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
         const double sv = pr.count > 1 ? pr.m2 / static_cast<double>(pr.count - 1) : 0.0;
         r.sampling_variance = plan->total_variance == 0.0 ? 0.0 : sv;
         r.estimator_variance = r.sampling_variance / static_cast<double>(independent);
+    }
+    if (!node_rec.empty() && result->local_vega_nodes && result->node_capacity >= plan->grid_values) {
+        // Node sensitivities: exact means; pseudo-MC standard errors from the
+        // batch means of the 128-unit CTA tiles, RQMC from the scramble means.
+        const uint32_t nv = plan->grid_values;
+        for (uint32_t k = 0; k < nv; ++k) {
+            HostStat h;
+            if (!rqmc) {
+                const StatRecord& x = node_rec[k];
+                const double total = x.sum + x.corr;
+                const double n = static_cast<double>(P.units);
+                const double tiles = x.count;
+                const double batch = n / tiles;
+                const double s2 = tiles > 1.0 ? x.m2 / (tiles - 1.0) / (batch * batch) : 0.0;
+                h.sum = x.sum;
+                h.corr = x.corr;
+                h.count = P.units;
+                h.mean = total / n;
+                h.m2 = (s2 / tiles) * n * (n - 1.0);
+            } else {
+                std::vector<double> reps(P.scramble_count);
+                for (uint32_t sc = 0; sc < P.scramble_count; ++sc)
+                    reps[sc] = (node_rec[static_cast<size_t>(sc) * nv + k].sum + node_rec[static_cast<size_t>(sc) * nv + k].corr) /
+                               static_cast<double>(P.units);
+                h = two_pass(reps);
+            }
+            result->local_vega_nodes[k] = {h.sum, h.corr, h.count, h.mean, h.m2};
+            if (result->local_vega_node_estimates)
+                result->local_vega_node_estimates[k] = make_estimate(h, independent, 1.0);
+        }
     }
     if (plan->total_variance > 0.0 && independent < 2)
         return fail(MCG_ERR_INSUFFICIENT_UNITS, "at least two independent sampling units are required");

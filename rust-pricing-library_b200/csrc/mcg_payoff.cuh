@@ -313,3 +313,140 @@ MCG_HD double acc_payoff(const ProductParams& p, const ProductAcc& s,
 }
 
 }  // namespace mcg
+
+namespace mcg {
+
+// ------------------------------------------- reverse of the bridge terms
+
+// Log-survival derivatives of one exact interval,
+// BarrierBridgeInterval::evaluate, barrier_bridge.rs:446-528 (constant barrier).
+struct ExactIntervalDerivs {
+    double d_left_state, d_right_state, d_left_var, d_right_var;
+};
+
+MCG_HD ExactIntervalDerivs exact_interval_derivs(bool up, double ls, double rs, double barrier,
+                                                 double lv, double rv, double dt) {
+    ExactIntervalDerivs d{0.0, 0.0, 0.0, 0.0};
+    const double lb = log(barrier);
+    const double ld = up ? lb - log(ls) : log(ls) - lb;
+    const double rd = up ? lb - log(rs) : log(rs) - lb;
+    if (ld <= 0.0 || rd <= 0.0) return d;
+    const double average = 0.5 * lv + 0.5 * rv;
+    const double integrated = average * dt;
+    if (!isfinite(integrated) || integrated == 0.0) return d;
+    const double le = kLn2 + log(ld) + log(rd) - log(integrated);
+    if (le >= kLogMaxExpArgument) return d;
+    double led;
+    if (le <= kLogMinPositive) {
+        led = 1.0;
+    } else {
+        const double e = exp(le);
+        led = e / expm1(e);
+    }
+    const double ldd = led / ld;
+    const double rdd = led / rd;
+    const double ivd = -led / integrated;
+    const double sign = up ? 1.0 : -1.0;
+    const double avd = ivd * dt;
+    d.d_left_state = -sign * ldd / ls;
+    d.d_right_state = -sign * rdd / rs;
+    d.d_left_var = 0.5 * avd;
+    d.d_right_var = 0.5 * avd;
+    return d;
+}
+
+// Smoothed endpoint with its derivatives (barrier_bridge.rs:160-249, affine
+// scale 1): safety weight, effective log distance, d(hit weight)/d(state) and
+// d(effective log distance)/d(state).
+struct SmoothEndpointFull {
+    double safety, eld, hit_d_state, eld_d_state;
+};
+
+MCG_HD SmoothEndpointFull smooth_endpoint_full(bool up, double state, double barrier, double h) {
+    SmoothEndpointFull e{1.0, 1.0, 0.0, 0.0};
+    const double sign = up ? 1.0 : -1.0;
+    const double signed_hit = 1.0 * sign * (state - barrier);
+    const SmoothD hit = smooth_indicator(h, signed_hit, e.safety);
+    const SmoothD safe = smooth_positive_part(h, -signed_hit);
+    const double spot_barrier = 1.0 * barrier;
+    const double denominator = up ? spot_barrier - safe.value : spot_barrier + safe.value;
+    e.eld = up ? -log1p(-safe.value / spot_barrier) : log1p(safe.value / spot_barrier);
+    const double hit_x = hit.first;
+    const double safe_x = -safe.first;
+    const double distance_safe = 1.0 / denominator;
+    const double distance_x = distance_safe * safe_x;
+    const double x_state = 1.0 * sign;
+    e.hit_d_state = hit_x * x_state;
+    e.eld_d_state = distance_x * x_state;
+    return e;
+}
+
+// Log-survival derivatives of one smoothed interval with respect to the two
+// effective log distances and the two local variances (barrier_bridge.rs:276-357).
+struct SmoothIntervalDerivs {
+    double d_left_distance, d_right_distance, d_left_var, d_right_var;
+};
+
+MCG_HD SmoothIntervalDerivs smooth_interval_derivs(double ld, double rd, double lv, double rv,
+                                                   double dt) {
+    SmoothIntervalDerivs d{0.0, 0.0, 0.0, 0.0};
+    if (ld == 0.0 || rd == 0.0) return d;
+    const double average = 0.5 * lv + 0.5 * rv;
+    const double integrated = average * dt;
+    if (!isfinite(integrated) || integrated == 0.0) return d;
+    const double le = kLn2 + log(ld) + log(rd) - log(integrated);
+    if (le >= kLogMaxExpArgument) return d;
+    double led;
+    if (le <= kLogMinPositive) {
+        led = 1.0;
+    } else {
+        const double e = exp(le);
+        led = e / expm1(e);
+    }
+    const double ivd = -led / integrated;
+    const double avd = ivd * dt;
+    d.d_left_distance = led / ld;
+    d.d_right_distance = led / rd;
+    d.d_left_var = 0.5 * avd;
+    d.d_right_var = 0.5 * avd;
+    return d;
+}
+
+// Adjoint of the continuous-barrier bridge for one interval [k-1, k]:
+// contributions to the state seeds and the direct variance seeds of both
+// nodes, given the log-survival adjoint lsa
+// (pathwise_local_vol.rs:219-271; barrier.rs:82-118 for the smoothed reverse).
+struct IntervalAdjoint {
+    double left_state, right_state, left_var, right_var;
+};
+
+MCG_HD IntervalAdjoint barrier_interval_adjoint(bool up, double barrier, double h, double lsa,
+                                                double ls, double rs, double lv, double rv,
+                                                double dt) {
+    IntervalAdjoint a{0.0, 0.0, 0.0, 0.0};
+    if (!(dt > 0.0)) return a;
+    if (h > 0.0) {
+        const SmoothEndpointFull le = smooth_endpoint_full(up, ls, barrier, h);
+        const SmoothEndpointFull re = smooth_endpoint_full(up, rs, barrier, h);
+        const SmoothIntervalDerivs d = smooth_interval_derivs(le.eld, re.eld, lv, rv, dt);
+        a.left_state = 0.0 * le.hit_d_state + (lsa * d.d_left_distance) * le.eld_d_state;
+        a.right_state = 0.0 * re.hit_d_state + (lsa * d.d_right_distance) * re.eld_d_state;
+        a.left_var = lsa * d.d_left_var;
+        a.right_var = lsa * d.d_right_var;
+        return a;
+    }
+    const ExactIntervalDerivs d = exact_interval_derivs(up, ls, rs, barrier, lv, rv, dt);
+    a.left_state = lsa * d.d_left_state;
+    a.right_state = lsa * d.d_right_state;
+    a.left_var = lsa * d.d_left_var;
+    a.right_var = lsa * d.d_right_var;
+    return a;
+}
+
+// Adjoint of a smoothed hit factor at one node: -lsa * d(hit)/d(state) / safety.
+MCG_HD double hit_factor_adjoint(bool up, double barrier, double h, double lsa, double state) {
+    const SmoothEndpointFull e = smooth_endpoint_full(up, state, barrier, h);
+    return e.safety == 0.0 ? 0.0 : -lsa * e.hit_d_state / e.safety;
+}
+
+}  // namespace mcg

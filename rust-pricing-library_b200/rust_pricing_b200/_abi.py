@@ -101,6 +101,7 @@ class ProductResult(C.Structure):
         ("price", Estimate), ("delta", Estimate), ("gamma", Estimate), ("vega", Estimate),
         ("bump_delta", Estimate), ("bump_gamma", Estimate), ("bump_vega", Estimate),
         ("sampling_variance", C.c_double), ("estimator_variance", C.c_double),
+        ("adjoint_components", Statistics * 2), ("adjoint_delta", Estimate), ("adjoint_gamma", Estimate),
     ]
 
 
@@ -124,14 +125,18 @@ class Result(C.Structure):
 class ResultBuffers:
     """Caller-owned result storage for `products` products and `nodes` node entries."""
 
+    @property
+    def node_stats(self):
+        return self.node_stats_array
+
     def __init__(self, products: int, nodes: int = 0):
         self.products = (ProductResult * max(products, 1))()
-        self.node_stats = (Statistics * nodes)() if nodes else None
+        self.node_stats_array = (Statistics * nodes)() if nodes else None
         self.node_estimates = (Estimate * nodes)() if nodes else None
         self.result = Result()
         self.result.product_capacity = products
         self.result.products = C.cast(self.products, C.POINTER(ProductResult))
         self.result.node_capacity = nodes
         if nodes:
-            self.result.local_vega_nodes = C.cast(self.node_stats, C.POINTER(Statistics))
+            self.result.local_vega_nodes = C.cast(self.node_stats_array, C.POINTER(Statistics))
             self.result.local_vega_node_estimates = C.cast(self.node_estimates, C.POINTER(Estimate))

@@ -70,6 +70,8 @@ def oracle():
     lib.oracle_smoothed_bridge.restype = C.c_int
     lib.oracle_barrier_path.argtypes = [C.c_int, dbl, dbl, dp, dp, dp, u32, dp, dp]
     lib.oracle_barrier_path.restype = C.c_int
+    lib.oracle_interval_adjoint.argtypes = [C.c_int, dbl, dbl, dbl, dbl, dbl, dbl, dbl, dbl, dp]
+    lib.oracle_interval_adjoint.restype = C.c_int
     _oracle = lib
     return lib
 

@@ -36,4 +36,13 @@ int hm_barrier_path(int up, double barrier, double h, const double* states, cons
     return failed ? 1 : 0;
 }
 
+void hm_interval_adjoint(int up, double barrier, double h, double lsa, double ls, double rs, double lv,
+                         double rv, double dt, double* out) {
+    const IntervalAdjoint a = barrier_interval_adjoint(up != 0, barrier, h, lsa, ls, rs, lv, rv, dt);
+    out[0] = a.left_state;
+    out[1] = a.right_state;
+    out[2] = a.left_var;
+    out[3] = a.right_var;
+}
+
 }  // extern "C"

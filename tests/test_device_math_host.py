@@ -35,6 +35,7 @@ def hm():
     lib.hm_smoothing.argtypes = [C.c_double, C.c_double, dp]
     lib.hm_barrier_path.argtypes = [C.c_int, C.c_double, C.c_double, dp, dp, dp, C.c_uint, dp, dp]
     lib.hm_barrier_path.restype = C.c_int
+    lib.hm_interval_adjoint.argtypes = [C.c_int] + [C.c_double] * 8 + [dp]
     return lib
 
 
@@ -68,3 +69,20 @@ def test_barrier_bridge_matches_oracle(hm, oracle, h, up):
         assert oracle.oracle_barrier_path(up, barrier, h, H.dptr(s), H.dptr(v), H.dptr(t), n + 1, C.byref(b_s), H.dptr(b_d)) == 0
         assert a_s.value == b_s.value
         assert np.array_equal(a_d, b_d)
+
+
+@pytest.mark.parametrize("h", [0.0, 0.5])
+def test_barrier_interval_adjoint_matches_oracle(hm, oracle, h):
+    """The reverse of one bridge interval, used by the adjoint path kernel."""
+    rng = np.random.default_rng(5)
+    for _ in range(500):
+        up = int(rng.integers(0, 2))
+        barrier = 100.0
+        ls = barrier * np.exp((1 if not up else -1) * rng.uniform(-0.01, 0.2))
+        rs = barrier * np.exp((1 if not up else -1) * rng.uniform(-0.01, 0.2))
+        lv, rv, dt, lsa = rng.uniform(0.01, 0.09), rng.uniform(0.01, 0.09), 1.0 / 252, rng.normal()
+        a, b = np.zeros(4), np.zeros(4)
+        hm.hm_interval_adjoint(up, barrier, h, lsa, ls, rs, lv, rv, dt, H.dptr(a))
+        if oracle.oracle_interval_adjoint(up, barrier, h, lsa, ls, rs, lv, rv, dt, H.dptr(b)) != 0:
+            continue
+        assert np.array_equal(a, b), (up, ls, rs, a, b)
