@@ -323,6 +323,107 @@ mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double*
                                         uint32_t log_moneyness_count, double floor, double cap,
                                         double* values, uint32_t* repairs);
 
+/* ---- Early exercise: Longstaff--Schwartz regression ----
+ *
+ * Replaces SimulationPlan::execute_early_exercise and its RQMC twin
+ * (crates/pricing/src/engine/risk/early_exercise.rs:24-120,251-313): path
+ * matrices of a training and a valuation engine
+ * (crates/pricing/src/engine/mc/early_exercise.rs:28-450), the backward
+ * regression train_exercise_policy (crates/pricing/src/engine/mc/lsm.rs:1486-1695)
+ * over a polynomial basis in the standardised spot with column-pivoted QR
+ * (lsm.rs:1928-2230,2374-2652), and value_exercise_policy (lsm.rs:1347-1482).
+ *
+ * The plan descriptor holds one product of kind MCG_PRODUCT_AMERICAN; its
+ * `observation_times` are the exercise times, the last one the expiry (the
+ * American payoff graph observes exactly the exercise dates,
+ * crates/pricing/src/engine/payoff/compile.rs:67-101).  Its engine fields are
+ * the valuation engine; `mcg_lsm_desc` adds the training engine (same kind) and
+ * the regression configuration (LsmConfig).  Risk requests must be off. */
+#define MCG_LSM_MAX_DEGREE 7u
+#define MCG_LSM_MAX_BASIS (MCG_LSM_MAX_DEGREE + 1u)
+
+typedef enum mcg_continuation_kind {
+    MCG_CONTINUATION_POLYNOMIAL = 0, /* the reference's CPQR regression */
+    MCG_CONTINUATION_MLP = 1         /* learned continuation value, see mcg_lsm_desc */
+} mcg_continuation_kind;
+
+typedef struct mcg_lsm_desc {
+    /* PolynomialBasisSpec(feature_count 1, max_degree) over the spot state
+     * variable, CpqrConfig, itm_abs_tolerance and max_matrix_elements of the
+     * reference's LsmConfig (crates/pricing/src/engine/mc/lsm.rs:328-495). */
+    uint32_t max_degree; /* 1 .. MCG_LSM_MAX_DEGREE */
+    double itm_abs_tolerance;
+    double cpqr_abs_tolerance;
+    double cpqr_rel_tolerance;
+    uint64_t max_matrix_elements;
+    /* Training engine (LsmConfig::training_engine), the plan's engine kind. */
+    uint64_t training_seed;
+    uint64_t training_units;          /* pseudo: sampling units; RQMC: points per scramble */
+    uint32_t training_scramble_count; /* RQMC only */
+    int32_t training_antithetic;
+    int32_t training_brownian_bridge;
+    int32_t continuation;             /* mcg_continuation_kind */
+    /* Learned continuation (MCG_CONTINUATION_MLP, no counterpart in the
+     * reference): a 2 -> 64 -> 64 -> 1 SiLU network of (standardised spot,
+     * time), BF16 weights and FP32 accumulation, trained on the training paths. */
+    uint32_t mlp_epochs;
+    uint32_t mlp_batch;
+    float mlp_learning_rate;
+    uint64_t mlp_seed;
+} mcg_lsm_desc;
+
+/* One non-terminal exercise date's decision model: the reference's
+ * ExerciseDecisionModel (lsm.rs:796-818) with the PolynomialRegressionModel
+ * fields (lsm.rs:610-790).  Basis column c is the monomial z^c of the
+ * standardised spot z. */
+typedef struct mcg_lsm_date_model {
+    int32_t regression;             /* 0: ContinueAll (no ITM training path) */
+    uint32_t itm_rows;              /* ExerciseRegressionDiagnostics::itm_rows */
+    uint32_t candidate_rows;
+    uint32_t active_columns;        /* basis columns kept (all, or just z^0 when inactive) */
+    uint32_t diagonal_count;        /* min(itm_rows, active_columns) */
+    uint32_t rank;
+    int32_t feature_inactive;       /* FeatureScaling::inactive */
+    uint32_t reserved;
+    double feature_mean;
+    double feature_variance;        /* population variance */
+    double feature_scale;
+    double zero_scale_threshold;
+    uint32_t pivot_order[MCG_LSM_MAX_BASIS]; /* basis columns in pivot order */
+    double diagonal_abs[MCG_LSM_MAX_BASIS];  /* |R_kk| in pivot order */
+    double rank_threshold;
+    double coefficients[MCG_LSM_MAX_BASIS];  /* per basis column (max_degree + 1) */
+    double residual_sum_squares;
+} mcg_lsm_date_model;
+
+typedef struct mcg_lsm_result {
+    uint32_t date_capacity;         /* entries in `models` and `exercise_counts` */
+    mcg_lsm_date_model* models;     /* date_count - 1 entries, caller-owned */
+    uint64_t* exercise_counts;      /* date_count entries, caller-owned */
+    uint64_t stopping_capacity;     /* entries in `stopping_indices` (0 = not wanted) */
+    uint32_t* stopping_indices;     /* valuation stopping date per path, caller-owned */
+
+    mcg_statistics price_statistics; /* over sampling units (pseudo) or replicates (RQMC) */
+    mcg_estimate price;
+    double sampling_variance;
+    double estimator_variance;
+    double in_sample_value;         /* training paths valued by the policy fitted on them */
+    uint64_t training_paths;
+    uint64_t valuation_paths;
+    uint64_t independent_sampling_units;
+    uint32_t date_count;
+    uint32_t kernel_launches;
+    float device_ms;                /* whole evaluation */
+    float path_kernel_ms;           /* both path-matrix kernels */
+    float regression_ms;            /* backward regression of the training phase */
+    float valuation_ms;             /* policy valuation and statistics */
+    mcg_error_record error;
+} mcg_lsm_result;
+
+/* Train and value an early-exercise policy on the GPU.  Synchronises `stream`. */
+mcg_status mcg_lsm_price(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, void* stream,
+                         mcg_lsm_result* result);
+
 /* ---- Pricing without device allocation (no counterpart in the reference) ----
  *
  * For callers that must not allocate GPU memory while pricing (a service that

@@ -21,6 +21,12 @@ int ssvi_grid(const std::vector<double>& theta_t, const std::vector<double>& the
               const std::vector<double>& xn, double floor, double cap, std::vector<double>& out);
 std::vector<double> piecewise_sinh_nodes(double left, double right, size_t nl, size_t nr,
                                          double ls, double rs);
+int lsm_price(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, mcg_lsm_result* out, int threads);
+const char* lsm_last_error();
+int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vector<double>& spots,
+              uint64_t& path_count, mcg_error_record& err);
+int lsm_fit_api(const double* spots, const double* immediate, const double* targets, size_t rows,
+                const mcg_lsm_desc* lsm, mcg_lsm_date_model* out);
 }  // namespace oracle
 
 extern "C" {
@@ -113,6 +119,32 @@ int oracle_time_grid(const mcg_plan_desc* desc, double* nodes, uint32_t capacity
 }
 
 const char* oracle_last_error(void) { return oracle::last_error(); }
+
+int oracle_lsm_price(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, mcg_lsm_result* out,
+                     int threads) {
+    return oracle::lsm_price(desc, lsm, out, threads);
+}
+
+const char* oracle_lsm_last_error(void) { return oracle::lsm_last_error(); }
+
+// Spot matrix [date][path] of an early-exercise plan under `domain`; returns the
+// path count, or -status on a failure.
+int64_t oracle_lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, double* out,
+                         uint64_t capacity) {
+    std::vector<double> spots;
+    uint64_t paths = 0;
+    mcg_error_record err{};
+    const int rc = oracle::lsm_spots(desc, domain, threads, spots, paths, err);
+    if (rc != MCG_OK) return -static_cast<int64_t>(rc);
+    if (out && capacity >= spots.size()) std::memcpy(out, spots.data(), spots.size() * sizeof(double));
+    return static_cast<int64_t>(paths);
+}
+
+// One date's regression (fit_exercise_decision) on given rows.
+int oracle_lsm_fit(const double* spots, const double* immediate, const double* targets,
+                   uint64_t rows, const mcg_lsm_desc* lsm, mcg_lsm_date_model* out) {
+    return oracle::lsm_fit_api(spots, immediate, targets, rows, lsm, out);
+}
 
 int oracle_ssvi_grid(const double* theta_t, const double* theta_v, uint32_t theta_count,
                      double slope, double rho, double eta, double gamma, const double* tn,

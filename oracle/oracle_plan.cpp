@@ -367,6 +367,7 @@ struct Plan {
     std::vector<uint32_t> dirs;
     std::vector<Scramble> scr;  // scramble-major, dimension-minor
     uint32_t dimension = 0;
+    uint32_t domain = 0;  // RandomDomain of the pseudo stream: Valuation 0, LsmTrain 1
     bool risk_enabled() const { return req_delta || req_gamma || req_vega; }
     bool has_continuous_barrier() const {
         for (const auto& p : products)
@@ -1212,7 +1213,7 @@ void unit_shocks(const Plan& p, uint32_t scramble, uint64_t unit, double* out,
     }
     for (uint32_t d = 0; d < dims; ++d) {
         if (p.engine == MCG_ENGINE_PSEUDO) {
-            normals[d] = philox_normal(p.seed, unit, d, 0u);
+            normals[d] = philox_normal(p.seed, unit, d, p.domain);
         } else {
             const uint32_t w = sobol_word(&p.dirs[static_cast<size_t>(d) * 32u], static_cast<uint32_t>(unit));
             const uint32_t x = p.scr[static_cast<size_t>(scramble) * dims + d].apply(w);
@@ -1444,6 +1445,87 @@ int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacit
     *count = static_cast<uint32_t>(p.nodes.size());
     for (size_t i = 0; i < p.nodes.size() && i < capacity; ++i) nodes_out[i] = p.nodes[i];
     return MCG_OK;
+}
+
+// Path matrix of an early-exercise plan: the spot at every observation
+// (exercise) date, spots[date * paths + path], for the plan's engine under the
+// random domain `domain`.  Path order and mates follow pseudo_lsm_path_matrices
+// and rqmc_lsm_path_matrices (crates/pricing/src/engine/mc/early_exercise.rs:28-175,
+// 177-320): path = unit * 2 (+1 for the antithetic mate), RQMC units numbered
+// scramble-major.  Spots are post_spot of write_lsm_trajectory and
+// write_local_vol_lsm_trajectory (early_exercise.rs:330-450).
+int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vector<double>& spots,
+              uint64_t& path_count, mcg_error_record& err) {
+    Plan p;
+    if (!build_plan(desc, p)) return MCG_ERR_INVALID_ARGUMENT;
+    p.domain = domain;
+    const bool rqmc = p.engine == MCG_ENGINE_RQMC;
+    const uint64_t mult = p.antithetic ? 2 : 1;
+    const uint64_t units = p.units * (rqmc ? p.scrambles : 1);
+    const size_t dates = p.obs_t.size();
+    path_count = units * mult;
+    spots.assign(dates * path_count, 0.0);
+    const bool lv = p.model == MCG_MODEL_LOCAL_VOLATILITY;
+    std::vector<Failure> failures(static_cast<size_t>(std::max(1, threads)));
+    std::vector<uint64_t> failed_unit(failures.size(), ~0ull);
+    std::atomic<uint64_t> next{0};
+    constexpr uint64_t kChunk = 1024;
+    auto worker = [&](size_t t) {
+        std::vector<double> z(p.dimension), normals, scratch;
+        std::vector<Obs> obs(dates);
+        LvPath path;
+        for (;;) {
+            const uint64_t begin = next.fetch_add(kChunk);
+            if (begin >= units || failures[t].code != MCG_OK) break;
+            const uint64_t end = std::min(units, begin + kChunk);
+            for (uint64_t u = begin; u < end; ++u) {
+                const uint32_t scramble = rqmc ? static_cast<uint32_t>(u / p.units) : 0u;
+                const uint64_t local = rqmc ? u % p.units : u;
+                unit_shocks(p, scramble, local, z.data(), normals, scratch);
+                for (uint64_t m = 0; m < mult; ++m) {
+                    if (m == 1)
+                        for (double& v : z) v = -v;
+                    const uint64_t col = u * mult + m;
+                    if (lv) {
+                        if (!lv_evolve(p, 0, z.data(), path, failures[t])) {
+                            failed_unit[t] = u;
+                            return;
+                        }
+                        for (size_t d = 0; d < dates; ++d)
+                            spots[d * path_count + col] = 0.0 * p.spot + 1.0 * path.state[p.obs_node[d]];
+                    } else {
+                        bs_observations(p, z.data(), p.spot, p.vol, obs.data());
+                        for (size_t d = 0; d < dates; ++d) spots[d * path_count + col] = obs[d].post_spot;
+                    }
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < failures.size(); ++t) pool.emplace_back(worker, t);
+    for (auto& t : pool) t.join();
+    uint64_t first = ~0ull;
+    size_t which = 0;
+    for (size_t t = 0; t < failures.size(); ++t)
+        if (failures[t].code != MCG_OK && failed_unit[t] < first) {
+            first = failed_unit[t];
+            which = t;
+        }
+    if (first != ~0ull) {
+        err.code = failures[which].code;
+        err.step = failures[which].step;
+        err.sampling_unit = first;
+        err.value_bits = bits_of(failures[which].value);
+        return err.code;
+    }
+    return MCG_OK;
+}
+
+double plan_discount(const mcg_plan_desc* desc, double t) {
+    Curve c;
+    c.set(desc->discount_curve.times, desc->discount_curve.discount_factors,
+          desc->discount_curve.pillar_count);
+    return std::exp(c.log_discount(t));
 }
 
 }  // namespace oracle

@@ -140,3 +140,70 @@ class ResultBuffers:
         if nodes:
             self.result.local_vega_nodes = C.cast(self.node_stats_array, C.POINTER(Statistics))
             self.result.local_vega_node_estimates = C.cast(self.node_estimates, C.POINTER(Estimate))
+
+
+# ---- early exercise (Longstaff--Schwartz) ----
+LSM_MAX_DEGREE = 7
+LSM_MAX_BASIS = LSM_MAX_DEGREE + 1
+CONTINUATION_POLYNOMIAL, CONTINUATION_MLP = 0, 1
+DOMAIN_VALUATION, DOMAIN_LSM_TRAIN = 0, 1
+
+
+class LsmDesc(C.Structure):
+    _fields_ = [
+        ("max_degree", C.c_uint32), ("itm_abs_tolerance", C.c_double),
+        ("cpqr_abs_tolerance", C.c_double), ("cpqr_rel_tolerance", C.c_double),
+        ("max_matrix_elements", C.c_uint64),
+        ("training_seed", C.c_uint64), ("training_units", C.c_uint64),
+        ("training_scramble_count", C.c_uint32), ("training_antithetic", C.c_int32),
+        ("training_brownian_bridge", C.c_int32), ("continuation", C.c_int32),
+        ("mlp_epochs", C.c_uint32), ("mlp_batch", C.c_uint32), ("mlp_learning_rate", C.c_float),
+        ("mlp_seed", C.c_uint64),
+    ]
+
+
+class LsmDateModel(C.Structure):
+    _fields_ = [
+        ("regression", C.c_int32), ("itm_rows", C.c_uint32), ("candidate_rows", C.c_uint32),
+        ("active_columns", C.c_uint32), ("diagonal_count", C.c_uint32), ("rank", C.c_uint32),
+        ("feature_inactive", C.c_int32), ("reserved", C.c_uint32),
+        ("feature_mean", C.c_double), ("feature_variance", C.c_double),
+        ("feature_scale", C.c_double), ("zero_scale_threshold", C.c_double),
+        ("pivot_order", C.c_uint32 * LSM_MAX_BASIS), ("diagonal_abs", C.c_double * LSM_MAX_BASIS),
+        ("rank_threshold", C.c_double), ("coefficients", C.c_double * LSM_MAX_BASIS),
+        ("residual_sum_squares", C.c_double),
+    ]
+
+
+class LsmResult(C.Structure):
+    _fields_ = [
+        ("date_capacity", C.c_uint32), ("models", C.POINTER(LsmDateModel)),
+        ("exercise_counts", C.POINTER(C.c_uint64)),
+        ("stopping_capacity", C.c_uint64), ("stopping_indices", C.POINTER(C.c_uint32)),
+        ("price_statistics", Statistics), ("price", Estimate),
+        ("sampling_variance", C.c_double), ("estimator_variance", C.c_double),
+        ("in_sample_value", C.c_double),
+        ("training_paths", C.c_uint64), ("valuation_paths", C.c_uint64),
+        ("independent_sampling_units", C.c_uint64),
+        ("date_count", C.c_uint32), ("kernel_launches", C.c_uint32),
+        ("device_ms", C.c_float), ("path_kernel_ms", C.c_float),
+        ("regression_ms", C.c_float), ("valuation_ms", C.c_float),
+        ("error", ErrorRecord),
+    ]
+
+
+class LsmBuffers:
+    """Caller-owned storage for an early-exercise result of `dates` exercise
+    dates and, when `stopping` > 0, that many valuation stopping indices."""
+
+    def __init__(self, dates: int, stopping: int = 0):
+        self.models = (LsmDateModel * max(dates, 1))()
+        self.counts = (C.c_uint64 * max(dates, 1))()
+        self.stops = (C.c_uint32 * stopping)() if stopping else None
+        self.result = LsmResult()
+        self.result.date_capacity = dates
+        self.result.models = C.cast(self.models, C.POINTER(LsmDateModel))
+        self.result.exercise_counts = C.cast(self.counts, C.POINTER(C.c_uint64))
+        self.result.stopping_capacity = stopping
+        if stopping:
+            self.result.stopping_indices = C.cast(self.stops, C.POINTER(C.c_uint32))

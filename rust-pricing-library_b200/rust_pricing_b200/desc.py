@@ -168,3 +168,48 @@ class PlanSpec:
         if self.local_variance is None:
             return 0
         return len(self.local_variance.time_nodes) * len(self.local_variance.log_moneyness_nodes)
+
+
+@dataclass
+class LsmSpec:
+    """The reference's LsmConfig for one spot state variable
+    (crates/pricing/src/engine/mc/lsm.rs:328-495): polynomial degree, CPQR rank
+    tolerances, ITM tolerance, matrix-size limit, and the training engine (of
+    the valuation plan's kind)."""
+
+    training_seed: int
+    training_units: int
+    training_scramble_count: int = 0
+    training_antithetic: bool = False
+    training_brownian_bridge: bool = False
+    max_degree: int = 3
+    itm_abs_tolerance: float = 0.0
+    cpqr_abs_tolerance: float = 1e-14
+    cpqr_rel_tolerance: float = 1e-12
+    max_matrix_elements: int = 1_000_000
+    continuation: int = A.CONTINUATION_POLYNOMIAL
+    mlp_epochs: int = 0
+    mlp_batch: int = 0
+    mlp_learning_rate: float = 0.0
+    mlp_seed: int = 0
+    _keep: list = field(default_factory=list, repr=False)
+
+    def desc(self) -> A.LsmDesc:
+        d = A.LsmDesc()
+        d.max_degree = self.max_degree
+        d.itm_abs_tolerance = self.itm_abs_tolerance
+        d.cpqr_abs_tolerance = self.cpqr_abs_tolerance
+        d.cpqr_rel_tolerance = self.cpqr_rel_tolerance
+        d.max_matrix_elements = self.max_matrix_elements
+        d.training_seed = self.training_seed & 0xFFFFFFFFFFFFFFFF
+        d.training_units = self.training_units
+        d.training_scramble_count = self.training_scramble_count
+        d.training_antithetic = int(self.training_antithetic)
+        d.training_brownian_bridge = int(self.training_brownian_bridge)
+        d.continuation = self.continuation
+        d.mlp_epochs = self.mlp_epochs
+        d.mlp_batch = self.mlp_batch
+        d.mlp_learning_rate = self.mlp_learning_rate
+        d.mlp_seed = self.mlp_seed & 0xFFFFFFFFFFFFFFFF
+        self._keep[:] = [d]
+        return d

@@ -9,6 +9,10 @@ are committed; the tests only read them.
 * bs_analytical.json       -- fixtures/acceptance/european_bs_analytical.csv.
 * path_dependence.json     -- fixtures/path-dependence/reference-cases-v0.1.json
   (smoothing, extrema, exact and smoothed bridge cases; decimal strings).
+* early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
+  the American put requests (pseudo and RQMC, training and valuation engines,
+  LSM configuration) with the fitted decision models, exercise counts,
+  valuation stopping indices, in-sample value, price and fixed-policy risks.
 """
 import csv
 import json
@@ -79,10 +83,77 @@ def path_dependence():
     json.dump(keep, open(os.path.join(OUT, "path_dependence.json"), "w"), indent=1)
 
 
+def _engine(e):
+    rqmc = e["type"] == "randomized_quasi_monte_carlo"
+    return {
+        "engine": "rqmc" if rqmc else "pseudo",
+        "master_seed": e["master_scramble_seed"] if rqmc else e["master_seed"],
+        "sampling_units": e["points_per_scramble"] if rqmc else e["independent_sampling_units"],
+        "scramble_count": e.get("scramble_count"),
+        "antithetic": e["variance_reduction"]["antithetic"],
+        "brownian_bridge": e["variance_reduction"]["brownian_bridge"],
+    }
+
+
+def early_exercise():
+    src = os.path.join(REF, "fixtures/replay/early_exercise-windows-x86_64.json")
+    d = json.load(open(src))
+    cases = []
+    for c in d["cases"]:
+        req, res = c["request"], c["result"]
+        ee = res["monte_carlo"]["early_exercise"]
+        lsm = req["lsm"]
+        case = {
+            "name": c["name"],
+            "valuation": _engine(req["engine"]),
+            "training": _engine(lsm["training_engine"]),
+            "reduction_block_size": c["execution"]["monte_carlo"]["reduction_block_size"],
+            "lsm": {
+                "feature_count": lsm["basis"]["feature_count"],
+                "max_degree": lsm["basis"]["max_degree"],
+                "cpqr_abs_tolerance": lsm["cpqr"]["abs_rank_tolerance"],
+                "cpqr_rel_tolerance": lsm["cpqr"]["rel_rank_tolerance"],
+                "itm_abs_tolerance": lsm["itm_abs_tolerance"],
+                "max_matrix_elements": lsm["max_matrix_elements"],
+                "state_variables": [v["type"] for v in lsm["state_variables"]],
+            },
+            "spot": req["market"]["spot"],
+            "discount_curve": req["market"]["discount_curve"],
+            "dividend_curve": req["market"]["dividend_curve"],
+            "volatility": req["model"]["volatility"],
+            "valuation_date": req["valuation_date"],
+            "product": {k: req["product"][k] for k in ("exercise_dates", "expiry", "notional", "strike")},
+            "side": req["product"]["side"]["type"],
+            "risk": req["risk"],
+            "expected": {
+                "value": res["value"],
+                "sampling_variance": res["monte_carlo"]["sampling_variance"],
+                "estimator_variance": res["monte_carlo"]["estimator_variance"],
+                "sampling_variance_bits": c["execution"]["sampling_variance_bits"],
+                "estimator_variance_bits": c["execution"]["estimator_variance_bits"],
+                "evaluated_paths": int(c["execution"]["evaluated_paths"]),
+                "independent_sampling_units": c["execution"]["independent_sampling_units"],
+                "decision_models": ee["decision_models"],
+                "regression_diagnostics": ee["regression_diagnostics"],
+                "exercise_counts": ee["exercise_counts"],
+                "exercise_probabilities": ee["exercise_probabilities"],
+                "stopping_indices": ee["stopping_indices"],
+                "in_sample_value": ee["in_sample_value"],
+                "training_trajectories": ee["training_trajectories"],
+                "valuation_trajectories": ee["valuation_trajectories"],
+                "risks": res["risks"],
+            },
+        }
+        cases.append(case)
+    json.dump({"source": "fixtures/replay/early_exercise-windows-x86_64.json", "cases": cases},
+              open(os.path.join(OUT, "early_exercise.json"), "w"), indent=1)
+
+
 if __name__ == "__main__":
     if not os.path.isdir(REF):
         sys.exit(f"reference checkout not found at {REF}")
     replay()
     analytical()
     path_dependence()
+    early_exercise()
     print("golden fixtures written to", OUT)

@@ -72,6 +72,15 @@ def oracle():
     lib.oracle_barrier_path.restype = C.c_int
     lib.oracle_interval_adjoint.argtypes = [C.c_int, dbl, dbl, dbl, dbl, dbl, dbl, dbl, dbl, dp]
     lib.oracle_interval_adjoint.restype = C.c_int
+    lib.oracle_lsm_price.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.LsmDesc), C.POINTER(A.LsmResult),
+                                     C.c_int]
+    lib.oracle_lsm_price.restype = C.c_int
+    lib.oracle_lsm_last_error.restype = C.c_char_p
+    lib.oracle_lsm_spots.argtypes = [C.POINTER(A.PlanDesc), u32, C.c_int, C.POINTER(dbl), u64]
+    lib.oracle_lsm_spots.restype = C.c_int64
+    lib.oracle_lsm_fit.argtypes = [C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl), u64,
+                                   C.POINTER(A.LsmDesc), C.POINTER(A.LsmDateModel)]
+    lib.oracle_lsm_fit.restype = C.c_int
     _oracle = lib
     return lib
 
@@ -86,6 +95,21 @@ def oracle_evaluate(spec, threads: int | None = None):
     if rc != 0:
         raise RuntimeError(f"oracle status {A.STATUS_NAMES.get(rc, rc)}: "
                            f"{lib.oracle_last_error().decode()} error={buf.result.error.code}")
+    return buf
+
+
+def oracle_lsm(spec, lsm, stopping: bool = False, threads: int | None = None):
+    """Run the oracle's early-exercise evaluation; returns the LsmBuffers."""
+    lib = oracle()
+    paths = spec.sampling_units * (spec.scramble_count if spec.engine == A.ENGINE_RQMC else 1)
+    paths *= 2 if spec.antithetic else 1
+    buf = A.LsmBuffers(len(spec.observation_times), paths if stopping else 0)
+    desc, ldesc = spec.desc(), lsm.desc()
+    rc = lib.oracle_lsm_price(C.byref(desc), C.byref(ldesc), C.byref(buf.result),
+                              threads or os.cpu_count() or 1)
+    if rc != 0:
+        raise RuntimeError(f"oracle status {A.STATUS_NAMES.get(rc, rc)}: "
+                           f"{lib.oracle_lsm_last_error().decode()} {lib.oracle_last_error().decode()}")
     return buf
 
 
