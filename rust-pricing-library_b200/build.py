@@ -29,6 +29,7 @@ UNITS = [
     ("mcg_setup.cu", ["-fmad=false"]),
     ("mcg_host.cu", ["-fmad=false"]),
     ("mcg_noalloc.cu", ["-fmad=false"]),
+    ("mcg_lsm.cu", ["-fmad=false"]),
 ]
 
 

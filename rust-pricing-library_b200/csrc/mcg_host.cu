@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "mcg_kernels.cuh"
+#include "mcg_lsm.cuh"
 
 namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -1033,6 +1034,275 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
     return MCG_OK;
 }
 
+// ------------------------------------------------------------ early exercise
+
+// Device buffers of one mcg_lsm_price call, released on every return path.
+struct LsmBuffers {
+    DeviceArray<double> spots, cf, df, unit_values, means;
+    DeviceArray<uint32_t> stop, vstops;
+    DeviceArray<mcg_lsm_date_model> models;
+    DeviceArray<DD> partials, group_partials, sums;
+    DeviceArray<unsigned int> tickets;
+    DeviceArray<unsigned long long> counts, words;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    ~LsmBuffers() {
+        spots.release();
+        cf.release();
+        df.release();
+        unit_values.release();
+        means.release();
+        stop.release();
+        vstops.release();
+        models.release();
+        partials.release();
+        group_partials.release();
+        sums.release();
+        tickets.release();
+        counts.release();
+        words.release();
+        for (cudaEvent_t& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+mcg_status validate_lsm(const mcg_plan_desc* d, const mcg_lsm_desc* l, const mcg_lsm_result* r) {
+    if (!d || !l || !r) return fail(MCG_ERR_INVALID_ARGUMENT, "null argument");
+    if (d->abi_version != MCG_ABI_VERSION) return fail(MCG_ERR_INVALID_ARGUMENT, "abi_version mismatch");
+    if (d->product_count != 1 || !d->products || d->products[0].kind != MCG_PRODUCT_AMERICAN)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "an early-exercise plan holds exactly one American product");
+    if (d->request_delta || d->request_gamma || d->request_vega || d->request_local_vega_nodes)
+        return fail(MCG_ERR_UNSUPPORTED, "fixed-policy early-exercise risk is not implemented");
+    if (d->model != MCG_MODEL_BLACK_SCHOLES)
+        return fail(MCG_ERR_UNSUPPORTED, "early exercise under local volatility is not implemented");
+    if (l->continuation != MCG_CONTINUATION_POLYNOMIAL)
+        return fail(MCG_ERR_UNSUPPORTED, "continuation kind");
+    if (l->max_degree < 1 || l->max_degree > MCG_LSM_MAX_DEGREE)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "max_degree must be 1..7");
+    // validate_tolerance, lsm.rs:2295-2302
+    for (double t : {l->itm_abs_tolerance, l->cpqr_abs_tolerance, l->cpqr_rel_tolerance})
+        if (!std::isfinite(t) || t < 0.0) return fail(MCG_ERR_LSM, "tolerances must be finite and non-negative");
+    if (l->max_matrix_elements == 0) return fail(MCG_ERR_LSM, "max_matrix_elements must be positive");
+    if (l->training_units == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "training_units");
+    if (d->engine == MCG_ENGINE_RQMC && l->training_scramble_count == 0)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "training_scramble_count");
+    const uint32_t dates = d->observation_count;
+    if (dates == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "observation_times");
+    if (r->date_capacity < dates || !r->exercise_counts || (dates > 1 && !r->models))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "result needs date_capacity >= exercise dates");
+    return MCG_OK;
+}
+
+mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t stream, mcg_lsm_result* r) {
+    mcg_status st = validate_lsm(d, l, r);
+    if (st != MCG_OK) return st;
+    std::memset(&r->error, 0, sizeof(r->error));
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+        return fail(MCG_ERR_CUDA, "no CUDA device is visible");
+    // The path plans of both engines: the American product prices nothing by
+    // itself, so each plan carries a European placeholder of the same contract.
+    mcg_product_desc placeholder = d->products[0];
+    placeholder.kind = MCG_PRODUCT_EUROPEAN;
+    mcg_plan_desc vd = *d;
+    vd.products = &placeholder;
+    vd.payment_time = d->observation_times[d->observation_count - 1];
+    mcg_plan_desc td = vd;
+    td.master_seed = l->training_seed;
+    td.sampling_units = l->training_units;
+    td.scramble_count = l->training_scramble_count;
+    td.scramble_begin = 0;
+    td.antithetic = l->training_antithetic;
+    td.brownian_bridge = l->training_brownian_bridge;
+    mcg_plan vplan, tplan;
+    if ((st = build(&vd, vplan)) != MCG_OK) return st;
+    if ((st = build(&td, tplan)) != MCG_OK) return st;
+    const DevicePlan& TP = tplan.dp;
+    const DevicePlan& VP = vplan.dp;
+    const uint32_t dates = d->observation_count;
+    const bool rqmc = d->engine == MCG_ENGINE_RQMC;
+    const uint64_t t_units = TP.units * TP.scramble_count, v_units = VP.units * VP.scramble_count;
+    const uint64_t t_paths = t_units * (TP.antithetic ? 2 : 1), v_paths = v_units * (VP.antithetic ? 2 : 1);
+    HostCurve rc;
+    std::string why;
+    if (!load_curve(d->discount_curve, rc, "discount_curve", why)) return fail(MCG_ERR_MARKET, why);
+    std::vector<double> df(dates);
+    for (uint32_t i = 0; i < dates; ++i) {
+        df[i] = std::exp(rc.log_discount(d->observation_times[i]));
+        if (!std::isfinite(df[i]) || df[i] <= 0.0) return fail(MCG_ERR_LSM, "invalid discount factor");
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    const unsigned ctas = static_cast<unsigned>(std::max<uint64_t>(
+        1, std::min<uint64_t>((t_paths + 255) / 256, 2ull * static_cast<uint64_t>(sms))));
+    const unsigned group_ctas = static_cast<unsigned>(std::max(1, sms));
+    const uint32_t t_groups = rqmc ? TP.scramble_count : 1, v_groups = rqmc ? VP.scramble_count : 1;
+
+    LsmBuffers B;
+    MCG_CUDA(B.spots.alloc(static_cast<size_t>(dates) * t_paths));
+    MCG_CUDA(B.cf.alloc(t_paths));
+    MCG_CUDA(B.stop.alloc(t_paths));
+    MCG_CUDA(B.df.upload(df));
+    MCG_CUDA(B.models.alloc(std::max<uint32_t>(dates - 1, 1)));
+    MCG_CUDA(B.partials.alloc(static_cast<size_t>(ctas) * lsm_partial_stride()));
+    MCG_CUDA(B.tickets.alloc(3));
+    MCG_CUDA(B.words.alloc(2));  // [0] first non-finite training unit, [1] first failing date
+    MCG_CUDA(B.unit_values.alloc(v_units));
+    MCG_CUDA(B.counts.alloc(dates));
+    const bool want_stops = r->stopping_indices && r->stopping_capacity >= v_paths;
+    if (want_stops) MCG_CUDA(B.vstops.alloc(v_paths));
+    const uint32_t max_groups = std::max(t_groups, v_groups);
+    MCG_CUDA(B.group_partials.alloc(static_cast<size_t>(max_groups) * group_ctas));
+    MCG_CUDA(B.sums.alloc(3 * static_cast<size_t>(max_groups)));  // in-sample, valuation, squares
+    MCG_CUDA(B.means.alloc(static_cast<size_t>(max_groups)));
+    MCG_CUDA(cudaMemsetAsync(B.tickets.ptr, 0, 3 * sizeof(unsigned int), stream));
+    MCG_CUDA(cudaMemsetAsync(B.words.ptr, 0xff, 2 * sizeof(unsigned long long), stream));
+    MCG_CUDA(cudaMemsetAsync(B.counts.ptr, 0, dates * sizeof(unsigned long long), stream));
+    MCG_CUDA(cudaMemsetAsync(B.models.ptr, 0, std::max<uint32_t>(dates - 1, 1) * sizeof(mcg_lsm_date_model), stream));
+    for (cudaEvent_t& e : B.ev) MCG_CUDA(cudaEventCreate(&e));
+    uint32_t launches = 0;
+
+    // Training: path matrix, then the backward induction.
+    MCG_CUDA(cudaEventRecord(B.ev[0], stream));
+    MCG_CUDA(launch_lsm_bs_spots(TP, /*LsmTrain*/ 1u, B.spots.ptr, t_paths, &B.words.ptr[0], stream));
+    ++launches;
+    MCG_CUDA(cudaEventRecord(B.ev[1], stream));
+    LsmArgs A{};
+    A.spots = B.spots.ptr;
+    A.paths = t_paths;
+    A.dates = dates;
+    A.nb = l->max_degree + 1;
+    A.side = d->products[0].side;
+    A.strike = d->products[0].strike;
+    A.notional = d->products[0].notional;
+    A.itm_tol = l->itm_abs_tolerance;
+    A.abs_tol = l->cpqr_abs_tolerance;
+    A.rel_tol = l->cpqr_rel_tolerance;
+    A.max_elements = l->max_matrix_elements;
+    A.df = B.df.ptr;
+    A.cf = B.cf.ptr;
+    A.stop = B.stop.ptr;
+    A.models = B.models.ptr;
+    A.partials = B.partials.ptr;
+    A.tickets = B.tickets.ptr;
+    A.lsm_error = &B.words.ptr[1];
+    const int last = static_cast<int>(dates) - 1;
+    MCG_CUDA(launch_lsm_sweep(A, ctas, 1, -1, last - 1, stream));
+    ++launches;
+    for (int date = last - 1; date >= 0; --date) {
+        MCG_CUDA(launch_lsm_variance(A, ctas, date, stream));
+        MCG_CUDA(launch_lsm_gram(A, ctas, date, stream));
+        MCG_CUDA(launch_lsm_sweep(A, ctas, 0, date, date - 1, stream));
+        launches += 3;
+    }
+    // In-sample value of the training paths under their own policy.
+    DD* s_in = B.sums.ptr;
+    DD* s_val = B.sums.ptr + max_groups;
+    DD* s_sq = B.sums.ptr + 2 * max_groups;
+    MCG_CUDA(launch_lsm_group_sum(B.cf.ptr, TP.units, t_groups, TP.antithetic, nullptr, B.group_partials.ptr,
+                                  group_ctas, s_in, nullptr, stream));
+    launches += 2;
+    MCG_CUDA(cudaEventRecord(B.ev[2], stream));
+
+    // Valuation: fresh paths under the fitted policy.
+    LsmValueArgs V{};
+    V.df = B.df.ptr;
+    V.models = B.models.ptr;
+    V.dates = dates;
+    V.nb = A.nb;
+    V.side = A.side;
+    V.strike = A.strike;
+    V.notional = A.notional;
+    V.unit_values = B.unit_values.ptr;
+    V.stops = want_stops ? B.vstops.ptr : nullptr;
+    V.counts = B.counts.ptr;
+    MCG_CUDA(launch_lsm_bs_value(VP, V, stream));
+    ++launches;
+    MCG_CUDA(launch_lsm_group_sum(B.unit_values.ptr, VP.units, v_groups, 0, nullptr, B.group_partials.ptr,
+                                  group_ctas, s_val, B.means.ptr, stream));
+    launches += 2;
+    if (!rqmc) {
+        MCG_CUDA(launch_lsm_group_sum(B.unit_values.ptr, VP.units, 1, 0, B.means.ptr, B.group_partials.ptr,
+                                      group_ctas, s_sq, nullptr, stream));
+        launches += 2;
+    }
+    MCG_CUDA(cudaEventRecord(B.ev[3], stream));
+
+    std::vector<DD> sums(3 * static_cast<size_t>(max_groups));
+    unsigned long long words[2];
+    std::vector<unsigned long long> counts(dates);
+    MCG_CUDA(cudaMemcpyAsync(sums.data(), B.sums.ptr, sums.size() * sizeof(DD), cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaMemcpyAsync(words, B.words.ptr, sizeof(words), cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaMemcpyAsync(counts.data(), B.counts.ptr, dates * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, stream));
+    if (dates > 1)
+        MCG_CUDA(cudaMemcpyAsync(r->models, B.models.ptr, (dates - 1) * sizeof(mcg_lsm_date_model),
+                                 cudaMemcpyDeviceToHost, stream));
+    if (want_stops)
+        MCG_CUDA(cudaMemcpyAsync(r->stopping_indices, B.vstops.ptr, v_paths * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaStreamSynchronize(stream));
+    if (words[0] != ~0ull) {
+        r->error.code = MCG_ERR_LSM;
+        r->error.sampling_unit = words[0];
+        return fail(MCG_ERR_LSM, "non-finite training spot (NonFiniteFeature) in sampling unit " +
+                                     std::to_string(words[0]));
+    }
+    if (words[1] != ~0ull) {
+        const uint32_t date = static_cast<uint32_t>(words[1] >> 8);
+        r->error.code = MCG_ERR_LSM;
+        r->error.step = date;
+        return fail(MCG_ERR_LSM, "regression of exercise date " + std::to_string(date) +
+                                     " exceeds max_matrix_elements or is not finite");
+    }
+    float ms[3] = {0.f, 0.f, 0.f};
+    cudaEventElapsedTime(&ms[0], B.ev[0], B.ev[1]);
+    cudaEventElapsedTime(&ms[1], B.ev[1], B.ev[2]);
+    cudaEventElapsedTime(&ms[2], B.ev[2], B.ev[3]);
+    r->path_kernel_ms = ms[0];
+    r->regression_ms = ms[1];
+    r->valuation_ms = ms[2];
+    r->device_ms = ms[0] + ms[1] + ms[2];
+    for (uint32_t i = 0; i < dates; ++i) r->exercise_counts[i] = counts[i];
+
+    // In-sample value: mean of the collapsed training values (pseudo) or of
+    // the per-scramble replicates (RQMC), risk/early_exercise.rs:100-110,300-313.
+    if (rqmc) {
+        double s = 0.0, c = 0.0;
+        for (uint32_t g = 0; g < t_groups; ++g)
+            neumaier(s, c, (sums[g].hi + sums[g].lo) / static_cast<double>(TP.units));
+        r->in_sample_value = (s + c) / static_cast<double>(t_groups);
+    } else {
+        r->in_sample_value = (sums[0].hi + sums[0].lo) / static_cast<double>(TP.units);
+    }
+    HostStat hs;
+    uint64_t independent;
+    if (rqmc) {
+        std::vector<double> reps(v_groups);
+        for (uint32_t g = 0; g < v_groups; ++g)
+            reps[g] = (sums[max_groups + g].hi + sums[max_groups + g].lo) / static_cast<double>(VP.units);
+        hs = two_pass(reps);
+        independent = v_groups;
+    } else {
+        const DD tv = sums[max_groups], sq = sums[2 * static_cast<size_t>(max_groups)];
+        hs.sum = tv.hi;
+        hs.corr = tv.lo;
+        hs.count = VP.units;
+        hs.mean = (tv.hi + tv.lo) / static_cast<double>(VP.units);
+        hs.m2 = sq.hi + sq.lo;
+        independent = VP.units;
+    }
+    r->price_statistics = {hs.sum, hs.corr, hs.count, hs.mean, hs.m2};
+    r->price = make_estimate(hs, independent, 1.0);
+    r->sampling_variance = hs.count > 1 ? hs.m2 / static_cast<double>(hs.count - 1) : 0.0;
+    r->estimator_variance = r->sampling_variance / static_cast<double>(independent);
+    r->training_paths = t_paths;
+    r->valuation_paths = v_paths;
+    r->independent_sampling_units = independent;
+    r->date_count = dates;
+    r->kernel_launches = launches;
+    return MCG_OK;
+}
+
 }  // namespace
 
 namespace mcg {
@@ -1068,6 +1338,11 @@ mcg_status mcg_plan_evaluate(mcg_plan* plan, void* stream, mcg_result* result) {
 }
 
 void mcg_plan_destroy(mcg_plan* plan) { delete plan; }
+
+mcg_status mcg_lsm_price(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, void* stream,
+                         mcg_lsm_result* result) {
+    return lsm_price(plan, lsm, static_cast<cudaStream_t>(stream), result);
+}
 
 mcg_status mcg_price(const mcg_plan_desc* desc, void* stream, mcg_result* result) {
     mcg_plan* plan = nullptr;

@@ -41,7 +41,7 @@ __device__ __forceinline__ void report_error(ErrorWord* err, uint64_t unit, int 
 // Normal for dimension `dim` of one unit.  RQMC: scrambled Sobol word as
 // shift XOR the pre-applied scrambled directions of the set Gray-code bits
 // (qmc.rs:71-84,125-132: apply is GF(2)-linear, so apply(XOR v_k) =
-// XOR M v_k ^ shift); pseudo: Philox coordinate (unit, dim, Valuation).
+// XOR M v_k ^ shift); pseudo: Philox coordinate (unit, dim, domain).
 struct NormalSource {
     int32_t rqmc;
     uint64_t seed;
@@ -51,6 +51,7 @@ struct NormalSource {
     const uint32_t* shift;
     uint32_t cached_block;
     uint4 block;
+    uint32_t domain = 0;  // pseudo: RandomDomain (Valuation 0, LsmTrain 1)
 
     __device__ __forceinline__ uint32_t word(uint32_t dim) {
         if (rqmc) {
@@ -66,7 +67,7 @@ struct NormalSource {
         }
         const uint32_t blk = dim >> 2;
         if (blk != cached_block) {
-            block = philox_block(seed, unit, blk, 0u);
+            block = philox_block(seed, unit, blk, domain);
             cached_block = blk;
         }
         return lane_of(block, dim & 3u);

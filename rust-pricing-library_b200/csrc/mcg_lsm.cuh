@@ -1,0 +1,59 @@
+// mcg_lsm.cuh -- argument blocks of the early-exercise kernels (mcg_lsm.cu),
+// shared with the host orchestration (mcg_host.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mcg_plan.h"
+
+namespace mcg {
+
+// An unevaluated double-double sum hi + lo.
+struct DD {
+    double hi, lo;
+};
+
+struct LsmArgs {
+    const double* spots;  // [dates][paths]
+    uint64_t paths;
+    uint32_t dates;
+    uint32_t nb;          // basis columns: max_degree + 1
+    int32_t side;
+    double strike, notional, itm_tol;
+    double abs_tol, rel_tol;
+    unsigned long long max_elements;
+    const double* df;     // [dates] discount factors of the exercise dates
+    double* cf;           // [paths] realised cash flow discounted to time zero
+    uint32_t* stop;       // [paths] stopping date
+    mcg_lsm_date_model* models;  // [dates - 1]
+    DD* partials;         // [CTAs][kLsmPartials]
+    unsigned int* tickets;  // [3] per pass kind, zero between launches
+    unsigned long long* lsm_error;  // (date << 8) | code of the first failing date, atomicMin
+};
+
+struct LsmValueArgs {
+    const double* df;
+    const mcg_lsm_date_model* models;
+    uint32_t dates, nb;
+    int32_t side;
+    double strike, notional;
+    double* unit_values;               // [scrambles * units]: collapsed discounted value
+    uint32_t* stops;                   // [paths] or null
+    unsigned long long* counts;        // [dates]
+};
+
+cudaError_t launch_lsm_bs_spots(const DevicePlan& P, uint32_t domain, double* spots, uint64_t paths,
+                                unsigned long long* bad, cudaStream_t stream);
+cudaError_t launch_lsm_sweep(const LsmArgs& A, unsigned ctas, int init, int update, int gather,
+                             cudaStream_t stream);
+cudaError_t launch_lsm_variance(const LsmArgs& A, unsigned ctas, int d, cudaStream_t stream);
+cudaError_t launch_lsm_gram(const LsmArgs& A, unsigned ctas, int d, cudaStream_t stream);
+cudaError_t launch_lsm_bs_value(const DevicePlan& P, const LsmValueArgs& V, cudaStream_t stream);
+cudaError_t launch_lsm_group_sum(const double* values, uint64_t per_group, uint32_t groups, int pairs,
+                                 const double* centers, DD* partials, unsigned ctas, DD* out, double* means,
+                                 cudaStream_t stream);
+size_t lsm_partial_stride();
+
+}  // namespace mcg

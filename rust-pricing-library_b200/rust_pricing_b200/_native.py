@@ -18,6 +18,7 @@ EXPORTS = (
     "mcg_abi_version", "mcg_last_error", "mcg_plan_create", "mcg_plan_evaluate", "mcg_price",
     "mcg_plan_destroy", "mcg_plan_shape", "mcg_philox_normals", "mcg_rqmc_words",
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
+    "mcg_lsm_price",
 )
 
 _lib = None
@@ -68,6 +69,8 @@ def library() -> C.CDLL:
     lib.mcg_price_european_noalloc.restype = C.c_int
     lib.mcg_measure_fp64_peak.argtypes = [vp, C.POINTER(dbl)]
     lib.mcg_measure_fp64_peak.restype = C.c_int
+    lib.mcg_lsm_price.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.LsmDesc), vp, C.POINTER(A.LsmResult)]
+    lib.mcg_lsm_price.restype = C.c_int
     if lib.mcg_abi_version() != A.ABI_VERSION:
         raise EngineError(1, "engine library ABI version mismatch")
     _lib = lib
@@ -77,6 +80,17 @@ def library() -> C.CDLL:
 def check(status: int, error: A.ErrorRecord | None = None) -> None:
     if status != 0:
         raise EngineError(status, library().mcg_last_error().decode(), error)
+
+
+def lsm_price(spec, lsm, stopping: bool = False, stream: int = 0) -> A.LsmBuffers:
+    """mcg_lsm_price: train and value an early-exercise policy on the GPU."""
+    paths = spec.sampling_units * (spec.scramble_count if spec.engine == A.ENGINE_RQMC else 1)
+    paths *= 2 if spec.antithetic else 1
+    buf = A.LsmBuffers(len(spec.observation_times), paths if stopping else 0)
+    desc, ldesc = spec.desc(), lsm.desc()
+    status = library().mcg_lsm_price(C.byref(desc), C.byref(ldesc), C.c_void_p(stream), C.byref(buf.result))
+    check(status, buf.result.error)
+    return buf
 
 
 class Plan:

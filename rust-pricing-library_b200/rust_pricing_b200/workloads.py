@@ -12,6 +12,9 @@ crates/pricing/examples/benchmark_european_bs.rs).
                       rebate 1, priced on the same draws.
 * local_vol_adjoint -- the same surface, continuous down-and-out call with
                       compact-C2 smoothing 0.5 (0.5% of spot).
+* american_bs      -- American put by LSM: S=K=100, r=5%, q=0, sigma=25%, T=1,
+                      50 equally spaced exercise dates, cubic basis in spot,
+                      CPQR tolerances 1e-14 / 1e-12, ITM tolerance 0.
 """
 from __future__ import annotations
 
@@ -21,7 +24,7 @@ from typing import Callable, Optional
 import numpy as np
 
 from . import _abi as A
-from .desc import LocalVarianceSpec, PlanSpec, ProductSpec
+from .desc import LocalVarianceSpec, LsmSpec, PlanSpec, ProductSpec
 
 SEED = 0x0123456789ABCDEF
 RATE, DIVIDEND = 0.03, 0.01
@@ -124,3 +127,22 @@ def local_vol_adjoint(builder: GridBuilder, paths: int = 1 << 20, steps: int = 2
                     brownian_bridge=True, spot=100.0, local_variance=local_vol_grid(surface, builder),
                     smoothing_half_width=smoothing, request_delta=risk, request_gamma=risk,
                     gamma_bump=0.01, **flat_curves())
+
+
+def american_bs(dates: int = 50, units: int = 1 << 20, training_units: Optional[int] = None,
+                engine: int = A.ENGINE_PSEUDO, antithetic: bool = False, scrambles: int = 4,
+                max_degree: int = 3, vol: float = 0.25, rate: float = 0.05, strike: float = 100.0,
+                side: int = A.PUT, horizon: float = 1.0) -> tuple[PlanSpec, LsmSpec]:
+    """An American (Bermudan) option with `dates` equally spaced exercise dates
+    and its LsmConfig: pseudo `units` sampling units (RQMC: points per
+    scramble) for valuation and `training_units` for training."""
+    times = [horizon * i / dates for i in range(1, dates + 1)]
+    spec = PlanSpec(
+        observation_times=times, products=[ProductSpec(kind=A.PRODUCT_AMERICAN, side=side, strike=strike)],
+        model=A.MODEL_BLACK_SCHOLES, engine=engine, master_seed=SEED, sampling_units=units,
+        scramble_count=scrambles, antithetic=antithetic, volatility=vol, spot=100.0,
+        **flat_curves(rate, 0.0, horizon))
+    lsm = LsmSpec(training_seed=SEED ^ 0x5DEECE66D, training_units=training_units or units,
+                  training_scramble_count=scrambles, training_antithetic=antithetic, max_degree=max_degree,
+                  max_matrix_elements=1 << 40)
+    return spec, lsm

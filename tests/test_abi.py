@@ -46,6 +46,7 @@ STRUCTS = {
     "mcg_product_desc": A.ProductDesc, "mcg_plan_desc": A.PlanDesc, "mcg_statistics": A.Statistics,
     "mcg_estimate": A.Estimate, "mcg_product_result": A.ProductResult,
     "mcg_error_record": A.ErrorRecord, "mcg_result": A.Result,
+    "mcg_lsm_desc": A.LsmDesc, "mcg_lsm_date_model": A.LsmDateModel, "mcg_lsm_result": A.LsmResult,
 }
 
 
