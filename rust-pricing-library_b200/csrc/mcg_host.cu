@@ -1038,7 +1038,7 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
 
 // Device buffers of one mcg_lsm_price call, released on every return path.
 struct LsmBuffers {
-    DeviceArray<double> spots, cf, df, unit_values, means;
+    DeviceArray<double> spots, cf, df, unit_values, means, centers;
     DeviceArray<uint32_t> stop, vstops;
     DeviceArray<mcg_lsm_date_model> models;
     DeviceArray<DD> partials, group_partials, sums;
@@ -1051,6 +1051,7 @@ struct LsmBuffers {
         df.release();
         unit_values.release();
         means.release();
+        centers.release();
         stop.release();
         vstops.release();
         models.release();
@@ -1142,6 +1143,7 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     MCG_CUDA(B.cf.alloc(t_paths));
     MCG_CUDA(B.stop.alloc(t_paths));
     MCG_CUDA(B.df.upload(df));
+    MCG_CUDA(B.centers.upload(std::vector<double>(dates, d->products[0].strike)));
     MCG_CUDA(B.models.alloc(std::max<uint32_t>(dates - 1, 1)));
     MCG_CUDA(B.partials.alloc(static_cast<size_t>(ctas) * lsm_partial_stride()));
     MCG_CUDA(B.tickets.alloc(3));
@@ -1182,17 +1184,20 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     A.cf = B.cf.ptr;
     A.stop = B.stop.ptr;
     A.models = B.models.ptr;
+    A.centers = B.centers.ptr;
     A.partials = B.partials.ptr;
     A.tickets = B.tickets.ptr;
     A.lsm_error = &B.words.ptr[1];
     const int last = static_cast<int>(dates) - 1;
-    MCG_CUDA(launch_lsm_sweep(A, ctas, 1, -1, last - 1, stream));
+    MCG_CUDA(launch_lsm_init(A, ctas, stream));
     ++launches;
+    if (last >= 1) {
+        MCG_CUDA(launch_lsm_step(A, ctas, -1, last - 1, stream));
+        ++launches;
+    }
     for (int date = last - 1; date >= 0; --date) {
-        MCG_CUDA(launch_lsm_variance(A, ctas, date, stream));
-        MCG_CUDA(launch_lsm_gram(A, ctas, date, stream));
-        MCG_CUDA(launch_lsm_sweep(A, ctas, 0, date, date - 1, stream));
-        launches += 3;
+        MCG_CUDA(launch_lsm_step(A, ctas, date, date - 1, stream));
+        ++launches;
     }
     // In-sample value of the training paths under their own policy.
     DD* s_in = B.sums.ptr;

@@ -20,18 +20,16 @@
 // realised * df[stop] / df[d] is then cf / df[d], bit for bit), and its
 // stopping date.
 //
-// Backward induction, per non-terminal date d (three launches):
-//   sweep(d):    applies the decision of date d+1 to every path (exercise if
-//                immediate > continuation) while summing the residuals of that
-//                date's fit, and gathers count, sum and max |S| of the ITM rows
-//                of date d;
-//   variance(d): the population variance of the ITM spots about their mean;
-//   gram(d):     the Gram matrix of the standardised monomial basis and its
-//                right-hand side over the ITM rows; the last CTA solves.
-// Every sum is an error-free double-double accumulation (TwoSum, FMA TwoProd)
-// reduced in a fixed order, so it is the exactly rounded sum the reference's
-// sequential Neumaier sums approximate.  The last CTA to finish a pass (a
-// ticket counter, no waiting) merges the per-CTA partials and finalises.
+// Backward induction: one launch per non-terminal date d.  Each thread takes
+// its paths through the decision of date d+1 (exercise if immediate >
+// continuation, summing that fit's residuals) and, with the updated cash
+// flow, adds its ITM rows of date d to power sums of the spot about a centre
+// c near their mean, P_k = sum (S - c)^k (k <= 2 degree) and T_k = sum (S - c)^k y.
+// Mean, population variance and the Gram matrix of the standardised monomial
+// basis all follow from these sums by a binomial shift, so one pass replaces
+// the reference's three (scaling, design matrix, QR).  Every sum is a
+// compensated (TwoSum) double-double accumulation reduced in a fixed order.  The last CTA to finish (a
+// ticket counter, no waiting) merges the per-CTA partials and fits the date.
 //
 // The solve.  The reference runs Householder QR with column pivoting on the
 // ITM design matrix.  In exact arithmetic the pivot sequence, |R_kk| and the
@@ -154,7 +152,7 @@ __device__ __forceinline__ bool dd_equal(DD a, DD b) { return a.hi == b.hi && a.
 // ------------------------------------------------------------- arguments
 
 
-constexpr int kLsmPartials = kLsmMaxBasis * (kLsmMaxBasis + 1) / 2 + 2 * kLsmMaxBasis + 4;
+constexpr int kLsmPartials = (2 * kLsmMaxBasis - 1) + kLsmMaxBasis + 2;  // step-kernel sums + count/max
 
 // The fields of a date model the decisions read.
 struct Policy {
@@ -231,19 +229,47 @@ __device__ bool cta_reduce_publish(DD (&v)[K], DD* partials, unsigned int* ticke
     return s_last != 0;
 }
 
-// In the last CTA: merges the partials of every CTA for k < K in block order
-// (a lane-strided pass per warp, then a butterfly), into smem[k].
-template <int K>
+// In the last CTA: merges the partials of every CTA.  Components k < K are
+// double-double sums; with EXTRA, component K is a (count, max) pair.  Thread
+// (k, g) of C = K + EXTRA components and G = threads / C groups merges the
+// CTAs g, g + G, ... of component k; thread k then merges the G groups in
+// order into out[k].  Deterministic for a given grid.
+template <int K, bool EXTRA>
 __device__ void merge_partials(const DD* partials, DD* out) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < K; k += kLsmWarps) {
-        DD acc = {0.0, 0.0};
-        for (uint32_t b = lane; b < gridDim.x; b += 32) {
+    constexpr int C = K + (EXTRA ? 1 : 0);
+    constexpr int G = kLsmThreads / C;
+    __shared__ DD s_part[kLsmThreads];
+    const int t = threadIdx.x;
+    const int k = t % C, g = t / C;
+    const bool pair = EXTRA && k == K;
+    DD acc = {0.0, pair ? 1.0 : 0.0};
+    if (g < G) {
+#pragma unroll 4
+        for (uint32_t b = g; b < gridDim.x; b += G) {
             const DD* p = partials + static_cast<size_t>(b) * kLsmPartials + k;
-            acc = acc_merge(acc, DD{__ldcg(&p->hi), __ldcg(&p->lo)});
+            const DD q = {__ldcg(&p->hi), __ldcg(&p->lo)};
+            if (pair) {
+                acc.hi += q.hi;  // counts: exact integers below 2^53
+                acc.lo = fmax(acc.lo, q.lo);
+            } else {
+                acc = acc_merge(acc, q);
+            }
         }
-        acc = warp_reduce_dd(acc);
-        if (lane == 0) out[k] = acc;
+    }
+    s_part[t] = acc;
+    __syncthreads();
+    if (t < C) {
+        DD m = s_part[t];
+        for (int gg = 1; gg < G; ++gg) {
+            const DD q = s_part[gg * C + t];
+            if (pair) {
+                m.hi += q.hi;
+                m.lo = fmax(m.lo, q.lo);
+            } else {
+                m = acc_merge(m, q);
+            }
+        }
+        out[t] = m;
     }
     __syncthreads();
 }
@@ -304,59 +330,352 @@ __global__ void __launch_bounds__(kLsmThreads) lsm_bs_spots_kernel(const DeviceP
     if (!finite) atomicMin(bad, unit);
 }
 
-// ------------------------------------------------------------- training sweep
+// ------------------------------------------------------------- training step
 
-// One pass over every training path: initialise (first pass), apply the
-// decision of date `update` and sum that fit's residuals over its ITM rows,
-// and gather the ITM count, spot sum and max |spot| of date `gather`.
-__global__ void __launch_bounds__(kLsmThreads) lsm_sweep_kernel(const LsmArgs A, int init, int update,
-                                                                int gather) {
-    __shared__ DD s_red[kLsmWarps * 2];
+// Adds a double-double value to an accumulator.
+__device__ __forceinline__ DD acc_add_dd(DD a, DD b) {
+    double s, e;
+    two_sum(a.hi, b.hi, s, e);
+    return {s, a.lo + (e + b.lo)};
+}
+
+// Binomial coefficients for the shift of the power sums.
+__device__ __forceinline__ double binomial(int n, int k) {
+    // C(n, k) = n! / (k! (n - k)!) by the multiplicative formula over exact
+    // integers (every intermediate product is an integer below 2^53).
+    double c = 1.0;
+    for (int i = 1; i <= k; ++i) c = (c * static_cast<double>(n - k + i)) / static_cast<double>(i);
+    return c;
+}
+
+// The CPQR-equivalent solve of one date, run by one thread.  G (NB x NB) and
+// r (NB) are the Gram matrix and right-hand side of the standardised monomial
+// basis, double-double.  Pivoted Cholesky: the pivot is the largest remaining
+// squared column norm (the Schur-complement diagonal), ties to the smaller
+// basis column, as fit_cpqr chooses (lsm.rs:2441-2459); |R_kk|, the rank
+// threshold max(abs, rel * |R_00|) and the back substitution over the leading
+// `rank` pivots follow lsm.rs:2500-2533.
+template <int NB>
+__device__ void lsm_solve(const LsmArgs& A, mcg_lsm_date_model& m, int na, DD (&S)[NB][NB], DD (&b)[NB]) {
+    // Every array index below is a compile-time constant after unrolling, so
+    // the factorisation lives in registers; pivot swaps are predicated.
+    DD R[NB][NB], qty[NB], inv_diag[NB];
+    int perm[NB];
+    double diag[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        perm[i] = i;
+        qty[i] = dd_from(0.0);
+        diag[i] = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) R[i][j] = dd_from(0.0);
+    }
+    const int dcount = static_cast<int>(m.itm_rows) < na ? static_cast<int>(m.itm_rows) : na;
+#pragma unroll
+    for (int p = 0; p < NB; ++p) {
+        if (p >= dcount) break;
+        int sel = p;
+        DD best = S[p][p];
+        int best_perm = perm[p];
+#pragma unroll
+        for (int c = p + 1; c < NB; ++c) {
+            if (c >= na) break;
+            if (dd_greater(S[c][c], best) || (dd_equal(S[c][c], best) && perm[c] < best_perm)) {
+                sel = c;
+                best = S[c][c];
+                best_perm = perm[c];
+            }
+        }
+#pragma unroll
+        for (int c = p + 1; c < NB; ++c) {
+            if (c != sel) continue;
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                const DD t = S[k][p];
+                S[k][p] = S[k][c];
+                S[k][c] = t;
+            }
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                const DD t = S[p][k];
+                S[p][k] = S[c][k];
+                S[c][k] = t;
+            }
+#pragma unroll
+            for (int k = 0; k < p; ++k) {
+                const DD t = R[k][p];
+                R[k][p] = R[k][c];
+                R[k][c] = t;
+            }
+            const DD tb = b[p];
+            b[p] = b[c];
+            b[c] = tb;
+            const int tp = perm[p];
+            perm[p] = perm[c];
+            perm[c] = tp;
+        }
+        if (!(S[p][p].hi > 0.0)) continue;  // an exactly zero remaining column (lsm.rs:2461-2465)
+        const DD r = dd_sqrt(S[p][p]);
+        const DD inv_r = dd_div(dd_from(1.0), r);
+        R[p][p] = r;
+        inv_diag[p] = inv_r;
+#pragma unroll
+        for (int c = p + 1; c < NB; ++c)
+            if (c < na) R[p][c] = dd_mul(S[p][c], inv_r);
+#pragma unroll
+        for (int i = p + 1; i < NB; ++i)
+#pragma unroll
+            for (int j = i; j < NB; ++j)
+                if (j < na) {
+                    S[i][j] = dd_sub(S[i][j], dd_mul(R[p][i], R[p][j]));
+                    S[j][i] = S[i][j];
+                }
+        DD acc = b[p];
+#pragma unroll
+        for (int k = 0; k < p; ++k) acc = dd_sub(acc, dd_mul(R[k][p], qty[k]));
+        qty[p] = dd_mul(acc, inv_r);
+        diag[p] = fabs(dd_round(r));
+    }
+    const double first = dcount > 0 ? diag[0] : 0.0;
+    const double threshold = fmax(A.abs_tol, A.rel_tol * first);
+    int rank = 0;
+#pragma unroll
+    for (int p = 0; p < NB; ++p)
+        if (rank == p && p < dcount && diag[p] > threshold) ++rank;
+    DD coef[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) coef[i] = dd_from(0.0);
+#pragma unroll
+    for (int r = NB - 1; r >= 0; --r) {
+        if (r >= rank) continue;
+        DD acc = qty[r];
+#pragma unroll
+        for (int k = r + 1; k < NB; ++k)
+            if (k < rank) acc = dd_sub(acc, dd_mul(R[r][k], coef[k]));
+        coef[r] = dd_mul(acc, inv_diag[r]);
+    }
+    m.regression = 1;
+    m.active_columns = static_cast<uint32_t>(na);
+    m.diagonal_count = static_cast<uint32_t>(dcount);
+    m.rank = static_cast<uint32_t>(rank);
+    m.rank_threshold = threshold;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        if (k < na) m.pivot_order[k] = static_cast<uint32_t>(perm[k]);
+        if (k < dcount) m.diagonal_abs[k] = diag[k];
+    }
+    // coefficients back in basis order: coefficient of column perm[k] is coef[k]
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+            if (k < na && perm[k] == c) v = dd_round(coef[k]);
+        m.coefficients[c] = v;
+    }
+}
+
+// Fits date `d` from its merged sums, in the last CTA (every thread calls
+// it): n ITM rows, max |S|, the power sums P_k = sum (S - c)^k, k < 2 NB - 1,
+// about the date's centre c, and T_k = sum (S - c)^k y, k < NB, of the
+// targets y.  The feature scaling of FeatureScaling::fit (lsm.rs:537-574) comes
+// from the mean m = (n c + P_1) / n and the central sums M_k = sum (S - m)^k,
+// obtained from the P_k by the binomial shift in double-double (one thread per
+// k); the standardised Gram matrix is M_{i+j} / s^{i+j} (one thread per
+// entry); one thread factorises.  The mean becomes the centre of date d - 1.
+template <int NB>
+__device__ void lsm_fit_date(const LsmArgs& A, int d, unsigned long long n, double maxabs, const DD* P,
+                             const DD* T) {
+    constexpr int NP = 2 * NB - 1;
+    __shared__ DD s_M[NP], s_U[NB], s_G[NB][NB], s_rhs[NB], s_inv[NP];
+    __shared__ int s_go;
+    mcg_lsm_date_model& m = A.models[d];
+    const double c = A.centers[d];
+    const double nd = static_cast<double>(n);
+    // sum.total() / len and squared_deviations.total() / len: the rounded sum,
+    // then one division, as the reference rounds them.
+    const double mean = n ? dd_round(dd_add(dd_mul_d(dd_from(c), nd), dd_norm(P[1]))) / nd : 0.0;
+    double dh, dl;
+    two_sum(mean, -c, dh, dl);  // delta = mean - c exactly
+    const DD neg_delta = dd_neg(quick_two_sum(dh, dl));
+    const int t = threadIdx.x;
+    if (n && t < NP + NB) {
+        // t < NP: M_t = sum_j C(t, j) (-delta)^(t - j) P_j; else U_i likewise from T.
+        const int k = t < NP ? t : t - NP;
+        const DD* src = t < NP ? P : T;
+        DD acc = dd_from(0.0), pw = dd_from(1.0);
+        for (int j = k; j >= 0; --j) {
+            acc = dd_add(acc, dd_mul(dd_mul_d(pw, binomial(k, j)), dd_norm(src[j])));
+            pw = dd_mul(pw, neg_delta);
+        }
+        if (t < NP) s_M[k] = acc;
+        else s_U[k] = acc;
+    }
+    __syncthreads();
+    if (t == 0) {
+        m.candidate_rows = static_cast<uint32_t>(A.paths);
+        m.itm_rows = static_cast<uint32_t>(n);
+        m.regression = 0;
+        s_go = 0;
+        if (n && d > 0) A.centers[d - 1] = mean;
+        if (n == 0) {
+            // ContinueAll { ZeroItmTrainingPaths }
+        } else if (n > A.max_elements) {
+            lsm_fail(A.lsm_error, static_cast<uint32_t>(d));
+        } else {
+            const double variance = dd_round(s_M[2]) / nd;
+            const double scale = sqrt(variance);
+            const double threshold = (64.0 * kEpsilon64) * maxabs;
+            const bool inactive = scale <= threshold;
+            m.feature_mean = mean;
+            m.feature_variance = variance;
+            m.feature_scale = scale;
+            m.zero_scale_threshold = threshold;
+            m.feature_inactive = inactive ? 1 : 0;
+            if (n * static_cast<unsigned long long>(inactive ? 1 : NB) > A.max_elements) {
+                lsm_fail(A.lsm_error, static_cast<uint32_t>(d));
+            } else {
+                const DD inv_s = inactive ? dd_from(0.0) : dd_div(dd_from(1.0), dd_from(scale));
+                s_inv[0] = dd_from(1.0);
+                for (int k = 1; k < NP; ++k) s_inv[k] = dd_mul(s_inv[k - 1], inv_s);
+                s_go = 1;
+            }
+        }
+    }
+    __syncthreads();
+    if (!s_go) return;
+    if (t < NB * NB) {
+        const int i = t / NB, j = t % NB;
+        s_G[i][j] = dd_mul(s_M[i + j], s_inv[i + j]);
+    } else if (t < NB * NB + NB) {
+        const int i = t - NB * NB;
+        s_rhs[i] = dd_mul(s_U[i], s_inv[i]);
+    }
+    __syncthreads();
+    if (t == 0) {
+        DD G[NB][NB], rhs[NB];
+        for (int i = 0; i < NB; ++i) {
+            rhs[i] = s_rhs[i];
+            for (int j = 0; j < NB; ++j) G[i][j] = s_G[i][j];
+        }
+        lsm_solve<NB>(A, m, m.feature_inactive ? 1 : NB, G, rhs);
+        for (int k = 0; k < NB; ++k)
+            if (!isfinite(m.coefficients[k])) lsm_fail(A.lsm_error, static_cast<uint32_t>(d));
+    }
+}
+
+// The expiry cash flows cf = immediate(T) * df(T), stop = T of every training
+// path, and the mean of the ITM spots of the last non-terminal date, the
+// centre of that date's power sums.
+__global__ void __launch_bounds__(kLsmThreads) lsm_init_kernel(const LsmArgs A) {
+    __shared__ DD s_red[kLsmWarps];
     __shared__ DD s_fin[2];
+    __shared__ unsigned long long s_cnt[kLsmWarps];
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint32_t last = A.dates - 1;
+    double sum = 0.0;
+    unsigned long long cnt = 0;
+    for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.paths; p += stride) {
+        const double x = A.spots[static_cast<size_t>(last) * A.paths + p];
+        A.cf[p] = intrinsic(A.side, A.strike, A.notional, x) * A.df[last];
+        A.stop[p] = last;
+        if (last > 0) {
+            const double g = A.spots[static_cast<size_t>(last - 1) * A.paths + p];
+            if (intrinsic(A.side, A.strike, A.notional, g) > A.itm_tol) {
+                ++cnt;
+                sum += g;
+            }
+        }
+    }
+    DD acc[1] = {{sum, 0.0}};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    if (lane == 0) s_cnt[warp] = cnt;
+    __syncthreads();
+    DD extra = {0.0, 0.0};
+    if (threadIdx.x == 0) {
+        unsigned long long total = 0;
+        for (int w = 0; w < kLsmWarps; ++w) total += s_cnt[w];
+        extra = {static_cast<double>(total), 0.0};
+    }
+    if (!cta_reduce_publish<1>(acc, A.partials, &A.tickets[1], s_red, &extra)) return;
+    merge_partials<1, true>(A.partials, s_fin);
+    if (threadIdx.x == 0) {
+        const unsigned long long n = static_cast<unsigned long long>(s_fin[1].hi);
+        if (n && last > 0) A.centers[last - 1] = dd_round(s_fin[0]) / static_cast<double>(n);
+        A.tickets[1] = 0;
+    }
+}
+
+// One backward-induction step over every training path, one launch per date:
+//   * `update` >= 0: the decision of that date (exercise when immediate >
+//     continuation, for every path, lsm.rs:1604-1614) and the residual squares
+//     of its ITM rows against the pre-update targets (the fit's residual sum,
+//     lsm.rs:2535-2550);
+//   * `gather` >= 0: the ITM rows of that date with their targets cf / df
+//     (lsm.rs:1586-1597) after the update, as compensated power sums of
+//     u = S - c about the date's centre c (the ITM mean of the next date, close
+//     to this date's mean, so the binomial shift to the exact mean amplifies
+//     the per-term rounding of u^k by a factor near one).
+// The last CTA merges every CTA's sums in CTA order and fits `gather`.
+template <int NB>
+__global__ void __launch_bounds__(kLsmThreads, 2) lsm_step_kernel(const LsmArgs A, int update, int gather) {
+    constexpr int NP = 2 * NB - 1;
+    constexpr int K = NP + NB + 1;  // power sums, target sums, residual squares
+    static_assert(K + 1 <= kLsmPartials && K <= kLsmThreads && NB * NB + NB <= kLsmThreads,
+                  "partials stride or CTA too small");
+    __shared__ DD s_red[kLsmWarps * K];
+    __shared__ DD s_fin[K + 1];
     __shared__ unsigned long long s_cnt[kLsmWarps];
     __shared__ double s_max[kLsmWarps];
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    const uint32_t last = A.dates - 1;
     Policy mu{};
     if (update >= 0) mu = policy_of(A.models[update], A.nb);
     const bool decide = update >= 0 && mu.regression;
     const double df_u = update >= 0 ? A.df[update] : 1.0;
-    DD acc[2] = {{0.0, 0.0}, {0.0, 0.0}};  // residual squares of `update`, ITM spot sum of `gather`
+    const double df_g = gather >= 0 ? A.df[gather] : 1.0;
+    const double c = gather >= 0 ? A.centers[gather] : 0.0;
+    // Per-thread partial sums are plain (a thread sees a few dozen paths); the
+    // cross-thread and cross-CTA merges are double-double.
+    double part[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[k] = 0.0;
     unsigned long long cnt = 0;
     double maxabs = 1.0;
     for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.paths; p += stride) {
-        double cf;
-        if (init) {
-            const double x = A.spots[static_cast<size_t>(last) * A.paths + p];
-            cf = intrinsic(A.side, A.strike, A.notional, x) * A.df[last];
-            A.stop[p] = last;
-        } else {
-            cf = A.cf[p];
-        }
+        double cf = A.cf[p];
         if (decide) {
             const double x = A.spots[static_cast<size_t>(update) * A.paths + p];
             const double imm = intrinsic(A.side, A.strike, A.notional, x);
-            const double cont = predict(mu, A.nb, x);
+            const double cont = predict(mu, NB, x);
             if (imm > A.itm_tol) {
                 const double res = cf / df_u - cont;
-                acc[0] = acc_add(acc[0], res * res);
+                part[K - 1] += res * res;
             }
             if (imm > cont) {
                 cf = imm * df_u;
                 A.stop[p] = static_cast<uint32_t>(update);
             }
         }
-        if (init || decide) A.cf[p] = cf;
+        if (decide) A.cf[p] = cf;
         if (gather >= 0) {
             const double x = A.spots[static_cast<size_t>(gather) * A.paths + p];
             if (intrinsic(A.side, A.strike, A.notional, x) > A.itm_tol) {
                 ++cnt;
-                acc[1] = acc_add(acc[1], x);
                 maxabs = fmax(maxabs, fabs(x));
+                const double u = x - c;
+                const double y = cf / df_g;
+                double pw = 1.0;
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    if (k) pw *= u;
+                    part[k] += pw;
+                    if (k < NB) part[NP + k] += pw * y;
+                }
             }
         }
     }
-    // integer count and maximum: exact in any order
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -370,234 +689,26 @@ __global__ void __launch_bounds__(kLsmThreads) lsm_sweep_kernel(const LsmArgs A,
     __syncthreads();
     DD extra = {0.0, 1.0};  // the CTA's ITM count and max |spot|, both exact as doubles
     if (threadIdx.x == 0) {
-        unsigned long long c = 0;
-        double m = 1.0;
-        for (int w = 0; w < kLsmWarps; ++w) {
-            c += s_cnt[w];
-            m = fmax(m, s_max[w]);
-        }
-        extra = {static_cast<double>(c), m};
-    }
-    if (!cta_reduce_publish<2>(acc, A.partials, &A.tickets[0], s_red, &extra)) return;
-    merge_partials<2>(A.partials, s_fin);
-    if (threadIdx.x == 0) {
         unsigned long long total = 0;
-        double m = 1.0;
-        for (uint32_t b = 0; b < gridDim.x; ++b) {
-            const DD* q = A.partials + static_cast<size_t>(b) * kLsmPartials + 2;
-            total += static_cast<unsigned long long>(__ldcg(&q->hi));
-            m = fmax(m, __ldcg(&q->lo));
+        double mx = 1.0;
+        for (int w = 0; w < kLsmWarps; ++w) {
+            total += s_cnt[w];
+            mx = fmax(mx, s_max[w]);
         }
-        if (decide) A.models[update].residual_sum_squares = dd_round(s_fin[0]);
-        if (gather >= 0) {
-            mcg_lsm_date_model& g = A.models[gather];
-            g.candidate_rows = static_cast<uint32_t>(A.paths);
-            g.itm_rows = static_cast<uint32_t>(total);
-            g.regression = 0;
-            if (total > 0) {
-                g.feature_mean = dd_round(s_fin[1]) / static_cast<double>(total);
-                g.zero_scale_threshold = (64.0 * kEpsilon64) * m;
-                if (total > A.max_elements) lsm_fail(A.lsm_error, static_cast<uint32_t>(gather));
-            }
-        }
-        A.tickets[0] = 0;
+        extra = {static_cast<double>(total), mx};
     }
-}
-
-// Population variance of the ITM spots of date `d` about their mean
-// (FeatureScaling::fit, lsm.rs:537-574).
-__global__ void __launch_bounds__(kLsmThreads) lsm_variance_kernel(const LsmArgs A, int d) {
-    __shared__ DD s_red[kLsmWarps * 1];
-    __shared__ DD s_fin[1];
-    const mcg_lsm_date_model m = A.models[d];
-    if (m.itm_rows == 0) return;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    DD acc[1] = {{0.0, 0.0}};
-    for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.paths; p += stride) {
-        const double x = A.spots[static_cast<size_t>(d) * A.paths + p];
-        if (intrinsic(A.side, A.strike, A.notional, x) > A.itm_tol) {
-            const double dv = x - m.feature_mean;
-            acc[0] = acc_add(acc[0], dv * dv);
-        }
-    }
-    if (!cta_reduce_publish<1>(acc, A.partials, &A.tickets[1], s_red)) return;
-    merge_partials<1>(A.partials, s_fin);
-    if (threadIdx.x == 0) {
-        mcg_lsm_date_model& g = A.models[d];
-        g.feature_variance = dd_round(s_fin[0]) / static_cast<double>(m.itm_rows);
-        g.feature_scale = sqrt(g.feature_variance);
-        g.feature_inactive = g.feature_scale <= g.zero_scale_threshold ? 1 : 0;
-        A.tickets[1] = 0;
-    }
-}
-
-// The CPQR-equivalent solve of one date (one thread).  `gram` holds the upper
-// triangle of the NB x NB Gram matrix row by row, the NB right-hand sides, and
-// the NB sums of rounded squares fl(b_j * b_j): the reference's first pivot
-// compares exactly those column norms (column_squared_norm, lsm.rs:2594-2613),
-// and for standardised data sum z^2 ties with sum 1 = n in exact arithmetic, so
-// the first choice is made on the same rounded quantities.  Later pivots use
-// the Schur-complement diagonals.
-template <int NB>
-__device__ void lsm_solve(const LsmArgs& A, int d, const DD* gram) {
-    mcg_lsm_date_model& m = A.models[d];
-    const uint32_t rows = m.itm_rows;
-    const int na = m.feature_inactive ? 1 : NB;  // active basis columns: all, or z^0 alone
-    if (static_cast<unsigned long long>(rows) * static_cast<unsigned long long>(na) > A.max_elements) {
-        lsm_fail(A.lsm_error, static_cast<uint32_t>(d));
-        return;
-    }
-    DD S[NB][NB], b[NB], R[NB][NB], qty[NB];
-    int perm[NB];
-    int idx = 0;
-    for (int i = 0; i < NB; ++i)
-        for (int j = i; j < NB; ++j) {
-            S[i][j] = gram[idx];
-            S[j][i] = gram[idx];
-            ++idx;
-        }
-    for (int i = 0; i < NB; ++i) {
-        b[i] = gram[idx + i];
-        perm[i] = i;
-        qty[i] = dd_from(0.0);
-        for (int j = 0; j < NB; ++j) R[i][j] = dd_from(0.0);
-    }
-    for (int i = 0; i < na; ++i)
-        for (int j = 0; j < na; ++j) S[i][j] = dd_norm(S[i][j]);
-    for (int i = 0; i < na; ++i) b[i] = dd_norm(b[i]);
-    const int dcount = static_cast<int>(rows) < na ? static_cast<int>(rows) : na;
-    const DD* rounded_squares = gram + idx + NB;
-    double diag[NB];
-    for (int p = 0; p < dcount; ++p) {
-        // pivot: the largest remaining squared norm, ties to the smaller basis column
-        int sel = p;
-        if (p == 0) {
-            double best = -1.0;
-            for (int c = 0; c < na; ++c) {
-                const double sn = dd_round(rounded_squares[c]);
-                if (sn > best || (sn == best && perm[c] < perm[sel])) {
-                    sel = c;
-                    best = sn;
-                }
-            }
-        } else {
-            DD best = S[p][p];
-            for (int c = p + 1; c < na; ++c)
-                if (dd_greater(S[c][c], best) || (dd_equal(S[c][c], best) && perm[c] < perm[sel])) {
-                    sel = c;
-                    best = S[c][c];
-                }
-        }
-        if (sel != p) {
-            for (int k = 0; k < na; ++k) {
-                const DD t = S[k][p];
-                S[k][p] = S[k][sel];
-                S[k][sel] = t;
-            }
-            for (int k = 0; k < na; ++k) {
-                const DD t = S[p][k];
-                S[p][k] = S[sel][k];
-                S[sel][k] = t;
-            }
-            for (int k = 0; k < p; ++k) {
-                const DD t = R[k][p];
-                R[k][p] = R[k][sel];
-                R[k][sel] = t;
-            }
-            const DD tb = b[p];
-            b[p] = b[sel];
-            b[sel] = tb;
-            const int tp = perm[p];
-            perm[p] = perm[sel];
-            perm[sel] = tp;
-        }
-        if (!(S[p][p].hi > 0.0)) {  // an exactly zero remaining column (lsm.rs:2461-2465)
-            diag[p] = 0.0;
-            continue;
-        }
-        const DD r = dd_sqrt(S[p][p]);
-        R[p][p] = r;
-        for (int c = p + 1; c < na; ++c) R[p][c] = dd_div(S[p][c], r);
-        for (int i = p + 1; i < na; ++i)
-            for (int j = p + 1; j < na; ++j) S[i][j] = dd_sub(S[i][j], dd_mul(R[p][i], R[p][j]));
-        // forward substitution R^T qty = b
-        DD acc = b[p];
-        for (int k = 0; k < p; ++k) acc = dd_sub(acc, dd_mul(R[k][p], qty[k]));
-        qty[p] = dd_div(acc, r);
-        diag[p] = fabs(dd_round(r));
-    }
-    const double first = dcount > 0 ? diag[0] : 0.0;
-    const double threshold = fmax(A.abs_tol, A.rel_tol * first);
-    int rank = 0;
-    while (rank < dcount && diag[rank] > threshold) ++rank;
-    DD coef[NB];
-    for (int i = 0; i < NB; ++i) coef[i] = dd_from(0.0);
-    for (int r = rank - 1; r >= 0; --r) {
-        DD acc = qty[r];
-        for (int k = r + 1; k < rank; ++k) acc = dd_sub(acc, dd_mul(R[r][k], coef[k]));
-        coef[r] = dd_div(acc, R[r][r]);
-    }
-    m.regression = 1;
-    m.active_columns = static_cast<uint32_t>(na);
-    m.diagonal_count = static_cast<uint32_t>(dcount);
-    m.rank = static_cast<uint32_t>(rank);
-    m.rank_threshold = threshold;
-    for (int k = 0; k < kLsmMaxBasis; ++k) {
-        m.pivot_order[k] = 0;
-        m.diagonal_abs[k] = 0.0;
-        m.coefficients[k] = 0.0;
-    }
-    for (int k = 0; k < na; ++k) m.pivot_order[k] = static_cast<uint32_t>(perm[k]);
-    for (int k = 0; k < dcount; ++k) m.diagonal_abs[k] = diag[k];
-    for (int k = 0; k < na; ++k) m.coefficients[perm[k]] = dd_round(coef[k]);
-    for (int k = 0; k < NB; ++k)
-        if (!isfinite(m.coefficients[k])) lsm_fail(A.lsm_error, static_cast<uint32_t>(d));
-}
-
-// Gram matrix and right-hand side of date `d` over its ITM rows; the last CTA
-// solves and publishes the date's decision model.
-template <int NB>
-__global__ void __launch_bounds__(kLsmThreads) lsm_gram_kernel(const LsmArgs A, int d) {
-    constexpr int K = NB * (NB + 1) / 2 + 2 * NB;
-    static_assert(K <= kLsmPartials && K <= kLsmThreads, "partials stride too small");
-    __shared__ DD s_red[kLsmWarps * K];
-    __shared__ DD s_fin[K];
-    const mcg_lsm_date_model m = A.models[d];
-    if (m.itm_rows == 0) return;  // ContinueAll { ZeroItmTrainingPaths }
-    const bool inactive = m.feature_inactive != 0;
-    const double df_d = A.df[d];
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     DD acc[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] = {0.0, 0.0};
-    for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.paths; p += stride) {
-        const double x = A.spots[static_cast<size_t>(d) * A.paths + p];
-        if (!(intrinsic(A.side, A.strike, A.notional, x) > A.itm_tol)) continue;
-        const double z = inactive ? 0.0 : (x - m.feature_mean) / m.feature_scale;
-        double bv[NB];
-        bv[0] = 1.0;
-#pragma unroll
-        for (int e = 1; e < NB; ++e) bv[e] = bv[e - 1] * z;
-        const double y = A.cf[p] / df_d;
-        int idx = 0;
-#pragma unroll
-        for (int i = 0; i < NB; ++i)
-#pragma unroll
-            for (int j = i; j < NB; ++j) {
-                acc[idx] = acc_prod(acc[idx], bv[i], bv[j]);
-                ++idx;
-            }
-#pragma unroll
-        for (int i = 0; i < NB; ++i) acc[idx + i] = acc_prod(acc[idx + i], bv[i], y);
-#pragma unroll
-        for (int i = 0; i < NB; ++i) acc[idx + NB + i] = acc_add(acc[idx + NB + i], bv[i] * bv[i]);
-    }
-    if (!cta_reduce_publish<K>(acc, A.partials, &A.tickets[2], s_red)) return;
-    merge_partials<K>(A.partials, s_fin);
+    for (int k = 0; k < K; ++k) acc[k] = {part[k], 0.0};
+    if (!cta_reduce_publish<K>(acc, A.partials, &A.tickets[0], s_red, &extra)) return;
+    merge_partials<K, true>(A.partials, s_fin);
+    const unsigned long long n = static_cast<unsigned long long>(s_fin[K].hi);
+    const double mx = s_fin[K].lo;
     if (threadIdx.x == 0) {
-        lsm_solve<NB>(A, d, s_fin);
-        A.tickets[2] = 0;
+        if (decide) A.models[update].residual_sum_squares = dd_round(s_fin[K - 1]);
+        A.tickets[0] = 0;
     }
+    if (gather >= 0) lsm_fit_date<NB>(A, gather, n, mx, s_fin, s_fin + NP);
 }
 
 // ------------------------------------------------------------------ valuation
@@ -725,26 +836,20 @@ cudaError_t launch_lsm_bs_spots(const DevicePlan& P, uint32_t domain, double* sp
     return cudaGetLastError();
 }
 
-cudaError_t launch_lsm_sweep(const LsmArgs& A, unsigned ctas, int init, int update, int gather,
-                             cudaStream_t stream) {
-    lsm_sweep_kernel<<<ctas, kLsmThreads, 0, stream>>>(A, init, update, gather);
+cudaError_t launch_lsm_init(const LsmArgs& A, unsigned ctas, cudaStream_t stream) {
+    lsm_init_kernel<<<ctas, kLsmThreads, 0, stream>>>(A);
     return cudaGetLastError();
 }
 
-cudaError_t launch_lsm_variance(const LsmArgs& A, unsigned ctas, int d, cudaStream_t stream) {
-    lsm_variance_kernel<<<ctas, kLsmThreads, 0, stream>>>(A, d);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_lsm_gram(const LsmArgs& A, unsigned ctas, int d, cudaStream_t stream) {
+cudaError_t launch_lsm_step(const LsmArgs& A, unsigned ctas, int update, int gather, cudaStream_t stream) {
     switch (A.nb) {
-    case 2: lsm_gram_kernel<2><<<ctas, kLsmThreads, 0, stream>>>(A, d); break;
-    case 3: lsm_gram_kernel<3><<<ctas, kLsmThreads, 0, stream>>>(A, d); break;
-    case 4: lsm_gram_kernel<4><<<ctas, kLsmThreads, 0, stream>>>(A, d); break;
-    case 5: lsm_gram_kernel<5><<<ctas, kLsmThreads, 0, stream>>>(A, d); break;
-    case 6: lsm_gram_kernel<6><<<ctas, kLsmThreads, 0, stream>>>(A, d); break;
-    case 7: lsm_gram_kernel<7><<<ctas, kLsmThreads, 0, stream>>>(A, d); break;
-    case 8: lsm_gram_kernel<8><<<ctas, kLsmThreads, 0, stream>>>(A, d); break;
+    case 2: lsm_step_kernel<2><<<ctas, kLsmThreads, 0, stream>>>(A, update, gather); break;
+    case 3: lsm_step_kernel<3><<<ctas, kLsmThreads, 0, stream>>>(A, update, gather); break;
+    case 4: lsm_step_kernel<4><<<ctas, kLsmThreads, 0, stream>>>(A, update, gather); break;
+    case 5: lsm_step_kernel<5><<<ctas, kLsmThreads, 0, stream>>>(A, update, gather); break;
+    case 6: lsm_step_kernel<6><<<ctas, kLsmThreads, 0, stream>>>(A, update, gather); break;
+    case 7: lsm_step_kernel<7><<<ctas, kLsmThreads, 0, stream>>>(A, update, gather); break;
+    case 8: lsm_step_kernel<8><<<ctas, kLsmThreads, 0, stream>>>(A, update, gather); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

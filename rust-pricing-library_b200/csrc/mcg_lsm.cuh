@@ -28,6 +28,7 @@ struct LsmArgs {
     double* cf;           // [paths] realised cash flow discounted to time zero
     uint32_t* stop;       // [paths] stopping date
     mcg_lsm_date_model* models;  // [dates - 1]
+    double* centers;      // [dates] centre of each date's power sums (a nearby ITM mean)
     DD* partials;         // [CTAs][kLsmPartials]
     unsigned int* tickets;  // [3] per pass kind, zero between launches
     unsigned long long* lsm_error;  // (date << 8) | code of the first failing date, atomicMin
@@ -46,10 +47,8 @@ struct LsmValueArgs {
 
 cudaError_t launch_lsm_bs_spots(const DevicePlan& P, uint32_t domain, double* spots, uint64_t paths,
                                 unsigned long long* bad, cudaStream_t stream);
-cudaError_t launch_lsm_sweep(const LsmArgs& A, unsigned ctas, int init, int update, int gather,
-                             cudaStream_t stream);
-cudaError_t launch_lsm_variance(const LsmArgs& A, unsigned ctas, int d, cudaStream_t stream);
-cudaError_t launch_lsm_gram(const LsmArgs& A, unsigned ctas, int d, cudaStream_t stream);
+cudaError_t launch_lsm_init(const LsmArgs& A, unsigned ctas, cudaStream_t stream);
+cudaError_t launch_lsm_step(const LsmArgs& A, unsigned ctas, int update, int gather, cudaStream_t stream);
 cudaError_t launch_lsm_bs_value(const DevicePlan& P, const LsmValueArgs& V, cudaStream_t stream);
 cudaError_t launch_lsm_group_sum(const double* values, uint64_t per_group, uint32_t groups, int pairs,
                                  const double* centers, DD* partials, unsigned ctas, DD* out, double* means,
