@@ -364,13 +364,26 @@ typedef struct mcg_lsm_desc {
     int32_t training_brownian_bridge;
     int32_t continuation;             /* mcg_continuation_kind */
     /* Learned continuation (MCG_CONTINUATION_MLP, no counterpart in the
-     * reference): a 2 -> 64 -> 64 -> 1 SiLU network of (standardised spot,
-     * time), BF16 weights and FP32 accumulation, trained on the training paths. */
-    uint32_t mlp_epochs;
-    uint32_t mlp_batch;
-    float mlp_learning_rate;
-    uint64_t mlp_seed;
+     * reference): one 2 -> 64 -> 64 -> 1 SiLU network of the scaled spot
+     * 4 (S - K) / K and the scaled time 2 t / T - 1, BF16 operands and FP32
+     * accumulation, fitted by Adam in the same backward induction as the
+     * regression: at each date, from the previous date's weights, on the ITM
+     * training rows and their discounted cash flows.  Its policy exercises
+     * an ITM path when the immediate value beats the predicted continuation.
+     * The polynomial policy is fitted too and is used instead (fallback) when
+     * the network's training diverges or its in-sample value is lower.
+     * Adam steps per date: max(epochs x batches, 400) at the last
+     * non-terminal date, max(epochs x batches, 50) at the others. */
+    uint32_t mlp_epochs;      /* passes over each date's rows; 0 = 1 */
+    uint32_t mlp_batch;       /* training rows per Adam step; 0 = 16384 */
+    float mlp_learning_rate;  /* Adam step size; 0 = 2e-3 */
+    uint64_t mlp_seed;        /* initial weights */
 } mcg_lsm_desc;
+
+/* Parameters of the continuation network, FP32, in this order:
+ * W1[64][2], b1[64], W2[64][64], b2[64], W3[64], b3. */
+#define MCG_MLP_HIDDEN 64u
+#define MCG_MLP_PARAMS (64u * 2u + 64u + 64u * 64u + 64u + 64u + 1u)
 
 /* One non-terminal exercise date's decision model: the reference's
  * ExerciseDecisionModel (lsm.rs:796-818) with the PolynomialRegressionModel
@@ -417,12 +430,29 @@ typedef struct mcg_lsm_result {
     float path_kernel_ms;           /* both path-matrix kernels */
     float regression_ms;            /* backward regression of the training phase */
     float valuation_ms;             /* policy valuation and statistics */
+    /* Learned continuation only. */
+    int32_t continuation_used;      /* the policy valued: mcg_continuation_kind */
+    uint32_t mlp_steps;             /* Adam steps taken */
+    float mlp_ms;                   /* device time of the network's training */
+    float mlp_final_loss;           /* mean squared error of the last step (scaled targets) */
+    double polynomial_in_sample;    /* in-sample value of the regression policy */
+    double mlp_in_sample;           /* in-sample value of the network policy */
+    uint32_t mlp_param_capacity;    /* entries in `mlp_params` (0 = not wanted) */
+    float* mlp_params;              /* trained parameters, caller-owned */
     mcg_error_record error;
 } mcg_lsm_result;
 
 /* Train and value an early-exercise policy on the GPU.  Synchronises `stream`. */
 mcg_status mcg_lsm_price(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, void* stream,
                          mcg_lsm_result* result);
+
+/* The continuation network on given rows, exposed for the gradient checks (no
+ * counterpart in the reference): outputs for `count` rows of inputs x[2 i],
+ * x[2 i + 1]; and the gradient of sum_i mask_i (f(x_i) - y_i)^2 with respect to
+ * the MCG_MLP_PARAMS parameters, with that sum in *loss.  Host arrays. */
+mcg_status mcg_mlp_forward(const float* params, const float* x, uint32_t count, float* out);
+mcg_status mcg_mlp_gradient(const float* params, const float* x, const float* y, const uint8_t* mask,
+                            uint32_t count, float* grad, float* loss);
 
 /* ---- Pricing without device allocation (no counterpart in the reference) ----
  *

@@ -30,6 +30,7 @@ UNITS = [
     ("mcg_host.cu", ["-fmad=false"]),
     ("mcg_noalloc.cu", ["-fmad=false"]),
     ("mcg_lsm.cu", ["-fmad=false"]),
+    ("mcg_mlp.cu", []),
 ]
 
 

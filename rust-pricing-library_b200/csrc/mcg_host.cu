@@ -23,6 +23,7 @@
 
 #include "mcg_kernels.cuh"
 #include "mcg_lsm.cuh"
+#include "mcg_mlp.cuh"
 
 namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -1038,7 +1039,10 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
 
 // Device buffers of one mcg_lsm_price call, released on every return path.
 struct LsmBuffers {
-    DeviceArray<double> spots, cf, df, unit_values, means, centers;
+    DeviceArray<double> spots, cf, df, unit_values, means, centers, cf_mlp, centers_mlp;
+    DeviceArray<float> mlp_params, mlp_moments, mlp_partials, mlp_loss, mlp_snapshots;
+    DeviceArray<uint32_t> stop_mlp;
+    cudaEvent_t mlp_ev[2] = {nullptr, nullptr};
     DeviceArray<uint32_t> stop, vstops;
     DeviceArray<mcg_lsm_date_model> models;
     DeviceArray<DD> partials, group_partials, sums;
@@ -1052,6 +1056,16 @@ struct LsmBuffers {
         unit_values.release();
         means.release();
         centers.release();
+        cf_mlp.release();
+        centers_mlp.release();
+        mlp_params.release();
+        mlp_moments.release();
+        mlp_partials.release();
+        mlp_loss.release();
+        mlp_snapshots.release();
+        stop_mlp.release();
+        for (cudaEvent_t& e : mlp_ev)
+            if (e) cudaEventDestroy(e);
         stop.release();
         vstops.release();
         models.release();
@@ -1075,8 +1089,11 @@ mcg_status validate_lsm(const mcg_plan_desc* d, const mcg_lsm_desc* l, const mcg
         return fail(MCG_ERR_UNSUPPORTED, "fixed-policy early-exercise risk is not implemented");
     if (d->model != MCG_MODEL_BLACK_SCHOLES)
         return fail(MCG_ERR_UNSUPPORTED, "early exercise under local volatility is not implemented");
-    if (l->continuation != MCG_CONTINUATION_POLYNOMIAL)
+    if (l->continuation != MCG_CONTINUATION_POLYNOMIAL && l->continuation != MCG_CONTINUATION_MLP)
         return fail(MCG_ERR_UNSUPPORTED, "continuation kind");
+    if (l->continuation == MCG_CONTINUATION_MLP &&
+        (!std::isfinite(l->mlp_learning_rate) || l->mlp_learning_rate < 0.0f || l->mlp_epochs > 1000u))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "mlp_learning_rate / mlp_epochs");
     if (l->max_degree < 1 || l->max_degree > MCG_LSM_MAX_DEGREE)
         return fail(MCG_ERR_INVALID_ARGUMENT, "max_degree must be 1..7");
     // validate_tolerance, lsm.rs:2295-2302
@@ -1154,7 +1171,7 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     if (want_stops) MCG_CUDA(B.vstops.alloc(v_paths));
     const uint32_t max_groups = std::max(t_groups, v_groups);
     MCG_CUDA(B.group_partials.alloc(static_cast<size_t>(max_groups) * group_ctas));
-    MCG_CUDA(B.sums.alloc(3 * static_cast<size_t>(max_groups)));  // in-sample, valuation, squares
+    MCG_CUDA(B.sums.alloc(4 * static_cast<size_t>(max_groups)));  // in-sample, valuation, squares, network in-sample
     MCG_CUDA(B.means.alloc(static_cast<size_t>(max_groups)));
     MCG_CUDA(cudaMemsetAsync(B.tickets.ptr, 0, 3 * sizeof(unsigned int), stream));
     MCG_CUDA(cudaMemsetAsync(B.words.ptr, 0xff, 2 * sizeof(unsigned long long), stream));
@@ -1208,6 +1225,133 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     launches += 2;
     MCG_CUDA(cudaEventRecord(B.ev[2], stream));
 
+    // In-sample value from the group sums: mean of the collapsed training values
+    // (pseudo) or of the per-scramble replicates (RQMC), risk/early_exercise.rs:100-110,300-313.
+    auto in_sample_of = [&](const std::vector<DD>& sums, size_t base) {
+        if (rqmc) {
+            double s = 0.0, c = 0.0;
+            for (uint32_t g = 0; g < t_groups; ++g)
+                neumaier(s, c, (sums[base + g].hi + sums[base + g].lo) / static_cast<double>(TP.units));
+            return (s + c) / static_cast<double>(t_groups);
+        }
+        return (sums[base].hi + sums[base].lo) / static_cast<double>(TP.units);
+    };
+
+    // Learned continuation: the network's own backward induction on the same
+    // training paths, then the choice between the two policies.
+    bool use_mlp = false;
+    r->continuation_used = MCG_CONTINUATION_POLYNOMIAL;
+    r->mlp_steps = 0;
+    r->mlp_ms = 0.f;
+    r->mlp_final_loss = 0.f;
+    r->polynomial_in_sample = 0.0;
+    r->mlp_in_sample = 0.0;
+    if (l->continuation == MCG_CONTINUATION_MLP && dates > 1) {
+        const uint64_t batch = l->mlp_batch ? l->mlp_batch : 16384u;
+        const uint32_t epochs = l->mlp_epochs ? l->mlp_epochs : 1u;
+        const float lr = l->mlp_learning_rate > 0.0f ? l->mlp_learning_rate : 2e-3f;
+        // Glorot-uniform initial weights from a splitmix64 stream, zero biases.
+        std::vector<float> params(kMlpParams, 0.0f);
+        uint64_t state = l->mlp_seed;
+        auto uniform = [&]() {
+            uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            z ^= z >> 31;
+            return static_cast<double>(z >> 11) * 0x1.0p-53 * 2.0 - 1.0;
+        };
+        const double a1 = std::sqrt(6.0 / (2 + kMlpHidden)), a2 = std::sqrt(6.0 / (2 * kMlpHidden)),
+                     a3 = std::sqrt(6.0 / (kMlpHidden + 1));
+        for (int i = 0; i < 2 * kMlpHidden; ++i) params[kMlpW1 + i] = static_cast<float>(a1 * uniform());
+        for (int i = 0; i < kMlpHidden * kMlpHidden; ++i) params[kMlpW2 + i] = static_cast<float>(a2 * uniform());
+        for (int i = 0; i < kMlpHidden; ++i) params[kMlpW3 + i] = static_cast<float>(a3 * uniform());
+        MCG_CUDA(B.mlp_params.upload(params));
+        MCG_CUDA(B.mlp_moments.alloc(2 * static_cast<size_t>(kMlpParams)));
+        MCG_CUDA(cudaMemsetAsync(B.mlp_moments.ptr, 0, 2 * kMlpParams * sizeof(float), stream));
+        MCG_CUDA(B.mlp_partials.alloc(static_cast<size_t>(std::max(sms, 1)) * kMlpPartial));
+        MCG_CUDA(B.mlp_loss.alloc(1));
+        // the weights each date was decided with, for the valuation
+        MCG_CUDA(B.mlp_snapshots.alloc(static_cast<size_t>(dates - 1) * kMlpParams));
+        MCG_CUDA(B.cf_mlp.alloc(t_paths));
+        MCG_CUDA(B.stop_mlp.alloc(t_paths));
+        MCG_CUDA(B.centers_mlp.upload(std::vector<double>(dates, d->products[0].strike)));
+        for (cudaEvent_t& e : B.mlp_ev) MCG_CUDA(cudaEventCreate(&e));
+        LsmArgs AM = A;
+        AM.cf = B.cf_mlp.ptr;
+        AM.stop = B.stop_mlp.ptr;
+        AM.centers = B.centers_mlp.ptr;
+        MCG_CUDA(cudaEventRecord(B.mlp_ev[0], stream));
+        MCG_CUDA(launch_lsm_init(AM, ctas, stream));
+        ++launches;
+        const double horizon = d->observation_times[last];
+        const uint64_t nbatch = (t_paths + batch - 1) / batch;
+        uint32_t step = 0;
+        for (int date = last - 1; date >= 0; --date) {
+            const double tin = 2.0 * d->observation_times[date] / horizon - 1.0;
+            const uint64_t floor_steps = date == last - 1 ? 400u : 50u;
+            const uint64_t steps = std::max<uint64_t>(static_cast<uint64_t>(epochs) * nbatch, floor_steps);
+            for (uint64_t k = 0; k < steps; ++k) {
+                const uint64_t b = k % nbatch;
+                MlpRows rows{};
+                rows.spots = B.spots.ptr + static_cast<size_t>(date) * t_paths;
+                rows.cf = B.cf_mlp.ptr;
+                rows.first = b * batch;
+                rows.count = std::min<uint64_t>(batch, t_paths - rows.first);
+                rows.df = df[date];
+                rows.time_input = tin;
+                rows.side = A.side;
+                rows.strike = A.strike;
+                rows.notional = A.notional;
+                rows.itm_tol = A.itm_tol;
+                const unsigned mctas = mlp_gradient_ctas(rows.count);
+                MCG_CUDA(launch_mlp_gradient(B.mlp_params.ptr, rows, B.mlp_partials.ptr, mctas, stream));
+                MCG_CUDA(launch_mlp_adam(B.mlp_partials.ptr, mctas, B.mlp_params.ptr, B.mlp_moments.ptr, ++step,
+                                         lr, B.mlp_loss.ptr, stream));
+                launches += 2;
+            }
+            MCG_CUDA(cudaMemcpyAsync(B.mlp_snapshots.ptr + static_cast<size_t>(date) * kMlpParams, B.mlp_params.ptr,
+                                     kMlpParams * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+            MlpDecision dec{};
+            dec.spots = B.spots.ptr + static_cast<size_t>(date) * t_paths;
+            dec.cf = B.cf_mlp.ptr;
+            dec.stop = B.stop_mlp.ptr;
+            dec.paths = t_paths;
+            dec.date = static_cast<uint32_t>(date);
+            dec.df = df[date];
+            dec.time_input = tin;
+            dec.side = A.side;
+            dec.strike = A.strike;
+            dec.notional = A.notional;
+            dec.itm_tol = A.itm_tol;
+            MCG_CUDA(launch_mlp_decide(B.mlp_params.ptr, dec, stream));
+            ++launches;
+        }
+        MCG_CUDA(cudaEventRecord(B.mlp_ev[1], stream));
+        DD* s_in_mlp = B.sums.ptr + 3 * max_groups;
+        MCG_CUDA(launch_lsm_group_sum(B.cf_mlp.ptr, TP.units, t_groups, TP.antithetic, nullptr,
+                                      B.group_partials.ptr, group_ctas, s_in_mlp, nullptr, stream));
+        launches += 2;
+        std::vector<DD> early(4 * static_cast<size_t>(max_groups));
+        float loss = 0.f;
+        MCG_CUDA(cudaMemcpyAsync(early.data(), B.sums.ptr, early.size() * sizeof(DD), cudaMemcpyDeviceToHost,
+                                 stream));
+        MCG_CUDA(cudaMemcpyAsync(params.data(), B.mlp_params.ptr, kMlpParams * sizeof(float),
+                                 cudaMemcpyDeviceToHost, stream));
+        MCG_CUDA(cudaMemcpyAsync(&loss, B.mlp_loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, stream));
+        MCG_CUDA(cudaStreamSynchronize(stream));
+        bool finite = std::isfinite(loss);
+        for (float v : params) finite &= std::isfinite(v);
+        r->polynomial_in_sample = in_sample_of(early, 0);
+        r->mlp_in_sample = in_sample_of(early, 3 * static_cast<size_t>(max_groups));
+        r->mlp_steps = step;
+        r->mlp_final_loss = loss;
+        cudaEventElapsedTime(&r->mlp_ms, B.mlp_ev[0], B.mlp_ev[1]);
+        use_mlp = finite && r->mlp_in_sample >= r->polynomial_in_sample;
+        if (use_mlp) r->continuation_used = MCG_CONTINUATION_MLP;
+        if (r->mlp_params && r->mlp_param_capacity >= static_cast<uint32_t>(kMlpParams))
+            std::memcpy(r->mlp_params, params.data(), kMlpParams * sizeof(float));
+    }
+
     // Valuation: fresh paths under the fitted policy.
     LsmValueArgs V{};
     V.df = B.df.ptr;
@@ -1220,7 +1364,11 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     V.unit_values = B.unit_values.ptr;
     V.stops = want_stops ? B.vstops.ptr : nullptr;
     V.counts = B.counts.ptr;
-    MCG_CUDA(launch_lsm_bs_value(VP, V, stream));
+    if (use_mlp) {
+        MCG_CUDA(launch_lsm_bs_value_mlp(VP, V, B.mlp_snapshots.ptr, 1.0 / d->observation_times[last], stream));
+    } else {
+        MCG_CUDA(launch_lsm_bs_value(VP, V, stream));
+    }
     ++launches;
     MCG_CUDA(launch_lsm_group_sum(B.unit_values.ptr, VP.units, v_groups, 0, nullptr, B.group_partials.ptr,
                                   group_ctas, s_val, B.means.ptr, stream));
@@ -1232,7 +1380,7 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     }
     MCG_CUDA(cudaEventRecord(B.ev[3], stream));
 
-    std::vector<DD> sums(3 * static_cast<size_t>(max_groups));
+    std::vector<DD> sums(4 * static_cast<size_t>(max_groups));
     unsigned long long words[2];
     std::vector<unsigned long long> counts(dates);
     MCG_CUDA(cudaMemcpyAsync(sums.data(), B.sums.ptr, sums.size() * sizeof(DD), cudaMemcpyDeviceToHost, stream));
@@ -1269,16 +1417,7 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     r->device_ms = ms[0] + ms[1] + ms[2];
     for (uint32_t i = 0; i < dates; ++i) r->exercise_counts[i] = counts[i];
 
-    // In-sample value: mean of the collapsed training values (pseudo) or of
-    // the per-scramble replicates (RQMC), risk/early_exercise.rs:100-110,300-313.
-    if (rqmc) {
-        double s = 0.0, c = 0.0;
-        for (uint32_t g = 0; g < t_groups; ++g)
-            neumaier(s, c, (sums[g].hi + sums[g].lo) / static_cast<double>(TP.units));
-        r->in_sample_value = (s + c) / static_cast<double>(t_groups);
-    } else {
-        r->in_sample_value = (sums[0].hi + sums[0].lo) / static_cast<double>(TP.units);
-    }
+    r->in_sample_value = in_sample_of(sums, use_mlp ? 3 * static_cast<size_t>(max_groups) : 0);
     HostStat hs;
     uint64_t independent;
     if (rqmc) {
@@ -1347,6 +1486,57 @@ void mcg_plan_destroy(mcg_plan* plan) { delete plan; }
 mcg_status mcg_lsm_price(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, void* stream,
                          mcg_lsm_result* result) {
     return lsm_price(plan, lsm, static_cast<cudaStream_t>(stream), result);
+}
+
+mcg_status mcg_mlp_forward(const float* params, const float* x, uint32_t count, float* out) {
+    if (!params || !x || !out || count == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "mcg_mlp_forward arguments");
+    DeviceArray<float> p, dx, dout;
+    cudaError_t e = p.upload(std::vector<float>(params, params + kMlpParams));
+    if (e == cudaSuccess) e = dx.upload(std::vector<float>(x, x + 2 * static_cast<size_t>(count)));
+    if (e == cudaSuccess) e = dout.alloc(count);
+    if (e == cudaSuccess) e = launch_mlp_forward(p.ptr, dx.ptr, count, dout.ptr, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout.ptr, count * sizeof(float), cudaMemcpyDeviceToHost);
+    p.release();
+    dx.release();
+    dout.release();
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("mcg_mlp_forward: ") + cudaGetErrorString(e));
+    return MCG_OK;
+}
+
+mcg_status mcg_mlp_gradient(const float* params, const float* x, const float* y, const uint8_t* mask,
+                            uint32_t count, float* grad, float* loss) {
+    if (!params || !x || !y || !mask || !grad || !loss || count == 0)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "mcg_mlp_gradient arguments");
+    DeviceArray<float> p, dx, dy, partials, sums;
+    DeviceArray<uint8_t> dm;
+    const unsigned ctas = mlp_gradient_ctas(count);
+    cudaError_t e = p.upload(std::vector<float>(params, params + kMlpParams));
+    if (e == cudaSuccess) e = dx.upload(std::vector<float>(x, x + 2 * static_cast<size_t>(count)));
+    if (e == cudaSuccess) e = dy.upload(std::vector<float>(y, y + count));
+    if (e == cudaSuccess) e = dm.upload(std::vector<uint8_t>(mask, mask + count));
+    if (e == cudaSuccess) e = partials.alloc(static_cast<size_t>(ctas) * kMlpPartial);
+    if (e == cudaSuccess) e = sums.alloc(kMlpPartial);
+    if (e == cudaSuccess) {
+        MlpRows rows{};
+        rows.count = count;
+        rows.x = dx.ptr;
+        rows.y = dy.ptr;
+        rows.mask = dm.ptr;
+        e = launch_mlp_gradient(p.ptr, rows, partials.ptr, ctas, nullptr);
+    }
+    if (e == cudaSuccess) e = launch_mlp_sum(partials.ptr, ctas, sums.ptr, nullptr);
+    std::vector<float> host(kMlpPartial);
+    if (e == cudaSuccess) e = cudaMemcpy(host.data(), sums.ptr, kMlpPartial * sizeof(float), cudaMemcpyDeviceToHost);
+    p.release();
+    dx.release();
+    dy.release();
+    partials.release();
+    sums.release();
+    dm.release();
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("mcg_mlp_gradient: ") + cudaGetErrorString(e));
+    std::memcpy(grad, host.data(), kMlpParams * sizeof(float));
+    *loss = host[kMlpParams];
+    return MCG_OK;
 }
 
 mcg_status mcg_price(const mcg_plan_desc* desc, void* stream, mcg_result* result) {

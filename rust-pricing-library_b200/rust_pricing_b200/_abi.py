@@ -147,6 +147,8 @@ LSM_MAX_DEGREE = 7
 LSM_MAX_BASIS = LSM_MAX_DEGREE + 1
 CONTINUATION_POLYNOMIAL, CONTINUATION_MLP = 0, 1
 DOMAIN_VALUATION, DOMAIN_LSM_TRAIN = 0, 1
+MLP_HIDDEN = 64
+MLP_PARAMS = 64 * 2 + 64 + 64 * 64 + 64 + 64 + 1
 
 
 class LsmDesc(C.Structure):
@@ -188,6 +190,9 @@ class LsmResult(C.Structure):
         ("date_count", C.c_uint32), ("kernel_launches", C.c_uint32),
         ("device_ms", C.c_float), ("path_kernel_ms", C.c_float),
         ("regression_ms", C.c_float), ("valuation_ms", C.c_float),
+        ("continuation_used", C.c_int32), ("mlp_steps", C.c_uint32), ("mlp_ms", C.c_float),
+        ("mlp_final_loss", C.c_float), ("polynomial_in_sample", C.c_double), ("mlp_in_sample", C.c_double),
+        ("mlp_param_capacity", C.c_uint32), ("mlp_params", C.POINTER(C.c_float)),
         ("error", ErrorRecord),
     ]
 
@@ -200,7 +205,10 @@ class LsmBuffers:
         self.models = (LsmDateModel * max(dates, 1))()
         self.counts = (C.c_uint64 * max(dates, 1))()
         self.stops = (C.c_uint32 * stopping)() if stopping else None
+        self.mlp_params = (C.c_float * MLP_PARAMS)()
         self.result = LsmResult()
+        self.result.mlp_param_capacity = MLP_PARAMS
+        self.result.mlp_params = C.cast(self.mlp_params, C.POINTER(C.c_float))
         self.result.date_capacity = dates
         self.result.models = C.cast(self.models, C.POINTER(LsmDateModel))
         self.result.exercise_counts = C.cast(self.counts, C.POINTER(C.c_uint64))

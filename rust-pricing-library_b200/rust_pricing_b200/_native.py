@@ -18,7 +18,7 @@ EXPORTS = (
     "mcg_abi_version", "mcg_last_error", "mcg_plan_create", "mcg_plan_evaluate", "mcg_price",
     "mcg_plan_destroy", "mcg_plan_shape", "mcg_philox_normals", "mcg_rqmc_words",
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
-    "mcg_lsm_price",
+    "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient",
 )
 
 _lib = None
@@ -71,6 +71,11 @@ def library() -> C.CDLL:
     lib.mcg_measure_fp64_peak.restype = C.c_int
     lib.mcg_lsm_price.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.LsmDesc), vp, C.POINTER(A.LsmResult)]
     lib.mcg_lsm_price.restype = C.c_int
+    fp = C.POINTER(C.c_float)
+    lib.mcg_mlp_forward.argtypes = [fp, fp, u32, fp]
+    lib.mcg_mlp_forward.restype = C.c_int
+    lib.mcg_mlp_gradient.argtypes = [fp, fp, fp, C.POINTER(C.c_uint8), u32, fp, fp]
+    lib.mcg_mlp_gradient.restype = C.c_int
     if lib.mcg_abi_version() != A.ABI_VERSION:
         raise EngineError(1, "engine library ABI version mismatch")
     _lib = lib
@@ -91,6 +96,33 @@ def lsm_price(spec, lsm, stopping: bool = False, stream: int = 0) -> A.LsmBuffer
     status = library().mcg_lsm_price(C.byref(desc), C.byref(ldesc), C.c_void_p(stream), C.byref(buf.result))
     check(status, buf.result.error)
     return buf
+
+
+def mlp_forward(params, x):
+    """mcg_mlp_forward on host arrays: params (MLP_PARAMS,), x (n, 2) -> (n,)."""
+    import numpy as np
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xs = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.zeros(len(xs), dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    check(library().mcg_mlp_forward(p.ctypes.data_as(fp), xs.ctypes.data_as(fp), len(xs), out.ctypes.data_as(fp)))
+    return out
+
+
+def mlp_gradient(params, x, y, mask):
+    """mcg_mlp_gradient: gradient of sum mask (f(x) - y)^2 and that sum."""
+    import numpy as np
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xs = np.ascontiguousarray(x, dtype=np.float32)
+    ys = np.ascontiguousarray(y, dtype=np.float32)
+    ms = np.ascontiguousarray(mask, dtype=np.uint8)
+    grad = np.zeros(A.MLP_PARAMS, dtype=np.float32)
+    loss = C.c_float()
+    fp = C.POINTER(C.c_float)
+    check(library().mcg_mlp_gradient(p.ctypes.data_as(fp), xs.ctypes.data_as(fp), ys.ctypes.data_as(fp),
+                                      ms.ctypes.data_as(C.POINTER(C.c_uint8)), len(xs), grad.ctypes.data_as(fp),
+                                      C.byref(loss)))
+    return grad, loss.value
 
 
 class Plan:
