@@ -156,14 +156,62 @@ def cpu_baseline(points: int, scrambles: int, threads: int, grid_builder=None):
     return path_steps / dt, dt, path_steps
 
 
+def time_to_bp(ms: float, se: float, price: float) -> float:
+    """Device time to a 1 bp standard error (SE <= 1e-4 |price|), scaling the
+    measured time by the variance ratio."""
+    target = 1e-4 * abs(price)
+    return ms * (se / target) ** 2 if target > 0 else float("inf")
+
+
+def lsm_secondary():
+    """The early-exercise configuration (American put S=K=100, r=5%, sigma=25%,
+    T=1, 50 dates, 2^20 training + 2^20 valuation paths): the reference's
+    polynomial policy and the learned continuation, against the 5000-step
+    Bermudan binomial tree.  One untimed warm-up, then one timed evaluation each."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from bermudan_tree import bermudan_equally_spaced
+    from rust_pricing_b200 import _abi as A, _native as N, workloads as W
+    tree = bermudan_equally_spaced(100.0, 100.0, 0.05, 0.0, 0.25, 1.0, 50, steps=5000)
+    out = {"workload": "American put by LSM, 50 dates, 2^20 + 2^20 paths, cubic basis; judge: 5000-step "
+                       "Bermudan binomial tree", "tree": tree}
+    for name, kind in (("plain", A.CONTINUATION_POLYNOMIAL), ("learned", A.CONTINUATION_MLP)):
+        spec, lsm = W.american_bs(dates=50, units=1 << 20)
+        lsm.continuation = kind
+        lsm.mlp_seed = 7
+        N.lsm_price(spec, lsm)
+        r = N.lsm_price(spec, lsm).result
+        # fitting is a fixed cost; only the valuation scales with the paths
+        fixed = r.path_kernel_ms + r.regression_ms + r.mlp_ms
+        out[name] = {"device_ms": r.device_ms, "fit_ms": fixed, "valuation_ms": r.device_ms - fixed,
+                     "price": r.price.value, "standard_error": r.price.standard_error,
+                     "error_vs_tree": r.price.value - tree, "policy": "mlp" if r.continuation_used else "polynomial",
+                     "path_steps_per_s": 2 * (1 << 20) * 50 / (r.device_ms * 1e-3),
+                     "ms_to_1bp_standard_error": fixed + time_to_bp(r.device_ms - fixed, r.price.standard_error,
+                                                                    r.price.value),
+                     "kernel_launches": r.kernel_launches}
+    return out
+
+
+def sized_cpu_sample(threads: int, grid_builder=None, target_s: float = 15.0):
+    """Points per scramble (a power of two, 2 scrambles) for about `target_s`
+    seconds of oracle work on this host, from a short calibration run."""
+    rate, _, _ = cpu_baseline(1 << 11, 1, threads, grid_builder)
+    points, scrambles = 1 << 11, 2
+    while points < (1 << 20) and 2 * scrambles * points * STEPS / rate <= target_s:
+        points *= 2
+    while scrambles < 16 and 2 * scrambles * points * STEPS / rate <= target_s:
+        scrambles *= 2
+    return points, scrambles
+
+
 def run_reference(args, rank, world):
     """CPU executor (oracle port) on all host cores; rank 0 only."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    sample_points, sample_scrambles = 1 << 15, 2
     for _ in range(args.warmup and 1):
         cpu_baseline(1 << 10, 1, threads)
+    sample_points, sample_scrambles = sized_cpu_sample(threads)
     times = []
     for _ in range(args.steps):
         value, dt, ps = cpu_baseline(sample_points, sample_scrambles, threads)
@@ -280,10 +328,14 @@ def main():
         "clocks": clocks.summary(),
         "prices": [buf.products[k].price.value for k in range(len(spec.products))],
         "price_standard_errors": [buf.products[k].price.standard_error for k in range(len(spec.products))],
+        "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, buf.products[k].price.standard_error,
+                                                buf.products[k].price.value) for k in range(len(spec.products))],
     }
+    if rank == 0 and world == 1:
+        line["secondary"] = {"early_exercise": lsm_secondary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sample_points, sample_scrambles = 1 << 15, 2
+        sample_points, sample_scrambles = sized_cpu_sample(threads, grid_builder=gpu_grid)
         value_cpu, dt, ps = cpu_baseline(sample_points, sample_scrambles, threads, grid_builder=gpu_grid)
         line["cpu_baseline"] = {"value": value_cpu, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{sample_points} points x {sample_scrambles} scrambles x {STEPS} steps "
