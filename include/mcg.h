@@ -454,6 +454,48 @@ mcg_status mcg_mlp_forward(const float* params, const float* x, uint32_t count, 
 mcg_status mcg_mlp_gradient(const float* params, const float* x, const float* y, const uint8_t* mask,
                             uint32_t count, float* grad, float* loss);
 
+/* ---- A book of trades in one launch (no counterpart in the reference) ----
+ *
+ * Thousands of single-product plans -- each with its own model (Black-Scholes
+ * or local volatility with its own grid), maturity and step count, strike and
+ * product -- priced by one persistent kernel that pulls (trade, tile-range)
+ * work items from a queue ordered heaviest first, followed by the per-trade
+ * tile reduction.  Each trade's price statistics are bit for bit those of
+ * mcg_plan_evaluate on its own plan.  Trades must be pseudo-MC with the same
+ * sampling_units, one product, no risk request, and (local volatility) no
+ * antithetic pairing.  The launch shape (tiles per work item, resident CTAs
+ * per SM) is chosen at creation by timing candidate shapes on a stratified
+ * sample of the book (`autotune`), and the evaluation can be captured once in
+ * a CUDA graph (`use_graph`) and replayed. */
+typedef struct mcg_book mcg_book;
+
+typedef struct mcg_book_options {
+    int32_t autotune;        /* 1: time candidate launch shapes at creation and keep the fastest */
+    uint32_t tiles_per_item; /* 128-unit tiles per work item when not autotuned; 0 = 4 */
+    uint32_t ctas_per_sm;    /* resident CTAs per SM when not autotuned; 0 = as many as fit */
+    int32_t use_graph;       /* 1: capture the evaluation in a CUDA graph at creation */
+} mcg_book_options;
+
+typedef struct mcg_book_report {
+    uint32_t trade_count;
+    uint32_t items;            /* work items of one evaluation */
+    uint32_t tiles_per_item;   /* the launch shape in use */
+    uint32_t ctas_per_sm;
+    uint32_t ctas;
+    uint32_t kernel_launches;  /* per evaluation */
+    int32_t graph;             /* 1: evaluated by replaying the captured graph */
+    float device_ms;           /* one evaluation, CUDA events */
+    float autotune_ms;         /* host wall time the autotuner spent at creation */
+    uint64_t path_steps;       /* simulated path-steps of one evaluation */
+    mcg_error_record error;    /* first failing trade: code, its index in `step`, unit, value */
+} mcg_book_report;
+
+mcg_status mcg_book_create(const mcg_plan_desc* trades, uint32_t trade_count, const mcg_book_options* options,
+                           mcg_book** out_book);
+/* `prices` receives one estimate per trade; `report` may be NULL. */
+mcg_status mcg_book_evaluate(mcg_book* book, void* stream, mcg_estimate* prices, mcg_book_report* report);
+void mcg_book_destroy(mcg_book* book);
+
 /* ---- Pricing without device allocation (no counterpart in the reference) ----
  *
  * For callers that must not allocate GPU memory while pricing (a service that

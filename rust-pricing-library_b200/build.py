@@ -31,6 +31,7 @@ UNITS = [
     ("mcg_noalloc.cu", ["-fmad=false"]),
     ("mcg_lsm.cu", ["-fmad=false"]),
     ("mcg_mlp.cu", []),
+    ("mcg_book.cu", ["-fmad=false"]),
 ]
 
 

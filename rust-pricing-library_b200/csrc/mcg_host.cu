@@ -14,7 +14,9 @@
 // the per-scramble records and builds the estimates of
 // crates/pricing/src/engine/risk/report.rs:454-473.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <memory>
 #include <cstdio>
 #include <cstring>
 #include <queue>
@@ -24,6 +26,7 @@
 #include "mcg_kernels.cuh"
 #include "mcg_lsm.cuh"
 #include "mcg_mlp.cuh"
+#include "mcg_book.cuh"
 
 namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -468,7 +471,7 @@ double resolve_gamma_bump(const mcg_plan_desc* d) {
     return d->gamma_bump_relative ? d->spot * d->gamma_bump : d->gamma_bump;
 }
 
-mcg_status build(const mcg_plan_desc* d, mcg_plan& plan) {
+mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers = true) {
     if (!d) return fail(MCG_ERR_INVALID_ARGUMENT, "null descriptor");
     if (d->abi_version != MCG_ABI_VERSION) return fail(MCG_ERR_INVALID_ARGUMENT, "abi_version mismatch");
     if (d->model != MCG_MODEL_BLACK_SCHOLES && d->model != MCG_MODEL_LOCAL_VOLATILITY)
@@ -737,8 +740,9 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan) {
         P.scr_shift = plan.scr_shift.ptr;
     }
     (void)steps;
-    // Reduction buffers.
+    // Reduction buffers (a book trade shares the book's).
     plan.tiles = static_cast<uint32_t>((P.units + kThreads - 1) / kThreads);
+    if (!reduction_buffers) return MCG_OK;
     MCG_CUDA(plan.partials.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * plan.product_count * kComponents));
     MCG_CUDA(plan.records.alloc(static_cast<size_t>(P.scramble_count) * plan.product_count * kComponents));
     MCG_CUDA(plan.error.alloc(1));
@@ -1447,6 +1451,290 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     return MCG_OK;
 }
 
+// --------------------------------------------------------------- book of trades
+
+}  // namespace
+
+struct mcg_book {
+    std::vector<mcg_plan*> plans;
+    std::vector<BookItem> host_items;
+    std::vector<uint64_t> item_cost;
+    std::vector<uint32_t> trade_path, trade_steps;
+    DeviceArray<DevicePlan> dplans;
+    DeviceArray<uint32_t> masks;
+    DeviceArray<BookItem> items;
+    DeviceArray<unsigned int> cursor;
+    DeviceArray<StatRecord> partials, records;
+    DeviceArray<ErrorWord> errors;
+    uint32_t trades = 0, tiles = 0, max_values = 0, max_nodes = 0, max_slots = 1;
+    uint32_t tiles_per_item = 4, ctas_per_sm = 1, ctas = 1;
+    uint64_t units = 0, path_steps = 0;
+    size_t smem = 0;
+    int sms = 148;
+    float autotune_ms = 0.f;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    ~mcg_book() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        for (mcg_plan* p : plans) delete p;
+        dplans.release();
+        masks.release();
+        items.release();
+        cursor.release();
+        partials.release();
+        records.release();
+        errors.release();
+    }
+};
+
+namespace {
+
+// Work items of `tiles_per_item` tiles, ordered heaviest first (cost = tiles x
+// steps, local volatility weighted 3x for its interpolation and logarithm);
+// ties keep trade order, so the queue is deterministic.
+void book_items(mcg_book& b, uint32_t tiles_per_item, const std::vector<uint32_t>& trades) {
+    b.host_items.clear();
+    std::vector<std::pair<uint64_t, size_t>> order;
+    for (uint32_t t : trades)
+        for (uint32_t first = 0; first < b.tiles; first += tiles_per_item) {
+            const uint32_t n = std::min(tiles_per_item, b.tiles - first);
+            BookItem it{t, first, n, b.trade_path[t]};
+            const uint64_t cost = static_cast<uint64_t>(n) * b.trade_steps[t] * (it.path == kBookLocalVol ? 3 : 1);
+            order.emplace_back(cost, b.host_items.size());
+            b.host_items.push_back(it);
+        }
+    std::stable_sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<BookItem> sorted;
+    sorted.reserve(order.size());
+    for (auto& o : order) sorted.push_back(b.host_items[o.second]);
+    b.host_items.swap(sorted);
+}
+
+BookLaunch book_launch(mcg_book& b) {
+    BookLaunch L{};
+    L.plans = b.dplans.ptr;
+    L.masks = b.masks.ptr;
+    L.items = b.items.ptr;
+    L.item_count = static_cast<uint32_t>(b.host_items.size());
+    L.next = b.cursor.ptr;
+    L.partials = b.partials.ptr;
+    L.tiles_per_trade = b.tiles;
+    L.errors = b.errors.ptr;
+    L.max_values = b.max_values;
+    L.max_nodes = b.max_nodes;
+    L.max_slots = b.max_slots;
+    return L;
+}
+
+// The evaluation's launches: queue reset, error words, persistent kernel, reduction.
+cudaError_t book_enqueue(mcg_book& b, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(b.cursor.ptr, 0, sizeof(unsigned int), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.errors.ptr, 0xff, b.trades * sizeof(ErrorWord), stream);
+    if (e == cudaSuccess) e = launch_book(book_launch(b), b.ctas, b.smem, stream);
+    if (e == cudaSuccess) {
+        reduce_tiles_kernel<<<dim3(kComponents, b.trades), 256, 0, stream>>>(b.partials.ptr, b.tiles, kComponents,
+                                                                          b.records.ptr);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+mcg_status book_set_shape(mcg_book& b, uint32_t tiles_per_item, uint32_t ctas_per_sm,
+                          const std::vector<uint32_t>& trades) {
+    b.tiles_per_item = tiles_per_item;
+    b.ctas_per_sm = ctas_per_sm;
+    b.ctas = static_cast<uint32_t>(b.sms) * ctas_per_sm;
+    book_items(b, tiles_per_item, trades);
+    b.items.release();
+    MCG_CUDA(b.items.upload(b.host_items));
+    return MCG_OK;
+}
+
+mcg_status book_create(const mcg_plan_desc* trades, uint32_t n, const mcg_book_options* opt, mcg_book** out) {
+    if (!out) return fail(MCG_ERR_INVALID_ARGUMENT, "null out_book");
+    *out = nullptr;
+    if (!trades || n == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "empty book");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+        return fail(MCG_ERR_CUDA, "no CUDA device is visible");
+    std::unique_ptr<mcg_book> b(new (std::nothrow) mcg_book());
+    if (!b) return fail(MCG_ERR_ALLOCATION, "book allocation");
+    b->trades = n;
+    b->units = trades[0].sampling_units;
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, 0);
+    std::vector<DevicePlan> dp(n);
+    std::vector<uint32_t> masks(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const mcg_plan_desc& d = trades[i];
+        const std::string who = "trade " + std::to_string(i) + ": ";
+        if (d.engine != MCG_ENGINE_PSEUDO || d.product_count != 1 || d.request_delta || d.request_gamma ||
+            d.request_vega || d.request_local_vega_nodes)
+            return fail(MCG_ERR_UNSUPPORTED, who + "a book trade is pseudo-MC, one product, price only");
+        if (d.sampling_units != b->units)
+            return fail(MCG_ERR_INVALID_ARGUMENT, who + "every trade of a book has the same sampling_units");
+        if (d.model == MCG_MODEL_LOCAL_VOLATILITY && d.antithetic)
+            return fail(MCG_ERR_UNSUPPORTED, who + "local-volatility book trades are not antithetic");
+        auto* plan = new (std::nothrow) mcg_plan();
+        if (!plan) return fail(MCG_ERR_ALLOCATION, "plan allocation");
+        b->plans.push_back(plan);
+        const mcg_status st = build(&d, *plan, false);
+        if (st != MCG_OK) return fail(st, who + g_last_error);
+        dp[i] = plan->dp;
+        masks[i] = plan->mask;
+        const bool lv = d.model == MCG_MODEL_LOCAL_VOLATILITY;
+        b->trade_path.push_back(lv ? kBookLocalVol : (plan->single_terminal ? kBookBsTerminal : kBookBsPath));
+        const uint32_t steps = lv ? plan->dp.steps : (plan->single_terminal ? 1u : plan->dp.observation_count);
+        b->trade_steps.push_back(steps);
+        b->path_steps += b->units * steps * (d.antithetic ? 2u : 1u);
+        if (lv) {
+            b->max_values = std::max(b->max_values, plan->dp.nt * plan->dp.nx);
+            b->max_nodes = std::max(b->max_nodes, plan->dp.nx);
+            b->max_slots = std::max(b->max_slots, plan->dp.slot_count);
+        }
+    }
+    b->tiles = b->plans[0]->tiles;
+    b->smem = book_smem_bytes(b->max_values, b->max_nodes, b->max_slots);
+    if (b->smem > 200 * 1024) return fail(MCG_ERR_UNSUPPORTED, "book grids too large for shared memory");
+    MCG_CUDA(book_prepare(b->smem));
+    int fit = 1;
+    MCG_CUDA(book_occupancy(b->smem, &fit));
+    fit = std::max(fit, 1);
+    MCG_CUDA(b->dplans.upload(dp));
+    MCG_CUDA(b->masks.upload(masks));
+    MCG_CUDA(b->cursor.alloc(1));
+    MCG_CUDA(b->partials.alloc(static_cast<size_t>(n) * b->tiles * kComponents));
+    MCG_CUDA(b->records.alloc(static_cast<size_t>(n) * kComponents));
+    MCG_CUDA(b->errors.alloc(n));
+    std::vector<uint32_t> all(n);
+    for (uint32_t i = 0; i < n; ++i) all[i] = i;
+    mcg_book_options o{};
+    if (opt) o = *opt;
+    uint32_t tpi = o.tiles_per_item ? o.tiles_per_item : 4u;
+    uint32_t cps = o.ctas_per_sm ? std::min<uint32_t>(o.ctas_per_sm, static_cast<uint32_t>(fit))
+                                 : static_cast<uint32_t>(fit);
+    if (o.autotune) {
+        // Candidate shapes timed on a stratified sample (every k-th trade of
+        // the book, at most 128 trades), the fastest kept.
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<uint32_t> sample;
+        const uint32_t stride = std::max(1u, n / 128u);
+        for (uint32_t i = 0; i < n; i += stride) sample.push_back(i);
+        cudaStream_t s;
+        MCG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        cudaEvent_t e0, e1;
+        MCG_CUDA(cudaEventCreate(&e0));
+        MCG_CUDA(cudaEventCreate(&e1));
+        float best = 1e30f;
+        uint32_t best_tpi = tpi, best_cps = cps;
+        std::vector<uint32_t> cps_candidates;
+        for (uint32_t c : {2u, 4u})
+            if (c <= static_cast<uint32_t>(fit)) cps_candidates.push_back(c);
+        if (std::find(cps_candidates.begin(), cps_candidates.end(), static_cast<uint32_t>(fit)) == cps_candidates.end())
+            cps_candidates.push_back(static_cast<uint32_t>(fit));
+        mcg_status st = MCG_OK;
+        for (uint32_t cand_tpi : {1u, 4u, 16u}) {
+            for (uint32_t cand_cps : cps_candidates) {
+                if ((st = book_set_shape(*b, cand_tpi, cand_cps, sample)) != MCG_OK) break;
+                float ms = 0.f;
+                for (int rep = 0; rep < 2; ++rep) {  // the first run warms the caches
+                    if (cudaEventRecord(e0, s) != cudaSuccess || book_enqueue(*b, s) != cudaSuccess ||
+                        cudaEventRecord(e1, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+                        st = fail(MCG_ERR_CUDA, "book autotune launch failed");
+                        break;
+                    }
+                    cudaEventElapsedTime(&ms, e0, e1);
+                }
+                if (st != MCG_OK) break;
+                if (ms < best) {
+                    best = ms;
+                    best_tpi = cand_tpi;
+                    best_cps = cand_cps;
+                }
+            }
+            if (st != MCG_OK) break;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(s);
+        if (st != MCG_OK) return st;
+        tpi = best_tpi;
+        cps = best_cps;
+        b->autotune_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    mcg_status st = book_set_shape(*b, tpi, cps, all);
+    if (st != MCG_OK) return st;
+    if (o.use_graph) {
+        MCG_CUDA(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking));
+        MCG_CUDA(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t ce = book_enqueue(*b, b->capture_stream);
+        const cudaError_t ee = cudaStreamEndCapture(b->capture_stream, &b->graph);
+        if (ce != cudaSuccess || ee != cudaSuccess)
+            return fail(MCG_ERR_CUDA, std::string("book graph capture: ") +
+                                          cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+        MCG_CUDA(cudaGraphInstantiate(&b->graph_exec, b->graph, 0));
+    }
+    *out = b.release();
+    return MCG_OK;
+}
+
+mcg_status book_evaluate(mcg_book* b, cudaStream_t stream, mcg_estimate* prices, mcg_book_report* report) {
+    if (!b || !prices) return fail(MCG_ERR_INVALID_ARGUMENT, "null book or prices");
+    cudaEvent_t e0, e1;
+    MCG_CUDA(cudaEventCreate(&e0));
+    MCG_CUDA(cudaEventCreate(&e1));
+    MCG_CUDA(cudaEventRecord(e0, stream));
+    if (b->graph_exec) {
+        MCG_CUDA(cudaGraphLaunch(b->graph_exec, stream));
+    } else {
+        MCG_CUDA(book_enqueue(*b, stream));
+    }
+    MCG_CUDA(cudaEventRecord(e1, stream));
+    std::vector<StatRecord> rec(static_cast<size_t>(b->trades) * kComponents);
+    std::vector<ErrorWord> errs(b->trades);
+    MCG_CUDA(cudaMemcpyAsync(rec.data(), b->records.ptr, rec.size() * sizeof(StatRecord), cudaMemcpyDeviceToHost,
+                             stream));
+    MCG_CUDA(cudaMemcpyAsync(errs.data(), b->errors.ptr, errs.size() * sizeof(ErrorWord), cudaMemcpyDeviceToHost,
+                             stream));
+    MCG_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (report) {
+        std::memset(report, 0, sizeof(*report));
+        report->trade_count = b->trades;
+        report->items = static_cast<uint32_t>(b->host_items.size());
+        report->tiles_per_item = b->tiles_per_item;
+        report->ctas_per_sm = b->ctas_per_sm;
+        report->ctas = b->ctas;
+        report->kernel_launches = 2;
+        report->graph = b->graph_exec ? 1 : 0;
+        report->device_ms = ms;
+        report->autotune_ms = b->autotune_ms;
+        report->path_steps = b->path_steps;
+    }
+    for (uint32_t t = 0; t < b->trades; ++t)
+        if (errs[t].key != ~0ull) {
+            if (report) {
+                report->error.code = static_cast<int32_t>(errs[t].key & 0xff);
+                report->error.step = t;
+                report->error.sampling_unit = errs[t].key >> 8;
+            }
+            return fail(static_cast<mcg_status>(errs[t].key & 0xff),
+                        "trade " + std::to_string(t) + ", sampling unit " + std::to_string(errs[t].key >> 8) +
+                            " failed");
+        }
+    for (uint32_t t = 0; t < b->trades; ++t) {
+        const StatRecord& s = rec[static_cast<size_t>(t) * kComponents + MCG_PRICE];
+        const HostStat h{s.sum, s.corr, static_cast<uint64_t>(s.count), s.mean, s.m2};
+        prices[t] = make_estimate(h, b->units, 1.0);
+    }
+    return MCG_OK;
+}
+
 }  // namespace
 
 namespace mcg {
@@ -1487,6 +1775,17 @@ mcg_status mcg_lsm_price(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, voi
                          mcg_lsm_result* result) {
     return lsm_price(plan, lsm, static_cast<cudaStream_t>(stream), result);
 }
+
+mcg_status mcg_book_create(const mcg_plan_desc* trades, uint32_t trade_count, const mcg_book_options* options,
+                           mcg_book** out_book) {
+    return book_create(trades, trade_count, options, out_book);
+}
+
+mcg_status mcg_book_evaluate(mcg_book* book, void* stream, mcg_estimate* prices, mcg_book_report* report) {
+    return book_evaluate(book, static_cast<cudaStream_t>(stream), prices, report);
+}
+
+void mcg_book_destroy(mcg_book* book) { delete book; }
 
 mcg_status mcg_mlp_forward(const float* params, const float* x, uint32_t count, float* out) {
     if (!params || !x || !out || count == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "mcg_mlp_forward arguments");

@@ -215,3 +215,16 @@ class LsmBuffers:
         self.result.stopping_capacity = stopping
         if stopping:
             self.result.stopping_indices = C.cast(self.stops, C.POINTER(C.c_uint32))
+
+
+# ---- batched book ----
+class BookOptions(C.Structure):
+    _fields_ = [("autotune", C.c_int32), ("tiles_per_item", C.c_uint32), ("ctas_per_sm", C.c_uint32),
+                ("use_graph", C.c_int32)]
+
+
+class BookReport(C.Structure):
+    _fields_ = [("trade_count", C.c_uint32), ("items", C.c_uint32), ("tiles_per_item", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("ctas", C.c_uint32), ("kernel_launches", C.c_uint32),
+                ("graph", C.c_int32), ("device_ms", C.c_float), ("autotune_ms", C.c_float),
+                ("path_steps", C.c_uint64), ("error", ErrorRecord)]

@@ -18,7 +18,8 @@ EXPORTS = (
     "mcg_abi_version", "mcg_last_error", "mcg_plan_create", "mcg_plan_evaluate", "mcg_price",
     "mcg_plan_destroy", "mcg_plan_shape", "mcg_philox_normals", "mcg_rqmc_words",
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
-    "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient",
+    "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient", "mcg_book_create", "mcg_book_evaluate",
+    "mcg_book_destroy",
 )
 
 _lib = None
@@ -76,6 +77,11 @@ def library() -> C.CDLL:
     lib.mcg_mlp_forward.restype = C.c_int
     lib.mcg_mlp_gradient.argtypes = [fp, fp, fp, C.POINTER(C.c_uint8), u32, fp, fp]
     lib.mcg_mlp_gradient.restype = C.c_int
+    lib.mcg_book_create.argtypes = [C.POINTER(A.PlanDesc), u32, C.POINTER(A.BookOptions), C.POINTER(vp)]
+    lib.mcg_book_create.restype = C.c_int
+    lib.mcg_book_evaluate.argtypes = [vp, vp, C.POINTER(A.Estimate), C.POINTER(A.BookReport)]
+    lib.mcg_book_evaluate.restype = C.c_int
+    lib.mcg_book_destroy.argtypes = [vp]
     if lib.mcg_abi_version() != A.ABI_VERSION:
         raise EngineError(1, "engine library ABI version mismatch")
     _lib = lib
@@ -149,6 +155,45 @@ class Plan:
     def close(self) -> None:
         if self.handle:
             library().mcg_plan_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Book:
+    """An mcg_book handle: a book of single-product plans priced in one launch."""
+
+    def __init__(self, specs, autotune: bool = True, tiles_per_item: int = 0, ctas_per_sm: int = 0,
+                 use_graph: bool = True):
+        self.specs = list(specs)
+        descs = (A.PlanDesc * len(self.specs))()
+        for i, sp in enumerate(self.specs):
+            descs[i] = sp.desc()  # each spec keeps its arrays alive
+        self._descs = descs
+        opts = A.BookOptions(int(autotune), tiles_per_item, ctas_per_sm, int(use_graph))
+        self.handle = C.c_void_p()
+        check(library().mcg_book_create(descs, len(self.specs), C.byref(opts), C.byref(self.handle)))
+
+    def evaluate(self, stream: int = 0):
+        prices = (A.Estimate * len(self.specs))()
+        report = A.BookReport()
+        status = library().mcg_book_evaluate(self.handle, C.c_void_p(stream), prices, C.byref(report))
+        check(status, report.error)
+        return prices, report
+
+    def close(self) -> None:
+        if self.handle:
+            library().mcg_book_destroy(self.handle)
             self.handle = C.c_void_p()
 
     def __del__(self):

@@ -12,6 +12,11 @@ crates/pricing/examples/benchmark_european_bs.rs).
                       rebate 1, priced on the same draws.
 * local_vol_adjoint -- the same surface, continuous down-and-out call with
                       compact-C2 smoothing 0.5 (0.5% of spot).
+* batched_book     -- a book of trades (seeded): maturities U(0.1, 3) years
+                      with daily steps, strikes U(70, 130), 40 % European /
+                      25 % Asian / 20 % continuous down-and-out / 15 % lookback,
+                      half Black--Scholes (sigma U(0.15, 0.35)), half local
+                      volatility on their own SSVI grids (rho, eta perturbed).
 * american_bs      -- American put by LSM: S=K=100, r=5%, q=0, sigma=25%, T=1,
                       50 equally spaced exercise dates, cubic basis in spot,
                       CPQR tolerances 1e-14 / 1e-12, ITM tolerance 0.
@@ -146,3 +151,45 @@ def american_bs(dates: int = 50, units: int = 1 << 20, training_units: Optional[
                   training_scramble_count=scrambles, training_antithetic=antithetic, max_degree=max_degree,
                   max_matrix_elements=1 << 40)
     return spec, lsm
+
+
+BOOK_SEED = 20260904
+
+
+def batched_book(builder: GridBuilder, trades: int = 4096, units: int = 1 << 16, seed: int = BOOK_SEED,
+                 expiries: int = 30) -> list[PlanSpec]:
+    """The batched-book configuration: `trades` single-product plans, each
+    with its own seed, maturity, step count, strike, product and model."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    kinds = np.array([A.PRODUCT_EUROPEAN] * 8 + [A.PRODUCT_ASIAN] * 5 + [A.PRODUCT_CONTINUOUS_BARRIER] * 4 +
+                     [A.PRODUCT_LOOKBACK] * 3)
+    for i in range(trades):
+        horizon = float(rng.uniform(0.1, 3.0))
+        steps = max(1, int(round(252 * horizon)))
+        strike = float(rng.uniform(70.0, 130.0))
+        kind = int(kinds[rng.integers(0, len(kinds))])
+        local = bool(rng.integers(0, 2))
+        vol = float(rng.uniform(0.15, 0.35))
+        rho = float(rng.uniform(-0.6, -0.2))
+        eta = float(rng.uniform(0.7, 1.3))
+        barrier = float(rng.uniform(60.0, 90.0))
+        times = daily_times(steps, horizon)
+        if kind == A.PRODUCT_ASIAN:
+            product = ProductSpec(kind=kind, strike=strike, weights=[1.0 / steps] * steps)
+        elif kind == A.PRODUCT_CONTINUOUS_BARRIER:
+            product = ProductSpec(kind=kind, strike=strike, barrier=barrier, barrier_direction=A.BARRIER_DOWN,
+                                  barrier_style=A.KNOCK_OUT)
+        else:
+            product = ProductSpec(kind=kind, strike=strike)
+        if kind == A.PRODUCT_EUROPEAN and not local:
+            times = [horizon]
+        spec = PlanSpec(observation_times=times, products=[product], engine=A.ENGINE_PSEUDO,
+                        master_seed=(SEED + 7919 * i) & 0xFFFFFFFFFFFFFFFF, sampling_units=units, spot=100.0,
+                        volatility=vol, **flat_curves(horizon=horizon))
+        if local:
+            surface = SsviSurface(steps=steps, expiries=min(expiries, steps), horizon=horizon, rho=rho, eta=eta)
+            spec.model = A.MODEL_LOCAL_VOLATILITY
+            spec.local_variance = local_vol_grid(surface, builder)
+        specs.append(spec)
+    return specs
