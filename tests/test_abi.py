@@ -47,6 +47,7 @@ STRUCTS = {
     "mcg_estimate": A.Estimate, "mcg_product_result": A.ProductResult,
     "mcg_error_record": A.ErrorRecord, "mcg_result": A.Result,
     "mcg_lsm_desc": A.LsmDesc, "mcg_lsm_date_model": A.LsmDateModel, "mcg_lsm_result": A.LsmResult,
+    "mcg_book_options": A.BookOptions, "mcg_book_report": A.BookReport,
 }
 
 
