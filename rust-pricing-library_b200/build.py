@@ -32,6 +32,7 @@ UNITS = [
     ("mcg_lsm.cu", ["-fmad=false"]),
     ("mcg_mlp.cu", []),
     ("mcg_book.cu", ["-fmad=false"]),
+    ("mcg_lv32.cu", []),
 ]
 
 

@@ -32,6 +32,8 @@ namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
                            StatRecord* partials, uint32_t mask, ErrorWord* err, int detail,
                            cudaStream_t stream, int& evolutions_out);
+cudaError_t launch_lv32_path(const DevicePlan& P, StatRecord* partials, uint32_t mask, ErrorWord* err,
+                             cudaStream_t stream);
 cudaError_t launch_bs_path(const DevicePlan& P, bool single_terminal, uint64_t unit_begin, uint64_t units,
                            uint32_t scrambles, StatRecord* partials, uint32_t mask, ErrorWord* err,
                            int detail, cudaStream_t stream);
@@ -368,8 +370,13 @@ struct mcg_plan {
     uint64_t chunk_units = 0;
     DeviceArray<double> tape, adj_vega, adj_delta, node_tiles;
     DeviceArray<StatRecord> adj_partials, adj_records, node_records;
+    DeviceArray<float> fwd_f, ratio_f;
+    DeviceArray<float4> step_f;
 
     ~mcg_plan() {
+        fwd_f.release();
+        ratio_f.release();
+        step_f.release();
         ops.release();
         node_time.release();
         dt.release();
@@ -478,8 +485,12 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         return fail(MCG_ERR_UNSUPPORTED, "model");
     if (d->engine != MCG_ENGINE_PSEUDO && d->engine != MCG_ENGINE_RQMC)
         return fail(MCG_ERR_UNSUPPORTED, "engine");
-    if (d->precision != MCG_PRECISION_F64)
-        return fail(MCG_ERR_UNSUPPORTED, "precision: this entry point evaluates FP64 plans");
+    if (d->precision != MCG_PRECISION_F64 && d->precision != MCG_PRECISION_F32_BULK)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "precision");
+    if (d->precision == MCG_PRECISION_F32_BULK &&
+        (d->model != MCG_MODEL_LOCAL_VOLATILITY || d->request_delta || d->request_gamma || d->request_vega ||
+         d->request_local_vega_nodes))
+        return fail(MCG_ERR_UNSUPPORTED, "the FP32 path bulk prices local-volatility plans without risk");
     if (!(d->spot > 0.0) || !std::isfinite(d->spot)) return fail(MCG_ERR_INVALID_ARGUMENT, "spot");
     if (d->observation_count == 0 || !d->observation_times)
         return fail(MCG_ERR_INVALID_ARGUMENT, "observation_times");
@@ -634,6 +645,22 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
             while (k <= steps && bits_of(nodes[k]) != b) ++k;
             if (k > steps) return fail(MCG_ERR_MARKET, "observation time missing from the time grid");
             oon[k] = static_cast<int32_t>(i);
+        }
+        if (d->precision == MCG_PRECISION_F32_BULK) {
+            std::vector<float> inv_f(steps + 1), ra_f(steps);
+            std::vector<float4> sk(steps);
+            for (uint32_t i = 0; i <= steps; ++i) inv_f[i] = static_cast<float>(1.0 / fw[i]);
+            for (uint32_t i = 0; i < steps; ++i) {
+                ra_f[i] = static_cast<float>(ra[i]);
+                sk[i] = make_float4(static_cast<float>(dtv[i]), static_cast<float>(sq[i]), static_cast<float>(tw[i]),
+                                    static_cast<float>(isq[i]));
+            }
+            MCG_CUDA(plan.fwd_f.upload(inv_f));
+            MCG_CUDA(plan.ratio_f.upload(ra_f));
+            MCG_CUDA(plan.step_f.upload(sk));
+            P.fwd_f = plan.fwd_f.ptr;
+            P.ratio_f = plan.ratio_f.ptr;
+            P.step_f = plan.step_f.ptr;
         }
         MCG_CUDA(plan.node_time.upload(nodes));
         MCG_CUDA(plan.dt.upload(dtv));
@@ -826,7 +853,9 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
     uint32_t launches = 0;
     cudaError_t e;
     // Per-product partials use kComponents stride; reduce only masked slots below.
-    if (P.model == MCG_MODEL_LOCAL_VOLATILITY) {
+    if (P.model == MCG_MODEL_LOCAL_VOLATILITY && P.precision == MCG_PRECISION_F32_BULK) {
+        e = launch_lv32_path(P, plan->partials.ptr, plan->mask, plan->error.ptr, stream);
+    } else if (P.model == MCG_MODEL_LOCAL_VOLATILITY) {
         int evolutions;
         e = launch_lv_path(P, 0, P.units, P.scramble_count, plan->partials.ptr, plan->mask, plan->error.ptr, 0,
                            stream, evolutions);
@@ -915,6 +944,12 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
     result->device_ms = ms;
     result->path_kernel_ms = path_ms;
     result->kernel_launches = launches;
+    if (ew.key != ~0ull && P.precision == MCG_PRECISION_F32_BULK) {
+        result->error.code = static_cast<int32_t>(ew.key & 0xff);
+        result->error.sampling_unit = ew.key >> 8;
+        return fail(static_cast<mcg_status>(result->error.code),
+                    "sampling unit " + std::to_string(result->error.sampling_unit) + " failed (FP32 path bulk)");
+    }
     if (ew.key != ~0ull) {
         // Re-run the first failing unit alone to recover step and value bits.
         const uint64_t unit = ew.key >> 8;

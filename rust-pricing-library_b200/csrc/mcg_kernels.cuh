@@ -42,6 +42,12 @@ __device__ __forceinline__ void report_error(ErrorWord* err, uint64_t unit, int 
 // shift XOR the pre-applied scrambled directions of the set Gray-code bits
 // (qmc.rs:71-84,125-132: apply is GF(2)-linear, so apply(XOR v_k) =
 // XOR M v_k ^ shift); pseudo: Philox coordinate (unit, dim, domain).
+//
+// The Gray code of point p splits as gray(p & ~31) ^ gray(p & 31) (the two
+// halves of p ^ (p >> 1) touch disjoint bits), so for a warp of 32
+// consecutive points the high part is the same in every lane -- a uniform
+// loop of broadcast loads -- and the lane part is five predicated XORs.  The
+// word is the same XOR of the same directions, bit for bit.
 struct NormalSource {
     int32_t rqmc;
     uint64_t seed;
@@ -57,11 +63,18 @@ struct NormalSource {
         if (rqmc) {
             const uint32_t* d = dirs + static_cast<size_t>(dim) * 32u;
             uint32_t x = __ldg(shift + dim);
-            uint32_t g = gray;
+            const uint32_t low = unit & 31u;
+            const uint32_t gl = low ^ (low >> 1);
+            uint32_t g = gray ^ gl;  // gray(unit & ~31)
             while (g) {
                 const int b = __ffs(g) - 1;
                 x ^= __ldg(d + b);
                 g &= g - 1u;
+            }
+#pragma unroll
+            for (int b = 0; b < 5; ++b) {
+                const uint32_t v = __ldg(d + b);
+                x ^= (gl >> b) & 1u ? v : 0u;
             }
             return x;
         }

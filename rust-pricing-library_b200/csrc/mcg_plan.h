@@ -78,8 +78,9 @@ struct DevicePlan {
     const double* time_weight;   // LV: grid time weight per step
     const double* fwd;           // LV: 3 x (steps + 1) forward normalizers (base, down, up)
     const double* ratio;         // LV: 3 x steps forward ratios F[i+1]/F[i]
-    const float* fwd_f;          // FP32 copies for the bulk path
-    const float* ratio_f;
+    const float* fwd_f;          // FP32 bulk: reciprocal base forward normalisers 1/F_i (steps + 1)
+    const float* ratio_f;        // FP32 bulk: base forward ratios F_{i+1}/F_i (steps)
+    const float4* step_f;        // FP32 bulk: per step {dt, sqrt(dt), time weight, 1/sqrt(dt)}
 
     // Black--Scholes observation data (observation_count entries)
     const double* obs_time;
