@@ -54,6 +54,13 @@ def parse():
     ap.add_argument("--scrambles", type=int, default=SCRAMBLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
+                    help="path arithmetic of the timed workload (f32: FP32 path bulk)")
+    ap.add_argument("--secondary", default="all",
+                    help="comma list of secondary measurements: early_exercise, book, f32; all; none")
+    ap.add_argument("--lsm-units", type=int, default=1 << 20)
+    ap.add_argument("--book-trades", type=int, default=4096)
+    ap.add_argument("--book-units", type=int, default=1 << 16)
     return ap.parse_args()
 
 
@@ -62,10 +69,12 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def workload(points, scrambles, builder, scramble_begin=0):
+def workload(points, scrambles, builder, scramble_begin=0, precision="f64"):
+    from rust_pricing_b200 import _abi as A
     from rust_pricing_b200 import workloads as W
     spec = W.local_vol_rqmc(builder, points=points, scrambles=scrambles)
     spec.scramble_begin = scramble_begin
+    spec.precision = A.PRECISION_F32_BULK if precision == "f32" else A.PRECISION_F64
     return spec
 
 
@@ -163,7 +172,66 @@ def time_to_bp(ms: float, se: float, price: float) -> float:
     return ms * (se / target) ** 2 if target > 0 else float("inf")
 
 
-def lsm_secondary():
+def book_secondary(trades: int, units: int):
+    """The batched-book configuration: `trades` seeded single-product trades
+    (maturities U(0.1, 3) y with daily steps, strikes U(70, 130), 40/25/20/15 %
+    European/Asian/continuous down-and-out/lookback, half Black--Scholes, half
+    local volatility on their own SSVI grids), `units` pseudo paths each, in
+    one persistent launch replayed from a CUDA graph, against pricing the same
+    trades one plan per call."""
+    from rust_pricing_b200 import _native as N, workloads as W
+    t0 = time.perf_counter()
+    specs = W.batched_book(gpu_grid, trades=trades, units=units)
+    t1 = time.perf_counter()
+    book = N.Book(specs, autotune=True, use_graph=True)
+    t2 = time.perf_counter()
+    book.evaluate()
+    prices, rep = book.evaluate()
+    book.close()
+    out = {"workload": f"{trades} trades x {units} pseudo paths (seed {W.BOOK_SEED}), one persistent launch",
+           "device_ms": rep.device_ms, "path_steps": rep.path_steps,
+           "path_steps_per_s": rep.path_steps / (rep.device_ms * 1e-3), "work_items": rep.items,
+           "tiles_per_item": rep.tiles_per_item, "ctas_per_sm": rep.ctas_per_sm, "graph": bool(rep.graph),
+           "autotune_s": rep.autotune_ms * 1e-3, "create_s": t2 - t1, "generate_s": t1 - t0}
+    # plain: the first trades, one plan and one evaluation each
+    n = min(256, trades)
+    plans = [N.Plan(sp) for sp in specs[:n]]
+    for p in plans[:4]:
+        p.evaluate()
+    steps_plain, dev_plain = 0, 0.0
+    t3 = time.perf_counter()
+    for p, sp in zip(plans, specs[:n]):
+        r = p.evaluate()
+        dev_plain += r.result.device_ms
+        steps_plain += r.result.evaluated_paths * r.result.time_steps if sp.model == 1 else (
+            r.result.evaluated_paths * (1 if len(sp.observation_times) == 1 else len(sp.observation_times)))
+    wall_plain = time.perf_counter() - t3
+    for p in plans:
+        p.close()
+    out["plain_one_plan_per_call"] = {"trades": n, "device_ms": dev_plain, "wall_ms": wall_plain * 1e3,
+                                      "path_steps_per_s": steps_plain / wall_plain}
+    out["batched_over_plain_throughput"] = out["path_steps_per_s"] / (steps_plain / wall_plain)
+    return out
+
+
+def f32_secondary(points: int, scrambles: int, prices64):
+    """The timed workload with the FP32 path bulk: time and the error of each
+    price against the FP64 run's."""
+    from rust_pricing_b200 import _native as N
+    spec = workload(points, scrambles, gpu_grid, precision="f32")
+    with N.Plan(spec) as plan:
+        plan.evaluate()
+        times, r = [], None
+        for _ in range(3):
+            r = plan.evaluate()
+            times.append(r.result.device_ms)
+    p32 = [r.products[k].price.value for k in range(len(spec.products))]
+    return {"ms_per_step": min(times), "path_steps_per_s": points * scrambles * STEPS / (min(times) * 1e-3),
+            "prices": p32, "relative_error_vs_f64": [(a - b) / b for a, b in zip(p32, prices64)],
+            "error_in_standard_errors": None}
+
+
+def lsm_secondary(units: int = 1 << 20):
     """The early-exercise configuration (American put S=K=100, r=5%, sigma=25%,
     T=1, 50 dates, 2^20 training + 2^20 valuation paths): the reference's
     polynomial policy and the learned continuation, against the 5000-step
@@ -172,10 +240,10 @@ def lsm_secondary():
     from bermudan_tree import bermudan_equally_spaced
     from rust_pricing_b200 import _abi as A, _native as N, workloads as W
     tree = bermudan_equally_spaced(100.0, 100.0, 0.05, 0.0, 0.25, 1.0, 50, steps=5000)
-    out = {"workload": "American put by LSM, 50 dates, 2^20 + 2^20 paths, cubic basis; judge: 5000-step "
+    out = {"workload": f"American put by LSM, 50 dates, {units} + {units} paths, cubic basis; judge: 5000-step "
                        "Bermudan binomial tree", "tree": tree}
     for name, kind in (("plain", A.CONTINUATION_POLYNOMIAL), ("learned", A.CONTINUATION_MLP)):
-        spec, lsm = W.american_bs(dates=50, units=1 << 20)
+        spec, lsm = W.american_bs(dates=50, units=units)
         lsm.continuation = kind
         lsm.mlp_seed = 7
         N.lsm_price(spec, lsm)
@@ -185,7 +253,7 @@ def lsm_secondary():
         out[name] = {"device_ms": r.device_ms, "fit_ms": fixed, "valuation_ms": r.device_ms - fixed,
                      "price": r.price.value, "standard_error": r.price.standard_error,
                      "error_vs_tree": r.price.value - tree, "policy": "mlp" if r.continuation_used else "polynomial",
-                     "path_steps_per_s": 2 * (1 << 20) * 50 / (r.device_ms * 1e-3),
+                     "path_steps_per_s": 2 * units * 50 / (r.device_ms * 1e-3),
                      "ms_to_1bp_standard_error": fixed + time_to_bp(r.device_ms - fixed, r.price.standard_error,
                                                                     r.price.value),
                      "kernel_launches": r.kernel_launches}
@@ -195,7 +263,7 @@ def lsm_secondary():
 def sized_cpu_sample(threads: int, grid_builder=None, target_s: float = 15.0):
     """Points per scramble (a power of two, 2 scrambles) for about `target_s`
     seconds of oracle work on this host, from a short calibration run."""
-    rate, _, _ = cpu_baseline(1 << 11, 1, threads, grid_builder)
+    rate, _, _ = cpu_baseline(1 << 14, 1, threads, grid_builder)
     points, scrambles = 1 << 11, 2
     while points < (1 << 20) and 2 * scrambles * points * STEPS / rate <= target_s:
         points *= 2
@@ -252,7 +320,8 @@ def main():
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
     handle = stream.cuda_stream
-    spec = workload(args.points, args.scrambles, gpu_grid, scramble_begin=rank * args.scrambles)
+    spec = workload(args.points, args.scrambles, gpu_grid, scramble_begin=rank * args.scrambles,
+                    precision=args.precision)
     plan = N.Plan(spec)
     path_steps_rank = args.points * args.scrambles * STEPS
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -290,7 +359,8 @@ def main():
     N.check(N.library().mcg_measure_fp64_peak(C.c_void_p(handle), C.byref(peak)))
     path_ms = statistics.mean(kernel_ms)
     achieved = FLOPS_PER_PATH_STEP * path_steps_rank / (path_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+    roofline = {"bound": "fp64" if args.precision == "f64" else "fp64 (FP32 path bulk: the FP64 figure only bounds it)",
+                "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": achieved / peak.value if peak.value else None, "traffic": None,
                 "peak_source": "measured live: mcg_measure_fp64_peak (DFMA chains, this GPU)",
                 "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel_ms": path_ms}
@@ -316,7 +386,8 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "f64" else "f32 path bulk, f64 payoffs",
+        "data": "synthetic",
         "config": {"workload": "local-vol RQMC: SSVI->Dupire 31x100 grid, 252 daily steps, 2^20 Sobol points x 16 "
                                "scrambles, Brownian bridge, Asian call + discrete down-and-out on the same draws",
                    "points_per_scramble": args.points, "scrambles_per_gpu": args.scrambles, "time_steps": STEPS,
@@ -331,8 +402,20 @@ def main():
         "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, buf.products[k].price.standard_error,
                                                 buf.products[k].price.value) for k in range(len(spec.products))],
     }
-    if rank == 0 and world == 1:
-        line["secondary"] = {"early_exercise": lsm_secondary()}
+    wanted = {"early_exercise", "book", "f32"} if args.secondary == "all" else (
+        set() if args.secondary == "none" else set(args.secondary.split(",")))
+    if rank == 0 and world == 1 and wanted:
+        sec = {}
+        if "early_exercise" in wanted:
+            sec["early_exercise"] = lsm_secondary(args.lsm_units)
+        if "f32" in wanted and args.precision == "f64":
+            f32 = f32_secondary(args.points, args.scrambles, line["prices"])
+            f32["error_in_standard_errors"] = [e * p / se for e, p, se in zip(
+                f32["relative_error_vs_f64"], line["prices"], line["price_standard_errors"])]
+            sec["f32_bulk"] = f32
+        if "book" in wanted:
+            sec["batched_book"] = book_secondary(args.book_trades, args.book_units)
+        line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample_points, sample_scrambles = sized_cpu_sample(threads, grid_builder=gpu_grid)
