@@ -372,9 +372,11 @@ typedef struct mcg_lsm_desc {
      * an ITM path when the immediate value beats the predicted continuation.
      * The polynomial policy is fitted too and is used instead (fallback) when
      * the network's training diverges or its in-sample value is lower.
-     * Adam steps per date: max(epochs x batches, 400) at the last
-     * non-terminal date, max(epochs x batches, 50) at the others. */
-    uint32_t mlp_epochs;      /* passes over each date's rows; 0 = 1 */
+     * Adam steps per date: with mlp_epochs = 0, max(batches, 400) at the last
+     * non-terminal date (trained from scratch) and max(batches, 50) at the
+     * others (warm-started); otherwise epochs x batches, 4x at the last
+     * non-terminal date. */
+    uint32_t mlp_epochs;      /* passes over each date's rows; 0 = the default schedule */
     uint32_t mlp_batch;       /* training rows per Adam step; 0 = 16384 */
     float mlp_learning_rate;  /* Adam step size; 0 = 2e-3 */
     uint64_t mlp_seed;        /* initial weights */

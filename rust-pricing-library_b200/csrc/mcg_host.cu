@@ -1327,8 +1327,13 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
         uint32_t step = 0;
         for (int date = last - 1; date >= 0; --date) {
             const double tin = 2.0 * d->observation_times[date] / horizon - 1.0;
-            const uint64_t floor_steps = date == last - 1 ? 400u : 50u;
-            const uint64_t steps = std::max<uint64_t>(static_cast<uint64_t>(epochs) * nbatch, floor_steps);
+            // Default schedule: at least 400 Adam steps at the first (from-scratch)
+            // date and 50 at the warm-started ones; an explicit epoch count gives
+            // exactly epochs x batches (4x at the first date).
+            const uint64_t first = date == last - 1 ? 4u : 1u;
+            const uint64_t steps = l->mlp_epochs
+                                       ? first * static_cast<uint64_t>(epochs) * nbatch
+                                       : std::max<uint64_t>(nbatch, date == last - 1 ? 400u : 50u);
             for (uint64_t k = 0; k < steps; ++k) {
                 const uint64_t b = k % nbatch;
                 MlpRows rows{};

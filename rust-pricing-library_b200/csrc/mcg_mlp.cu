@@ -63,7 +63,10 @@ __device__ void load_net(NetShared& s, const float* __restrict__ p) {
     __syncthreads();
 }
 
-__device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
+// Logistic function on the special-function unit (exp2 and reciprocal
+// approximations, ~2 ulp): the network is an approximation itself, and the
+// gradient checks bound the whole forward/backward pass.
+__device__ __forceinline__ float sigmoid(float x) { return __fdividef(1.0f, 1.0f + __expf(-x)); }
 __device__ __forceinline__ float silu(float x) { return x * sigmoid(x); }
 __device__ __forceinline__ float silu_grad(float x) {
     const float s = sigmoid(x);
@@ -268,8 +271,9 @@ __global__ void __launch_bounds__(kMlpThreads) mlp_gradient_kernel(const float* 
                     for (int j = 0; j < 2; ++j) {
                         const float v = acc[mt][nt][2 * h + j];
                         const int col = nt * 8 + 2 * t + j;
-                        gw3v[j] += dlt[mt][h] * silu(v);
-                        dh[j] = dlt[mt][h] * S.net.w3[col] * silu_grad(v);
+                        const float sg = sigmoid(v);  // one logistic for silu and its derivative
+                        gw3v[j] += dlt[mt][h] * (v * sg);
+                        dh[j] = dlt[mt][h] * S.net.w3[col] * (sg * (1.0f + v * (1.0f - sg)));
                         gb2v[j] += dh[j];
                     }
                     *reinterpret_cast<uint32_t*>(d2w + (mt * 16 + h * 8 + g) * kStride + nt * 8 + 2 * t) =
@@ -400,7 +404,8 @@ __global__ void mlp_adam_kernel(const float* __restrict__ partials, unsigned cta
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kMlpParams) return;
     float rows = 0.0f, gsum = 0.0f;
-    for (unsigned c = 0; c < ctas; ++c) {
+#pragma unroll 8
+    for (unsigned c = 0; c < ctas; ++c) {  // in CTA order; the loads run ahead of the adds
         gsum += partials[static_cast<size_t>(c) * kMlpPartial + i];
         rows += partials[static_cast<size_t>(c) * kMlpPartial + kMlpParams + 1];
     }
