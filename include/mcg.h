@@ -338,7 +338,8 @@ mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double*
  * American payoff graph observes exactly the exercise dates,
  * crates/pricing/src/engine/payoff/compile.rs:67-101).  Its engine fields are
  * the valuation engine; `mcg_lsm_desc` adds the training engine (same kind) and
- * the regression configuration (LsmConfig).  Risk requests must be off. */
+ * the regression configuration (LsmConfig).  Risk requests (Black-Scholes) ask
+ * for the fixed-policy Greeks of mcg_lsm_result. */
 #define MCG_LSM_MAX_DEGREE 7u
 #define MCG_LSM_MAX_BASIS (MCG_LSM_MAX_DEGREE + 1u)
 
@@ -432,6 +433,21 @@ typedef struct mcg_lsm_result {
     float path_kernel_ms;           /* both path-matrix kernels */
     float regression_ms;            /* backward regression of the training phase */
     float valuation_ms;             /* policy valuation and statistics */
+    /* Fixed-policy risk (the plan's request_delta / request_gamma /
+     * request_vega, Black-Scholes): pathwise AAD of each valuation path's
+     * discounted exercise value at its stopping date -- Delta and Vega by the
+     * reverse sweep, Gamma as the central difference of AAD Deltas, and the
+     * bump-and-revalue validation components -- reduced like the plan
+     * components (constant_vol_fixed_policy_pseudo/rqmc_statistics,
+     * crates/pricing/src/engine/mc/early_exercise.rs:454-600;
+     * fixed_policy_pathwise_values, crates/pricing/src/engine/processes/black_scholes.rs:358-415). */
+    mcg_statistics risk_components[MCG_PATHWISE_COMPONENTS];
+    mcg_estimate delta;
+    mcg_estimate gamma;
+    mcg_estimate vega;
+    mcg_estimate bump_delta;
+    mcg_estimate bump_gamma;
+    mcg_estimate bump_vega;
     /* Learned continuation only. */
     int32_t continuation_used;      /* the policy valued: mcg_continuation_kind */
     uint32_t mlp_steps;             /* Adam steps taken */

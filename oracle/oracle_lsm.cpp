@@ -29,6 +29,8 @@ namespace oracle {
 int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vector<double>& spots,
               uint64_t& path_count, mcg_error_record& err);
 double plan_discount(const mcg_plan_desc* desc, double t);
+int lsm_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, const double* df, int threads,
+                          mcg_lsm_result* result);
 
 namespace {
 
@@ -397,6 +399,16 @@ int lsm_price(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, mcg_lsm_result
     out->date_count = static_cast<uint32_t>(dates);
     if (out->models)
         for (size_t d = 0; d + 1 < dates; ++d) out->models[d] = models[d].rec;
+    // Fixed-policy risk: the valuation stopping dates held fixed, Greeks of
+    // the discounted exercise values (early_exercise.rs:454-600).
+    std::memset(out->risk_components, 0, sizeof(out->risk_components));
+    out->delta = out->gamma = out->vega = mcg_estimate{};
+    out->bump_delta = out->bump_gamma = out->bump_vega = mcg_estimate{};
+    if (desc->request_delta || desc->request_gamma || desc->request_vega) {
+        if (desc->model != MCG_MODEL_BLACK_SCHOLES) return MCG_ERR_UNSUPPORTED;
+        rc = lsm_fixed_policy_risk(desc, stop.data(), df.data(), threads, out);
+        if (rc != MCG_OK) return rc;
+    }
     return MCG_OK;
 }
 

@@ -1521,6 +1521,144 @@ int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vect
     return MCG_OK;
 }
 
+// Fixed-policy pathwise risk of an early-exercise plan under Black--Scholes:
+// per sampling unit, the 18 components of fixed_policy_pathwise_values
+// (crates/pricing/src/engine/processes/black_scholes.rs:358-415) for the
+// discounted exercise value at each path's stopping date (its
+// pathwise_aad_for_output, :567-643), antithetic mates averaged, reduced as
+// constant_vol_fixed_policy_pseudo/rqmc_statistics
+// (crates/pricing/src/engine/mc/early_exercise.rs:454-600) do.
+int lsm_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, const double* df, int threads,
+                          mcg_lsm_result* result) {
+    Plan p;
+    if (!build_plan(desc, p)) return MCG_ERR_INVALID_ARGUMENT;
+    const bool rqmc = p.engine == MCG_ENGINE_RQMC;
+    const uint64_t mult = p.antithetic ? 2 : 1;
+    const mcg_product_desc& pr = desc->products[0];
+    const bool call = pr.side == MCG_CALL;
+    const size_t n = p.obs_t.size();
+    auto eval = [&](const double* z, uint32_t k, double spot, double vol, std::vector<Obs>& obs, double& price,
+                    double& delta, double& vega) {
+        bs_observations(p, z, spot, vol, obs.data());
+        const double s = obs[k].post_spot;
+        const double in = call ? s - pr.strike : pr.strike - s;
+        const double value = (in >= 0.0 ? in : 0.0) * pr.notional;
+        const double adj = (in >= 0.0 ? pr.notional : 0.0) * (call ? 1.0 : -1.0);
+        double d = 0.0, v = 0.0;
+        if (adj != 0.0) {
+            d += adj * 1.0 * obs[k].f / spot;
+            v += adj * 1.0 * obs[k].f * (-vol * p.obs_t[k] + obs[k].w);
+        }
+        price = df[k] * value;
+        delta = df[k] * d;
+        vega = df[k] * v;
+    };
+    auto unit_components = [&](const double* z, uint32_t k, std::vector<Obs>& obs, double* values) {
+        double bp, bd, bv, dp, dd, dv, up, ud, uv, x, y, w;
+        eval(z, k, p.spot, p.vol, obs, bp, bd, bv);
+        double gamma = 0.0;
+        if (p.req_gamma) {
+            const double bump = p.gamma_bump;
+            eval(z, k, p.spot - bump, p.vol, obs, x, dd, w);
+            eval(z, k, p.spot + bump, p.vol, obs, x, ud, w);
+            gamma = (ud - dd) / (2.0 * bump);
+        }
+        const double sb = p.spot_bump;
+        eval(z, k, p.spot - sb, p.vol, obs, dp, dd, dv);
+        eval(z, k, p.spot + sb, p.vol, obs, up, ud, uv);
+        const double bump_delta = (up - dp) / (2.0 * sb);
+        const double bump_gamma = (up - 2.0 * bp + dp) / (sb * sb);
+        double bump_vega = 0.0;
+        if (p.vol_bump != 0.0) {
+            const double vb = p.vol_bump;
+            eval(z, k, p.spot, p.vol - vb, obs, x, y, w);
+            double hi;
+            eval(z, k, p.spot, p.vol + vb, obs, hi, y, w);
+            bump_vega = (hi - x) / (2.0 * vb);
+        }
+        for (int c = 0; c < kComponents; ++c) values[c] = 0.0;
+        values[MCG_PRICE] = bp;
+        values[MCG_DELTA] = bd;
+        values[MCG_VEGA] = bv;
+        values[MCG_GAMMA] = gamma;
+        values[MCG_BUMP_DELTA] = bump_delta;
+        values[MCG_DELTA_DIFFERENCE] = bump_delta - bd;
+        values[MCG_BUMP_VEGA] = bump_vega;
+        values[MCG_VEGA_DIFFERENCE] = bump_vega - bv;
+        values[MCG_BUMP_GAMMA] = bump_gamma;
+        values[MCG_GAMMA_DIFFERENCE] = bump_gamma - gamma;
+    };
+    // One scramble (RQMC) or the whole pseudo run: fixed blocks, fixed tree.
+    auto reduce = [&](uint32_t scramble, std::vector<Statistics>& out) {
+        const uint64_t units = p.units;
+        const uint64_t nblocks = (units + p.block - 1) / p.block;
+        std::vector<std::vector<Statistics>> blocks(nblocks, std::vector<Statistics>(kComponents));
+        std::atomic<uint64_t> next{0};
+        auto worker = [&]() {
+            std::vector<double> z(p.dimension), mate(p.dimension), normals, scratch;
+            std::vector<Obs> obs(n);
+            double a[kComponents], b[kComponents];
+            for (;;) {
+                const uint64_t blk = next.fetch_add(1);
+                if (blk >= nblocks) break;
+                for (uint64_t u = blk * p.block; u < std::min(units, (blk + 1) * p.block); ++u) {
+                    unit_shocks(p, scramble, u, z.data(), normals, scratch);
+                    const uint64_t base = ((rqmc ? static_cast<uint64_t>(scramble) * units : 0) + u) * mult;
+                    unit_components(z.data(), stops[base], obs, a);
+                    if (mult == 2) {
+                        for (size_t i = 0; i < z.size(); ++i) mate[i] = -z[i];
+                        unit_components(mate.data(), stops[base + 1], obs, b);
+                        for (int c = 0; c < kComponents; ++c) a[c] = (a[c] + b[c]) * 0.5;
+                    }
+                    for (int c = 0; c < kComponents; ++c) blocks[blk][c].add(a[c]);
+                }
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(worker);
+        for (auto& t : pool) t.join();
+        out.assign(kComponents, Statistics{});
+        for (int c = 0; c < kComponents; ++c) {
+            std::vector<NeumaierSum> sums;
+            std::vector<CenteredMoment> moms;
+            for (uint64_t b = 0; b < nblocks; ++b) {
+                sums.push_back(blocks[b][c].sum);
+                moms.push_back(blocks[b][c].moments);
+            }
+            out[c].sum = fixed_tree_reduce(sums, NeumaierSum::merged);
+            out[c].moments = fixed_tree_reduce(moms, CenteredMoment::merged);
+        }
+    };
+    std::vector<Statistics> total;
+    uint64_t independent;
+    if (!rqmc) {
+        reduce(0, total);
+        independent = p.units;
+    } else {
+        std::vector<std::vector<double>> reps(kComponents);
+        for (uint32_t s = 0; s < p.scrambles; ++s) {
+            std::vector<Statistics> within;
+            reduce(s, within);
+            for (int c = 0; c < kComponents; ++c)
+                reps[c].push_back(within[c].sum.total() / static_cast<double>(p.units));
+        }
+        total.assign(kComponents, Statistics{});
+        for (int c = 0; c < kComponents; ++c) {
+            total[c].moments = CenteredMoment::two_pass(reps[c]);
+            for (double v : reps[c]) total[c].sum.add(v);
+        }
+        independent = p.scrambles;
+    }
+    for (int c = 0; c < kComponents; ++c) result->risk_components[c] = to_c(total[c]);
+    result->delta = estimate(total[MCG_DELTA], independent, 1.0);
+    result->gamma = estimate(total[MCG_GAMMA], independent, 1.0);
+    result->vega = estimate(total[MCG_VEGA], independent, 1.0);
+    result->bump_delta = estimate(total[MCG_BUMP_DELTA], independent, 1.0);
+    result->bump_gamma = estimate(total[MCG_BUMP_GAMMA], independent, 1.0);
+    result->bump_vega = estimate(total[MCG_BUMP_VEGA], independent, 1.0);
+    return MCG_OK;
+}
+
 double plan_discount(const mcg_plan_desc* desc, double t) {
     Curve c;
     c.set(desc->discount_curve.times, desc->discount_curve.discount_factors,

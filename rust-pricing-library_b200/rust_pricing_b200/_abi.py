@@ -190,6 +190,9 @@ class LsmResult(C.Structure):
         ("date_count", C.c_uint32), ("kernel_launches", C.c_uint32),
         ("device_ms", C.c_float), ("path_kernel_ms", C.c_float),
         ("regression_ms", C.c_float), ("valuation_ms", C.c_float),
+        ("risk_components", Statistics * PATHWISE_COMPONENTS),
+        ("delta", Estimate), ("gamma", Estimate), ("vega", Estimate),
+        ("bump_delta", Estimate), ("bump_gamma", Estimate), ("bump_vega", Estimate),
         ("continuation_used", C.c_int32), ("mlp_steps", C.c_uint32), ("mlp_ms", C.c_float),
         ("mlp_final_loss", C.c_float), ("polynomial_in_sample", C.c_double), ("mlp_in_sample", C.c_double),
         ("mlp_param_capacity", C.c_uint32), ("mlp_params", C.POINTER(C.c_float)),

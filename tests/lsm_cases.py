@@ -25,6 +25,16 @@ def _engine_kwargs(e: dict) -> dict:
                 antithetic=e["antithetic"], brownian_bridge=e["brownian_bridge"])
 
 
+def _risk_kwargs(r: dict) -> dict:
+    """Risk requests of a replay case: delta/vega flags and the gamma bump."""
+    kw = dict(request_delta=bool(r.get("delta")), request_vega=bool(r.get("vega")))
+    g = r.get("gamma")
+    if g:
+        bump = g["bump"]
+        kw.update(request_gamma=True, gamma_bump_relative=bump["type"] == "relative", gamma_bump=bump["value"])
+    return kw
+
+
 def plan(case: dict) -> tuple[PlanSpec, LsmSpec]:
     """The compiled American plan and LSM configuration of one replay request."""
     times = [act365(case["valuation_date"], d) for d in case["product"]["exercise_dates"]]
@@ -36,7 +46,7 @@ def plan(case: dict) -> tuple[PlanSpec, LsmSpec]:
         reduction_block_size=case["reduction_block_size"], spot=case["spot"],
         discount_times=case["discount_curve"]["times"], discount_factors=case["discount_curve"]["discount_factors"],
         dividend_times=case["dividend_curve"]["times"], dividend_factors=case["dividend_curve"]["discount_factors"],
-        volatility=case["volatility"], **_engine_kwargs(case["valuation"]))
+        volatility=case["volatility"], **_engine_kwargs(case["valuation"]), **_risk_kwargs(case["risk"]))
     t = case["training"]
     cfg = case["lsm"]
     lsm = LsmSpec(training_seed=t["master_seed"], training_units=t["sampling_units"],

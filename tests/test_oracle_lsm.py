@@ -79,6 +79,35 @@ def test_replay_early_exercise(case):
         assert close([m.residual_sum_squares], [w["residual_sum_squares"]])
 
 
+RISK_CASES = [c for c in CASES if c["risk"].get("delta")]
+
+
+def check_risks(r, risks):
+    """Raw delta, gamma and vega estimates of a fixed-policy risk replay, to the bit."""
+    for name in ("delta", "gamma", "vega"):
+        got, want = getattr(r, name), risks[name]["raw"]
+        assert got.value == want["value"], name
+        assert got.standard_error == want["standard_error"], name
+        assert got.confidence_lower == want["confidence_lower"], name
+        assert got.confidence_upper == want["confidence_upper"], name
+        assert got.effective_sampling_units == want["effective_sampling_units"], name
+
+
+@pytest.mark.parametrize("case", RISK_CASES, ids=lambda c: c["name"])
+def test_replay_fixed_policy_risk(case):
+    """Fixed-policy delta, gamma and vega of the American put
+    (early_exercise.rs:454-600 over black_scholes.rs:358-415): the stopping
+    dates of the valuation paths held, the discounted exercise value
+    differentiated pathwise, gamma from deltas at S0 +- 1 % of spot."""
+    spec, lsm = L.plan(case)
+    buf = H.oracle_lsm(spec, lsm, stopping=True, threads=3)
+    check_risks(buf.result, case["expected"]["risks"])
+    # the price component of the risk pass re-derives the valuation price
+    comp = buf.result.risk_components[A.PRICE]
+    assert comp.sum + comp.correction == pytest.approx(
+        buf.result.price.value * buf.result.independent_sampling_units, rel=1e-13)
+
+
 def test_thread_count_does_not_change_the_result():
     spec, lsm = L.plan(CASES[0])
     a = H.oracle_lsm(spec, lsm, stopping=True, threads=1)
