@@ -1087,8 +1087,11 @@ struct LsmBuffers {
     DeviceArray<DD> partials, group_partials, sums;
     DeviceArray<unsigned int> tickets;
     DeviceArray<unsigned long long> counts, words;
+    DeviceArray<StatRecord> risk_partials, risk_records;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     ~LsmBuffers() {
+        risk_partials.release();
+        risk_records.release();
         spots.release();
         cf.release();
         df.release();
@@ -1124,10 +1127,15 @@ mcg_status validate_lsm(const mcg_plan_desc* d, const mcg_lsm_desc* l, const mcg
     if (d->abi_version != MCG_ABI_VERSION) return fail(MCG_ERR_INVALID_ARGUMENT, "abi_version mismatch");
     if (d->product_count != 1 || !d->products || d->products[0].kind != MCG_PRODUCT_AMERICAN)
         return fail(MCG_ERR_INVALID_ARGUMENT, "an early-exercise plan holds exactly one American product");
-    if (d->request_delta || d->request_gamma || d->request_vega || d->request_local_vega_nodes)
-        return fail(MCG_ERR_UNSUPPORTED, "fixed-policy early-exercise risk is not implemented");
+    if (d->request_local_vega_nodes)
+        return fail(MCG_ERR_UNSUPPORTED, "local vega nodes need a local-volatility plan");
     if (d->model != MCG_MODEL_BLACK_SCHOLES)
         return fail(MCG_ERR_UNSUPPORTED, "early exercise under local volatility is not implemented");
+    if (d->request_gamma) {
+        const double b = resolve_gamma_bump(d);
+        if (!std::isfinite(b) || b <= 0.0 || b >= d->spot)
+            return fail(MCG_ERR_INVALID_ARGUMENT, "gamma bump must lie in (0, spot)");
+    }
     if (l->continuation != MCG_CONTINUATION_POLYNOMIAL && l->continuation != MCG_CONTINUATION_MLP)
         return fail(MCG_ERR_UNSUPPORTED, "continuation kind");
     if (l->continuation == MCG_CONTINUATION_MLP &&
@@ -1163,6 +1171,9 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     mcg_plan_desc vd = *d;
     vd.products = &placeholder;
     vd.payment_time = d->observation_times[d->observation_count - 1];
+    // Risk is taken by the fixed-policy pass below, not by the path plans.
+    const bool risk = d->request_delta || d->request_gamma || d->request_vega;
+    vd.request_delta = vd.request_gamma = vd.request_vega = 0;
     mcg_plan_desc td = vd;
     td.master_seed = l->training_seed;
     td.sampling_units = l->training_units;
@@ -1207,7 +1218,7 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     MCG_CUDA(B.unit_values.alloc(v_units));
     MCG_CUDA(B.counts.alloc(dates));
     const bool want_stops = r->stopping_indices && r->stopping_capacity >= v_paths;
-    if (want_stops) MCG_CUDA(B.vstops.alloc(v_paths));
+    if (want_stops || risk) MCG_CUDA(B.vstops.alloc(v_paths));
     const uint32_t max_groups = std::max(t_groups, v_groups);
     MCG_CUDA(B.group_partials.alloc(static_cast<size_t>(max_groups) * group_ctas));
     MCG_CUDA(B.sums.alloc(4 * static_cast<size_t>(max_groups)));  // in-sample, valuation, squares, network in-sample
@@ -1406,7 +1417,7 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     V.strike = A.strike;
     V.notional = A.notional;
     V.unit_values = B.unit_values.ptr;
-    V.stops = want_stops ? B.vstops.ptr : nullptr;
+    V.stops = want_stops || risk ? B.vstops.ptr : nullptr;
     V.counts = B.counts.ptr;
     if (use_mlp) {
         MCG_CUDA(launch_lsm_bs_value_mlp(VP, V, B.mlp_snapshots.ptr, 1.0 / d->observation_times[last], stream));
@@ -1420,6 +1431,29 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     if (!rqmc) {
         MCG_CUDA(launch_lsm_group_sum(B.unit_values.ptr, VP.units, 1, 0, B.means.ptr, B.group_partials.ptr,
                                       group_ctas, s_sq, nullptr, stream));
+        launches += 2;
+    }
+    // Fixed-policy risk: the valuation stopping dates held, per-tile records
+    // of the pathwise components merged per scramble.
+    const uint32_t risk_tiles = lsm_risk_tiles(VP.units);
+    if (risk) {
+        MCG_CUDA(B.risk_partials.alloc(static_cast<size_t>(v_groups) * risk_tiles * kComponents));
+        MCG_CUDA(B.risk_records.alloc(static_cast<size_t>(v_groups) * kComponents));
+        LsmRiskArgs R{};
+        R.df = B.df.ptr;
+        R.stops = B.vstops.ptr;
+        R.side = A.side;
+        R.strike = A.strike;
+        R.notional = A.notional;
+        R.gamma = d->request_gamma ? 1 : 0;
+        R.gamma_bump = resolve_gamma_bump(d);
+        // validation bumps, crates/pricing/src/engine/compile/simulation.rs:481-502
+        R.spot_bump = d->request_gamma ? R.gamma_bump : std::min(d->spot * 1.0e-4, 0.5 * d->spot);
+        R.vol_bump = d->volatility == 0.0 ? 0.0 : std::min(1.0e-4, d->volatility * 0.5);
+        MCG_CUDA(launch_lsm_bs_risk(VP, R, B.risk_partials.ptr, stream));
+        reduce_tiles_kernel<<<dim3(kComponents, v_groups), 256, 0, stream>>>(B.risk_partials.ptr, risk_tiles,
+                                                                            kComponents, B.risk_records.ptr);
+        MCG_CUDA(cudaGetLastError());
         launches += 2;
     }
     MCG_CUDA(cudaEventRecord(B.ev[3], stream));
@@ -1436,6 +1470,10 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
                                  cudaMemcpyDeviceToHost, stream));
     if (want_stops)
         MCG_CUDA(cudaMemcpyAsync(r->stopping_indices, B.vstops.ptr, v_paths * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, stream));
+    std::vector<StatRecord> risk_rec(risk ? static_cast<size_t>(v_groups) * kComponents : 0);
+    if (risk)
+        MCG_CUDA(cudaMemcpyAsync(risk_rec.data(), B.risk_records.ptr, risk_rec.size() * sizeof(StatRecord),
                                  cudaMemcpyDeviceToHost, stream));
     MCG_CUDA(cudaStreamSynchronize(stream));
     if (words[0] != ~0ull) {
@@ -1488,6 +1526,36 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     r->independent_sampling_units = independent;
     r->date_count = dates;
     r->kernel_launches = launches;
+    // Fixed-policy Greeks: pseudo statistics over sampling units, RQMC over
+    // the per-scramble replicate means (early_exercise.rs:454-600).
+    std::memset(r->risk_components, 0, sizeof(r->risk_components));
+    r->delta = r->gamma = r->vega = mcg_estimate{};
+    r->bump_delta = r->bump_gamma = r->bump_vega = mcg_estimate{};
+    if (risk) {
+        HostStat rs[kComponents];
+        for (int c = 0; c < kComponents; ++c) {
+            if (c >= 10) {
+                rs[c].count = independent;
+            } else if (!rqmc) {
+                const StatRecord& x = risk_rec[c];
+                rs[c] = {x.sum, x.corr, static_cast<uint64_t>(x.count), x.mean, x.m2};
+            } else {
+                std::vector<double> reps(v_groups);
+                for (uint32_t g = 0; g < v_groups; ++g) {
+                    const StatRecord& x = risk_rec[static_cast<size_t>(g) * kComponents + c];
+                    reps[g] = (x.sum + x.corr) / static_cast<double>(VP.units);
+                }
+                rs[c] = two_pass(reps);
+            }
+            r->risk_components[c] = {rs[c].sum, rs[c].corr, rs[c].count, rs[c].mean, rs[c].m2};
+        }
+        r->delta = make_estimate(rs[MCG_DELTA], independent, 1.0);
+        r->gamma = make_estimate(rs[MCG_GAMMA], independent, 1.0);
+        r->vega = make_estimate(rs[MCG_VEGA], independent, 1.0);
+        r->bump_delta = make_estimate(rs[MCG_BUMP_DELTA], independent, 1.0);
+        r->bump_gamma = make_estimate(rs[MCG_BUMP_GAMMA], independent, 1.0);
+        r->bump_vega = make_estimate(rs[MCG_BUMP_VEGA], independent, 1.0);
+    }
     return MCG_OK;
 }
 

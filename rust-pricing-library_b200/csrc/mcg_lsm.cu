@@ -779,6 +779,128 @@ __global__ void __launch_bounds__(kLsmThreads) lsm_bs_value_kernel(const DeviceP
         if (s_counts[i]) atomicAdd(&V.counts[i], static_cast<unsigned long long>(s_counts[i]));
 }
 
+// ------------------------------------------------------------ fixed-policy risk
+
+// Price, AAD delta and AAD vega of one path's exercise cash flow at stopping
+// date k under (spot, vol): pathwise_aad_for_output
+// (crates/pricing/src/engine/processes/black_scholes.rs:567-643) for the
+// American payoff graph's output k, observation k of
+// path_observations_from_normals (:297-331).  `w` is the path's Brownian
+// value at t_k, `z` its first normal (single-date plans take the exact
+// terminal step sqrt(sigma^2 t) z).
+struct ExerciseAad {
+    double price, delta, vega;
+};
+
+__device__ __forceinline__ ExerciseAad exercise_aad(const DevicePlan& P, const LsmRiskArgs& R, uint32_t k,
+                                                    double w, double z, double spot, double vol) {
+    const double t = P.obs_time[k];
+    const double tv = vol * vol * t;
+    const double lr = P.observation_count == 1 ? -0.5 * tv + sqrt(tv) * z : -0.5 * tv + vol * w;
+    const double f = P.obs_fwd[k] * (spot / P.spot) * exp(lr);
+    const double s = 0.0 * spot + 1.0 * f;
+    const bool call = R.side == MCG_CALL;
+    const double in = call ? s - R.strike : R.strike - s;
+    const double value = (in >= 0.0 ? in : 0.0) * R.notional;
+    const double adj = (in >= 0.0 ? R.notional : 0.0) * (call ? 1.0 : -1.0);
+    double delta = 0.0, vega = 0.0;
+    if (adj != 0.0) {
+        delta += adj * 1.0 * f / spot;
+        vega += adj * 1.0 * f * (-vol * t + w);
+    }
+    const double df = R.df[k];
+    return {df * value, df * delta, df * vega};
+}
+
+// The ten pathwise components of fixed_policy_pathwise_values
+// (black_scholes.rs:358-415): base price/delta/vega, gamma from the AAD deltas
+// at spot +- gamma_bump, bumped delta/gamma from prices at spot +- spot_bump,
+// bumped vega from prices at vol +- vol_bump, and the differences.
+__device__ __forceinline__ void fixed_policy_values(const DevicePlan& P, const LsmRiskArgs& R, uint32_t k,
+                                                    double w, double z, double (&v)[kComponents]) {
+    const double S = P.spot, vol = P.vol;
+    const ExerciseAad base = exercise_aad(P, R, k, w, z, S, vol);
+    double gamma = 0.0;
+    if (R.gamma) {
+        const double b = R.gamma_bump;
+        const double dd = exercise_aad(P, R, k, w, z, S - b, vol).delta;
+        const double du = exercise_aad(P, R, k, w, z, S + b, vol).delta;
+        gamma = (du - dd) / (2.0 * b);
+    }
+    const double sb = R.spot_bump;
+    const double pd = exercise_aad(P, R, k, w, z, S - sb, vol).price;
+    const double pu = exercise_aad(P, R, k, w, z, S + sb, vol).price;
+    const double bump_delta = (pu - pd) / (2.0 * sb);
+    const double bump_gamma = (pu - 2.0 * base.price + pd) / (sb * sb);
+    double bump_vega = 0.0;
+    if (R.vol_bump != 0.0) {
+        const double vb = R.vol_bump;
+        const double lo = exercise_aad(P, R, k, w, z, S, vol - vb).price;
+        const double hi = exercise_aad(P, R, k, w, z, S, vol + vb).price;
+        bump_vega = (hi - lo) / (2.0 * vb);
+    }
+#pragma unroll
+    for (int c = 0; c < kComponents; ++c) v[c] = 0.0;
+    v[MCG_PRICE] = base.price;
+    v[MCG_DELTA] = base.delta;
+    v[MCG_VEGA] = base.vega;
+    v[MCG_GAMMA] = gamma;
+    v[MCG_BUMP_DELTA] = bump_delta;
+    v[MCG_DELTA_DIFFERENCE] = bump_delta - base.delta;
+    v[MCG_BUMP_VEGA] = bump_vega;
+    v[MCG_VEGA_DIFFERENCE] = bump_vega - base.vega;
+    v[MCG_BUMP_GAMMA] = bump_gamma;
+    v[MCG_GAMMA_DIFFERENCE] = bump_gamma - gamma;
+}
+
+// One thread per sampling unit: regenerate the unit's normals up to the later
+// stopping date of its (antithetic) paths, evaluate the components of each
+// path at its own stopping date, average the pair, reduce per 128-unit tile
+// (constant_vol_fixed_policy_pseudo/rqmc_statistics,
+// crates/pricing/src/engine/mc/early_exercise.rs:454-600).
+__global__ void __launch_bounds__(kThreads) lsm_bs_risk_kernel(const DevicePlan P, const LsmRiskArgs R,
+                                                               StatRecord* partials) {
+    __shared__ Stat s_red[4 * kComponents];
+    const uint32_t scramble = blockIdx.y;
+    const uint64_t point = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    const bool valid = point < P.units;
+    const uint64_t unit = valid ? point : 0;
+    NormalSource ns;
+    ns.rqmc = P.engine == MCG_ENGINE_RQMC;
+    ns.seed = P.seed;
+    ns.unit = unit;
+    ns.gray = static_cast<uint32_t>(unit ^ (unit >> 1));
+    ns.dirs = P.scr_dirs ? P.scr_dirs + static_cast<size_t>(scramble) * P.dimension * 32u : nullptr;
+    ns.shift = P.scr_shift ? P.scr_shift + static_cast<size_t>(scramble) * P.dimension : nullptr;
+    ns.cached_block = 0xffffffffu;
+    ns.domain = 0;
+    const int pairs = P.antithetic ? 2 : 1;
+    const uint32_t n = P.observation_count;
+    const uint64_t base = (static_cast<uint64_t>(scramble) * P.units + unit) * pairs;
+    uint32_t k[2] = {min(R.stops[base], n - 1), pairs == 2 ? min(R.stops[base + 1], n - 1) : 0u};
+    const uint32_t last = max(k[0], k[1]);
+    double w[2] = {0.0, 0.0}, wk[2] = {0.0, 0.0}, z0 = 0.0;
+    for (uint32_t i = 0; i <= last; ++i) {
+        const double z = P.zero_variance ? 0.0 : ns.normal(i);
+        if (i == 0) z0 = z;
+        for (int e = 0; e < pairs; ++e) {
+            const double ze = e == 0 ? z : -z;
+            w[e] += P.obs_sqrt_step[i] * ze;
+            if (i == k[e]) wk[e] = w[e];
+        }
+    }
+    double vals[kComponents];
+    fixed_policy_values(P, R, k[0], wk[0], z0, vals);
+    if (pairs == 2) {
+        double mate[kComponents];
+        fixed_policy_values(P, R, k[1], wk[1], -z0, mate);
+#pragma unroll
+        for (int c = 0; c < kComponents; ++c) vals[c] = (vals[c] + mate[c]) * 0.5;
+    }
+    StatRecord* out = partials + (static_cast<size_t>(scramble) * gridDim.x + blockIdx.x) * kComponents;
+    cta_reduce_write<kComponents>(vals, valid, 0x3ffu, out, s_red);
+}
+
 // ----------------------------------------------------------------- reductions
 
 // Sum of per-unit values of each group (blockIdx.y): the value itself, the
@@ -869,6 +991,15 @@ cudaError_t launch_lsm_group_sum(const double* values, uint64_t per_group, uint3
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     lsm_group_finish_kernel<<<groups, 32, 0, stream>>>(partials, ctas, per_group, out, means);
+    return cudaGetLastError();
+}
+
+uint32_t lsm_risk_tiles(uint64_t units) { return static_cast<uint32_t>((units + kThreads - 1) / kThreads); }
+
+cudaError_t launch_lsm_bs_risk(const DevicePlan& P, const LsmRiskArgs& R, StatRecord* partials,
+                               cudaStream_t stream) {
+    const dim3 grid(lsm_risk_tiles(P.units), P.scramble_count);
+    lsm_bs_risk_kernel<<<grid, kThreads, 0, stream>>>(P, R, partials);
     return cudaGetLastError();
 }
 

@@ -45,6 +45,17 @@ struct LsmValueArgs {
     unsigned long long* counts;        // [dates]
 };
 
+// Fixed-policy risk of the valuation paths (Black--Scholes): the stopping
+// date of every path held, the discounted exercise value differentiated.
+struct LsmRiskArgs {
+    const double* df;        // [dates]
+    const uint32_t* stops;   // [paths] valuation stopping dates
+    int32_t side;
+    double strike, notional;
+    int gamma;               // gamma requested: AAD deltas at spot +- gamma_bump
+    double gamma_bump, spot_bump, vol_bump;
+};
+
 cudaError_t launch_lsm_bs_spots(const DevicePlan& P, uint32_t domain, double* spots, uint64_t paths,
                                 unsigned long long* bad, cudaStream_t stream);
 cudaError_t launch_lsm_init(const LsmArgs& A, unsigned ctas, cudaStream_t stream);
@@ -53,6 +64,10 @@ cudaError_t launch_lsm_bs_value(const DevicePlan& P, const LsmValueArgs& V, cuda
 cudaError_t launch_lsm_group_sum(const double* values, uint64_t per_group, uint32_t groups, int pairs,
                                  const double* centers, DD* partials, unsigned ctas, DD* out, double* means,
                                  cudaStream_t stream);
+// Per-CTA statistics records [scramble][tile][MCG_PATHWISE_COMPONENTS] of the
+// fixed-policy risk components; `tiles` = lsm_risk_tiles(units).
+cudaError_t launch_lsm_bs_risk(const DevicePlan& P, const LsmRiskArgs& R, StatRecord* partials, cudaStream_t stream);
+uint32_t lsm_risk_tiles(uint64_t units);
 size_t lsm_partial_stride();
 
 }  // namespace mcg

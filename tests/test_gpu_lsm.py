@@ -14,6 +14,7 @@ The replay fixture's own values are checked as well.
 import numpy as np
 import pytest
 
+import gpu_common as G
 import helpers as H
 import lsm_cases as L
 from rust_pricing_b200 import _abi as A
@@ -70,11 +71,51 @@ def assert_same_result(spec, lsm, got, want, stops=True):
     assert_models(spec, lsm, got, want)
 
 
+def bump_noise(spec, price):
+    """Rounding floor of the validation bumps: last-ulp differences of the
+    bumped prices (a few eps |price|) divided by the bump (second differences
+    by its square).  A bumped gamma of a path that is linear in the spot is
+    pure rounding noise at this level."""
+    sb = (spec.gamma_bump * spec.spot if spec.gamma_bump_relative else spec.gamma_bump) \
+        if spec.request_gamma else min(spec.spot * 1e-4, 0.5 * spec.spot)
+    vb = min(1e-4, 0.5 * spec.volatility)
+    u = 1e3 * 2.220446049250313e-16 * abs(price)
+    return {"bump_delta": u / sb, "bump_gamma": u / sb ** 2, "bump_vega": u / vb,
+            A.BUMP_DELTA: u / sb, A.DELTA_DIFFERENCE: u / sb, A.BUMP_GAMMA: u / sb ** 2,
+            A.GAMMA_DIFFERENCE: u / sb ** 2, A.BUMP_VEGA: u / vb, A.VEGA_DIFFERENCE: u / vb}
+
+
+def assert_same_risk(spec, got, want):
+    """Fixed-policy Greeks against the oracle with the parity tolerances of
+    the European engine: direct estimates (AAD delta/vega, gamma from AAD
+    deltas) 1e-12, the validation bumps 1e-8 (they divide last-ulp libm
+    differences by the bump), both on the scale max(|total|, spread), the
+    bumps above their rounding floor."""
+    g, w = got.result, want.result
+    noise = bump_noise(spec, w.price.value)
+    for name, bump in (("delta", 0), ("gamma", 0), ("vega", 0), ("bump_delta", 1), ("bump_gamma", 1),
+                       ("bump_vega", 1)):
+        a, b = getattr(g, name), getattr(w, name)
+        tol = G.BUMP_TOL if bump else G.DIRECT_TOL
+        assert abs(a.value - b.value) <= tol * max(abs(b.value), b.standard_error, 1e-300) + noise.get(name, 0.0), (
+            name, a.value, b.value)
+        assert abs(a.standard_error - b.standard_error) <= (1e-6 if bump else 1e-9) * max(
+            b.standard_error, 1e-300) + noise.get(name, 0.0), name
+        assert a.effective_sampling_units == b.effective_sampling_units, name
+    for c in range(10):
+        a, b = g.risk_components[c], w.risk_components[c]
+        assert a.count == b.count, c
+        scale = G._scale(b)
+        if c in G.DIFFERENCE_OF:
+            scale = max(scale, G._scale(w.risk_components[G.DIFFERENCE_OF[c]]))
+        tol = G.BUMP_TOL if c in G.BUMP_COMPONENTS else G.DIRECT_TOL
+        floor = noise.get(c, 0.0) * b.count
+        assert abs(a.total() - b.total()) <= tol * max(scale, 1e-300) + floor, (c, a.total(), b.total())
+
+
 @pytest.mark.parametrize("case", L.cases(), ids=lambda c: c["name"])
 def test_replay_fixture_on_the_gpu(engine, case):
     spec, lsm = L.plan(case)
-    if case["risk"].get("delta"):
-        pytest.skip("fixed-policy risk is priced by the oracle only")
     got = N.lsm_price(spec, lsm, stopping=True)
     want = H.oracle_lsm(spec, lsm, stopping=True, threads=4)
     assert_same_result(spec, lsm, got, want)
@@ -83,6 +124,12 @@ def test_replay_fixture_on_the_gpu(engine, case):
     assert list(got.counts[:len(spec.observation_times)]) == e["exercise_counts"]
     assert rel(got.result.price.value, e["value"]["value"]) <= PRICE_TOL
     assert rel(got.result.in_sample_value, e["in_sample_value"]) <= PRICE_TOL
+    if case["risk"].get("delta"):
+        assert_same_risk(spec, got, want)
+        for name in ("delta", "gamma", "vega"):
+            a, b = getattr(got.result, name), e["risks"][name]["raw"]
+            assert abs(a.value - b["value"]) <= G.DIRECT_TOL * max(abs(b["value"]), b["standard_error"]), name
+            assert rel(a.standard_error, b["standard_error"]) <= 1e-9, name
 
 
 CASES = {
@@ -130,12 +177,71 @@ def test_matrix_limit_is_an_lsm_error(engine):
     assert err.value.name == "lsm"
 
 
+RISK_CASES = {
+    "pseudo-antithetic-odd-units": lambda: W.american_bs(dates=7, units=5001, training_units=3001,
+                                                         antithetic=True),
+    "rqmc-antithetic": lambda: W.american_bs(dates=10, units=1 << 10, engine=A.ENGINE_RQMC, antithetic=True,
+                                             scrambles=4),
+    "call-12-dates": lambda: W.american_bs(dates=12, units=1 << 13, side=A.CALL, strike=95.0),
+    "one-date": lambda: W.american_bs(dates=1, units=1 << 12),
+}
+
+
+@pytest.mark.parametrize("gamma", [True, False], ids=["gamma", "delta-vega"])
+@pytest.mark.parametrize("name", sorted(RISK_CASES))
+def test_fixed_policy_risk_matches_the_oracle(engine, name, gamma):
+    spec, lsm = RISK_CASES[name]()
+    spec.request_delta = spec.request_vega = True
+    spec.request_gamma = gamma
+    got = N.lsm_price(spec, lsm, stopping=True)
+    want = H.oracle_lsm(spec, lsm, stopping=True, threads=8)
+    assert_same_result(spec, lsm, got, want)
+    assert_same_risk(spec, got, want)
+    # the price component re-derives the valuation price under the fixed policy
+    p = got.result.risk_components[A.PRICE]
+    assert rel((p.sum + p.correction) / got.result.independent_sampling_units, got.result.price.value) <= 1e-12
+
+
+def test_one_date_risk_equals_the_european_engine(engine):
+    """With one exercise date the stopping policy is 'at expiry' and the
+    fixed-policy Greeks are the European pathwise ones."""
+    spec, lsm = W.american_bs(dates=1, units=1 << 14)
+    spec.request_delta = spec.request_gamma = spec.request_vega = True
+    got = N.lsm_price(spec, lsm)
+    eu = W.american_bs(dates=1, units=1 << 14)[0]
+    eu.products[0].kind = A.PRODUCT_EUROPEAN
+    eu.request_delta = eu.request_gamma = eu.request_vega = True
+    with N.Plan(eu) as plan:
+        ref = plan.evaluate().products[0]
+    for name in ("delta", "gamma", "vega", "bump_delta", "bump_gamma", "bump_vega"):
+        a, b = getattr(got.result, name), getattr(ref, name)
+        assert abs(a.value - b.value) <= 1e-12 * max(abs(b.value), b.standard_error), name
+
+
+def test_learned_policy_has_fixed_policy_risk(engine):
+    spec, lsm = W.american_bs(dates=6, units=1 << 13)
+    spec.request_delta = spec.request_vega = True
+    lsm.continuation = A.CONTINUATION_MLP
+    got = N.lsm_price(spec, lsm)
+    r = got.result
+    p = r.risk_components[A.PRICE]
+    assert rel((p.sum + p.correction) / r.independent_sampling_units, r.price.value) <= 1e-12
+    # an American put: delta in (-1, 0), vega positive
+    assert -1.0 < r.delta.value < 0.0 and r.vega.value > 0.0
+
+
 def test_rejects_what_it_does_not_price(engine):
     spec, lsm = W.american_bs(dates=4, units=1 << 10)
-    spec.request_delta = True
+    spec.request_local_vega_nodes = True
     with pytest.raises(N.EngineError) as err:
         N.lsm_price(spec, lsm)
     assert err.value.name == "unsupported"
+    spec, lsm = W.american_bs(dates=4, units=1 << 10)
+    spec.request_gamma = True
+    spec.gamma_bump_relative, spec.gamma_bump = False, spec.spot
+    with pytest.raises(N.EngineError) as err:
+        N.lsm_price(spec, lsm)
+    assert err.value.name == "invalid_argument"
     spec, lsm = W.american_bs(dates=4, units=1 << 10)
     spec.products[0].kind = A.PRODUCT_EUROPEAN
     with pytest.raises(N.EngineError) as err:
