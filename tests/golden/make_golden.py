@@ -9,6 +9,10 @@ are committed; the tests only read them.
 * bs_analytical.json       -- fixtures/acceptance/european_bs_analytical.csv.
 * path_dependence.json     -- fixtures/path-dependence/reference-cases-v0.1.json
   (smoothing, extrema, exact and smoothed bridge cases; decimal strings).
+* replay_local_vol.json    -- fixtures/replay/local_volatility-{windows-x86_64,macos-aarch64}.json:
+  the 3 x 5 local-variance grid requests (pseudo and RQMC, price-only and
+  Delta/Gamma/Vega) with both platforms' values, standard errors and
+  variance bits.
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
   the American put requests (pseudo and RQMC, training and valuation engines,
   LSM configuration) with the fitted decision models, exercise counts,
@@ -66,6 +70,50 @@ def replay():
         cases.append(case)
     json.dump({"source": "fixtures/replay/european_bs-windows-x86_64.json", "cases": cases},
               open(os.path.join(OUT, "replay_european_bs.json"), "w"), indent=1)
+
+
+def _estimate(e):
+    return {k: e[k] for k in ("value", "standard_error", "confidence_lower", "confidence_upper",
+                              "effective_sampling_units")}
+
+
+def local_volatility():
+    platforms = {p: json.load(open(os.path.join(REF, f"fixtures/replay/local_volatility-{p}.json")))
+                 for p in ("windows-x86_64", "macos-aarch64")}
+    cases = []
+    for i, c in enumerate(platforms["windows-x86_64"]["cases"]):
+        req = c["request"]
+        grid = req["model"]["local_variance_grid"]
+        case = {
+            "name": c["name"],
+            **_engine(req["engine"]),
+            "reduction_block_size": c["execution"]["monte_carlo"]["reduction_block_size"],
+            "spot": req["market"]["spot"],
+            "discount_curve": req["market"]["discount_curve"],
+            "dividend_curve": req["market"]["dividend_curve"],
+            "local_variance_grid": {k: grid[k] for k in ("time_nodes", "log_forward_moneyness_nodes", "values",
+                                                         "floor", "cap")},
+            "valuation_date": req["valuation_date"],
+            "product": {k: req["product"][k] for k in ("expiry", "notional", "strike")},
+            "side": req["product"]["side"]["type"],
+            "risk": {k: req["risk"][k] for k in ("delta", "gamma", "vega") if k in req["risk"]},
+            "expected": {},
+        }
+        for name, d in platforms.items():
+            pc = d["cases"][i]
+            assert pc["name"] == c["name"]
+            res = pc["result"]
+            case["expected"][name] = {
+                "value": _estimate(res["value"]),
+                "sampling_variance_bits": pc["execution"]["sampling_variance_bits"],
+                "estimator_variance_bits": pc["execution"]["estimator_variance_bits"],
+                "evaluated_paths": int(pc["execution"]["evaluated_paths"]),
+                "risks": {k: _estimate(res["risks"][k]["raw"]) for k in ("delta", "gamma", "vega")
+                          if k in res["risks"]},
+            }
+        cases.append(case)
+    json.dump({"source": "fixtures/replay/local_volatility-{windows-x86_64,macos-aarch64}.json", "cases": cases},
+              open(os.path.join(OUT, "replay_local_vol.json"), "w"), indent=1)
 
 
 def analytical():
@@ -156,4 +204,5 @@ if __name__ == "__main__":
     analytical()
     path_dependence()
     early_exercise()
+    local_volatility()
     print("golden fixtures written to", OUT)

@@ -12,6 +12,7 @@ import math
 import pytest
 
 import helpers as H
+import lv_cases as L
 import gpu_common as G
 from bs_closed_form import black_scholes
 from rust_pricing_b200 import _abi as A
@@ -30,6 +31,22 @@ def test_replay_against_reference_values(engine, case):
     for est, key in ((p.price, "price"), (p.delta, "delta"), (p.gamma, "gamma"), (p.vega, "vega")):
         assert abs(est.value - e[key]) <= 1e-12 * abs(e[key]), key
         assert abs(est.standard_error - e[key + "_standard_error"]) <= 1e-9 * e[key + "_standard_error"]
+    G.assert_parity(spec, engine_buf=buf)
+
+
+@pytest.mark.parametrize("case", L.cases(), ids=lambda c: c["name"])
+def test_local_vol_replay_against_reference_values(engine, case):
+    """The 3 x 5 local-variance grid requests of the reference's replay fixture
+    (pseudo 8192 antithetic units; RQMC 512 x 8, bridge): price, CRN Delta and
+    Gamma, reverse-sweep Vega within 1e-12 of the reference's values."""
+    spec = L.plan(case)
+    buf = G.run_engine(spec)
+    p = buf.products[0]
+    e = case["expected"]["windows-x86_64"]
+    ests = [("price", p.price, e["value"])] + [(k, getattr(p, k), v) for k, v in e["risks"].items()]
+    for name, est, want in ests:
+        assert abs(est.value - want["value"]) <= G.DIRECT_TOL * max(abs(want["value"]), want["standard_error"]), name
+        assert abs(est.standard_error - want["standard_error"]) <= 1e-9 * want["standard_error"], name
     G.assert_parity(spec, engine_buf=buf)
 
 

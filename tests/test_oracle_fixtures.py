@@ -6,6 +6,9 @@
 * Path dependence: compact-C2 smoothing, smooth extrema and the exact and
   smoothed bridge survival match the independent high-precision cases of
   fixtures/path-dependence/reference-cases-v0.1.json.
+* Local volatility: the pseudo-MC and RQMC cases of
+  fixtures/replay/local_volatility-*.json (3 x 5 grid, price-only and
+  Delta/Gamma/Vega) reproduce price, standard error and variance bits.
 * Analytic: the closed-form judge reproduces fixtures/acceptance/european_bs_analytical.csv.
 """
 import ctypes as C
@@ -18,6 +21,7 @@ import numpy as np
 import pytest
 
 import helpers as H
+import lv_cases as L
 from bs_closed_form import black_scholes
 from rust_pricing_b200 import _abi as A
 from rust_pricing_b200.desc import PlanSpec, ProductSpec
@@ -69,6 +73,49 @@ def test_replay_european_bs(case):
                      ("bump_vega_value_bits", p.bump_vega)):
         expected = struct.unpack(">d", bytes.fromhex(e[key]))[0]
         assert abs(est.value - expected) <= 1e-9 * abs(expected)
+
+
+LV_CASES = L.cases()
+
+
+def ulps(a: float, b: float) -> int:
+    """Distance in units in the last place between two finite doubles of one sign."""
+    ia, ib = (struct.unpack(">q", struct.pack(">d", x))[0] for x in (a, b))
+    return abs(ia - ib)
+
+
+def nearest_ulps(got: float, wants) -> int:
+    return min(ulps(got, w) for w in wants)
+
+
+@pytest.mark.parametrize("case", LV_CASES, ids=lambda c: c["name"])
+def test_replay_local_volatility(case):
+    """Log-Euler local volatility against both platforms' fixtures.  The price
+    and the Delta/Vega values equal a platform's to the last bit; standard
+    errors and variances are within 2 ulps and Gamma within 4 ulps of the
+    nearer platform, or inside the two platforms' own spread where that is
+    wider (their libm exp/log differ in the last bit of some paths; the RQMC
+    Gamma standard error of the two fixtures differs by 250 ulps)."""
+    r = H.oracle_evaluate(L.plan(case), threads=4)
+    p = r.products[0]
+    plats = list(case["expected"].values())
+    assert r.result.evaluated_paths == plats[0]["evaluated_paths"]
+    assert nearest_ulps(p.price.value, [e["value"]["value"] for e in plats]) == 0
+    for f in ("standard_error", "confidence_lower", "confidence_upper"):
+        assert nearest_ulps(getattr(p.price, f), [e["value"][f] for e in plats]) <= 2, f
+    assert p.price.effective_sampling_units == plats[0]["value"]["effective_sampling_units"]
+    for name, key in (("sampling_variance", "sampling_variance_bits"),
+                      ("estimator_variance", "estimator_variance_bits")):
+        want = [struct.unpack(">d", bytes.fromhex(e[key]))[0] for e in plats]
+        assert nearest_ulps(getattr(p, name), want) <= 2, name
+    for name in plats[0]["risks"]:
+        got = getattr(p, name)
+        assert nearest_ulps(got.value, [e["risks"][name]["value"] for e in plats]) <= (4 if name == "gamma" else 0), name
+        ses = [e["risks"][name]["standard_error"] for e in plats]
+        spread = max(ses) - min(ses)  # 250 ulps for the RQMC Gamma (8 scramble means)
+        assert nearest_ulps(got.standard_error, ses) <= 2 or \
+            min(ses) - spread <= got.standard_error <= max(ses) + spread, name
+        assert got.effective_sampling_units == plats[0]["risks"][name]["effective_sampling_units"]
 
 
 def test_replay_independent_of_thread_count():
