@@ -580,6 +580,9 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         if (risk && single) plan.mask = 0x3ffu;
         if (has_continuous) plan.mask |= 0xffu << 10;
     } else {
+        // exercise-date times, for the early-exercise engine's network inputs
+        MCG_CUDA(plan.obs_time.upload(std::vector<double>(d->observation_times, d->observation_times + n)));
+        P.obs_time = plan.obs_time.ptr;
         plan.adjoint = d->request_vega || d->request_local_vega_nodes;
         plan.adjoint_nodes = d->request_local_vega_nodes != 0;
         plan.adjoint_gamma = plan.adjoint && d->request_delta && d->request_gamma;
@@ -1088,8 +1091,12 @@ struct LsmBuffers {
     DeviceArray<unsigned int> tickets;
     DeviceArray<unsigned long long> counts, words;
     DeviceArray<StatRecord> risk_partials, risk_records;
+    DeviceArray<double> vspots;      // local volatility: valuation path store (when the training one is too small)
+    DeviceArray<ErrorWord> path_errors;  // local volatility: [0] training, [1] valuation
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     ~LsmBuffers() {
+        vspots.release();
+        path_errors.release();
         risk_partials.release();
         risk_records.release();
         spots.release();
@@ -1129,8 +1136,11 @@ mcg_status validate_lsm(const mcg_plan_desc* d, const mcg_lsm_desc* l, const mcg
         return fail(MCG_ERR_INVALID_ARGUMENT, "an early-exercise plan holds exactly one American product");
     if (d->request_local_vega_nodes)
         return fail(MCG_ERR_UNSUPPORTED, "local vega nodes need a local-volatility plan");
-    if (d->model != MCG_MODEL_BLACK_SCHOLES)
-        return fail(MCG_ERR_UNSUPPORTED, "early exercise under local volatility is not implemented");
+    if (d->model != MCG_MODEL_BLACK_SCHOLES && d->model != MCG_MODEL_LOCAL_VOLATILITY)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "model");
+    if (d->model == MCG_MODEL_LOCAL_VOLATILITY && (d->request_delta || d->request_gamma || d->request_vega))
+        return fail(MCG_ERR_UNSUPPORTED,
+                    "fixed-policy risk under local volatility needs VegaKT reporting, which is not built");
     if (d->request_gamma) {
         const double b = resolve_gamma_bump(d);
         if (!std::isfinite(b) || b <= 0.0 || b >= d->spot)
@@ -1232,7 +1242,15 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
 
     // Training: path matrix, then the backward induction.
     MCG_CUDA(cudaEventRecord(B.ev[0], stream));
-    MCG_CUDA(launch_lsm_bs_spots(TP, /*LsmTrain*/ 1u, B.spots.ptr, t_paths, &B.words.ptr[0], stream));
+    const bool lv = d->model == MCG_MODEL_LOCAL_VOLATILITY;
+    if (lv) {
+        const ErrorWord init[2] = {{~0ull, 0, 0, 0, 0}, {~0ull, 0, 0, 0, 0}};
+        MCG_CUDA(B.path_errors.alloc(2));
+        MCG_CUDA(cudaMemcpyAsync(B.path_errors.ptr, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        MCG_CUDA(launch_lsm_lv_spots(TP, /*LsmTrain*/ 1u, B.spots.ptr, t_paths, &B.path_errors.ptr[0], stream));
+    } else {
+        MCG_CUDA(launch_lsm_bs_spots(TP, /*LsmTrain*/ 1u, B.spots.ptr, t_paths, &B.words.ptr[0], stream));
+    }
     ++launches;
     MCG_CUDA(cudaEventRecord(B.ev[1], stream));
     LsmArgs A{};
@@ -1419,6 +1437,19 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     V.unit_values = B.unit_values.ptr;
     V.stops = want_stops || risk ? B.vstops.ptr : nullptr;
     V.counts = B.counts.ptr;
+    if (lv) {
+        // Local volatility stores the valuation paths too (the training store
+        // is free once the policy is fitted), then applies the policy to them.
+        double* vs = B.spots.ptr;
+        if (v_paths > t_paths) {
+            MCG_CUDA(B.vspots.alloc(static_cast<size_t>(dates) * v_paths));
+            vs = B.vspots.ptr;
+        }
+        MCG_CUDA(launch_lsm_lv_spots(VP, /*Valuation*/ 0u, vs, v_paths, &B.path_errors.ptr[1], stream));
+        ++launches;
+        V.spots = vs;
+        V.paths = v_paths;
+    }
     if (use_mlp) {
         MCG_CUDA(launch_lsm_bs_value_mlp(VP, V, B.mlp_snapshots.ptr, 1.0 / d->observation_times[last], stream));
     } else {
@@ -1475,7 +1506,20 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     if (risk)
         MCG_CUDA(cudaMemcpyAsync(risk_rec.data(), B.risk_records.ptr, risk_rec.size() * sizeof(StatRecord),
                                  cudaMemcpyDeviceToHost, stream));
+    ErrorWord path_errors[2] = {{~0ull, 0, 0, 0, 0}, {~0ull, 0, 0, 0, 0}};
+    if (lv)
+        MCG_CUDA(cudaMemcpyAsync(path_errors, B.path_errors.ptr, sizeof(path_errors), cudaMemcpyDeviceToHost,
+                                 stream));
     MCG_CUDA(cudaStreamSynchronize(stream));
+    for (int k = 0; k < 2; ++k)
+        if (path_errors[k].key != ~0ull) {
+            // LocalVolError::NonFiniteState of the Log-Euler step (local_vol.rs:24-73)
+            r->error.code = static_cast<int32_t>(path_errors[k].key & 0xff);
+            r->error.sampling_unit = path_errors[k].key >> 8;
+            return fail(static_cast<mcg_status>(r->error.code),
+                        std::string(k ? "valuation" : "training") + " path of sampling unit " +
+                            std::to_string(r->error.sampling_unit) + " left the positive finite states");
+        }
     if (words[0] != ~0ull) {
         r->error.code = MCG_ERR_LSM;
         r->error.sampling_unit = words[0];

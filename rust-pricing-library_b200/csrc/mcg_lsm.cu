@@ -740,14 +740,17 @@ __global__ void __launch_bounds__(kLsmThreads) lsm_bs_value_kernel(const DeviceP
         double realized[2] = {0.0, 0.0};
         uint32_t stop[2] = {n - 1, n - 1};
         bool open[2] = {true, pairs == 2};
+        const double* row = V.spots ? V.spots + unit * pairs : nullptr;
         for (uint32_t i = 0; i < n && (open[0] || open[1]); ++i) {
-            const double z = P.zero_variance ? 0.0 : ns.normal(i);
+            const double z = (P.zero_variance || row) ? 0.0 : ns.normal(i);
             const double t = P.obs_time[i];
             const double tv = P.vol * P.vol * t;
             for (int e = 0; e < pairs; ++e) {
                 const double ze = e == 0 ? z : -z;
                 double f;
-                if (n == 1) {
+                if (row) {
+                    f = row[static_cast<size_t>(i) * V.paths + e];
+                } else if (n == 1) {
                     f = P.obs_fwd[0] * 1.0 * exp(-0.5 * tv + sqrt(tv) * ze);
                 } else {
                     w[e] += P.obs_sqrt_step[i] * ze;

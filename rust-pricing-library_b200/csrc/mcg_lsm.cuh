@@ -43,7 +43,12 @@ struct LsmValueArgs {
     double* unit_values;               // [scrambles * units]: collapsed discounted value
     uint32_t* stops;                   // [paths] or null
     unsigned long long* counts;        // [dates]
+    const double* spots;               // stored valuation paths [dates][paths] (local volatility), or
+                                       // null: Black--Scholes paths generated in the kernel
+    uint64_t paths;
 };
+
+struct ErrorWord;
 
 // Fixed-policy risk of the valuation paths (Black--Scholes): the stopping
 // date of every path held, the discounted exercise value differentiated.
@@ -58,6 +63,10 @@ struct LsmRiskArgs {
 
 cudaError_t launch_lsm_bs_spots(const DevicePlan& P, uint32_t domain, double* spots, uint64_t paths,
                                 unsigned long long* bad, cudaStream_t stream);
+// Local-volatility path store (mcg_lv.cu): date-major spots of every path at
+// the exercise dates; the first failing unit in `err`.
+cudaError_t launch_lsm_lv_spots(const DevicePlan& P, uint32_t domain, double* spots, uint64_t paths, ErrorWord* err,
+                                cudaStream_t stream);
 cudaError_t launch_lsm_init(const LsmArgs& A, unsigned ctas, cudaStream_t stream);
 cudaError_t launch_lsm_step(const LsmArgs& A, unsigned ctas, int update, int gather, cudaStream_t stream);
 cudaError_t launch_lsm_bs_value(const DevicePlan& P, const LsmValueArgs& V, cudaStream_t stream);

@@ -51,6 +51,112 @@ template __global__ void lv_path_kernel<3, 1>(const DevicePlan, uint64_t, StatRe
 template __global__ void lv_path_kernel<3, 2>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
 template __global__ void lv_path_kernel<6, 1>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
 
+// Early-exercise path store under local volatility: the Log-Euler paths of
+// lv_tile on the base runtime (both antithetic signs, E = pairs), their state
+// at every exercise date written date-major, spots[d * paths + unit * E + e]
+// (write_local_vol_lsm_trajectory, crates/pricing/src/engine/mc/early_exercise.rs:389-450;
+// the observation's post-dividend spot is 0 * S0 + 1 * state).  `domain` is
+// the Philox RandomDomain (Valuation 0, LsmTrain 1) of pseudo paths.
+template <int E>
+__global__ void __launch_bounds__(kThreads) lsm_lv_spots_kernel(const DevicePlan P, uint32_t domain,
+                                                                double* spots, uint64_t paths, ErrorWord* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nx = static_cast<int>(P.nx);
+    const size_t nv = static_cast<size_t>(P.nt) * P.nx;
+    double* s_v = reinterpret_cast<double*>(smem_raw);
+    double* s_x = s_v + nv;
+    long long* s_xk = reinterpret_cast<long long*>(s_x + nx);
+    double* s_w = reinterpret_cast<double*>(s_xk + nx);
+    for (size_t i = threadIdx.x; i < nv; i += kThreads) s_v[i] = P.grid_v[i];
+    for (int i = threadIdx.x; i < nx; i += kThreads) {
+        s_x[i] = P.grid_x[i];
+        s_xk[i] = total_key(P.grid_x[i]);
+    }
+    __syncthreads();
+    const GridView g{s_v, s_x, s_xk, nx};
+    const uint32_t scramble = blockIdx.y;
+    const uint64_t point = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    const bool valid = point < P.units;
+    const uint64_t local = valid ? point : 0;
+    NormalSource ns;
+    ns.rqmc = P.engine == MCG_ENGINE_RQMC;
+    ns.seed = P.seed;
+    ns.unit = local;
+    ns.gray = static_cast<uint32_t>(local ^ (local >> 1));
+    ns.dirs = P.scr_dirs ? P.scr_dirs + static_cast<size_t>(scramble) * P.dimension * 32u : nullptr;
+    ns.shift = P.scr_shift ? P.scr_shift + static_cast<size_t>(scramble) * P.dimension : nullptr;
+    ns.cached_block = 0xffffffffu;
+    ns.domain = domain;
+    const uint64_t unit = static_cast<uint64_t>(scramble) * P.units + local;
+    double f[E];
+    int hint[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        f[e] = P.spot_variant[0];
+        hint[e] = 0;
+    }
+    int fail_code = 0;
+    uint32_t fail_step = 0;
+    double fail_value = 0.0;
+    double* w = s_w + threadIdx.x;
+    for (uint32_t oi = 0; oi < P.op_count; ++oi) {
+        const Op op = P.ops[oi];
+        if (op.kind == kOpZero) {
+            w[op.out * kThreads] = 0.0;
+            continue;
+        }
+        if (op.kind == kOpTerminal) {
+            w[op.out * kThreads] = op.sd * ns.normal(op.rank);
+            continue;
+        }
+        if (op.kind == kOpInterior) {
+            const double z = ns.normal(op.rank);
+            w[op.out * kThreads] = op.wl * w[op.left * kThreads] + op.wr * w[op.right * kThreads] + op.sd * z;
+            continue;
+        }
+        const uint32_t s = static_cast<uint32_t>(op.step);
+        const double shock = op.kind == kOpStep ? (w[op.right * kThreads] - w[op.left * kThreads]) * P.inv_sqrt_dt[s]
+                                                : ns.normal(op.rank);
+        const int tc = P.time_cell[s];
+        const double tw = P.time_weight[s];
+        const double dt = P.dt[s];
+        const double sq = P.sqrt_dt[s];
+        const int32_t obs = P.obs_of_node[s + 1];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const double z = e == 0 ? shock : -shock;
+            const double x = log(f[e] / P.fwd[s]);
+            const double v = interp_variance(g, tc, tw, x, hint[e]);
+            f[e] *= P.ratio[s] * exp(-0.5 * v * dt + sqrt(v) * sq * z);
+            if (!(isfinite(f[e]) && f[e] > 0.0) && !fail_code) {
+                fail_code = MCG_ERR_NON_FINITE_STATE;
+                fail_step = s + 1;
+                fail_value = f[e];
+            }
+            if (obs >= 0 && valid) spots[static_cast<size_t>(obs) * paths + unit * E + e] = 0.0 * P.spot + 1.0 * f[e];
+        }
+    }
+    if (valid && fail_code) report_error(err, unit, fail_code, fail_step, fail_value, false);
+}
+
+template __global__ void lsm_lv_spots_kernel<1>(const DevicePlan, uint32_t, double*, uint64_t, ErrorWord*);
+template __global__ void lsm_lv_spots_kernel<2>(const DevicePlan, uint32_t, double*, uint64_t, ErrorWord*);
+
+cudaError_t launch_lsm_lv_spots(const DevicePlan& P, uint32_t domain, double* spots, uint64_t paths, ErrorWord* err,
+                                cudaStream_t stream) {
+    const size_t smem = (static_cast<size_t>(P.nt) * P.nx + 2 * P.nx) * sizeof(double) +
+                        static_cast<size_t>(P.slot_count) * kThreads * sizeof(double);
+    const dim3 grid(static_cast<unsigned>((P.units + kThreads - 1) / kThreads), P.scramble_count);
+    auto go = [&](auto kernel) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        kernel<<<grid, kThreads, smem, stream>>>(P, domain, spots, paths, err);
+        return cudaGetLastError();
+    };
+    return P.antithetic ? go(lsm_lv_spots_kernel<2>) : go(lsm_lv_spots_kernel<1>);
+}
+
 // Launch helper: picks the instantiation for (evolutions, products).
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
                            StatRecord* partials, uint32_t mask, ErrorWord* err, int detail,

@@ -513,18 +513,21 @@ __global__ void __launch_bounds__(kMlpThreads) lsm_bs_value_mlp_kernel(const Dev
     double realized[2] = {0.0, 0.0};
     uint32_t stop[2] = {n - 1, n - 1};
     bool open[2] = {valid, valid && pairs == 2};
+    const double* row = V.spots && valid ? V.spots + unit * pairs : nullptr;
     for (uint32_t i = 0; i < n; ++i) {
         // CTA-uniform: every warp finished the previous date before the weights change
         if (!__syncthreads_or(open[0] || open[1])) break;
         if (i + 1 < n) load_net(S.net, params + static_cast<size_t>(i) * kMlpParams);
-        const double z = (P.zero_variance || !valid) ? 0.0 : ns.normal(i);
+        const double z = (P.zero_variance || !valid || V.spots) ? 0.0 : ns.normal(i);
         const double t = P.obs_time[i];
         const double tv = P.vol * P.vol * t;
         const float tin = static_cast<float>(2.0 * t * inv_horizon - 1.0);
         for (int e = 0; e < pairs; ++e) {
             const double ze = e == 0 ? z : -z;
             double f;
-            if (n == 1) {
+            if (V.spots) {
+                f = row ? row[static_cast<size_t>(i) * V.paths + e] : V.strike;
+            } else if (n == 1) {
                 f = P.obs_fwd[0] * 1.0 * exp(-0.5 * tv + sqrt(tv) * ze);
             } else {
                 w[e] += P.obs_sqrt_step[i] * ze;

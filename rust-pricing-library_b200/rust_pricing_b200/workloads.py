@@ -153,6 +153,29 @@ def american_bs(dates: int = 50, units: int = 1 << 20, training_units: Optional[
     return spec, lsm
 
 
+def american_lv(grid: LocalVarianceSpec, dates: int = 50, units: int = 1 << 20, training_units: Optional[int] = None,
+                engine: int = A.ENGINE_PSEUDO, antithetic: bool = False, scrambles: int = 4,
+                bridge: bool = False, max_degree: int = 3, rate: float = 0.05, strike: float = 100.0,
+                side: int = A.PUT, horizon: float = 1.0) -> tuple[PlanSpec, LsmSpec]:
+    """The American option of `american_bs` under a local-variance grid (the
+    training and valuation paths are Log-Euler paths on the grid's time grid
+    joined with the exercise dates)."""
+    spec, lsm = american_bs(dates=dates, units=units, training_units=training_units, engine=engine,
+                            antithetic=antithetic, scrambles=scrambles, max_degree=max_degree, vol=0.0,
+                            rate=rate, strike=strike, side=side, horizon=horizon)
+    spec.model = A.MODEL_LOCAL_VOLATILITY
+    spec.local_variance = grid
+    spec.brownian_bridge = bridge
+    lsm.training_brownian_bridge = bridge
+    return spec, lsm
+
+
+def flat_grid(vol: float, horizon: float = 1.0) -> LocalVarianceSpec:
+    """A 2 x 2 local-variance grid holding sigma^2 everywhere: its Log-Euler
+    paths on the exercise dates are the exact Black--Scholes paths."""
+    return LocalVarianceSpec([0.0, horizon], [-1.0, 1.0], np.full((2, 2), vol * vol), 1e-8, 4.0)
+
+
 BOOK_SEED = 20260904
 
 

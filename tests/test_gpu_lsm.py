@@ -177,6 +177,63 @@ def test_matrix_limit_is_an_lsm_error(engine):
     assert err.value.name == "lsm"
 
 
+@pytest.fixture(scope="module")
+def ssvi_grid():
+    surface = W.SsviSurface(steps=252, expiries=30)
+    return W.local_vol_grid(surface, G.gpu_grid)
+
+
+LV_CASES = {
+    "lv-pseudo-12-dates": dict(dates=12, units=1 << 13),
+    "lv-pseudo-antithetic-bridge-odd-units": dict(dates=7, units=5001, training_units=3001, antithetic=True,
+                                                   bridge=True),
+    "lv-rqmc-antithetic-bridge": dict(dates=10, units=1 << 10, engine=A.ENGINE_RQMC, antithetic=True,
+                                      scrambles=4, bridge=True),
+    "lv-call-degree-5": dict(dates=6, units=1 << 12, side=A.CALL, max_degree=5, strike=95.0),
+}
+
+
+@pytest.mark.parametrize("name", sorted(LV_CASES))
+def test_local_volatility_matches_the_oracle(engine, ssvi_grid, name):
+    """Early exercise under the SSVI local-variance grid: training and
+    valuation Log-Euler path stores, the same regression and policy."""
+    spec, lsm = W.american_lv(ssvi_grid, **LV_CASES[name])
+    got = N.lsm_price(spec, lsm, stopping=True)
+    want = H.oracle_lsm(spec, lsm, stopping=True, threads=8)
+    assert_same_result(spec, lsm, got, want)
+
+
+@pytest.mark.parametrize("engine_kind", [A.ENGINE_PSEUDO, A.ENGINE_RQMC], ids=["pseudo", "rqmc"])
+def test_flat_local_volatility_is_black_scholes(engine, engine_kind):
+    kw = dict(dates=12, units=1 << 13, engine=engine_kind, antithetic=True)
+    bs = N.lsm_price(*W.american_bs(vol=0.25, **kw), stopping=True)
+    lv = N.lsm_price(*W.american_lv(W.flat_grid(0.25), **kw), stopping=True)
+    assert list(lv.stops) == list(bs.stops)
+    assert rel(lv.result.price.value, bs.result.price.value) <= 1e-13
+
+
+def test_local_volatility_learned_policy(engine, ssvi_grid):
+    spec, lsm = W.american_lv(ssvi_grid, dates=10, units=1 << 14)
+    lsm.continuation = A.CONTINUATION_MLP
+    got = N.lsm_price(spec, lsm)
+    poly = N.lsm_price(*W.american_lv(ssvi_grid, dates=10, units=1 << 14))
+    r = got.result
+    assert r.continuation_used in (A.CONTINUATION_MLP, A.CONTINUATION_POLYNOMIAL)
+    # the policy kept is the one with the higher in-sample value on the same training paths
+    assert r.polynomial_in_sample == poly.result.in_sample_value
+    assert r.in_sample_value >= r.polynomial_in_sample
+    # an exercise policy can only lose value against the optimum: the kept one is not worse
+    assert r.price.value >= poly.result.price.value - 6 * poly.result.price.standard_error
+
+
+def test_local_volatility_risk_is_refused(engine, ssvi_grid):
+    spec, lsm = W.american_lv(ssvi_grid, dates=4, units=1 << 10)
+    spec.request_delta = True
+    with pytest.raises(N.EngineError) as err:
+        N.lsm_price(spec, lsm)
+    assert err.value.name == "unsupported"
+
+
 RISK_CASES = {
     "pseudo-antithetic-odd-units": lambda: W.american_bs(dates=7, units=5001, training_units=3001,
                                                          antithetic=True),

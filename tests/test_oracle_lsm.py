@@ -23,6 +23,7 @@ import pytest
 import helpers as H
 import lsm_cases as L
 from rust_pricing_b200 import _abi as A
+from rust_pricing_b200 import workloads as W
 
 
 def bits(x: float) -> str:
@@ -106,6 +107,22 @@ def test_replay_fixed_policy_risk(case):
     comp = buf.result.risk_components[A.PRICE]
     assert comp.sum + comp.correction == pytest.approx(
         buf.result.price.value * buf.result.independent_sampling_units, rel=1e-13)
+
+
+@pytest.mark.parametrize("engine", [A.ENGINE_PSEUDO, A.ENGINE_RQMC], ids=["pseudo", "rqmc"])
+def test_flat_local_volatility_is_black_scholes(engine):
+    """write_local_vol_lsm_trajectory (early_exercise.rs:389-450) on a flat
+    local-variance grid whose time grid is the exercise dates: the Log-Euler
+    step of a constant variance is the exact lognormal step and draws the same
+    normal per date, so every stopping date and exercise count equals the
+    Black--Scholes engine's and the prices agree to rounding."""
+    kw = dict(dates=12, units=1 << 12, engine=engine, antithetic=True)
+    bs = H.oracle_lsm(*W.american_bs(vol=0.25, **kw), stopping=True, threads=4)
+    lv = H.oracle_lsm(*W.american_lv(W.flat_grid(0.25), **kw), stopping=True, threads=4)
+    assert list(lv.stops) == list(bs.stops)
+    assert list(lv.counts[:12]) == list(bs.counts[:12])
+    assert abs(lv.result.price.value - bs.result.price.value) <= 1e-13 * bs.result.price.value
+    assert abs(lv.result.in_sample_value - bs.result.in_sample_value) <= 1e-13 * bs.result.in_sample_value
 
 
 def test_thread_count_does_not_change_the_result():
