@@ -323,6 +323,56 @@ mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double*
                                         uint32_t log_moneyness_count, double floor, double cap,
                                         double* values, uint32_t* repairs);
 
+/* ---- Implied-variance surfaces ----
+ *
+ * The surfaces LocalVarianceGrid::from_surface turns into a Dupire grid
+ * (crates/pricing/src/market/local_variance.rs:149-206):
+ *   standard SSVI with a PCHIP theta curve and a power-law or Heston-like phi
+ *     (crates/pricing/src/market/ssvi.rs:61-176,347-388,410-525,
+ *      crates/pricing/src/market/pchip.rs:111-237);
+ *   eSSVI slices (time, theta, psi, rho*psi) interpolated linearly in time,
+ *     scaled towards zero before the first slice, theta extended with the
+ *     terminal slope after the last (crates/pricing/src/market/essvi.rs:104-396).
+ * Validation follows the reference's constructors with its local_vol_vegakt_v1
+ * tolerance (absolute 1e-14, relative 1e-12). */
+typedef enum {
+    MCG_SURFACE_SSVI_POWER_LAW = 0,
+    MCG_SURFACE_SSVI_HESTON_LIKE = 1,
+    MCG_SURFACE_ESSVI = 2
+} mcg_surface_kind;
+
+typedef struct {
+    int32_t kind;                  /* mcg_surface_kind */
+    /* SSVI: theta curve knots and the PCHIP long-end slope */
+    const double* theta_times;
+    const double* theta_values;
+    uint32_t theta_count;
+    double terminal_theta_slope;   /* SSVI and eSSVI: d theta / dt after the last knot/slice */
+    double rho;                    /* SSVI correlation */
+    double eta, gamma;             /* power-law phi = eta / (theta^gamma (1 + theta)^(1 - gamma)) */
+    double lambda;                 /* Heston-like phi = (z - 1 + e^-z) / z^2, z = lambda theta */
+    /* eSSVI slices, increasing in time */
+    const double* slice_times;
+    const double* slice_thetas;
+    const double* slice_psis;
+    const double* slice_rho_psis;
+    uint32_t slice_count;
+} mcg_surface_desc;
+
+/* Dupire local-variance grid of any surface kind, computed on the device;
+ * as mcg_ssvi_local_variance_grid. */
+mcg_status mcg_surface_local_variance_grid(const mcg_surface_desc* surface, const double* time_nodes,
+                                           uint32_t time_count, const double* log_moneyness_nodes,
+                                           uint32_t log_moneyness_count, double floor, double cap,
+                                           double* values, uint32_t* repairs);
+
+/* Total variance and its derivatives at `count` (time, log-moneyness) points,
+ * evaluated by the device code the grid uses:
+ * out[4 i + 0..3] = w, dw/dk, d2w/dk2, dw/dt
+ * (ImpliedVarianceSurface::total_variance_derivatives). */
+mcg_status mcg_surface_total_variance(const mcg_surface_desc* surface, const double* times,
+                                      const double* log_moneyness, uint32_t count, double* out);
+
 /* ---- Early exercise: Longstaff--Schwartz regression ----
  *
  * Replaces SimulationPlan::execute_early_exercise and its RQMC twin

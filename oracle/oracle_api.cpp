@@ -16,6 +16,10 @@ int unit_shocks_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit,
 int unit_values_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out);
 int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacity, uint32_t* count);
 std::vector<double> pchip_derivatives(const std::vector<double>& t, const std::vector<double>& v);
+int surface_grid(const mcg_surface_desc& d, const std::vector<double>& tn, const std::vector<double>& xn,
+                 double floor, double cap, std::vector<double>& out);
+bool surface_derivatives(const mcg_surface_desc& d, const std::vector<double>& pd, double time, double k,
+                         double out[4]);
 int ssvi_grid(const std::vector<double>& theta_t, const std::vector<double>& theta_v, double slope,
               double rho, double eta, double gamma, const std::vector<double>& tn,
               const std::vector<double>& xn, double floor, double cap, std::vector<double>& out);
@@ -157,6 +161,25 @@ int oracle_ssvi_grid(const double* theta_t, const double* theta_v, uint32_t thet
                                           std::vector<double>(xn, xn + nx), floor, cap, values);
     if (repairs >= 0) std::memcpy(out, values.data(), values.size() * sizeof(double));
     return repairs;
+}
+
+// Dupire grid of any surface kind (mcg_surface_desc); repairs or -1.
+int oracle_surface_grid(const mcg_surface_desc* d, const double* tn, uint32_t nt, const double* xn, uint32_t nx,
+                        double floor, double cap, double* out) {
+    std::vector<double> values;
+    const int repairs = oracle::surface_grid(*d, std::vector<double>(tn, tn + nt), std::vector<double>(xn, xn + nx),
+                                             floor, cap, values);
+    if (repairs >= 0) std::memcpy(out, values.data(), values.size() * sizeof(double));
+    return repairs;
+}
+
+// w, w_k, w_kk, w_t of a surface at (t, k); 0, or -1 where the surface fails.
+int oracle_surface_total_variance(const mcg_surface_desc* d, double t, double k, double* out) {
+    std::vector<double> pd;
+    if (d->kind != MCG_SURFACE_ESSVI)
+        pd = oracle::pchip_derivatives(std::vector<double>(d->theta_times, d->theta_times + d->theta_count),
+                                       std::vector<double>(d->theta_values, d->theta_values + d->theta_count));
+    return oracle::surface_derivatives(*d, pd, t, k, out) ? 0 : -1;
 }
 
 int oracle_piecewise_sinh_nodes(double left, double right, uint32_t nl, uint32_t nr,

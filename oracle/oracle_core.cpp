@@ -1,5 +1,6 @@
 // oracle_core.cpp -- sampling, bridge, statistics, curve and grid primitives of
 // the CPU oracle.  TEST INFRASTRUCTURE ONLY (see oracle_core.h).
+#include "../include/mcg.h"
 #include "oracle_core.h"
 
 #include <algorithm>
@@ -437,6 +438,156 @@ int ssvi_grid(const std::vector<double>& theta_t, const std::vector<double>& the
             else if (raw <= 0.0) { value = floor; ++repairs; }
             else if (raw < floor) { value = floor; ++repairs; }
             else if (raw > cap) { value = cap; ++repairs; }
+            out[i * xn.size() + j] = value;
+        }
+    }
+    return repairs;
+}
+
+// ---------------------------------------------------------------- surfaces
+
+// PhiSpec::evaluate, crates/pricing/src/market/ssvi.rs:121-176 (power law and
+// Heston-like with its small-z series below |z| = 1e-4).
+void phi_of(const mcg_surface_desc& d, double theta, double& phi, double& dphi) {
+    if (d.kind == MCG_SURFACE_SSVI_POWER_LAW) {
+        phi = d.eta / (std::pow(theta, d.gamma) * std::pow(1.0 + theta, 1.0 - d.gamma));
+        dphi = -phi * (d.gamma / theta + (1.0 - d.gamma) / (1.0 + theta));
+        return;
+    }
+    const double z = d.lambda * theta;
+    if (std::fabs(z) <= 1.0e-4) {
+        phi = 0.5 + z * (-1.0 / 6.0 + z * (1.0 / 24.0 + z * (-1.0 / 120.0 +
+                                                               z * (1.0 / 720.0 + z * (-1.0 / 5040.0 + z / 40320.0)))));
+        const double dz = -1.0 / 6.0 + z * (1.0 / 12.0 + z * (-1.0 / 40.0 + z * (1.0 / 180.0 +
+                                                                                  z * (-1.0 / 1008.0 + z / 6720.0))));
+        dphi = d.lambda * dz;
+        return;
+    }
+    const double e = std::exp(-z);
+    phi = (z - 1.0 + e) / (z * z);
+    dphi = d.lambda * (2.0 - z - (z + 2.0) * e) / (z * z * z);
+}
+
+// EssviSurface::parameters with interpolate / long_parameters,
+// crates/pricing/src/market/essvi.rs:192-240,299-340.
+void essvi_parameters(const mcg_surface_desc& d, double time, double p[6]) {
+    const double* T = d.slice_times;
+    const double* TH = d.slice_thetas;
+    const double* PS = d.slice_psis;
+    const double* RP = d.slice_rho_psis;
+    const size_t n = d.slice_count;
+    if (time < T[0]) {
+        const double inv = 1.0 / T[0];
+        const double scale = time * inv;
+        const double q[6] = {scale * TH[0], scale * PS[0], scale * RP[0], TH[0] * inv, PS[0] * inv, RP[0] * inv};
+        std::memcpy(p, q, sizeof(q));
+        return;
+    }
+    auto interp = [&](size_t l, size_t r) {
+        const double width = T[r] - T[l];
+        const double weight = (time - T[l]) / width;
+        p[0] = TH[l] + weight * (TH[r] - TH[l]);
+        p[1] = PS[l] + weight * (PS[r] - PS[l]);
+        p[2] = RP[l] + weight * (RP[r] - RP[l]);
+        p[3] = (TH[r] - TH[l]) / width;
+        p[4] = (PS[r] - PS[l]) / width;
+        p[5] = (RP[r] - RP[l]) / width;
+    };
+    auto long_end = [&](size_t last) {
+        p[0] = TH[last] + d.terminal_theta_slope * (time - T[last]);
+        p[1] = PS[last];
+        p[2] = RP[last];
+        p[3] = d.terminal_theta_slope;
+        p[4] = 0.0;
+        p[5] = 0.0;
+    };
+    const int64_t key = total_key(time);
+    size_t lo = 0, hi = n;
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (total_key(T[mid]) < key) lo = mid + 1; else hi = mid;
+    }
+    if (lo < n && total_key(T[lo]) == key) {
+        if (lo + 1 < n) interp(lo, lo + 1); else long_end(lo);
+    } else if (lo < n) {
+        interp(lo - 1, lo);
+    } else {
+        long_end(n - 1);
+    }
+}
+
+// ImpliedVarianceSurface::total_variance_derivatives of both surfaces:
+// StandardSsvi (ssvi.rs:410-479) and evaluate_total_variance (essvi.rs:342-396).
+// out = {w, w_k, w_kk, w_t}; false on a non-finite or non-positive result.
+bool surface_derivatives(const mcg_surface_desc& d, const std::vector<double>& pd, double time, double k,
+                         double out[4]) {
+    if (d.kind == MCG_SURFACE_ESSVI) {
+        double p[6];
+        essvi_parameters(d, time, p);
+        const double theta = p[0], psi = p[1], rho_psi = p[2], dtheta = p[3], dpsi = p[4], drho_psi = p[5];
+        const double phi = psi / theta;
+        const double rho = rho_psi / psi;
+        const double rho_d = (drho_psi * psi - rho_psi * dpsi) / (psi * psi);
+        const double phi_d = (dpsi * theta - psi * dtheta) / (theta * theta);
+        const double y = phi * k;
+        const double y_d = k * phi_d;
+        const double a = y + rho;
+        const double q = std::sqrt(a * a + 1.0 - rho * rho);
+        const double q_d = (a * (y_d + rho_d) - rho * rho_d) / q;
+        const double shape = 1.0 + rho * y + q;
+        const double shape_d = rho_d * y + rho * y_d + q_d;
+        out[0] = theta * shape / 2.0;
+        out[1] = theta * phi * (rho + a / q) / 2.0;
+        out[2] = theta * phi * phi * (1.0 - rho * rho) / (2.0 * q * q * q);
+        out[3] = dtheta * shape / 2.0 + theta * shape_d / 2.0;
+    } else {
+        const std::vector<double> t(d.theta_times, d.theta_times + d.theta_count);
+        const std::vector<double> v(d.theta_values, d.theta_values + d.theta_count);
+        double theta, dtheta, phi, dphi;
+        pchip_evaluate(t, v, pd, d.terminal_theta_slope, time, theta, dtheta);
+        phi_of(d, theta, phi, dphi);
+        const double rho = d.rho;
+        const double y = phi * k;
+        const double a = y + rho;
+        const double q = std::sqrt(a * a + 1.0 - rho * rho);
+        const double shape = 1.0 + rho * y + q;
+        const double common = rho + a / q;
+        out[0] = theta * shape / 2.0;
+        out[1] = theta * phi * common / 2.0;
+        out[2] = theta * phi * phi * (1.0 - rho * rho) / (2.0 * q * q * q);
+        out[3] = (shape / 2.0 + theta * k * dphi * common / 2.0) * dtheta;
+    }
+    for (int i = 0; i < 4; ++i)
+        if (!std::isfinite(out[i])) return false;
+    return out[0] > 0.0;
+}
+
+// LocalVarianceGrid::from_surface (local_variance.rs:149-206) over any surface
+// kind.  Returns the repair count, or -1 on a surface error.
+int surface_grid(const mcg_surface_desc& d, const std::vector<double>& tn, const std::vector<double>& xn,
+                 double floor, double cap, std::vector<double>& out) {
+    std::vector<double> pd;
+    if (d.kind != MCG_SURFACE_ESSVI)
+        pd = pchip_derivatives(std::vector<double>(d.theta_times, d.theta_times + d.theta_count),
+                               std::vector<double>(d.theta_values, d.theta_values + d.theta_count));
+    out.assign(tn.size() * xn.size(), 0.0);
+    int repairs = 0;
+    for (size_t i = 0; i < tn.size(); ++i) {
+        const double st = tn[i] == 0.0 ? tn[1] : tn[i];
+        for (size_t j = 0; j < xn.size(); ++j) {
+            const double x = xn[j];
+            double w[4];
+            if (!surface_derivatives(d, pd, st, x, w)) return -1;
+            // durrleman_density_factor, ssvi.rs:226-273
+            const double u = 1.0 - x * w[1] / (2.0 * w[0]);
+            const double density = u * u - (w[1] * w[1] / 4.0) * (1.0 / w[0] + 1.0 / 4.0) + w[2] / 2.0;
+            if (!std::isfinite(density) || density <= 0.0) return -1;
+            const double raw = w[3] / density;
+            // classify_local_variance, local_variance.rs:607-627
+            double value = raw;
+            if (std::isnan(raw) || raw == -INFINITY || raw <= 0.0 || raw < floor) value = floor;
+            else if (raw == INFINITY || raw > cap) value = cap;
+            if (value != raw || std::isnan(raw)) ++repairs;
             out[i * xn.size() + j] = value;
         }
     }

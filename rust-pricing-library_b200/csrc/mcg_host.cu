@@ -27,6 +27,7 @@
 #include "mcg_lsm.cuh"
 #include "mcg_mlp.cuh"
 #include "mcg_book.cuh"
+#include "mcg_surface.cuh"
 
 namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -43,13 +44,6 @@ __global__ void reduce_tiles_kernel(const StatRecord*, uint32_t, uint32_t, StatR
 __global__ void philox_normals_kernel(uint64_t, uint64_t, uint64_t, uint32_t, uint32_t, double*);
 __global__ void rqmc_words_kernel(const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint64_t,
                                   uint64_t, uint32_t*);
-struct Pchip {
-    const double* t;
-    const double* v;
-    const double* d;
-    uint32_t n;
-    double slope;
-};
 __global__ void fp64_peak_kernel(double*, int);
 struct AdjointArgs {
     int32_t which;
@@ -73,9 +67,6 @@ cudaError_t launch_lv_adjoint_combine(const double* vega, const double* delta, u
                                       cudaStream_t stream);
 cudaError_t launch_lv_node_reduce(const double* node_tiles, uint32_t tiles_per_scramble, uint32_t scrambles,
                                   uint32_t nv, StatRecord* out, cudaStream_t stream);
-__global__ void ssvi_grid_kernel(Pchip, double, double, double, const double*, uint32_t,
-                                 const double*, uint32_t, double, double, double*, uint32_t*,
-                                 uint32_t*);
 }  // namespace mcg
 
 using namespace mcg;
@@ -2050,22 +2041,21 @@ mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint6
     return MCG_OK;
 }
 
-mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double* theta_values, uint32_t theta_count,
-                                        double terminal_slope, double rho, double eta, double gamma,
-                                        const double* time_nodes, uint32_t time_count,
-                                        const double* log_moneyness_nodes, uint32_t log_moneyness_count,
-                                        double floor, double cap, double* values, uint32_t* repairs) {
-    if (!theta_times || !theta_values || theta_count < 2 || !time_nodes || time_count < 2 ||
-        !log_moneyness_nodes || log_moneyness_count < 2 || !values)
-        return fail(MCG_ERR_INVALID_ARGUMENT, "ssvi grid inputs");
-    if (!(gamma > 0.0 && gamma < 1.0) || !(eta > 0.0) || !(rho > -1.0 && rho < 1.0))
-        return fail(MCG_ERR_MARKET, "SSVI parameters outside their domain");
-    // PCHIP derivatives on the host (pchip.rs:178-237); one-off knot data.
-    const uint32_t n = theta_count;
-    std::vector<double> h(n - 1), s(n - 1), dv(n, 0.0);
+}  // extern "C"
+
+namespace {
+
+// SurfaceValidationTolerance::local_vol_vegakt_v1 (crates/pricing/src/market/ssvi.rs:30-58).
+double tol_effective(double l, double r) { return std::max(1.0e-14, 1.0e-12 * std::max({1.0, std::fabs(l), std::fabs(r)})); }
+bool permits_non_strict(double l, double r) { return l - r <= tol_effective(l, r); }
+bool permits_strict(double l, double r) { return r - l > tol_effective(l, r); }
+
+// PCHIP knot derivatives (ThetaPchip, crates/pricing/src/market/pchip.rs:178-237).
+std::vector<double> pchip_knot_derivatives(const double* t, const double* v, uint32_t n) {
+    std::vector<double> h(n - 1), sl(n - 1), dv(n, 0.0);
     for (uint32_t i = 0; i + 1 < n; ++i) {
-        h[i] = theta_times[i + 1] - theta_times[i];
-        s[i] = (theta_values[i + 1] - theta_values[i]) / h[i];
+        h[i] = t[i + 1] - t[i];
+        sl[i] = (v[i + 1] - v[i]) / h[i];
     }
     auto sg = [](double x) { return std::signbit(x) ? -1.0 : 1.0; };
     auto endpoint = [&](double aw, double nw, double as, double ns) {
@@ -2075,55 +2065,263 @@ mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double*
         return dd;
     };
     if (n == 2) {
-        dv[0] = dv[1] = s[0];
-    } else {
-        dv[0] = endpoint(h[0], h[1], s[0], s[1]);
-        for (uint32_t i = 1; i + 1 < n; ++i) {
-            const double l = s[i - 1], r = s[i];
-            if (l == 0.0 || r == 0.0 || sg(l) != sg(r)) {
-                dv[i] = 0.0;
-            } else {
-                const double w1 = 2.0 * h[i] + h[i - 1];
-                const double w2 = h[i] + 2.0 * h[i - 1];
-                dv[i] = (w1 + w2) / (w1 / l + w2 / r);
-            }
-        }
-        dv[n - 1] = endpoint(h[n - 2], h[n - 3], s[n - 2], s[n - 3]);
+        dv[0] = dv[1] = sl[0];
+        return dv;
     }
-    double *dt = nullptr, *dvv = nullptr, *dd = nullptr, *tn = nullptr, *xn = nullptr, *out = nullptr;
-    uint32_t* counters = nullptr;
+    dv[0] = endpoint(h[0], h[1], sl[0], sl[1]);
+    for (uint32_t i = 1; i + 1 < n; ++i) {
+        const double l = sl[i - 1], r = sl[i];
+        if (l == 0.0 || r == 0.0 || sg(l) != sg(r)) {
+            dv[i] = 0.0;
+        } else {
+            const double w1 = 2.0 * h[i] + h[i - 1];
+            const double w2 = h[i] + 2.0 * h[i - 1];
+            dv[i] = (w1 + w2) / (w1 / l + w2 / r);
+        }
+    }
+    dv[n - 1] = endpoint(h[n - 2], h[n - 3], sl[n - 2], sl[n - 3]);
+    return dv;
+}
+
+// Host phi(theta) for the SSVI admissibility checks (PhiSpec::evaluate, ssvi.rs:121-176).
+void host_phi(const mcg_surface_desc& d, double theta, double& phi, double& dphi) {
+    if (d.kind == MCG_SURFACE_SSVI_POWER_LAW) {
+        phi = d.eta / (std::pow(theta, d.gamma) * std::pow(1.0 + theta, 1.0 - d.gamma));
+        dphi = -phi * (d.gamma / theta + (1.0 - d.gamma) / (1.0 + theta));
+        return;
+    }
+    const double z = d.lambda * theta;
+    if (std::fabs(z) <= 1.0e-4) {
+        phi = 0.5 + z * (-1.0 / 6.0 +
+                         z * (1.0 / 24.0 + z * (-1.0 / 120.0 + z * (1.0 / 720.0 + z * (-1.0 / 5040.0 + z / 40320.0)))));
+        dphi = d.lambda *
+               (-1.0 / 6.0 + z * (1.0 / 12.0 + z * (-1.0 / 40.0 + z * (1.0 / 180.0 + z * (-1.0 / 1008.0 + z / 6720.0)))));
+        return;
+    }
+    const double e = std::exp(-z);
+    phi = (z - 1.0 + e) / (z * z);
+    dphi = d.lambda * (2.0 - z - (z + 2.0) * e) / (z * z * z);
+}
+
+bool all_finite(const double* x, uint32_t n) {
+    for (uint32_t i = 0; i < n; ++i)
+        if (!std::isfinite(x[i])) return false;
+    return true;
+}
+
+// The surface constructors' checks: ThetaPchip::new (pchip.rs:27-90),
+// StandardSsvi::new with PhiSpec::validate and validate_butterfly_bounds
+// (ssvi.rs:77-118,347-388,501-525), EssviSlice::new / EssviSurface::new /
+// validate_slice (essvi.rs:14-172,262-297).
+std::string validate_surface(const mcg_surface_desc& d) {
+    if (!std::isfinite(d.terminal_theta_slope) || d.terminal_theta_slope < 0.0) return "terminal_theta_slope";
+    if (d.kind == MCG_SURFACE_ESSVI) {
+        const uint32_t n = d.slice_count;
+        if (n < 2 || !d.slice_times || !d.slice_thetas || !d.slice_psis || !d.slice_rho_psis)
+            return "eSSVI needs at least two slices";
+        for (uint32_t i = 0; i < n; ++i) {
+            const double t = d.slice_times[i], th = d.slice_thetas[i], ps = d.slice_psis[i], rp = d.slice_rho_psis[i];
+            if (!std::isfinite(t) || !std::isfinite(th) || !std::isfinite(ps) || !std::isfinite(rp))
+                return "eSSVI slice " + std::to_string(i) + " is not finite";
+            if (t <= 0.0 || th <= 0.0 || ps <= 0.0) return "eSSVI slice " + std::to_string(i) + " time/theta/psi";
+            const double rho = rp / ps;
+            if (!std::isfinite(rho) || std::fabs(rho) >= 1.0) return "eSSVI slice " + std::to_string(i) + " rho";
+            const double wing = ps * (1.0 + std::fabs(rho));
+            if (!std::isfinite(wing) || !permits_strict(wing, 4.0))
+                return "eSSVI slice " + std::to_string(i) + " strict_wing_slope";
+            const double curvature = ps * ps * (1.0 + std::fabs(rho));
+            const double limit = 4.0 * th;
+            if (!std::isfinite(curvature) || !std::isfinite(limit) || !permits_non_strict(curvature, limit))
+                return "eSSVI slice " + std::to_string(i) + " curvature_bound";
+        }
+        for (uint32_t i = 0; i + 1 < n; ++i) {
+            if (d.slice_times[i + 1] <= d.slice_times[i]) return "eSSVI slices unsorted";
+            if (d.slice_thetas[i + 1] < d.slice_thetas[i]) return "eSSVI theta_non_decreasing";
+            if (d.slice_psis[i + 1] < d.slice_psis[i]) return "eSSVI psi_non_decreasing";
+            const double change = std::fabs(d.slice_rho_psis[i + 1] - d.slice_rho_psis[i]);
+            if (!permits_non_strict(change, d.slice_psis[i + 1] - d.slice_psis[i])) return "eSSVI rho_psi_change_bound";
+        }
+        return "";
+    }
+    if (d.kind != MCG_SURFACE_SSVI_POWER_LAW && d.kind != MCG_SURFACE_SSVI_HESTON_LIKE) return "surface kind";
+    const uint32_t n = d.theta_count;
+    if (n < 2 || !d.theta_times || !d.theta_values) return "theta curve needs at least two knots";
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!std::isfinite(d.theta_times[i]) || d.theta_times[i] <= 0.0) return "theta knot time";
+        if (!std::isfinite(d.theta_values[i]) || d.theta_values[i] <= 0.0) return "theta value";
+        if (i && d.theta_times[i] <= d.theta_times[i - 1]) return "theta knots unsorted";
+        if (i && d.theta_values[i] < d.theta_values[i - 1]) return "theta decreasing";
+    }
+    if (!std::isfinite(d.rho) || std::fabs(d.rho) >= 1.0) return "rho";
+    if (d.kind == MCG_SURFACE_SSVI_POWER_LAW) {
+        if (!std::isfinite(d.eta) || d.eta <= 0.0) return "eta";
+        if (!std::isfinite(d.gamma) || !(d.gamma > 0.0 && d.gamma < 1.0)) return "gamma";
+        if (!permits_non_strict(d.gamma, 0.5)) return "power_law_gamma_at_most_one_half";
+        const double wing = d.eta * (1.0 + std::fabs(d.rho));
+        if (!std::isfinite(wing) || !permits_non_strict(wing, 2.0)) return "power_law_eta_wing_bound";
+    } else {
+        if (!std::isfinite(d.lambda) || d.lambda <= 0.0) return "lambda";
+        if (!permits_non_strict((1.0 + std::fabs(d.rho)) / 4.0, d.lambda)) return "heston_like_lambda_lower_bound";
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const double theta = d.theta_values[i];
+        double phi, dphi;
+        host_phi(d, theta, phi, dphi);
+        if (!std::isfinite(phi) || phi <= 0.0 || !std::isfinite(dphi)) return "phi";
+        const double cf = 1.0 + std::fabs(d.rho);
+        const double wing = theta * phi * cf;
+        if (!std::isfinite(wing) || !permits_strict(wing, 4.0)) return "strict_wing_slope";
+        const double curvature = theta * phi * phi * cf;
+        if (!std::isfinite(curvature) || !permits_non_strict(curvature, 4.0)) return "curvature_bound";
+        if (dphi >= 0.0) return "phi_strictly_decreasing";
+        const double skew = phi + theta * dphi;
+        if (skew < -tol_effective(skew, 0.0)) return "theta_phi_non_decreasing";
+    }
+    return "";
+}
+
+// A device array released when it leaves scope.
+template <class T>
+struct ScopedArray : DeviceArray<T> {
+    ~ScopedArray() { this->release(); }
+};
+
+// Device copies of a validated surface.
+struct DeviceSurface {
+    Surface s{};
+    DeviceArray<double> t, v, d, st, sth, sps, srp;
+    ~DeviceSurface() {
+        t.release();
+        v.release();
+        d.release();
+        st.release();
+        sth.release();
+        sps.release();
+        srp.release();
+    }
+};
+
+mcg_status load_surface(const mcg_surface_desc* desc, DeviceSurface& out) {
+    if (!desc) return fail(MCG_ERR_INVALID_ARGUMENT, "null surface");
+    const std::string why = validate_surface(*desc);
+    if (!why.empty()) return fail(MCG_ERR_MARKET, "surface: " + why);
+    Surface& s = out.s;
+    s.kind = desc->kind;
+    s.slope = desc->terminal_theta_slope;
+    s.rho = desc->rho;
+    s.eta = desc->eta;
+    s.gamma = desc->gamma;
+    s.lambda = desc->lambda;
+    if (desc->kind == MCG_SURFACE_ESSVI) {
+        const uint32_t n = desc->slice_count;
+        MCG_CUDA(out.st.upload(std::vector<double>(desc->slice_times, desc->slice_times + n)));
+        MCG_CUDA(out.sth.upload(std::vector<double>(desc->slice_thetas, desc->slice_thetas + n)));
+        MCG_CUDA(out.sps.upload(std::vector<double>(desc->slice_psis, desc->slice_psis + n)));
+        MCG_CUDA(out.srp.upload(std::vector<double>(desc->slice_rho_psis, desc->slice_rho_psis + n)));
+        s.st = out.st.ptr;
+        s.stheta = out.sth.ptr;
+        s.spsi = out.sps.ptr;
+        s.srho_psi = out.srp.ptr;
+        s.slices = n;
+    } else {
+        const uint32_t n = desc->theta_count;
+        MCG_CUDA(out.t.upload(std::vector<double>(desc->theta_times, desc->theta_times + n)));
+        MCG_CUDA(out.v.upload(std::vector<double>(desc->theta_values, desc->theta_values + n)));
+        MCG_CUDA(out.d.upload(pchip_knot_derivatives(desc->theta_times, desc->theta_values, n)));
+        s.t = out.t.ptr;
+        s.v = out.v.ptr;
+        s.d = out.d.ptr;
+        s.n = n;
+    }
+    return MCG_OK;
+}
+
+mcg_status surface_grid(const mcg_surface_desc* desc, const double* time_nodes, uint32_t time_count,
+                        const double* log_moneyness_nodes, uint32_t log_moneyness_count, double floor, double cap,
+                        double* values, uint32_t* repairs) {
+    if (!time_nodes || time_count < 2 || !log_moneyness_nodes || log_moneyness_count < 2 || !values)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "grid inputs");
+    if (!all_finite(time_nodes, time_count) || !all_finite(log_moneyness_nodes, log_moneyness_count))
+        return fail(MCG_ERR_MARKET, "grid nodes must be finite");
+    for (uint32_t i = 0; i < time_count; ++i)
+        if (time_nodes[i] < 0.0 || (i && !(time_nodes[i] > time_nodes[i - 1])))
+            return fail(MCG_ERR_MARKET, "grid time nodes must be non-negative and increasing");
+    for (uint32_t j = 1; j < log_moneyness_count; ++j)
+        if (!(log_moneyness_nodes[j] > log_moneyness_nodes[j - 1]))
+            return fail(MCG_ERR_MARKET, "log-moneyness nodes must be increasing");
+    if (!(floor > 0.0) || !(cap > floor) || !std::isfinite(cap)) return fail(MCG_ERR_MARKET, "floor/cap");
+    DeviceSurface S;
+    mcg_status st = load_surface(desc, S);
+    if (st != MCG_OK) return st;
     const size_t nv = static_cast<size_t>(time_count) * log_moneyness_count;
-    MCG_CUDA(cudaMalloc(&dt, n * 8));
-    MCG_CUDA(cudaMalloc(&dvv, n * 8));
-    MCG_CUDA(cudaMalloc(&dd, n * 8));
-    MCG_CUDA(cudaMalloc(&tn, time_count * 8));
-    MCG_CUDA(cudaMalloc(&xn, log_moneyness_count * 8));
-    MCG_CUDA(cudaMalloc(&out, nv * 8));
-    MCG_CUDA(cudaMalloc(&counters, 2 * 4));
-    cudaMemcpy(dt, theta_times, n * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dvv, theta_values, n * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dd, dv.data(), n * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(tn, time_nodes, time_count * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(xn, log_moneyness_nodes, log_moneyness_count * 8, cudaMemcpyHostToDevice);
-    cudaMemset(counters, 0, 8);
-    Pchip pc{dt, dvv, dd, n, terminal_slope};
-    ssvi_grid_kernel<<<static_cast<unsigned>((nv + 127) / 128), 128>>>(pc, rho, eta, gamma, tn, time_count, xn,
-                                                                      log_moneyness_count, floor, cap, out,
-                                                                      counters, counters + 1);
-    cudaError_t e = cudaGetLastError();
+    ScopedArray<double> tn, xn, out;
+    ScopedArray<uint32_t> counters;
+    MCG_CUDA(tn.upload(std::vector<double>(time_nodes, time_nodes + time_count)));
+    MCG_CUDA(xn.upload(std::vector<double>(log_moneyness_nodes, log_moneyness_nodes + log_moneyness_count)));
+    MCG_CUDA(out.alloc(nv));
+    MCG_CUDA(counters.upload(std::vector<uint32_t>(2, 0u)));
+    cudaError_t e = launch_surface_grid(S.s, tn.ptr, time_count, xn.ptr, log_moneyness_count, floor, cap, out.ptr,
+                                        counters.ptr, 0);
     uint32_t host_counters[2] = {0, 0};
-    if (e == cudaSuccess) e = cudaMemcpy(values, out, nv * 8, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(host_counters, counters, 8, cudaMemcpyDeviceToHost);
-    cudaFree(dt);
-    cudaFree(dvv);
-    cudaFree(dd);
-    cudaFree(tn);
-    cudaFree(xn);
-    cudaFree(out);
-    cudaFree(counters);
+    if (e == cudaSuccess) e = cudaMemcpy(values, out.ptr, nv * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(host_counters, counters.ptr, 8, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
     if (repairs) *repairs = host_counters[0];
-    if (host_counters[1]) return fail(MCG_ERR_MARKET, "SSVI surface has a non-positive variance or density");
+    if (host_counters[1]) return fail(MCG_ERR_MARKET, "surface has a non-positive variance or density");
+    return MCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mcg_status mcg_ssvi_local_variance_grid(const double* theta_times, const double* theta_values, uint32_t theta_count,
+                                        double terminal_slope, double rho, double eta, double gamma,
+                                        const double* time_nodes, uint32_t time_count,
+                                        const double* log_moneyness_nodes, uint32_t log_moneyness_count,
+                                        double floor, double cap, double* values, uint32_t* repairs) {
+    mcg_surface_desc d{};
+    d.kind = MCG_SURFACE_SSVI_POWER_LAW;
+    d.theta_times = theta_times;
+    d.theta_values = theta_values;
+    d.theta_count = theta_count;
+    d.terminal_theta_slope = terminal_slope;
+    d.rho = rho;
+    d.eta = eta;
+    d.gamma = gamma;
+    return surface_grid(&d, time_nodes, time_count, log_moneyness_nodes, log_moneyness_count, floor, cap, values,
+                        repairs);
+}
+
+mcg_status mcg_surface_local_variance_grid(const mcg_surface_desc* surface, const double* time_nodes,
+                                           uint32_t time_count, const double* log_moneyness_nodes,
+                                           uint32_t log_moneyness_count, double floor, double cap, double* values,
+                                           uint32_t* repairs) {
+    return surface_grid(surface, time_nodes, time_count, log_moneyness_nodes, log_moneyness_count, floor, cap,
+                        values, repairs);
+}
+
+mcg_status mcg_surface_total_variance(const mcg_surface_desc* surface, const double* times,
+                                      const double* log_moneyness, uint32_t count, double* out) {
+    if (!times || !log_moneyness || !out || count == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "surface points");
+    for (uint32_t i = 0; i < count; ++i)
+        if (!std::isfinite(times[i]) || times[i] <= 0.0 || !std::isfinite(log_moneyness[i]))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "surface query point " + std::to_string(i));
+    DeviceSurface S;
+    mcg_status st = load_surface(surface, S);
+    if (st != MCG_OK) return st;
+    ScopedArray<double> t, k, o;
+    ScopedArray<uint32_t> failures;
+    MCG_CUDA(t.upload(std::vector<double>(times, times + count)));
+    MCG_CUDA(k.upload(std::vector<double>(log_moneyness, log_moneyness + count)));
+    MCG_CUDA(o.alloc(4 * static_cast<size_t>(count)));
+    MCG_CUDA(failures.upload(std::vector<uint32_t>(1, 0u)));
+    cudaError_t e = launch_surface_eval(S.s, t.ptr, k.ptr, count, o.ptr, failures.ptr, 0);
+    uint32_t bad = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(out, o.ptr, 4 * static_cast<size_t>(count) * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&bad, failures.ptr, 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+    if (bad) return fail(MCG_ERR_MARKET, "surface has a non-finite or non-positive total variance");
     return MCG_OK;
 }
 

@@ -7,9 +7,10 @@
 //    a fixed tree (the role of fixed_tree_reduce,
 //    crates/pricing-numerics/src/reduction.rs:244-272).
 //  * philox_normals_kernel / rqmc_words_kernel: sampling known-answer entry points.
-//  * ssvi_grid_kernel: the Dupire local-variance grid of an SSVI surface
-//    (crates/pricing/src/market/local_variance.rs:149-206).
+//  * surface_grid_kernel: the Dupire local-variance grid of an SSVI or eSSVI
+//    surface (crates/pricing/src/market/local_variance.rs:149-206).
 #include "mcg_kernels.cuh"
+#include "mcg_surface.cuh"
 
 namespace mcg {
 
@@ -103,97 +104,32 @@ __global__ void rqmc_words_kernel(const uint32_t* table, const uint32_t* shifts,
 
 // ----------------------------------------------------------- SSVI grid
 
-struct Pchip {
-    const double* t;
-    const double* v;
-    const double* d;
-    uint32_t n;
-    double slope;
-};
-
-// ThetaPchip::evaluate, crates/pricing/src/market/pchip.rs:111-176.
-__device__ void pchip_eval(const Pchip& c, double time, double& theta, double& deriv) {
-    if (time == 0.0) time = 0.0;
-    if (time < c.t[0]) {
-        deriv = c.v[0] / c.t[0];
-        theta = time * deriv;
-        return;
-    }
-    const long long key = total_key(time);
-    uint32_t lo = 0, hi = c.n;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) / 2;
-        if (total_key(c.t[mid]) < key) lo = mid + 1; else hi = mid;
-    }
-    if (lo < c.n && total_key(c.t[lo]) == key) {
-        theta = c.v[lo];
-        deriv = c.d[lo];
-        return;
-    }
-    if (lo < c.n) {
-        const uint32_t r = lo, l = lo - 1;
-        const double width = c.t[r] - c.t[l];
-        const double sc = (time - c.t[l]) / width;
-        const double sc2 = sc * sc;
-        const double sc3 = sc2 * sc;
-        const double h00 = 2.0 * sc3 - 3.0 * sc2 + 1.0;
-        const double h10 = sc3 - 2.0 * sc2 + sc;
-        const double h01 = -2.0 * sc3 + 3.0 * sc2;
-        const double h11 = sc3 - sc2;
-        theta = h00 * c.v[l] + h10 * width * c.d[l] + h01 * c.v[r] + h11 * width * c.d[r];
-        const double d00 = (6.0 * sc2 - 6.0 * sc) / width;
-        const double d10 = 3.0 * sc2 - 4.0 * sc + 1.0;
-        const double d01 = (-6.0 * sc2 + 6.0 * sc) / width;
-        const double d11 = 3.0 * sc2 - 2.0 * sc;
-        deriv = d00 * c.v[l] + d10 * c.d[l] + d01 * c.v[r] + d11 * c.d[r];
-        return;
-    }
-    const uint32_t last = c.n - 1;
-    theta = c.v[last] + c.slope * (time - c.t[last]);
-    deriv = c.slope;
-}
-
-// One thread per grid node: StandardSsvi::total_variance_derivatives
-// (ssvi.rs:410-479) with the power-law phi (ssvi.rs:121-176), the Durrleman
-// density factor (ssvi.rs:226-273) and the floor/cap classification
-// (local_variance.rs:607-627).  The t = 0 row is evaluated at the first
-// positive time node (local_variance.rs:164).
-__global__ void ssvi_grid_kernel(Pchip theta, double rho, double eta, double gamma,
-                                 const double* tn, uint32_t nt, const double* xn, uint32_t nx,
-                                 double floor, double cap, double* out, uint32_t* repairs,
-                                 uint32_t* failures) {
+// One thread per grid node: the surface's total variance derivatives at
+// (t, k), the Durrleman density factor (ssvi.rs:226-273) and the floor/cap
+// classification (local_variance.rs:607-627).  The t = 0 row is evaluated at
+// the first positive time node (local_variance.rs:164).  counters[0] counts
+// repairs, counters[1] nodes where the surface or the density is invalid.
+__global__ void surface_grid_kernel(const Surface S, const double* tn, uint32_t nt, const double* xn, uint32_t nx,
+                                    double floor, double cap, double* out, uint32_t* counters) {
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= nt * nx) return;
     const uint32_t i = idx / nx, j = idx % nx;
     const double st = tn[i] == 0.0 ? tn[1] : tn[i];
-    double th, dth;
-    pchip_eval(theta, st, th, dth);
-    const double phi = eta / (pow(th, gamma) * pow(1.0 + th, 1.0 - gamma));
-    const double phi_td = -phi * (gamma / th + (1.0 - gamma) / (1.0 + th));
     const double x = xn[j];
-    const double y = phi * x;
-    const double a = y + rho;
-    const double q = sqrt(a * a + 1.0 - rho * rho);
-    const double shape = 1.0 + rho * y + q;
-    const double w = th * shape / 2.0;
-    const double common = rho + a / q;
-    const double wk = th * phi * common / 2.0;
-    const double wkk = th * phi * phi * (1.0 - rho * rho) / (2.0 * q * q * q);
-    const double partial = shape / 2.0 + th * x * phi_td * common / 2.0;
-    const double wt = partial * dth;
-    if (!(w > 0.0) || !isfinite(w) || !isfinite(wt)) {
-        atomicAdd(failures, 1u);
+    TotalVariance tv;
+    if (!surface_total_variance(S, st, x, tv)) {
+        atomicAdd(&counters[1], 1u);
         out[idx] = floor;
         return;
     }
-    const double u = 1.0 - x * wk / (2.0 * w);
-    const double density = u * u - (wk * wk / 4.0) * (1.0 / w + 1.0 / 4.0) + wkk / 2.0;
+    const double u = 1.0 - x * tv.wk / (2.0 * tv.w);
+    const double density = u * u - (tv.wk * tv.wk / 4.0) * (1.0 / tv.w + 1.0 / 4.0) + tv.wkk / 2.0;
     if (!isfinite(density) || density <= 0.0) {
-        atomicAdd(failures, 1u);
+        atomicAdd(&counters[1], 1u);
         out[idx] = floor;
         return;
     }
-    const double raw = wt / density;
+    const double raw = tv.wt / density;
     double value = raw;
     bool repaired = true;
     if (isnan(raw)) value = floor;
@@ -203,8 +139,35 @@ __global__ void ssvi_grid_kernel(Pchip theta, double rho, double eta, double gam
     else if (raw < floor) value = floor;
     else if (raw > cap) value = cap;
     else repaired = false;
-    if (repaired) atomicAdd(repairs, 1u);
+    if (repaired) atomicAdd(&counters[0], 1u);
     out[idx] = value;
+}
+
+// Total variance derivatives at explicit points (the surface known-answer entry point).
+__global__ void surface_eval_kernel(const Surface S, const double* times, const double* ks, uint32_t count,
+                                    double* out, uint32_t* failures) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    TotalVariance tv;
+    if (!surface_total_variance(S, times[i], ks[i], tv)) atomicAdd(failures, 1u);
+    out[4 * i + 0] = tv.w;
+    out[4 * i + 1] = tv.wk;
+    out[4 * i + 2] = tv.wkk;
+    out[4 * i + 3] = tv.wt;
+}
+
+cudaError_t launch_surface_grid(const Surface& s, const double* tn, uint32_t nt, const double* xn, uint32_t nx,
+                                double floor, double cap, double* out, uint32_t* counters, cudaStream_t stream) {
+    const size_t nv = static_cast<size_t>(nt) * nx;
+    surface_grid_kernel<<<static_cast<unsigned>((nv + 127) / 128), 128, 0, stream>>>(s, tn, nt, xn, nx, floor, cap,
+                                                                                    out, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_surface_eval(const Surface& s, const double* times, const double* ks, uint32_t count,
+                                double* out, uint32_t* failures, cudaStream_t stream) {
+    surface_eval_kernel<<<(count + 127) / 128, 128, 0, stream>>>(s, times, ks, count, out, failures);
+    return cudaGetLastError();
 }
 
 }  // namespace mcg

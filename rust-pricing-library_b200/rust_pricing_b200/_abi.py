@@ -43,6 +43,18 @@ class Curve(C.Structure):
     _fields_ = [("pillar_count", C.c_uint32), ("times", _dp), ("discount_factors", _dp)]
 
 
+SURFACE_SSVI_POWER_LAW, SURFACE_SSVI_HESTON_LIKE, SURFACE_ESSVI = 0, 1, 2
+
+
+class SurfaceDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("theta_times", _dp), ("theta_values", _dp), ("theta_count", C.c_uint32),
+        ("terminal_theta_slope", C.c_double), ("rho", C.c_double), ("eta", C.c_double), ("gamma", C.c_double),
+        ("lambda_", C.c_double), ("slice_times", _dp), ("slice_thetas", _dp), ("slice_psis", _dp),
+        ("slice_rho_psis", _dp), ("slice_count", C.c_uint32),
+    ]
+
+
 class LocalVarianceGrid(C.Structure):
     _fields_ = [
         ("time_count", C.c_uint32), ("log_moneyness_count", C.c_uint32),

@@ -19,7 +19,7 @@ EXPORTS = (
     "mcg_plan_destroy", "mcg_plan_shape", "mcg_philox_normals", "mcg_rqmc_words",
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
     "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient", "mcg_book_create", "mcg_book_evaluate",
-    "mcg_book_destroy",
+    "mcg_book_destroy", "mcg_surface_local_variance_grid", "mcg_surface_total_variance",
 )
 
 _lib = None
@@ -66,6 +66,11 @@ def library() -> C.CDLL:
     lib.mcg_ssvi_local_variance_grid.argtypes = [dp, dp, u32, dbl, dbl, dbl, dbl, dp, u32, dp, u32,
                                                  dbl, dbl, dp, C.POINTER(u32)]
     lib.mcg_ssvi_local_variance_grid.restype = C.c_int
+    lib.mcg_surface_local_variance_grid.argtypes = [C.POINTER(A.SurfaceDesc), dp, u32, dp, u32, dbl, dbl, dp,
+                                                    C.POINTER(u32)]
+    lib.mcg_surface_local_variance_grid.restype = C.c_int
+    lib.mcg_surface_total_variance.argtypes = [C.POINTER(A.SurfaceDesc), dp, dp, u32, dp]
+    lib.mcg_surface_total_variance.restype = C.c_int
     lib.mcg_price_european_noalloc.argtypes = [C.POINTER(A.PlanDesc), vp, C.POINTER(A.Result)]
     lib.mcg_price_european_noalloc.restype = C.c_int
     lib.mcg_measure_fp64_peak.argtypes = [vp, C.POINTER(dbl)]
@@ -91,6 +96,34 @@ def library() -> C.CDLL:
 def check(status: int, error: A.ErrorRecord | None = None) -> None:
     if status != 0:
         raise EngineError(status, library().mcg_last_error().decode(), error)
+
+
+def surface_grid(surface, time_nodes, log_moneyness_nodes, floor: float = 1e-8, cap: float = 4.0):
+    """mcg_surface_local_variance_grid: (values[nt, nx], repairs)."""
+    import numpy as np
+    tn = np.ascontiguousarray(time_nodes, dtype=np.float64)
+    xn = np.ascontiguousarray(log_moneyness_nodes, dtype=np.float64)
+    out = np.zeros(len(tn) * len(xn))
+    rep = C.c_uint32()
+    dp = C.POINTER(C.c_double)
+    d = surface.desc()
+    check(library().mcg_surface_local_variance_grid(C.byref(d), tn.ctypes.data_as(dp), len(tn),
+                                                     xn.ctypes.data_as(dp), len(xn), floor, cap,
+                                                     out.ctypes.data_as(dp), C.byref(rep)))
+    return out.reshape(len(tn), len(xn)), rep.value
+
+
+def surface_total_variance(surface, times, log_moneyness):
+    """mcg_surface_total_variance: (n, 4) array of w, w_k, w_kk, w_t."""
+    import numpy as np
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    k = np.ascontiguousarray(log_moneyness, dtype=np.float64)
+    out = np.zeros(4 * len(t))
+    dp = C.POINTER(C.c_double)
+    d = surface.desc()
+    check(library().mcg_surface_total_variance(C.byref(d), t.ctypes.data_as(dp), k.ctypes.data_as(dp), len(t),
+                                                out.ctypes.data_as(dp)))
+    return out.reshape(len(t), 4)
 
 
 def lsm_price(spec, lsm, stopping: bool = False, stream: int = 0) -> A.LsmBuffers:

@@ -52,6 +52,46 @@ class LocalVarianceSpec:
 
 
 @dataclass
+class SurfaceSpec:
+    """An implied-variance surface (mcg_surface_desc): standard SSVI with a
+    PCHIP theta curve and power-law or Heston-like phi
+    (crates/pricing/src/market/ssvi.rs), or eSSVI slices
+    (crates/pricing/src/market/essvi.rs)."""
+
+    kind: int
+    theta_times: Sequence[float] = ()
+    theta_values: Sequence[float] = ()
+    terminal_theta_slope: float = 0.0
+    rho: float = 0.0
+    eta: float = 0.0
+    gamma: float = 0.0
+    lam: float = 0.0
+    slice_times: Sequence[float] = ()
+    slice_thetas: Sequence[float] = ()
+    slice_psis: Sequence[float] = ()
+    slice_rho_psis: Sequence[float] = ()
+    _keep: list = field(default_factory=list, repr=False)
+
+    def desc(self) -> A.SurfaceDesc:
+        keep = self._keep
+        keep.clear()
+        d = A.SurfaceDesc()
+        d.kind = self.kind
+        arrays = {}
+        for name in ("theta_times", "theta_values", "slice_times", "slice_thetas", "slice_psis", "slice_rho_psis"):
+            values = getattr(self, name)
+            arrays[name] = _f64(values) if len(values) else None
+            keep.append(arrays[name])
+            setattr(d, name, _ptr(arrays[name]))
+        d.theta_count = len(self.theta_times)
+        d.slice_count = len(self.slice_times)
+        d.terminal_theta_slope = self.terminal_theta_slope
+        d.rho, d.eta, d.gamma, d.lambda_ = self.rho, self.eta, self.gamma, self.lam
+        keep.append(d)
+        return d
+
+
+@dataclass
 class PlanSpec:
     observation_times: Sequence[float]
     products: Sequence[ProductSpec]

@@ -13,6 +13,9 @@ are committed; the tests only read them.
   the 3 x 5 local-variance grid requests (pseudo and RQMC, price-only and
   Delta/Gamma/Vega) with both platforms' values, standard errors and
   variance bits.
+* surfaces.json            -- fixtures/local-vol/reference-cases-v0.1.json: the standard SSVI
+  (power-law and Heston-like phi), eSSVI interpolation and constant-volatility
+  Dupire cases (70-digit decimal values).
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
   the American put requests (pseudo and RQMC, training and valuation engines,
   LSM configuration) with the fitted decision models, exercise counts,
@@ -116,6 +119,14 @@ def local_volatility():
               open(os.path.join(OUT, "replay_local_vol.json"), "w"), indent=1)
 
 
+def surfaces():
+    src = os.path.join(REF, "fixtures/local-vol/reference-cases-v0.1.json")
+    d = json.load(open(src))
+    keep = {k: d[k] for k in ("standard_ssvi", "essvi_interpolation", "constant_vol_dupire")}
+    keep["source"] = "fixtures/local-vol/reference-cases-v0.1.json"
+    json.dump(keep, open(os.path.join(OUT, "surfaces.json"), "w"), indent=1)
+
+
 def analytical():
     src = os.path.join(REF, "fixtures/acceptance/european_bs_analytical.csv")
     rows = list(csv.DictReader(open(src)))
@@ -205,4 +216,5 @@ if __name__ == "__main__":
     path_dependence()
     early_exercise()
     local_volatility()
+    surfaces()
     print("golden fixtures written to", OUT)

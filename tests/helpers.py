@@ -60,6 +60,10 @@ def oracle():
     lib.oracle_last_error.restype = C.c_char_p
     lib.oracle_ssvi_grid.argtypes = [dp, dp, u32, dbl, dbl, dbl, dbl, dp, u32, dp, u32, dbl, dbl, dp]
     lib.oracle_ssvi_grid.restype = C.c_int
+    lib.oracle_surface_grid.argtypes = [C.POINTER(A.SurfaceDesc), dp, u32, dp, u32, dbl, dbl, dp]
+    lib.oracle_surface_grid.restype = C.c_int
+    lib.oracle_surface_total_variance.argtypes = [C.POINTER(A.SurfaceDesc), dbl, dbl, dp]
+    lib.oracle_surface_total_variance.restype = C.c_int
     lib.oracle_piecewise_sinh_nodes.argtypes = [dbl, dbl, u32, u32, dbl, dbl, dp]
     lib.oracle_piecewise_sinh_nodes.restype = C.c_int
     lib.oracle_smoothing.argtypes = [dbl, dbl, dp]

@@ -47,7 +47,7 @@ STRUCTS = {
     "mcg_estimate": A.Estimate, "mcg_product_result": A.ProductResult,
     "mcg_error_record": A.ErrorRecord, "mcg_result": A.Result,
     "mcg_lsm_desc": A.LsmDesc, "mcg_lsm_date_model": A.LsmDateModel, "mcg_lsm_result": A.LsmResult,
-    "mcg_book_options": A.BookOptions, "mcg_book_report": A.BookReport,
+    "mcg_book_options": A.BookOptions, "mcg_book_report": A.BookReport, "mcg_surface_desc": A.SurfaceDesc,
 }
 
 
@@ -56,7 +56,8 @@ def test_ctypes_layout_matches_c_compiler():
     for cname, cls in STRUCTS.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
         for field, _ in cls._fields_:
-            lines.append(f'printf("{cname}.{field} %zu\\n", offsetof({cname}, {field}));')
+            # a trailing underscore keeps a C name that is a Python keyword (lambda)
+            lines.append(f'printf("{cname}.{field} %zu\\n", offsetof({cname}, {field.rstrip("_")}));')
     lines.append("return 0;}")
     with tempfile.TemporaryDirectory() as d:
         src, exe = os.path.join(d, "layout.c"), os.path.join(d, "layout")
