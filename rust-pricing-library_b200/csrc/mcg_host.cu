@@ -41,6 +41,7 @@ cudaError_t launch_bs_path(const DevicePlan& P, bool single_terminal, uint64_t u
 __global__ void scramble_table_kernel(const uint32_t*, uint32_t, uint32_t, uint32_t, uint64_t, uint32_t*,
                                       uint32_t*);
 __global__ void reduce_tiles_kernel(const StatRecord*, uint32_t, uint32_t, StatRecord*);
+__global__ void scramble_low_kernel(const uint32_t*, uint32_t, uint32_t*);
 __global__ void philox_normals_kernel(uint64_t, uint64_t, uint64_t, uint32_t, uint32_t, double*);
 __global__ void rqmc_words_kernel(const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint64_t,
                                   uint64_t, uint32_t*);
@@ -352,7 +353,7 @@ struct mcg_plan {
     DeviceArray<double> node_time, dt, sqrt_dt, inv_sqrt_dt, time_weight, fwd, ratio, obs_time,
         obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, weights;
     DeviceArray<int32_t> obs_of_node, time_cell;
-    DeviceArray<uint32_t> scr_dirs, scr_shift, directions;
+    DeviceArray<uint32_t> scr_dirs, scr_shift, scr_low, directions;
     DeviceArray<StatRecord> partials, records;
     DeviceArray<ErrorWord> error;
     uint32_t tiles = 0;
@@ -387,6 +388,7 @@ struct mcg_plan {
         time_cell.release();
         scr_dirs.release();
         scr_shift.release();
+        scr_low.release();
         directions.release();
         partials.release();
         records.release();
@@ -759,6 +761,13 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         MCG_CUDA(cudaDeviceSynchronize());
         P.scr_dirs = plan.scr_dirs.ptr;
         P.scr_shift = plan.scr_shift.ptr;
+        {
+            const uint32_t rows = P.scramble_count * P.dimension;
+            MCG_CUDA(plan.scr_low.alloc(static_cast<size_t>(rows) * 32u));
+            scramble_low_kernel<<<(rows * 32u + 127) / 128, 128>>>(plan.scr_dirs.ptr, rows, plan.scr_low.ptr);
+            MCG_CUDA(cudaGetLastError());
+            P.scr_low = plan.scr_low.ptr;
+        }
     }
     (void)steps;
     // Reduction buffers (a book trade shares the book's).

@@ -87,6 +87,23 @@ struct NormalSource {
     }
 
     __device__ __forceinline__ double normal(uint32_t dim) { return as241(open_unit(word(dim))); }
+
+    // RQMC word with the whole warp: the 32 lanes hold 32 consecutive points
+    // of one 32-aligned block, so gray(p) = gray(p & ~31) ^ gray(p & 31) with
+    // the first part common to the warp.  Lane b contributes table word b
+    // where bit b of the common part is set (one coalesced load and one XOR
+    // reduction); the lane part is the precomputed low word of its lane.
+    // Bit-identical to word(); every lane of the warp must call it.
+    const uint32_t* low;   // this scramble's [dim][32] low words
+    uint32_t high_gray;    // gray(p & ~31), common to the warp
+    uint32_t lane_low;     // p & 31
+    __device__ __forceinline__ uint32_t word_warp(uint32_t dim) {
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t v = __ldg(dirs + static_cast<size_t>(dim) * 32u + lane);
+        const uint32_t h = __reduce_xor_sync(0xffffffffu, (high_gray >> lane) & 1u ? v : 0u);
+        return __ldg(shift + dim) ^ h ^ __ldg(low + static_cast<size_t>(dim) * 32u + lane_low);
+    }
+    __device__ __forceinline__ double normal_warp(uint32_t dim) { return as241(open_unit(word_warp(dim))); }
 };
 
 // ------------------------------------------------------- grid interpolation

@@ -15,41 +15,35 @@
 
 namespace mcg {
 
-template <int E, int NP>
-__global__ void __launch_bounds__(kThreads) lv_path_kernel(const DevicePlan P, uint64_t unit_begin,
+// Occupancy: one evolution with at most two products fits 6 CTAs of 128
+// threads (<= 80 registers) without spills, 5 with a continuous barrier; the
+// multi-evolution (antithetic, CRN) kernels keep their registers.  The grid
+// values are read through L1 (24.8 KB for 31 x 100), so shared memory holds
+// only the x nodes and the bridge slots and does not limit occupancy.
+template <int E, int NP, int RQ, int CB>
+__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (CB == 0 ? 6 : 5) : 1) lv_path_kernel(const DevicePlan P, uint64_t unit_begin,
                                                            StatRecord* partials, uint32_t mask,
                                                            ErrorWord* err, int detail) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = static_cast<int>(P.nx);
-    const size_t nv = static_cast<size_t>(P.nt) * P.nx;
-    double* s_v = reinterpret_cast<double*>(smem_raw);
-    double* s_x = s_v + nv;
+    double* s_x = reinterpret_cast<double*>(smem_raw);
     long long* s_xk = reinterpret_cast<long long*>(s_x + nx);
     double* s_w = reinterpret_cast<double*>(s_xk + nx);  // bridge slots [slot][thread]
     Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(P.slot_count) * kThreads);
-    for (size_t i = threadIdx.x; i < nv; i += kThreads) s_v[i] = P.grid_v[i];
     for (int i = threadIdx.x; i < nx; i += kThreads) {
         s_x[i] = P.grid_x[i];
         s_xk[i] = total_key(P.grid_x[i]);
     }
     __syncthreads();
-    const GridView g{s_v, s_x, s_xk, nx};
+    const GridView g{P.grid_v, s_x, s_xk, nx};  // grid values through L1
     const uint32_t scramble = blockIdx.y;
     const uint64_t point = unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
     const bool valid = point < unit_begin + (detail ? 1 : P.units) && point < P.units;
     StatRecord* tile_out = partials + (static_cast<size_t>(scramble) * gridDim.x + blockIdx.x) * P.product_count * kComponents;
-    lv_tile<E, NP>(P, g, s_w, s_red, scramble, point, valid, tile_out, mask, err, detail);
+    lv_tile<E, NP, RQ, CB>(P, g, s_w, s_red, scramble, point, valid, tile_out, mask, err, detail,
+                           (unit_begin & 31u) == 0);
 }
 
-
-template __global__ void lv_path_kernel<1, 1>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
-template __global__ void lv_path_kernel<1, 2>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
-template __global__ void lv_path_kernel<1, 4>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
-template __global__ void lv_path_kernel<2, 1>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
-template __global__ void lv_path_kernel<2, 2>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
-template __global__ void lv_path_kernel<3, 1>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
-template __global__ void lv_path_kernel<3, 2>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
-template __global__ void lv_path_kernel<6, 1>(const DevicePlan, uint64_t, StatRecord*, uint32_t, ErrorWord*, int);
 
 // Early-exercise path store under local volatility: the Log-Euler paths of
 // lv_tile on the base runtime (both antithetic signs, E = pairs), their state
@@ -166,7 +160,7 @@ cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t un
     const int E = pairs * per;
     evolutions_out = E;
     const int np = static_cast<int>(P.product_count);
-    const size_t smem = (static_cast<size_t>(P.nt) * P.nx + 2 * P.nx) * sizeof(double) +
+    const size_t smem = (2 * static_cast<size_t>(P.nx)) * sizeof(double) +
                         static_cast<size_t>(P.slot_count) * kThreads * sizeof(double) +
                         4 * kComponents * sizeof(Stat);
     const dim3 grid(static_cast<unsigned>((units + kThreads - 1) / kThreads), scrambles);
@@ -177,14 +171,26 @@ cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t un
         kernel<<<grid, kThreads, smem, stream>>>(P, unit_begin, partials, mask, err, detail);
         return cudaGetLastError();
     };
-    if (E == 1 && np == 1) return go(lv_path_kernel<1, 1>);
-    if (E == 1 && np == 2) return go(lv_path_kernel<1, 2>);
-    if (E == 1 && np <= 4) return go(lv_path_kernel<1, 4>);
-    if (E == 2 && np == 1) return go(lv_path_kernel<2, 1>);
-    if (E == 2 && np == 2) return go(lv_path_kernel<2, 2>);
-    if (E == 3 && np == 1) return go(lv_path_kernel<3, 1>);
-    if (E == 3 && np == 2) return go(lv_path_kernel<3, 2>);
-    if (E == 6 && np == 1) return go(lv_path_kernel<6, 1>);
+    bool cb = false;
+    for (int k = 0; k < np; ++k) cb |= P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+    const bool rq = P.engine == MCG_ENGINE_RQMC;
+    // (evolutions, products) x (engine, continuous barrier) instantiations
+#define MCG_LV_PICK(EE, NN)                                                           \
+    do {                                                                              \
+        if (rq && cb) return go(lv_path_kernel<EE, NN, 1, 1>);                        \
+        if (rq) return go(lv_path_kernel<EE, NN, 1, 0>);                              \
+        if (cb) return go(lv_path_kernel<EE, NN, 0, 1>);                              \
+        return go(lv_path_kernel<EE, NN, 0, 0>);                                      \
+    } while (0)
+    if (E == 1 && np == 1) MCG_LV_PICK(1, 1);
+    if (E == 1 && np == 2) MCG_LV_PICK(1, 2);
+    if (E == 1 && np <= 4) MCG_LV_PICK(1, 4);
+    if (E == 2 && np == 1) MCG_LV_PICK(2, 1);
+    if (E == 2 && np == 2) MCG_LV_PICK(2, 2);
+    if (E == 3 && np == 1) MCG_LV_PICK(3, 1);
+    if (E == 3 && np == 2) MCG_LV_PICK(3, 2);
+    if (E == 6 && np == 1) MCG_LV_PICK(6, 1);
+#undef MCG_LV_PICK
     return cudaErrorNotSupported;
 }
 

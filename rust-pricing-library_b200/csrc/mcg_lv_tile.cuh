@@ -6,7 +6,8 @@
 //
 // Per unit: normals (Philox or scrambled Sobol) -> time-ordered Brownian-bridge
 // program -> Log-Euler steps on the forward-normalised state
-//   x = ln(f / F_i),  v = bilinear(t_i, x),  f <- f * (F_{i+1}/F_i) * exp(-v dt/2 + sqrt(v) sqrt(dt) z)
+//   x = ln(f / F_i),  v = bilinear(t_i, x),  f <- f * (F_{i+1}/F_i) * exp(-v dt/2 + sqrt(v) sqrt(dt) z),
+//   with x advanced by the same exponent (x <- x - v dt/2 + sqrt(v) sqrt(dt) z)
 // (crates/pricing/src/engine/processes/local_vol.rs:459-619) for up to three
 // spot runtimes (base, S-h, S+h for CRN Delta/Gamma,
 // crates/pricing/src/engine/risk/pathwise_local_vol.rs:332-355) and both
@@ -34,22 +35,34 @@ __device__ __forceinline__ double ev_sign(int e) {
 // One 128-unit tile of Log-Euler paths: unit `point` of scramble `scramble`
 // per thread, the grid `g` and the bridge slots `s_w` ([slot][thread]) in
 // shared memory, the CTA's records written at tile_out[k * kComponents + c].
-template <int E, int NP>
+// RQ / CB: 1 or 0 specialise the kernel on the engine (RQMC or Philox) and
+// on whether any product is a continuous barrier, so the code and state of
+// the other case are compiled out; -1 decides both from the plan at run
+// time.  The arithmetic is the same either way.
+template <int E, int NP, int RQ = -1, int CB = -1>
 __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, double* s_w, Stat* s_red,
                                         uint32_t scramble, uint64_t point, bool valid, StatRecord* tile_out,
-                                        uint32_t mask, ErrorWord* err, int detail) {
+                                        uint32_t mask, ErrorWord* err, int detail, bool warp_sobol = false) {
     const uint64_t unit = valid ? point : 0;
 
     NormalSource ns;
-    ns.rqmc = P.engine == MCG_ENGINE_RQMC;
+    ns.rqmc = RQ < 0 ? P.engine == MCG_ENGINE_RQMC : RQ != 0;
     ns.seed = P.seed;
     ns.unit = unit;
     ns.gray = static_cast<uint32_t>(unit ^ (unit >> 1));
     ns.dirs = P.scr_dirs ? P.scr_dirs + static_cast<size_t>(scramble) * P.dimension * 32u : nullptr;
     ns.shift = P.scr_shift ? P.scr_shift + static_cast<size_t>(scramble) * P.dimension : nullptr;
     ns.cached_block = 0xffffffffu;
+    // Warp-cooperative Sobol words when the warp's points form one aligned block of 32.
+    const bool wsob = warp_sobol && ns.rqmc;
+    if (wsob) {
+        const uint32_t q = static_cast<uint32_t>(point) & ~31u;
+        ns.high_gray = q ^ (q >> 1);
+        ns.lane_low = static_cast<uint32_t>(point) & 31u;
+        ns.low = P.scr_low + static_cast<size_t>(scramble) * P.dimension * 32u;
+    }
 
-    double f[E], prev_f[E], prev_v[E];
+    double f[E], xs[E], prev_f[E], prev_v[E];
     int hint[E];
     ProductAcc acc[E][NP];
     bool failed = false;
@@ -59,13 +72,14 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         f[e] = P.spot_variant[ev_which<E>(e)];
+        xs[e] = 0.0;  // ln(f / F_0): F_0 is the spot of the runtime
         prev_f[e] = f[e];
         prev_v[e] = 0.0;
         hint[e] = 0;
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             acc_init(acc[e][k]);
-            if (k < static_cast<int>(P.product_count) &&
+            if (CB != 0 && k < static_cast<int>(P.product_count) &&
                 P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
                 barrier_begin(P.products[k], acc[e][k], P.smoothing, f[e], failed);
         }
@@ -79,11 +93,11 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             continue;
         }
         if (op.kind == kOpTerminal) {
-            w[op.out * kThreads] = op.sd * ns.normal(op.rank);
+            w[op.out * kThreads] = op.sd * (wsob ? ns.normal_warp(op.rank) : ns.normal(op.rank));
             continue;
         }
         if (op.kind == kOpInterior) {
-            const double z = ns.normal(op.rank);
+            const double z = wsob ? ns.normal_warp(op.rank) : ns.normal(op.rank);
             w[op.out * kThreads] =
                 op.wl * w[op.left * kThreads] + op.wr * w[op.right * kThreads] + op.sd * z;
             continue;
@@ -93,7 +107,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
         if (op.kind == kOpStep)
             shock = (w[op.right * kThreads] - w[op.left * kThreads]) * P.inv_sqrt_dt[s];
         else
-            shock = ns.normal(op.rank);
+            shock = wsob ? ns.normal_warp(op.rank) : ns.normal(op.rank);
         const int tc = P.time_cell[s];
         const double tw = P.time_weight[s];
         const double dt = P.dt[s];
@@ -102,11 +116,15 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int which = ev_which<E>(e);
-            const double* F = P.fwd + static_cast<size_t>(which) * (steps + 1);
             const double z = ev_sign<E>(e) * shock;
-            const double x = log(f[e] / F[s]);
+            // x = ln(f / F_s), carried by the steps' own exponents (the forward
+            // ratios cancel) in place of a division and a logarithm per step;
+            // it differs from the reference's ln(f / F_s) by rounding only
+            // (~1e-16 per step), and only through the interpolated variance.
+            // The state f itself follows the reference's recurrence.
+            const double x = xs[e];
             const double v = interp_variance(g, tc, tw, x, hint[e]);
-            if (s > 0) {
+            if (CB != 0 && s > 0) {
 #pragma unroll
                 for (int k = 0; k < NP; ++k)
                     if (k < static_cast<int>(P.product_count) &&
@@ -115,9 +133,13 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                                          prev_v[e], v, P.dt[s - 1], failed);
             }
             const double ratio = P.ratio[static_cast<size_t>(which) * steps + s];
-            const double e_factor = ratio * exp(-0.5 * v * dt + sqrt(v) * sq * z);
-            prev_f[e] = f[e];
-            prev_v[e] = v;
+            const double incr = -0.5 * v * dt + sqrt(v) * sq * z;
+            const double e_factor = ratio * exp(incr);
+            xs[e] += incr;
+            if (CB != 0) {
+                prev_f[e] = f[e];
+                prev_v[e] = v;
+            }
             f[e] *= e_factor;
             if (!(isfinite(f[e]) && f[e] > 0.0) && !fail_code) {
                 fail_code = MCG_ERR_NON_FINITE_STATE;
@@ -144,7 +166,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             price[e][k] = 0.0;
             if (k >= static_cast<int>(P.product_count)) continue;
             const ProductParams& pp = P.products[k];
-            if (pp.kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
+            if (CB != 0 && pp.kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
                 const double* F = P.fwd + static_cast<size_t>(which) * (steps + 1);
                 const double x = log(f[e] / F[steps]);
                 const double v = interp_variance(g, static_cast<int>(P.nt) - 2, 1.0, x, hint[e]);
@@ -200,7 +222,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
 #pragma unroll
         for (int c = 0; c < kComponents; ++c)
             vals[c] = kPairs == 2 ? (comp[0][c] + comp[1][c]) * 0.5 : comp[0][c];
-        if (P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
+        if (CB != 0 && P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
 #pragma unroll
             for (int q = 0; q < 8; ++q) vals[10 + q] = diag_src[k][q];
         }

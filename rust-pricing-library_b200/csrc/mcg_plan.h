@@ -99,6 +99,9 @@ struct DevicePlan {
     // RQMC: scrambled direction table [scramble][dim][32] and shifts [scramble][dim]
     const uint32_t* scr_dirs;
     const uint32_t* scr_shift;
+    // RQMC: per-lane low Gray-code words [scramble][dim][32]: for lane l the
+    // XOR of the table words of the set bits of gray(l)
+    const uint32_t* scr_low;
 
     // risk
     int32_t risk;          // BS: pathwise values with bumps

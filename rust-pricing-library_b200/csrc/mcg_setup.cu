@@ -53,6 +53,19 @@ __global__ void scramble_table_kernel(const uint32_t* directions, uint32_t dims,
     }
 }
 
+// Per-lane low Gray-code words: low[row][l] = XOR of table[row][b] over the
+// set bits b of gray(l), l < 32 (row = scramble * dims + dim).
+__global__ void scramble_low_kernel(const uint32_t* table, uint32_t rows, uint32_t* low) {
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= rows * 32u) return;
+    const uint32_t row = idx >> 5, l = idx & 31u;
+    const uint32_t g = l ^ (l >> 1);
+    uint32_t x = 0;
+    for (uint32_t b = 0; b < 5; ++b)
+        if ((g >> b) & 1u) x ^= table[static_cast<size_t>(row) * 32u + b];
+    low[idx] = x;
+}
+
 // Merge `tiles` records of one (scramble, slot): thread t folds tiles
 // t, t+256, ... in order, then a pairwise tree over the 256 threads.
 __global__ void reduce_tiles_kernel(const StatRecord* partials, uint32_t tiles, uint32_t slots,
