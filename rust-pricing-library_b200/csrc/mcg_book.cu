@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kThreads) book_kernel(const BookLaunch L) {
     DevicePlan& P = *reinterpret_cast<DevicePlan*>(smem_raw);
     double* s_v = reinterpret_cast<double*>(smem_raw + align16(sizeof(DevicePlan)));
     double* s_x = s_v + L.max_values;
-    long long* s_xk = reinterpret_cast<long long*>(s_x + L.max_nodes);
+    double* s_xk = s_x + L.max_nodes;  // reciprocal cell widths
     double* s_w = reinterpret_cast<double*>(s_xk + L.max_nodes);
     Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(L.max_slots) * kThreads);
     for (;;) {
@@ -52,11 +52,11 @@ __global__ void __launch_bounds__(kThreads) book_kernel(const BookLaunch L) {
             for (size_t i = threadIdx.x; i < nv; i += kThreads) s_v[i] = P.grid_v[i];
             for (int i = threadIdx.x; i < nx; i += kThreads) {
                 s_x[i] = P.grid_x[i];
-                s_xk[i] = total_key(P.grid_x[i]);
+                s_xk[i] = i + 1 < nx ? 1.0 / (P.grid_x[i + 1] - P.grid_x[i]) : 0.0;
             }
             __syncthreads();
         }
-        const GridView g{s_v, s_x, s_xk, nx};
+        const GridView g{s_v, s_x, nullptr, nx, s_xk};
         const uint32_t mask = L.masks[item.trade];
         ErrorWord* err = L.errors + item.trade;
         for (uint32_t t = 0; t < item.tiles; ++t) {

@@ -353,6 +353,7 @@ struct mcg_plan {
     DeviceArray<double> node_time, dt, sqrt_dt, inv_sqrt_dt, time_weight, fwd, ratio, obs_time,
         obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, weights;
     DeviceArray<int32_t> obs_of_node, time_cell;
+    DeviceArray<LvStep> lv_steps;
     DeviceArray<uint32_t> scr_dirs, scr_shift, scr_low, directions;
     DeviceArray<StatRecord> partials, records;
     DeviceArray<ErrorWord> error;
@@ -386,6 +387,7 @@ struct mcg_plan {
         weights.release();
         obs_of_node.release();
         time_cell.release();
+        lv_steps.release();
         scr_dirs.release();
         scr_shift.release();
         scr_low.release();
@@ -657,6 +659,13 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
             P.fwd_f = plan.fwd_f.ptr;
             P.ratio_f = plan.ratio_f.ptr;
             P.step_f = plan.step_f.ptr;
+        }
+        {
+            std::vector<LvStep> packed(steps);
+            for (uint32_t s = 0; s < steps; ++s)
+                packed[s] = LvStep{dtv[s], sq[s], isq[s], tw[s], ra[s], tc[s], oon[s + 1]};
+            MCG_CUDA(plan.lv_steps.upload(packed));
+            P.lv_steps = plan.lv_steps.ptr;
         }
         MCG_CUDA(plan.node_time.upload(nodes));
         MCG_CUDA(plan.dt.upload(dtv));

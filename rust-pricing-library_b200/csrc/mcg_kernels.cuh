@@ -113,11 +113,15 @@ struct NormalSource {
 // binary search under total_cmp), the time cell and weight of each step are
 // plan constants.
 struct GridView {
-    const double* v;        // nt x nx values (shared memory when they fit)
+    const double* v;        // nt x nx values (shared memory or global through L1)
     const double* x;        // nx nodes
     const long long* xkey;  // total-order keys of the nodes
     int nx;
+    const double* inv_dx;   // nx - 1 reciprocal cell widths (interp_variance_walk)
 };
+// A view carries either xkey (for interp_variance: the LSM path store and the
+// adjoint sweep) or inv_dx (for interp_variance_walk: the path tiles).
+
 
 __device__ __forceinline__ double interp_variance(const GridView& g, int tc, double tw, double xq,
                                                   int& hint) {
@@ -131,6 +135,28 @@ __device__ __forceinline__ double interp_variance(const GridView& g, int tc, dou
     const int c = min(max(count - 1, 0), g.nx - 2);
     hint = c;
     const double xw = (xv - g.x[c]) / (g.x[c + 1] - g.x[c]);
+    const double* row = g.v + static_cast<size_t>(tc) * g.nx;
+    const double* next = row + g.nx;
+    const double lower = row[c] * (1.0 - xw) + row[c + 1] * xw;
+    const double upper = next[c] * (1.0 - xw) + next[c + 1] * xw;
+    return lower * (1.0 - tw) + upper * tw;
+}
+
+// The path kernels' form of interp_variance: the same clamp, cell walk and
+// bilinear weights, with the walk comparing the nodes themselves (finite
+// nodes: the same cells as total_cmp, and at a node both neighbouring cells
+// give its value) and the x weight as a product with the reciprocal width.
+__device__ __forceinline__ double interp_variance_walk(const GridView& g, int tc, double tw, double xq,
+                                                       int& hint) {
+    double xv = xq;
+    if (xq < g.x[0]) xv = g.x[0];
+    else if (xq > g.x[g.nx - 1]) xv = g.x[g.nx - 1];
+    int count = min(hint + 1, g.nx);
+    while (count < g.nx && g.x[count] <= xv) ++count;
+    while (count > 0 && g.x[count - 1] > xv) --count;
+    const int c = min(max(count - 1, 0), g.nx - 2);
+    hint = c;
+    const double xw = (xv - g.x[c]) * g.inv_dx[c];
     const double* row = g.v + static_cast<size_t>(tc) * g.nx;
     const double* next = row + g.nx;
     const double lower = row[c] * (1.0 - xw) + row[c + 1] * xw;

@@ -15,27 +15,27 @@
 
 namespace mcg {
 
-// Occupancy: one evolution with at most two products fits 6 CTAs of 128
-// threads (<= 80 registers) without spills, 5 with a continuous barrier; the
+// Occupancy: one evolution with at most two products runs 7 CTAs of 128
+// threads (<= 72 registers; an 8-byte spill), 5 with a continuous barrier; the
 // multi-evolution (antithetic, CRN) kernels keep their registers.  The grid
 // values are read through L1 (24.8 KB for 31 x 100), so shared memory holds
 // only the x nodes and the bridge slots and does not limit occupancy.
 template <int E, int NP, int RQ, int CB>
-__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (CB == 0 ? 6 : 5) : 1) lv_path_kernel(const DevicePlan P, uint64_t unit_begin,
+__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (CB == 0 ? 7 : 5) : 1) lv_path_kernel(const DevicePlan P, uint64_t unit_begin,
                                                            StatRecord* partials, uint32_t mask,
                                                            ErrorWord* err, int detail) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = static_cast<int>(P.nx);
     double* s_x = reinterpret_cast<double*>(smem_raw);
-    long long* s_xk = reinterpret_cast<long long*>(s_x + nx);
-    double* s_w = reinterpret_cast<double*>(s_xk + nx);  // bridge slots [slot][thread]
+    double* s_idx = s_x + nx;                            // reciprocal cell widths
+    double* s_w = s_idx + nx;                            // bridge slots [slot][thread]
     Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(P.slot_count) * kThreads);
     for (int i = threadIdx.x; i < nx; i += kThreads) {
         s_x[i] = P.grid_x[i];
-        s_xk[i] = total_key(P.grid_x[i]);
+        s_idx[i] = i + 1 < nx ? 1.0 / (P.grid_x[i + 1] - P.grid_x[i]) : 0.0;
     }
     __syncthreads();
-    const GridView g{P.grid_v, s_x, s_xk, nx};  // grid values through L1
+    const GridView g{P.grid_v, s_x, nullptr, nx, s_idx};  // grid values through L1
     const uint32_t scramble = blockIdx.y;
     const uint64_t point = unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
     const bool valid = point < unit_begin + (detail ? 1 : P.units) && point < P.units;

@@ -103,16 +103,17 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             continue;
         }
         const uint32_t s = static_cast<uint32_t>(op.step);
+        const LvStep st = P.lv_steps[s];
         double shock;
         if (op.kind == kOpStep)
-            shock = (w[op.right * kThreads] - w[op.left * kThreads]) * P.inv_sqrt_dt[s];
+            shock = (w[op.right * kThreads] - w[op.left * kThreads]) * st.inv_sqrt_dt;
         else
             shock = wsob ? ns.normal_warp(op.rank) : ns.normal(op.rank);
-        const int tc = P.time_cell[s];
-        const double tw = P.time_weight[s];
-        const double dt = P.dt[s];
-        const double sq = P.sqrt_dt[s];
-        const int32_t obs = P.obs_of_node[s + 1];
+        const int tc = st.time_cell;
+        const double tw = st.time_weight;
+        const double dt = st.dt;
+        const double sq = st.sqrt_dt;
+        const int32_t obs = st.obs_next;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int which = ev_which<E>(e);
@@ -123,7 +124,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             // (~1e-16 per step), and only through the interpolated variance.
             // The state f itself follows the reference's recurrence.
             const double x = xs[e];
-            const double v = interp_variance(g, tc, tw, x, hint[e]);
+            const double v = interp_variance_walk(g, tc, tw, x, hint[e]);
             if (CB != 0 && s > 0) {
 #pragma unroll
                 for (int k = 0; k < NP; ++k)
@@ -132,7 +133,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                         barrier_interval(P.products[k], acc[e][k], P.smoothing, prev_f[e], f[e],
                                          prev_v[e], v, P.dt[s - 1], failed);
             }
-            const double ratio = P.ratio[static_cast<size_t>(which) * steps + s];
+            const double ratio = which == 0 ? st.ratio : P.ratio[static_cast<size_t>(which) * steps + s];
             const double incr = -0.5 * v * dt + sqrt(v) * sq * z;
             const double e_factor = ratio * exp(incr);
             xs[e] += incr;
@@ -169,7 +170,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             if (CB != 0 && pp.kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
                 const double* F = P.fwd + static_cast<size_t>(which) * (steps + 1);
                 const double x = log(f[e] / F[steps]);
-                const double v = interp_variance(g, static_cast<int>(P.nt) - 2, 1.0, x, hint[e]);
+                const double v = interp_variance_walk(g, static_cast<int>(P.nt) - 2, 1.0, x, hint[e]);
                 barrier_interval(pp, acc[e][k], P.smoothing, prev_f[e], f[e], prev_v[e], v,
                                  P.dt[steps - 1], failed);
                 double diag[8];

@@ -41,6 +41,14 @@ struct Op {
     double wl, wr, sd;
 };
 
+// Per-step constants of the base runtime, one 48-byte record per step (three
+// 16-byte loads, read uniformly by a warp).
+struct __align__(16) LvStep {
+    double dt, sqrt_dt, inv_sqrt_dt, time_weight, ratio;
+    int32_t time_cell;
+    int32_t obs_next;  // observation index of node s + 1, or -1
+};
+
 struct ProductParams {
     int32_t kind, side;
     double strike, notional;
@@ -81,6 +89,7 @@ struct DevicePlan {
     const float* fwd_f;          // FP32 bulk: reciprocal base forward normalisers 1/F_i (steps + 1)
     const float* ratio_f;        // FP32 bulk: base forward ratios F_{i+1}/F_i (steps)
     const float4* step_f;        // FP32 bulk: per step {dt, sqrt(dt), time weight, 1/sqrt(dt)}
+    const LvStep* lv_steps;      // LV: the base runtime's per-step constants, packed
 
     // Black--Scholes observation data (observation_count entries)
     const double* obs_time;
