@@ -83,9 +83,11 @@ __device__ __forceinline__ float interp_f32(const float* v, const float* xs, int
     return lower + (upper - lower) * tw;
 }
 
-template <int E, int NP>
-__global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P, StatRecord* partials, uint32_t mask,
-                                                             ErrorWord* err) {
+// RQ / CB specialise on the engine and on "any continuous barrier", as the
+// FP64 kernel does; one evolution runs 8 CTAs of 128 threads per SM.
+template <int E, int NP, int RQ, int CB>
+__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2 && CB == 0) ? 8 : 1)
+    lv32_path_kernel(const DevicePlan P, StatRecord* partials, uint32_t mask, ErrorWord* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = static_cast<int>(P.nx);
     const int nv = static_cast<int>(P.nt * P.nx);
@@ -102,13 +104,21 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
     const bool valid = point < P.units;
     const uint64_t unit = valid ? point : 0;
     NormalSource ns;
-    ns.rqmc = P.engine == MCG_ENGINE_RQMC;
+    ns.rqmc = RQ != 0;
     ns.seed = P.seed;
     ns.unit = unit;
     ns.gray = static_cast<uint32_t>(unit ^ (unit >> 1));
     ns.dirs = P.scr_dirs ? P.scr_dirs + static_cast<size_t>(scramble) * P.dimension * 32u : nullptr;
     ns.shift = P.scr_shift ? P.scr_shift + static_cast<size_t>(scramble) * P.dimension : nullptr;
     ns.cached_block = 0xffffffffu;
+    // warp-cooperative Sobol words (the launch's points are 32-aligned per warp)
+    if (RQ) {
+        const uint32_t q = static_cast<uint32_t>(point) & ~31u;
+        ns.high_gray = q ^ (q >> 1);
+        ns.lane_low = static_cast<uint32_t>(point) & 31u;
+        ns.low = P.scr_low + static_cast<size_t>(scramble) * P.dimension * 32u;
+    }
+    auto word = [&](uint32_t dim) { return RQ ? ns.word_warp(dim) : ns.word(dim); };
 
     // The state is the forward-normalised spot g = f / F_i, a martingale
     // (f_{i+1} / F_{i+1} = (f_i / F_i) exp(-v dt / 2 + sqrt(v dt) z)): no FP32
@@ -129,7 +139,7 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             acc_init(acc[e][k]);
-            if (k < static_cast<int>(P.product_count) && P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
+            if (CB && k < static_cast<int>(P.product_count) && P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
                 barrier_begin(P.products[k], acc[e][k], P.smoothing, P.spot, failed);
         }
     }
@@ -142,11 +152,11 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
             continue;
         }
         if (op.kind == kOpTerminal) {
-            w[op.out * kThreads] = static_cast<float>(op.sd) * normal_from_word(ns.word(op.rank));
+            w[op.out * kThreads] = static_cast<float>(op.sd) * normal_from_word(word(op.rank));
             continue;
         }
         if (op.kind == kOpInterior) {
-            const float z = normal_from_word(ns.word(op.rank));
+            const float z = normal_from_word(word(op.rank));
             w[op.out * kThreads] = static_cast<float>(op.wl) * w[op.left * kThreads] +
                                    static_cast<float>(op.wr) * w[op.right * kThreads] + static_cast<float>(op.sd) * z;
             continue;
@@ -156,7 +166,7 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
         if (op.kind == kOpStep)
             shock = (w[op.right * kThreads] - w[op.left * kThreads]) * P.step_f[s].w;
         else
-            shock = normal_from_word(ns.word(op.rank));
+            shock = normal_from_word(word(op.rank));
         const int tc = P.time_cell[s];
         const float4 kc = P.step_f[s];
         const float dt = kc.x, sq = kc.y, tw = kc.z;
@@ -167,7 +177,7 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
             const float z = (e == 0) ? shock : -shock;
             const float x = __logf(f[e]);
             const float v = interp_f32(s_v, s_x, nx, tc, tw, x, hint[e]);
-            if (s > 0) {
+            if (CB && s > 0) {
 #pragma unroll
                 for (int k = 0; k < NP; ++k)
                     if (k < static_cast<int>(P.product_count) &&
@@ -175,8 +185,10 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
                         barrier_interval(P.products[k], acc[e][k], P.smoothing, prev_f[e],
                                          static_cast<double>(f[e]) * fwd_prev, prev_v[e], v, P.dt[s - 1], failed);
             }
-            prev_f[e] = static_cast<float>(static_cast<double>(f[e]) * fwd_prev);
-            prev_v[e] = v;
+            if (CB) {
+                prev_f[e] = static_cast<float>(static_cast<double>(f[e]) * fwd_prev);
+                prev_v[e] = v;
+            }
             f[e] *= expf(-0.5f * v * dt + sqrtf(v) * sq * z);
             bad_state |= !(isfinite(f[e]) && f[e] > 0.0f);
             if (obs >= 0) {
@@ -197,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
             price[e][k] = 0.0;
             if (k >= static_cast<int>(P.product_count)) continue;
             const ProductParams& pp = P.products[k];
-            if (pp.kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
+            if (CB && pp.kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
                 const float x = __logf(f[e]);
                 const float v = interp_f32(s_v, s_x, nx, static_cast<int>(P.nt) - 2, 1.0f, x, hint[e]);
                 const double terminal = static_cast<double>(f[e]) * P.fwd[steps];
@@ -219,7 +231,7 @@ __global__ void __launch_bounds__(kThreads) lv32_path_kernel(const DevicePlan P,
 #pragma unroll
         for (int c = 0; c < kComponents; ++c) vals[c] = 0.0;
         vals[MCG_PRICE] = E == 2 ? (price[0][k] + price[E - 1][k]) * 0.5 : price[0][k];
-        if (P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
+        if (CB && P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
 #pragma unroll
             for (int q = 0; q < 8; ++q) vals[10 + q] = diag_src[k][q];
         }
@@ -246,12 +258,23 @@ cudaError_t launch_lv32_path(const DevicePlan& P, StatRecord* partials, uint32_t
         kernel<<<grid, kThreads, smem, stream>>>(P, partials, mask, err);
         return cudaGetLastError();
     };
-    if (E == 1 && np == 1) return go(lv32_path_kernel<1, 1>);
-    if (E == 1 && np == 2) return go(lv32_path_kernel<1, 2>);
-    if (E == 1 && np <= 4) return go(lv32_path_kernel<1, 4>);
-    if (E == 2 && np == 1) return go(lv32_path_kernel<2, 1>);
-    if (E == 2 && np == 2) return go(lv32_path_kernel<2, 2>);
-    if (E == 2 && np <= 4) return go(lv32_path_kernel<2, 4>);
+    bool cb = false;
+    for (int k = 0; k < np; ++k) cb |= P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+    const bool rq = P.engine == MCG_ENGINE_RQMC;
+#define MCG_LV32_PICK(EE, NN)                                                         \
+    do {                                                                              \
+        if (rq && cb) return go(lv32_path_kernel<EE, NN, 1, 1>);                      \
+        if (rq) return go(lv32_path_kernel<EE, NN, 1, 0>);                            \
+        if (cb) return go(lv32_path_kernel<EE, NN, 0, 1>);                            \
+        return go(lv32_path_kernel<EE, NN, 0, 0>);                                    \
+    } while (0)
+    if (E == 1 && np == 1) MCG_LV32_PICK(1, 1);
+    if (E == 1 && np == 2) MCG_LV32_PICK(1, 2);
+    if (E == 1 && np <= 4) MCG_LV32_PICK(1, 4);
+    if (E == 2 && np == 1) MCG_LV32_PICK(2, 1);
+    if (E == 2 && np == 2) MCG_LV32_PICK(2, 2);
+    if (E == 2 && np <= 4) MCG_LV32_PICK(2, 4);
+#undef MCG_LV32_PICK
     return cudaErrorNotSupported;
 }
 
