@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
                     help="path arithmetic of the timed workload (f32: FP32 path bulk)")
     ap.add_argument("--secondary", default="all",
-                    help="comma list of secondary measurements: early_exercise, book, f32; all; none")
+                    help="comma list of secondary measurements: early_exercise, book, f32, adjoint; all; none")
+    ap.add_argument("--adjoint-paths", type=int, default=1 << 20)
     ap.add_argument("--lsm-units", type=int, default=1 << 20)
     ap.add_argument("--book-trades", type=int, default=4096)
     ap.add_argument("--book-units", type=int, default=1 << 16)
@@ -211,6 +212,56 @@ def book_secondary(trades: int, units: int):
     out["plain_one_plan_per_call"] = {"trades": n, "device_ms": dev_plain, "wall_ms": wall_plain * 1e3,
                                       "path_steps_per_s": steps_plain / wall_plain}
     out["batched_over_plain_throughput"] = out["path_steps_per_s"] / (steps_plain / wall_plain)
+    return out
+
+
+def time_to_pct(ms: float, se: float, value: float) -> float:
+    """Device time to a 1 % standard error of a Greek (SE <= 0.01 |value|)."""
+    target = 1e-2 * abs(value)
+    return ms * (se / target) ** 2 if target > 0 else float("inf")
+
+
+def adjoint_secondary(paths: int = 1 << 20):
+    """The adjoint configuration: a continuous down-and-out call (B = 80,
+    rebate 1) under the SSVI local-variance grid, compact-C2 smoothing 0.5,
+    `paths` pseudo paths x 252 daily steps.
+      adjoint: one forward pass and one reverse sweep give the price, the
+        adjoint Delta, the Vega and all 3100 grid-node sensitivities;
+      adjoint_full: CRN Delta/Gamma, adjoint Delta, bumped-adjoint Gamma,
+        Vega and the nodes (three spot runtimes forward and reversed);
+      plain: the price with CRN Delta/Gamma (the reference's local-volatility
+        Delta and Gamma are central bumps); a node sensitivity without the
+        adjoint is two bumped revaluations of the price."""
+    from rust_pricing_b200 import _native as N, workloads as W
+    out = {"workload": f"continuous down-and-out call under SSVI local vol, compact-C2 0.5, {paths} pseudo "
+                       "paths x 252 steps"}
+    configs = {"adjoint": dict(delta=False, vega=True), "adjoint_full": dict(delta=True, vega=True),
+               "plain": dict(delta=True, vega=False), "price_only": dict(delta=False, vega=False)}
+    runs = {}
+    for name, c in configs.items():
+        spec = W.local_vol_adjoint(gpu_grid, paths=paths, risk=c["delta"])
+        spec.request_vega = spec.request_local_vega_nodes = c["vega"]
+        with N.Plan(spec) as plan:
+            plan.evaluate()
+            runs[name] = plan.evaluate()
+    for name in ("adjoint", "adjoint_full"):
+        r = runs[name]
+        p, ms = r.products[0], r.result.device_ms
+        out[name] = {"device_ms": ms, "price": p.price.value, "adjoint_delta": p.adjoint_delta.value,
+                     "adjoint_delta_se": p.adjoint_delta.standard_error, "vega": p.vega.value,
+                     "vega_se": p.vega.standard_error,
+                     "ms_to_1pct_delta": time_to_pct(ms, p.adjoint_delta.standard_error, p.adjoint_delta.value),
+                     "ms_to_1pct_vega": time_to_pct(ms, p.vega.standard_error, p.vega.value),
+                     "node_sensitivities": len(r.node_estimates) if r.node_estimates is not None else 0}
+    pl, po = runs["plain"], runs["price_only"]
+    pp, ms_p, ms_0 = pl.products[0], pl.result.device_ms, po.result.device_ms
+    out["plain"] = {"device_ms": ms_p, "price": pp.price.value, "crn_delta": pp.delta.value,
+                    "crn_delta_se": pp.delta.standard_error,
+                    "ms_to_1pct_delta": time_to_pct(ms_p, pp.delta.standard_error, pp.delta.value),
+                    "price_only_ms": ms_0, "ms_for_3000_node_sensitivities_by_bumping": 2 * 3000 * ms_0}
+    out["plain_over_adjoint_time_to_1pct_delta"] = out["plain"]["ms_to_1pct_delta"] / out["adjoint"]["ms_to_1pct_delta"]
+    out["plain_over_adjoint_node_sensitivities"] = (out["plain"]["ms_for_3000_node_sensitivities_by_bumping"] /
+                                                    out["adjoint"]["device_ms"])
     return out
 
 
@@ -402,7 +453,7 @@ def main():
         "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, buf.products[k].price.standard_error,
                                                 buf.products[k].price.value) for k in range(len(spec.products))],
     }
-    wanted = {"early_exercise", "book", "f32"} if args.secondary == "all" else (
+    wanted = {"early_exercise", "book", "f32", "adjoint"} if args.secondary == "all" else (
         set() if args.secondary == "none" else set(args.secondary.split(",")))
     if rank == 0 and world == 1 and wanted:
         sec = {}
@@ -415,6 +466,8 @@ def main():
             sec["f32_bulk"] = f32
         if "book" in wanted:
             sec["batched_book"] = book_secondary(args.book_trades, args.book_units)
+        if "adjoint" in wanted:
+            sec["adjoint"] = adjoint_secondary(args.adjoint_paths)
         line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -373,6 +373,47 @@ mcg_status mcg_surface_local_variance_grid(const mcg_surface_desc* surface, cons
 mcg_status mcg_surface_total_variance(const mcg_surface_desc* surface, const double* times,
                                       const double* log_moneyness, uint32_t count, double* out);
 
+/* ---- VegaKT: local-vega node allocation to reporting-IV buckets ----
+ *
+ * Replaces allocate_local_vol_nodes and project_local_vega_nodes_to_reporting_iv
+ * (crates/pricing/src/engine/risk/local_vol_allocation.rs:108-163,
+ *  crates/pricing/src/engine/risk/vegakt.rs:541-570,856-949) with the active
+ * density domains of analytic_call_density_rows_from_surface over the
+ * reporting-IV surface (vegakt.rs:90-156, compile_local_vol_vega_kt_runtime in
+ * crates/pricing/src/engine/compile/local_vol.rs:104-148,
+ * crates/pricing/src/engine/processes/local_vol_valuation.rs:67-123).
+ * The reference projects every path's node sensitivities and averages; the
+ * projection is linear, so the engine projects the node-sensitivity means of
+ * mcg_result.local_vega_node_estimates (one call, on the host).  Edge counts
+ * are per evaluated path, as the reference counts them. */
+typedef struct {
+    const double* maturity_nodes;          /* increasing; the grid's positive times must be among them */
+    uint32_t maturity_count;
+    const double* log_moneyness_nodes;     /* increasing */
+    uint32_t log_moneyness_count;
+    const double* implied_volatilities;    /* maturity_count x log_moneyness_count, positive */
+    const double* forwards;                /* forward at each maturity node */
+    double relative_density_threshold;     /* in (0, 1] */
+} mcg_vega_kt_basis;
+
+typedef struct {
+    uint32_t bucket_capacity;
+    double* raw_buckets;                   /* maturity_count x log_moneyness_count */
+    double scalar_vega;                    /* sum of the buckets */
+    double signed_residual;                /* initial_time + density_excluded, as the report's projection
+                                              (crates/pricing/src/engine/risk/report.rs:206-216) */
+    double density_excluded;               /* node sensitivity outside the active density domains */
+    double pre_projection;                 /* all nodes (the scalar local Vega) = scalar_vega + signed_residual */
+    double initial_time;                   /* the t = 0 row */
+    double left_edge_sensitivity, right_edge_sensitivity;
+    uint64_t left_edge_count, right_edge_count;
+} mcg_vega_kt_projection;
+
+mcg_status mcg_vega_kt_project(const double* grid_time_nodes, uint32_t time_count,
+                               const double* grid_log_moneyness_nodes, uint32_t log_moneyness_count,
+                               const double* node_sensitivities, uint64_t evaluated_paths,
+                               const mcg_vega_kt_basis* basis, mcg_vega_kt_projection* out);
+
 /* ---- Early exercise: Longstaff--Schwartz regression ----
  *
  * Replaces SimulationPlan::execute_early_exercise and its RQMC twin

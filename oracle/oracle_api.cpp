@@ -16,6 +16,8 @@ int unit_shocks_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit,
 int unit_values_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out);
 int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacity, uint32_t* count);
 std::vector<double> pchip_derivatives(const std::vector<double>& t, const std::vector<double>& v);
+int vega_kt_project(const double* times, uint32_t nt, const double* xs, uint32_t nx, const double* nodes,
+                    uint64_t paths, const mcg_vega_kt_basis* basis, mcg_vega_kt_projection* out);
 int surface_grid(const mcg_surface_desc& d, const std::vector<double>& tn, const std::vector<double>& xn,
                  double floor, double cap, std::vector<double>& out);
 bool surface_derivatives(const mcg_surface_desc& d, const std::vector<double>& pd, double time, double k,
@@ -180,6 +182,12 @@ int oracle_surface_total_variance(const mcg_surface_desc* d, double t, double k,
         pd = oracle::pchip_derivatives(std::vector<double>(d->theta_times, d->theta_times + d->theta_count),
                                        std::vector<double>(d->theta_values, d->theta_values + d->theta_count));
     return oracle::surface_derivatives(*d, pd, t, k, out) ? 0 : -1;
+}
+
+// VegaKT node allocation of node sensitivities (grid rows x nodes).
+int oracle_vega_kt_project(const double* times, uint32_t nt, const double* xs, uint32_t nx, const double* nodes,
+                           uint64_t paths, const mcg_vega_kt_basis* basis, mcg_vega_kt_projection* out) {
+    return oracle::vega_kt_project(times, nt, xs, nx, nodes, paths, basis, out);
 }
 
 int oracle_piecewise_sinh_nodes(double left, double right, uint32_t nl, uint32_t nr,

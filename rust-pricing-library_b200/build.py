@@ -33,6 +33,7 @@ UNITS = [
     ("mcg_mlp.cu", []),
     ("mcg_book.cu", ["-fmad=false"]),
     ("mcg_lv32.cu", []),
+    ("mcg_vegakt.cu", []),
 ]
 
 

@@ -55,6 +55,20 @@ class SurfaceDesc(C.Structure):
     ]
 
 
+class VegaKtBasis(C.Structure):
+    _fields_ = [("maturity_nodes", _dp), ("maturity_count", C.c_uint32), ("log_moneyness_nodes", _dp),
+                ("log_moneyness_count", C.c_uint32), ("implied_volatilities", _dp), ("forwards", _dp),
+                ("relative_density_threshold", C.c_double)]
+
+
+class VegaKtProjection(C.Structure):
+    _fields_ = [("bucket_capacity", C.c_uint32), ("raw_buckets", _dp), ("scalar_vega", C.c_double),
+                ("signed_residual", C.c_double), ("density_excluded", C.c_double), ("pre_projection", C.c_double),
+                ("initial_time", C.c_double),
+                ("left_edge_sensitivity", C.c_double), ("right_edge_sensitivity", C.c_double),
+                ("left_edge_count", C.c_uint64), ("right_edge_count", C.c_uint64)]
+
+
 class LocalVarianceGrid(C.Structure):
     _fields_ = [
         ("time_count", C.c_uint32), ("log_moneyness_count", C.c_uint32),

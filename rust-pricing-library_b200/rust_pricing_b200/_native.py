@@ -19,7 +19,7 @@ EXPORTS = (
     "mcg_plan_destroy", "mcg_plan_shape", "mcg_philox_normals", "mcg_rqmc_words",
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
     "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient", "mcg_book_create", "mcg_book_evaluate",
-    "mcg_book_destroy", "mcg_surface_local_variance_grid", "mcg_surface_total_variance",
+    "mcg_book_destroy", "mcg_surface_local_variance_grid", "mcg_surface_total_variance", "mcg_vega_kt_project",
 )
 
 _lib = None
@@ -71,6 +71,9 @@ def library() -> C.CDLL:
     lib.mcg_surface_local_variance_grid.restype = C.c_int
     lib.mcg_surface_total_variance.argtypes = [C.POINTER(A.SurfaceDesc), dp, dp, u32, dp]
     lib.mcg_surface_total_variance.restype = C.c_int
+    lib.mcg_vega_kt_project.argtypes = [dp, u32, dp, u32, dp, u64, C.POINTER(A.VegaKtBasis),
+                                        C.POINTER(A.VegaKtProjection)]
+    lib.mcg_vega_kt_project.restype = C.c_int
     lib.mcg_price_european_noalloc.argtypes = [C.POINTER(A.PlanDesc), vp, C.POINTER(A.Result)]
     lib.mcg_price_european_noalloc.restype = C.c_int
     lib.mcg_measure_fp64_peak.argtypes = [vp, C.POINTER(dbl)]
@@ -124,6 +127,44 @@ def surface_total_variance(surface, times, log_moneyness):
     check(library().mcg_surface_total_variance(C.byref(d), t.ctypes.data_as(dp), k.ctypes.data_as(dp), len(t),
                                                 out.ctypes.data_as(dp)))
     return out.reshape(len(t), 4)
+
+
+class VegaKtBasisSpec:
+    """A reporting-IV basis (maturities x log-moneyness implied volatilities),
+    the forwards at its maturities and the relative density threshold."""
+
+    def __init__(self, maturities, log_moneyness, implied_volatilities, forwards, threshold: float = 1e-8):
+        import numpy as np
+        self.arrays = [np.ascontiguousarray(a, dtype=np.float64).ravel()
+                       for a in (maturities, log_moneyness, implied_volatilities, forwards)]
+        self.threshold = threshold
+
+    def desc(self) -> A.VegaKtBasis:
+        dp = C.POINTER(C.c_double)
+        m, x, iv, f = self.arrays
+        return A.VegaKtBasis(m.ctypes.data_as(dp), len(m), x.ctypes.data_as(dp), len(x), iv.ctypes.data_as(dp),
+                             f.ctypes.data_as(dp), self.threshold)
+
+    def buckets(self) -> int:
+        return len(self.arrays[0]) * len(self.arrays[1])
+
+
+def vega_kt_project(time_nodes, log_moneyness_nodes, node_sensitivities, evaluated_paths: int,
+                    basis: VegaKtBasisSpec):
+    """mcg_vega_kt_project (host code): (projection record, raw buckets)."""
+    import numpy as np
+    tn = np.ascontiguousarray(time_nodes, dtype=np.float64)
+    xn = np.ascontiguousarray(log_moneyness_nodes, dtype=np.float64)
+    nodes = np.ascontiguousarray(node_sensitivities, dtype=np.float64).ravel()
+    out = A.VegaKtProjection()
+    buckets = np.zeros(basis.buckets())
+    dp = C.POINTER(C.c_double)
+    out.bucket_capacity = len(buckets)
+    out.raw_buckets = buckets.ctypes.data_as(dp)
+    b = basis.desc()
+    check(library().mcg_vega_kt_project(tn.ctypes.data_as(dp), len(tn), xn.ctypes.data_as(dp), len(xn),
+                                         nodes.ctypes.data_as(dp), evaluated_paths, C.byref(b), C.byref(out)))
+    return out, buckets
 
 
 def lsm_price(spec, lsm, stopping: bool = False, stream: int = 0) -> A.LsmBuffers:

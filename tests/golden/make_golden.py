@@ -102,6 +102,9 @@ def local_volatility():
             "risk": {k: req["risk"][k] for k in ("delta", "gamma", "vega") if k in req["risk"]},
             "expected": {},
         }
+        if "vega_kt" in req["risk"]:
+            case["vega_kt"] = {"config": req["risk"]["vega_kt"],
+                               "reporting_iv_basis": req["model"]["reporting_iv_basis"]}
         for name, d in platforms.items():
             pc = d["cases"][i]
             assert pc["name"] == c["name"]
@@ -115,7 +118,23 @@ def local_volatility():
                           if k in res["risks"]},
             }
         cases.append(case)
-    json.dump({"source": "fixtures/replay/local_volatility-{windows-x86_64,macos-aarch64}.json", "cases": cases},
+    # The node-allocation audit: the diagnostic local-node allocation's VegaKT
+    # values for the two full-risk cases (the "current" side of each difference).
+    audit = json.load(open(os.path.join(REF, "fixtures/replay/local-vol-node-allocation-change-audit-v1.json")))
+    allocation = {}
+    for path, _, current in audit["differences"]:
+        parts = path.strip("/").split("/")
+        idx = int(parts[1])
+        key = "/".join(parts[5:])
+        if "covariance" in key or key.startswith("estimates") or key in ("policy_label", "truncation_order"):
+            continue
+        allocation.setdefault(cases[idx]["name"], {})[key] = current
+    for c in cases:
+        if c["name"] in allocation:
+            c["node_allocation"] = allocation[c["name"]]
+    json.dump({"source": "fixtures/replay/local_volatility-{windows-x86_64,macos-aarch64}.json; node allocation: "
+                         "fixtures/replay/local-vol-node-allocation-change-audit-v1.json (macos-aarch64)",
+               "cases": cases},
               open(os.path.join(OUT, "replay_local_vol.json"), "w"), indent=1)
 
 

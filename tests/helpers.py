@@ -64,6 +64,9 @@ def oracle():
     lib.oracle_surface_grid.restype = C.c_int
     lib.oracle_surface_total_variance.argtypes = [C.POINTER(A.SurfaceDesc), dbl, dbl, dp]
     lib.oracle_surface_total_variance.restype = C.c_int
+    lib.oracle_vega_kt_project.argtypes = [dp, u32, dp, u32, dp, u64, C.POINTER(A.VegaKtBasis),
+                                           C.POINTER(A.VegaKtProjection)]
+    lib.oracle_vega_kt_project.restype = C.c_int
     lib.oracle_piecewise_sinh_nodes.argtypes = [dbl, dbl, u32, u32, dbl, dbl, dp]
     lib.oracle_piecewise_sinh_nodes.restype = C.c_int
     lib.oracle_smoothing.argtypes = [dbl, dbl, dp]

@@ -16,6 +16,7 @@ import lv_cases as L
 import gpu_common as G
 from bs_closed_form import black_scholes
 from rust_pricing_b200 import _abi as A
+from rust_pricing_b200 import _native as N
 from rust_pricing_b200 import workloads as W
 from rust_pricing_b200.desc import PlanSpec, ProductSpec
 from test_oracle_fixtures import replay_cases, replay_spec
@@ -48,6 +49,22 @@ def test_local_vol_replay_against_reference_values(engine, case):
         assert abs(est.value - want["value"]) <= G.DIRECT_TOL * max(abs(want["value"]), want["standard_error"]), name
         assert abs(est.standard_error - want["standard_error"]) <= 1e-9 * want["standard_error"], name
     G.assert_parity(spec, engine_buf=buf)
+
+
+@pytest.mark.parametrize("case", [c for c in L.cases() if "node_allocation" in c], ids=lambda c: c["name"])
+def test_local_vol_vega_kt_node_allocation(engine, case):
+    """The engine's local-vega node sensitivities of the LV replay risk cases,
+    allocated to the reporting-IV buckets by mcg_vega_kt_project, against the
+    reference's node-allocation audit values (1e-12: the node sums are reduced
+    on the device in another order)."""
+    spec = L.plan(case)
+    spec.request_local_vega_nodes = True
+    buf = G.run_engine(spec)
+    means = [e.value for e in buf.node_estimates]
+    g = case["local_variance_grid"]
+    out, buckets = N.vega_kt_project(g["time_nodes"], g["log_forward_moneyness_nodes"], means,
+                                     buf.result.evaluated_paths, L.vega_kt_basis(case))
+    L.check_node_allocation(out, buckets, case["node_allocation"], 1e-12)
 
 
 @pytest.mark.parametrize("engine_kind", [A.ENGINE_PSEUDO, A.ENGINE_RQMC])

@@ -118,6 +118,53 @@ def test_replay_local_volatility(case):
         assert got.effective_sampling_units == plats[0]["risks"][name]["effective_sampling_units"]
 
 
+VEGA_KT_CASES = [c for c in LV_CASES if "node_allocation" in c]
+
+
+def node_means(buf):
+    return np.array([e.value for e in buf.node_estimates])
+
+
+@pytest.mark.parametrize("case", VEGA_KT_CASES, ids=lambda c: c["name"])
+def test_vega_kt_node_allocation(case):
+    """allocate_local_vol_nodes over the local-vega node sensitivities of the
+    LV replay risk cases, against the node-allocation audit fixture
+    (fixtures/replay/local-vol-node-allocation-change-audit-v1.json): raw
+    buckets, scalar VegaKT, the residual outside the active density domain and
+    the left-edge statistics.  The oracle projects the node means (the
+    projection is linear; the reference projects every path and averages), so
+    agreement is to rounding, 1e-13; the engine's host projection of the same
+    means gives the same numbers."""
+    spec = L.plan(case)
+    spec.request_local_vega_nodes = True
+    buf = H.oracle_evaluate(spec, threads=4)
+    means = node_means(buf)
+    paths = buf.result.evaluated_paths
+    out, buckets = L.oracle_vega_kt(case, means, paths)
+    L.check_node_allocation(out, buckets, case["node_allocation"], 1e-13)
+    # reconciliation: buckets + residual (excluded nodes and the initial-time row) = scalar local Vega
+    assert abs(out.scalar_vega + out.signed_residual - out.pre_projection) <= 1e-12 * abs(out.pre_projection)
+    assert out.signed_residual == out.initial_time + out.density_excluded
+    assert abs(out.pre_projection - buf.products[0].vega.value) <= 1e-12 * abs(buf.products[0].vega.value)
+    from rust_pricing_b200 import _native as N
+    g = case["local_variance_grid"]
+    eng, eb = N.vega_kt_project(g["time_nodes"], g["log_forward_moneyness_nodes"], means, paths, L.vega_kt_basis(case))
+    assert list(eb) == list(buckets)
+    for f in ("scalar_vega", "signed_residual", "density_excluded", "initial_time", "left_edge_sensitivity",
+              "left_edge_count"):
+        assert getattr(eng, f) == getattr(out, f), f
+
+
+def test_vega_kt_rejects_a_grid_time_without_a_density_row():
+    from rust_pricing_b200 import _native as N
+    case = VEGA_KT_CASES[0]
+    g = case["local_variance_grid"]
+    times = [0.0, 0.5, 1.0]   # 0.5 is not a reporting maturity
+    with pytest.raises(N.EngineError) as err:
+        N.vega_kt_project(times, g["log_forward_moneyness_nodes"], np.ones(15), 10, L.vega_kt_basis(case))
+    assert err.value.name == "invalid_argument"
+
+
 def test_replay_independent_of_thread_count():
     case = replay_cases()[0]
     a = H.oracle_evaluate(replay_spec(case), threads=1).products[0]
