@@ -60,7 +60,11 @@ struct AdjointArgs {
     double* out_vega;
     double* out_delta;
     double* node_tiles;
+    double* out_price;
+    double* out_diag;
 };
+cudaError_t launch_lv_adjoint_price(const double* price, const double* diag, uint64_t units, int pairs,
+                                    uint32_t tile_offset, uint32_t mask, StatRecord* partials, cudaStream_t stream);
 size_t lv_adjoint_smem(const DevicePlan& P);
 cudaError_t launch_lv_adjoint(const DevicePlan& P, const AdjointArgs& A, ErrorWord* err, cudaStream_t stream);
 cudaError_t launch_lv_adjoint_combine(const double* vega, const double* delta, uint64_t units, int pairs,
@@ -351,7 +355,7 @@ struct mcg_plan {
     // device storage
     DeviceArray<Op> ops;
     DeviceArray<double> node_time, dt, sqrt_dt, inv_sqrt_dt, time_weight, fwd, ratio, obs_time,
-        obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, weights;
+        obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, grid_vol2, weights;
     DeviceArray<int32_t> obs_of_node, time_cell;
     DeviceArray<LvStep> lv_steps;
     DeviceArray<uint32_t> scr_dirs, scr_shift, scr_low, directions;
@@ -360,8 +364,9 @@ struct mcg_plan {
     uint32_t tiles = 0;
     // local-volatility adjoint (Vega, adjoint Delta/Gamma, node sensitivities)
     bool adjoint = false, adjoint_nodes = false, adjoint_gamma = false;
+    bool price_from_adjoint = false;  // no CRN runtimes: the sweeps' forward passes give the price
     uint64_t chunk_units = 0;
-    DeviceArray<double> tape, adj_vega, adj_delta, node_tiles;
+    DeviceArray<double> tape, adj_vega, adj_delta, node_tiles, adj_price, adj_diag;
     DeviceArray<StatRecord> adj_partials, adj_records, node_records;
     DeviceArray<float> fwd_f, ratio_f;
     DeviceArray<float4> step_f;
@@ -384,6 +389,7 @@ struct mcg_plan {
         grid_t.release();
         grid_x.release();
         grid_v.release();
+        grid_vol2.release();
         weights.release();
         obs_of_node.release();
         time_cell.release();
@@ -398,6 +404,8 @@ struct mcg_plan {
         tape.release();
         adj_vega.release();
         adj_delta.release();
+        adj_price.release();
+        adj_diag.release();
         node_tiles.release();
         adj_partials.release();
         adj_records.release();
@@ -679,6 +687,11 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         MCG_CUDA(plan.grid_t.upload(gt));
         MCG_CUDA(plan.grid_x.upload(gx));
         MCG_CUDA(plan.grid_v.upload(gv));
+        {
+            std::vector<double> v2(gv.size());
+            for (size_t i = 0; i < gv.size(); ++i) v2[i] = 2.0 * std::sqrt(gv[i]);
+            MCG_CUDA(plan.grid_vol2.upload(v2));
+        }
         P.node_time = plan.node_time.ptr;
         P.dt = plan.dt.ptr;
         P.sqrt_dt = plan.sqrt_dt.ptr;
@@ -691,6 +704,7 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         P.grid_t = plan.grid_t.ptr;
         P.grid_x = plan.grid_x.ptr;
         P.grid_v = plan.grid_v.ptr;
+        P.grid_vol2 = plan.grid_vol2.ptr;
         P.nt = g.time_count;
         P.nx = g.log_moneyness_count;
         plan.grid_values = static_cast<uint32_t>(gv.size());
@@ -791,6 +805,13 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         MCG_CUDA(plan.tape.alloc(static_cast<size_t>(2 * P.steps + 1) * plan.chunk_units));
         MCG_CUDA(plan.adj_vega.alloc(6 * plan.chunk_units));
         MCG_CUDA(plan.adj_delta.alloc(6 * plan.chunk_units));
+        // Without CRN Delta/Gamma the base sweeps' forward passes are the
+        // plan's paths: they give the price and no separate price pass runs.
+        plan.price_from_adjoint = !P.lv_bumps && P.precision == MCG_PRECISION_F64;
+        if (plan.price_from_adjoint) {
+            MCG_CUDA(plan.adj_price.alloc(2 * plan.chunk_units));
+            if (plan.mask & (0xffu << 10)) MCG_CUDA(plan.adj_diag.alloc(2 * 8 * plan.chunk_units));
+        }
         MCG_CUDA(plan.adj_partials.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * 3));
         MCG_CUDA(plan.adj_records.alloc(static_cast<size_t>(P.scramble_count) * 3));
         if (plan.adjoint_nodes) {
@@ -867,6 +888,8 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
     // Per-product partials use kComponents stride; reduce only masked slots below.
     if (P.model == MCG_MODEL_LOCAL_VOLATILITY && P.precision == MCG_PRECISION_F32_BULK) {
         e = launch_lv32_path(P, plan->partials.ptr, plan->mask, plan->error.ptr, stream);
+    } else if (P.model == MCG_MODEL_LOCAL_VOLATILITY && plan->price_from_adjoint) {
+        e = cudaSuccess;  // the price comes from the adjoint sweeps below
     } else if (P.model == MCG_MODEL_LOCAL_VOLATILITY) {
         int evolutions;
         e = launch_lv_path(P, 0, P.units, P.scramble_count, plan->partials.ptr, plan->mask, plan->error.ptr, 0,
@@ -876,13 +899,15 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
                            plan->mask, plan->error.ptr, 0, stream);
     }
     if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("path kernel: ") + cudaGetErrorString(e));
-    ++launches;
-    MCG_CUDA(cudaEventRecord(tp, stream));
     const uint32_t width = plan->product_count * kComponents;
-    reduce_tiles_kernel<<<dim3(width, P.scramble_count), 256, 0, stream>>>(plan->partials.ptr, plan->tiles,
-                                                                           width, plan->records.ptr);
-    MCG_CUDA(cudaGetLastError());
-    ++launches;
+    if (!plan->price_from_adjoint) {
+        ++launches;
+        MCG_CUDA(cudaEventRecord(tp, stream));
+        reduce_tiles_kernel<<<dim3(width, P.scramble_count), 256, 0, stream>>>(plan->partials.ptr, plan->tiles,
+                                                                               width, plan->records.ptr);
+        MCG_CUDA(cudaGetLastError());
+        ++launches;
+    }
     std::vector<StatRecord> adj_rec, node_rec;
     if (plan->adjoint) {
         const int pairs = P.antithetic ? 2 : 1;
@@ -908,6 +933,11 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
                         A.out_vega = plan->adj_vega.ptr + static_cast<size_t>(pr * 3 + which) * n;
                         A.out_delta = plan->adj_delta.ptr + static_cast<size_t>(pr * 3 + which) * n;
                         A.node_tiles = (which == 0 && plan->adjoint_nodes) ? plan->node_tiles.ptr : nullptr;
+                        if (which == 0 && plan->price_from_adjoint) {
+                            A.out_price = plan->adj_price.ptr + static_cast<size_t>(pr) * n;
+                            A.out_diag = plan->adj_diag.ptr ? plan->adj_diag.ptr + static_cast<size_t>(pr) * 8 * n
+                                                            : nullptr;
+                        }
                         e = launch_lv_adjoint(P, A, plan->error.ptr, stream);
                         if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("adjoint kernel: ") + cudaGetErrorString(e));
                         ++launches;
@@ -918,6 +948,12 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
                                               plan->adj_partials.ptr, stream);
                 if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
                 ++launches;
+                if (plan->price_from_adjoint) {
+                    e = launch_lv_adjoint_price(plan->adj_price.ptr, plan->adj_diag.ptr, n, pairs, tile_offset,
+                                                plan->mask, plan->partials.ptr, stream);
+                    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+                    ++launches;
+                }
                 (void)tiles_chunk;
             }
         }
@@ -925,6 +961,13 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
                                                                           plan->adj_records.ptr);
         MCG_CUDA(cudaGetLastError());
         ++launches;
+        if (plan->price_from_adjoint) {
+            MCG_CUDA(cudaEventRecord(tp, stream));
+            reduce_tiles_kernel<<<dim3(width, P.scramble_count), 256, 0, stream>>>(plan->partials.ptr, plan->tiles,
+                                                                                   width, plan->records.ptr);
+            MCG_CUDA(cudaGetLastError());
+            ++launches;
+        }
         adj_rec.resize(static_cast<size_t>(P.scramble_count) * 3);
         if (plan->adjoint_nodes) {
             e = launch_lv_node_reduce(plan->node_tiles.ptr, plan->tiles, P.scramble_count, plan->grid_values,

@@ -36,6 +36,8 @@ struct AdjointArgs {
     double* out_vega;       // [units]
     double* out_delta;      // [units]
     double* node_tiles;     // [global tile][nt * nx] or null
+    double* out_price;      // [units] discounted payoff of the forward pass, or null
+    double* out_diag;       // [8][units] continuous-barrier diagnostics, or null
 };
 
 struct InterpFull {
@@ -130,29 +132,27 @@ __device__ __forceinline__ void flush_rows(double* window, int lo, int hi, int n
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kAdjThreads) lv_adjoint_kernel(const DevicePlan P, AdjointArgs A,
-                                                                 ErrorWord* err) {
+// The grid values and their 2 sqrt(v) are read through L1 (shared memory
+// holds the x nodes, the node window and the bridge slots), which lets 5 CTAs
+// share an SM.
+__global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const DevicePlan P, AdjointArgs A,
+                                                                    ErrorWord* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = static_cast<int>(P.nx);
     const int nt = static_cast<int>(P.nt);
     const size_t nv = static_cast<size_t>(nt) * nx;
-    double* s_v = reinterpret_cast<double*>(smem_raw);
-    double* s_vol2 = s_v + nv;
-    double* s_x = s_vol2 + nv;
+    const double* s_vol2 = P.grid_vol2;
+    double* s_x = reinterpret_cast<double*>(smem_raw);
     long long* s_xk = reinterpret_cast<long long*>(s_x + nx);
     double* s_win = reinterpret_cast<double*>(s_xk + nx);
     double* s_w = s_win + 3 * nx;  // bridge slots [slot][thread]
-    for (size_t i = threadIdx.x; i < nv; i += kAdjThreads) {
-        s_v[i] = P.grid_v[i];
-        s_vol2[i] = 2.0 * sqrt(P.grid_v[i]);
-    }
     for (int i = threadIdx.x; i < nx; i += kAdjThreads) {
         s_x[i] = P.grid_x[i];
         s_xk[i] = total_key(P.grid_x[i]);
     }
     for (int i = threadIdx.x; i < 3 * nx; i += kAdjThreads) s_win[i] = 0.0;
     __syncthreads();
-    const GridView g{s_v, s_x, s_xk, nx};
+    const GridView g{P.grid_v, s_x, s_xk, nx};
 
     const uint64_t local = static_cast<uint64_t>(blockIdx.x) * kAdjThreads + threadIdx.x;
     const bool valid = local < A.units;
@@ -247,6 +247,11 @@ __global__ void __launch_bounds__(kAdjThreads) lv_adjoint_kernel(const DevicePla
         barrier_interval(pp, acc, h, prev_f, f, prev_v, inN.value, P.dt[steps - 1], failed);
         double diag[8];
         const double surv = barrier_finish(acc, h, steps, diag);
+        if (A.out_price && valid) {
+            A.out_price[local] = P.discount * barrier_value(pp, f, surv);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) A.out_diag[static_cast<size_t>(q) * ustride + local] = diag[q];
+        }
         const double in = call ? f - pp.strike : pp.strike - f;
         const double vanilla = fmax(in, 0.0) * pp.notional;
         const double vd = in >= 0.0 ? (call ? 1.0 : -1.0) * pp.notional : 0.0;
@@ -263,6 +268,7 @@ __global__ void __launch_bounds__(kAdjThreads) lv_adjoint_kernel(const DevicePla
         exact_active = !(acc.initial_touched || acc.touched);
         lsa = P.discount * sd * surv;
     } else {
+        if (A.out_price && valid) A.out_price[local] = P.discount * acc_payoff(pp, acc, h);
         // d payoff / d observed spot (tape.rs:594-781 reverse semantics)
         const double term = acc.terminal;
         switch (pp.kind) {
@@ -426,6 +432,34 @@ __global__ void __launch_bounds__(kThreads) lv_adjoint_combine_kernel(
     cta_reduce_write<3>(vals, valid, 0x7u, partials + static_cast<size_t>(tile_offset + blockIdx.x) * slots, s_red);
 }
 
+// Price (and continuous-barrier diagnostics) of the units of a chunk, taken
+// from the adjoint sweeps' forward passes when no separate price pass runs:
+// antithetic pairs averaged as the path kernel averages them, one
+// kComponents record per CTA tile of the plan's partials.
+__global__ void __launch_bounds__(kThreads) lv_adjoint_price_kernel(const double* price, const double* diag,
+                                                                    uint64_t units, int pairs, uint32_t tile_offset,
+                                                                    uint32_t mask, StatRecord* partials) {
+    __shared__ Stat s_red[4 * kComponents];
+    const uint64_t u = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    const bool valid = u < units;
+    double vals[kComponents];
+#pragma unroll
+    for (int c = 0; c < kComponents; ++c) vals[c] = 0.0;
+    if (valid) {
+        for (int pr = 0; pr < pairs; ++pr) {
+            const double p = price[static_cast<size_t>(pr) * units + u];
+            vals[MCG_PRICE] = pr == 0 ? p : (vals[MCG_PRICE] + p) * 0.5;
+            if (diag)
+                for (int q = 0; q < 8; ++q) {
+                    const double d = diag[(static_cast<size_t>(pr) * 8 + q) * units + u];
+                    vals[10 + q] = pr == 0 ? d : (vals[10 + q] + d) * 0.5;
+                }
+        }
+    }
+    cta_reduce_write<kComponents>(vals, valid, mask,
+                                  partials + static_cast<size_t>(tile_offset + blockIdx.x) * kComponents, s_red);
+}
+
 // Node sums over tiles, per scramble: Neumaier sum in tile order and the
 // two-pass second moment of the tile sums (batch means).
 __global__ void lv_node_reduce_kernel(const double* node_tiles, uint32_t tiles_per_scramble,
@@ -446,8 +480,7 @@ __global__ void lv_node_reduce_kernel(const double* node_tiles, uint32_t tiles_p
 }
 
 size_t lv_adjoint_smem(const DevicePlan& P) {
-    const size_t nv = static_cast<size_t>(P.nt) * P.nx;
-    return (2 * nv + 2 * P.nx + 3 * P.nx) * sizeof(double) +
+    return (2 * static_cast<size_t>(P.nx) + 3 * P.nx) * sizeof(double) +
            static_cast<size_t>(P.slot_count) * kAdjThreads * sizeof(double);
 }
 
@@ -467,6 +500,13 @@ cudaError_t launch_lv_adjoint_combine(const double* vega, const double* delta, u
     const unsigned blocks = static_cast<unsigned>((units + kThreads - 1) / kThreads);
     lv_adjoint_combine_kernel<<<blocks, kThreads, 0, stream>>>(vega, delta, units, pairs, have_gamma, h,
                                                                tile_offset, partials, 3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lv_adjoint_price(const double* price, const double* diag, uint64_t units, int pairs,
+                                    uint32_t tile_offset, uint32_t mask, StatRecord* partials, cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>((units + kThreads - 1) / kThreads);
+    lv_adjoint_price_kernel<<<blocks, kThreads, 0, stream>>>(price, diag, units, pairs, tile_offset, mask, partials);
     return cudaGetLastError();
 }
 

@@ -102,6 +102,7 @@ struct DevicePlan {
     const double* grid_t;
     const double* grid_x;
     const double* grid_v;
+    const double* grid_vol2;     // 2 sqrt(v) of every grid value (local Vega per node adjoint)
     const float* grid_v_f;
     uint32_t nt, nx;
 
