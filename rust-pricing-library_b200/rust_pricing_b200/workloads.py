@@ -195,7 +195,8 @@ def batched_book(builder: GridBuilder, trades: int = 4096, units: int = 1 << 16,
         local = bool(rng.integers(0, 2))
         vol = float(rng.uniform(0.15, 0.35))
         rho = float(rng.uniform(-0.6, -0.2))
-        eta = float(rng.uniform(0.7, 1.3))
+        # the power-law wing bound eta (1 + |rho|) <= 2 of StandardSsvi::new
+        eta = min(float(rng.uniform(0.7, 1.3)), 2.0 / (1.0 + abs(rho)))
         barrier = float(rng.uniform(60.0, 90.0))
         times = daily_times(steps, horizon)
         if kind == A.PRODUCT_ASIAN:
