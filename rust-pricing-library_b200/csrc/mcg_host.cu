@@ -1415,25 +1415,21 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
             const uint64_t steps = l->mlp_epochs
                                        ? first * static_cast<uint64_t>(epochs) * nbatch
                                        : std::max<uint64_t>(nbatch, date == last - 1 ? 400u : 50u);
-            for (uint64_t k = 0; k < steps; ++k) {
-                const uint64_t b = k % nbatch;
-                MlpRows rows{};
-                rows.spots = B.spots.ptr + static_cast<size_t>(date) * t_paths;
-                rows.cf = B.cf_mlp.ptr;
-                rows.first = b * batch;
-                rows.count = std::min<uint64_t>(batch, t_paths - rows.first);
-                rows.df = df[date];
-                rows.time_input = tin;
-                rows.side = A.side;
-                rows.strike = A.strike;
-                rows.notional = A.notional;
-                rows.itm_tol = A.itm_tol;
-                const unsigned mctas = mlp_gradient_ctas(rows.count);
-                MCG_CUDA(launch_mlp_gradient(B.mlp_params.ptr, rows, B.mlp_partials.ptr, mctas, stream));
-                MCG_CUDA(launch_mlp_adam(B.mlp_partials.ptr, mctas, B.mlp_params.ptr, B.mlp_moments.ptr, ++step,
-                                         lr, B.mlp_loss.ptr, stream));
-                launches += 2;
-            }
+            // the date's Adam steps in one cooperative launch (gradient pass,
+            // grid barrier, update, grid barrier per step)
+            MlpRows rows{};
+            rows.spots = B.spots.ptr + static_cast<size_t>(date) * t_paths;
+            rows.cf = B.cf_mlp.ptr;
+            rows.df = df[date];
+            rows.time_input = tin;
+            rows.side = A.side;
+            rows.strike = A.strike;
+            rows.notional = A.notional;
+            rows.itm_tol = A.itm_tol;
+            MCG_CUDA(launch_mlp_train(B.mlp_params.ptr, B.mlp_moments.ptr, B.mlp_partials.ptr, rows, t_paths, batch,
+                                      static_cast<uint32_t>(steps), step, lr, B.mlp_loss.ptr, stream));
+            step += static_cast<uint32_t>(steps);
+            ++launches;
             MCG_CUDA(cudaMemcpyAsync(B.mlp_snapshots.ptr + static_cast<size_t>(date) * kMlpParams, B.mlp_params.ptr,
                                      kMlpParams * sizeof(float), cudaMemcpyDeviceToDevice, stream));
             MlpDecision dec{};

@@ -17,6 +17,7 @@
 // dH2^T H1 with each warp owning 16 output rows of W2 in registers.  Every
 // gradient sum is taken in a fixed order (lanes, warps, CTAs), so a step is
 // reproducible bit for bit.
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -224,10 +225,10 @@ __device__ __forceinline__ void load_row(const MlpRows& R, uint64_t r, float& x0
     m = 1.0f;
 }
 
-__global__ void __launch_bounds__(kMlpThreads) mlp_gradient_kernel(const float* __restrict__ params, const MlpRows R,
-                                                                   float* __restrict__ partials) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    GradShared& S = *reinterpret_cast<GradShared*>(smem_raw);
+// One gradient pass of the CTA over its tiles of the step's rows (tiles
+// blockIdx.x, + gridDim.x, ...), written as the CTA's partial record.
+__device__ __forceinline__ void gradient_pass(GradShared& S, const float* __restrict__ params, const MlpRows& R,
+                                              float* __restrict__ partials) {
     load_net(S.net, params);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     for (int i = lane; i < kSmall; i += 32) S.small[warp][i] = 0.0f;
@@ -397,12 +398,18 @@ __global__ void __launch_bounds__(kMlpThreads) mlp_gradient_kernel(const float* 
     }
 }
 
+__global__ void __launch_bounds__(kMlpThreads) mlp_gradient_kernel(const float* __restrict__ params, const MlpRows R,
+                                                                   float* __restrict__ partials) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GradShared& S = *reinterpret_cast<GradShared*>(smem_raw);
+    gradient_pass(S, params, R, partials);
+}
+
 // Sums the per-CTA records in CTA order and takes one Adam step on the mean
-// gradient (beta1 0.9, beta2 0.999, eps 1e-8).  moments = [m | v].
-__global__ void mlp_adam_kernel(const float* __restrict__ partials, unsigned ctas, float* __restrict__ params,
-                                float* __restrict__ moments, uint32_t step, float lr, float* loss_out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kMlpParams) return;
+// gradient (beta1 0.9, beta2 0.999, eps 1e-8) for parameter i.  moments = [m | v].
+__device__ __forceinline__ void adam_param(int i, const float* __restrict__ partials, unsigned ctas,
+                                           float* __restrict__ params, float* __restrict__ moments, uint32_t step,
+                                           float lr, float* loss_out) {
     float rows = 0.0f, gsum = 0.0f;
 #pragma unroll 8
     for (unsigned c = 0; c < ctas; ++c) {  // in CTA order; the loads run ahead of the adds
@@ -423,6 +430,40 @@ __global__ void mlp_adam_kernel(const float* __restrict__ partials, unsigned cta
         float l = 0.0f;
         for (unsigned c = 0; c < ctas; ++c) l += partials[static_cast<size_t>(c) * kMlpPartial + kMlpParams];
         *loss_out = l / rows;
+    }
+}
+
+__global__ void mlp_adam_kernel(const float* __restrict__ partials, unsigned ctas, float* __restrict__ params,
+                                float* __restrict__ moments, uint32_t step, float lr, float* loss_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kMlpParams) return;
+    adam_param(i, partials, ctas, params, moments, step, lr, loss_out);
+}
+
+// A date's whole training in one cooperative launch: per step, every CTA's
+// gradient pass over its tiles of batch (k mod nbatch), a grid barrier, the
+// Adam update spread over the grid's threads, a grid barrier.  The same
+// arithmetic in the same order as alternating mlp_gradient_kernel and
+// mlp_adam_kernel launches (a CTA whose tiles run out writes a zero record,
+// which adds nothing), without two launches per step.
+__global__ void __launch_bounds__(kMlpThreads) mlp_train_kernel(float* __restrict__ params,
+                                                                float* __restrict__ moments,
+                                                                float* __restrict__ partials, MlpRows R0,
+                                                                uint64_t total, uint64_t batch, uint32_t steps,
+                                                                uint32_t step0, float lr, float* loss_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GradShared& S = *reinterpret_cast<GradShared*>(smem_raw);
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const uint64_t nbatch = (total + batch - 1) / batch;
+    for (uint32_t k = 0; k < steps; ++k) {
+        MlpRows R = R0;
+        R.first = (k % nbatch) * batch;
+        R.count = min(batch, total - R.first);
+        gradient_pass(S, params, R, partials);
+        grid.sync();
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kMlpParams; i += gridDim.x * blockDim.x)
+            adam_param(i, partials, gridDim.x, params, moments, step0 + k + 1, lr, k + 1 == steps ? loss_out : nullptr);
+        grid.sync();
     }
 }
 
@@ -588,6 +629,25 @@ cudaError_t launch_mlp_gradient(const float* params, const MlpRows& rows, float*
     if (e != cudaSuccess) return e;
     mlp_gradient_kernel<<<ctas, kMlpThreads, smem, stream>>>(params, rows, partials);
     return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_train(float* params, float* moments, float* partials, const MlpRows& rows, uint64_t total,
+                             uint64_t batch, uint32_t steps, uint32_t step0, float learning_rate, float* loss_out,
+                             cudaStream_t stream) {
+    const size_t smem = sizeof(GradShared);
+    cudaError_t e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mlp_train_kernel, kMlpThreads, smem);
+    if (e != cudaSuccess) return e;
+    // as many CTAs as a full batch has tiles, all co-resident
+    const unsigned ctas = std::min<unsigned>(mlp_gradient_ctas(std::min(batch, total)),
+                                             static_cast<unsigned>(std::max(per_sm, 1) * device_sms()));
+    MlpRows r = rows;
+    void* args[] = {&params, &moments, &partials, &r, &total, &batch, &steps, &step0, &learning_rate, &loss_out};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(mlp_train_kernel), dim3(ctas), dim3(kMlpThreads),
+                                       args, smem, stream);
 }
 
 cudaError_t launch_mlp_adam(const float* partials, unsigned ctas, float* params, float* moments, uint32_t step,

@@ -53,6 +53,11 @@ struct MlpDecision {
 
 cudaError_t launch_mlp_gradient(const float* params, const MlpRows& rows, float* partials, unsigned ctas,
                                 cudaStream_t stream);
+// A date's `steps` Adam steps over batches of `batch` of its `total` rows
+// (batch k mod ceil(total / batch)), one cooperative launch.
+cudaError_t launch_mlp_train(float* params, float* moments, float* partials, const MlpRows& rows, uint64_t total,
+                             uint64_t batch, uint32_t steps, uint32_t step0, float learning_rate, float* loss_out,
+                             cudaStream_t stream);
 cudaError_t launch_mlp_adam(const float* partials, unsigned ctas, float* params, float* moments, uint32_t step,
                             float learning_rate, float* loss_out, cudaStream_t stream);
 cudaError_t launch_mlp_sum(const float* partials, unsigned ctas, float* out, cudaStream_t stream);
