@@ -429,8 +429,8 @@ mcg_status mcg_vega_kt_project(const double* grid_time_nodes, uint32_t time_coun
  * American payoff graph observes exactly the exercise dates,
  * crates/pricing/src/engine/payoff/compile.rs:67-101).  Its engine fields are
  * the valuation engine; `mcg_lsm_desc` adds the training engine (same kind) and
- * the regression configuration (LsmConfig).  Risk requests (Black-Scholes) ask
- * for the fixed-policy Greeks of mcg_lsm_result. */
+ * the regression configuration (LsmConfig).  Risk requests ask for the
+ * fixed-policy Greeks of mcg_lsm_result (Black-Scholes and local volatility). */
 #define MCG_LSM_MAX_DEGREE 7u
 #define MCG_LSM_MAX_BASIS (MCG_LSM_MAX_DEGREE + 1u)
 
@@ -531,7 +531,17 @@ typedef struct mcg_lsm_result {
      * bump-and-revalue validation components -- reduced like the plan
      * components (constant_vol_fixed_policy_pseudo/rqmc_statistics,
      * crates/pricing/src/engine/mc/early_exercise.rs:454-600;
-     * fixed_policy_pathwise_values, crates/pricing/src/engine/processes/black_scholes.rs:358-415). */
+     * fixed_policy_pathwise_values, crates/pricing/src/engine/processes/black_scholes.rs:358-415).
+     * Under local volatility (local_vol_fixed_policy_pseudo/rqmc_statistics_with_vega_kt,
+     * crates/pricing/src/engine/risk/early_exercise.rs:465-700, over
+     * local_vol_pathwise_values_and_buckets_inner,
+     * crates/pricing/src/engine/risk/pathwise_local_vol.rs:127-361): Delta and
+     * Gamma by central bumps of the spot on common paths (bump = the gamma bump,
+     * or 1e-4 of spot), Vega by the reverse sweep seeded at the stopping date,
+     * and -- with request_local_vega_nodes -- the per-node local-vega means and
+     * their statistics in `local_vega_nodes` / `local_vega_node_estimates`
+     * (node_capacity >= the grid's value count), which mcg_vega_kt_project
+     * turns into VegaKT buckets. */
     mcg_statistics risk_components[MCG_PATHWISE_COMPONENTS];
     mcg_estimate delta;
     mcg_estimate gamma;
@@ -548,6 +558,10 @@ typedef struct mcg_lsm_result {
     double mlp_in_sample;           /* in-sample value of the network policy */
     uint32_t mlp_param_capacity;    /* entries in `mlp_params` (0 = not wanted) */
     float* mlp_params;              /* trained parameters, caller-owned */
+    /* Local volatility with request_local_vega_nodes: per grid node (time-major). */
+    uint32_t node_capacity;
+    mcg_statistics* local_vega_nodes;
+    mcg_estimate* local_vega_node_estimates;
     mcg_error_record error;
 } mcg_lsm_result;
 

@@ -31,6 +31,8 @@ int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vect
 double plan_discount(const mcg_plan_desc* desc, double t);
 int lsm_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, const double* df, int threads,
                           mcg_lsm_result* result);
+int lsm_lv_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, const double* df, int threads,
+                             mcg_lsm_result* result);
 
 namespace {
 
@@ -404,9 +406,13 @@ int lsm_price(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, mcg_lsm_result
     std::memset(out->risk_components, 0, sizeof(out->risk_components));
     out->delta = out->gamma = out->vega = mcg_estimate{};
     out->bump_delta = out->bump_gamma = out->bump_vega = mcg_estimate{};
-    if (desc->request_delta || desc->request_gamma || desc->request_vega) {
-        if (desc->model != MCG_MODEL_BLACK_SCHOLES) return MCG_ERR_UNSUPPORTED;
-        rc = lsm_fixed_policy_risk(desc, stop.data(), df.data(), threads, out);
+    if (desc->request_delta || desc->request_gamma || desc->request_vega || desc->request_local_vega_nodes) {
+        if (desc->model == MCG_MODEL_BLACK_SCHOLES) {
+            if (desc->request_local_vega_nodes) return MCG_ERR_UNSUPPORTED;
+            rc = lsm_fixed_policy_risk(desc, stop.data(), df.data(), threads, out);
+        } else {
+            rc = lsm_lv_fixed_policy_risk(desc, stop.data(), df.data(), threads, out);
+        }
         if (rc != MCG_OK) return rc;
     }
     return MCG_OK;

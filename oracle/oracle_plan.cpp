@@ -1659,6 +1659,165 @@ int lsm_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, cons
     return MCG_OK;
 }
 
+// One LV valuation path's fixed-policy values: the discounted exercise value
+// at its stopping date k (the American payoff graph's output k,
+// local_vol_pathwise_values_and_buckets_inner with a cash-flow selection,
+// crates/pricing/src/engine/risk/pathwise_local_vol.rs:127-361): price,
+// reverse-sweep Vega and node values (seed at the stop node), CRN Delta and
+// Gamma from the bumped spot runtimes.
+bool lv_fixed_values(const Plan& p, const mcg_product_desc& pd, const double* shocks, uint32_t k, double dfk,
+                     double* values, double* nodes, Failure& f) {
+    for (int c = 0; c < kComponents; ++c) values[c] = 0.0;
+    const bool call = pd.side == MCG_CALL;
+    auto exercise = [&](int which, const LvPath& path, double& adj) {
+        const double s = 0.0 * p.bump_spot[which] + 1.0 * path.state[p.obs_node[k]];
+        const double in = call ? s - pd.strike : pd.strike - s;
+        adj = (in >= 0.0 ? pd.notional : 0.0) * (call ? 1.0 : -1.0);
+        return dfk * ((in >= 0.0 ? in : 0.0) * pd.notional);
+    };
+    LvPath path;
+    if (!lv_evolve(p, 0, shocks, path, f)) return false;
+    double adj;
+    const double price = exercise(0, path, adj);
+    values[MCG_PRICE] = price;
+    if (p.req_vega || p.req_nodes) {
+        const size_t count = p.nodes.size();
+        std::vector<double> seeds(count, 0.0), vseeds(count, 0.0), grid_adj;
+        seeds[p.obs_node[k]] += dfk * adj * 1.0;
+        double lambda0, x_sum;
+        if (!lv_reverse(p, 0, path, seeds, vseeds, grid_adj, lambda0, x_sum, f)) return false;
+        NeumaierSum v;
+        for (size_t j = 0; j < grid_adj.size(); ++j) {
+            const double node = grid_adj[j] * 2.0 * std::sqrt(p.grid.v[j]);
+            v.add(node);
+            if (nodes) nodes[j] = node;
+        }
+        values[MCG_VEGA] = v.total();
+    }
+    if (p.req_delta || p.req_gamma) {
+        LvPath bumped;
+        double a;
+        if (!lv_evolve(p, 1, shocks, bumped, f)) return false;
+        const double down = exercise(1, bumped, a);
+        if (!lv_evolve(p, 2, shocks, bumped, f)) return false;
+        const double up = exercise(2, bumped, a);
+        const double h = p.spot_bump;
+        const double delta = (up - down) / (2.0 * h);
+        values[MCG_DELTA] = delta;
+        values[MCG_BUMP_DELTA] = delta;
+        if (p.req_gamma) {
+            const double gamma = (up - 2.0 * price + down) / (h * h);
+            values[MCG_GAMMA] = gamma;
+            values[MCG_BUMP_GAMMA] = gamma;
+        }
+    }
+    return true;
+}
+
+// Fixed-policy risk of an early-exercise plan under local volatility,
+// local_vol_fixed_policy_pseudo/rqmc_statistics_with_vega_kt
+// (crates/pricing/src/engine/risk/early_exercise.rs:465-700): per unit the
+// pair-averaged values (average_local_vol_pathwise), pseudo: a two-pass over
+// the units' values in order; RQMC: per-scramble means of Neumaier sums, then
+// a two-pass over the scramble means.  Node values are reduced the same way.
+int lsm_lv_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, const double* df, int threads,
+                             mcg_lsm_result* result) {
+    Plan p;
+    if (!build_plan(desc, p)) return MCG_ERR_INVALID_ARGUMENT;
+    const bool rqmc = p.engine == MCG_ENGINE_RQMC;
+    const uint64_t mult = p.antithetic ? 2 : 1;
+    const uint64_t units = p.units * (rqmc ? p.scrambles : 1);
+    const mcg_product_desc& pd = desc->products[0];
+    const size_t nv = p.grid.v.size();
+    const bool want_nodes = p.req_nodes && result->local_vega_nodes && result->node_capacity >= nv;
+    const size_t width = kComponents + (want_nodes ? nv : 0);
+    std::vector<double> vals(units * width, 0.0);
+    std::vector<Failure> failures(static_cast<size_t>(std::max(1, threads)));
+    std::vector<uint64_t> failed(failures.size(), ~0ull);
+    std::atomic<uint64_t> next{0};
+    auto worker = [&](size_t t) {
+        std::vector<double> z(p.dimension), mate(p.dimension), normals, scratch, a(kComponents), b(kComponents);
+        std::vector<double> na(nv), nb(nv);
+        for (;;) {
+            const uint64_t u = next.fetch_add(1);
+            if (u >= units || failures[t].code != MCG_OK) break;
+            const uint32_t scramble = rqmc ? static_cast<uint32_t>(u / p.units) : 0u;
+            const uint64_t local = rqmc ? u % p.units : u;
+            unit_shocks(p, scramble, local, z.data(), normals, scratch);
+            const uint32_t k0 = stops[u * mult];
+            if (!lv_fixed_values(p, pd, z.data(), k0, df[k0], a.data(), want_nodes ? na.data() : nullptr,
+                                 failures[t])) {
+                failed[t] = u;
+                return;
+            }
+            double* out = vals.data() + u * width;
+            if (mult == 2) {
+                for (size_t i = 0; i < z.size(); ++i) mate[i] = -z[i];
+                const uint32_t k1 = stops[u * mult + 1];
+                if (!lv_fixed_values(p, pd, mate.data(), k1, df[k1], b.data(), want_nodes ? nb.data() : nullptr,
+                                     failures[t])) {
+                    failed[t] = u;
+                    return;
+                }
+                for (int c = 0; c < kComponents; ++c) out[c] = (a[c] + b[c]) * 0.5;
+                if (want_nodes)
+                    for (size_t j = 0; j < nv; ++j) out[kComponents + j] = (na[j] + nb[j]) * 0.5;
+            } else {
+                for (int c = 0; c < kComponents; ++c) out[c] = a[c];
+                if (want_nodes)
+                    for (size_t j = 0; j < nv; ++j) out[kComponents + j] = na[j];
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < failures.size(); ++t) pool.emplace_back(worker, t);
+    for (auto& t : pool) t.join();
+    for (size_t t = 0; t < failures.size(); ++t)
+        if (failures[t].code != MCG_OK) {
+            result->error.code = failures[t].code;
+            result->error.step = failures[t].step;
+            result->error.sampling_unit = failed[t];
+            return failures[t].code;
+        }
+    // ordered reduction of one column
+    auto reduce = [&](size_t col, Statistics& st) {
+        std::vector<double> column;
+        if (!rqmc) {
+            column.resize(units);
+            for (uint64_t u = 0; u < units; ++u) column[u] = vals[u * width + col];
+        } else {
+            for (uint32_t s = 0; s < p.scrambles; ++s) {
+                NeumaierSum sum;
+                for (uint64_t i = 0; i < p.units; ++i) sum.add(vals[(s * p.units + i) * width + col]);
+                column.push_back(sum.total() / static_cast<double>(p.units));
+            }
+        }
+        st = Statistics{};
+        for (double v : column) st.sum.add(v);
+        st.moments = CenteredMoment::two_pass(column);
+    };
+    const uint64_t independent = rqmc ? p.scrambles : p.units;
+    std::vector<Statistics> total(kComponents);
+    for (int c = 0; c < kComponents; ++c) {
+        reduce(static_cast<size_t>(c), total[c]);
+        result->risk_components[c] = to_c(total[c]);
+    }
+    result->delta = estimate(total[MCG_DELTA], independent, 1.0);
+    result->gamma = estimate(total[MCG_GAMMA], independent, 1.0);
+    result->vega = estimate(total[MCG_VEGA], independent, 1.0);
+    result->bump_delta = estimate(total[MCG_BUMP_DELTA], independent, 1.0);
+    result->bump_gamma = estimate(total[MCG_BUMP_GAMMA], independent, 1.0);
+    result->bump_vega = estimate(total[MCG_BUMP_VEGA], independent, 1.0);
+    if (want_nodes)
+        for (size_t j = 0; j < nv; ++j) {
+            Statistics st;
+            reduce(kComponents + j, st);
+            result->local_vega_nodes[j] = to_c(st);
+            if (result->local_vega_node_estimates) result->local_vega_node_estimates[j] = estimate(st, independent, 1.0);
+        }
+    return MCG_OK;
+}
+
 double plan_discount(const mcg_plan_desc* desc, double t) {
     Curve c;
     c.set(desc->discount_curve.times, desc->discount_curve.discount_factors,

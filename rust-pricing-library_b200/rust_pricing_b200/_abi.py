@@ -222,7 +222,8 @@ class LsmResult(C.Structure):
         ("continuation_used", C.c_int32), ("mlp_steps", C.c_uint32), ("mlp_ms", C.c_float),
         ("mlp_final_loss", C.c_float), ("polynomial_in_sample", C.c_double), ("mlp_in_sample", C.c_double),
         ("mlp_param_capacity", C.c_uint32), ("mlp_params", C.POINTER(C.c_float)),
-        ("error", ErrorRecord),
+        ("node_capacity", C.c_uint32), ("local_vega_nodes", C.POINTER(Statistics)),
+                ("local_vega_node_estimates", C.POINTER(Estimate)), ("error", ErrorRecord),
     ]
 
 
@@ -230,7 +231,9 @@ class LsmBuffers:
     """Caller-owned storage for an early-exercise result of `dates` exercise
     dates and, when `stopping` > 0, that many valuation stopping indices."""
 
-    def __init__(self, dates: int, stopping: int = 0):
+    def __init__(self, dates: int, stopping: int = 0, nodes: int = 0):
+        self.node_stats = (Statistics * nodes)() if nodes else None
+        self.node_estimates = (Estimate * nodes)() if nodes else None
         self.models = (LsmDateModel * max(dates, 1))()
         self.counts = (C.c_uint64 * max(dates, 1))()
         self.stops = (C.c_uint32 * stopping)() if stopping else None
@@ -244,6 +247,10 @@ class LsmBuffers:
         self.result.stopping_capacity = stopping
         if stopping:
             self.result.stopping_indices = C.cast(self.stops, C.POINTER(C.c_uint32))
+        self.result.node_capacity = nodes
+        if nodes:
+            self.result.local_vega_nodes = C.cast(self.node_stats, C.POINTER(Statistics))
+            self.result.local_vega_node_estimates = C.cast(self.node_estimates, C.POINTER(Estimate))
 
 
 # ---- batched book ----

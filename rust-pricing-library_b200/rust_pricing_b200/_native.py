@@ -171,7 +171,8 @@ def lsm_price(spec, lsm, stopping: bool = False, stream: int = 0) -> A.LsmBuffer
     """mcg_lsm_price: train and value an early-exercise policy on the GPU."""
     paths = spec.sampling_units * (spec.scramble_count if spec.engine == A.ENGINE_RQMC else 1)
     paths *= 2 if spec.antithetic else 1
-    buf = A.LsmBuffers(len(spec.observation_times), paths if stopping else 0)
+    nodes = spec.grid_value_count() if spec.request_local_vega_nodes else 0
+    buf = A.LsmBuffers(len(spec.observation_times), paths if stopping else 0, nodes)
     desc, ldesc = spec.desc(), lsm.desc()
     status = library().mcg_lsm_price(C.byref(desc), C.byref(ldesc), C.c_void_p(stream), C.byref(buf.result))
     check(status, buf.result.error)

@@ -110,7 +110,8 @@ def oracle_lsm(spec, lsm, stopping: bool = False, threads: int | None = None):
     lib = oracle()
     paths = spec.sampling_units * (spec.scramble_count if spec.engine == A.ENGINE_RQMC else 1)
     paths *= 2 if spec.antithetic else 1
-    buf = A.LsmBuffers(len(spec.observation_times), paths if stopping else 0)
+    nodes = spec.grid_value_count() if spec.request_local_vega_nodes else 0
+    buf = A.LsmBuffers(len(spec.observation_times), paths if stopping else 0, nodes)
     desc, ldesc = spec.desc(), lsm.desc()
     rc = lib.oracle_lsm_price(C.byref(desc), C.byref(ldesc), C.byref(buf.result),
                               threads or os.cpu_count() or 1)

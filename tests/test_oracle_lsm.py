@@ -125,6 +125,30 @@ def test_flat_local_volatility_is_black_scholes(engine):
     assert abs(lv.result.in_sample_value - bs.result.in_sample_value) <= 1e-13 * bs.result.in_sample_value
 
 
+def test_flat_local_volatility_fixed_policy_risk_is_black_scholes():
+    """local_vol_fixed_policy_pseudo_statistics_with_vega_kt (early_exercise.rs:465-700)
+    on a flat local-variance grid: the reverse sweep's Vega (sum of the node
+    sensitivities, seed at each path's stopping date) is the Black--Scholes
+    pathwise Vega of fixed_policy_pathwise_values path by path, and the LV
+    Delta/Gamma (central spot bumps on common paths) are the Black--Scholes
+    bump-and-revalue validation components."""
+    kw = dict(dates=12, units=1 << 12, antithetic=True)
+    sb, lb = W.american_bs(vol=0.25, **kw)
+    sb.request_delta = sb.request_gamma = sb.request_vega = True
+    sl, ll = W.american_lv(W.flat_grid(0.25), **kw)
+    sl.request_delta = sl.request_gamma = sl.request_vega = sl.request_local_vega_nodes = True
+    bs = H.oracle_lsm(sb, lb, stopping=True, threads=4).result
+    buf = H.oracle_lsm(sl, ll, stopping=True, threads=4)
+    lv = buf.result
+    assert abs(lv.vega.value - bs.vega.value) <= 1e-12 * abs(bs.vega.value)
+    assert abs(lv.vega.standard_error - bs.vega.standard_error) <= 1e-10 * bs.vega.standard_error
+    for mine, theirs in (("delta", "bump_delta"), ("gamma", "bump_gamma")):
+        a, b = getattr(lv, mine), getattr(bs, theirs)
+        assert abs(a.value - b.value) <= 1e-10 * max(abs(b.value), b.standard_error), mine
+    nodes = np.array([e.value for e in buf.node_estimates])
+    assert abs(nodes.sum() - lv.vega.value) <= 1e-12 * abs(lv.vega.value)
+
+
 def test_thread_count_does_not_change_the_result():
     spec, lsm = L.plan(CASES[0])
     a = H.oracle_lsm(spec, lsm, stopping=True, threads=1)
