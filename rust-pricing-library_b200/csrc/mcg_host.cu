@@ -62,9 +62,15 @@ struct AdjointArgs {
     double* node_tiles;
     double* out_price;
     double* out_diag;
+    const uint32_t* stops;
+    uint32_t stop_stride;
+    const double* exercise_df;
 };
 cudaError_t launch_lv_adjoint_price(const double* price, const double* diag, uint64_t units, int pairs,
                                     uint32_t tile_offset, uint32_t mask, StatRecord* partials, cudaStream_t stream);
+cudaError_t launch_lv_fixed_policy_combine(const double* price, const double* vega, uint64_t units, int pairs,
+                                           int crn, int gamma, int want_vega, double h, uint32_t tile_offset,
+                                           StatRecord* partials, cudaStream_t stream);
 size_t lv_adjoint_smem(const DevicePlan& P);
 cudaError_t launch_lv_adjoint(const DevicePlan& P, const AdjointArgs& A, ErrorWord* err, cudaStream_t stream);
 cudaError_t launch_lv_adjoint_combine(const double* vega, const double* delta, uint64_t units, int pairs,
@@ -859,6 +865,33 @@ HostStat two_pass(const std::vector<double>& values) {
     return h;
 }
 
+// Statistics of grid node k from the per-scramble node records: pseudo-MC
+// from the 128-path tile sums (batch means), RQMC from the scramble means.
+HostStat node_statistics(const std::vector<StatRecord>& node_rec, uint32_t nv, uint32_t k, uint64_t units,
+                         uint32_t scrambles, bool rqmc) {
+    HostStat h;
+    if (!rqmc) {
+        const StatRecord& x = node_rec[k];
+        const double total = x.sum + x.corr;
+        const double n = static_cast<double>(units);
+        const double tiles = x.count;
+        const double batch = n / tiles;
+        const double s2 = tiles > 1.0 ? x.m2 / (tiles - 1.0) / (batch * batch) : 0.0;
+        h.sum = x.sum;
+        h.corr = x.corr;
+        h.count = units;
+        h.mean = total / n;
+        h.m2 = (s2 / tiles) * n * (n - 1.0);
+    } else {
+        std::vector<double> reps(scrambles);
+        for (uint32_t sc = 0; sc < scrambles; ++sc)
+            reps[sc] = (node_rec[static_cast<size_t>(sc) * nv + k].sum + node_rec[static_cast<size_t>(sc) * nv + k].corr) /
+                       static_cast<double>(units);
+        h = two_pass(reps);
+    }
+    return h;
+}
+
 mcg_estimate make_estimate(const HostStat& s, uint64_t units, double scale) {
     const double inv = 1.0 / static_cast<double>(units);
     const double value = s.total() * inv * scale;
@@ -1099,26 +1132,7 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
         // batch means of the 128-unit CTA tiles, RQMC from the scramble means.
         const uint32_t nv = plan->grid_values;
         for (uint32_t k = 0; k < nv; ++k) {
-            HostStat h;
-            if (!rqmc) {
-                const StatRecord& x = node_rec[k];
-                const double total = x.sum + x.corr;
-                const double n = static_cast<double>(P.units);
-                const double tiles = x.count;
-                const double batch = n / tiles;
-                const double s2 = tiles > 1.0 ? x.m2 / (tiles - 1.0) / (batch * batch) : 0.0;
-                h.sum = x.sum;
-                h.corr = x.corr;
-                h.count = P.units;
-                h.mean = total / n;
-                h.m2 = (s2 / tiles) * n * (n - 1.0);
-            } else {
-                std::vector<double> reps(P.scramble_count);
-                for (uint32_t sc = 0; sc < P.scramble_count; ++sc)
-                    reps[sc] = (node_rec[static_cast<size_t>(sc) * nv + k].sum + node_rec[static_cast<size_t>(sc) * nv + k].corr) /
-                               static_cast<double>(P.units);
-                h = two_pass(reps);
-            }
+            const HostStat h = node_statistics(node_rec, nv, k, P.units, P.scramble_count, rqmc);
             result->local_vega_nodes[k] = {h.sum, h.corr, h.count, h.mean, h.m2};
             if (result->local_vega_node_estimates)
                 result->local_vega_node_estimates[k] = make_estimate(h, independent, 1.0);
@@ -1143,6 +1157,7 @@ struct LsmBuffers {
     DeviceArray<unsigned int> tickets;
     DeviceArray<unsigned long long> counts, words;
     DeviceArray<StatRecord> risk_partials, risk_records;
+    DeviceArray<double> risk_price;  // local volatility: exercise-value prices [pair][runtime][unit]
     DeviceArray<double> vspots;      // local volatility: valuation path store (when the training one is too small)
     DeviceArray<ErrorWord> path_errors;  // local volatility: [0] training, [1] valuation
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -1151,6 +1166,7 @@ struct LsmBuffers {
         path_errors.release();
         risk_partials.release();
         risk_records.release();
+        risk_price.release();
         spots.release();
         cf.release();
         df.release();
@@ -1186,13 +1202,13 @@ mcg_status validate_lsm(const mcg_plan_desc* d, const mcg_lsm_desc* l, const mcg
     if (d->abi_version != MCG_ABI_VERSION) return fail(MCG_ERR_INVALID_ARGUMENT, "abi_version mismatch");
     if (d->product_count != 1 || !d->products || d->products[0].kind != MCG_PRODUCT_AMERICAN)
         return fail(MCG_ERR_INVALID_ARGUMENT, "an early-exercise plan holds exactly one American product");
-    if (d->request_local_vega_nodes)
-        return fail(MCG_ERR_UNSUPPORTED, "local vega nodes need a local-volatility plan");
     if (d->model != MCG_MODEL_BLACK_SCHOLES && d->model != MCG_MODEL_LOCAL_VOLATILITY)
         return fail(MCG_ERR_INVALID_ARGUMENT, "model");
-    if (d->model == MCG_MODEL_LOCAL_VOLATILITY && (d->request_delta || d->request_gamma || d->request_vega))
-        return fail(MCG_ERR_UNSUPPORTED,
-                    "fixed-policy risk under local volatility needs VegaKT reporting, which is not built");
+    if (d->request_local_vega_nodes && d->model != MCG_MODEL_LOCAL_VOLATILITY)
+        return fail(MCG_ERR_UNSUPPORTED, "local vega nodes need a local-volatility plan");
+    if (d->model == MCG_MODEL_LOCAL_VOLATILITY && d->precision != MCG_PRECISION_F64 &&
+        (d->request_delta || d->request_gamma || d->request_vega || d->request_local_vega_nodes))
+        return fail(MCG_ERR_UNSUPPORTED, "early-exercise risk runs in FP64");
     if (d->request_gamma) {
         const double b = resolve_gamma_bump(d);
         if (!std::isfinite(b) || b <= 0.0 || b >= d->spot)
@@ -1234,8 +1250,8 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     vd.products = &placeholder;
     vd.payment_time = d->observation_times[d->observation_count - 1];
     // Risk is taken by the fixed-policy pass below, not by the path plans.
-    const bool risk = d->request_delta || d->request_gamma || d->request_vega;
-    vd.request_delta = vd.request_gamma = vd.request_vega = 0;
+    const bool risk = d->request_delta || d->request_gamma || d->request_vega || d->request_local_vega_nodes;
+    vd.request_delta = vd.request_gamma = vd.request_vega = vd.request_local_vega_nodes = 0;
     mcg_plan_desc td = vd;
     td.master_seed = l->training_seed;
     td.sampling_units = l->training_units;
@@ -1515,7 +1531,74 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     // Fixed-policy risk: the valuation stopping dates held, per-tile records
     // of the pathwise components merged per scramble.
     const uint32_t risk_tiles = lsm_risk_tiles(VP.units);
-    if (risk) {
+    // Local volatility: the fixed-policy risk runs the adjoint sweeps of a risk
+    // plan (the valuation plan with the requests) in exercise-value mode, one
+    // per spot runtime (base for the price, Vega and nodes; down and up for
+    // the CRN Delta/Gamma), every path paying at its own stopping date.
+    mcg_plan rplan;
+    std::vector<StatRecord> lv_node_rec;
+    if (risk && lv) {
+        mcg_plan_desc rd = vd;
+        rd.request_delta = d->request_delta;
+        rd.request_gamma = d->request_gamma;
+        rd.request_vega = 1;
+        rd.request_local_vega_nodes = d->request_local_vega_nodes;
+        if ((st = build(&rd, rplan)) != MCG_OK) return st;
+        const DevicePlan& RP = rplan.dp;
+        const int pairs = RP.antithetic ? 2 : 1;
+        const bool crn = RP.lv_bumps != 0;
+        const uint64_t chunk = rplan.chunk_units;
+        MCG_CUDA(B.risk_partials.alloc(static_cast<size_t>(v_groups) * rplan.tiles * kComponents));
+        MCG_CUDA(B.risk_records.alloc(static_cast<size_t>(v_groups) * kComponents));
+        MCG_CUDA(B.risk_price.alloc(6 * chunk));
+        const ErrorWord init{~0ull, 0, 0, 0, 0};
+        MCG_CUDA(cudaMemcpyAsync(rplan.error.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        for (uint32_t sc = 0; sc < RP.scramble_count; ++sc)
+            for (uint64_t begin = 0; begin < RP.units; begin += chunk) {
+                const uint64_t n = std::min<uint64_t>(chunk, RP.units - begin);
+                const uint32_t tile_offset = sc * rplan.tiles + static_cast<uint32_t>(begin / kThreads);
+                for (int pr = 0; pr < pairs; ++pr)
+                    for (int which : {1, 2, 0}) {
+                        if (which != 0 && !crn) continue;
+                        AdjointArgs AA{};
+                        AA.which = which;
+                        AA.sign = pr == 0 ? 1.0 : -1.0;
+                        AA.node_weight = pairs == 2 ? 0.5 : 1.0;
+                        AA.node_add = pr;
+                        AA.scramble = sc;
+                        AA.unit_begin = begin;
+                        AA.units = n;
+                        AA.tile_offset = tile_offset;
+                        AA.tape_f = rplan.tape.ptr;
+                        AA.tape_z = rplan.tape.ptr + static_cast<size_t>(RP.steps + 1) * chunk;
+                        AA.out_vega = rplan.adj_vega.ptr + static_cast<size_t>(pr * 3 + which) * n;
+                        AA.out_delta = rplan.adj_delta.ptr + static_cast<size_t>(pr * 3 + which) * n;
+                        AA.node_tiles = (which == 0 && rplan.adjoint_nodes) ? rplan.node_tiles.ptr : nullptr;
+                        AA.out_price = B.risk_price.ptr + static_cast<size_t>(pr * 3 + which) * n;
+                        AA.stops = B.vstops.ptr + ((static_cast<uint64_t>(sc) * RP.units + begin) * pairs + pr);
+                        AA.stop_stride = static_cast<uint32_t>(pairs);
+                        AA.exercise_df = B.df.ptr;
+                        MCG_CUDA(launch_lv_adjoint(RP, AA, rplan.error.ptr, stream));
+                        ++launches;
+                    }
+                MCG_CUDA(launch_lv_fixed_policy_combine(B.risk_price.ptr, rplan.adj_vega.ptr, n, pairs, crn ? 1 : 0,
+                                                        d->request_gamma ? 1 : 0, 1, RP.spot_bump, tile_offset,
+                                                        B.risk_partials.ptr, stream));
+                ++launches;
+            }
+        reduce_tiles_kernel<<<dim3(kComponents, v_groups), 256, 0, stream>>>(B.risk_partials.ptr, rplan.tiles,
+                                                                            kComponents, B.risk_records.ptr);
+        MCG_CUDA(cudaGetLastError());
+        ++launches;
+        if (rplan.adjoint_nodes && r->local_vega_nodes && r->node_capacity >= rplan.grid_values) {
+            MCG_CUDA(launch_lv_node_reduce(rplan.node_tiles.ptr, rplan.tiles, RP.scramble_count, rplan.grid_values,
+                                           rplan.node_records.ptr, stream));
+            ++launches;
+            lv_node_rec.resize(static_cast<size_t>(RP.scramble_count) * rplan.grid_values);
+            MCG_CUDA(cudaMemcpyAsync(lv_node_rec.data(), rplan.node_records.ptr, lv_node_rec.size() * sizeof(StatRecord),
+                                     cudaMemcpyDeviceToHost, stream));
+        }
+    } else if (risk) {
         MCG_CUDA(B.risk_partials.alloc(static_cast<size_t>(v_groups) * risk_tiles * kComponents));
         MCG_CUDA(B.risk_records.alloc(static_cast<size_t>(v_groups) * kComponents));
         LsmRiskArgs R{};
@@ -1623,6 +1706,22 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     std::memset(r->risk_components, 0, sizeof(r->risk_components));
     r->delta = r->gamma = r->vega = mcg_estimate{};
     r->bump_delta = r->bump_gamma = r->bump_vega = mcg_estimate{};
+    if (risk && lv) {
+        ErrorWord ew{~0ull, 0, 0, 0, 0};
+        MCG_CUDA(cudaMemcpy(&ew, rplan.error.ptr, sizeof(ew), cudaMemcpyDeviceToHost));
+        if (ew.key != ~0ull) {
+            r->error.code = static_cast<int32_t>(ew.key & 0xff);
+            r->error.sampling_unit = ew.key >> 8;
+            return fail(static_cast<mcg_status>(r->error.code),
+                        "fixed-policy risk: sampling unit " + std::to_string(r->error.sampling_unit) + " failed");
+        }
+        const uint32_t nv = rplan.grid_values;
+        for (uint32_t k = 0; k < nv && !lv_node_rec.empty(); ++k) {
+            const HostStat h = node_statistics(lv_node_rec, nv, k, VP.units, VP.scramble_count, rqmc);
+            r->local_vega_nodes[k] = {h.sum, h.corr, h.count, h.mean, h.m2};
+            if (r->local_vega_node_estimates) r->local_vega_node_estimates[k] = make_estimate(h, independent, 1.0);
+        }
+    }
     if (risk) {
         HostStat rs[kComponents];
         for (int c = 0; c < kComponents; ++c) {

@@ -38,6 +38,13 @@ struct AdjointArgs {
     double* node_tiles;     // [global tile][nt * nx] or null
     double* out_price;      // [units] discounted payoff of the forward pass, or null
     double* out_diag;       // [8][units] continuous-barrier diagnostics, or null
+    // Early exercise under a fixed policy: when set, the payoff is the exercise
+    // value max(+-(S_k - K), 0) * notional at the path's stopping date
+    // k = stops[local * stop_stride], discounted by exercise_df[k]
+    // (the American payoff graph's output k with its cash-flow discount).
+    const uint32_t* stops;
+    uint32_t stop_stride;
+    const double* exercise_df;
 };
 
 struct InterpFull {
@@ -187,6 +194,9 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     int fail_code = 0;
     uint32_t fail_step = 0;
     int32_t argmax = 0;
+    const bool fixed = A.stops != nullptr;
+    const uint32_t k_stop = fixed && valid ? A.stops[local * A.stop_stride] : 0u;
+    double f_stop = f;
     if (barrier) barrier_begin(pp, acc, h, f, failed);
     if (valid) A.tape_f[local] = f;
     double* w = s_w + threadIdx.x;
@@ -228,6 +238,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
             A.tape_f[static_cast<size_t>(s + 1) * ustride + local] = f;
         }
         const int32_t obs = P.obs_of_node[s + 1];
+        if (fixed && obs == static_cast<int32_t>(k_stop)) f_stop = f;
         if (obs >= 0) {
             if (pp.kind == MCG_PRODUCT_LOOKBACK) {
                 if (obs == 0 || (call ? !(acc.a >= f) : !(acc.a <= f))) argmax = obs;
@@ -267,6 +278,12 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
         terminal_adj = P.discount * td * 1.0;
         exact_active = !(acc.initial_touched || acc.touched);
         lsa = P.discount * sd * surv;
+    } else if (fixed) {
+        // exercise value at the stopping date and its spot adjoint
+        const double dfk = A.exercise_df[k_stop];
+        const double in = call ? f_stop - pp.strike : pp.strike - f_stop;
+        if (A.out_price && valid) A.out_price[local] = dfk * ((in >= 0.0 ? in : 0.0) * pp.notional);
+        terminal_adj = dfk * ((in >= 0.0 ? pp.notional : 0.0) * (call ? 1.0 : -1.0)) * 1.0;
     } else {
         if (A.out_price && valid) A.out_price[local] = P.discount * acc_payoff(pp, acc, h);
         // d payoff / d observed spot (tape.rs:594-781 reverse semantics)
@@ -318,6 +335,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     auto obs_seed = [&](uint32_t node) -> double {
         const int32_t obs = P.obs_of_node[node];
         if (obs < 0 || barrier) return 0.0;
+        if (fixed) return obs == static_cast<int32_t>(k_stop) ? terminal_adj : 0.0;
         if (pp.kind == MCG_PRODUCT_ASIAN) return P.discount * (asian_g * pp.weights[obs]) * 1.0;
         if (pp.kind == MCG_PRODUCT_LOOKBACK) return obs == argmax ? P.discount * asian_g * 1.0 : 0.0;
         return 0.0;
@@ -332,8 +350,8 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     double f_next = f;
     InterpFull in_next = inN;
     double sa_next = obs_seed(steps);
-    if (!barrier && (pp.kind == MCG_PRODUCT_EUROPEAN || pp.kind == MCG_PRODUCT_DIGITAL ||
-                     pp.kind == MCG_PRODUCT_DISCRETE_BARRIER))
+    if (!barrier && !fixed &&
+        (pp.kind == MCG_PRODUCT_EUROPEAN || pp.kind == MCG_PRODUCT_DIGITAL || pp.kind == MCG_PRODUCT_DISCRETE_BARRIER))
         sa_next += terminal_adj;
     if (barrier) {
         sa_next += terminal_adj;
@@ -460,6 +478,47 @@ __global__ void __launch_bounds__(kThreads) lv_adjoint_price_kernel(const double
                                   partials + static_cast<size_t>(tile_offset + blockIdx.x) * kComponents, s_red);
 }
 
+// Fixed-policy risk components of a chunk's units: the exercise-value
+// prices of the base and bumped spot runtimes (price[(pr * 3 + which) * units + u]),
+// the base sweep's Vega; CRN Delta/Gamma as the path kernel forms them,
+// antithetic pairs averaged component-wise (average_local_vol_pathwise).
+__global__ void __launch_bounds__(kThreads) lv_fixed_policy_combine_kernel(
+    const double* price, const double* vega, uint64_t units, int pairs, int crn, int gamma, int want_vega, double h,
+    uint32_t tile_offset, StatRecord* partials) {
+    __shared__ Stat s_red[4 * kComponents];
+    const uint64_t u = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    const bool valid = u < units;
+    double vals[kComponents];
+#pragma unroll
+    for (int c = 0; c < kComponents; ++c) vals[c] = 0.0;
+    if (valid) {
+        for (int pr = 0; pr < pairs; ++pr) {
+            double comp[kComponents];
+#pragma unroll
+            for (int c = 0; c < kComponents; ++c) comp[c] = 0.0;
+            const double base = price[(static_cast<size_t>(pr) * 3 + 0) * units + u];
+            comp[MCG_PRICE] = base;
+            if (want_vega) comp[MCG_VEGA] = vega[(static_cast<size_t>(pr) * 3 + 0) * units + u];
+            if (crn) {
+                const double down = price[(static_cast<size_t>(pr) * 3 + 1) * units + u];
+                const double up = price[(static_cast<size_t>(pr) * 3 + 2) * units + u];
+                const double delta = (up - down) / (2.0 * h);
+                comp[MCG_DELTA] = delta;
+                comp[MCG_BUMP_DELTA] = delta;
+                if (gamma) {
+                    const double g = (up - 2.0 * base + down) / (h * h);
+                    comp[MCG_GAMMA] = g;
+                    comp[MCG_BUMP_GAMMA] = g;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < kComponents; ++c) vals[c] = pr == 0 ? comp[c] : (vals[c] + comp[c]) * 0.5;
+        }
+    }
+    cta_reduce_write<kComponents>(vals, valid, 0x3ffu,
+                                  partials + static_cast<size_t>(tile_offset + blockIdx.x) * kComponents, s_red);
+}
+
 // Node sums over tiles, per scramble: Neumaier sum in tile order and the
 // two-pass second moment of the tile sums (batch means).
 __global__ void lv_node_reduce_kernel(const double* node_tiles, uint32_t tiles_per_scramble,
@@ -507,6 +566,15 @@ cudaError_t launch_lv_adjoint_price(const double* price, const double* diag, uin
                                     uint32_t tile_offset, uint32_t mask, StatRecord* partials, cudaStream_t stream) {
     const unsigned blocks = static_cast<unsigned>((units + kThreads - 1) / kThreads);
     lv_adjoint_price_kernel<<<blocks, kThreads, 0, stream>>>(price, diag, units, pairs, tile_offset, mask, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lv_fixed_policy_combine(const double* price, const double* vega, uint64_t units, int pairs,
+                                           int crn, int gamma, int want_vega, double h, uint32_t tile_offset,
+                                           StatRecord* partials, cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>((units + kThreads - 1) / kThreads);
+    lv_fixed_policy_combine_kernel<<<blocks, kThreads, 0, stream>>>(price, vega, units, pairs, crn, gamma, want_vega,
+                                                                    h, tile_offset, partials);
     return cudaGetLastError();
 }
 

@@ -226,12 +226,48 @@ def test_local_volatility_learned_policy(engine, ssvi_grid):
     assert r.price.value >= poly.result.price.value - 6 * poly.result.price.standard_error
 
 
-def test_local_volatility_risk_is_refused(engine, ssvi_grid):
-    spec, lsm = W.american_lv(ssvi_grid, dates=4, units=1 << 10)
-    spec.request_delta = True
-    with pytest.raises(N.EngineError) as err:
-        N.lsm_price(spec, lsm)
-    assert err.value.name == "unsupported"
+LV_RISK_CASES = {
+    "lv-pseudo-antithetic-bridge": dict(dates=8, units=3001, training_units=2001, antithetic=True, bridge=True),
+    "lv-rqmc-antithetic-bridge": dict(dates=6, units=1 << 9, engine=A.ENGINE_RQMC, antithetic=True, scrambles=4,
+                                      bridge=True),
+}
+
+
+@pytest.mark.parametrize("name", sorted(LV_RISK_CASES))
+def test_local_volatility_fixed_policy_risk_matches_the_oracle(engine, ssvi_grid, name):
+    """Fixed-policy Delta/Gamma (CRN spot bumps), Vega and node sensitivities
+    of an American put under the SSVI local-variance grid: the adjoint sweeps
+    in exercise-value mode against the oracle's
+    local_vol_fixed_policy_*_statistics restatement."""
+    spec, lsm = W.american_lv(ssvi_grid, **LV_RISK_CASES[name])
+    spec.request_delta = spec.request_gamma = spec.request_vega = spec.request_local_vega_nodes = True
+    got = N.lsm_price(spec, lsm, stopping=True)
+    want = H.oracle_lsm(spec, lsm, stopping=True, threads=8)
+    assert_same_result(spec, lsm, got, want)
+    g, w = got.result, want.result
+    for name_ in ("delta", "gamma", "vega", "bump_delta", "bump_gamma"):
+        a, b = getattr(g, name_), getattr(w, name_)
+        assert abs(a.value - b.value) <= G.DIRECT_TOL * max(abs(b.value), b.standard_error), (name_, a.value, b.value)
+        assert abs(a.standard_error - b.standard_error) <= 1e-9 * b.standard_error, name_
+    p = g.risk_components[A.PRICE]
+    assert rel((p.sum + p.correction) / g.independent_sampling_units, g.price.value) <= 1e-12
+    gm = np.array([e.value for e in got.node_estimates])
+    wm = np.array([e.value for e in want.node_estimates])
+    assert np.max(np.abs(gm - wm)) <= 1e-11 * np.max(np.abs(wm))
+    assert abs(gm.sum() - g.vega.value) <= 1e-11 * abs(g.vega.value)
+
+
+def test_flat_local_volatility_fixed_policy_vega_is_black_scholes(engine):
+    kw = dict(dates=10, units=1 << 12, antithetic=True)
+    sb, lb = W.american_bs(vol=0.25, **kw)
+    sb.request_delta = sb.request_gamma = sb.request_vega = True
+    sl, ll = W.american_lv(W.flat_grid(0.25), **kw)
+    sl.request_delta = sl.request_gamma = sl.request_vega = True
+    bs = N.lsm_price(sb, lb).result
+    lv = N.lsm_price(sl, ll).result
+    assert abs(lv.vega.value - bs.vega.value) <= 1e-12 * abs(bs.vega.value)
+    assert abs(lv.delta.value - bs.bump_delta.value) <= 1e-10 * max(abs(bs.bump_delta.value), bs.bump_delta.standard_error)
+
 
 
 RISK_CASES = {
