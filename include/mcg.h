@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MCG_ABI_VERSION 1u
+#define MCG_ABI_VERSION 2u
 
 /* Component layout of one sampling unit, crates/pricing/src/engine/plan/simulation.rs:26-62. */
 #define MCG_PRICE 0
@@ -146,9 +146,22 @@ typedef struct mcg_product_desc {
     int32_t has_rebate;
     double barrier;
     double rebate;
-    /* Arithmetic Asian weights, one per plan observation (NULL for other kinds),
-     * crates/pricing/src/engine/payoff/compile.rs:159-202. */
+    /* One value per plan observation.  Arithmetic Asian: the weight of the
+     * observation (required; crates/pricing/src/engine/payoff/compile.rs:159-202).
+     * Discrete barrier and fixed lookback: optional monitoring flags, 0.0 where
+     * the observation is not one of the product's monitoring dates (a barrier
+     * whose expiry is not monitored); NULL monitors every observation. */
     const double* observation_weights;
+    /* Seasoned state, the literals of the reference's graphs for dates before
+     * the first simulated observation.  Asian: the weighted sum of the known
+     * fixings, accumulated in observation order (compile.rs:162-176).  Fixed
+     * lookback: the running extremum before the first simulated monitoring date,
+     * from the historical extremum and/or the valuation-date fixing
+     * (compile.rs:405-440).  Discrete barrier: 1.0 when the barrier was hit
+     * before the valuation date, else 0.0 (compile.rs:293-297).  Ignored
+     * unless has_initial_state is nonzero. */
+    int32_t has_initial_state;
+    double initial_state;
 } mcg_product_desc;
 
 /* The compiled plan: the hot-path part of the reference's SimulationPlan. */

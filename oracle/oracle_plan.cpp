@@ -342,6 +342,11 @@ bool smooth_interval(bool up, double ls, double rs, double lb, double rb, double
 struct Product {
     mcg_product_desc d;
     std::vector<double> weights;
+    // Discrete barrier / lookback monitoring flags (every observation without flags).
+    bool monitored(size_t i) const {
+        return (d.kind != MCG_PRODUCT_DISCRETE_BARRIER && d.kind != MCG_PRODUCT_LOOKBACK) ||
+               weights.empty() || weights[i] != 0.0;
+    }
 };
 
 struct Plan {
@@ -567,7 +572,8 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
         return ind * base;
     }
     case MCG_PRODUCT_ASIAN: {
-        double sum = 0.0;
+        // Known fixings first (compile.rs:162-176), then the simulated observations.
+        double sum = d.has_initial_state ? d.initial_state : 0.0;
         for (size_t i = 0; i < n; ++i) sum = sum + spots[i] * pr.weights[i];
         const double in = call ? sum - d.strike : d.strike - sum;
         const double pos = in >= 0.0 ? in : 0.0;
@@ -578,10 +584,18 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
         return pos * d.notional;
     }
     case MCG_PRODUCT_LOOKBACK: {
-        double ext = spots[0];
-        size_t arg = 0;
-        for (size_t i = 1; i < n; ++i) {
-            if (call) {
+        // The historical extremum (or valuation-date fixing) is a literal, the
+        // first simulated monitoring date otherwise (compile.rs:426-452).
+        bool seeded = d.has_initial_state != 0;
+        double ext = seeded ? d.initial_state : 0.0;
+        size_t arg = n;  // n: the literal holds the extremum
+        for (size_t i = 0; i < n; ++i) {
+            if (!pr.monitored(i)) continue;
+            if (!seeded) {
+                ext = spots[i];
+                arg = i;
+                seeded = true;
+            } else if (call) {
                 if (!(ext >= spots[i])) { ext = spots[i]; arg = i; }
             } else {
                 if (!(ext <= spots[i])) { ext = spots[i]; arg = i; }
@@ -589,7 +603,7 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
         }
         const double in = call ? ext - d.strike : d.strike - ext;
         const double pos = in >= 0.0 ? in : 0.0;
-        if (adj) adj[arg] = (in >= 0.0 ? d.notional : 0.0) * (call ? 1.0 : -1.0);
+        if (adj && arg < n) adj[arg] = (in >= 0.0 ? d.notional : 0.0) * (call ? 1.0 : -1.0);
         return pos * d.notional;
     }
     case MCG_PRODUCT_DISCRETE_BARRIER: {
@@ -598,7 +612,7 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
         const double pos = in >= 0.0 ? in : 0.0;
         const double vanilla = pos * d.notional;
         const bool up = d.barrier_direction == MCG_BARRIER_UP;
-        double hit = 0.0;
+        double hit = d.has_initial_state ? d.initial_state : 0.0;  // historical hit, compile.rs:293-297
         std::vector<double> hist, weights, firsts;
         if (adj && h > 0.0) {
             hist.resize(n);
@@ -606,6 +620,14 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
             firsts.resize(n);
         }
         for (size_t i = 0; i < n; ++i) {
+            if (!pr.monitored(i)) {
+                if (adj && h > 0.0) {
+                    hist[i] = hit;
+                    weights[i] = 0.0;
+                    firsts[i] = 0.0;
+                }
+                continue;
+            }
             const double dist = up ? spots[i] - d.barrier : d.barrier - spots[i];
             double wgt;
             if (h > 0.0) {

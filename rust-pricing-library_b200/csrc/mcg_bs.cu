@@ -39,6 +39,10 @@ __global__ void __launch_bounds__(kThreads) bs_path_kernel(const DevicePlan P, u
     bs_path_tile<NP>(P, s_red, scramble, point, valid, tile_out, mask, err, detail);
 }
 
+cudaError_t launch_bs_path_risk(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
+                                StatRecord* partials, uint32_t mask, ErrorWord* err, int detail,
+                                cudaStream_t stream);
+
 cudaError_t launch_bs_path(const DevicePlan& P, bool single_terminal, uint64_t unit_begin, uint64_t units,
                            uint32_t scrambles, StatRecord* partials, uint32_t mask, ErrorWord* err,
                            int detail, cudaStream_t stream) {
@@ -50,7 +54,7 @@ cudaError_t launch_bs_path(const DevicePlan& P, bool single_terminal, uint64_t u
             bs_terminal_kernel<false><<<grid, kThreads, 0, stream>>>(P, unit_begin, partials, mask, err, detail);
         return cudaGetLastError();
     }
-    if (P.risk) return cudaErrorNotSupported;
+    if (P.risk) return launch_bs_path_risk(P, unit_begin, units, scrambles, partials, mask, err, detail, stream);
     const int np = static_cast<int>(P.product_count);
     if (np == 1) bs_path_kernel<1><<<grid, kThreads, 0, stream>>>(P, unit_begin, partials, mask, err, detail);
     else if (np == 2) bs_path_kernel<2><<<grid, kThreads, 0, stream>>>(P, unit_begin, partials, mask, err, detail);

@@ -183,7 +183,7 @@ __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, u
     for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
-            acc_init(acc[e][k]);
+            acc_init(acc[e][k], P.products[k]);
             if (k < static_cast<int>(P.product_count) &&
                 P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
                 barrier_begin(P.products[k], acc[e][k], P.smoothing, P.spot, failed);

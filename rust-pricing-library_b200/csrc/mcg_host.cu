@@ -468,6 +468,8 @@ mcg_status validate_products(const mcg_plan_desc* d, std::vector<ProductParams>&
         q.has_rebate = p.has_rebate;
         q.barrier = p.barrier;
         q.rebate = p.rebate;
+        q.has_initial = p.has_initial_state != 0;
+        q.initial = p.initial_state;
         if (p.kind < MCG_PRODUCT_EUROPEAN || p.kind > MCG_PRODUCT_CONTINUOUS_BARRIER)
             return fail(MCG_ERR_UNSUPPORTED, "product kind " + std::to_string(p.kind));
         if (!(p.notional > 0.0) || !std::isfinite(p.strike) || p.strike <= 0.0)
@@ -477,6 +479,14 @@ mcg_status validate_products(const mcg_plan_desc* d, std::vector<ProductParams>&
             return fail(MCG_ERR_INVALID_ARGUMENT, "barrier level must be positive");
         if (p.kind == MCG_PRODUCT_ASIAN && !p.observation_weights)
             return fail(MCG_ERR_INVALID_ARGUMENT, "Asian product needs observation weights");
+        if (p.has_initial_state) {
+            if (p.kind != MCG_PRODUCT_ASIAN && p.kind != MCG_PRODUCT_LOOKBACK &&
+                p.kind != MCG_PRODUCT_DISCRETE_BARRIER)
+                return fail(MCG_ERR_UNSUPPORTED, "seasoned state of a product without observation history");
+            if (!std::isfinite(p.initial_state) ||
+                (p.kind == MCG_PRODUCT_DISCRETE_BARRIER && p.initial_state != 0.0 && p.initial_state != 1.0))
+                return fail(MCG_ERR_INVALID_ARGUMENT, "initial_state");
+        }
         if (p.kind != MCG_PRODUCT_EUROPEAN && p.kind != MCG_PRODUCT_DIGITAL) single = false;
         out.push_back(q);
     }
@@ -566,7 +576,8 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         plan.total_variance = d->volatility * d->volatility * expiry;
         P.zero_variance = plan.total_variance == 0.0;
         P.risk = risk;
-        if (risk && !single) return fail(MCG_ERR_UNSUPPORTED, "Black-Scholes risk for path-dependent products");
+        if (risk && !single && d->product_count != 1)
+            return fail(MCG_ERR_UNSUPPORTED, "Black-Scholes path risk prices one product per plan");
         std::vector<double> of(n), ot(n), sq(n);
         double prev = 0.0;
         for (uint32_t i = 0; i < n; ++i) {
@@ -586,7 +597,7 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         P.dimension = n;
         plan.single_terminal = single;
         plan.mask = 1u;
-        if (risk && single) plan.mask = 0x3ffu;
+        if (risk) plan.mask = 0x3ffu;
         if (has_continuous) plan.mask |= 0xffu << 10;
     } else {
         // exercise-date times, for the early-exercise engine's network inputs
@@ -805,6 +816,20 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
     MCG_CUDA(plan.partials.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * plan.product_count * kComponents));
     MCG_CUDA(plan.records.alloc(static_cast<size_t>(P.scramble_count) * plan.product_count * kComponents));
     MCG_CUDA(plan.error.alloc(1));
+    if (!lv && P.risk && !plan.single_terminal) {
+        // Scratch of the path-risk kernel: W_k per thread, and the hit state,
+        // weight and slope per observation for a smoothed discrete barrier.
+        const bool smooth_barrier =
+            plan.products[0].kind == MCG_PRODUCT_DISCRETE_BARRIER && P.smoothing > 0.0;
+        P.bs_tape_rows = P.observation_count * (smooth_barrier ? 4u : 1u);
+        const uint64_t budget = (256ull << 20) / (sizeof(double) * P.bs_tape_rows * P.scramble_count);
+        const uint64_t units_rounded = (P.units + kThreads - 1) / kThreads * kThreads;
+        const uint64_t per_scramble =
+            std::min<uint64_t>(units_rounded, std::max<uint64_t>(kThreads, budget / kThreads * kThreads));
+        P.bs_tape_units = per_scramble * P.scramble_count;
+        MCG_CUDA(plan.tape.alloc(static_cast<size_t>(P.bs_tape_rows) * P.bs_tape_units));
+        P.bs_tape = plan.tape.ptr;
+    }
     if (plan.adjoint) {
         // Per-step checkpoints of one chunk of units: states (steps + 1) and shocks (steps).
         plan.chunk_units = std::min<uint64_t>(P.units, 1ull << 20);
@@ -933,6 +958,11 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
     }
     if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("path kernel: ") + cudaGetErrorString(e));
     const uint32_t width = plan->product_count * kComponents;
+    if (P.bs_tape) {
+        // the path-risk kernel runs in scratch-sized chunks of units
+        const uint64_t per_launch = P.bs_tape_units / P.scramble_count / kThreads * kThreads;
+        launches += static_cast<uint32_t>((P.units + per_launch - 1) / per_launch) - 1;
+    }
     if (!plan->price_from_adjoint) {
         ++launches;
         MCG_CUDA(cudaEventRecord(tp, stream));

@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2 && CB == 0) ? 8 :
         hint[e] = 0;
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
-            acc_init(acc[e][k]);
+            acc_init(acc[e][k], P.products[k]);
             if (CB && k < static_cast<int>(P.product_count) && P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
                 barrier_begin(P.products[k], acc[e][k], P.smoothing, P.spot, failed);
         }

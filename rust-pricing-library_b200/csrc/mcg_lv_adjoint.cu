@@ -189,11 +189,11 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     double prev_f = f, prev_v = 0.0;
     int hint = 0;
     ProductAcc acc;
-    acc_init(acc);
+    acc_init(acc, pp);
     bool failed = false;
     int fail_code = 0;
     uint32_t fail_step = 0;
-    int32_t argmax = 0;
+    int32_t argmax = -1;  // observation holding the lookback extremum (-1: the seasoned literal)
     const bool fixed = A.stops != nullptr;
     const uint32_t k_stop = fixed && valid ? A.stops[local * A.stop_stride] : 0u;
     double f_stop = f;
@@ -241,7 +241,9 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
         if (fixed && obs == static_cast<int32_t>(k_stop)) f_stop = f;
         if (obs >= 0) {
             if (pp.kind == MCG_PRODUCT_LOOKBACK) {
-                if (obs == 0 || (call ? !(acc.a >= f) : !(acc.a <= f))) argmax = obs;
+                if (monitored(pp, static_cast<uint32_t>(obs)) &&
+                    (acc.counts == 0u || (call ? !(acc.a >= f) : !(acc.a <= f))))
+                    argmax = obs;
             }
             acc_observe(pp, acc, static_cast<uint32_t>(obs), f, h, failed);
         }

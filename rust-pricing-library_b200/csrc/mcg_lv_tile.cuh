@@ -78,7 +78,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
         hint[e] = 0;
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
-            acc_init(acc[e][k]);
+            acc_init(acc[e][k], P.products[k]);
             if (CB != 0 && k < static_cast<int>(P.product_count) &&
                 P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
                 barrier_begin(P.products[k], acc[e][k], P.smoothing, f[e], failed);

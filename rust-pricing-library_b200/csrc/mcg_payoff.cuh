@@ -23,7 +23,7 @@ struct ProductAcc {
     double hit_log;  // smoothed continuous barrier: sum of log safety weights
     double hit_prod; // smoothed continuous barrier: product of safety weights
     double terminal; // last observed spot
-    uint32_t counts; // continuous barrier status counts: finite | zero<<8 | under<<16 | certain<<24 (saturating per byte is avoided by 10-bit fields below)
+    uint32_t counts; // continuous barrier status counts (10-bit fields); lookback: 1 once `a` holds an extremum
     uint32_t counts2;
     int32_t touched; // exact continuous barrier: an endpoint touched
     int32_t initial_touched;
@@ -41,6 +41,23 @@ MCG_HD void acc_init(ProductAcc& s) {
     s.initial_touched = 0;
 }
 
+// Initial state of a product: the seasoned literals of compile.rs:162-176
+// (Asian known fixings), :293-297 (historical barrier hit) and :431-436
+// (lookback historical extremum / valuation-date fixing).
+MCG_HD void acc_init(ProductAcc& s, const ProductParams& p) {
+    acc_init(s);
+    if (p.has_initial) {
+        s.a = p.initial;
+        if (p.kind == MCG_PRODUCT_LOOKBACK) s.counts = 1u;
+    }
+}
+
+// Whether observation `obs` is a monitoring date of a discrete barrier or a
+// lookback (every observation when the product carries no flags).
+MCG_HD bool monitored(const ProductParams& p, uint32_t obs) {
+    return p.weights == nullptr || p.weights[obs] != 0.0;
+}
+
 // Observation update: discrete products (compile.rs:159-202 Asian, :204-403
 // discrete barrier, :405-474 lookback, tape.rs:1038-1080 opcode semantics).
 MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
@@ -52,8 +69,10 @@ MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
         s.a = s.a + spot * p.weights[obs];
         break;
     case MCG_PRODUCT_LOOKBACK:
-        if (obs == 0) {
+        if (!monitored(p, obs)) break;
+        if (s.counts == 0u) {
             s.a = spot;
+            s.counts = 1u;
         } else if (p.side == MCG_CALL) {
             if (!(s.a >= spot)) s.a = spot;
         } else {
@@ -61,6 +80,7 @@ MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
         }
         break;
     case MCG_PRODUCT_DISCRETE_BARRIER: {
+        if (!monitored(p, obs)) break;
         const double dist =
             p.barrier_direction == MCG_BARRIER_UP ? spot - p.barrier : p.barrier - spot;
         double w;

@@ -56,7 +56,9 @@ struct ProductParams {
     double payout;
     int32_t barrier_direction, barrier_style, has_rebate;
     double barrier, rebate;
-    const double* weights;  // device, one per observation (Asian)
+    const double* weights;  // device, one per observation (Asian weights; barrier/lookback monitoring flags)
+    int32_t has_initial;    // seasoned state (Asian known-fixing sum, lookback extremum, barrier hit)
+    double initial;
 };
 
 struct DevicePlan {
@@ -119,6 +121,11 @@ struct DevicePlan {
     int32_t lv_bumps;      // LV: CRN delta/gamma evolutions
     double gamma_bump, spot_bump, vol_bump;
     double smoothing;
+    // BS pathwise risk of a multi-observation product: per-thread scratch of
+    // `bs_tape_units` threads x bs_tape_rows rows ([row][thread]).
+    double* bs_tape;
+    uint64_t bs_tape_units;
+    uint32_t bs_tape_rows;
 
     ProductParams products[kMaxProducts];
 };

@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 PATHWISE_COMPONENTS = 18
 
 PRICE, DELTA, VEGA, GAMMA = 0, 1, 2, 3
@@ -84,6 +84,7 @@ class ProductDesc(C.Structure):
         ("barrier_direction", C.c_int32), ("barrier_style", C.c_int32), ("has_rebate", C.c_int32),
         ("barrier", C.c_double), ("rebate", C.c_double),
         ("observation_weights", _dp),
+        ("has_initial_state", C.c_int32), ("initial_state", C.c_double),
     ]
 
 

@@ -40,6 +40,7 @@ class ProductSpec:
     barrier: float = 0.0
     rebate: Optional[float] = None
     weights: Optional[Sequence[float]] = None
+    initial_state: Optional[float] = None
 
 
 @dataclass
@@ -179,6 +180,8 @@ class PlanSpec:
                 w = _f64(p.weights)
                 keep.append(w)
                 q.observation_weights = _ptr(w)
+            q.has_initial_state = int(p.initial_state is not None)
+            q.initial_state = 0.0 if p.initial_state is None else p.initial_state
         keep.append(products)
         d.product_count = len(self.products)
         d.products = C.cast(products, C.POINTER(A.ProductDesc))

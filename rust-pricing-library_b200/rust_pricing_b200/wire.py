@@ -1,0 +1,561 @@
+"""Pricing requests and results in the reference's v3 wire format.
+
+`compile_request` turns a `pricing_request` document
+(schemas/v3/pricing_request.schema.json, parsed by crates/pricing/src/wire.rs
+and validated by crates/pricing/src/api/request.rs:60-230) into the engine's
+plan the way SimulationPlan::compile does
+(crates/pricing/src/engine/compile/simulation.rs:93-330):
+
+* times are ACT/365F year fractions from the valuation date
+  (DayCountConvention::year_fraction, crates/pricing/src/core/date.rs:225-231);
+* the plan observes every distinct simulated date of the payoff graph once, in
+  date order (CompiledPayoff::terminal_observations, payoff/tape.rs:229-247);
+* the discount factor is taken at the payment date;
+* dates before the valuation date enter as the graph's literals: the known
+  Asian fixings, the lookback's historical extremum and valuation-date
+  fixing, and the barrier's historical hit (payoff/compile.rs:159-474), which
+  the plan carries as a product's seasoned state.
+
+`price_request` evaluates the compiled plan on the GPU through the C ABI and
+`result_document` writes the `pricing_result` value and risk estimates in the
+reference's layout, with its market scaling (1 % spot Delta and Gamma, one
+volatility point Vega) and 95 % normal confidence bounds
+(crates/pricing/src/engine/risk/report.rs:255-300,454-489).
+
+Requests outside the engine's hot path raise `UnsupportedRequest`: discrete
+dividends, the Bass local-volatility model, smoothing-width ladders,
+observations on the valuation date itself that the graph simulates, and the
+American/LSM state variables other than spot.
+"""
+from __future__ import annotations
+
+import datetime as _dt
+import math
+from dataclasses import dataclass, field
+from typing import Optional
+
+from . import _abi as A
+from .desc import LocalVarianceSpec, LsmSpec, PlanSpec, ProductSpec
+
+NORMAL_95 = 1.959_963_984_540_054  # crates/pricing/src/engine/plan/simulation.rs:24
+SCHEMA_VERSION = 3
+
+
+class WireError(ValueError):
+    """A request document that does not follow the v3 schema."""
+
+
+class UnsupportedRequest(WireError):
+    """A valid request that this engine does not price."""
+
+
+def parse_date(text: str) -> _dt.date:
+    try:
+        return _dt.date.fromisoformat(text)
+    except (TypeError, ValueError) as exc:
+        raise WireError(f"invalid date {text!r}") from exc
+
+
+def year_fraction(start: _dt.date, end: _dt.date) -> float:
+    """ACT/365F: whole days over 365 (crates/pricing/src/core/date.rs:225-231)."""
+    return float((end - start).days) / 365.0
+
+
+def _get(obj: dict, key: str, where: str):
+    if not isinstance(obj, dict) or key not in obj:
+        raise WireError(f"{where}: missing field {key!r}")
+    return obj[key]
+
+
+def _side(product: dict) -> int:
+    side = _get(_get(product, "side", "product"), "type", "product.side")
+    if side not in ("call", "put"):
+        raise WireError(f"product.side: unknown side {side!r}")
+    return A.CALL if side == "call" else A.PUT
+
+
+def _positive(value, where: str) -> float:
+    v = float(value)
+    if not (v > 0.0 and math.isfinite(v)):
+        raise WireError(f"{where} must be positive and finite")
+    return v
+
+
+@dataclass
+class CompiledRequest:
+    """A request compiled to the engine's plan, with what the result needs."""
+
+    plan: PlanSpec
+    lsm: Optional[LsmSpec]
+    product_type: str
+    estimator: str
+    independent_units: int
+    spot: float
+    request_delta: bool
+    request_gamma: bool
+    request_vega: bool
+    smile_dynamics: str
+    vega_kt: Optional[dict] = None
+    observation_dates: list = field(default_factory=list)
+
+
+# ------------------------------------------------------------------ engine
+
+def _engine(engine: dict, where: str) -> dict:
+    kind = _get(engine, "type", where)
+    vr = _get(engine, "variance_reduction", where)
+    common = dict(antithetic=bool(_get(vr, "antithetic", where)),
+                  brownian_bridge=bool(_get(vr, "brownian_bridge", where)))
+    if kind == "pseudo_monte_carlo":
+        units = int(_get(engine, "independent_sampling_units", where))
+        if units < 1:
+            raise WireError(f"{where}.independent_sampling_units must be positive")
+        return dict(engine=A.ENGINE_PSEUDO, master_seed=int(_get(engine, "master_seed", where)),
+                    sampling_units=units, scramble_count=0, **common)
+    if kind == "randomized_quasi_monte_carlo":
+        points = int(_get(engine, "points_per_scramble", where))
+        if points < 1 or points & (points - 1):
+            raise WireError(f"{where}.points_per_scramble must be a power of two")
+        return dict(engine=A.ENGINE_RQMC, master_seed=int(_get(engine, "master_scramble_seed", where)),
+                    sampling_units=points, scramble_count=int(_get(engine, "scramble_count", where)), **common)
+    raise WireError(f"{where}: unknown engine type {kind!r}")
+
+
+# ----------------------------------------------------------------- product
+
+@dataclass
+class _Product:
+    spec: ProductSpec
+    dates: list          # simulated observation dates (sorted, unique, after valuation)
+    expiry: _dt.date
+    payment: _dt.date
+
+
+def _simulated(dates, valuation, what: str):
+    """Dates the graph simulates must lie after the valuation date: an
+    observation at time zero consumes a normal in the reference's path
+    generator, which this engine's plans do not model."""
+    for d in dates:
+        if d == valuation:
+            raise UnsupportedRequest(f"{what} on the valuation date is simulated at time zero")
+    return sorted(set(dates))
+
+
+def _european(p: dict, valuation) -> _Product:
+    expiry = parse_date(_get(p, "expiry", "product"))
+    spec = ProductSpec(kind=A.PRODUCT_EUROPEAN, side=_side(p), strike=_positive(p["strike"], "product.strike"),
+                       notional=_positive(_get(p, "notional", "product"), "product.notional"))
+    return _Product(spec, _simulated([expiry], valuation, "the expiry"), expiry, expiry)
+
+
+def _american(p: dict, valuation) -> _Product:
+    expiry = parse_date(_get(p, "expiry", "product"))
+    dates = [parse_date(d) for d in _get(p, "exercise_dates", "product")]
+    if any(d < valuation for d in dates):
+        raise WireError("american exercise dates before the valuation date (AmericanPastExerciseUnsupported)")
+    spec = ProductSpec(kind=A.PRODUCT_AMERICAN, side=_side(p), strike=_positive(p["strike"], "product.strike"),
+                       notional=_positive(_get(p, "notional", "product"), "product.notional"))
+    return _Product(spec, _simulated(dates, valuation, "an exercise date"), expiry, expiry)
+
+
+def _digital(p: dict, valuation) -> _Product:
+    expiry = parse_date(_get(p, "expiry", "product"))
+    payment = parse_date(p["payment_date"]) if "payment_date" in p else expiry
+    if payment < expiry:
+        raise WireError("digital payment date before expiry")
+    kind = _get(_get(p, "payout_kind", "product"), "type", "product.payout_kind")
+    if kind not in ("cash", "asset"):
+        raise WireError(f"product.payout_kind: unknown kind {kind!r}")
+    spec = ProductSpec(kind=A.PRODUCT_DIGITAL, side=_side(p), strike=_positive(p["strike"], "product.strike"),
+                       payout=_positive(_get(p, "payout", "product"), "product.payout"),
+                       digital_payout=A.DIGITAL_CASH if kind == "cash" else A.DIGITAL_ASSET)
+    return _Product(spec, _simulated([expiry], valuation, "the expiry"), expiry, payment)
+
+
+def _barrier(p: dict, valuation) -> _Product:
+    expiry = parse_date(_get(p, "expiry", "product"))
+    payment = parse_date(_get(p, "payment_date", "product"))
+    monitoring = [parse_date(d) for d in _get(p, "monitoring_dates", "product")]
+    if not monitoring or any(a >= b for a, b in zip(monitoring, monitoring[1:])) or monitoring[-1] > expiry:
+        raise WireError("barrier monitoring dates must be increasing and end on or before expiry")
+    continuous = _get(_get(p, "monitoring", "product"), "type", "product.monitoring") == "continuous"
+    direction = _get(_get(p, "direction", "product"), "type", "product.direction")
+    style = _get(_get(p, "style", "product"), "type", "product.style")
+    past = [d for d in monitoring if d < valuation]
+    history = p.get("historical_hit")
+    if bool(past) != (history is not None):
+        raise WireError("barrier history must be given exactly when monitoring dates precede valuation")
+    live = [d for d in monitoring if d >= valuation]
+    spec = ProductSpec(kind=A.PRODUCT_CONTINUOUS_BARRIER if continuous else A.PRODUCT_DISCRETE_BARRIER,
+                       side=_side(p), strike=_positive(p["strike"], "product.strike"),
+                       notional=_positive(_get(p, "notional", "product"), "product.notional"),
+                       barrier=_positive(_get(p, "barrier", "product"), "product.barrier"),
+                       barrier_direction=A.BARRIER_UP if direction == "up" else A.BARRIER_DOWN,
+                       barrier_style=A.KNOCK_OUT if style == "knock_out" else A.KNOCK_IN,
+                       rebate=float(p["rebate"]) if p.get("rebate") is not None else None)
+    if continuous:
+        # The bridge runs from the valuation date through every plan interval;
+        # the reference's window ends at the last monitoring date
+        # (compile/simulation.rs:215-256).
+        if monitoring[-1] != expiry:
+            raise UnsupportedRequest("continuous barrier monitored to a date before expiry")
+        if history:
+            raise UnsupportedRequest("continuous barrier already hit before the valuation date")
+        # Time-zero points are dropped for a continuous barrier (simulation.rs:224-225).
+        dates = sorted(set([d for d in live if d > valuation] + [expiry]))
+        return _Product(spec, _simulated(dates, valuation, "the expiry"), expiry, payment)
+    dates = _simulated(sorted(set(live + [expiry])), valuation, "a barrier monitoring date")
+    monitored = set(live)
+    if any(d not in monitored for d in dates):
+        spec.weights = [1.0 if d in monitored else 0.0 for d in dates]
+    if history is not None:
+        spec.initial_state = 1.0 if history else 0.0
+    return _Product(spec, dates, expiry, payment)
+
+
+def _asian(p: dict, valuation) -> _Product:
+    payment = parse_date(_get(p, "payment_date", "product"))
+    observations = _get(p, "observations", "product")
+    if not observations:
+        raise WireError("asian observations must not be empty")
+    dates = [parse_date(_get(o, "date", "observation")) for o in observations]
+    if any(a >= b for a, b in zip(dates, dates[1:])):
+        raise WireError("asian observation dates must be strictly increasing")
+    known_sum, weights, sim = 0.0, [], []
+    seen_unknown = False
+    for o, d in zip(observations, dates):
+        value = _get(o, "value", "observation")
+        w = float(_get(o, "weight", "observation"))
+        kind = _get(value, "type", "observation.value")
+        if kind == "known":
+            if d > valuation:
+                raise WireError("asian observation after the valuation date cannot carry a known fixing")
+            # Literal fixings in observation order (compile.rs:162-176); the
+            # dates increase, so every known fixing precedes the simulated ones.
+            known_sum = known_sum + float(_get(value, "fixing", "observation.value")) * w
+        elif kind == "unknown":
+            if d < valuation:
+                raise WireError("asian observation before the valuation date requires a known fixing")
+            seen_unknown = True
+            sim.append(d)
+            weights.append(w)
+        else:
+            raise WireError(f"observation.value: unknown type {kind!r}")
+    total = math.fsum(float(o["weight"]) for o in observations)
+    if not (abs(total - 1.0) <= max(1e-12, 1e-12 * len(observations))):
+        # ArithmeticAsianSpec::new (crates/pricing/src/product/spec.rs:653-663)
+        raise WireError("asian observation weights must sum to one")
+    if not seen_unknown:
+        raise UnsupportedRequest("asian with every fixing known has no simulated observation")
+    spec = ProductSpec(kind=A.PRODUCT_ASIAN, side=_side(p), strike=_positive(p["strike"], "product.strike"),
+                       notional=_positive(_get(p, "notional", "product"), "product.notional"), weights=weights)
+    if len(sim) != len(observations):
+        spec.initial_state = known_sum
+    return _Product(spec, _simulated(sim, valuation, "an asian observation"), dates[-1], payment)
+
+
+def _lookback(p: dict, valuation) -> _Product:
+    payment = parse_date(_get(p, "payment_date", "product"))
+    monitoring = [parse_date(d) for d in _get(p, "monitoring_dates", "product")]
+    if not monitoring or any(a >= b for a, b in zip(monitoring, monitoring[1:])):
+        raise WireError("lookback monitoring dates must be strictly increasing")
+    call = _side(p) == A.CALL
+    extremum = p.get("historical_extremum")
+    fixing = p.get("valuation_date_fixing")
+    has_past = any(d < valuation for d in monitoring)
+    if has_past != (extremum is not None):
+        raise WireError("lookback historical extremum must be given exactly when monitoring dates precede valuation")
+    if fixing is not None and valuation not in monitoring:
+        raise WireError("lookback valuation-date fixing requires a monitoring date equal to the valuation date")
+    # The literal head of the running extremum (compile.rs:426-452): the
+    # historical extremum, then the valuation-date fixing under Maximum /
+    # Minimum (ties keep the left operand).
+    state = None
+    if extremum is not None:
+        state = _positive(extremum, "product.historical_extremum")
+    if fixing is not None:
+        f = _positive(fixing, "product.valuation_date_fixing")
+        if state is None:
+            state = f
+        elif call:
+            state = state if state >= f else f
+        else:
+            state = state if state <= f else f
+    live = [d for d in monitoring if d > valuation or (d == valuation and fixing is None)]
+    if not live:
+        raise UnsupportedRequest("lookback with every monitoring date fixed has no simulated observation")
+    spec = ProductSpec(kind=A.PRODUCT_LOOKBACK, side=A.CALL if call else A.PUT,
+                       strike=_positive(p["strike"], "product.strike"),
+                       notional=_positive(_get(p, "notional", "product"), "product.notional"),
+                       initial_state=state)
+    return _Product(spec, _simulated(live, valuation, "a lookback monitoring date"), monitoring[-1], payment)
+
+
+_PRODUCTS = {
+    "european_vanilla": _european,
+    "american_vanilla": _american,
+    "digital": _digital,
+    "barrier": _barrier,
+    "arithmetic_asian": _asian,
+    "fixed_lookback": _lookback,
+}
+
+
+# ------------------------------------------------------------ curves, model
+
+def _curve(c: dict, where: str):
+    times = [float(t) for t in _get(c, "times", where)]
+    factors = [float(f) for f in _get(c, "discount_factors", where)]
+    if len(times) != len(factors) or len(times) < 1:
+        raise WireError(f"{where}: times and discount_factors differ in length")
+    return times, factors
+
+
+def log_discount(times, factors, t: float) -> float:
+    """Log-linear discount curve: ln DF at a pillar, linear in ln DF between
+    pillars and along the last segment beyond them (the curve the engine's
+    plan compile uses, crates/pricing/src/market/curve.rs)."""
+    logs = [math.log(f) for f in factors]
+    for i, ti in enumerate(times):
+        if ti == t:
+            return logs[i]
+    right = next((i for i, ti in enumerate(times) if ti > t), len(times) - 1)
+    left = right - 1
+    w = (t - times[left]) / (times[right] - times[left])
+    return logs[left] + w * (logs[right] - logs[left])
+
+
+def _model(doc: dict, plan_kw: dict, expiry_time: float, warnings: list):
+    model = _get(doc, "model", "request")
+    kind = _get(model, "type", "model")
+    if kind in ("black_scholes", "black_76"):
+        # Both integrate the forward with one volatility in the simulation
+        # plan (compile/simulation.rs:280-288).
+        vol = float(_get(model, "volatility", "model"))
+        if not (vol >= 0.0 and math.isfinite(vol)):
+            raise WireError("model.volatility must be finite and non-negative")
+        plan_kw.update(model=A.MODEL_BLACK_SCHOLES, volatility=vol)
+        return None
+    if kind == "local_volatility":
+        g = _get(model, "local_variance_grid", "model")
+        tn = [float(t) for t in _get(g, "time_nodes", "local_variance_grid")]
+        xn = [float(x) for x in _get(g, "log_forward_moneyness_nodes", "local_variance_grid")]
+        shape = list(_get(g, "shape", "local_variance_grid"))
+        values = [float(v) for v in _get(g, "values", "local_variance_grid")]
+        if shape != [len(tn), len(xn)] or len(values) != len(tn) * len(xn):
+            raise WireError("local_variance_grid: shape does not match the nodes and values")
+        plan_kw.update(model=A.MODEL_LOCAL_VOLATILITY, volatility=0.0,
+                       local_variance=LocalVarianceSpec(tn, xn, values, float(g["floor"]), float(g["cap"])))
+        return model.get("reporting_iv_basis")
+    if kind == "bass_local_volatility":
+        raise UnsupportedRequest("the Bass local-volatility model is not on this engine's path")
+    raise WireError(f"model: unknown type {kind!r}")
+
+
+# ----------------------------------------------------------------- compile
+
+def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledRequest:
+    """The engine plan of one v3 `pricing_request` document.
+
+    `reduction_block_size` is the reference's ExecutionPolicy block size
+    (crates/pricing/src/engine/mc/execution.rs), not part of the request."""
+    if _get(doc, "document_kind", "request") != "pricing_request":
+        raise WireError("document_kind must be 'pricing_request'")
+    if _get(doc, "schema_version", "request") != SCHEMA_VERSION:
+        raise UnsupportedRequest(f"schema_version {doc['schema_version']} (this engine reads version 3)")
+    valuation = parse_date(_get(doc, "valuation_date", "request"))
+    product_doc = _get(doc, "product", "request")
+    ptype = _get(product_doc, "type", "product")
+    if ptype not in _PRODUCTS:
+        raise UnsupportedRequest(f"product type {ptype!r}")
+    product = _PRODUCTS[ptype](product_doc, valuation)
+    if product.expiry < valuation:
+        raise WireError("expiry before the valuation date")
+    has_lsm = "lsm" in doc
+    if (ptype == "american_vanilla") != has_lsm:
+        raise WireError("lsm configuration is required for, and only for, american_vanilla")
+
+    market = _get(doc, "market", "request")
+    if _get(market, "type", "market") != "equity":
+        raise WireError("market.type must be 'equity'")
+    if market.get("discrete_dividends"):
+        raise UnsupportedRequest("discrete dividends (affine dividend transform) are not on this engine's path")
+    spot = _positive(_get(market, "spot", "market"), "market.spot")
+    dt, dfs = _curve(_get(market, "discount_curve", "market"), "market.discount_curve")
+    qt, qfs = _curve(_get(market, "dividend_curve", "market"), "market.dividend_curve")
+
+    engine = _engine(_get(doc, "engine", "request"), "engine")
+    times = [year_fraction(valuation, d) for d in product.dates]
+    payment_time = year_fraction(valuation, product.payment)
+    plan_kw = dict(observation_times=times, products=[product.spec], spot=spot,
+                   discount_times=dt, discount_factors=dfs, dividend_times=qt, dividend_factors=qfs,
+                   reduction_block_size=reduction_block_size, payment_time=payment_time, **engine)
+    warnings: list = []
+    basis = _model(doc, plan_kw, times[-1], warnings)
+
+    risk = _get(doc, "risk", "request")
+    for key in ("delta", "vega", "smile_dynamics"):
+        _get(risk, key, "risk")
+    if risk.get("payoff_smoothing_width_ladder"):
+        raise UnsupportedRequest("payoff smoothing width ladders (batched bump plans)")
+    req_delta, req_vega = bool(risk["delta"]), bool(risk["vega"])
+    gamma = risk.get("gamma")
+    plan_kw.update(request_delta=req_delta, request_vega=req_vega, request_gamma=gamma is not None)
+    if gamma is not None:
+        bump = _get(gamma, "bump", "risk.gamma")
+        kind = _get(bump, "type", "risk.gamma.bump")
+        if kind not in ("relative", "absolute"):
+            raise WireError(f"risk.gamma.bump: unknown type {kind!r}")
+        plan_kw.update(gamma_bump_relative=kind == "relative",
+                       gamma_bump=_positive(_get(bump, "value", "risk.gamma.bump"), "risk.gamma.bump.value"))
+    smoothing = risk.get("payoff_smoothing")
+    if smoothing is not None:
+        if _get(smoothing, "type", "risk.payoff_smoothing") != "compact_c2":
+            raise WireError("risk.payoff_smoothing: unknown kernel")
+        plan_kw["smoothing_half_width"] = _positive(_get(smoothing, "half_width", "risk.payoff_smoothing"),
+                                                    "risk.payoff_smoothing.half_width")
+    if "checkpoint_interval" in risk:
+        plan_kw["checkpoint_interval"] = int(risk["checkpoint_interval"])
+    vega_kt = None
+    if risk.get("vega_kt") is not None:
+        if plan_kw.get("model") != A.MODEL_LOCAL_VOLATILITY or basis is None:
+            raise WireError("risk.vega_kt needs a local-volatility model with a reporting_iv_basis")
+        plan_kw["request_local_vega_nodes"] = True
+        vega_kt = {"config": risk["vega_kt"], "reporting_iv_basis": basis}
+
+    plan = PlanSpec(**plan_kw)
+    if plan.engine == A.ENGINE_RQMC and plan.scramble_count < 1:
+        raise WireError("engine.scramble_count must be positive")
+    lsm = None
+    if has_lsm:
+        lsm = _lsm(doc["lsm"], plan)
+    units = plan.scramble_count if plan.engine == A.ENGINE_RQMC else plan.sampling_units
+    return CompiledRequest(plan=plan, lsm=lsm, product_type=ptype,
+                           estimator="randomized_quasi_monte_carlo" if plan.engine == A.ENGINE_RQMC
+                           else "pseudo_monte_carlo",
+                           independent_units=units, spot=spot, request_delta=req_delta,
+                           request_gamma=gamma is not None, request_vega=req_vega,
+                           smile_dynamics=_get(risk["smile_dynamics"], "type", "risk.smile_dynamics"),
+                           vega_kt=vega_kt, observation_dates=[d.isoformat() for d in product.dates])
+
+
+def _lsm(cfg: dict, plan: PlanSpec) -> LsmSpec:
+    """LsmConfig (crates/pricing/src/engine/mc/lsm.rs:328-495) of a spot state."""
+    states = [_get(s, "type", "lsm.state_variables") for s in _get(cfg, "state_variables", "lsm")]
+    if states != ["spot"]:
+        raise UnsupportedRequest("LSM state variables other than one spot")
+    basis = _get(cfg, "basis", "lsm")
+    if int(_get(basis, "feature_count", "lsm.basis")) != 1:
+        raise UnsupportedRequest("LSM bases of more than one feature")
+    training = _engine(_get(cfg, "training_engine", "lsm"), "lsm.training_engine")
+    if training["engine"] != plan.engine:
+        raise UnsupportedRequest("an LSM training engine of another kind than the valuation engine")
+    cpqr = _get(cfg, "cpqr", "lsm")
+    return LsmSpec(training_seed=training["master_seed"], training_units=training["sampling_units"],
+                   training_scramble_count=training["scramble_count"], training_antithetic=training["antithetic"],
+                   training_brownian_bridge=training["brownian_bridge"],
+                   max_degree=int(_get(basis, "max_degree", "lsm.basis")),
+                   itm_abs_tolerance=float(_get(cfg, "itm_abs_tolerance", "lsm")),
+                   cpqr_abs_tolerance=float(_get(cpqr, "abs_rank_tolerance", "lsm.cpqr")),
+                   cpqr_rel_tolerance=float(_get(cpqr, "rel_rank_tolerance", "lsm.cpqr")),
+                   max_matrix_elements=int(_get(cfg, "max_matrix_elements", "lsm")))
+
+
+# ------------------------------------------------------------------ result
+
+def _estimate(e, estimator: str, scale: float = 1.0) -> dict:
+    """An Estimate of the result document.  The market-scaled estimate of a
+    risk is estimate_from_statistics with `scale` (report.rs:454-473):
+    value * scale and standard error * |scale|, with the 95 % bounds
+    recomputed from them."""
+    value = e.value * scale
+    se = e.standard_error * abs(scale)
+    half = NORMAL_95 * se
+    if scale == 1.0:
+        lower, upper = e.confidence_lower, e.confidence_upper
+    else:
+        lower, upper = value - half, value + half
+    return {"value": value, "standard_error": se, "confidence_lower": lower, "confidence_upper": upper,
+            "estimator": {"type": estimator}, "effective_sampling_units": int(e.effective_sampling_units)}
+
+
+def _risk(e, estimator: str, scale: float, raw_unit: str, scaled_unit: str) -> dict:
+    return {"raw": _estimate(e, estimator), "market_scaled": _estimate(e, estimator, scale),
+            "raw_unit": {"type": raw_unit}, "market_scaled_unit": {"type": scaled_unit}}
+
+
+def result_document(req: CompiledRequest, price, delta=None, gamma=None, vega=None,
+                    sampling_variance: Optional[float] = None, estimator_variance: Optional[float] = None,
+                    evaluated_paths: Optional[int] = None, vega_kt: Optional[dict] = None,
+                    warnings: Optional[list] = None) -> dict:
+    """A `pricing_result` document (schemas/v3/pricing_result.schema.json) of
+    the engine's estimates: value, risks with raw and market-scaled values
+    (report.rs:255-300), diagnostics and the Monte Carlo variances."""
+    est = req.estimator
+    risks: dict = {}
+    s = req.spot * 0.01
+    if req.request_delta and delta is not None:
+        risks["delta"] = _risk(delta, est, s, "delta_raw", "delta_one_percent_spot")
+    if req.request_gamma and gamma is not None:
+        risks["gamma"] = _risk(gamma, est, s * s, "gamma_raw", "gamma_one_percent_spot_squared")
+    if req.request_vega and vega is not None:
+        risks["vega"] = _risk(vega, est, 0.01, "vega_raw", "vega_one_vol_point")
+    if vega_kt is not None:
+        risks["vega_kt"] = vega_kt
+    doc = {"document_kind": "pricing_result", "schema_version": SCHEMA_VERSION,
+           "value": _estimate(price, est), "risks": risks,
+           "diagnostics": {"warnings": list(warnings or [])}}
+    if sampling_variance is not None:
+        doc["monte_carlo"] = {"sampling_variance": sampling_variance, "estimator_variance": estimator_variance,
+                              "independent_sampling_units": req.independent_units,
+                              "evaluated_paths": str(evaluated_paths)}
+    return doc
+
+
+def _vega_kt_report(req: CompiledRequest, node_means, evaluated_paths: int) -> dict:
+    """VegaKT raw buckets and projection of the local-vega node sensitivities
+    (engine/risk/vegakt.rs:856, risk/local_vol_allocation.rs:108-163)."""
+    from ._native import VegaKtBasisSpec, vega_kt_project
+    plan, kt = req.plan, req.vega_kt
+    basis = kt["reporting_iv_basis"]
+    maturities = [float(t) for t in basis["maturity_nodes"]]
+    forwards = [plan.spot * math.exp(log_discount(plan.dividend_times, plan.dividend_factors, t)
+                                     - log_discount(plan.discount_times, plan.discount_factors, t))
+                for t in maturities]
+    spec = VegaKtBasisSpec(maturities, basis["log_forward_moneyness_nodes"], basis["implied_volatilities"],
+                           forwards, float(kt["config"]["relative_density_threshold"]))
+    g = plan.local_variance
+    out, buckets = vega_kt_project(g.time_nodes, g.log_moneyness_nodes, node_means, evaluated_paths, spec)
+    xs = list(basis["log_forward_moneyness_nodes"])
+    vols = list(basis["implied_volatilities"])
+    coordinates = [{"maturity": t, "log_moneyness": x, "implied_volatility": vols[i * len(xs) + j]}
+                   for i, t in enumerate(maturities) for j, x in enumerate(xs)]
+    return {"coordinates": coordinates, "raw_buckets": [float(b) for b in buckets],
+            "projection": {"scalar_vega": out.scalar_vega, "signed_residual": out.signed_residual,
+                           "pre_projection": out.pre_projection,
+                           "reporting_stats": {"left_edge_count": int(out.left_edge_count),
+                                               "right_edge_count": int(out.right_edge_count),
+                                               "left_edge_sensitivity": out.left_edge_sensitivity,
+                                               "right_edge_sensitivity": out.right_edge_sensitivity}},
+            "residual_diagnostics": {"initial_time": out.initial_time,
+                                     "excluded_probability_mass": out.density_excluded}}
+
+
+def price_request(doc: dict, *, reduction_block_size: int = 4096, stream: int = 0) -> dict:
+    """Price one v3 request on the GPU and return its `pricing_result` document."""
+    from . import _native as N
+    req = compile_request(doc, reduction_block_size=reduction_block_size)
+    if req.lsm is not None:
+        buf = N.lsm_price(req.plan, req.lsm, stream=stream)
+        r = buf.result
+        return result_document(req, r.price, r.delta, r.gamma, r.vega, r.sampling_variance,
+                               r.estimator_variance, r.valuation_paths)
+    with N.Plan(req.plan) as plan:
+        buf = plan.evaluate(stream)
+    p = buf.products[0]
+    r = buf.result
+    kt = None
+    if req.vega_kt is not None:
+        kt = _vega_kt_report(req, [e.value for e in buf.node_estimates], r.evaluated_paths)
+    return result_document(req, p.price, p.delta, p.gamma, p.vega, p.sampling_variance, p.estimator_variance,
+                           r.evaluated_paths, kt)

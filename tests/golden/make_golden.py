@@ -6,6 +6,9 @@ are committed; the tests only read them.
 
 * replay_european_bs.json  -- fixtures/replay/european_bs-windows-x86_64.json:
   request parameters and result values of the pseudo and RQMC full-risk cases.
+
+Every replay case also keeps its verbatim v3 request document ("request"),
+which the wire-format tests compile.
 * bs_analytical.json       -- fixtures/acceptance/european_bs_analytical.csv.
 * path_dependence.json     -- fixtures/path-dependence/reference-cases-v0.1.json
   (smoothing, extrema, exact and smoothed bridge cases; decimal strings).
@@ -16,6 +19,11 @@ are committed; the tests only read them.
 * surfaces.json            -- fixtures/local-vol/reference-cases-v0.1.json: the standard SSVI
   (power-law and Heston-like phi), eSSVI interpolation and constant-volatility
   Dupire cases (70-digit decimal values).
+* replay_path_dependence.json -- fixtures/replay/path_dependence-{windows-x86_64,macos-aarch64}.json:
+  the digital, discrete and continuous barrier, arithmetic Asian and fixed
+  lookback requests (verbatim v3 request documents, Black--Scholes, pseudo and
+  RQMC, exact and compact-C2 smoothed, price-only and full risk) with both
+  platforms' estimates, variance bits and bump-and-revalue validation bits.
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
   the American put requests (pseudo and RQMC, training and valuation engines,
   LSM configuration) with the fitted decision models, exercise counts,
@@ -39,6 +47,7 @@ def replay():
         eng = req["engine"]
         case = {
             "name": c["name"],
+            "request": req,
             "engine": eng["type"],
             "master_seed": eng.get("master_seed", eng.get("master_scramble_seed")),
             "sampling_units": eng.get("independent_sampling_units", eng.get("points_per_scramble")),
@@ -89,6 +98,7 @@ def local_volatility():
         grid = req["model"]["local_variance_grid"]
         case = {
             "name": c["name"],
+            "request": req,
             **_engine(req["engine"]),
             "reduction_block_size": c["execution"]["monte_carlo"]["reduction_block_size"],
             "spot": req["market"]["spot"],
@@ -138,6 +148,40 @@ def local_volatility():
               open(os.path.join(OUT, "replay_local_vol.json"), "w"), indent=1)
 
 
+def path_dependence_replay():
+    platforms = {p: json.load(open(os.path.join(REF, f"fixtures/replay/path_dependence-{p}.json")))
+                 for p in ("windows-x86_64", "macos-aarch64")}
+    cases = []
+    for i, c in enumerate(platforms["windows-x86_64"]["cases"]):
+        case = {
+            "name": c["name"],
+            "request": c["request"],
+            "reduction_block_size": c["execution"]["monte_carlo"]["reduction_block_size"],
+            "expected": {},
+        }
+        for name, d in platforms.items():
+            pc = d["cases"][i]
+            assert pc["name"] == c["name"] and pc["request"] == c["request"]
+            res, ex = pc["result"], pc["execution"]
+            case["expected"][name] = {
+                "value": _estimate(res["value"]),
+                "risks": {k: {"raw": _estimate(r["raw"]), "market_scaled": _estimate(r["market_scaled"]),
+                              "raw_unit": r["raw_unit"]["type"],
+                              "market_scaled_unit": r["market_scaled_unit"]["type"]}
+                          for k, r in res["risks"].items()},
+                "sampling_variance_bits": ex["sampling_variance_bits"],
+                "estimator_variance_bits": ex["estimator_variance_bits"],
+                "evaluated_paths": int(ex["evaluated_paths"]),
+                "independent_sampling_units": ex["independent_sampling_units"],
+                "risk_methods": ex["risk_methods"],
+                "bump_value_bits": {k: v["bump_and_revalue"]["value_bits"]
+                                    for k, v in (ex.get("risk_validation") or {}).items() if v},
+            }
+        cases.append(case)
+    json.dump({"source": "fixtures/replay/path_dependence-{windows-x86_64,macos-aarch64}.json", "cases": cases},
+              open(os.path.join(OUT, "replay_path_dependence.json"), "w"), indent=1)
+
+
 def surfaces():
     src = os.path.join(REF, "fixtures/local-vol/reference-cases-v0.1.json")
     d = json.load(open(src))
@@ -183,6 +227,7 @@ def early_exercise():
         lsm = req["lsm"]
         case = {
             "name": c["name"],
+            "request": req,
             "valuation": _engine(req["engine"]),
             "training": _engine(lsm["training_engine"]),
             "reduction_block_size": c["execution"]["monte_carlo"]["reduction_block_size"],
@@ -235,5 +280,6 @@ if __name__ == "__main__":
     path_dependence()
     early_exercise()
     local_volatility()
+    path_dependence_replay()
     surfaces()
     print("golden fixtures written to", OUT)

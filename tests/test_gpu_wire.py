@@ -1,0 +1,133 @@
+"""v3 request documents priced on the GPU, and the path-risk kernel.
+
+* The reference's path-dependence replay requests (digital, discrete and
+  continuous barrier, Asian with a known fixing, lookback with a historical
+  extremum; pseudo and RQMC; exact and compact-C2 smoothed; full risk) go
+  through wire.price_request unchanged: every value and bound within 1e-12 of
+  the nearer platform's fixture, standard errors within 1e-9, and every
+  component within the parity tolerances of the oracle on the same plan.
+* The European, local-volatility (VegaKT) and early-exercise replay requests
+  give the fixture's values through the same entry point.
+* Seasoned state and monitoring flags (historical barrier hit, unmonitored
+  expiry, Asian known-fixing sum, lookback literal extremum) agree with the
+  oracle under Black--Scholes path risk and under the local-volatility adjoint.
+"""
+import copy
+
+import pytest
+
+import gpu_common as G
+import lsm_cases as LC
+import lv_cases as LV
+import wire_cases as WC
+from rust_pricing_b200 import _abi as A
+from rust_pricing_b200 import wire
+from test_oracle_fixtures import replay_cases
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", WC.path_dependence_cases(), ids=lambda c: c["name"])
+def test_path_dependence_requests_on_the_gpu(engine, case):
+    doc = wire.price_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    WC.assert_matches_fixture(doc, case, rel=1e-12, se_rel=1e-9, price_bits=False)
+    req = wire.compile_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    G.assert_parity(req.plan)
+
+
+@pytest.mark.parametrize("case", replay_cases(), ids=lambda c: c["name"])
+def test_european_requests_on_the_gpu(engine, case):
+    doc = wire.price_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    e = case["expected"]
+    for name, key in (("value", "price"),):
+        assert abs(doc[name]["value"] - e[key]) <= 1e-12 * abs(e[key])
+    for key in ("delta", "gamma", "vega"):
+        assert abs(doc["risks"][key]["raw"]["value"] - e[key]) <= 1e-12 * abs(e[key]), key
+
+
+@pytest.mark.parametrize("case", LV.cases(), ids=lambda c: c["name"])
+def test_local_vol_requests_on_the_gpu(engine, case):
+    doc = wire.price_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    e = case["expected"]["windows-x86_64"]
+    want = [("value", doc["value"], e["value"])] + [(k, doc["risks"][k]["raw"], v) for k, v in e["risks"].items()]
+    for name, got, w in want:
+        assert abs(got["value"] - w["value"]) <= G.DIRECT_TOL * max(abs(w["value"]), w["standard_error"]), name
+    if "node_allocation" in case:
+        kt = doc["risks"]["vega_kt"]
+        a = case["node_allocation"]
+        assert abs(kt["raw_buckets"][0] - a["raw_buckets/0"]) <= 1e-12 * max(abs(a["raw_buckets/0"]), 1.0)
+        assert abs(kt["projection"]["scalar_vega"] - a["projection/scalar_vega"]) <= \
+            1e-12 * max(abs(a["projection/scalar_vega"]), 1.0)
+
+
+@pytest.mark.parametrize("case", LC.cases(), ids=lambda c: c["name"])
+def test_early_exercise_requests_on_the_gpu(engine, case):
+    doc = wire.price_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    v = case["expected"]["value"]
+    assert abs(doc["value"]["value"] - v["value"]) <= 1e-12 * abs(v["value"])
+    assert doc["value"]["effective_sampling_units"] == v["effective_sampling_units"]
+
+
+def _request(name):
+    return copy.deepcopy(next(c for c in WC.path_dependence_cases() if c["name"] == name)["request"])
+
+
+def _seasoned_requests():
+    out = []
+    d = _request("discrete_barrier_smoothed_full_risk")
+    d["product"]["monitoring_dates"] = ["2026-06-04", "2027-03-05"]
+    d["product"]["historical_hit"] = False
+    out.append(("barrier_unmonitored_expiry", d))
+    d = copy.deepcopy(d)
+    d["product"]["historical_hit"] = True
+    out.append(("barrier_hit_before_valuation", d))
+    d = _request("discrete_barrier_smoothed_full_risk")
+    del d["risk"]["payoff_smoothing"]
+    d["product"]["style"] = {"type": "knock_in"}
+    d["product"]["direction"] = {"type": "down"}
+    d["product"]["barrier"] = 90.0
+    out.append(("exact_down_and_in", d))
+    d = _request("fixed_lookback_full_risk")
+    d["product"]["side"] = {"type": "put"}
+    d["product"]["historical_extremum"] = 92.0
+    out.append(("lookback_put_history", d))
+    d = _request("arithmetic_asian_full_risk")
+    d["product"]["side"] = {"type": "put"}
+    out.append(("asian_put_known_fixing", d))
+    return out
+
+
+def _local_vol(doc):
+    """The same request under a flat-ish 3 x 5 local-variance grid."""
+    lv = copy.deepcopy(doc)
+    lv["model"] = {"type": "local_volatility", "local_variance_grid": {
+        "time_nodes": [0.0, 0.5, 1.0], "log_forward_moneyness_nodes": [-1.0, -0.5, 0.0, 0.5, 1.0],
+        "shape": [3, 5], "values": [0.05, 0.045, 0.04, 0.042, 0.05] * 3, "floor": 1e-8, "cap": 4.0}}
+    lv["risk"].pop("payoff_smoothing", None)
+    lv["risk"]["gamma"] = {"bump": {"type": "relative", "value": 0.01}}
+    return lv
+
+
+@pytest.mark.parametrize("name, doc", _seasoned_requests(), ids=lambda x: x if isinstance(x, str) else "")
+def test_seasoned_products_against_the_oracle(engine, name, doc):
+    req = wire.compile_request(doc, reduction_block_size=512)
+    G.assert_parity(req.plan)
+    lv = wire.compile_request(_local_vol(doc), reduction_block_size=512)
+    G.assert_parity(lv.plan)
+
+
+def test_path_risk_over_several_scratch_chunks(engine):
+    """An Asian with 500 daily simulated fixings on 2^17 units needs more than
+    one chunk of the path-risk kernel's 256 MiB scratch: the launch loop
+    covers every unit and the tiles land where the reduction expects them."""
+    import datetime as dt
+    doc = _request("arithmetic_asian_full_risk")
+    doc["engine"]["independent_sampling_units"] = 1 << 17
+    start = dt.date(2026, 9, 5)
+    dates = [(start + dt.timedelta(days=i)).isoformat() for i in range(500)]
+    doc["product"]["observations"] = [doc["product"]["observations"][0]] + [
+        {"date": d, "value": {"type": "unknown"}, "weight": 0.8 / 500} for d in dates]
+    doc["product"]["payment_date"] = dates[-1]
+    req = wire.compile_request(doc, reduction_block_size=4096)
+    assert len(req.plan.observation_times) == 500
+    G.assert_parity(req.plan, threads=16)

@@ -1,0 +1,227 @@
+"""The v3 wire format: request documents compiled to plans, and result documents.
+
+* Every replay request of the reference's fixtures (European BS, local
+  volatility with VegaKT, early exercise, path-dependent products) compiles to
+  the plan the hand-mapped tests use: the oracle gives the same bits on both.
+* The path-dependence requests, compiled by the wire module and run on the
+  oracle, reproduce fixtures/replay/path_dependence-*.json through the result
+  document: value and sampling variance to the last bit on one platform, every
+  raw and market-scaled risk estimate within 1e-12 relative.
+* Seasoned products: known Asian fixings, a lookback's historical extremum and
+  valuation-date fixing, a barrier's historical hit and an unmonitored expiry
+  become the plan's seasoned state and monitoring flags.
+* Requests off the engine's path raise UnsupportedRequest; malformed ones WireError.
+"""
+import copy
+import math
+import struct
+
+import pytest
+
+import helpers as H
+import lsm_cases as LC
+import lv_cases as LV
+import wire_cases as WC
+from rust_pricing_b200 import _abi as A
+from rust_pricing_b200 import wire
+from test_oracle_fixtures import replay_cases, replay_spec
+
+
+def bits(x: float) -> str:
+    return struct.pack(">d", x).hex()
+
+
+def oracle_document(req, threads=4):
+    buf = H.oracle_evaluate(req.plan, threads=threads)
+    p, r = buf.products[0], buf.result
+    return wire.result_document(req, p.price, p.delta, p.gamma, p.vega, p.sampling_variance,
+                                p.estimator_variance, r.evaluated_paths), buf
+
+
+def same_estimates(a, b):
+    for name in ("price", "delta", "gamma", "vega", "bump_delta", "bump_gamma", "bump_vega"):
+        x, y = getattr(a, name), getattr(b, name)
+        assert (bits(x.value), bits(x.standard_error)) == (bits(y.value), bits(y.standard_error)), name
+    assert bits(a.sampling_variance) == bits(b.sampling_variance)
+
+
+@pytest.mark.parametrize("case", WC.path_dependence_cases(), ids=lambda c: c["name"])
+def test_path_dependence_replay_through_the_wire(case):
+    req = wire.compile_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    doc, _ = oracle_document(req)
+    WC.assert_matches_fixture(doc, case, rel=1e-12, price_bits=True)
+
+
+@pytest.mark.parametrize("case", replay_cases(), ids=lambda c: c["name"])
+def test_european_replay_request_compiles_to_the_replay_plan(case):
+    req = wire.compile_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    a = H.oracle_evaluate(req.plan, threads=4).products[0]
+    b = H.oracle_evaluate(replay_spec(case), threads=4).products[0]
+    same_estimates(a, b)
+    e = case["expected"]
+    doc = wire.result_document(req, a.price, a.delta, a.gamma, a.vega)
+    assert doc["value"]["value"] == e["price"]
+    assert doc["risks"]["vega"]["raw"]["value"] == e["vega"]
+    assert doc["risks"]["vega"]["market_scaled"]["value"] == e["vega"] * 0.01
+
+
+@pytest.mark.parametrize("case", LV.cases(), ids=lambda c: c["name"])
+def test_local_vol_replay_request_compiles_to_the_replay_plan(case):
+    req = wire.compile_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    hand = LV.plan(case)
+    assert req.plan.model == A.MODEL_LOCAL_VOLATILITY
+    assert list(req.plan.local_variance.values) == list(hand.local_variance.values)
+    assert req.plan.observation_times == hand.observation_times
+    assert req.plan.request_local_vega_nodes == ("vega_kt" in case)
+    req.plan.request_local_vega_nodes = False
+    a = H.oracle_evaluate(req.plan, threads=4).products[0]
+    b = H.oracle_evaluate(hand, threads=4).products[0]
+    same_estimates(a, b)
+    if "vega_kt" in case:
+        # The basis forwards the wire module computes equal the tests' own.
+        basis = LV.vega_kt_basis(case)
+        maturities = req.vega_kt["reporting_iv_basis"]["maturity_nodes"]
+        fwd = [req.plan.spot * math.exp(
+            wire.log_discount(req.plan.dividend_times, req.plan.dividend_factors, t)
+            - wire.log_discount(req.plan.discount_times, req.plan.discount_factors, t)) for t in maturities]
+        assert fwd == list(basis.arrays[3])
+
+
+@pytest.mark.parametrize("case", LC.cases(), ids=lambda c: c["name"])
+def test_early_exercise_replay_request_compiles_to_the_replay_plan(case):
+    req = wire.compile_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    spec, lsm = LC.plan(case)
+    assert req.lsm is not None
+    assert req.plan.observation_times == spec.observation_times
+    got = H.oracle_lsm(req.plan, req.lsm, threads=3).result
+    want = H.oracle_lsm(spec, lsm, threads=3).result
+    assert bits(got.price.value) == bits(want.price.value)
+    assert bits(got.sampling_variance) == bits(want.sampling_variance)
+    assert got.price.value == case["expected"]["value"]["value"]
+
+
+# ------------------------------------------------------------ seasoned state
+
+def _case(name):
+    return copy.deepcopy(next(c for c in WC.path_dependence_cases() if c["name"] == name)["request"])
+
+
+def test_asian_known_fixings_are_the_seasoned_sum():
+    doc = _case("arithmetic_asian_full_risk")
+    obs = doc["product"]["observations"]
+    req = wire.compile_request(doc)
+    p = req.plan.products[0]
+    assert p.kind == A.PRODUCT_ASIAN
+    assert p.initial_state == 0.0 + 98.0 * 0.2
+    assert p.weights == [0.3, 0.5]
+    assert req.observation_dates == [o["date"] for o in obs[1:]]
+    # A known fixing after the valuation date is rejected (request.rs:136).
+    bad = copy.deepcopy(doc)
+    bad["product"]["observations"][1]["value"] = {"type": "known", "fixing": 100.0}
+    with pytest.raises(wire.WireError):
+        wire.compile_request(bad)
+    bad = copy.deepcopy(doc)
+    bad["product"]["observations"][0]["value"] = {"type": "unknown"}
+    with pytest.raises(wire.WireError):
+        wire.compile_request(bad)
+
+
+def test_lookback_history_and_valuation_date_fixing():
+    doc = _case("fixed_lookback_full_risk")
+    req = wire.compile_request(doc)
+    assert req.plan.products[0].initial_state == 105.0
+    doc["product"]["monitoring_dates"] = ["2026-06-04", "2026-09-04", "2027-03-05", "2027-09-04"]
+    doc["product"]["valuation_date_fixing"] = 107.5
+    req = wire.compile_request(doc)
+    assert req.plan.products[0].initial_state == 107.5  # Maximum(105, 107.5)
+    assert len(req.plan.observation_times) == 2
+    doc["product"]["side"] = {"type": "put"}
+    assert wire.compile_request(doc).plan.products[0].initial_state == 105.0  # Minimum
+    # Without the fixing, the valuation-date monitoring is a time-zero observation.
+    del doc["product"]["valuation_date_fixing"]
+    with pytest.raises(wire.UnsupportedRequest):
+        wire.compile_request(doc)
+    doc["product"].pop("historical_extremum")
+    with pytest.raises(wire.WireError):
+        wire.compile_request(doc)
+
+
+def test_barrier_history_and_unmonitored_expiry():
+    doc = _case("discrete_barrier_smoothed_full_risk")
+    doc["product"]["monitoring_dates"] = ["2026-06-04", "2027-03-05"]
+    doc["product"]["historical_hit"] = False
+    req = wire.compile_request(doc)
+    p = req.plan.products[0]
+    assert p.initial_state == 0.0
+    assert p.weights == [1.0, 0.0]  # the expiry observes the payoff but not the barrier
+    assert len(req.plan.observation_times) == 2
+    doc["product"]["historical_hit"] = True
+    assert wire.compile_request(doc).plan.products[0].initial_state == 1.0
+    del doc["product"]["historical_hit"]
+    with pytest.raises(wire.WireError):
+        wire.compile_request(doc)
+
+
+def test_oracle_honours_seasoned_state_and_flags():
+    """A barrier hit before valuation is knocked out for good; an unmonitored
+    observation leaves a barrier alone; a lookback whose historical extremum
+    is out of reach pays it."""
+    doc = _case("discrete_barrier_smoothed_full_risk")
+    doc["product"]["monitoring_dates"] = ["2026-06-04", "2027-03-05", "2027-09-04"]
+    doc["product"]["historical_hit"] = True
+    doc["risk"] = {"delta": False, "vega": False, "smile_dynamics": {"type": "sticky_log_moneyness"}}
+    req = wire.compile_request(doc, reduction_block_size=256)
+    out, _ = oracle_document(req)
+    df = req.plan.discount_factors[-1]
+    assert out["value"]["value"] == pytest.approx(2.0 * df, rel=1e-15)  # the rebate on every path
+    assert out["value"]["standard_error"] == 0.0
+    doc = _case("fixed_lookback_full_risk")
+    doc["product"]["historical_extremum"] = 1e6
+    doc["risk"] = {"delta": True, "vega": True, "smile_dynamics": {"type": "sticky_log_moneyness"}}
+    req = wire.compile_request(doc, reduction_block_size=256)
+    out, _ = oracle_document(req)
+    assert out["value"]["value"] == pytest.approx((1e6 - 100.0) * df, rel=1e-14)
+    assert out["risks"]["delta"]["raw"]["value"] == 0.0
+    assert out["risks"]["vega"]["raw"]["value"] == 0.0
+
+
+# ----------------------------------------------------------------- errors
+
+@pytest.mark.parametrize("edit, error", [
+    (lambda d: d.update(document_kind="pricing_result"), wire.WireError),
+    (lambda d: d.update(schema_version=2), wire.UnsupportedRequest),
+    (lambda d: d["market"].update(discrete_dividends=[{"event_id": 1, "ex_time": 0.5,
+                                                        "quote": {"type": "fixed_cash", "amount": 1.0}}]),
+     wire.UnsupportedRequest),
+    (lambda d: d.update(model={"type": "bass_local_volatility", "parameters": {}}), wire.UnsupportedRequest),
+    (lambda d: d["risk"].update(payoff_smoothing_width_ladder=[1.0, 2.0]), wire.UnsupportedRequest),
+    (lambda d: d["product"].update(expiry="2026-09-04", payment_date="2026-09-04"), wire.UnsupportedRequest),
+    (lambda d: d["product"].update(type="graph"), wire.UnsupportedRequest),
+    (lambda d: d.pop("engine"), wire.WireError),
+    (lambda d: d.update(lsm={}), wire.WireError),
+    (lambda d: d["engine"].update(type="quantum"), wire.WireError),
+])
+def test_rejected_requests(edit, error):
+    doc = _case("digital_exact_price_only")
+    edit(doc)
+    with pytest.raises(error):
+        wire.compile_request(doc)
+
+
+def test_market_scaling_of_risks():
+    """report.rs:255-300: Delta x S/100, Gamma x (S/100)^2, Vega / 100, with the
+    confidence bounds of the scaled standard error."""
+    case = next(c for c in WC.path_dependence_cases() if c["name"] == "arithmetic_asian_full_risk")
+    e = case["expected"]["windows-x86_64"]
+    req = wire.compile_request(case["request"])
+
+    class Est:
+        def __init__(self, d):
+            self.__dict__.update(d)
+
+    doc = wire.result_document(req, Est(e["value"]), *(Est(e["risks"][k]["raw"]) for k in ("delta", "gamma", "vega")))
+    for k in ("delta", "gamma", "vega"):
+        assert doc["risks"][k]["market_scaled"]["value"] == e["risks"][k]["market_scaled"]["value"]
+        assert doc["risks"][k]["market_scaled"]["standard_error"] == e["risks"][k]["market_scaled"]["standard_error"]
+        assert doc["risks"][k]["market_scaled"]["confidence_lower"] == e["risks"][k]["market_scaled"]["confidence_lower"]
+    assert doc["value"]["estimator"] == {"type": "pseudo_monte_carlo"}
