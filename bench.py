@@ -56,8 +56,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
                     help="path arithmetic of the timed workload (f32: FP32 path bulk)")
+    ap.add_argument("--path-risk-units", type=int, default=1 << 20,
+                    help="pseudo paths of the BS path-risk secondary measurement")
     ap.add_argument("--secondary", default="all",
-                    help="comma list of secondary measurements: early_exercise, book, f32, adjoint; all; none")
+                    help="comma list of secondary measurements: early_exercise, book, f32, adjoint, "
+                         "path_risk; all; none")
     ap.add_argument("--adjoint-paths", type=int, default=1 << 20)
     ap.add_argument("--lsm-units", type=int, default=1 << 20)
     ap.add_argument("--book-trades", type=int, default=4096)
@@ -265,6 +268,50 @@ def adjoint_secondary(paths: int = 1 << 20):
     return out
 
 
+def path_risk_secondary(units: int = 1 << 20, cpu_units: int = 1 << 14):
+    """Black--Scholes pathwise risk of path-dependent products (the reference's
+    pathwise_values over pathwise_aad): an arithmetic Asian call on 252 daily
+    fixings and a continuous down-and-out call (B = 80, rebate 1, compact-C2
+    0.5), S = K = 100, r = 3 %, q = 1 %, sigma = 0.2, T = 1, `units` pseudo
+    paths, Delta / Gamma (1 % relative bump) / Vega with the CRN validation
+    bumps: 7 evaluations of every path.  The oracle on the host's cores
+    prices `cpu_units` paths of the same plan for comparison."""
+    from rust_pricing_b200 import _abi as A, _native as N
+    from rust_pricing_b200.desc import PlanSpec, ProductSpec
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+    times = [(i + 1) / STEPS for i in range(STEPS)]
+    products = {
+        "asian_call": ProductSpec(kind=A.PRODUCT_ASIAN, strike=100.0, weights=[1.0 / STEPS] * STEPS),
+        "continuous_down_and_out": ProductSpec(kind=A.PRODUCT_CONTINUOUS_BARRIER, strike=100.0, barrier=80.0,
+                                               barrier_direction=A.BARRIER_DOWN, barrier_style=A.KNOCK_OUT,
+                                               rebate=1.0),
+    }
+    out = {"workload": f"BS path risk, {units} pseudo paths x {STEPS} observations, Delta/Gamma/Vega + CRN "
+                       "validation bumps (7 evaluations per path)"}
+    for name, prod in products.items():
+        spec = PlanSpec(observation_times=times, products=[prod], sampling_units=units, master_seed=20260904,
+                        request_delta=True, request_gamma=True, request_vega=True, gamma_bump=0.01,
+                        smoothing_half_width=0.5 if prod.kind == A.PRODUCT_CONTINUOUS_BARRIER else 0.0)
+        with N.Plan(spec) as plan:
+            plan.evaluate()
+            r = min((plan.evaluate() for _ in range(3)), key=lambda b: b.result.device_ms)
+        p, ms = r.products[0], r.result.device_ms
+        evaluations = units * STEPS * 7
+        spec.sampling_units = cpu_units
+        t0 = time.perf_counter()
+        H.oracle_evaluate(spec, threads=os.cpu_count() or 1)
+        cpu_s = time.perf_counter() - t0
+        out[name] = {"device_ms": ms, "path_step_evaluations_per_s": evaluations / (ms * 1e-3),
+                     "price": p.price.value, "delta": p.delta.value, "delta_se": p.delta.standard_error,
+                     "gamma": p.gamma.value, "vega": p.vega.value, "vega_se": p.vega.standard_error,
+                     "ms_to_1pct_delta": time_to_pct(ms, p.delta.standard_error, p.delta.value),
+                     "kernel_launches": r.result.kernel_launches,
+                     "cpu_oracle_path_step_evaluations_per_s": cpu_units * STEPS * 7 / cpu_s,
+                     "cpu_threads": os.cpu_count() or 1}
+    return out
+
+
 def f32_secondary(points: int, scrambles: int, prices64):
     """The timed workload with the FP32 path bulk: time and the error of each
     price against the FP64 run's."""
@@ -453,7 +500,7 @@ def main():
         "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, buf.products[k].price.standard_error,
                                                 buf.products[k].price.value) for k in range(len(spec.products))],
     }
-    wanted = {"early_exercise", "book", "f32", "adjoint"} if args.secondary == "all" else (
+    wanted = {"early_exercise", "book", "f32", "adjoint", "path_risk"} if args.secondary == "all" else (
         set() if args.secondary == "none" else set(args.secondary.split(",")))
     if rank == 0 and world == 1 and wanted:
         sec = {}
@@ -468,6 +515,8 @@ def main():
             sec["batched_book"] = book_secondary(args.book_trades, args.book_units)
         if "adjoint" in wanted:
             sec["adjoint"] = adjoint_secondary(args.adjoint_paths)
+        if "path_risk" in wanted:
+            sec["bs_path_risk"] = path_risk_secondary(args.path_risk_units)
         line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -19,7 +19,8 @@
 // and the antithetic mate's is its exact negation, so each unit computes it
 // once into the per-thread scratch tape ([k][thread], coalesced) and all
 // fourteen evaluations read it back; a smoothed discrete barrier also keeps
-// its hit states, weights and weight slopes there for the reverse sweep.
+// its hit states, weights and weight slopes there for the reverse sweep, a
+// continuous barrier its observed states and node adjoints.
 #include "mcg_kernels.cuh"
 
 namespace mcg {
@@ -30,20 +31,37 @@ struct PathAad {
     double price, delta, vega;
 };
 
-// Spot at observation k of the path with sign `sign` (antithetic mate -1).
-__device__ __forceinline__ double observe(const DevicePlan& P, const double* w_tape, size_t stride,
-                                          uint32_t k, double sign, double scale, double vol, double& w) {
-    w = sign * w_tape[static_cast<size_t>(k) * stride];
+// Per-thread scratch rows ([row][thread], `stride` threads apart): the
+// cumulative Brownian values W_k of the primary path, the exponentials
+// exp(-sigma^2 t_k / 2 + sigma W_k) of the path being evaluated at the plan's
+// volatility, and the product's extra rows.
+struct Scratch {
+    const double* w;
+    double* e;
+    double* x;
+    size_t stride;
+};
+
+// Spot at observation k of the path with sign `sign` (antithetic mate -1):
+// F_k (S/S0) exp(-sigma^2 t_k / 2 + sigma W_k).  The five evaluations at the
+// plan's volatility read the exponential from the scratch (the same value the
+// expression gives), only the two volatility bumps evaluate it.
+__device__ __forceinline__ double observe(const DevicePlan& P, const Scratch& T, uint32_t k, double sign,
+                                          double scale, double vol, bool cached, double& w) {
+    const size_t at = static_cast<size_t>(k) * T.stride;
+    w = sign * T.w[at];
+    if (cached) return P.obs_fwd[k] * scale * T.e[at];
     const double tv = vol * vol * P.obs_time[k];
     return P.obs_fwd[k] * scale * exp(-0.5 * tv + vol * w);
 }
 
 // pathwise_aad of a discrete product (European, Digital, Asian, lookback,
 // discrete barrier) on one path.
-__device__ PathAad discrete_aad(const DevicePlan& P, const ProductParams& pp, const double* w_tape,
-                                double* h_tape, size_t stride, double sign, double spot, double vol,
-                                bool& failed) {
+__device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
+                                                double sign, double spot, double vol, bool cached, bool& failed) {
     const uint32_t n = P.observation_count;
+    double* h_tape = T.x;
+    const size_t stride = T.stride;
     const double scale = spot / P.spot;
     const double h = P.smoothing;
     const bool call = pp.side == MCG_CALL;
@@ -53,7 +71,7 @@ __device__ PathAad discrete_aad(const DevicePlan& P, const ProductParams& pp, co
     int32_t arg = -1;  // lookback: observation holding the extremum (-1: the seasoned literal)
     for (uint32_t k = 0; k < n; ++k) {
         double w;
-        const double f = observe(P, w_tape, stride, k, sign, scale, vol, w);
+        const double f = observe(P, T, k, sign, scale, vol, cached, w);
         if (pp.kind == MCG_PRODUCT_LOOKBACK && monitored(pp, k) &&
             (acc.counts == 0u || (call ? !(acc.a >= f) : !(acc.a <= f))))
             arg = static_cast<int32_t>(k);
@@ -153,7 +171,7 @@ __device__ PathAad discrete_aad(const DevicePlan& P, const ProductParams& pp, co
         }
         if (adj == 0.0) continue;
         double w;
-        const double f = observe(P, w_tape, stride, static_cast<uint32_t>(k), sign, scale, vol, w);
+        const double f = observe(P, T, static_cast<uint32_t>(k), sign, scale, vol, cached, w);
         delta += adj * 1.0 * f / spot;
         vega += adj * 1.0 * f * (-vol * P.obs_time[k] + w);
     }
@@ -166,24 +184,55 @@ __device__ PathAad discrete_aad(const DevicePlan& P, const ProductParams& pp, co
 
 // pathwise_aad of a continuous barrier: the bridge over [0, t_1], ..., and
 // its adjoint (black_scholes.rs:94-293, 648-753); diag receives components
-// 10..17 of the evaluation.
-__device__ PathAad continuous_aad(const DevicePlan& P, const ProductParams& pp, const double* w_tape,
-                                  size_t stride, double sign, double spot, double vol, double* diag,
-                                  bool& failed) {
+// 10..17 of the evaluation.  Scratch rows: f_k at [0, n) of `f_tape` and
+// the node state adjoints sa_0..sa_n at [n, 2n + 1).  Each smoothed endpoint
+// is evaluated once per sweep and shared by the two intervals that meet there.
+__device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
+                                                  double sign, double spot, double vol, bool cached, double* diag,
+                                                  bool& failed) {
     const uint32_t n = P.observation_count;
+    double* f_tape = T.x;
+    const size_t stride = T.stride;
+    const double* w_tape = T.w;
     const double scale = spot / P.spot;
     const double h = P.smoothing;
     const double var = vol * vol;
     const bool up = pp.barrier_direction == MCG_BARRIER_UP;
+    const double B = pp.barrier;
+    double* sa_tape = f_tape + static_cast<size_t>(n) * stride;
     ProductAcc acc;
     acc_init(acc, pp);
-    barrier_begin(pp, acc, h, spot, failed);
+    double ld = 0.0;  // smoothed: effective log distance of the interval's left endpoint
+    if (h > 0.0) {
+        double safety;
+        smooth_endpoint(up, spot, B, h, safety, ld, failed);
+        acc.hit_log = 0.0 + log(safety);
+        acc.hit_prod = 1.0 * safety;
+    } else {
+        barrier_begin(pp, acc, h, spot, failed);
+    }
     double prev_f = spot, prev_t = 0.0, f = spot;
     for (uint32_t k = 0; k < n; ++k) {
         double w;
-        f = observe(P, w_tape, stride, k, sign, scale, vol, w);
+        f = observe(P, T, k, sign, scale, vol, cached, w);
+        f_tape[static_cast<size_t>(k) * stride] = f;
         const double t = P.obs_time[k];
-        barrier_interval(pp, acc, h, prev_f, f, var, var, t - prev_t, failed);
+        const double dt = t - prev_t;
+        if (h > 0.0) {
+            // barrier_interval with the left endpoint carried over
+            double rsafe, rd, log_surv;
+            smooth_endpoint(up, f, B, h, rsafe, rd, failed);
+            if (dt > 0.0) {
+                const int status = smooth_interval(ld, rd, var, var, dt, log_surv, failed);
+                acc.hit_log = acc.hit_log + log(rsafe);
+                acc.hit_prod = acc.hit_prod * rsafe;
+                acc.log_sum += log_surv;
+                count_status(acc, status);
+            }
+            ld = rd;
+        } else {
+            barrier_interval(pp, acc, h, prev_f, f, var, var, dt, failed);
+        }
         prev_f = f;
         prev_t = t;
     }
@@ -207,57 +256,59 @@ __device__ PathAad continuous_aad(const DevicePlan& P, const ProductParams& pp, 
     const bool exact_active = !(acc.initial_touched || acc.touched);
     const bool flows = h > 0.0 || exact_active;
     const double lsa = sd * surv;
-    // Variance adjoint over the intervals in order, then the state adjoints
-    // node by node: sa_k = right part of interval k-1 + left part of
-    // interval k + the smoothed hit factor (the terminal seed first at n).
+    // One sweep over the intervals: the variance adjoint in interval order and
+    // sa_k = ((0 + right part of interval k-1) + left part of interval k)
+    // + the smoothed hit factor at k; the terminal seed enters sa_n first.
     double var_adj = 0.0;
+    double carry = n == 0 ? 0.0 + td * 1.0 : 0.0;  // sa of the next node before its left part
     if (flows) {
+        SmoothEndpointFull el{1.0, 1.0, 0.0, 0.0};
+        if (h > 0.0) el = smooth_endpoint_full(up, spot, B, h);
         prev_f = spot;
         prev_t = 0.0;
         for (uint32_t k = 0; k < n; ++k) {
-            double w;
-            const double fk = observe(P, w_tape, stride, k, sign, scale, vol, w);
+            const double fk = f_tape[static_cast<size_t>(k) * stride];
             const double t = P.obs_time[k];
-            const IntervalAdjoint ia = barrier_interval_adjoint(up, pp.barrier, h, lsa, prev_f, fk, var, var, t - prev_t);
-            var_adj += ia.left_var + ia.right_var;
+            const double dt = t - prev_t;
+            double left = 0.0, right = 0.0, hit = 0.0;
+            SmoothEndpointFull er{1.0, 1.0, 0.0, 0.0};
+            if (h > 0.0) {
+                er = smooth_endpoint_full(up, fk, B, h);
+                if (dt > 0.0) {
+                    const SmoothIntervalDerivs d = smooth_interval_derivs(el.eld, er.eld, var, var, dt);
+                    left = 0.0 * el.hit_d_state + (lsa * d.d_left_distance) * el.eld_d_state;
+                    right = 0.0 * er.hit_d_state + (lsa * d.d_right_distance) * er.eld_d_state;
+                    var_adj += (lsa * d.d_left_var) + (lsa * d.d_right_var);
+                }
+                hit = el.safety == 0.0 ? 0.0 : -lsa * el.hit_d_state / el.safety;
+            } else {
+                const IntervalAdjoint ia = barrier_interval_adjoint(up, B, h, lsa, prev_f, fk, var, var, dt);
+                left = ia.left_state;
+                right = ia.right_state;
+                var_adj += ia.left_var + ia.right_var;
+            }
+            double sa = carry + left;
+            if (h > 0.0) sa += hit;
+            sa_tape[static_cast<size_t>(k) * stride] = sa;
+            carry = (k + 1 == n) ? (0.0 + td * 1.0) + right : 0.0 + right;
+            el = er;
             prev_f = fk;
             prev_t = t;
         }
+        if (h > 0.0) carry += el.safety == 0.0 ? 0.0 : -lsa * el.hit_d_state / el.safety;
+    } else {
+        for (uint32_t k = 0; k < n; ++k) sa_tape[static_cast<size_t>(k) * stride] = 0.0;
+        carry = 0.0 + td * 1.0;
     }
-    double delta = 0.0;
+    sa_tape[static_cast<size_t>(n) * stride] = carry;
+    double delta = sa_tape[0];
     double vega = 2.0 * vol * var_adj;
-    {
-        // node 0: the initial state
-        double sa = 0.0;
-        double f_next = 0.0, w_next = 0.0;
-        if (n > 0) f_next = observe(P, w_tape, stride, 0, sign, scale, vol, w_next);
-        IntervalAdjoint right{0.0, 0.0, 0.0, 0.0};
-        if (flows) {
-            right = barrier_interval_adjoint(up, pp.barrier, h, lsa, spot, f_next, var, var, P.obs_time[0]);
-            sa += right.left_state;
-            if (h > 0.0) sa += hit_factor_adjoint(up, pp.barrier, h, lsa, spot);
-        }
-        delta = sa;
-        double prev_t2 = P.obs_time[0];
-        for (uint32_t k = 0; k < n; ++k) {
-            // node k + 1 holds observation k
-            const double fk = f_next, wk = w_next;
-            double s = 0.0;
-            if (k + 1 == n) s += td * 1.0;
-            if (flows) s += right.right_state;
-            if (k + 1 < n) {
-                f_next = observe(P, w_tape, stride, k + 1, sign, scale, vol, w_next);
-                if (flows) {
-                    const double t = P.obs_time[k + 1];
-                    right = barrier_interval_adjoint(up, pp.barrier, h, lsa, fk, f_next, var, var, t - prev_t2);
-                    prev_t2 = t;
-                    s += right.left_state;
-                }
-            }
-            if (flows && h > 0.0) s += hit_factor_adjoint(up, pp.barrier, h, lsa, fk);
-            delta += s * fk / spot;
-            vega += s * fk * (-vol * P.obs_time[k] + wk);
-        }
+    for (uint32_t k = 0; k < n; ++k) {
+        const double s = sa_tape[static_cast<size_t>(k + 1) * stride];
+        const double fk = f_tape[static_cast<size_t>(k) * stride];
+        const double wk = sign * w_tape[static_cast<size_t>(k) * stride];
+        delta += s * fk / spot;
+        vega += s * fk * (-vol * P.obs_time[k] + wk);
     }
     PathAad r;
     r.price = P.discount * value;
@@ -267,41 +318,53 @@ __device__ PathAad continuous_aad(const DevicePlan& P, const ProductParams& pp, 
 }
 
 template <bool kCont>
-__device__ __forceinline__ PathAad path_aad(const DevicePlan& P, const ProductParams& pp, const double* w_tape,
-                                            double* h_tape, size_t stride, double sign, double spot, double vol,
-                                            double* diag, bool& failed) {
+__device__ __forceinline__ PathAad path_aad(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
+                                            double sign, double spot, double vol, bool cached, double* diag,
+                                            bool& failed) {
     if constexpr (kCont)
-        return continuous_aad(P, pp, w_tape, stride, sign, spot, vol, diag, failed);
+        return continuous_aad(P, pp, T, sign, spot, vol, cached, diag, failed);
     else
-        return discrete_aad(P, pp, w_tape, h_tape, stride, sign, spot, vol, failed);
+        return discrete_aad(P, pp, T, sign, spot, vol, cached, failed);
 }
 
 // The components of one primary or mate path (pathwise_values, :417-472).
+// The seven evaluations run in one loop over (spot, volatility) points, so the
+// evaluation body is instantiated once.
 template <bool kCont>
-__device__ void path_values(const DevicePlan& P, const ProductParams& pp, const double* w_tape, double* h_tape,
-                            size_t stride, double sign, double* v, bool& failed) {
+__device__ __forceinline__ void path_values(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
+                                            double sign, double* v, bool& failed) {
+    // the exponentials of this path at the plan's volatility
+    for (uint32_t k = 0; k < P.observation_count; ++k) {
+        const size_t at = static_cast<size_t>(k) * T.stride;
+        const double tv = P.vol * P.vol * P.obs_time[k];
+        T.e[at] = exp(-0.5 * tv + P.vol * (sign * T.w[at]));
+    }
     double diag[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     double scratch[8];
-    const PathAad base = path_aad<kCont>(P, pp, w_tape, h_tape, stride, sign, P.spot, P.vol, diag, failed);
-    double gamma = 0.0;
-    if (P.req_gamma) {
-        const double b = P.gamma_bump;
-        const PathAad dn = path_aad<kCont>(P, pp, w_tape, h_tape, stride, sign, P.spot - b, P.vol, scratch, failed);
-        const PathAad up = path_aad<kCont>(P, pp, w_tape, h_tape, stride, sign, P.spot + b, P.vol, scratch, failed);
-        gamma = (up.delta - dn.delta) / (2.0 * b);
+    const double b = P.gamma_bump, sb = P.spot_bump, vb = P.vol_bump;
+    // base, gamma down/up, validation spot down/up, validation volatility down/up
+    const double spots[7] = {P.spot, P.spot - b, P.spot + b, P.spot - sb, P.spot + sb, P.spot, P.spot};
+    const double vols[7] = {P.vol, P.vol, P.vol, P.vol, P.vol, P.vol - vb, P.vol + vb};
+    PathAad r[7];
+    auto evaluate = [&](int i) {
+        r[i] = PathAad{0.0, 0.0, 0.0};
+        if ((i == 1 || i == 2) && !P.req_gamma) return;
+        if (i >= 5 && P.vol_bump == 0.0) return;
+        r[i] = path_aad<kCont>(P, pp, T, sign, spots[i], vols[i], i < 5, i == 0 ? diag : scratch, failed);
+    };
+    if constexpr (kCont) {
+        // one copy of the (large) bridge body
+#pragma unroll 1
+        for (int i = 0; i < 7; ++i) evaluate(i);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 7; ++i) evaluate(i);
     }
-    const double sb = P.spot_bump;
-    const PathAad dn = path_aad<kCont>(P, pp, w_tape, h_tape, stride, sign, P.spot - sb, P.vol, scratch, failed);
-    const PathAad up = path_aad<kCont>(P, pp, w_tape, h_tape, stride, sign, P.spot + sb, P.vol, scratch, failed);
-    const double bump_delta = (up.price - dn.price) / (2.0 * sb);
-    const double bump_gamma = (up.price - 2.0 * base.price + dn.price) / (sb * sb);
-    double bump_vega = 0.0;
-    if (P.vol_bump != 0.0) {
-        const double vb = P.vol_bump;
-        const double a = path_aad<kCont>(P, pp, w_tape, h_tape, stride, sign, P.spot, P.vol - vb, scratch, failed).price;
-        const double b = path_aad<kCont>(P, pp, w_tape, h_tape, stride, sign, P.spot, P.vol + vb, scratch, failed).price;
-        bump_vega = (b - a) / (2.0 * vb);
-    }
+    const PathAad base = r[0];
+    const double gamma = P.req_gamma ? (r[2].delta - r[1].delta) / (2.0 * b) : 0.0;
+    const double bump_delta = (r[4].price - r[3].price) / (2.0 * sb);
+    const double bump_gamma = (r[4].price - 2.0 * base.price + r[3].price) / (sb * sb);
+    const double bump_vega = vb != 0.0 ? (r[6].price - r[5].price) / (2.0 * vb) : 0.0;
     v[MCG_PRICE] = base.price;
     v[MCG_DELTA] = base.delta;
     v[MCG_VEGA] = base.vega;
@@ -321,7 +384,7 @@ __device__ void path_values(const DevicePlan& P, const ProductParams& pp, const 
 // One thread per unit of [unit_begin, unit_end); CTA records of tile
 // unit/128 of scramble blockIdx.y.
 template <bool kCont>
-__global__ void __launch_bounds__(kThreads) bs_path_risk_kernel(const DevicePlan P, uint64_t unit_begin,
+__global__ void __launch_bounds__(kThreads, kCont ? 4 : 6) bs_path_risk_kernel(const DevicePlan P, uint64_t unit_begin,
                                                                 uint64_t unit_end, StatRecord* partials,
                                                                 uint32_t mask, ErrorWord* err, int detail) {
     __shared__ Stat s_red[4 * kComponents];
@@ -331,8 +394,9 @@ __global__ void __launch_bounds__(kThreads) bs_path_risk_kernel(const DevicePlan
     const uint64_t unit = valid ? point : 0;
     const size_t stride = static_cast<size_t>(gridDim.x) * gridDim.y * kThreads;
     const size_t local = (static_cast<size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * kThreads + threadIdx.x;
+    const size_t n = P.observation_count;
     double* w_tape = P.bs_tape + local;
-    double* h_tape = P.bs_tape + static_cast<size_t>(P.observation_count) * stride + local;
+    const Scratch T{w_tape, P.bs_tape + n * stride + local, P.bs_tape + 2 * n * stride + local, stride};
     NormalSource ns;
     ns.rqmc = P.engine == MCG_ENGINE_RQMC;
     ns.seed = P.seed;
@@ -351,10 +415,10 @@ __global__ void __launch_bounds__(kThreads) bs_path_risk_kernel(const DevicePlan
     const ProductParams& pp = P.products[0];
     bool failed = false;
     double vals[kComponents];
-    path_values<kCont>(P, pp, w_tape, h_tape, stride, 1.0, vals, failed);
+    path_values<kCont>(P, pp, T, 1.0, vals, failed);
     if (P.antithetic) {
         double mate[kComponents];
-        path_values<kCont>(P, pp, w_tape, h_tape, stride, -1.0, mate, failed);
+        path_values<kCont>(P, pp, T, -1.0, mate, failed);
 #pragma unroll
         for (int c = 0; c < kComponents; ++c) vals[c] = (vals[c] + mate[c]) * 0.5;
     }

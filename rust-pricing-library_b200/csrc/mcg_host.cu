@@ -817,12 +817,16 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
     MCG_CUDA(plan.records.alloc(static_cast<size_t>(P.scramble_count) * plan.product_count * kComponents));
     MCG_CUDA(plan.error.alloc(1));
     if (!lv && P.risk && !plan.single_terminal) {
-        // Scratch of the path-risk kernel: W_k per thread, and the hit state,
-        // weight and slope per observation for a smoothed discrete barrier.
+        // Scratch of the path-risk kernel (at most 2 GiB): W_k and the path's
+        // exponentials per thread, plus the hit state, weight and slope per
+        // observation for a smoothed discrete barrier, or the observed states
+        // and n + 1 node adjoints for a continuous barrier.
         const bool smooth_barrier =
             plan.products[0].kind == MCG_PRODUCT_DISCRETE_BARRIER && P.smoothing > 0.0;
-        P.bs_tape_rows = P.observation_count * (smooth_barrier ? 4u : 1u);
-        const uint64_t budget = (256ull << 20) / (sizeof(double) * P.bs_tape_rows * P.scramble_count);
+        const bool continuous = plan.products[0].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+        P.bs_tape_rows = smooth_barrier ? 5u * P.observation_count
+                                        : (continuous ? 4u * P.observation_count + 1u : 2u * P.observation_count);
+        const uint64_t budget = (2048ull << 20) / (sizeof(double) * P.bs_tape_rows * P.scramble_count);
         const uint64_t units_rounded = (P.units + kThreads - 1) / kThreads * kThreads;
         const uint64_t per_scramble =
             std::min<uint64_t>(units_rounded, std::max<uint64_t>(kThreads, budget / kThreads * kThreads));
