@@ -60,7 +60,7 @@ def parse():
                     help="pseudo paths of the BS path-risk secondary measurement")
     ap.add_argument("--secondary", default="all",
                     help="comma list of secondary measurements: early_exercise, book, f32, adjoint, "
-                         "path_risk; all; none")
+                         "path_risk, dual; all; none")
     ap.add_argument("--adjoint-paths", type=int, default=1 << 20)
     ap.add_argument("--lsm-units", type=int, default=1 << 20)
     ap.add_argument("--book-trades", type=int, default=4096)
@@ -312,6 +312,38 @@ def path_risk_secondary(units: int = 1 << 20, cpu_units: int = 1 << 14):
     return out
 
 
+def dual_secondary(units: int = 1 << 14, cpu_units: int = 2048):
+    """Andersen--Broadie upper bound of the early-exercise configuration's
+    American put (S = K = 100, r = 5 %, sigma = 25 %, T = 1, 50 exercise
+    dates; cubic policy on 2^16 antithetic training units): `units` antithetic
+    outer paths, 256 inner paths where the policy continues and 129 where it
+    exercises, from every non-terminal date.  The oracle on the host's cores
+    runs `cpu_units` outer units of the same plan for comparison."""
+    from rust_pricing_b200 import _native as N, workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+    from bermudan_tree import bermudan_equally_spaced
+    spec, lsm = W.american_bs(dates=50, units=units, training_units=1 << 16, antithetic=True)
+    n2, n3, seed = 256, 129, 0x1234
+    N.lsm_dual(spec, lsm, n2, n3, seed)
+    r = min((N.lsm_dual(spec, lsm, n2, n3, seed) for _ in range(2)), key=lambda x: x.device_ms)
+    tree = bermudan_equally_spaced(100.0, 100.0, 0.05, 0.0, 0.25, 1.0, 50, steps=5000)
+    spec.sampling_units = cpu_units
+    t0 = time.perf_counter()
+    c = H.oracle_lsm_dual(spec, lsm, n2, n3, seed, threads=os.cpu_count() or 1)
+    cpu_s = time.perf_counter() - t0
+    return {"workload": f"Andersen-Broadie dual, American put, 50 dates, {units} x 2 outer paths, "
+                        f"N2 = {n2}, N3 = {n3} inner paths; judge: 5000-step Bermudan tree",
+            "tree": tree, "device_ms": r.device_ms, "nested_ms": r.nested_ms,
+            "lower_bound": r.lower_bound.value, "lower_se": r.lower_bound.standard_error,
+            "upper_bound": r.upper_bound.value, "upper_se": r.upper_bound.standard_error,
+            "duality_gap": r.duality_gap.value, "gap_se": r.duality_gap.standard_error,
+            "inner_paths": r.inner_paths, "inner_paths_per_s": r.inner_paths / (r.nested_ms * 1e-3),
+            "kernel_launches": r.kernel_launches,
+            "cpu_oracle_inner_paths_per_s": c.inner_paths / cpu_s, "cpu_threads": os.cpu_count() or 1,
+            "cpu_sample": f"{cpu_units} outer units, training included ({cpu_s:.1f} s)"}
+
+
 def f32_secondary(points: int, scrambles: int, prices64):
     """The timed workload with the FP32 path bulk: time and the error of each
     price against the FP64 run's."""
@@ -500,7 +532,7 @@ def main():
         "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, buf.products[k].price.standard_error,
                                                 buf.products[k].price.value) for k in range(len(spec.products))],
     }
-    wanted = {"early_exercise", "book", "f32", "adjoint", "path_risk"} if args.secondary == "all" else (
+    wanted = {"early_exercise", "book", "f32", "adjoint", "path_risk", "dual"} if args.secondary == "all" else (
         set() if args.secondary == "none" else set(args.secondary.split(",")))
     if rank == 0 and world == 1 and wanted:
         sec = {}
@@ -517,6 +549,8 @@ def main():
             sec["adjoint"] = adjoint_secondary(args.adjoint_paths)
         if "path_risk" in wanted:
             sec["bs_path_risk"] = path_risk_secondary(args.path_risk_units)
+        if "dual" in wanted:
+            sec["dual_upper_bound"] = dual_secondary()
         line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

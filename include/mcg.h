@@ -582,6 +582,47 @@ typedef struct mcg_lsm_result {
 mcg_status mcg_lsm_price(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, void* stream,
                          mcg_lsm_result* result);
 
+/* ---- Andersen--Broadie dual upper bound of an early-exercise price ----
+ *
+ * Policy-based nested simulation around the fitted LSM policy
+ * (AndersenBroadiePlan, crates/pricing/src/engine/risk/dual.rs:132-462;
+ * Andersen and Broadie 2004, section 3).  Every outer valuation path is
+ * stopped by the policy (the lower bound, equal to mcg_lsm_price's price on
+ * the same request); at each exercise date before the last, inner paths from
+ * the path's state, run to their own policy stop, estimate the continuation
+ * value (exercise_inner_paths where the policy exercises, else
+ * continuation_inner_paths); the martingale of those estimates gives each
+ * path's duality gap.  Black--Scholes, pseudo-MC training and valuation
+ * engines, polynomial continuation, no Greeks, one American product.  Inner
+ * normals are Philox words of `inner_seed` at counter (path, dimension / 4,
+ * 0x4455414c), path = outer trajectory * max(N2, N3) + inner index,
+ * dimension = branch date * exercise dates + date. */
+typedef struct mcg_dual_desc {
+    uint32_t continuation_inner_paths; /* N2 */
+    uint32_t exercise_inner_paths;     /* N3 */
+    uint64_t inner_seed;
+} mcg_dual_desc;
+
+typedef struct mcg_dual_result {
+    /* Per-unit statistics of (lower, upper, gap); an antithetic unit is the
+     * average 0.5 primary + 0.5 mate. */
+    mcg_statistics components[3];
+    mcg_estimate lower_bound;
+    mcg_estimate upper_bound;
+    mcg_estimate duality_gap;
+    double price_confidence_interval_95[2]; /* lower - 1.96 SE, upper + 1.96 SE */
+    uint64_t outer_trajectories;
+    uint64_t inner_paths;                   /* inner paths simulated */
+    uint32_t exercise_date_count;
+    uint32_t kernel_launches;
+    float device_ms;
+    float nested_ms;                        /* the inner-path kernel */
+    mcg_error_record error;
+} mcg_dual_result;
+
+mcg_status mcg_lsm_dual(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
+                        void* stream, mcg_dual_result* result);
+
 /* The continuation network on given rows, exposed for the gradient checks (no
  * counterpart in the reference): outputs for `count` rows of inputs x[2 i],
  * x[2 i + 1]; and the gradient of sum_i mask_i (f(x_i) - y_i)^2 with respect to

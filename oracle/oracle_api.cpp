@@ -30,7 +30,9 @@ std::vector<double> piecewise_sinh_nodes(double left, double right, size_t nl, s
 int lsm_price(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, mcg_lsm_result* out, int threads);
 const char* lsm_last_error();
 int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vector<double>& spots,
-              uint64_t& path_count, mcg_error_record& err);
+              uint64_t& path_count, mcg_error_record& err, std::vector<double>* brownians);
+int lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
+             mcg_dual_result* out, int threads);
 int lsm_fit_api(const double* spots, const double* immediate, const double* targets, size_t rows,
                 const mcg_lsm_desc* lsm, mcg_lsm_date_model* out);
 }  // namespace oracle
@@ -140,13 +142,18 @@ int64_t oracle_lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads
     std::vector<double> spots;
     uint64_t paths = 0;
     mcg_error_record err{};
-    const int rc = oracle::lsm_spots(desc, domain, threads, spots, paths, err);
+    const int rc = oracle::lsm_spots(desc, domain, threads, spots, paths, err, nullptr);
     if (rc != MCG_OK) return -static_cast<int64_t>(rc);
     if (out && capacity >= spots.size()) std::memcpy(out, spots.data(), spots.size() * sizeof(double));
     return static_cast<int64_t>(paths);
 }
 
 // One date's regression (fit_exercise_decision) on given rows.
+int oracle_lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
+                    mcg_dual_result* out, int threads) {
+    return oracle::lsm_dual(desc, lsm, dual, out, threads);
+}
+
 int oracle_lsm_fit(const double* spots, const double* immediate, const double* targets,
                    uint64_t rows, const mcg_lsm_desc* lsm, mcg_lsm_date_model* out) {
     return oracle::lsm_fit_api(spots, immediate, targets, rows, lsm, out);

@@ -16,7 +16,9 @@
 // The path matrices come from oracle_plan.cpp (lsm_spots).  The regression is
 // single-threaded, as in the reference.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <thread>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -27,8 +29,9 @@
 namespace oracle {
 
 int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vector<double>& spots,
-              uint64_t& path_count, mcg_error_record& err);
+              uint64_t& path_count, mcg_error_record& err, std::vector<double>* brownians = nullptr);
 double plan_discount(const mcg_plan_desc* desc, double t);
+double plan_forward(const mcg_plan_desc* desc, double t);
 int lsm_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, const double* df, int threads,
                           mcg_lsm_result* result);
 int lsm_lv_fixed_policy_risk(const mcg_plan_desc* desc, const uint32_t* stops, const double* df, int threads,
@@ -296,6 +299,54 @@ std::vector<double> unit_values(const std::vector<double>& cf, bool antithetic, 
     return out;
 }
 
+// Backward induction over the training paths (train_exercise_policy,
+// lsm.rs:1486-1695): one fitted decision model per date before the last and
+// the in-sample value of the training paths under it.
+int train_policy(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, int threads, const std::vector<double>& df,
+                 std::vector<DateModel>& models, uint64_t& tp, double& in_sample_value, mcg_error_record& err) {
+    const size_t dates = desc->observation_count;
+    const mcg_product_desc& pr = desc->products[0];
+    const Config cfg{lsm->max_degree, lsm->itm_abs_tolerance, lsm->cpqr_abs_tolerance,
+                     lsm->cpqr_rel_tolerance, lsm->max_matrix_elements};
+    const bool rqmc = desc->engine == MCG_ENGINE_RQMC;
+    mcg_plan_desc train = *desc;
+    train.master_seed = lsm->training_seed;
+    train.sampling_units = lsm->training_units;
+    train.scramble_count = lsm->training_scramble_count;
+    train.scramble_begin = 0;
+    train.antithetic = lsm->training_antithetic;
+    train.brownian_bridge = lsm->training_brownian_bridge;
+    std::vector<double> spots;
+    tp = 0;
+    int rc = lsm_spots(&train, kDomainLsmTrain, threads, spots, tp, err);
+    if (rc != MCG_OK) return rc;
+    std::vector<double> imm(spots.size());
+    for (size_t i = 0; i < spots.size(); ++i) imm[i] = intrinsic(pr, spots[i]);
+    std::vector<double> realized(imm.begin() + (dates - 1) * tp, imm.begin() + dates * tp);
+    std::vector<uint32_t> stop(tp, static_cast<uint32_t>(dates - 1));
+    std::vector<double> targets(tp);
+    models.assign(dates - 1, DateModel{});
+    for (size_t d = dates - 1; d-- > 0;) {
+        for (size_t p = 0; p < tp; ++p) targets[p] = realized[p] * df[stop[p]] / df[d];
+        rc = fit_date(cfg, &imm[d * tp], &spots[d * tp], targets, tp, models[d]);
+        if (rc != MCG_OK) return rc;
+        for (size_t p = 0; p < tp; ++p)
+            if (models[d].exercise(imm[d * tp + p], spots[d * tp + p], cfg.degree)) {
+                realized[p] = imm[d * tp + p];
+                stop[p] = static_cast<uint32_t>(d);
+            }
+    }
+    std::vector<double> in_sample(tp);
+    for (size_t p = 0; p < tp; ++p) in_sample[p] = realized[p] * df[stop[p]];
+    const std::vector<double> in_units =
+        unit_values(in_sample, lsm->training_antithetic != 0, rqmc, lsm->training_units,
+                    lsm->training_scramble_count);
+    NeumaierSum in_sum;
+    for (double v : in_units) in_sum.add(v);
+    in_sample_value = in_sum.total() / static_cast<double>(in_units.size());
+    return MCG_OK;
+}
+
 }  // namespace
 
 // The early-exercise evaluation of mcg_lsm_price on the CPU.
@@ -318,41 +369,12 @@ int lsm_price(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, mcg_lsm_result
     const bool rqmc = desc->engine == MCG_ENGINE_RQMC;
 
     // Training phase.
-    mcg_plan_desc train = *desc;
-    train.master_seed = lsm->training_seed;
-    train.sampling_units = lsm->training_units;
-    train.scramble_count = lsm->training_scramble_count;
-    train.scramble_begin = 0;
-    train.antithetic = lsm->training_antithetic;
-    train.brownian_bridge = lsm->training_brownian_bridge;
-    std::vector<double> spots;
+    std::vector<DateModel> models;
     uint64_t tp = 0;
-    int rc = lsm_spots(&train, kDomainLsmTrain, threads, spots, tp, out->error);
+    int rc = train_policy(desc, lsm, threads, df, models, tp, out->in_sample_value, out->error);
     if (rc != MCG_OK) return rc;
-    std::vector<double> imm(spots.size());
-    for (size_t i = 0; i < spots.size(); ++i) imm[i] = intrinsic(pr, spots[i]);
-    std::vector<double> realized(imm.begin() + (dates - 1) * tp, imm.begin() + dates * tp);
-    std::vector<uint32_t> stop(tp, static_cast<uint32_t>(dates - 1));
-    std::vector<double> targets(tp);
-    std::vector<DateModel> models(dates - 1);
-    for (size_t d = dates - 1; d-- > 0;) {
-        for (size_t p = 0; p < tp; ++p) targets[p] = realized[p] * df[stop[p]] / df[d];
-        rc = fit_date(cfg, &imm[d * tp], &spots[d * tp], targets, tp, models[d]);
-        if (rc != MCG_OK) return rc;
-        for (size_t p = 0; p < tp; ++p)
-            if (models[d].exercise(imm[d * tp + p], spots[d * tp + p], cfg.degree)) {
-                realized[p] = imm[d * tp + p];
-                stop[p] = static_cast<uint32_t>(d);
-            }
-    }
-    std::vector<double> in_sample(tp);
-    for (size_t p = 0; p < tp; ++p) in_sample[p] = realized[p] * df[stop[p]];
-    const std::vector<double> in_units =
-        unit_values(in_sample, lsm->training_antithetic != 0, rqmc, lsm->training_units,
-                    lsm->training_scramble_count);
-    NeumaierSum in_sum;
-    for (double v : in_units) in_sum.add(v);
-    out->in_sample_value = in_sum.total() / static_cast<double>(in_units.size());
+    std::vector<double> spots, imm, realized;
+    std::vector<uint32_t> stop;
 
     // Valuation phase.
     uint64_t vp = 0;
@@ -415,6 +437,203 @@ int lsm_price(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, mcg_lsm_result
         }
         if (rc != MCG_OK) return rc;
     }
+    return MCG_OK;
+}
+
+namespace {
+
+constexpr uint32_t kDomainDualInner = 0x4455414cu;  // dual.rs:22, INNER_DOMAIN
+
+bool finite_or_fail(double v, const char* stage) {
+    if (std::isfinite(v)) return true;
+    g_lsm_error = std::string("non-finite ") + stage;
+    return false;
+}
+
+// DualPath, dual.rs:462-500: equation (9) telescoped; the policy is applied
+// after the first exercise as well.
+struct DualPath {
+    NeumaierSum correction;
+    double gap = -INFINITY;
+    bool observe(double payoff, double continuation, bool exercise, bool terminal) {
+        const double value = exercise ? payoff : continuation;
+        const double candidate = (payoff - value) - correction.total();
+        if (!finite_or_fail(candidate, "dual gap candidate")) return false;
+        gap = std::max(gap, candidate);
+        if (exercise && !terminal) {
+            const double c = payoff - continuation;
+            if (!finite_or_fail(c, "dual exercise correction")) return false;
+            correction.add(c);
+            if (!finite_or_fail(correction.total(), "dual accumulated correction")) return false;
+        }
+        return true;
+    }
+};
+
+}  // namespace
+
+// AndersenBroadiePlan::evaluate on the CPU (dual.rs:216-404): the fitted
+// policy of train_policy, outer valuation paths stopped by it, inner
+// rollouts from every non-terminal exercise date, per-unit (lower, upper,
+// gap) reduced in fixed blocks as DeterministicExecutor does.
+int lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
+             mcg_dual_result* out, int threads) {
+    g_lsm_error.clear();
+    if (!desc || !lsm || !dual || !out) return lsm_fail("null argument");
+    std::memset(&out->error, 0, sizeof(out->error));
+    if (desc->product_count != 1 || desc->products[0].kind != MCG_PRODUCT_AMERICAN)
+        return lsm_fail("one American product expected");
+    if (desc->model != MCG_MODEL_BLACK_SCHOLES || desc->engine != MCG_ENGINE_PSEUDO ||
+        lsm->continuation != MCG_CONTINUATION_POLYNOMIAL || desc->request_delta || desc->request_gamma ||
+        desc->request_vega || desc->request_local_vega_nodes)
+        return MCG_ERR_UNSUPPORTED;
+    if (dual->continuation_inner_paths < 1 || dual->exercise_inner_paths < 1)
+        return lsm_fail("inner path counts must be positive");
+    if (lsm->max_degree < 1 || lsm->max_degree > MCG_LSM_MAX_DEGREE) return lsm_fail("max_degree");
+    const size_t dates = desc->observation_count;
+    const mcg_product_desc& pr = desc->products[0];
+    std::vector<double> df(dates);
+    for (size_t d = 0; d < dates; ++d) df[d] = plan_discount(desc, desc->observation_times[d]);
+    std::vector<DateModel> models;
+    uint64_t tp = 0;
+    double in_sample = 0.0;
+    int rc = train_policy(desc, lsm, threads, df, models, tp, in_sample, out->error);
+    if (rc != MCG_OK) return rc;
+    std::vector<double> spots, brown;
+    uint64_t vp = 0;
+    rc = lsm_spots(desc, kDomainValuation, threads, spots, vp, out->error, &brown);
+    if (rc != MCG_OK) return rc;
+    const uint32_t degree = lsm->max_degree;
+    const double vol = desc->volatility;
+    const double* t = desc->observation_times;
+    // forwards of the exercise dates (as the path store uses them) and the
+    // step roots sqrt(t_j - t_{j-1}) of the inner paths
+    std::vector<double> fwd(dates), sqdt(dates, 0.0);
+    for (size_t d = 0; d < dates; ++d) fwd[d] = plan_forward(desc, t[d]);
+    for (size_t d = 1; d < dates; ++d) sqdt[d] = std::sqrt(t[d] - t[d - 1]);
+    const uint64_t units = desc->sampling_units;
+    const uint64_t lanes = desc->antithetic ? 2 : 1;
+    const uint64_t stride = std::max(dual->continuation_inner_paths, dual->exercise_inner_paths);
+    std::vector<double> values(3 * units);
+    std::vector<std::string> errors(static_cast<size_t>(std::max(1, threads)));
+    std::atomic<uint64_t> next{0};
+    std::atomic<bool> failed{false};
+    std::atomic<uint64_t> inner_total{0};
+    auto outer = [&](uint64_t trajectory, double res[3], uint64_t& inner_count) -> bool {
+        double lower = 0.0;
+        bool have_lower = false;
+        DualPath dp;
+        for (size_t d = 0; d < dates; ++d) {
+            const double s = spots[d * vp + trajectory];
+            const double payoff = intrinsic(pr, s);
+            const bool terminal = d + 1 == dates;
+            const bool exercise = terminal || models[d].exercise(payoff, s, degree);
+            const double discounted = payoff * df[d];
+            if (!finite_or_fail(discounted, "dual discounted payoff")) return false;
+            if (exercise && !have_lower) {
+                lower = discounted;
+                have_lower = true;
+            }
+            double continuation = 0.0;
+            if (!terminal) {
+                // rollout_mean, dual.rs:340-400
+                const uint32_t configured = exercise ? dual->exercise_inner_paths : dual->continuation_inner_paths;
+                const uint32_t paths = vol == 0.0 ? 1u : configured;
+                NeumaierSum sum;
+                for (uint32_t inner = 0; inner < paths; ++inner) {
+                    const uint64_t path = trajectory * stride + inner;
+                    double w = brown[d * vp + trajectory];
+                    for (size_t j = d + 1; j < dates; ++j) {
+                        const uint32_t dim = static_cast<uint32_t>(d * dates + j);
+                        const double z = vol == 0.0 ? 0.0 : philox_normal(dual->inner_seed, path, dim, kDomainDualInner);
+                        w += sqdt[j] * z;
+                        const double variance = vol * vol * t[j];
+                        const double canonical = fwd[j] * std::exp(-0.5 * variance + vol * w);
+                        const double spot_j = 0.0 * desc->spot + 1.0 * canonical;
+                        if (!finite_or_fail(spot_j, "dual inner spot")) return false;
+                        const double imm = intrinsic(pr, spot_j);
+                        if (j + 1 == dates || models[j].exercise(imm, spot_j, degree)) {
+                            const double v = imm * df[j];
+                            if (!finite_or_fail(v, "dual inner payoff")) return false;
+                            sum.add(v);
+                            break;
+                        }
+                    }
+                }
+                inner_count += paths;
+                continuation = sum.total() / static_cast<double>(paths);
+                if (!finite_or_fail(continuation, "dual inner mean")) return false;
+            }
+            if (!dp.observe(discounted, continuation, exercise, terminal)) return false;
+        }
+        res[0] = lower;
+        res[1] = lower + dp.gap;
+        res[2] = dp.gap;
+        return finite_or_fail(res[1], "dual upper sample");
+    };
+    auto worker = [&](size_t tid) {
+        uint64_t inner_count = 0;
+        for (;;) {
+            const uint64_t u = next.fetch_add(1);
+            if (u >= units || failed.load()) break;
+            double a[3], b[3];
+            if (!outer(u * lanes, a, inner_count)) {
+                errors[tid] = g_lsm_error;
+                failed = true;
+                break;
+            }
+            if (lanes == 2) {
+                if (!outer(u * lanes + 1, b, inner_count)) {
+                    errors[tid] = g_lsm_error;
+                    failed = true;
+                    break;
+                }
+                for (int c = 0; c < 3; ++c) a[c] = 0.5 * a[c] + 0.5 * b[c];
+            }
+            for (int c = 0; c < 3; ++c) values[3 * u + c] = a[c];
+        }
+        inner_total += inner_count;
+    };
+    std::vector<std::thread> pool;
+    for (size_t i = 0; i < errors.size(); ++i) pool.emplace_back(worker, i);
+    for (auto& th : pool) th.join();
+    if (failed) {
+        for (auto& e : errors)
+            if (!e.empty()) g_lsm_error = e;
+        out->error.code = MCG_ERR_LSM;
+        return MCG_ERR_LSM;
+    }
+    // DeterministicExecutor blocks of reduction_block_size, merged in the fixed tree.
+    const uint64_t block = desc->reduction_block_size ? desc->reduction_block_size : 4096;
+    const uint64_t nblocks = (units + block - 1) / block;
+    const double inv = 1.0 / static_cast<double>(units);
+    mcg_estimate* est[3] = {&out->lower_bound, &out->upper_bound, &out->duality_gap};
+    for (int c = 0; c < 3; ++c) {
+        std::vector<NeumaierSum> sums(nblocks);
+        std::vector<CenteredMoment> moms(nblocks);
+        for (uint64_t b = 0; b < nblocks; ++b) {
+            Statistics st;
+            for (uint64_t u = b * block; u < std::min(units, (b + 1) * block); ++u) st.add(values[3 * u + c]);
+            sums[b] = st.sum;
+            moms[b] = st.moments;
+        }
+        Statistics total;
+        total.sum = fixed_tree_reduce(sums, NeumaierSum::merged);
+        total.moments = fixed_tree_reduce(moms, CenteredMoment::merged);
+        out->components[c] = {total.sum.sum, total.sum.correction, total.moments.count, total.moments.mean,
+                              total.moments.second_moment};
+        const double value = total.sum.total() * inv * 1.0;
+        const double var = total.moments.count > 1
+                               ? total.moments.second_moment / static_cast<double>(total.moments.count - 1)
+                               : 0.0;
+        const double se = std::sqrt(var * inv) * 1.0;
+        *est[c] = {value, se, value - kNormal95 * se, value + kNormal95 * se, units};
+    }
+    out->price_confidence_interval_95[0] = out->lower_bound.confidence_lower;
+    out->price_confidence_interval_95[1] = out->upper_bound.confidence_upper;
+    out->outer_trajectories = units * lanes;
+    out->inner_paths = inner_total.load();
+    out->exercise_date_count = static_cast<uint32_t>(dates);
     return MCG_OK;
 }
 

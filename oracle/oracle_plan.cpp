@@ -1477,7 +1477,7 @@ int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacit
 // scramble-major.  Spots are post_spot of write_lsm_trajectory and
 // write_local_vol_lsm_trajectory (early_exercise.rs:330-450).
 int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vector<double>& spots,
-              uint64_t& path_count, mcg_error_record& err) {
+              uint64_t& path_count, mcg_error_record& err, std::vector<double>* brownians) {
     Plan p;
     if (!build_plan(desc, p)) return MCG_ERR_INVALID_ARGUMENT;
     p.domain = domain;
@@ -1487,6 +1487,7 @@ int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vect
     const size_t dates = p.obs_t.size();
     path_count = units * mult;
     spots.assign(dates * path_count, 0.0);
+    if (brownians) brownians->assign(dates * path_count, 0.0);
     const bool lv = p.model == MCG_MODEL_LOCAL_VOLATILITY;
     std::vector<Failure> failures(static_cast<size_t>(std::max(1, threads)));
     std::vector<uint64_t> failed_unit(failures.size(), ~0ull);
@@ -1518,6 +1519,8 @@ int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vect
                     } else {
                         bs_observations(p, z.data(), p.spot, p.vol, obs.data());
                         for (size_t d = 0; d < dates; ++d) spots[d * path_count + col] = obs[d].post_spot;
+                        if (brownians)
+                            for (size_t d = 0; d < dates; ++d) (*brownians)[d * path_count + col] = obs[d].w;
                     }
                 }
             }
@@ -1845,6 +1848,17 @@ double plan_discount(const mcg_plan_desc* desc, double t) {
     c.set(desc->discount_curve.times, desc->discount_curve.discount_factors,
           desc->discount_curve.pillar_count);
     return std::exp(c.log_discount(t));
+}
+
+// The forward of the plan's spot at t (forward_at, as the path store uses it).
+double plan_forward(const mcg_plan_desc* desc, double t) {
+    Plan p;
+    p.spot = desc->spot;
+    p.rc.set(desc->discount_curve.times, desc->discount_curve.discount_factors,
+             desc->discount_curve.pillar_count);
+    p.qc.set(desc->dividend_curve.times, desc->dividend_curve.discount_factors,
+             desc->dividend_curve.pillar_count);
+    return forward_at(p, p.spot, t);
 }
 
 }  // namespace oracle

@@ -27,6 +27,7 @@ UNITS = [
     ("mcg_lv_adjoint.cu", ["-fmad=false"]),
     ("mcg_bs.cu", ["-fmad=false"]),
     ("mcg_bs_risk.cu", ["-fmad=false"]),
+    ("mcg_dual.cu", ["-fmad=false"]),
     ("mcg_setup.cu", ["-fmad=false"]),
     ("mcg_host.cu", ["-fmad=false"]),
     ("mcg_noalloc.cu", ["-fmad=false"]),

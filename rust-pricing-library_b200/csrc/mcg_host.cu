@@ -19,6 +19,7 @@
 #include <memory>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <queue>
 #include <string>
 #include <vector>
@@ -1784,6 +1785,143 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     return MCG_OK;
 }
 
+// AndersenBroadiePlan::compile/evaluate (crates/pricing/src/engine/risk/dual.rs:140-404):
+// the policy trained and the outer paths valued by lsm_price, then the
+// nested simulation of mcg_dual.cu around that policy.
+mcg_status lsm_dual(const mcg_plan_desc* d, const mcg_lsm_desc* l, const mcg_dual_desc* x, cudaStream_t stream,
+                    mcg_dual_result* r) {
+    if (!d || !l || !x || !r) return fail(MCG_ERR_INVALID_ARGUMENT, "null argument");
+    std::memset(r, 0, sizeof(*r));
+    if (d->product_count != 1 || !d->products || d->products[0].kind != MCG_PRODUCT_AMERICAN)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "the dual prices exactly one American product");
+    if (d->model != MCG_MODEL_BLACK_SCHOLES)
+        return fail(MCG_ERR_UNSUPPORTED, "the dual upper bound runs under Black-Scholes");
+    if (d->engine != MCG_ENGINE_PSEUDO)
+        return fail(MCG_ERR_UNSUPPORTED, "the dual upper bound needs pseudo-MC training and valuation engines");
+    if (l->continuation != MCG_CONTINUATION_POLYNOMIAL)
+        return fail(MCG_ERR_UNSUPPORTED, "the dual upper bound uses the polynomial policy");
+    if (d->request_delta || d->request_gamma || d->request_vega || d->request_local_vega_nodes)
+        return fail(MCG_ERR_UNSUPPORTED, "Greeks of the dual (use a fixed-policy risk request)");
+    if (x->continuation_inner_paths == 0 || x->exercise_inner_paths == 0)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "inner path counts must be positive");
+    const uint32_t dates = d->observation_count;
+    const uint64_t lanes = d->antithetic ? 2 : 1;
+    const uint64_t stride = std::max(x->continuation_inner_paths, x->exercise_inner_paths);
+    const uint64_t trajectories = d->sampling_units * lanes;
+    if (d->sampling_units == 0 || trajectories / lanes != d->sampling_units ||
+        trajectories > std::numeric_limits<uint64_t>::max() / stride ||
+        static_cast<uint64_t>(dates) * dates > 0xffffffffull)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "random-coordinate count overflows");
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    struct EventGuard {
+        cudaEvent_t* e;
+        ~EventGuard() {
+            for (int i = 0; i < 4; ++i)
+                if (e[i]) cudaEventDestroy(e[i]);
+        }
+    } guard{ev};
+    for (cudaEvent_t& e : ev) MCG_CUDA(cudaEventCreate(&e));
+    MCG_CUDA(cudaEventRecord(ev[0], stream));
+    // The policy (and the lower bound's valuation, the same outer paths).
+    std::vector<mcg_lsm_date_model> models(std::max<uint32_t>(dates - 1, 1));
+    std::vector<uint64_t> counts(dates);
+    mcg_lsm_result lr{};
+    lr.date_capacity = dates;
+    lr.models = models.data();
+    lr.exercise_counts = counts.data();
+    mcg_status st = lsm_price(d, l, stream, &lr);
+    if (st != MCG_OK) {
+        r->error = lr.error;
+        return st;
+    }
+    mcg_product_desc placeholder = d->products[0];
+    placeholder.kind = MCG_PRODUCT_EUROPEAN;
+    mcg_plan_desc vd = *d;
+    vd.products = &placeholder;
+    vd.payment_time = d->observation_times[dates - 1];
+    mcg_plan vplan;
+    if ((st = build(&vd, vplan)) != MCG_OK) return st;
+    const DevicePlan& P = vplan.dp;
+    HostCurve rc;
+    std::string why;
+    if (!load_curve(d->discount_curve, rc, "discount_curve", why)) return fail(MCG_ERR_MARKET, why);
+    std::vector<double> df(dates), sq(dates, 0.0);
+    for (uint32_t i = 0; i < dates; ++i) df[i] = std::exp(rc.log_discount(d->observation_times[i]));
+    for (uint32_t i = 1; i < dates; ++i) sq[i] = std::sqrt(d->observation_times[i] - d->observation_times[i - 1]);
+    DeviceArray<mcg_lsm_date_model> dmodels;
+    DeviceArray<double> ddf, dsq, spot, brownian, continuation;
+    DeviceArray<uint8_t> exercise;
+    DeviceArray<unsigned long long> words;
+    DeviceArray<StatRecord> partials, records;
+    MCG_CUDA(dmodels.upload(models));
+    MCG_CUDA(ddf.upload(df));
+    MCG_CUDA(dsq.upload(sq));
+    const size_t cells = static_cast<size_t>(dates) * trajectories;
+    MCG_CUDA(spot.alloc(cells));
+    MCG_CUDA(brownian.alloc(cells));
+    MCG_CUDA(continuation.alloc(cells));
+    MCG_CUDA(exercise.alloc(cells));
+    MCG_CUDA(words.alloc(2));
+    const uint32_t tiles = static_cast<uint32_t>((P.units + kThreads - 1) / kThreads);
+    MCG_CUDA(partials.alloc(static_cast<size_t>(tiles) * 3));
+    MCG_CUDA(records.alloc(3));
+    const unsigned long long init[2] = {~0ull, 0ull};
+    MCG_CUDA(cudaMemcpyAsync(words.ptr, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    DualArgs A{};
+    A.models = dmodels.ptr;
+    A.nb = l->max_degree + 1;
+    A.df = ddf.ptr;
+    A.sqrt_step = dsq.ptr;
+    A.side = d->products[0].side;
+    A.strike = d->products[0].strike;
+    A.notional = d->products[0].notional;
+    A.trajectories = trajectories;
+    A.path_stride = stride;
+    A.continuation_inner_paths = x->continuation_inner_paths;
+    A.exercise_inner_paths = x->exercise_inner_paths;
+    A.inner_seed = x->inner_seed;
+    A.spot = spot.ptr;
+    A.brownian = brownian.ptr;
+    A.exercise = exercise.ptr;
+    A.continuation = continuation.ptr;
+    A.failure = &words.ptr[0];
+    A.inner_count = &words.ptr[1];
+    uint32_t launches = lr.kernel_launches;
+    MCG_CUDA(launch_dual(P, A, partials.ptr, stream, ev[1], ev[2], launches));
+    reduce_tiles_kernel<<<dim3(3, 1), 256, 0, stream>>>(partials.ptr, tiles, 3, records.ptr);
+    MCG_CUDA(cudaGetLastError());
+    ++launches;
+    MCG_CUDA(cudaEventRecord(ev[3], stream));
+    StatRecord rec[3];
+    unsigned long long w[2];
+    MCG_CUDA(cudaMemcpyAsync(rec, records.ptr, sizeof(rec), cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaMemcpyAsync(w, words.ptr, sizeof(w), cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaStreamSynchronize(stream));
+    if (w[0] != ~0ull) {
+        r->error.code = MCG_ERR_LSM;
+        r->error.sampling_unit = w[0] / lanes;
+        return fail(MCG_ERR_LSM, "non-finite dual intermediate on outer trajectory " + std::to_string(w[0]));
+    }
+    mcg_estimate* est[3] = {&r->lower_bound, &r->upper_bound, &r->duality_gap};
+    for (int c = 0; c < 3; ++c) {
+        const HostStat h{rec[c].sum, rec[c].corr, static_cast<uint64_t>(rec[c].count), rec[c].mean, rec[c].m2};
+        r->components[c] = {h.sum, h.corr, h.count, h.mean, h.m2};
+        *est[c] = make_estimate(h, P.units, 1.0);
+    }
+    r->price_confidence_interval_95[0] = r->lower_bound.confidence_lower;
+    r->price_confidence_interval_95[1] = r->upper_bound.confidence_upper;
+    r->outer_trajectories = trajectories;
+    r->inner_paths = w[1];
+    r->exercise_date_count = dates;
+    r->kernel_launches = launches;
+    float ms = 0.f, nested = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[3]);
+    cudaEventElapsedTime(&nested, ev[1], ev[2]);
+    r->device_ms = ms;
+    r->nested_ms = nested;
+    return MCG_OK;
+}
+
 // --------------------------------------------------------------- book of trades
 
 }  // namespace
@@ -2107,6 +2245,11 @@ void mcg_plan_destroy(mcg_plan* plan) { delete plan; }
 mcg_status mcg_lsm_price(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, void* stream,
                          mcg_lsm_result* result) {
     return lsm_price(plan, lsm, static_cast<cudaStream_t>(stream), result);
+}
+
+mcg_status mcg_lsm_dual(const mcg_plan_desc* plan, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
+                        void* stream, mcg_dual_result* result) {
+    return lsm_dual(plan, lsm, dual, static_cast<cudaStream_t>(stream), result);
 }
 
 mcg_status mcg_book_create(const mcg_plan_desc* trades, uint32_t trade_count, const mcg_book_options* options,

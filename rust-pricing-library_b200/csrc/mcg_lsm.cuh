@@ -61,6 +61,31 @@ struct LsmRiskArgs {
     double gamma_bump, spot_bump, vol_bump;
 };
 
+// Andersen--Broadie dual (mcg_dual.cu): the fitted policy, the outer paths'
+// states and decisions [date][trajectory], and the continuation estimates of
+// the inner rollouts.
+struct DualArgs {
+    const mcg_lsm_date_model* models;  // [dates - 1]
+    uint32_t nb;                       // basis columns: max_degree + 1
+    const double* df;                  // [dates]
+    const double* sqrt_step;           // [dates]: sqrt(t_j - t_{j-1}), 0 at j = 0
+    int32_t side;
+    double strike, notional;
+    uint64_t trajectories;             // units x lanes
+    uint64_t path_stride;              // max(N2, N3)
+    uint32_t continuation_inner_paths, exercise_inner_paths;
+    uint64_t inner_seed;
+    double* spot;                      // [dates][trajectories]
+    double* brownian;
+    uint8_t* exercise;
+    double* continuation;
+    unsigned long long* failure;       // first trajectory with a non-finite intermediate
+    unsigned long long* inner_count;   // inner paths simulated
+};
+
+cudaError_t launch_dual(const DevicePlan& P, const DualArgs& A, StatRecord* partials, cudaStream_t stream,
+                        cudaEvent_t nested_begin, cudaEvent_t nested_end, uint32_t& launches);
+
 cudaError_t launch_lsm_bs_spots(const DevicePlan& P, uint32_t domain, double* spots, uint64_t paths,
                                 unsigned long long* bad, cudaStream_t stream);
 // Local-volatility path store (mcg_lv.cu): date-major spots of every path at

@@ -228,6 +228,24 @@ class LsmResult(C.Structure):
     ]
 
 
+class DualDesc(C.Structure):
+    """mcg_dual_desc: the Andersen--Broadie inner path counts and seed."""
+    _fields_ = [("continuation_inner_paths", C.c_uint32), ("exercise_inner_paths", C.c_uint32),
+                ("inner_seed", C.c_uint64)]
+
+
+class DualResult(C.Structure):
+    _fields_ = [
+        ("components", Statistics * 3),
+        ("lower_bound", Estimate), ("upper_bound", Estimate), ("duality_gap", Estimate),
+        ("price_confidence_interval_95", C.c_double * 2),
+        ("outer_trajectories", C.c_uint64), ("inner_paths", C.c_uint64),
+        ("exercise_date_count", C.c_uint32), ("kernel_launches", C.c_uint32),
+        ("device_ms", C.c_float), ("nested_ms", C.c_float),
+        ("error", ErrorRecord),
+    ]
+
+
 class LsmBuffers:
     """Caller-owned storage for an early-exercise result of `dates` exercise
     dates and, when `stopping` > 0, that many valuation stopping indices."""

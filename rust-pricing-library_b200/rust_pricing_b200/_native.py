@@ -20,6 +20,7 @@ EXPORTS = (
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
     "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient", "mcg_book_create", "mcg_book_evaluate",
     "mcg_book_destroy", "mcg_surface_local_variance_grid", "mcg_surface_total_variance", "mcg_vega_kt_project",
+    "mcg_lsm_dual",
 )
 
 _lib = None
@@ -80,6 +81,9 @@ def library() -> C.CDLL:
     lib.mcg_measure_fp64_peak.restype = C.c_int
     lib.mcg_lsm_price.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.LsmDesc), vp, C.POINTER(A.LsmResult)]
     lib.mcg_lsm_price.restype = C.c_int
+    lib.mcg_lsm_dual.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.LsmDesc), C.POINTER(A.DualDesc), vp,
+                                 C.POINTER(A.DualResult)]
+    lib.mcg_lsm_dual.restype = C.c_int
     fp = C.POINTER(C.c_float)
     lib.mcg_mlp_forward.argtypes = [fp, fp, u32, fp]
     lib.mcg_mlp_forward.restype = C.c_int
@@ -177,6 +181,19 @@ def lsm_price(spec, lsm, stopping: bool = False, stream: int = 0) -> A.LsmBuffer
     status = library().mcg_lsm_price(C.byref(desc), C.byref(ldesc), C.c_void_p(stream), C.byref(buf.result))
     check(status, buf.result.error)
     return buf
+
+
+def lsm_dual(spec, lsm, continuation_inner_paths: int, exercise_inner_paths: int, inner_seed: int,
+             stream: int = 0) -> A.DualResult:
+    """mcg_lsm_dual: Andersen--Broadie lower and upper bounds of an
+    early-exercise price around the fitted LSM policy, on the GPU."""
+    out = A.DualResult()
+    desc, ldesc = spec.desc(), lsm.desc()
+    dual = A.DualDesc(continuation_inner_paths, exercise_inner_paths, inner_seed & 0xFFFFFFFFFFFFFFFF)
+    status = library().mcg_lsm_dual(C.byref(desc), C.byref(ldesc), C.byref(dual), C.c_void_p(stream),
+                                    C.byref(out))
+    check(status, out.error)
+    return out
 
 
 def mlp_forward(params, x):

@@ -85,6 +85,9 @@ def oracle():
     lib.oracle_lsm_last_error.restype = C.c_char_p
     lib.oracle_lsm_spots.argtypes = [C.POINTER(A.PlanDesc), u32, C.c_int, C.POINTER(dbl), u64]
     lib.oracle_lsm_spots.restype = C.c_int64
+    lib.oracle_lsm_dual.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.LsmDesc), C.POINTER(A.DualDesc),
+                                    C.POINTER(A.DualResult), C.c_int]
+    lib.oracle_lsm_dual.restype = C.c_int
     lib.oracle_lsm_fit.argtypes = [C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl), u64,
                                    C.POINTER(A.LsmDesc), C.POINTER(A.LsmDateModel)]
     lib.oracle_lsm_fit.restype = C.c_int
@@ -119,6 +122,19 @@ def oracle_lsm(spec, lsm, stopping: bool = False, threads: int | None = None):
         raise RuntimeError(f"oracle status {A.STATUS_NAMES.get(rc, rc)}: "
                            f"{lib.oracle_lsm_last_error().decode()} {lib.oracle_last_error().decode()}")
     return buf
+
+
+def oracle_lsm_dual(spec, lsm, n2: int, n3: int, seed: int, threads: int | None = None):
+    """Run the oracle's Andersen--Broadie dual; returns the DualResult."""
+    lib = oracle()
+    out = A.DualResult()
+    desc, ldesc = spec.desc(), lsm.desc()
+    dual = A.DualDesc(n2, n3, seed & 0xFFFFFFFFFFFFFFFF)
+    rc = lib.oracle_lsm_dual(C.byref(desc), C.byref(ldesc), C.byref(dual), C.byref(out),
+                             threads or os.cpu_count() or 1)
+    if rc != 0:
+        raise RuntimeError(f"oracle status {A.STATUS_NAMES.get(rc, rc)}: {lib.oracle_lsm_last_error().decode()}")
+    return out
 
 
 def dptr(array):
