@@ -58,6 +58,8 @@ def parse():
                     help="path arithmetic of the timed workload (f32: FP32 path bulk)")
     ap.add_argument("--path-risk-units", type=int, default=1 << 20,
                     help="pseudo paths of the BS path-risk secondary measurement")
+    ap.add_argument("--dual-units", type=int, default=1 << 14,
+                    help="antithetic outer units of the Andersen-Broadie secondary measurement")
     ap.add_argument("--secondary", default="all",
                     help="comma list of secondary measurements: early_exercise, book, f32, adjoint, "
                          "path_risk, dual; all; none")
@@ -550,7 +552,7 @@ def main():
         if "path_risk" in wanted:
             sec["bs_path_risk"] = path_risk_secondary(args.path_risk_units)
         if "dual" in wanted:
-            sec["dual_upper_bound"] = dual_secondary()
+            sec["dual_upper_bound"] = dual_secondary(args.dual_units)
         line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
