@@ -9,9 +9,9 @@
 //      black_scholes.rs:297-331);
 //   2. `dual_inner_kernel`: one warp per (outer path, non-terminal exercise
 //      date): the rollout_mean of that date (dual.rs:340-400).  Lanes
-//      simulate inner paths 32 at a time, each from the outer path's state to
-//      its own policy stop; lane 0 adds their discounted payoffs in inner-path
-//      order to a Neumaier sum, so the mean is the reference's sequential sum;
+//      simulate inner paths, each from the outer path's state to its own
+//      policy stop; lane 0 adds their discounted payoffs in inner-path order
+//      to a Neumaier sum, so the mean is the reference's sequential sum;
 //   3. `dual_combine_kernel`: one thread per unit runs DualPath (dual.rs:462-500)
 //      over the dates with those continuation estimates and writes the CTA's
 //      statistics records of (lower, upper, gap).
@@ -93,12 +93,21 @@ __global__ void __launch_bounds__(kThreads) dual_outer_kernel(const DevicePlan P
 }
 
 // rollout_mean of (trajectory, branch date): one warp each, four per CTA;
-// tasks [first_task, first_task + tasks) of trajectory x (dates - 1).
+// tasks [first_task, first_task + tasks) of trajectory x (dates - 1).  Inner
+// paths go in chunks of 32 x kDualSlots: in one loop each lane advances its
+// current path by one date per iteration and takes its next path of the chunk
+// as soon as one stops (so a lane never waits for a slower lane's path), the
+// discounted payoffs land in shared memory by inner index, and lane 0 adds
+// the chunk to the Neumaier sum in that order.
+constexpr int kDualSlots = 8;
+
 __global__ void __launch_bounds__(kThreads) dual_inner_kernel(const DevicePlan P, DualArgs A, uint64_t first_task,
                                                               uint64_t tasks) {
+    __shared__ double s_values[kThreads / 32][32 * kDualSlots];
     const uint64_t task = first_task + static_cast<uint64_t>(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     if (task >= first_task + tasks) return;  // whole warps leave together
+    double* values = s_values[threadIdx.x / 32];
     const uint32_t dates = P.observation_count;
     const uint32_t branches = dates - 1;
     const uint64_t trajectory = task / branches;
@@ -110,41 +119,50 @@ __global__ void __launch_bounds__(kThreads) dual_inner_kernel(const DevicePlan P
     const double w0 = A.brownian[at];
     double sum = 0.0, corr = 0.0;  // lane 0's sequential Neumaier sum
     bool bad = false;
-    for (uint32_t base = 0; base < paths; base += 32) {
-        const uint32_t inner = base + static_cast<uint32_t>(lane);
-        double value = 0.0;
-        if (inner < paths) {
+    for (uint32_t c0 = 0; c0 < paths; c0 += 32u * kDualSlots) {
+        int slot = 0;
+        uint32_t inner = c0 + static_cast<uint32_t>(lane);
+        bool active = inner < paths;
+        double w = w0;
+        uint32_t j = d + 1;
+        uint32_t cached = 0xffffffffu;
+        uint4 block = make_uint4(0u, 0u, 0u, 0u);
+        while (__any_sync(0xffffffffu, active)) {
+            if (!active) continue;
             const uint64_t path = trajectory * A.path_stride + inner;
-            double w = w0;
-            uint32_t cached = 0xffffffffu;
-            uint4 block = make_uint4(0u, 0u, 0u, 0u);
-            for (uint32_t j = d + 1; j < dates; ++j) {
-                double z = 0.0;
-                if (P.vol != 0.0) {
-                    const uint32_t dim = d * dates + j;
-                    if ((dim >> 2) != cached) {
-                        cached = dim >> 2;
-                        block = philox_block(A.inner_seed, path, cached, kDualDomain);
-                    }
-                    z = as241(open_unit(lane_of(block, dim & 3u)));
+            double z = 0.0;
+            if (P.vol != 0.0) {
+                const uint32_t dim = d * dates + j;
+                if ((dim >> 2) != cached) {
+                    cached = dim >> 2;
+                    block = philox_block(A.inner_seed, path, cached, kDualDomain);
                 }
-                w += A.sqrt_step[j] * z;
-                const double variance = P.vol * P.vol * P.obs_time[j];
-                const double canonical = P.obs_fwd[j] * exp(-0.5 * variance + P.vol * w);
-                const double s = 0.0 * P.spot + 1.0 * canonical;
-                if (!isfinite(s)) bad = true;
-                const double imm = dual_intrinsic(A, s);
-                if (j + 1 == dates || policy_exercises(A, j, imm, s)) {
-                    value = imm * A.df[j];
-                    break;
-                }
+                z = as241(open_unit(lane_of(block, dim & 3u)));
+            }
+            w += A.sqrt_step[j] * z;
+            const double variance = P.vol * P.vol * P.obs_time[j];
+            const double canonical = P.obs_fwd[j] * exp(-0.5 * variance + P.vol * w);
+            const double s = 0.0 * P.spot + 1.0 * canonical;
+            if (!isfinite(s)) bad = true;
+            const double imm = dual_intrinsic(A, s);
+            if (j + 1 == dates || policy_exercises(A, j, imm, s)) {
+                values[lane + 32 * slot] = imm * A.df[j];
+                ++slot;
+                inner += 32;
+                active = slot < kDualSlots && inner < paths;
+                w = w0;
+                j = d + 1;
+                cached = 0xffffffffu;
+            } else {
+                ++j;
             }
         }
-        const uint32_t count = paths - base < 32u ? paths - base : 32u;
-        for (uint32_t l = 0; l < count; ++l) {
-            const double v = __shfl_sync(0xffffffffu, value, static_cast<int>(l));
-            if (lane == 0) neumaier_add(sum, corr, v);
+        __syncwarp();
+        if (lane == 0) {
+            const uint32_t count = paths - c0 < 32u * kDualSlots ? paths - c0 : 32u * kDualSlots;
+            for (uint32_t i = 0; i < count; ++i) neumaier_add(sum, corr, values[i]);
         }
+        __syncwarp();
     }
     bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
