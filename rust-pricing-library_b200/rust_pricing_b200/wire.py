@@ -22,10 +22,13 @@ reference's layout, with its market scaling (1 % spot Delta and Gamma, one
 volatility point Vega) and 95 % normal confidence bounds
 (crates/pricing/src/engine/risk/report.rs:255-300,454-489).
 
+`evaluate_width_ladder` evaluates a request's compact-C2 half-width ladder
+(PricingPlan::evaluate_width_ladder) on the same random coordinates.
+
 Requests outside the engine's hot path raise `UnsupportedRequest`: discrete
-dividends, the Bass local-volatility model, smoothing-width ladders,
-observations on the valuation date itself that the graph simulates, and the
-American/LSM state variables other than spot.
+dividends, the Bass local-volatility model, observations on the valuation
+date itself that the graph simulates, and the American/LSM state variables
+other than spot.
 """
 from __future__ import annotations
 
@@ -397,7 +400,7 @@ def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledR
     for key in ("delta", "vega", "smile_dynamics"):
         _get(risk, key, "risk")
     if risk.get("payoff_smoothing_width_ladder"):
-        raise UnsupportedRequest("payoff smoothing width ladders (batched bump plans)")
+        raise UnsupportedRequest("a width-ladder request is evaluated by evaluate_width_ladder")
     req_delta, req_vega = bool(risk["delta"]), bool(risk["vega"])
     gamma = risk.get("gamma")
     plan_kw.update(request_delta=req_delta, request_vega=req_vega, request_gamma=gamma is not None)
@@ -539,6 +542,57 @@ def _vega_kt_report(req: CompiledRequest, node_means, evaluated_paths: int) -> d
                                                "right_edge_sensitivity": out.right_edge_sensitivity}},
             "residual_diagnostics": {"initial_time": out.initial_time,
                                      "excluded_probability_mass": out.density_excluded}}
+
+
+def width_ladder(doc: dict) -> list:
+    """The request's compact-C2 half-width ladder (PayoffSmoothingWidthLadder::new,
+    crates/pricing/src/risk/request.rs:24-52): non-empty, positive, strictly
+    monotone (two entries: distinct)."""
+    ladder = [float(w) for w in _get(doc, "risk", "request").get("payoff_smoothing_width_ladder") or []]
+    if not ladder:
+        raise WireError("risk.payoff_smoothing_width_ladder is empty")
+    for w in ladder:
+        _positive(w, "risk.payoff_smoothing_width_ladder")
+    if len(ladder) > 2:
+        ascending = ladder[1] > ladder[0]
+        if not all((b > a) if ascending else (b < a) for a, b in zip(ladder, ladder[1:])):
+            raise WireError("risk.payoff_smoothing_width_ladder must be strictly monotone")
+    elif len(ladder) == 2 and ladder[0] == ladder[1]:
+        raise WireError("risk.payoff_smoothing_width_ladder must be strictly monotone")
+    return ladder
+
+
+def evaluate_width_ladder(doc: dict, *, reduction_block_size: int = 4096, price=None) -> dict:
+    """PricingPlan::evaluate_width_ladder (crates/pricing/src/engine/risk/pricing.rs:53-84,329-393):
+    the primary request (its own smoothing, the ladder removed) and the same
+    request at every half-width of the ladder, all on the same engine seeds and
+    therefore the same random coordinates; each entry carries its raw
+    difference from the previous entry (price, Delta, Gamma, Vega).  `price`
+    evaluates one request document (default: price_request on the GPU)."""
+    price = price or (lambda d: price_request(d, reduction_block_size=reduction_block_size))
+    ladder = width_ladder(doc)
+    base = json_copy(doc)
+    base["risk"].pop("payoff_smoothing_width_ladder", None)
+    primary = price(base)
+    entries = []
+    for half_width in ladder:
+        request = json_copy(base)
+        request["risk"]["payoff_smoothing"] = {"type": "compact_c2", "half_width": half_width}
+        result = price(request)
+        difference = None
+        if entries:
+            prev = entries[-1]["result"]
+            difference = {"price": result["value"]["value"] - prev["value"]["value"]}
+            for k in ("delta", "gamma", "vega"):
+                cur, old = result["risks"].get(k), prev["risks"].get(k)
+                difference[k] = cur["raw"]["value"] - old["raw"]["value"] if cur and old else None
+        entries.append({"half_width": half_width, "result": result, "adjacent_difference": difference})
+    return {"primary": primary, "entries": entries}
+
+
+def json_copy(doc):
+    import copy
+    return copy.deepcopy(doc)
 
 
 def price_request(doc: dict, *, reduction_block_size: int = 4096, stream: int = 0) -> dict:

@@ -131,3 +131,20 @@ def test_path_risk_over_several_scratch_chunks(engine):
     req = wire.compile_request(doc, reduction_block_size=4096)
     assert len(req.plan.observation_times) == 500
     G.assert_parity(req.plan, threads=16)
+
+
+def test_width_ladder_on_the_gpu(engine):
+    """The half-width ladder of a smoothed discrete barrier with full risk on
+    the GPU: each entry is the GPU's price of that width alone, and within
+    the parity tolerances of the oracle's ladder."""
+    doc = _request("discrete_barrier_smoothed_full_risk")
+    doc["risk"]["payoff_smoothing_width_ladder"] = [1.0, 2.0, 4.0]
+    ladder = wire.evaluate_width_ladder(doc, reduction_block_size=256)
+    plain = copy.deepcopy(doc)
+    del plain["risk"]["payoff_smoothing_width_ladder"]
+    for e in ladder["entries"]:
+        alone = copy.deepcopy(plain)
+        alone["risk"]["payoff_smoothing"] = {"type": "compact_c2", "half_width": e["half_width"]}
+        assert e["result"] == wire.price_request(alone, reduction_block_size=256)
+        G.assert_parity(wire.compile_request(alone, reduction_block_size=256).plan)
+    assert ladder["primary"] == wire.price_request(plain, reduction_block_size=256)

@@ -194,7 +194,7 @@ def test_oracle_honours_seasoned_state_and_flags():
                                                         "quote": {"type": "fixed_cash", "amount": 1.0}}]),
      wire.UnsupportedRequest),
     (lambda d: d.update(model={"type": "bass_local_volatility", "parameters": {}}), wire.UnsupportedRequest),
-    (lambda d: d["risk"].update(payoff_smoothing_width_ladder=[1.0, 2.0]), wire.UnsupportedRequest),
+    (lambda d: d["risk"].update(payoff_smoothing_width_ladder=[1.0, 2.0]), wire.UnsupportedRequest),  # ladder entry
     (lambda d: d["product"].update(expiry="2026-09-04", payment_date="2026-09-04"), wire.UnsupportedRequest),
     (lambda d: d["product"].update(type="graph"), wire.UnsupportedRequest),
     (lambda d: d.pop("engine"), wire.WireError),
@@ -206,6 +206,43 @@ def test_rejected_requests(edit, error):
     edit(doc)
     with pytest.raises(error):
         wire.compile_request(doc)
+
+
+def test_width_ladder_on_the_oracle():
+    """PricingPlan::evaluate_width_ladder: the primary (its own smoothing) and
+    one result per half-width in ladder order, each identical to pricing that
+    request alone (same seeds: the same random coordinates), with the raw
+    differences of adjacent entries."""
+    doc = _case("digital_smoothed_full_risk")
+    doc["risk"]["payoff_smoothing_width_ladder"] = [4.0, 2.0, 1.0]
+
+    def price(d):
+        out, _ = oracle_document(wire.compile_request(d, reduction_block_size=256))
+        return out
+
+    ladder = wire.evaluate_width_ladder(doc, price=price)
+    plain = copy.deepcopy(doc)
+    del plain["risk"]["payoff_smoothing_width_ladder"]
+    assert ladder["primary"] == price(plain)
+    assert [e["half_width"] for e in ladder["entries"]] == [4.0, 2.0, 1.0]
+    assert ladder["entries"][0]["adjacent_difference"] is None
+    for prev, cur in zip(ladder["entries"], ladder["entries"][1:]):
+        alone = copy.deepcopy(plain)
+        alone["risk"]["payoff_smoothing"] = {"type": "compact_c2", "half_width": cur["half_width"]}
+        assert cur["result"] == price(alone)
+        d = cur["adjacent_difference"]
+        assert d["price"] == cur["result"]["value"]["value"] - prev["result"]["value"]["value"]
+        assert d["vega"] == cur["result"]["risks"]["vega"]["raw"]["value"] - prev["result"]["risks"]["vega"]["raw"]["value"]
+    # the widths smooth the digital differently
+    assert ladder["entries"][0]["result"]["value"]["value"] != ladder["entries"][-1]["result"]["value"]["value"]
+
+
+@pytest.mark.parametrize("ladder", [[], [1.0, 1.0], [1.0, 2.0, 1.5], [-1.0]])
+def test_width_ladder_validation(ladder):
+    doc = _case("digital_smoothed_full_risk")
+    doc["risk"]["payoff_smoothing_width_ladder"] = ladder
+    with pytest.raises(wire.WireError):
+        wire.width_ladder(doc)
 
 
 def test_market_scaling_of_risks():
