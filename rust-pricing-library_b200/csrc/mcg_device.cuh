@@ -73,19 +73,22 @@ __device__ __forceinline__ double poly8(double x, double c0, double c1, double c
 }
 
 // inverse_standard_normal, random.rs:176-266, same branch structure and
-// operation order; the tail uses CUDA's log and sqrt.
-__device__ __forceinline__ double as241(double p) {
-    const double centered = p - 0.5;
-    if (fabs(centered) <= 0.425) {
-        const double a = 0.180625 - centered * centered;
-        const double num = poly8(a, 0x1.b18d91e9eef75p+1, 0x1.0a4888b1a436ep+7, 0x1.ece5d2213c0ccp+10,
-                                 0x1.ad1d8cd4ee71dp+13, 0x1.66c3e869b752ap+15, 0x1.06c1c55b78f20p+16,
-                                 0x1.052d26b2e4604p+15, 0x1.39a296f7d925ep+11);
-        const double den = poly8(a, 1.0, 0x1.5281b386e1ab5p+5, 0x1.5797efdc8b3f7p+9,
-                                 0x1.512322e75c89fp+12, 0x1.4b772d5d65266p+14, 0x1.3317caa64f4bep+15,
-                                 0x1.c0e457cb1ae76p+14, 0x1.46a7eca984b6ap+12);
-        return centered * num / den;
-    }
+// operation order; the tail uses CUDA's log and sqrt.  The two branches are
+// also callable on their own (the batched normals of the path kernels take
+// the central branch for every lane and the tail only for the lanes that
+// need it).
+__device__ __forceinline__ double as241_central(double centered) {
+    const double a = 0.180625 - centered * centered;
+    const double num = poly8(a, 0x1.b18d91e9eef75p+1, 0x1.0a4888b1a436ep+7, 0x1.ece5d2213c0ccp+10,
+                             0x1.ad1d8cd4ee71dp+13, 0x1.66c3e869b752ap+15, 0x1.06c1c55b78f20p+16,
+                             0x1.052d26b2e4604p+15, 0x1.39a296f7d925ep+11);
+    const double den = poly8(a, 1.0, 0x1.5281b386e1ab5p+5, 0x1.5797efdc8b3f7p+9,
+                             0x1.512322e75c89fp+12, 0x1.4b772d5d65266p+14, 0x1.3317caa64f4bep+15,
+                             0x1.c0e457cb1ae76p+14, 0x1.46a7eca984b6ap+12);
+    return centered * num / den;
+}
+
+__device__ __forceinline__ double as241_tail(double p, double centered) {
     const double tail = centered < 0.0 ? p : 1.0 - p;
     const double r = sqrt(-log(tail));
     double m;
@@ -107,6 +110,12 @@ __device__ __forceinline__ double as241(double p) {
                   0x1.269bff1f8c190p-49);
     }
     return centered < 0.0 ? -m : m;
+}
+
+__device__ __forceinline__ double as241(double p) {
+    const double centered = p - 0.5;
+    if (fabs(centered) <= 0.425) return as241_central(centered);
+    return as241_tail(p, centered);
 }
 
 // Single-precision AS241 for the FP32 bulk path (same branches, FP32 rounding).

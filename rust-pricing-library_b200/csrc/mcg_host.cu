@@ -361,6 +361,7 @@ struct mcg_plan {
     std::vector<ProductParams> products;
     // device storage
     DeviceArray<Op> ops;
+    DeviceArray<uint32_t> z_ranks;
     DeviceArray<double> node_time, dt, sqrt_dt, inv_sqrt_dt, time_weight, fwd, ratio, obs_time,
         obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, grid_vol2, weights;
     DeviceArray<int32_t> obs_of_node, time_cell;
@@ -383,6 +384,7 @@ struct mcg_plan {
         ratio_f.release();
         step_f.release();
         ops.release();
+        z_ranks.release();
         node_time.release();
         dt.release();
         sqrt_dt.release();
@@ -761,6 +763,13 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         MCG_CUDA(plan.ops.upload(ops));
         P.ops = plan.ops.ptr;
         P.op_count = static_cast<uint32_t>(ops.size());
+        std::vector<uint32_t> ranks;
+        for (const Op& op : ops)
+            if (op.kind == kOpTerminal || op.kind == kOpInterior || op.kind == kOpStepDirect)
+                ranks.push_back(static_cast<uint32_t>(op.rank));
+        MCG_CUDA(plan.z_ranks.upload(ranks));
+        P.z_ranks = plan.z_ranks.ptr;
+        P.z_count = static_cast<uint32_t>(ranks.size());
         P.slot_count = slots;
         const size_t smem = (gv.size() + 2 * gx.size()) * sizeof(double) +
                             static_cast<size_t>(slots) * kThreads * sizeof(double) +

@@ -30,6 +30,8 @@ __global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (CB == 0 ? 7 :
     double* s_idx = s_x + nx;                            // reciprocal cell widths
     double* s_w = s_idx + nx;                            // bridge slots [slot][thread]
     Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(P.slot_count) * kThreads);
+    double* s_z = reinterpret_cast<double*>(s_red + 4 * kComponents);       // batched normals [k][thread]
+    uint16_t* s_zlist = reinterpret_cast<uint16_t*>(s_z + kZBatch * kThreads);  // tail lists, per warp
     for (int i = threadIdx.x; i < nx; i += kThreads) {
         s_x[i] = P.grid_x[i];
         s_idx[i] = i + 1 < nx ? 1.0 / (P.grid_x[i + 1] - P.grid_x[i]) : 0.0;
@@ -41,7 +43,7 @@ __global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (CB == 0 ? 7 :
     const bool valid = point < unit_begin + (detail ? 1 : P.units) && point < P.units;
     StatRecord* tile_out = partials + (static_cast<size_t>(scramble) * gridDim.x + blockIdx.x) * P.product_count * kComponents;
     lv_tile<E, NP, RQ, CB>(P, g, s_w, s_red, scramble, point, valid, tile_out, mask, err, detail,
-                           (unit_begin & 31u) == 0);
+                           (unit_begin & 31u) == 0, s_z, s_zlist);
 }
 
 
@@ -162,7 +164,8 @@ cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t un
     const int np = static_cast<int>(P.product_count);
     const size_t smem = (2 * static_cast<size_t>(P.nx)) * sizeof(double) +
                         static_cast<size_t>(P.slot_count) * kThreads * sizeof(double) +
-                        4 * kComponents * sizeof(Stat);
+                        4 * kComponents * sizeof(Stat) + kZBatch * kThreads * sizeof(double) +
+                        (kThreads / 32) * 32 * kZBatch * sizeof(uint16_t);
     const dim3 grid(static_cast<unsigned>((units + kThreads - 1) / kThreads), scrambles);
     auto go = [&](auto kernel) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -39,10 +39,49 @@ __device__ __forceinline__ double ev_sign(int e) {
 // on whether any product is a continuous barrier, so the code and state of
 // the other case are compiled out; -1 decides both from the plan at run
 // time.  The arithmetic is the same either way.
+// Batched normals: kZBatch normals of the program per thread at a time, in
+// s_z[k][thread].  The warp forms the uniforms, takes AS241's central branch
+// for every lane, and evaluates the tail branch only for the lanes that need
+// it, 32 at a time from a compacted list (s_zlist, 32 * kZBatch entries per
+// warp); the values are those of as241 bit for bit, without a warp executing
+// the tail branch for each normal that one of its lanes sends there.
+constexpr int kZBatch = 8;
+
+__device__ __forceinline__ void fill_normals(const DevicePlan& P, NormalSource& ns, bool wsob, uint32_t first,
+                                             uint32_t count, double* s_z, uint16_t* s_zlist) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    uint16_t* list = s_zlist + warp * (32u * kZBatch);
+    uint32_t tails = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t rank = __ldg(P.z_ranks + first + k);
+        const double p = open_unit(wsob ? ns.word_warp(rank) : ns.word(rank));
+        const double c = p - 0.5;
+        const bool tail = !(fabs(c) <= 0.425);
+        const double central = as241_central(c);
+        s_z[k * kThreads + threadIdx.x] = tail ? p : central;
+        const unsigned m = __ballot_sync(0xffffffffu, tail);
+        if (tail) list[tails + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(k * 32u + lane);
+        tails += static_cast<uint32_t>(__popc(m));
+    }
+    __syncwarp();
+    for (uint32_t b = 0; b < tails; b += 32u) {
+        const uint32_t i = b + lane;
+        if (i < tails) {
+            const uint32_t idx = list[i];
+            double* at = s_z + (idx >> 5) * kThreads + warp * 32u + (idx & 31u);
+            const double p = *at;
+            *at = as241_tail(p, p - 0.5);
+        }
+    }
+    __syncwarp();
+}
+
 template <int E, int NP, int RQ = -1, int CB = -1>
 __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, double* s_w, Stat* s_red,
                                         uint32_t scramble, uint64_t point, bool valid, StatRecord* tile_out,
-                                        uint32_t mask, ErrorWord* err, int detail, bool warp_sobol = false) {
+                                        uint32_t mask, ErrorWord* err, int detail, bool warp_sobol = false,
+                                        double* s_z = nullptr, uint16_t* s_zlist = nullptr) {
     const uint64_t unit = valid ? point : 0;
 
     NormalSource ns;
@@ -86,6 +125,20 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
     }
     double* w = s_w + threadIdx.x;
     const uint32_t steps = P.steps;
+    // The program's normals in order: from the batch in shared memory, or
+    // one at a time (s_z null).
+    uint32_t zi = 0, zbase = 0, zend = 0;
+    auto next_normal = [&](uint32_t rank) -> double {
+        if (s_z == nullptr) return wsob ? ns.normal_warp(rank) : ns.normal(rank);
+        if (zi == zend) {
+            zbase = zi;
+            const uint32_t n = P.z_count - zi < static_cast<uint32_t>(kZBatch) ? P.z_count - zi
+                                                                              : static_cast<uint32_t>(kZBatch);
+            fill_normals(P, ns, wsob, zi, n, s_z, s_zlist);
+            zend = zi + n;
+        }
+        return s_z[(zi++ - zbase) * kThreads + threadIdx.x];
+    };
     for (uint32_t oi = 0; oi < P.op_count; ++oi) {
         const Op op = P.ops[oi];
         if (op.kind == kOpZero) {
@@ -93,11 +146,11 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             continue;
         }
         if (op.kind == kOpTerminal) {
-            w[op.out * kThreads] = op.sd * (wsob ? ns.normal_warp(op.rank) : ns.normal(op.rank));
+            w[op.out * kThreads] = op.sd * next_normal(op.rank);
             continue;
         }
         if (op.kind == kOpInterior) {
-            const double z = wsob ? ns.normal_warp(op.rank) : ns.normal(op.rank);
+            const double z = next_normal(op.rank);
             w[op.out * kThreads] =
                 op.wl * w[op.left * kThreads] + op.wr * w[op.right * kThreads] + op.sd * z;
             continue;
@@ -108,7 +161,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
         if (op.kind == kOpStep)
             shock = (w[op.right * kThreads] - w[op.left * kThreads]) * st.inv_sqrt_dt;
         else
-            shock = wsob ? ns.normal_warp(op.rank) : ns.normal(op.rank);
+            shock = next_normal(op.rank);
         const int tc = st.time_cell;
         const double tw = st.time_weight;
         const double dt = st.dt;

@@ -76,6 +76,8 @@ struct DevicePlan {
     // program
     const Op* ops;
     uint32_t op_count;
+    const uint32_t* z_ranks;  // local volatility: the normal ranks the program consumes, in order
+    uint32_t z_count;
     uint32_t slot_count;
 
     // per-step constants (steps entries unless noted)
