@@ -12,7 +12,8 @@ Workload (one "step" = one evaluation of the whole workload):
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
 Weak scaling: rank r evaluates scrambles [16 r, 16 r + 16) of one plan, so each
-GPU's work is fixed; the per-scramble means are gathered to rank 0.
+GPU's work is fixed; after the timed region each rank's price statistics are
+gathered to rank 0 and merged (rust_pricing_b200/shards.py).
 `--impl reference` times the CPU restatement of the reference's executor (the
 oracle) on this host's cores on a bounded sample of the same workload.
 """
@@ -482,7 +483,14 @@ def main():
         t = torch.tensor([total_ms], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-        # gather the per-scramble price means (the estimator's replicate values)
+    # Prices of the whole job: every rank's scramble-shard statistics merged on
+    # rank 0 in rank order (one rank: the plan's own estimates).
+    if world > 1:
+        from rust_pricing_b200 import shards
+        merged = shards.gather_prices(buf, len(spec.products), rank, world)
+    else:
+        merged = [{"value": buf.products[k].price.value, "standard_error": buf.products[k].price.standard_error}
+                  for k in range(len(spec.products))]
     ms_per_step = total_ms / args.steps
     value = world * path_steps_rank / (ms_per_step * 1e-3)
 
@@ -529,10 +537,10 @@ def main():
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
-        "prices": [buf.products[k].price.value for k in range(len(spec.products))],
-        "price_standard_errors": [buf.products[k].price.standard_error for k in range(len(spec.products))],
-        "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, buf.products[k].price.standard_error,
-                                                buf.products[k].price.value) for k in range(len(spec.products))],
+        "prices": [m["value"] for m in merged] if merged else None,
+        "price_standard_errors": [m["standard_error"] for m in merged] if merged else None,
+        "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, m["standard_error"], m["value"])
+                                     for m in merged] if merged else None,
     }
     wanted = {"early_exercise", "book", "f32", "adjoint", "path_risk", "dual"} if args.secondary == "all" else (
         set() if args.secondary == "none" else set(args.secondary.split(",")))
