@@ -20,7 +20,9 @@ plan the way SimulationPlan::compile does
 `result_document` writes the `pricing_result` value and risk estimates in the
 reference's layout, with its market scaling (1 % spot Delta and Gamma, one
 volatility point Vega) and 95 % normal confidence bounds
-(crates/pricing/src/engine/risk/report.rs:255-300,454-489).
+(crates/pricing/src/engine/risk/report.rs:255-300,454-489), and the replay
+block with the request's BLAKE3 fingerprint over its canonical encoding
+(crates/pricing/src/wire.rs:4144-4212).
 
 `evaluate_width_ladder` evaluates a request's compact-C2 half-width ladder
 (PricingPlan::evaluate_width_ladder) on the same random coordinates.
@@ -464,6 +466,84 @@ def _lsm(cfg: dict, plan: PlanSpec) -> LsmSpec:
                    max_matrix_elements=int(_get(cfg, "max_matrix_elements", "lsm")))
 
 
+# ------------------------------------------------------------ fingerprint
+
+# Request fields the schema types as integers; every other number is an f64.
+_INTEGER_FIELDS = frozenset((
+    "schema_version", "underlying_id", "currency_id", "curve_id", "event_id", "master_seed",
+    "master_scramble_seed", "independent_sampling_units", "points_per_scramble", "scramble_count",
+    "feature_count", "max_degree", "max_matrix_elements", "checkpoint_interval", "aad_tile_capacity", "shape"))
+
+
+def _canonical(value, key=None):
+    """The request as the reference re-serialises it (serde_json::Value):
+    object keys sorted, integer-typed fields as integers, other numbers as f64."""
+    if isinstance(value, dict):
+        return {k: _canonical(v, k) for k, v in value.items()}
+    if isinstance(value, list):
+        return [_canonical(v, key) for v in value]
+    if isinstance(value, bool) or value is None or isinstance(value, str):
+        return value
+    if isinstance(value, (int, float)):
+        return int(value) if key in _INTEGER_FIELDS else float(value)
+    raise WireError(f"unsupported JSON value {value!r}")
+
+
+def _encode(value, out: bytearray) -> None:
+    """encode_value (crates/pricing/src/wire.rs:4165-4212): tag, big-endian
+    u64 payload length, payload; u64/i64/f64 numbers big-endian, strings as
+    UTF-8, arrays and objects with a u64 count (object entries in key order)."""
+    import struct
+    if value is None:
+        tag, payload = 0, b""
+    elif isinstance(value, bool):
+        tag, payload = 1, bytes([int(value)])
+    elif isinstance(value, int):
+        tag, payload = (2, struct.pack(">Q", value)) if value >= 0 else (3, struct.pack(">q", value))
+    elif isinstance(value, float):
+        if not math.isfinite(value):
+            raise WireError("non-finite JSON number")
+        tag, payload = 4, struct.pack(">d", value)
+    elif isinstance(value, str):
+        tag, payload = 5, value.encode("utf-8")
+    elif isinstance(value, list):
+        body = bytearray(struct.pack(">Q", len(value)))
+        for v in value:
+            _encode(v, body)
+        tag, payload = 6, bytes(body)
+    else:
+        body = bytearray(struct.pack(">Q", len(value)))
+        for k in sorted(value):
+            _encode(k, body)
+            _encode(value[k], body)
+        tag, payload = 7, bytes(body)
+    out.append(tag)
+    out += struct.pack(">Q", len(payload))
+    out += payload
+
+
+def request_fingerprint(doc: dict) -> str:
+    """fingerprint_request (wire.rs:4144-4163): BLAKE3 of "pricing/request\0",
+    the schema version as a big-endian u32 and the canonical encoding."""
+    import struct
+    from .blake3 import blake3
+    body = bytearray(b"pricing/request\0" + struct.pack(">I", SCHEMA_VERSION))
+    _encode(_canonical(doc), body)
+    return "blake3-256:" + blake3(bytes(body)).hex()
+
+
+def replay_block(doc: dict) -> dict:
+    """The result's replay section: this engine's version and platform, the
+    request fingerprint, and an identity migration (v3 requests only)."""
+    import platform
+    from . import __version__
+    fp = request_fingerprint(doc)
+    return {"library_version": __version__, "platform": f"{platform.system().lower()}-{platform.machine()}-b200",
+            "request_fingerprint": fp, "schema_version": SCHEMA_VERSION,
+            "migration": {"current_schema_version": SCHEMA_VERSION, "original_schema_version": SCHEMA_VERSION,
+                          "migration_ids": [], "pre_migration_fingerprint": fp, "post_migration_fingerprint": fp}}
+
+
 # ------------------------------------------------------------------ result
 
 def _estimate(e, estimator: str, scale: float = 1.0) -> dict:
@@ -490,7 +570,7 @@ def _risk(e, estimator: str, scale: float, raw_unit: str, scaled_unit: str) -> d
 def result_document(req: CompiledRequest, price, delta=None, gamma=None, vega=None,
                     sampling_variance: Optional[float] = None, estimator_variance: Optional[float] = None,
                     evaluated_paths: Optional[int] = None, vega_kt: Optional[dict] = None,
-                    warnings: Optional[list] = None) -> dict:
+                    warnings: Optional[list] = None, request: Optional[dict] = None) -> dict:
     """A `pricing_result` document (schemas/v3/pricing_result.schema.json) of
     the engine's estimates: value, risks with raw and market-scaled values
     (report.rs:255-300), diagnostics and the Monte Carlo variances."""
@@ -512,6 +592,8 @@ def result_document(req: CompiledRequest, price, delta=None, gamma=None, vega=No
         doc["monte_carlo"] = {"sampling_variance": sampling_variance, "estimator_variance": estimator_variance,
                               "independent_sampling_units": req.independent_units,
                               "evaluated_paths": str(evaluated_paths)}
+    if request is not None:
+        doc["replay"] = replay_block(request)
     return doc
 
 
@@ -603,7 +685,7 @@ def price_request(doc: dict, *, reduction_block_size: int = 4096, stream: int = 
         buf = N.lsm_price(req.plan, req.lsm, stream=stream)
         r = buf.result
         return result_document(req, r.price, r.delta, r.gamma, r.vega, r.sampling_variance,
-                               r.estimator_variance, r.valuation_paths)
+                               r.estimator_variance, r.valuation_paths, request=doc)
     with N.Plan(req.plan) as plan:
         buf = plan.evaluate(stream)
     p = buf.products[0]
@@ -612,4 +694,4 @@ def price_request(doc: dict, *, reduction_block_size: int = 4096, stream: int = 
     if req.vega_kt is not None:
         kt = _vega_kt_report(req, [e.value for e in buf.node_estimates], r.evaluated_paths)
     return result_document(req, p.price, p.delta, p.gamma, p.vega, p.sampling_variance, p.estimator_variance,
-                           r.evaluated_paths, kt)
+                           r.evaluated_paths, kt, request=doc)

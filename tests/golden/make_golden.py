@@ -174,6 +174,7 @@ def path_dependence_replay():
                 "evaluated_paths": int(ex["evaluated_paths"]),
                 "independent_sampling_units": ex["independent_sampling_units"],
                 "risk_methods": ex["risk_methods"],
+                "request_fingerprint": res["replay"]["request_fingerprint"],
                 "bump_value_bits": {k: v["bump_and_revalue"]["value_bits"]
                                     for k, v in (ex.get("risk_validation") or {}).items() if v},
             }

@@ -148,3 +148,24 @@ def test_width_ladder_on_the_gpu(engine):
         assert e["result"] == wire.price_request(alone, reduction_block_size=256)
         G.assert_parity(wire.compile_request(alone, reduction_block_size=256).plan)
     assert ladder["primary"] == wire.price_request(plain, reduction_block_size=256)
+
+
+def test_facade_plan_on_the_gpu(engine):
+    """PricingPlan.compile/evaluate (the reference's Python facade): the same
+    document as price_request, a replay block with the reference's request
+    fingerprint, and a compiled plan that evaluates again to the same bits."""
+    import json
+    from rust_pricing_b200 import PricingPlan, PricingRequest
+    for case in WC.path_dependence_cases()[3:5]:
+        req = PricingRequest.from_json(json.dumps(case["request"]))
+        plan = PricingPlan.compile(req, worker_threads=1, reduction_block_size=case["reduction_block_size"])
+        first, second = plan.evaluate(), plan.evaluate()
+        assert first.document == second.document
+        assert first.document == wire.price_request(case["request"], reduction_block_size=case["reduction_block_size"])
+        assert first.document["replay"]["request_fingerprint"] == case["expected"]["windows-x86_64"]["request_fingerprint"]
+        WC.assert_matches_fixture(first.document, case, rel=1e-12, se_rel=1e-9, price_bits=False)
+        plan.close()
+    lsm = LC.cases()[0]
+    plan = PricingPlan.compile(PricingRequest(lsm["request"]), worker_threads=1,
+                               reduction_block_size=lsm["reduction_block_size"])
+    assert abs(plan.evaluate().value["value"] - lsm["expected"]["value"]["value"]) <= 1e-12 * lsm["expected"]["value"]["value"]

@@ -262,3 +262,35 @@ def test_market_scaling_of_risks():
         assert doc["risks"][k]["market_scaled"]["standard_error"] == e["risks"][k]["market_scaled"]["standard_error"]
         assert doc["risks"][k]["market_scaled"]["confidence_lower"] == e["risks"][k]["market_scaled"]["confidence_lower"]
     assert doc["value"]["estimator"] == {"type": "pseudo_monte_carlo"}
+
+
+def test_request_fingerprints_match_the_reference():
+    """fingerprint_request of every replay request equals the fixture's
+    request_fingerprint (BLAKE3 over the canonical encoding)."""
+    import json as _json
+    from rust_pricing_b200.blake3 import blake3
+    assert blake3(b"").hex() == "af1349b9f5f9a1a6a0404dea36dcc9499bcb25c9adc112b7cc9a93cae41f3262"
+    assert blake3(b"abc").hex() == "6437b3ac38465133ffb63b75273a8db548c558465d79db03fd359c6cd5bd9d85"
+    for case in WC.path_dependence_cases():
+        assert wire.request_fingerprint(case["request"]) == case["expected"]["windows-x86_64"]["request_fingerprint"]
+    # an integer written for a float field canonicalises to the same request
+    doc = copy.deepcopy(WC.path_dependence_cases()[0]["request"])
+    want = wire.request_fingerprint(doc)
+    doc["product"]["strike"] = 100
+    assert wire.request_fingerprint(doc) == want
+    assert _json.loads(_json.dumps(doc))  # plain JSON
+
+
+def test_facade_compile_and_validation():
+    from rust_pricing_b200 import PricingPlan, PricingRequest, ValidationError
+    case = WC.path_dependence_cases()[4]
+    req = PricingRequest.from_json(__import__("json").dumps(case["request"]))
+    plan = PricingPlan.compile(req, worker_threads=2, reduction_block_size=256)
+    assert plan.compiled.plan.reduction_block_size == 256
+    assert plan.request_fingerprint() == case["expected"]["windows-x86_64"]["request_fingerprint"]
+    with pytest.raises(ValidationError):
+        PricingRequest.from_json("[1, 2")
+    bad = copy.deepcopy(case["request"])
+    bad["market"]["discrete_dividends"] = [{"event_id": 1, "ex_time": 0.5, "quote": {"type": "fixed_cash", "amount": 1.0}}]
+    with pytest.raises(ValidationError):
+        PricingPlan.compile(PricingRequest(bad), worker_threads=1)
