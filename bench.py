@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--points", type=int, default=POINTS)
     ap.add_argument("--scrambles", type=int, default=SCRAMBLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
                     help="path arithmetic of the timed workload (f32: FP32 path bulk)")
     ap.add_argument("--path-risk-units", type=int, default=1 << 20,
