@@ -33,6 +33,9 @@ int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vect
               uint64_t& path_count, mcg_error_record& err, std::vector<double>* brownians);
 int lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
              mcg_dual_result* out, int threads);
+int lsm_scaling_api(const double* values, size_t n, double out[4]);
+int lsm_cpqr_api(const double* matrix, size_t rows, size_t cols, const double* target, double abs_tol,
+                 double rel_tol, uint32_t* pivot, uint32_t* rank, double* coefficients, double* rss);
 int lsm_fit_api(const double* spots, const double* immediate, const double* targets, size_t rows,
                 const mcg_lsm_desc* lsm, mcg_lsm_date_model* out);
 }  // namespace oracle
@@ -152,6 +155,15 @@ int64_t oracle_lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads
 int oracle_lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
                     mcg_dual_result* out, int threads) {
     return oracle::lsm_dual(desc, lsm, dual, out, threads);
+}
+
+int oracle_lsm_scaling(const double* values, uint64_t n, double* out) {
+    return oracle::lsm_scaling_api(values, n, out);
+}
+
+int oracle_lsm_cpqr(const double* matrix, uint64_t rows, uint32_t cols, const double* target, double abs_tol,
+                    double rel_tol, uint32_t* pivot, uint32_t* rank, double* coefficients, double* rss) {
+    return oracle::lsm_cpqr_api(matrix, rows, cols, target, abs_tol, rel_tol, pivot, rank, coefficients, rss);
 }
 
 int oracle_lsm_fit(const double* spots, const double* immediate, const double* targets,

@@ -639,6 +639,34 @@ int lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_
 
 const char* lsm_last_error() { return g_lsm_error.c_str(); }
 
+// FeatureScaling::fit of given values: out = mean, population variance,
+// scale, zero-scale threshold; the return value is the inactive flag.
+int lsm_scaling_api(const double* values, size_t n, double out[4]) {
+    const Scaling s = fit_scaling(std::vector<double>(values, values + n));
+    out[0] = s.mean;
+    out[1] = s.variance;
+    out[2] = s.scale;
+    out[3] = s.threshold;
+    return s.inactive ? 1 : 0;
+}
+
+// fit_cpqr of a row-major design matrix: pivot order, rank, coefficients in
+// the original column order and the residual sum of squares.
+int lsm_cpqr_api(const double* matrix, size_t rows, size_t cols, const double* target, double abs_tol,
+                 double rel_tol, uint32_t* pivot, uint32_t* rank, double* coefficients, double* rss) {
+    Cpqr fit;
+    if (!fit_cpqr(std::vector<double>(matrix, matrix + rows * cols), rows, cols,
+                  std::vector<double>(target, target + rows), abs_tol, rel_tol, fit))
+        return MCG_ERR_LSM;
+    for (size_t c = 0; c < cols; ++c) {
+        pivot[c] = static_cast<uint32_t>(fit.pivot[c]);
+        coefficients[c] = fit.coefficients[c];
+    }
+    *rank = static_cast<uint32_t>(fit.rank);
+    *rss = fit.rss;
+    return MCG_OK;
+}
+
 int lsm_fit_api(const double* spots, const double* immediate, const double* targets, size_t rows,
                 const mcg_lsm_desc* lsm, mcg_lsm_date_model* out) {
     g_lsm_error.clear();

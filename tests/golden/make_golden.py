@@ -24,6 +24,8 @@ which the wire-format tests compile.
   lookback requests (verbatim v3 request documents, Black--Scholes, pseudo and
   RQMC, exact and compact-C2 smoothed, price-only and full risk) with both
   platforms' estimates, variance bits and bump-and-revalue validation bits.
+* early_exercise_cases.json -- fixtures/early-exercise/reference-cases-v0.1.json: the
+  decision, monomial-basis, feature-scaling and CPQR cases (decimal strings).
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
   the American put requests (pseudo and RQMC, training and valuation engines,
   LSM configuration) with the fitted decision models, exercise counts,
@@ -183,6 +185,14 @@ def path_dependence_replay():
               open(os.path.join(OUT, "replay_path_dependence.json"), "w"), indent=1)
 
 
+def early_exercise_cases():
+    src = os.path.join(REF, "fixtures/early-exercise/reference-cases-v0.1.json")
+    d = json.load(open(src))
+    keep = {k: d[k] for k in ("decision_cases", "basis_cases", "scaling_cases", "qr_cases")}
+    keep["source"] = "fixtures/early-exercise/reference-cases-v0.1.json"
+    json.dump(keep, open(os.path.join(OUT, "early_exercise_cases.json"), "w"), indent=1)
+
+
 def surfaces():
     src = os.path.join(REF, "fixtures/local-vol/reference-cases-v0.1.json")
     d = json.load(open(src))
@@ -282,5 +292,6 @@ if __name__ == "__main__":
     early_exercise()
     local_volatility()
     path_dependence_replay()
+    early_exercise_cases()
     surfaces()
     print("golden fixtures written to", OUT)
