@@ -34,6 +34,10 @@ int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vect
 int lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
              mcg_dual_result* out, int threads);
 int lsm_scaling_api(const double* values, size_t n, double out[4]);
+int lv_step_adjoints_api(const double* times, uint32_t n_times, const double* forwards, const double* grid_t,
+                         uint32_t nt, const double* grid_x, uint32_t nx, const double* values, double initial,
+                         const double* shocks, const double* state_seeds, double* states_out,
+                         double* grid_adj_out);
 int lsm_cpqr_api(const double* matrix, size_t rows, size_t cols, const double* target, double abs_tol,
                  double rel_tol, uint32_t* pivot, uint32_t* rank, double* coefficients, double* rss);
 int lsm_fit_api(const double* spots, const double* immediate, const double* targets, size_t rows,
@@ -155,6 +159,14 @@ int64_t oracle_lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads
 int oracle_lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
                     mcg_dual_result* out, int threads) {
     return oracle::lsm_dual(desc, lsm, dual, out, threads);
+}
+
+int oracle_lv_step_adjoints(const double* times, uint32_t n_times, const double* forwards, const double* grid_t,
+                            uint32_t nt, const double* grid_x, uint32_t nx, const double* values, double initial,
+                            const double* shocks, const double* state_seeds, double* states_out,
+                            double* grid_adj_out) {
+    return oracle::lv_step_adjoints_api(times, n_times, forwards, grid_t, nt, grid_x, nx, values, initial, shocks,
+                                        state_seeds, states_out, grid_adj_out);
 }
 
 int oracle_lsm_scaling(const double* values, uint64_t n, double* out) {

@@ -1460,6 +1460,34 @@ int unit_values_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit,
     return MCG_OK;
 }
 
+// One Log-Euler path on given nodes, forwards, grid and shocks, and its
+// reverse sweep for given dPayoff/dS_k seeds (the equation-(10) step
+// adjoints of the reference's local-vol fixtures): the path's states and the
+// grid-value adjoints.
+int lv_step_adjoints_api(const double* times, uint32_t n_times, const double* forwards, const double* grid_t,
+                         uint32_t nt, const double* grid_x, uint32_t nx, const double* values, double initial,
+                         const double* shocks, const double* state_seeds, double* states_out,
+                         double* grid_adj_out) {
+    Plan p;
+    p.nodes.assign(times, times + n_times);
+    p.fwd[0].assign(forwards, forwards + n_times);
+    p.bump_spot[0] = initial;
+    p.grid.t.assign(grid_t, grid_t + nt);
+    p.grid.x.assign(grid_x, grid_x + nx);
+    p.grid.v.assign(values, values + static_cast<size_t>(nt) * nx);
+    p.grid.floor = 1e-8;
+    p.grid.cap = 4.0;
+    LvPath path;
+    Failure f;
+    if (!lv_evolve(p, 0, shocks, path, f)) return f.code;
+    std::vector<double> seeds(state_seeds, state_seeds + n_times), var_seeds(n_times, 0.0), grid_adj;
+    double initial_adjoint = 0.0, x_sum = 0.0;
+    if (!lv_reverse(p, 0, path, seeds, var_seeds, grid_adj, initial_adjoint, x_sum, f)) return f.code;
+    for (uint32_t i = 0; i < n_times; ++i) states_out[i] = path.state[i];
+    for (size_t i = 0; i < grid_adj.size(); ++i) grid_adj_out[i] = grid_adj[i];
+    return MCG_OK;
+}
+
 int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacity,
                   uint32_t* count) {
     Plan p;

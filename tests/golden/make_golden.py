@@ -24,6 +24,9 @@ which the wire-format tests compile.
   lookback requests (verbatim v3 request documents, Black--Scholes, pseudo and
   RQMC, exact and compact-C2 smoothed, price-only and full risk) with both
   platforms' estimates, variance bits and bump-and-revalue validation bits.
+* lv_step_adjoints.json     -- fixtures/local-vol/step-adjoints-v0.1.json: one Log-Euler path per
+  case (given nodes, forwards, 3 x 3 grid, shocks) with a quadratic payoff, its
+  states and 100-digit bump references of the grid-value derivatives.
 * early_exercise_cases.json -- fixtures/early-exercise/reference-cases-v0.1.json: the
   decision, monomial-basis, feature-scaling and CPQR cases (decimal strings).
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
@@ -185,6 +188,13 @@ def path_dependence_replay():
               open(os.path.join(OUT, "replay_path_dependence.json"), "w"), indent=1)
 
 
+def step_adjoints():
+    src = os.path.join(REF, "fixtures/local-vol/step-adjoints-v0.1.json")
+    d = json.load(open(src))
+    d["source"] = "fixtures/local-vol/step-adjoints-v0.1.json"
+    json.dump(d, open(os.path.join(OUT, "lv_step_adjoints.json"), "w"), indent=1)
+
+
 def early_exercise_cases():
     src = os.path.join(REF, "fixtures/early-exercise/reference-cases-v0.1.json")
     d = json.load(open(src))
@@ -293,5 +303,6 @@ if __name__ == "__main__":
     local_volatility()
     path_dependence_replay()
     early_exercise_cases()
+    step_adjoints()
     surfaces()
     print("golden fixtures written to", OUT)
