@@ -516,9 +516,16 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
     if (!(d->spot > 0.0) || !std::isfinite(d->spot)) return fail(MCG_ERR_INVALID_ARGUMENT, "spot");
     if (d->observation_count == 0 || !d->observation_times)
         return fail(MCG_ERR_INVALID_ARGUMENT, "observation_times");
+    // A Black-Scholes path may observe the valuation date itself (time 0: a
+    // zero-length step that still takes its normal, as the reference's
+    // path_observations_from_normals does); every other plan starts after it.
+    bool time_zero_ok = d->model == MCG_MODEL_BLACK_SCHOLES && d->observation_count > 1;
+    for (uint32_t i = 0; i < d->product_count && d->products; ++i)
+        time_zero_ok &= d->products[i].kind != MCG_PRODUCT_AMERICAN;
     for (uint32_t i = 0; i < d->observation_count; ++i) {
         const double t = d->observation_times[i];
-        if (!std::isfinite(t) || t <= 0.0 || (i && !(t > d->observation_times[i - 1])))
+        const bool zero_first = i == 0 && t == 0.0 && time_zero_ok;
+        if (!std::isfinite(t) || (t <= 0.0 && !zero_first) || (i && !(t > d->observation_times[i - 1])))
             return fail(MCG_ERR_INVALID_ARGUMENT, "observation_times must be positive and increasing");
     }
     if (d->sampling_units == 0) return fail(MCG_ERR_INVALID_ARGUMENT, "sampling_units");

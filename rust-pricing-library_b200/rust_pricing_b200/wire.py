@@ -28,9 +28,9 @@ block with the request's BLAKE3 fingerprint over its canonical encoding
 (PricingPlan::evaluate_width_ladder) on the same random coordinates.
 
 Requests outside the engine's hot path raise `UnsupportedRequest`: discrete
-dividends, the Bass local-volatility model, observations on the valuation
-date itself that the graph simulates, and the American/LSM state variables
-other than spot.
+dividends, the Bass local-volatility model, simulated observations on the
+valuation date outside multi-date Black--Scholes paths, and the
+American/LSM state variables other than spot.
 """
 from __future__ import annotations
 
@@ -137,12 +137,10 @@ class _Product:
 
 
 def _simulated(dates, valuation, what: str):
-    """Dates the graph simulates must lie after the valuation date: an
-    observation at time zero consumes a normal in the reference's path
-    generator, which this engine's plans do not model."""
-    for d in dates:
-        if d == valuation:
-            raise UnsupportedRequest(f"{what} on the valuation date is simulated at time zero")
+    """The distinct simulated dates in order.  A date equal to the valuation
+    date is a time-zero observation: a zero-length step that still takes its
+    normal in the reference's path generator; compile_request admits it for
+    Black--Scholes paths only."""
     return sorted(set(dates))
 
 
@@ -397,6 +395,10 @@ def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledR
                    reduction_block_size=reduction_block_size, payment_time=payment_time, **engine)
     warnings: list = []
     basis = _model(doc, plan_kw, times[-1], warnings)
+    if times[0] == 0.0 and (plan_kw["model"] != A.MODEL_BLACK_SCHOLES or ptype == "american_vanilla"
+                            or len(times) == 1):
+        raise UnsupportedRequest("an observation on the valuation date is simulated at time zero only on "
+                                 "multi-date Black-Scholes paths")
 
     risk = _get(doc, "risk", "request")
     for key in ("delta", "vega", "smile_dynamics"):

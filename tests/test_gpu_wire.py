@@ -169,3 +169,22 @@ def test_facade_plan_on_the_gpu(engine):
     plan = PricingPlan.compile(PricingRequest(lsm["request"]), worker_threads=1,
                                reduction_block_size=lsm["reduction_block_size"])
     assert abs(plan.evaluate().value["value"] - lsm["expected"]["value"]["value"]) <= 1e-12 * lsm["expected"]["value"]["value"]
+
+
+def test_time_zero_observations_against_the_oracle(engine):
+    """Black-Scholes paths observing the valuation date (time 0): a lookback
+    monitored from today (full risk) and an Asian with an unknown fixing
+    today (price only) agree with the oracle; the time-zero step takes the
+    path's first normal in both."""
+    doc = _request("fixed_lookback_full_risk")
+    doc["product"]["monitoring_dates"] = ["2026-09-04", "2027-03-05", "2027-09-04"]
+    del doc["product"]["historical_extremum"]
+    req = wire.compile_request(doc, reduction_block_size=256)
+    assert req.plan.observation_times[0] == 0.0
+    G.assert_parity(req.plan)
+    doc = _request("arithmetic_asian_full_risk")
+    doc["product"]["observations"][0] = {"date": "2026-09-04", "value": {"type": "unknown"}, "weight": 0.2}
+    doc["risk"] = {"delta": False, "vega": False, "smile_dynamics": {"type": "sticky_log_moneyness"}}
+    req = wire.compile_request(doc, reduction_block_size=256)
+    assert req.plan.observation_times[0] == 0.0
+    G.assert_parity(req.plan)

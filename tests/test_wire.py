@@ -137,10 +137,17 @@ def test_lookback_history_and_valuation_date_fixing():
     assert len(req.plan.observation_times) == 2
     doc["product"]["side"] = {"type": "put"}
     assert wire.compile_request(doc).plan.products[0].initial_state == 105.0  # Minimum
-    # Without the fixing, the valuation-date monitoring is a time-zero observation.
+    # Without the fixing, the valuation-date monitoring is a time-zero observation
+    # (Black-Scholes only: a zero-length step that still takes its normal).
     del doc["product"]["valuation_date_fixing"]
+    req = wire.compile_request(doc)
+    assert req.plan.observation_times[0] == 0.0 and len(req.plan.observation_times) == 3
+    lv = copy.deepcopy(doc)
+    lv["model"] = {"type": "local_volatility", "local_variance_grid": {
+        "time_nodes": [0.0, 1.0], "log_forward_moneyness_nodes": [-1.0, 1.0], "shape": [2, 2],
+        "values": [0.04] * 4, "floor": 1e-8, "cap": 4.0}}
     with pytest.raises(wire.UnsupportedRequest):
-        wire.compile_request(doc)
+        wire.compile_request(lv)
     doc["product"].pop("historical_extremum")
     with pytest.raises(wire.WireError):
         wire.compile_request(doc)
@@ -195,7 +202,7 @@ def test_oracle_honours_seasoned_state_and_flags():
      wire.UnsupportedRequest),
     (lambda d: d.update(model={"type": "bass_local_volatility", "parameters": {}}), wire.UnsupportedRequest),
     (lambda d: d["risk"].update(payoff_smoothing_width_ladder=[1.0, 2.0]), wire.UnsupportedRequest),  # ladder entry
-    (lambda d: d["product"].update(expiry="2026-09-04", payment_date="2026-09-04"), wire.UnsupportedRequest),
+    (lambda d: d["product"].update(expiry="2026-09-04", payment_date="2026-09-04"), wire.UnsupportedRequest),  # t = 0 only
     (lambda d: d["product"].update(type="graph"), wire.UnsupportedRequest),
     (lambda d: d.pop("engine"), wire.WireError),
     (lambda d: d.update(lsm={}), wire.WireError),
@@ -294,3 +301,16 @@ def test_facade_compile_and_validation():
     bad["market"]["discrete_dividends"] = [{"event_id": 1, "ex_time": 0.5, "quote": {"type": "fixed_cash", "amount": 1.0}}]
     with pytest.raises(ValidationError):
         PricingPlan.compile(PricingRequest(bad), worker_threads=1)
+
+
+def test_time_zero_observation_on_the_oracle():
+    """A lookback monitored from the valuation date (no fixing): the first
+    observation is the spot at time zero, a zero-length step that still takes
+    its normal, as the reference's path generator does; the oracle prices it
+    with finite estimates (the engine's parity is in the GPU tests)."""
+    doc = _case("fixed_lookback_full_risk")
+    doc["product"]["monitoring_dates"] = ["2026-09-04", "2027-03-05", "2027-09-04"]
+    del doc["product"]["historical_extremum"]
+    out, buf = oracle_document(wire.compile_request(doc, reduction_block_size=256))
+    assert math.isfinite(out["value"]["value"]) and out["value"]["value"] > 0.0
+    assert math.isfinite(out["risks"]["vega"]["raw"]["value"])
