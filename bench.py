@@ -501,7 +501,13 @@ def main():
     achieved = FLOPS_PER_PATH_STEP * path_steps_rank / (path_ms * 1e-3) / 1e12
     roofline = {"bound": "fp64" if args.precision == "f64" else "fp64 (FP32 path bulk: the FP64 figure only bounds it)",
                 "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "frac": achieved / peak.value if peak.value else None,
+                # DRAM bytes of one path-kernel launch, scaled by CTA count from the ncu capture
+                # of the 2^14-point x 16-scramble case (1.771776 MB read + 1.024 KB written over
+                # 2048 CTAs: grid, scramble tables and tile records, in proportion to the CTAs)
+                "traffic": (1.771776e6 + 1.024e3) * (args.points * args.scrambles / 128) / 2048,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2^14 x 16 case "
+                                  "(profiles/lv_path_kernels_fp64_fp32_c2_small.md), scaled by CTA count",
                 "peak_source": "measured live: mcg_measure_fp64_peak (DFMA chains, this GPU)",
                 "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel_ms": path_ms}
 
