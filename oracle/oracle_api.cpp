@@ -34,6 +34,11 @@ int lsm_spots(const mcg_plan_desc* desc, uint32_t domain, int threads, std::vect
 int lsm_dual(const mcg_plan_desc* desc, const mcg_lsm_desc* lsm, const mcg_dual_desc* dual,
              mcg_dual_result* out, int threads);
 int lsm_scaling_api(const double* values, size_t n, double out[4]);
+int lv_barrier_adjoints_api(const double* times, uint32_t n_times, const double* forwards, const double* grid_t,
+                            uint32_t nt, const double* grid_x, uint32_t nx, const double* values, double initial,
+                            const double* shocks, double barrier, int up, int knock_out, uint32_t monitor_end,
+                            double quadratic, double rebate, double discount, double* price_out,
+                            double* grid_adj_out);
 int lv_step_adjoints_api(const double* times, uint32_t n_times, const double* forwards, const double* grid_t,
                          uint32_t nt, const double* grid_x, uint32_t nx, const double* values, double initial,
                          const double* shocks, const double* state_seeds, double* states_out,
@@ -167,6 +172,16 @@ int oracle_lv_step_adjoints(const double* times, uint32_t n_times, const double*
                             double* grid_adj_out) {
     return oracle::lv_step_adjoints_api(times, n_times, forwards, grid_t, nt, grid_x, nx, values, initial, shocks,
                                         state_seeds, states_out, grid_adj_out);
+}
+
+int oracle_lv_barrier_adjoints(const double* times, uint32_t n_times, const double* forwards,
+                               const double* grid_t, uint32_t nt, const double* grid_x, uint32_t nx,
+                               const double* values, double initial, const double* shocks, double barrier, int up,
+                               int knock_out, uint32_t monitor_end, double quadratic, double rebate,
+                               double discount, double* price_out, double* grid_adj_out) {
+    return oracle::lv_barrier_adjoints_api(times, n_times, forwards, grid_t, nt, grid_x, nx, values, initial, shocks,
+                                           barrier, up, knock_out, monitor_end, quadratic, rebate, discount,
+                                           price_out, grid_adj_out);
 }
 
 int oracle_lsm_scaling(const double* values, uint64_t n, double* out) {

@@ -1488,6 +1488,60 @@ int lv_step_adjoints_api(const double* times, uint32_t n_times, const double* fo
     return MCG_OK;
 }
 
+// A continuous barrier on one Log-Euler path (the reference's direct-variance
+// fixture): exact bridge survival over the first `monitor_end` intervals with
+// node variances at the path's states, a knock-out/in payoff of the vanilla
+// q S_T^2 with a rebate, discounted; the price and the grid-value adjoints of
+// the reverse sweep with the bridge's state and direct-variance seeds.
+int lv_barrier_adjoints_api(const double* times, uint32_t n_times, const double* forwards, const double* grid_t,
+                            uint32_t nt, const double* grid_x, uint32_t nx, const double* values, double initial,
+                            const double* shocks, double barrier, int up, int knock_out, uint32_t monitor_end,
+                            double quadratic, double rebate, double discount, double* price_out,
+                            double* grid_adj_out) {
+    Plan p;
+    p.nodes.assign(times, times + n_times);
+    p.fwd[0].assign(forwards, forwards + n_times);
+    p.bump_spot[0] = initial;
+    p.grid.t.assign(grid_t, grid_t + nt);
+    p.grid.x.assign(grid_x, grid_x + nx);
+    p.grid.v.assign(values, values + static_cast<size_t>(nt) * nx);
+    p.grid.floor = 1e-8;
+    p.grid.cap = 4.0;
+    p.smoothing = 0.0;
+    LvPath path;
+    Failure f;
+    if (!lv_evolve(p, 0, shocks, path, f)) return f.code;
+    std::vector<double> nv;
+    if (!lv_node_variances(p, 0, path, nv, f)) return f.code;
+    mcg_product_desc d{};
+    d.kind = MCG_PRODUCT_CONTINUOUS_BARRIER;
+    d.barrier = barrier;
+    d.barrier_direction = up ? MCG_BARRIER_UP : MCG_BARRIER_DOWN;
+    d.barrier_style = knock_out ? MCG_KNOCK_OUT : MCG_KNOCK_IN;
+    BarrierEval be;
+    if (!barrier_bridge(p, d, path.state.data(), nv.data(), p.nodes.data(), monitor_end + 1, be, f)) return f.code;
+    const double st = path.state[n_times - 1];
+    const double vanilla = quadratic * st * st;
+    const double surv = be.survival;
+    const double value = knock_out ? rebate + surv * (vanilla - rebate) : vanilla + surv * (rebate - vanilla);
+    *price_out = discount * value;
+    std::vector<double> seeds(n_times, 0.0), var_seeds(n_times, 0.0), grid_adj;
+    seeds[n_times - 1] = discount * (knock_out ? surv : 1.0 - surv) * 2.0 * quadratic * st;
+    if (be.exact_active) {
+        const double lsa = discount * (knock_out ? vanilla - rebate : rebate - vanilla) * surv;
+        for (size_t k = 0; k < be.ex.size(); ++k) {
+            seeds[k] += lsa * be.ex[k].d_left_state;
+            seeds[k + 1] += lsa * be.ex[k].d_right_state;
+            var_seeds[k] += lsa * be.ex[k].d_left_var;
+            var_seeds[k + 1] += lsa * be.ex[k].d_right_var;
+        }
+    }
+    double initial_adjoint = 0.0, x_sum = 0.0;
+    if (!lv_reverse(p, 0, path, seeds, var_seeds, grid_adj, initial_adjoint, x_sum, f)) return f.code;
+    for (size_t i = 0; i < grid_adj.size(); ++i) grid_adj_out[i] = grid_adj[i];
+    return MCG_OK;
+}
+
 int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacity,
                   uint32_t* count) {
     Plan p;

@@ -27,6 +27,9 @@ which the wire-format tests compile.
 * lv_step_adjoints.json     -- fixtures/local-vol/step-adjoints-v0.1.json: one Log-Euler path per
   case (given nodes, forwards, 3 x 3 grid, shocks) with a quadratic payoff, its
   states and 100-digit bump references of the grid-value derivatives.
+* lv_direct_variance.json   -- fixtures/local-vol/direct-variance-v0.1.json: continuous barriers
+  (up/down, out/in, partial monitoring, touched) on one Log-Euler path with node
+  variances, and 100-digit bump references of the grid-value derivatives.
 * early_exercise_cases.json -- fixtures/early-exercise/reference-cases-v0.1.json: the
   decision, monomial-basis, feature-scaling and CPQR cases (decimal strings).
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
@@ -195,6 +198,14 @@ def step_adjoints():
     json.dump(d, open(os.path.join(OUT, "lv_step_adjoints.json"), "w"), indent=1)
 
 
+def direct_variance():
+    src = os.path.join(REF, "fixtures/local-vol/direct-variance-v0.1.json")
+    d = json.load(open(src))
+    keep = {k: d[k] for k in ("reference", "relative_tolerance", "absolute_tolerance", "cases")}
+    keep["source"] = "fixtures/local-vol/direct-variance-v0.1.json"
+    json.dump(keep, open(os.path.join(OUT, "lv_direct_variance.json"), "w"), indent=1)
+
+
 def early_exercise_cases():
     src = os.path.join(REF, "fixtures/early-exercise/reference-cases-v0.1.json")
     d = json.load(open(src))
@@ -304,5 +315,6 @@ if __name__ == "__main__":
     path_dependence_replay()
     early_exercise_cases()
     step_adjoints()
+    direct_variance()
     surfaces()
     print("golden fixtures written to", OUT)

@@ -50,3 +50,38 @@ def test_step_adjoints_match_the_decimal_references(case):
     np.testing.assert_allclose(states, e["states"], rtol=1e-13)
     for got, want in zip(adj, e["grid_variance"]):
         assert abs(got - want) <= rel * abs(want) or (want == 0.0 and got == 0.0), (got, want)
+
+
+DIRECT = json.load(open(os.path.join(H.GOLDEN, "lv_direct_variance.json")))
+
+
+@pytest.mark.parametrize("case", DIRECT["cases"], ids=lambda c: c["id"])
+def test_barrier_direct_variance_adjoints(case):
+    """fixtures/local-vol/direct-variance-v0.1.json: an exact continuous
+    barrier over the first `monitor_end` intervals of one Log-Euler path, with
+    node variances at the path's states, paying a rebate or q S_T^2; the
+    oracle's price and the grid-value adjoints of its reverse sweep (bridge
+    state seeds plus direct variance seeds at the nodes) within 1e-9 of the
+    100-digit references."""
+    lib = H.oracle()
+    dp = C.POINTER(C.c_double)
+    lib.oracle_lv_barrier_adjoints.argtypes = [dp, C.c_uint32, dp, dp, C.c_uint32, dp, C.c_uint32, dp, C.c_double,
+                                               dp, C.c_double, C.c_int, C.c_int, C.c_uint32, C.c_double,
+                                               C.c_double, C.c_double, dp, dp]
+    lib.oracle_lv_barrier_adjoints.restype = C.c_int
+    arr = lambda k: np.ascontiguousarray(case[k], dtype=np.float64)
+    times, fwd, gt, gx, gv, shocks = (arr(k) for k in ("times", "forwards", "grid_times", "nodes", "variances",
+                                                        "shocks"))
+    price = C.c_double()
+    adj = np.zeros(len(gv))
+    rc = lib.oracle_lv_barrier_adjoints(H.dptr(times), len(times), H.dptr(fwd), H.dptr(gt), len(gt), H.dptr(gx),
+                                        len(gx), H.dptr(gv), case["initial"], H.dptr(shocks), case["barrier"],
+                                        int(case["direction"] == "up"), int(case["style"] == "out"),
+                                        case["monitor_end"], case["quadratic"], case["rebate"], case["discount"],
+                                        C.byref(price), H.dptr(adj))
+    assert rc == 0
+    rel = DIRECT["relative_tolerance"]
+    e = case["expected"]
+    assert abs(price.value - e["price"]) <= rel * abs(e["price"])
+    for got, want in zip(adj, e["grid_variance"]):
+        assert abs(got - want) <= rel * abs(want) + 1e-12, (got, want)
