@@ -30,6 +30,8 @@ which the wire-format tests compile.
 * lv_direct_variance.json   -- fixtures/local-vol/direct-variance-v0.1.json: continuous barriers
   (up/down, out/in, partial monitoring, touched) on one Log-Euler path with node
   variances, and 100-digit bump references of the grid-value derivatives.
+* wire_v3_documents.json    -- fixtures/v3/*.golden.json: the format goldens of a v3 request and
+  result (European and American).
 * early_exercise_cases.json -- fixtures/early-exercise/reference-cases-v0.1.json: the
   decision, monomial-basis, feature-scaling and CPQR cases (decimal strings).
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
@@ -206,6 +208,14 @@ def direct_variance():
     json.dump(keep, open(os.path.join(OUT, "lv_direct_variance.json"), "w"), indent=1)
 
 
+def wire_documents():
+    out = {}
+    for name in ("pricing_request", "pricing_request_american", "pricing_result", "pricing_result_american"):
+        out[name] = json.load(open(os.path.join(REF, f"fixtures/v3/{name}.golden.json")))
+    out["source"] = "fixtures/v3/*.golden.json"
+    json.dump(out, open(os.path.join(OUT, "wire_v3_documents.json"), "w"), indent=1)
+
+
 def early_exercise_cases():
     src = os.path.join(REF, "fixtures/early-exercise/reference-cases-v0.1.json")
     d = json.load(open(src))
@@ -316,5 +326,6 @@ if __name__ == "__main__":
     early_exercise_cases()
     step_adjoints()
     direct_variance()
+    wire_documents()
     surfaces()
     print("golden fixtures written to", OUT)

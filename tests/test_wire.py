@@ -314,3 +314,28 @@ def test_time_zero_observation_on_the_oracle():
     out, buf = oracle_document(wire.compile_request(doc, reduction_block_size=256))
     assert math.isfinite(out["value"]["value"]) and out["value"]["value"] > 0.0
     assert math.isfinite(out["risks"]["vega"]["raw"]["value"])
+
+
+def test_documents_follow_the_v3_format_goldens():
+    """fixtures/v3/*.golden.json: the golden requests compile (European and
+    American), and a result document built from the engine's estimates has the
+    golden result's sections and field names (value estimate, diagnostics,
+    replay with migration)."""
+    import json as _json
+    import os as _os
+    g = _json.load(open(_os.path.join(H.GOLDEN, "wire_v3_documents.json")))
+    req = wire.compile_request(g["pricing_request"])
+    assert req.product_type == "european_vanilla" and req.plan.sampling_units == 1024 and req.plan.antithetic
+    am = wire.compile_request(g["pricing_request_american"])
+    assert am.lsm is not None
+    out, _ = oracle_document(req)
+    out["replay"] = wire.replay_block(g["pricing_request"])
+    golden = g["pricing_result"]
+    for section in ("document_kind", "schema_version", "value", "risks", "diagnostics", "replay"):
+        assert section in out
+    assert set(out["value"]) == set(golden["value"])
+    assert set(out["replay"]) == set(golden["replay"])
+    assert set(out["replay"]["migration"]) == set(golden["replay"]["migration"])
+    assert set(out["diagnostics"]) == set(golden["diagnostics"])
+    for k, v in g["pricing_result_american"].get("risks", {}).items():
+        assert set(v) == {"raw", "market_scaled", "raw_unit", "market_scaled_unit"}
