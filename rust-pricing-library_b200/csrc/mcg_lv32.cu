@@ -22,21 +22,29 @@ constexpr float kTwoM32 = 2.3283064365386963e-10f;
 
 // AS241 in FP32 from the 32-bit word: the centred value (w - 2^31 + 0.5) 2^-32
 // and the tail probability min(p, 1 - p) are formed from the integer, so the
-// tail never rounds to zero.  Coefficients are Wichura's published ones.
-__device__ __forceinline__ float normal_from_word(uint32_t w) {
-    const float centered = (static_cast<float>(static_cast<int32_t>(w - 0x80000000u)) + 0.5f) * kTwoM32;
-    if (fabsf(centered) <= 0.425f) {
-        const float a = 0.180625f - centered * centered;
-        const float num =
-            ((((((2509.0809287301227f * a + 33430.575583588128f) * a + 67265.770927008700f) * a +
-                 45921.953931549871f) * a + 13731.693765509461f) * a + 1971.5909503065514f) * a +
-             133.14166789178438f) * a + 3.3871328727963666f;
-        const float den =
-            ((((((5226.4952788528545f * a + 28729.085735721943f) * a + 39307.895800092710f) * a +
-                 21213.794301586596f) * a + 5394.1960214247511f) * a + 687.18700749205790f) * a +
-             42.313330701600911f) * a + 1.0f;
-        return centered * __fdividef(num, den);
-    }
+// tail never rounds to zero.  Coefficients are Wichura's published ones.  The
+// two branches are separate functions so a warp can take the central one for
+// every lane and the tail one only for the lanes that need it.
+__device__ __forceinline__ float normal32_centered(uint32_t w) {
+    return (static_cast<float>(static_cast<int32_t>(w - 0x80000000u)) + 0.5f) * kTwoM32;
+}
+
+__device__ __forceinline__ bool normal32_is_tail(float centered) { return !(fabsf(centered) <= 0.425f); }
+
+__device__ __forceinline__ float normal32_central(float centered) {
+    const float a = 0.180625f - centered * centered;
+    const float num =
+        ((((((2509.0809287301227f * a + 33430.575583588128f) * a + 67265.770927008700f) * a +
+             45921.953931549871f) * a + 13731.693765509461f) * a + 1971.5909503065514f) * a +
+         133.14166789178438f) * a + 3.3871328727963666f;
+    const float den =
+        ((((((5226.4952788528545f * a + 28729.085735721943f) * a + 39307.895800092710f) * a +
+             21213.794301586596f) * a + 5394.1960214247511f) * a + 687.18700749205790f) * a +
+         42.313330701600911f) * a + 1.0f;
+    return centered * __fdividef(num, den);
+}
+
+__device__ __forceinline__ float normal32_tail(uint32_t w, float centered) {
     const uint32_t k = centered < 0.0f ? w : 0xffffffffu - w;
     const float tail = (static_cast<float>(k) + 0.5f) * kTwoM32;
     const float r = sqrtf(-__logf(tail));
@@ -63,6 +71,45 @@ __device__ __forceinline__ float normal_from_word(uint32_t w) {
                            5.99832206555887937690e-1f) * a + 1.0f);
     }
     return centered < 0.0f ? -m : m;
+}
+
+// Batched normals, as in the FP64 kernel: kZBatch32 normals of the program per
+// thread at a time, in s_z[k][thread] (a float's bits, or the word while its
+// tail value is pending).  Every lane takes the central branch; the lanes in
+// the tail are listed per warp (s_zlist, 32 * kZBatch32 entries) and the tail
+// branch runs 32 list entries at a time, so a warp no longer executes it for
+// each normal that one of its lanes sends there.  The values are those of the
+// one-at-a-time quantile.
+constexpr int kZBatch32 = 8;
+
+template <typename Word>
+__device__ __forceinline__ void fill_normals32(const DevicePlan& P, Word word, uint32_t first, uint32_t count,
+                                               uint32_t* s_z, uint16_t* s_zlist) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    uint16_t* list = s_zlist + warp * (32u * kZBatch32);
+    uint32_t tails = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t w = word(__ldg(P.z_ranks + first + k));
+        const float c = normal32_centered(w);
+        const bool tail = normal32_is_tail(c);
+        const float central = normal32_central(c);
+        s_z[k * kThreads + threadIdx.x] = tail ? w : __float_as_uint(central);
+        const unsigned m = __ballot_sync(0xffffffffu, tail);
+        if (tail) list[tails + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(k * 32u + lane);
+        tails += static_cast<uint32_t>(__popc(m));
+    }
+    __syncwarp();
+    for (uint32_t b = 0; b < tails; b += 32u) {
+        const uint32_t i = b + lane;
+        if (i < tails) {
+            const uint32_t idx = list[i];
+            uint32_t* at = s_z + (idx >> 5) * kThreads + warp * 32u + (idx & 31u);
+            const uint32_t w = *at;
+            *at = __float_as_uint(normal32_tail(w, normal32_centered(w)));
+        }
+    }
+    __syncwarp();
 }
 
 // Bilinear local variance on the FP32 grid, x clamped flat to the node range
@@ -95,6 +142,8 @@ __global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2 && CB == 0) ? 8 :
     float* s_x = s_v + nv;
     float* s_w = s_x + ((nx + 3) & ~3);  // bridge slots [slot][thread]
     Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(P.slot_count) * kThreads);
+    uint32_t* s_z = reinterpret_cast<uint32_t*>(s_red + 4 * kComponents);  // batched normals [k][thread]
+    uint16_t* s_zlist = reinterpret_cast<uint16_t*>(s_z + kZBatch32 * kThreads);  // tail lists, per warp
     for (int i = threadIdx.x; i < nv; i += kThreads) s_v[i] = static_cast<float>(P.grid_v[i]);
     for (int i = threadIdx.x; i < nx; i += kThreads) s_x[i] = static_cast<float>(P.grid_x[i]);
     __syncthreads();
@@ -119,6 +168,18 @@ __global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2 && CB == 0) ? 8 :
         ns.low = P.scr_low + static_cast<size_t>(scramble) * P.dimension * 32u;
     }
     auto word = [&](uint32_t dim) { return RQ ? ns.word_warp(dim) : ns.word(dim); };
+    // The program's normals in order, kZBatch32 at a time.
+    uint32_t zi = 0, zbase = 0, zend = 0;
+    auto next_normal = [&]() -> float {
+        if (zi == zend) {
+            zbase = zi;
+            const uint32_t n = P.z_count - zi < static_cast<uint32_t>(kZBatch32) ? P.z_count - zi
+                                                                                : static_cast<uint32_t>(kZBatch32);
+            fill_normals32(P, word, zi, n, s_z, s_zlist);
+            zend = zi + n;
+        }
+        return __uint_as_float(s_z[(zi++ - zbase) * kThreads + threadIdx.x]);
+    };
 
     // The state is the forward-normalised spot g = f / F_i, a martingale
     // (f_{i+1} / F_{i+1} = (f_i / F_i) exp(-v dt / 2 + sqrt(v dt) z)): no FP32
@@ -152,11 +213,11 @@ __global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2 && CB == 0) ? 8 :
             continue;
         }
         if (op.kind == kOpTerminal) {
-            w[op.out * kThreads] = static_cast<float>(op.sd) * normal_from_word(word(op.rank));
+            w[op.out * kThreads] = static_cast<float>(op.sd) * next_normal();
             continue;
         }
         if (op.kind == kOpInterior) {
-            const float z = normal_from_word(word(op.rank));
+            const float z = next_normal();
             w[op.out * kThreads] = static_cast<float>(op.wl) * w[op.left * kThreads] +
                                    static_cast<float>(op.wr) * w[op.right * kThreads] + static_cast<float>(op.sd) * z;
             continue;
@@ -166,7 +227,7 @@ __global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2 && CB == 0) ? 8 :
         if (op.kind == kOpStep)
             shock = (w[op.right * kThreads] - w[op.left * kThreads]) * P.step_f[s].w;
         else
-            shock = normal_from_word(word(op.rank));
+            shock = next_normal();
         const int tc = P.time_cell[s];
         const float4 kc = P.step_f[s];
         const float dt = kc.x, sq = kc.y, tw = kc.z;
@@ -249,7 +310,8 @@ cudaError_t launch_lv32_path(const DevicePlan& P, StatRecord* partials, uint32_t
     const int E = P.antithetic ? 2 : 1;
     const int np = static_cast<int>(P.product_count);
     const size_t smem = (static_cast<size_t>(P.nt) * P.nx + ((P.nx + 3) & ~3u)) * sizeof(float) +
-                        static_cast<size_t>(P.slot_count) * kThreads * sizeof(float) + 4 * kComponents * sizeof(Stat);
+                        static_cast<size_t>(P.slot_count) * kThreads * sizeof(float) + 4 * kComponents * sizeof(Stat) +
+                        kZBatch32 * kThreads * sizeof(uint32_t) + (kThreads / 32) * 32 * kZBatch32 * sizeof(uint16_t);
     const dim3 grid(static_cast<unsigned>((P.units + kThreads - 1) / kThreads), P.scramble_count);
     auto go = [&](auto kernel) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
