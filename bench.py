@@ -62,8 +62,8 @@ def parse():
     ap.add_argument("--dual-units", type=int, default=1 << 14,
                     help="antithetic outer units of the Andersen-Broadie secondary measurement")
     ap.add_argument("--secondary", default="all",
-                    help="comma list of secondary measurements: early_exercise, book, f32, adjoint, "
-                         "path_risk, dual; all; none")
+                    help="comma list of secondary measurements: european, early_exercise, book, f32, "
+                         "adjoint, path_risk, dual; all; none")
     ap.add_argument("--adjoint-paths", type=int, default=1 << 20)
     ap.add_argument("--lsm-units", type=int, default=1 << 20)
     ap.add_argument("--book-trades", type=int, default=4096)
@@ -315,6 +315,46 @@ def path_risk_secondary(units: int = 1 << 20, cpu_units: int = 1 << 14):
     return out
 
 
+def european_secondary(paths: int = 1 << 20, cpu_units: int = 1 << 18):
+    """The plain European configuration: a Black--Scholes call S = K = 100,
+    r = 3 %, q = 1 %, sigma = 20 %, T = 1, one exact lognormal step, `paths`
+    pseudo paths (seed 0x0123456789abcdef), FP64, price with pathwise Delta and
+    Vega and Gamma by a 1 % relative bump (which also fills the CRN validation
+    components: 7 evaluations of every path), judged by the closed form.  The
+    oracle on the host's cores prices `cpu_units` paths of the same plan."""
+    from rust_pricing_b200 import _native as N, workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+    from bs_closed_form import black_scholes
+    spec = W.european_bs(paths=paths)
+    with N.Plan(spec) as plan:
+        plan.evaluate()
+        runs = [plan.evaluate() for _ in range(5)]
+    r = min(runs, key=lambda b: b.result.device_ms)
+    p, ms = r.products[0], r.result.device_ms
+    cf = black_scholes(True, 100.0, 100.0, 1.0, W.RATE, W.DIVIDEND, 0.2)
+    spec.sampling_units = cpu_units
+    threads = os.cpu_count() or 1
+    H.oracle_evaluate(spec, threads)
+    t0 = time.perf_counter()
+    H.oracle_evaluate(spec, threads)
+    cpu_s = time.perf_counter() - t0
+    out = {"workload": f"European BS call, {paths} pseudo paths, 1 exact step, FP64, price + pathwise Delta/Vega "
+                       "+ 1 % relative Gamma bump (7 path evaluations per unit); judge: closed form",
+           "device_ms": ms, "path_steps_per_s": paths / (ms * 1e-3),
+           "path_evaluations_per_s": 7 * paths / (ms * 1e-3), "kernel_launches": r.result.kernel_launches,
+           "ms_to_1bp_standard_error": time_to_bp(ms, p.price.standard_error, p.price.value),
+           "ms_to_1pct_delta": time_to_pct(ms, p.delta.standard_error, p.delta.value),
+           "ms_to_1pct_vega": time_to_pct(ms, p.vega.standard_error, p.vega.value),
+           "cpu_oracle_path_steps_per_s": cpu_units / cpu_s, "cpu_threads": threads,
+           "cpu_sample": f"{cpu_units} paths, full risk ({cpu_s:.2f} s)"}
+    for key, est in (("price", p.price), ("delta", p.delta), ("vega", p.vega), ("gamma", p.gamma)):
+        out[key] = {"value": est.value, "standard_error": est.standard_error, "closed_form": cf[key],
+                    "error_in_standard_errors": (est.value - cf[key]) / est.standard_error}
+    out["gpu_over_cpu_oracle"] = out["path_steps_per_s"] / out["cpu_oracle_path_steps_per_s"]
+    return out
+
+
 def dual_secondary(units: int = 1 << 14, cpu_units: int = 2048):
     """Andersen--Broadie upper bound of the early-exercise configuration's
     American put (S = K = 100, r = 5 %, sigma = 25 %, T = 1, 50 exercise
@@ -506,8 +546,8 @@ def main():
                 # of the 2^14-point x 16-scramble case (1.771776 MB read + 1.024 KB written over
                 # 2048 CTAs: grid, scramble tables and tile records, in proportion to the CTAs)
                 "traffic": (1.771776e6 + 1.024e3) * (args.points * args.scrambles / 128) / 2048,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2^14 x 16 case "
-                                  "(profiles/lv_path_kernels_fp64_fp32_c2_small.md), scaled by CTA count",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the path kernel on the "
+                                  "2^14-point x 16-scramble case, scaled by CTA count",
                 "peak_source": "measured live: mcg_measure_fp64_peak (DFMA chains, this GPU)",
                 "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel_ms": path_ms}
 
@@ -548,10 +588,12 @@ def main():
         "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, m["standard_error"], m["value"])
                                      for m in merged] if merged else None,
     }
-    wanted = {"early_exercise", "book", "f32", "adjoint", "path_risk", "dual"} if args.secondary == "all" else (
+    wanted = {"european", "early_exercise", "book", "f32", "adjoint", "path_risk", "dual"} if args.secondary == "all" else (
         set() if args.secondary == "none" else set(args.secondary.split(",")))
     if rank == 0 and world == 1 and wanted:
         sec = {}
+        if "european" in wanted:
+            sec["european"] = european_secondary()
         if "early_exercise" in wanted:
             sec["early_exercise"] = lsm_secondary(args.lsm_units)
         if "f32" in wanted and args.precision == "f64":

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MCG_ABI_VERSION 2u
+#define MCG_ABI_VERSION 3u
 
 /* Component layout of one sampling unit, crates/pricing/src/engine/plan/simulation.rs:26-62. */
 #define MCG_PRICE 0
@@ -276,6 +276,15 @@ typedef struct mcg_result {
     float device_ms;           /* device time of the evaluation (CUDA events) */
     float path_kernel_ms;      /* device time of the path kernel alone */
     mcg_error_record error;
+    /* RQMC: every scramble's mean of every component (the replicates whose
+     * two-pass moments the statistics above are, crates/pricing/src/engine/risk/valuation.rs:349-361),
+     * replicate_means[(s * product_count + k) * MCG_PATHWISE_COMPONENTS + c]
+     * for the plan's scrambles s in order; caller-owned, replicate_capacity
+     * entries, NULL when not wanted (and left untouched for pseudo-MC).
+     * Shards of one plan (scramble_begin) gathered in scramble order give,
+     * by the same two-pass, the whole plan's statistics bit for bit. */
+    uint32_t replicate_capacity;
+    double* replicate_means;
 } mcg_result;
 
 typedef struct mcg_plan mcg_plan;
@@ -317,7 +326,11 @@ mcg_status mcg_philox_normals(uint64_t master_seed, uint64_t first_unit, uint64_
 /* Scrambled Sobol words of `count` consecutive points of one scramble,
  * dimension-major out[d * count + i]
  * (crates/pricing/src/engine/sampling/qmc.rs:47-132,204-369).  `directions`
- * holds the Joe--Kuo direction words, dimensions x 32. */
+ * holds the Joe--Kuo direction words, dimensions x 32.  When first_point and
+ * count are multiples of 32 the words are formed the way the path kernels
+ * form them (a warp per 32 aligned points: common Gray-code part by an XOR
+ * reduction over the warp, lane part from the low-word table); otherwise one
+ * thread per point walks the set Gray-code bits.  first_point + count <= 2^32. */
 mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint64_t master_seed,
                           uint32_t scramble, uint64_t first_point, uint64_t count,
                           uint32_t* out_host);
@@ -685,10 +698,14 @@ void mcg_book_destroy(mcg_book* book);
  * per GPU that loads this library, held until the process exits.  Limits:
  * sampling units x scrambles <= 2^20 and scramble_count <= 64; larger
  * requests return MCG_ERR_INVALID_ARGUMENT.  All calls share the array: calls
- * that overlap on the GPU race and must be serialised by the caller.  The
- * first call on a device resolves the array's address; make it before any
- * stream capture.  `result->products` needs one slot; device_ms is not timed;
- * failures are described by mcg_last_error(). */
+ * that overlap on the GPU race and must be serialised by the caller.  Every
+ * call looks up the array's address on the current device (no address is
+ * kept across a device reset); the first call on a device may load the
+ * library's device code, so make it before any stream capture.  A call
+ * synchronises `stream` before it returns.  The descriptor checks are
+ * mcg_plan_create's; a failing sampling unit is reported with its step and
+ * value bits as mcg_plan_evaluate reports it.  `result->products` needs one
+ * slot; device_ms is not timed; failures are described by mcg_last_error(). */
 #define MCG_NOALLOC_SCRATCH_BYTES 5953280u
 mcg_status mcg_price_european_noalloc(const mcg_plan_desc* desc, void* stream, mcg_result* result);
 

@@ -1401,6 +1401,11 @@ int evaluate(const mcg_plan_desc* desc, mcg_result* result, int threads) {
             stats[i].moments = CenteredMoment::two_pass(replicate[i]);
             for (double v : replicate[i]) stats[i].sum.add(v);
         }
+        if (result->replicate_means && result->replicate_capacity >= uint64_t{p.scrambles} * P * kComponents)
+            for (uint32_t s = 0; s < p.scrambles; ++s)
+                for (size_t k = 0; k < P; ++k)
+                    for (int c = 0; c < kComponents; ++c)
+                        result->replicate_means[(s * P + k) * kComponents + c] = replicate[k * kWidth + c][s];
         independent = p.scrambles;
         result->evaluated_paths = p.units * p.scrambles * (p.antithetic ? 2 : 1);
     }

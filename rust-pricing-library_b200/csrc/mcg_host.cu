@@ -46,6 +46,8 @@ __global__ void scramble_low_kernel(const uint32_t*, uint32_t, uint32_t*);
 __global__ void philox_normals_kernel(uint64_t, uint64_t, uint64_t, uint32_t, uint32_t, double*);
 __global__ void rqmc_words_kernel(const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint64_t,
                                   uint64_t, uint32_t*);
+__global__ void rqmc_words_warp_kernel(const uint32_t*, const uint32_t*, const uint32_t*, uint32_t, uint32_t,
+                                       uint64_t, uint64_t, uint32_t*);
 __global__ void fp64_peak_kernel(double*, int);
 struct AdjointArgs {
     int32_t which;
@@ -1119,6 +1121,9 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
     result->time_steps = P.steps;
     result->effective_dimension = P.dimension;
     result->reduction_records = plan->tiles * P.scramble_count;
+    const bool want_replicates = rqmc && result->replicate_means &&
+                                 result->replicate_capacity >=
+                                     static_cast<uint64_t>(P.scramble_count) * plan->product_count * kComponents;
     for (uint32_t k = 0; k < plan->product_count; ++k) {
         mcg_product_result& r = result->products[k];
         HostStat stats[kComponents];
@@ -1140,6 +1145,10 @@ mcg_status evaluate(mcg_plan* plan, cudaStream_t stream, mcg_result* result) {
                         reps[s] = (x.sum + x.corr) / static_cast<double>(P.units);
                     }
                 h = two_pass(reps);
+                if (want_replicates)
+                    for (uint32_t s = 0; s < P.scramble_count; ++s)
+                        result->replicate_means[(static_cast<size_t>(s) * plan->product_count + k) * kComponents + c] =
+                            reps[s];
             }
             stats[c] = h;
             r.components[c] = {h.sum, h.corr, h.count, h.mean, h.m2};
@@ -2366,19 +2375,30 @@ mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint6
                           uint64_t first_point, uint64_t count, uint32_t* out_host) {
     if (!directions || !out_host || count == 0 || dimensions == 0)
         return fail(MCG_ERR_INVALID_ARGUMENT, "empty request");
-    uint32_t *dirs = nullptr, *table = nullptr, *shifts = nullptr, *out = nullptr;
+    if (first_point + count > (1ull << 32))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "Sobol point index beyond 2^32");
+    uint32_t *dirs = nullptr, *table = nullptr, *shifts = nullptr, *out = nullptr, *low = nullptr;
     const uint32_t scrambles = scramble + 1;
+    // Aligned requests go through the path kernels' warp-cooperative form.
+    const bool warp = (first_point & 31u) == 0 && (count & 31u) == 0;
     MCG_CUDA(cudaMalloc(&dirs, static_cast<size_t>(dimensions) * 32 * 4));
     MCG_CUDA(cudaMalloc(&table, static_cast<size_t>(scrambles) * dimensions * 32 * 4));
     MCG_CUDA(cudaMalloc(&shifts, static_cast<size_t>(scrambles) * dimensions * 4));
     MCG_CUDA(cudaMalloc(&out, count * dimensions * 4));
+    if (warp) MCG_CUDA(cudaMalloc(&low, static_cast<size_t>(scrambles) * dimensions * 32 * 4));
     cudaError_t e = cudaMemcpy(dirs, directions, static_cast<size_t>(dimensions) * 32 * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
         const uint32_t total = scrambles * dimensions;
         scramble_table_kernel<<<(total + 127) / 128, 128>>>(dirs, dimensions, scrambles, 0u, master_seed, table,
                                                            shifts);
-        rqmc_words_kernel<<<static_cast<unsigned>((count + 127) / 128), 128>>>(table, shifts, dimensions, scramble,
-                                                                              first_point, count, out);
+        if (warp) {
+            scramble_low_kernel<<<(total * 32u + 127) / 128, 128>>>(table, total, low);
+            rqmc_words_warp_kernel<<<static_cast<unsigned>((count + 127) / 128), 128>>>(
+                table, shifts, low, dimensions, scramble, first_point, count, out);
+        } else {
+            rqmc_words_kernel<<<static_cast<unsigned>((count + 127) / 128), 128>>>(table, shifts, dimensions,
+                                                                                  scramble, first_point, count, out);
+        }
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(out_host, out, count * dimensions * 4, cudaMemcpyDeviceToHost);
@@ -2386,6 +2406,7 @@ mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint6
     cudaFree(table);
     cudaFree(shifts);
     cudaFree(out);
+    if (low) cudaFree(low);
     if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
     return MCG_OK;
 }

@@ -19,11 +19,14 @@
 // is resident on every GPU that loads the library until the process exits.
 // Every call reuses the same array, so calls that overlap on the GPU (two
 // streams, or two host threads on one device) race and must be serialised by
-// the caller.  The first call on a device resolves the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.
+// the caller.  Every call resolves the array's device address on the current
+// device (cudaGetSymbolAddress, which allocates nothing), so no address is
+// kept across a device reset; the first call on a device may load this
+// library's device code (CUDA's lazy module loading), so make that first call
+// before any stream capture.  A call synchronises its stream before it
+// returns.
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -68,25 +71,15 @@ mcg_status noalloc_fail(mcg_status code, const std::string& why) {
     return code;
 }
 
-// Device address of g_noalloc_scratch, resolved once per device.
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-unsigned char* g_scratch_ptr[kMaxDevices] = {};
-
+// Device address of g_noalloc_scratch on the current device.  Resolved on
+// every call: the lookup allocates nothing, and a cached address would go
+// stale if the device were reset and the module loaded again.
 mcg_status scratch_for_current_device(unsigned char** out) {
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) return noalloc_fail(MCG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (device < 0 || device >= kMaxDevices) return noalloc_fail(MCG_ERR_UNSUPPORTED, "device index above 63");
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[device]) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr)
-            return noalloc_fail(MCG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_ptr[device] = static_cast<unsigned char*>(ptr);
-    }
-    *out = g_scratch_ptr[device];
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+        return noalloc_fail(MCG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    *out = static_cast<unsigned char*>(ptr);
     return MCG_OK;
 }
 
@@ -102,7 +95,7 @@ bool log_discount(const mcg_curve& c, double time, double& out) {
         c.discount_factors[0] != 1.0)
         return false;
     for (uint32_t i = 0; i < c.pillar_count; ++i)
-        if (!std::isfinite(c.times[i]) || !(c.discount_factors[i] > 0.0) ||
+        if (!std::isfinite(c.times[i]) || !std::isfinite(c.discount_factors[i]) || !(c.discount_factors[i] > 0.0) ||
             (i && !(c.times[i] > c.times[i - 1])))
             return false;
     if (time == 0.0) time = 0.0;
@@ -160,6 +153,8 @@ extern "C" mcg_status mcg_price_european_noalloc(const mcg_plan_desc* d, void* s
     const mcg_product_desc& pd = d->products[0];
     if (!(pd.notional > 0.0) || !(pd.strike > 0.0) || !std::isfinite(pd.strike))
         return noalloc_fail(MCG_ERR_INVALID_ARGUMENT, "product strike/notional must be positive");
+    if (pd.has_initial_state)  // as mcg_plan_create: a terminal product has no observation history
+        return noalloc_fail(MCG_ERR_UNSUPPORTED, "seasoned state of a product without observation history");
     if (!(d->smoothing_half_width >= 0.0) || !std::isfinite(d->smoothing_half_width))
         return noalloc_fail(MCG_ERR_INVALID_ARGUMENT, "smoothing_half_width");
     const bool rqmc = d->engine == MCG_ENGINE_RQMC;
@@ -277,9 +272,20 @@ extern "C" mcg_status mcg_price_european_noalloc(const mcg_plan_desc* d, void* s
     result->device_ms = 0.0f;
     result->path_kernel_ms = 0.0f;
     if (ew.key != ~0ull) {
+        // Re-run the first failing unit alone to recover its step and value
+        // bits, as mcg_plan_evaluate does.
+        const uint64_t unit = ew.key >> 8;
+        e = cudaMemcpyAsync(error, &clear, sizeof(clear), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = launch_bs_path(P, true, unit, 1, scrambles, partials, mask, error, 1, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&ew, error, sizeof(ew), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return noalloc_fail(MCG_ERR_CUDA, cudaGetErrorString(e));
         result->error.code = static_cast<int32_t>(ew.key & 0xff);
         result->error.sampling_unit = ew.key >> 8;
-        return noalloc_fail(static_cast<mcg_status>(result->error.code), "a sampling unit failed");
+        result->error.step = ew.step;
+        result->error.value_bits = ew.value_bits;
+        return noalloc_fail(static_cast<mcg_status>(result->error.code),
+                            "sampling unit " + std::to_string(result->error.sampling_unit) + " failed");
     }
     const uint64_t independent = rqmc ? scrambles : units;
     const double total_variance = d->volatility * d->volatility * expiry;

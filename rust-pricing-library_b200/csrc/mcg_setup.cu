@@ -115,6 +115,29 @@ __global__ void rqmc_words_kernel(const uint32_t* table, const uint32_t* shifts,
     for (uint32_t d = 0; d < dims; ++d) out[static_cast<size_t>(d) * count + i] = ns.word(d);
 }
 
+// The same words formed the way the path kernels form them: each warp holds
+// 32 consecutive, 32-aligned points (first % 32 == 0, count % 32 == 0) and
+// calls NormalSource::word_warp, the common Gray-code part by one coalesced
+// load and an XOR reduction, the lane part from the low table.
+__global__ void rqmc_words_warp_kernel(const uint32_t* table, const uint32_t* shifts, const uint32_t* low,
+                                       uint32_t dims, uint32_t scramble, uint64_t first, uint64_t count,
+                                       uint32_t* out) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t warp_first = i & ~static_cast<uint64_t>(31);
+    if (warp_first >= count) return;  // whole warps leave together (count % 32 == 0)
+    const uint32_t point = static_cast<uint32_t>(first + i);
+    NormalSource ns;
+    ns.rqmc = 1;
+    ns.gray = point ^ (point >> 1);
+    ns.dirs = table + static_cast<size_t>(scramble) * dims * 32u;
+    ns.shift = shifts + static_cast<size_t>(scramble) * dims;
+    const uint32_t q = point & ~31u;
+    ns.high_gray = q ^ (q >> 1);
+    ns.lane_low = point & 31u;
+    ns.low = low + static_cast<size_t>(scramble) * dims * 32u;
+    for (uint32_t d = 0; d < dims; ++d) out[static_cast<size_t>(d) * count + i] = ns.word_warp(d);
+}
+
 // ----------------------------------------------------------- SSVI grid
 
 // One thread per grid node: the surface's total variance derivatives at

@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 PATHWISE_COMPONENTS = 18
 
 PRICE, DELTA, VEGA, GAMMA = 0, 1, 2, 3
@@ -146,6 +146,7 @@ class Result(C.Structure):
         ("time_steps", C.c_uint32), ("effective_dimension", C.c_uint32),
         ("reduction_records", C.c_uint32), ("kernel_launches", C.c_uint32),
         ("device_ms", C.c_float), ("path_kernel_ms", C.c_float), ("error", ErrorRecord),
+        ("replicate_capacity", C.c_uint32), ("replicate_means", _dp),
     ]
 
 
@@ -156,7 +157,7 @@ class ResultBuffers:
     def node_stats(self):
         return self.node_stats_array
 
-    def __init__(self, products: int, nodes: int = 0):
+    def __init__(self, products: int, nodes: int = 0, scrambles: int = 0):
         self.products = (ProductResult * max(products, 1))()
         self.node_stats_array = (Statistics * nodes)() if nodes else None
         self.node_estimates = (Estimate * nodes)() if nodes else None
@@ -167,6 +168,21 @@ class ResultBuffers:
         if nodes:
             self.result.local_vega_nodes = C.cast(self.node_stats_array, C.POINTER(Statistics))
             self.result.local_vega_node_estimates = C.cast(self.node_estimates, C.POINTER(Estimate))
+        # RQMC: each scramble's component means, [scramble][product][component]
+        self.replicate_count = scrambles * products * PATHWISE_COMPONENTS
+        self.replicate_array = (C.c_double * self.replicate_count)() if scrambles else None
+        if scrambles:
+            self.result.replicate_capacity = self.replicate_count
+            self.result.replicate_means = C.cast(self.replicate_array, _dp)
+
+    def replicate_means(self, product: int, component: int = PRICE) -> list:
+        """The scramble means of one product's component, in scramble order."""
+        if self.replicate_array is None:
+            return []
+        n = len(self.products)
+        per = n * PATHWISE_COMPONENTS
+        scrambles = self.replicate_count // per
+        return [self.replicate_array[(s * n + product) * PATHWISE_COMPONENTS + component] for s in range(scrambles)]
 
 
 # ---- early exercise (Longstaff--Schwartz) ----

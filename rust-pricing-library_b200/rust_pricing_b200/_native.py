@@ -234,7 +234,8 @@ class Plan:
         self.nodes = spec.grid_value_count() * len(spec.products) if spec.request_local_vega_nodes else 0
 
     def evaluate(self, stream: int = 0) -> A.ResultBuffers:
-        buf = A.ResultBuffers(len(self.spec.products), self.nodes)
+        scrambles = self.spec.scramble_count if self.spec.engine == A.ENGINE_RQMC else 0
+        buf = A.ResultBuffers(len(self.spec.products), self.nodes, scrambles)
         status = library().mcg_plan_evaluate(self.handle, C.c_void_p(stream), C.byref(buf.result))
         check(status, buf.result.error)
         return buf

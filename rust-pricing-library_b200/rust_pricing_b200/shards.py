@@ -3,12 +3,19 @@ statistics.
 
 `bench.py --gpus N` gives rank r the scrambles [S r, S r + S) of one plan
 (`scramble_begin` of the descriptor); the paths are independent, so no
-collective touches the data path.  After the timed region every rank's
-per-product statistics of its scramble means travel to rank 0, which merges
-them in rank order with the reference's own merges -- NeumaierSum::merged and
-CenteredMoment::merged (Chan--Golub--LeVeque), fixed pairwise tree
-(crates/pricing-numerics/src/reduction.rs:3-272) -- and forms the estimate as
+collective touches the data path.  After the timed region every rank sends
+rank 0 its scrambles' means (the RQMC replicates, `replicate_means` of the
+result), rank 0 joins them in scramble order and runs the reference's
+replicate two-pass over all of them -- NeumaierSum over the replicates, then
+CenteredMoment::from_ordered_values_two_pass
+(crates/pricing/src/engine/risk/valuation.rs:349-361,
+crates/pricing-numerics/src/reduction.rs:3-122) -- the same operations, in the
+same order, as one evaluation of every scramble, so the merged estimate equals
+the single-GPU one bit for bit; the estimate is formed as
 estimate_from_statistics does (crates/pricing/src/engine/risk/report.rs:454-473).
+`merge` / `tree_merge` are the reference's NeumaierSum::merged and
+CenteredMoment::merged (Chan--Golub--LeVeque) with its fixed pairwise tree,
+for records that are not replicates (reduction.rs:123-272).
 """
 from __future__ import annotations
 
@@ -71,6 +78,23 @@ def tree_merge(stats: list) -> Stat:
     return level[0]
 
 
+def two_pass(values: list) -> Stat:
+    """NeumaierSum over the replicates in order, then the centred second
+    moment about their mean (from_ordered_values_two_pass): the engine's and
+    the oracle's RQMC statistics, operation for operation."""
+    if not values:
+        return Stat()
+    s, c = 0.0, 0.0
+    for v in values:
+        s, c = _neumaier_add(s, c, v)
+    mean = (s + c) / float(len(values))
+    qs, qc = 0.0, 0.0
+    for v in values:
+        d = v - mean
+        qs, qc = _neumaier_add(qs, qc, d * d)
+    return Stat(s, c, len(values), mean, qs + qc)
+
+
 def estimate(s: Stat, units: int) -> dict:
     """estimate_from_statistics with scale 1: value, standard error, 95 % bounds."""
     inv = 1.0 / float(units)
@@ -82,16 +106,20 @@ def estimate(s: Stat, units: int) -> dict:
 
 
 def gather_prices(buf, product_count: int, rank: int, world: int):
-    """All ranks: send this rank's price statistics; rank 0 returns the merged
-    estimate of every product over all ranks' scrambles (None elsewhere)."""
+    """All ranks: send this rank's scramble means of every product's price;
+    rank 0 returns the estimate of every product over all ranks' scrambles
+    (None elsewhere)."""
     import torch.distributed as dist
-    mine = [Stat.of(buf.products[k].components[0]) for k in range(product_count)]
+    mine = [buf.replicate_means(k) for k in range(product_count)]
+    if any(not m for m in mine):
+        raise ValueError("the shard merge needs the RQMC scramble means (replicate_means) of every product")
     gathered = [None] * world if rank == 0 else None
     dist.gather_object(mine, gathered, dst=0)
     if rank != 0:
         return None
     out = []
     for k in range(product_count):
-        merged = tree_merge([g[k] for g in gathered])
+        reps = [v for g in gathered for v in g[k]]  # rank order = scramble order
+        merged = two_pass(reps)
         out.append(estimate(merged, merged.count))
     return out

@@ -355,6 +355,47 @@ def _model(doc: dict, plan_kw: dict, expiry_time: float, warnings: list):
     raise WireError(f"model: unknown type {kind!r}")
 
 
+# ----------------------------------------------------------------- VegaKT policy
+
+# The reference's two VegaKT methods for a local-volatility request: the exact
+# market-IV risk of a statically replicable terminal payoff
+# (crates/pricing/src/engine/risk/vegakt_terminal_replication.rs:7) and the
+# allocation of the path simulation's local-vega node sensitivities to the
+# reporting buckets (crates/pricing/src/engine/risk/local_vol_allocation.rs:108-163).
+TERMINAL_REPLICATION = "terminal_payoff_replication_iv_v1"
+NODE_ALLOCATION = "local_vol_node_allocation_diagnostic_v1"
+
+
+def _terminal_replication_applies(ptype: str, times: list, plan_kw: dict, basis: dict) -> bool:
+    """Whether the reference prices this request's VegaKT by terminal
+    replication instead of node allocation
+    (compile_terminal_replication_vega_kt and compile_terminal_vega_kt,
+    crates/pricing/src/engine/risk/vegakt_terminal_replication.rs:10-40,
+    crates/pricing/src/engine/risk/vegakt_terminal_pricing.rs:21-71): no early
+    exercise, continuous barrier or payoff smoothing, identity dividend
+    coordinates, the expiry among the reporting basis's maturities, and a
+    payoff that is piecewise affine in the terminal spot alone
+    (try_terminal_payoff_gamma_measure, crates/pricing/src/engine/risk/vegakt_terminal.rs:200-330:
+    literals, the expiry's spot, sums, differences, minima, maxima and
+    constant scalings).  Of this engine's products that is the European
+    vanilla and an Asian or fixed lookback whose only simulated observation is
+    the expiry; digitals (an indicator) and barriers (hit state) are not.
+    A grid whose every time row is flat in log-moneyness is counted as
+    replicable too: the reference then checks the grid's cumulative variance
+    against the basis's implied volatilities and may route the request to its
+    terminal pathwise method, neither of which is node allocation."""
+    if ptype == "european_vanilla":
+        terminal = True
+    elif ptype in ("arithmetic_asian", "fixed_lookback"):
+        terminal = len(times) == 1
+    else:
+        terminal = False
+    if not terminal or plan_kw.get("smoothing_half_width", 0.0) > 0.0:
+        return False
+    maturities = [float(t) for t in basis.get("maturity_nodes", [])]
+    return times[-1] in maturities
+
+
 # ----------------------------------------------------------------- compile
 
 def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledRequest:
@@ -428,7 +469,9 @@ def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledR
         if plan_kw.get("model") != A.MODEL_LOCAL_VOLATILITY or basis is None:
             raise WireError("risk.vega_kt needs a local-volatility model with a reporting_iv_basis")
         plan_kw["request_local_vega_nodes"] = True
-        vega_kt = {"config": risk["vega_kt"], "reporting_iv_basis": basis}
+        replicable = _terminal_replication_applies(ptype, times, plan_kw, basis)
+        vega_kt = {"config": risk["vega_kt"], "reporting_iv_basis": basis,
+                   "policy": TERMINAL_REPLICATION if replicable else NODE_ALLOCATION}
 
     plan = PlanSpec(**plan_kw)
     if plan.engine == A.ENGINE_RQMC and plan.scramble_count < 1:
@@ -617,7 +660,8 @@ def _vega_kt_report(req: CompiledRequest, node_means, evaluated_paths: int) -> d
     vols = list(basis["implied_volatilities"])
     coordinates = [{"maturity": t, "log_moneyness": x, "implied_volatility": vols[i * len(xs) + j]}
                    for i, t in enumerate(maturities) for j, x in enumerate(xs)]
-    return {"coordinates": coordinates, "raw_buckets": [float(b) for b in buckets],
+    return {"policy_label": NODE_ALLOCATION,
+            "coordinates": coordinates, "raw_buckets": [float(b) for b in buckets],
             "projection": {"scalar_vega": out.scalar_vega, "signed_residual": out.signed_residual,
                            "pre_projection": out.pre_projection,
                            "reporting_stats": {"left_edge_count": int(out.left_edge_count),
@@ -679,10 +723,23 @@ def json_copy(doc):
     return copy.deepcopy(doc)
 
 
-def price_request(doc: dict, *, reduction_block_size: int = 4096, stream: int = 0) -> dict:
-    """Price one v3 request on the GPU and return its `pricing_result` document."""
+def price_request(doc: dict, *, reduction_block_size: int = 4096, stream: int = 0,
+                  node_allocation_diagnostic: bool = False) -> dict:
+    """Price one v3 request on the GPU and return its `pricing_result` document.
+
+    A local-volatility request whose VegaKT the reference computes by terminal
+    replication (see _terminal_replication_applies) raises UnsupportedRequest:
+    that market-IV method is not built here, and node allocation would give a
+    different VegaKT document.  `node_allocation_diagnostic=True` asks for the
+    node allocation anyway; the VegaKT document then names its method in
+    `policy_label`."""
     from . import _native as N
     req = compile_request(doc, reduction_block_size=reduction_block_size)
+    if req.vega_kt is not None and req.vega_kt["policy"] == TERMINAL_REPLICATION and not node_allocation_diagnostic:
+        raise UnsupportedRequest("VegaKT of a statically replicable terminal payoff: the reference reports its "
+                                 "terminal-replication market-IV risk (terminal_payoff_replication_iv_v1), which "
+                                 "this engine does not compute; pass node_allocation_diagnostic=True for the "
+                                 "local-vega node allocation")
     if req.lsm is not None:
         buf = N.lsm_price(req.plan, req.lsm, stream=stream)
         r = buf.result

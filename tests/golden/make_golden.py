@@ -1,8 +1,9 @@
 """Extracts golden vectors from the reference's fixtures into tests/golden/.
 
-Run in the build container, where the reference checkout is mounted at
-/root/reference (it is not present on GPU machines).  The extracted JSON files
-are committed; the tests only read them.
+Run where a checkout of the reference exists, with REFERENCE_ROOT set to its
+root (REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py; GPU
+machines have no checkout).  The extracted JSON files are committed; the tests
+only read them.
 
 * replay_european_bs.json  -- fixtures/replay/european_bs-windows-x86_64.json:
   request parameters and result values of the pseudo and RQMC full-risk cases.
@@ -44,7 +45,9 @@ import json
 import os
 import sys
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
+if __name__ == "__main__" and not REF:
+    sys.exit("set REFERENCE_ROOT to the reference checkout's root")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -99,7 +99,7 @@ def oracle_evaluate(spec, threads: int | None = None):
     """Run the oracle on a PlanSpec; returns the ResultBuffers."""
     lib = oracle()
     nodes = spec.grid_value_count() * len(spec.products) if spec.request_local_vega_nodes else 0
-    buf = A.ResultBuffers(len(spec.products), nodes)
+    buf = A.ResultBuffers(len(spec.products), nodes, spec.scramble_count if spec.engine == A.ENGINE_RQMC else 0)
     desc = spec.desc()
     rc = lib.oracle_evaluate(C.byref(desc), C.byref(buf.result), threads or os.cpu_count() or 1)
     if rc != 0:

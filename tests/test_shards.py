@@ -1,8 +1,8 @@
 """Scramble shards across ranks: two gloo ranks on the CPU each run the oracle
 on their own scrambles of one RQMC plan (scramble_begin = S r) and gather their
-price statistics to rank 0, whose merge equals the single-process evaluation
-of all 2 S scrambles (value and standard error within 1e-13; the merge and the
-single pass differ by rounding only)."""
+scramble means to rank 0, whose two-pass over all 2 S of them equals the
+single-process evaluation of all 2 S scrambles bit for bit (value, standard
+error and bounds)."""
 import multiprocessing as mp
 import os
 import socket
@@ -62,8 +62,15 @@ def test_two_rank_scramble_shards_merge_to_the_whole_plan():
         want = whole.products[k].price
         got = merged[k]
         assert got["effective_sampling_units"] == 2 * SCRAMBLES
-        assert abs(got["value"] - want.value) <= 1e-13 * abs(want.value)
-        assert abs(got["standard_error"] - want.standard_error) <= 1e-12 * want.standard_error
+        assert got["value"] == want.value
+        assert got["standard_error"] == want.standard_error
+        assert (got["confidence_lower"], got["confidence_upper"]) == (want.confidence_lower,
+                                                                      want.confidence_upper)
+        c = whole.products[k].components[A.PRICE]
+        reps = whole.replicate_means(k)
+        st = shards.two_pass(reps)
+        assert (st.sum, st.correction, st.count, st.mean, st.m2) == (c.sum, c.correction, c.count, c.mean,
+                                                                     c.second_moment)
 
 
 def test_merge_is_the_reference_merge():

@@ -339,3 +339,23 @@ def test_documents_follow_the_v3_format_goldens():
     assert set(out["diagnostics"]) == set(golden["diagnostics"])
     for k, v in g["pricing_result_american"].get("risks", {}).items():
         assert set(v) == {"raw", "market_scaled", "raw_unit", "market_scaled_unit"}
+
+
+@pytest.mark.parametrize("case", [c for c in LV.cases() if "vega_kt" in c], ids=lambda c: c["name"])
+def test_replicable_vega_kt_is_not_reported_by_node_allocation(case):
+    """A European under local volatility whose expiry is a reporting maturity:
+    the reference reports its VegaKT by terminal replication
+    (crates/pricing/src/engine/risk/vegakt_terminal_replication.rs:10-40), so
+    the wire layer refuses rather than return the node allocation; with payoff
+    smoothing the reference keeps node allocation, and so does the wire layer."""
+    req = wire.compile_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    assert req.vega_kt["policy"] == wire.TERMINAL_REPLICATION
+    with pytest.raises(wire.UnsupportedRequest, match="terminal-replication"):
+        wire.price_request(case["request"], reduction_block_size=case["reduction_block_size"])
+    smoothed = copy.deepcopy(case["request"])
+    smoothed["risk"]["payoff_smoothing"] = {"type": "compact_c2", "half_width": 0.5}
+    assert wire.compile_request(smoothed).vega_kt["policy"] == wire.NODE_ALLOCATION
+    off_basis = copy.deepcopy(case["request"])
+    basis = off_basis["model"]["reporting_iv_basis"]
+    basis["maturity_nodes"] = [t for t in basis["maturity_nodes"] if t != 1.0] + [1.5]
+    assert wire.compile_request(off_basis).vega_kt["policy"] == wire.NODE_ALLOCATION

@@ -89,3 +89,21 @@ def test_rejects_what_it_does_not_price(engine):
     with pytest.raises(N.EngineError) as err:
         price(engine.mcg_price_european_noalloc, spec)
     assert err.value.name == "unsupported"
+
+
+def test_rejects_what_plan_create_rejects(engine):
+    """The same descriptor checks as mcg_plan_create: a non-finite discount
+    factor is a market error, a seasoned state on a terminal product is
+    unsupported -- for both entry points."""
+    spec = W.european_bs(paths=1024)
+    spec.discount_factors = (1.0, float("inf"))
+    for entry in (engine.mcg_price, engine.mcg_price_european_noalloc):
+        with pytest.raises(N.EngineError) as err:
+            price(entry, spec)
+        assert err.value.name == "market"
+    spec = W.european_bs(paths=1024)
+    spec.products[0].initial_state = 0.0  # has_initial_state set
+    for entry in (engine.mcg_price, engine.mcg_price_european_noalloc):
+        with pytest.raises(N.EngineError) as err:
+            price(entry, spec)
+        assert err.value.name == "unsupported"
