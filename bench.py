@@ -315,7 +315,7 @@ def path_risk_secondary(units: int = 1 << 20, cpu_units: int = 1 << 14):
     return out
 
 
-def european_secondary(paths: int = 1 << 20, cpu_units: int = 1 << 18):
+def european_secondary(paths: int = 1 << 20, cpu_units: int = 1 << 24):
     """The plain European configuration: a Black--Scholes call S = K = 100,
     r = 3 %, q = 1 %, sigma = 20 %, T = 1, one exact lognormal step, `paths`
     pseudo paths (seed 0x0123456789abcdef), FP64, price with pathwise Delta and

@@ -142,10 +142,13 @@ __device__ __forceinline__ double interp_variance(const GridView& g, int tc, dou
     return lower * (1.0 - tw) + upper * tw;
 }
 
-// The path kernels' form of interp_variance: the same clamp, cell walk and
-// bilinear weights, with the walk comparing the nodes themselves (finite
-// nodes: the same cells as total_cmp, and at a node both neighbouring cells
-// give its value) and the x weight as a product with the reciprocal width.
+// The path kernels' form of interp_variance: the same clamp and cell walk,
+// with the walk comparing the nodes themselves (finite nodes: the same cells
+// as total_cmp, and at a node both neighbouring cells give its value), the x
+// weight as a product with the reciprocal width, and each linear
+// interpolation a + (b - a) w as one fused multiply-add (the reference's
+// a (1 - w) + b w to rounding: the variance enters the path only through
+// the step, whose results are held to 1e-12 of the reference, not to the bit).
 __device__ __forceinline__ double interp_variance_walk(const GridView& g, int tc, double tw, double xq,
                                                        int& hint) {
     double xv = xq;
@@ -159,9 +162,10 @@ __device__ __forceinline__ double interp_variance_walk(const GridView& g, int tc
     const double xw = (xv - g.x[c]) * g.inv_dx[c];
     const double* row = g.v + static_cast<size_t>(tc) * g.nx;
     const double* next = row + g.nx;
-    const double lower = row[c] * (1.0 - xw) + row[c + 1] * xw;
-    const double upper = next[c] * (1.0 - xw) + next[c + 1] * xw;
-    return lower * (1.0 - tw) + upper * tw;
+    const double r0 = row[c], r1 = row[c + 1], n0 = next[c], n1 = next[c + 1];
+    const double lower = fma(r1 - r0, xw, r0);
+    const double upper = fma(n1 - n0, xw, n0);
+    return fma(upper - lower, tw, lower);
 }
 
 // ------------------------------------------------------- CTA reduction

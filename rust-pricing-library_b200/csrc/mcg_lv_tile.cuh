@@ -150,9 +150,9 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             continue;
         }
         if (op.kind == kOpInterior) {
+            // wl W_L + wr W_R + sd z (bridge.rs:290-305), the sums fused
             const double z = next_normal(op.rank);
-            w[op.out * kThreads] =
-                op.wl * w[op.left * kThreads] + op.wr * w[op.right * kThreads] + op.sd * z;
+            w[op.out * kThreads] = fma(op.wl, w[op.left * kThreads], fma(op.wr, w[op.right * kThreads], op.sd * z));
             continue;
         }
         const uint32_t s = static_cast<uint32_t>(op.step);
@@ -166,6 +166,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
         const double tw = st.time_weight;
         const double dt = st.dt;
         const double sq = st.sqrt_dt;
+        const double mhdt = -0.5 * dt;  // exact: (-0.5 v) dt and v (-0.5 dt) round alike
         const int32_t obs = st.obs_next;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -187,7 +188,8 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                                          prev_v[e], v, P.dt[s - 1], failed);
             }
             const double ratio = which == 0 ? st.ratio : P.ratio[static_cast<size_t>(which) * steps + s];
-            const double incr = -0.5 * v * dt + sqrt(v) * sq * z;
+            // -v dt / 2 + sqrt(v) sqrt(dt) z with the last product and the sum fused
+            const double incr = fma(sqrt(v) * sq, z, v * mhdt);
             const double e_factor = ratio * exp(incr);
             xs[e] += incr;
             if (CB != 0) {
