@@ -12,7 +12,8 @@
 // the tiles per work item by the host's autotuner) pulls work items from a
 // queue ordered heaviest first (longest-processing-time first: step count x
 // tiles), one atomicAdd per item and no waiting.  An item stages its trade's
-// plan (and local-variance grid) into shared memory and evaluates its tiles;
+// plan (and the cell bounds of its local-variance grid) into shared memory and
+// evaluates its tiles;
 // tile records land at the trade's tile positions, so the reduction that
 // follows is the single-plan one.
 //
@@ -30,10 +31,8 @@ __global__ void __launch_bounds__(kThreads) book_kernel(const BookLaunch L) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_item;
     DevicePlan& P = *reinterpret_cast<DevicePlan*>(smem_raw);
-    double* s_v = reinterpret_cast<double*>(smem_raw + align16(sizeof(DevicePlan)));
-    double* s_x = s_v + L.max_values;
-    double* s_xk = s_x + L.max_nodes;  // reciprocal cell widths
-    double* s_w = reinterpret_cast<double*>(s_xk + L.max_nodes);
+    double2* s_b = reinterpret_cast<double2*>(smem_raw + align16(sizeof(DevicePlan)));  // cell bounds
+    double* s_w = reinterpret_cast<double*>(s_b + L.max_nodes);
     Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(L.max_slots) * kThreads);
     for (;;) {
         __syncthreads();  // the previous item is done with the shared plan and grid
@@ -48,15 +47,13 @@ __global__ void __launch_bounds__(kThreads) book_kernel(const BookLaunch L) {
         __syncthreads();
         const int nx = static_cast<int>(P.nx);
         if (item.path == kBookLocalVol) {
-            const size_t nv = static_cast<size_t>(P.nt) * P.nx;
-            for (size_t i = threadIdx.x; i < nv; i += kThreads) s_v[i] = P.grid_v[i];
-            for (int i = threadIdx.x; i < nx; i += kThreads) {
-                s_x[i] = P.grid_x[i];
-                s_xk[i] = i + 1 < nx ? 1.0 / (P.grid_x[i + 1] - P.grid_x[i]) : 0.0;
-            }
+            for (int i = threadIdx.x; i + 1 < nx; i += kThreads) s_b[i] = make_double2(P.grid_x[i], P.grid_x[i + 1]);
             __syncthreads();
         }
-        const GridView g{s_v, s_x, nullptr, nx, s_xk};
+        // The grid's cell records are read through L1, the cell bounds from shared memory.
+        const GridView g{nullptr, nullptr, nullptr, nx, s_b, P.grid_cells,
+                         item.path == kBookLocalVol ? P.grid_x[0] : 0.0,
+                         item.path == kBookLocalVol ? P.grid_x[nx - 1] : 0.0};
         const uint32_t mask = L.masks[item.trade];
         ErrorWord* err = L.errors + item.trade;
         for (uint32_t t = 0; t < item.tiles; ++t) {
@@ -77,7 +74,8 @@ __global__ void __launch_bounds__(kThreads) book_kernel(const BookLaunch L) {
 }  // namespace
 
 size_t book_smem_bytes(uint32_t max_values, uint32_t max_nodes, uint32_t max_slots) {
-    return align16(sizeof(DevicePlan)) + (static_cast<size_t>(max_values) + 2 * max_nodes) * sizeof(double) +
+    (void)max_values;  // the grid values are read through L1
+    return align16(sizeof(DevicePlan)) + static_cast<size_t>(max_nodes) * sizeof(double2) +
            static_cast<size_t>(max_slots) * kThreads * sizeof(double) + 4 * kComponents * sizeof(Stat);
 }
 

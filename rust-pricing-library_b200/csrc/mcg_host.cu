@@ -368,6 +368,9 @@ struct mcg_plan {
         obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, grid_vol2, weights;
     DeviceArray<int32_t> obs_of_node, time_cell;
     DeviceArray<LvStep> lv_steps;
+    DeviceArray<int4> step_prog;
+    DeviceArray<BridgeNode> bridge_nodes;
+    DeviceArray<double2> grid_cells;
     DeviceArray<uint32_t> scr_dirs, scr_shift, scr_low, directions;
     DeviceArray<StatRecord> partials, records;
     DeviceArray<ErrorWord> error;
@@ -405,6 +408,9 @@ struct mcg_plan {
         obs_of_node.release();
         time_cell.release();
         lv_steps.release();
+        step_prog.release();
+        bridge_nodes.release();
+        grid_cells.release();
         scr_dirs.release();
         scr_shift.release();
         scr_low.release();
@@ -704,6 +710,19 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
             MCG_CUDA(plan.lv_steps.upload(packed));
             P.lv_steps = plan.lv_steps.ptr;
         }
+        {
+            // {v[t][c], slope of cell c} per row: the path tiles' bilinear form.
+            const uint32_t ncell = g.log_moneyness_count - 1;
+            std::vector<double2> cells(static_cast<size_t>(g.time_count) * ncell);
+            for (uint32_t t = 0; t < g.time_count; ++t)
+                for (uint32_t c = 0; c < ncell; ++c) {
+                    const double* row = gv.data() + static_cast<size_t>(t) * g.log_moneyness_count;
+                    const double inv = 1.0 / (gx[c + 1] - gx[c]);
+                    cells[static_cast<size_t>(t) * ncell + c] = make_double2(row[c], (row[c + 1] - row[c]) * inv);
+                }
+            MCG_CUDA(plan.grid_cells.upload(cells));
+            P.grid_cells = plan.grid_cells.ptr;
+        }
         MCG_CUDA(plan.node_time.upload(nodes));
         MCG_CUDA(plan.dt.upload(dtv));
         MCG_CUDA(plan.sqrt_dt.upload(sq));
@@ -772,6 +791,42 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         MCG_CUDA(plan.ops.upload(ops));
         P.ops = plan.ops.ptr;
         P.op_count = static_cast<uint32_t>(ops.size());
+        {
+            // The path tiles' form of the program: per step, the bridge nodes
+            // produced just before it and its bracketing slots.
+            std::vector<int4> prog(steps, make_int4(0, 0, -1, -1));
+            std::vector<BridgeNode> bnodes;
+            int32_t zero_slot = 0;
+            size_t pending = 0;
+            uint32_t next_step = 0;
+            for (const Op& op : ops) {
+                if (op.kind == kOpZero) {
+                    zero_slot = op.out;
+                } else if (op.kind == kOpTerminal) {
+                    bnodes.push_back(BridgeNode{0.0, 0.0, op.sd, op.out, zero_slot, zero_slot, op.rank});
+                } else if (op.kind == kOpInterior) {
+                    bnodes.push_back(BridgeNode{op.wl, op.wr, op.sd, op.out, op.left, op.right, op.rank});
+                } else {
+                    if (op.step != static_cast<int32_t>(next_step))
+                        return fail(MCG_ERR_BRIDGE, "internal: path program steps out of order");
+                    int4& r = prog[next_step++];
+                    r.x = static_cast<int32_t>(pending);
+                    r.y = static_cast<int32_t>(bnodes.size() - pending);
+                    pending = bnodes.size();
+                    if (op.kind == kOpStep) {
+                        r.z = op.left;
+                        r.w = op.right;
+                    }
+                }
+            }
+            if (next_step != steps || pending != bnodes.size())
+                return fail(MCG_ERR_BRIDGE, "internal: path program does not end with a step");
+            MCG_CUDA(plan.step_prog.upload(prog));
+            P.step_prog = plan.step_prog.ptr;
+            MCG_CUDA(plan.bridge_nodes.upload(bnodes));
+            P.bridge_nodes = plan.bridge_nodes.ptr;
+            P.zero_slot = zero_slot;
+        }
         std::vector<uint32_t> ranks;
         for (const Op& op : ops)
             if (op.kind == kOpTerminal || op.kind == kOpInterior || op.kind == kOpStepDirect)

@@ -117,10 +117,15 @@ struct GridView {
     const double* x;        // nx nodes
     const long long* xkey;  // total-order keys of the nodes
     int nx;
-    const double* inv_dx;   // nx - 1 reciprocal cell widths (interp_variance_walk)
+    // interp_variance_walk (the path tiles): cell bounds {x[c], x[c+1]}
+    // (nx - 1, shared memory), the cells {v[t][c], slope} of every row
+    // (DevicePlan::grid_cells, through L1) and the clamp interval.
+    const double2* bounds;
+    const double2* cells;
+    double x_first, x_last;
 };
 // A view carries either xkey (for interp_variance: the LSM path store and the
-// adjoint sweep) or inv_dx (for interp_variance_walk: the path tiles).
+// adjoint sweep) or bounds and cells (for interp_variance_walk: the path tiles).
 
 
 __device__ __forceinline__ double interp_variance(const GridView& g, int tc, double tw, double xq,
@@ -142,29 +147,31 @@ __device__ __forceinline__ double interp_variance(const GridView& g, int tc, dou
     return lower * (1.0 - tw) + upper * tw;
 }
 
-// The path kernels' form of interp_variance: the same clamp and cell walk,
-// with the walk comparing the nodes themselves (finite nodes: the same cells
-// as total_cmp, and at a node both neighbouring cells give its value), the x
-// weight as a product with the reciprocal width, and each linear
-// interpolation a + (b - a) w as one fused multiply-add (the reference's
-// a (1 - w) + b w to rounding: the variance enters the path only through
-// the step, whose results are held to 1e-12 of the reference, not to the bit).
+// The path kernels' form of interp_variance: the same clamp and cell as the
+// reference's total-order search (a walk from the previous cell: up while
+// x[c+1] <= x, down while x[c] > x, within [0, nx - 2] -- for finite,
+// strictly increasing nodes the last node <= x, the ends clamped), one
+// 16-byte shared load per cell visited; each row's linear interpolation
+// v[t][c] + slope (x - x[c]) as one fused multiply-add from the row's cell
+// record, and the time interpolation lower + (upper - lower) tw as another.
+// The reference's a (1 - w) + b w to rounding: the variance enters the path
+// only through the step, whose results are held to 1e-12 of the reference.
 __device__ __forceinline__ double interp_variance_walk(const GridView& g, int tc, double tw, double xq,
                                                        int& hint) {
     double xv = xq;
-    if (xq < g.x[0]) xv = g.x[0];
-    else if (xq > g.x[g.nx - 1]) xv = g.x[g.nx - 1];
-    int count = min(hint + 1, g.nx);
-    while (count < g.nx && g.x[count] <= xv) ++count;
-    while (count > 0 && g.x[count - 1] > xv) --count;
-    const int c = min(max(count - 1, 0), g.nx - 2);
+    if (xq < g.x_first) xv = g.x_first;
+    else if (xq > g.x_last) xv = g.x_last;
+    int c = hint;
+    double2 b = g.bounds[c];
+    while (c < g.nx - 2 && b.y <= xv) b = g.bounds[++c];
+    while (c > 0 && b.x > xv) b = g.bounds[--c];
     hint = c;
-    const double xw = (xv - g.x[c]) * g.inv_dx[c];
-    const double* row = g.v + static_cast<size_t>(tc) * g.nx;
-    const double* next = row + g.nx;
-    const double r0 = row[c], r1 = row[c + 1], n0 = next[c], n1 = next[c + 1];
-    const double lower = fma(r1 - r0, xw, r0);
-    const double upper = fma(n1 - n0, xw, n0);
+    const double dx = xv - b.x;
+    const double2* row = g.cells + static_cast<size_t>(tc) * (g.nx - 1) + c;
+    const double2 lo = row[0];
+    const double2 hi = row[g.nx - 1];
+    const double lower = fma(lo.y, dx, lo.x);
+    const double upper = fma(hi.y, dx, hi.x);
     return fma(upper - lower, tw, lower);
 }
 

@@ -15,35 +15,47 @@
 
 namespace mcg {
 
-// Occupancy: one evolution with at most two products runs 7 CTAs of 128
-// threads (<= 72 registers; an 8-byte spill), 5 with a continuous barrier; the
-// multi-evolution (antithetic, CRN) kernels keep their registers.  The grid
-// values are read through L1 (24.8 KB for 31 x 100), so shared memory holds
-// only the x nodes and the bridge slots and does not limit occupancy.
-template <int E, int NP, int RQ, int CB>
-__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (CB == 0 ? 7 : 5) : 1) lv_path_kernel(const DevicePlan P, uint64_t unit_begin,
-                                                           StatRecord* partials, uint32_t mask,
-                                                           ErrorWord* err, int detail) {
+// Occupancy: one evolution with at most two discrete products runs two paths
+// per thread (Q = 2: two tiles per CTA, their dependency chains interleaved
+// and the per-step record, grid rows, product dispatch and Sobol direction
+// rows shared) at 5 CTAs of 128 threads per SM (96 registers); one path per
+// thread runs 7 CTAs, 5 with a continuous barrier; the multi-evolution
+// (antithetic, CRN) kernels already carry several chains per thread.  The grid values are read through L1 (24.8 KB for
+// 31 x 100), so shared memory holds only the x nodes, the bridge slots and the
+// batched normals.
+template <int E, int NP, int RQ, int CB, int Q>
+__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (Q == 2 ? 5 : (CB == 0 ? 7 : 5)) : 1)
+    lv_path_kernel(const DevicePlan P, uint64_t unit_begin, StatRecord* partials, uint32_t mask, ErrorWord* err,
+                   int detail) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = static_cast<int>(P.nx);
-    double* s_x = reinterpret_cast<double*>(smem_raw);
-    double* s_idx = s_x + nx;                            // reciprocal cell widths
-    double* s_w = s_idx + nx;                            // bridge slots [slot][thread]
-    Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(P.slot_count) * kThreads);
-    double* s_z = reinterpret_cast<double*>(s_red + 4 * kComponents);       // batched normals [k][thread]
-    uint16_t* s_zlist = reinterpret_cast<uint16_t*>(s_z + kZBatch * kThreads);  // tail lists, per warp
-    for (int i = threadIdx.x; i < nx; i += kThreads) {
-        s_x[i] = P.grid_x[i];
-        s_idx[i] = i + 1 < nx ? 1.0 / (P.grid_x[i + 1] - P.grid_x[i]) : 0.0;
-    }
+    double2* s_b = reinterpret_cast<double2*>(smem_raw);  // cell bounds {x[c], x[c+1]}
+    double* s_w = reinterpret_cast<double*>(s_b + nx);    // bridge slots [q][slot][thread]
+    Stat* s_red = reinterpret_cast<Stat*>(s_w + static_cast<size_t>(Q) * P.slot_count * kThreads);
+    double* s_z = reinterpret_cast<double*>(s_red + 4 * kComponents);       // batched normals [k][q][thread]
+    uint16_t* s_zlist = reinterpret_cast<uint16_t*>(s_z + z_batch<Q>() * Q * kThreads);  // tail lists, per warp
+    for (int i = threadIdx.x; i + 1 < nx; i += kThreads) s_b[i] = make_double2(P.grid_x[i], P.grid_x[i + 1]);
     __syncthreads();
-    const GridView g{P.grid_v, s_x, nullptr, nx, s_idx};  // grid values through L1
+    // cell records through L1, bounds in shared memory
+    const GridView g{nullptr, nullptr, nullptr, nx, s_b, P.grid_cells, P.grid_x[0], P.grid_x[nx - 1]};
     const uint32_t scramble = blockIdx.y;
-    const uint64_t point = unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
-    const bool valid = point < unit_begin + (detail ? 1 : P.units) && point < P.units;
-    StatRecord* tile_out = partials + (static_cast<size_t>(scramble) * gridDim.x + blockIdx.x) * P.product_count * kComponents;
-    lv_tile<E, NP, RQ, CB>(P, g, s_w, s_red, scramble, point, valid, tile_out, mask, err, detail,
-                           (unit_begin & 31u) == 0, s_z, s_zlist);
+    const size_t rec = static_cast<size_t>(P.product_count) * kComponents;
+    if constexpr (Q == 1) {
+        const uint64_t point = unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+        const bool valid = point < unit_begin + (detail ? 1 : P.units) && point < P.units;
+        StatRecord* tile_out = partials + (static_cast<size_t>(scramble) * gridDim.x + blockIdx.x) * rec;
+        lv_tile<E, NP, RQ, CB>(P, g, s_w, s_red, scramble, point, valid, tile_out, mask, err, detail,
+                               (unit_begin & 31u) == 0, s_z, s_zlist);
+    } else {
+        // The whole plan from unit 0: CTA b holds tiles 2b and 2b + 1.
+        const uint64_t tiles = (P.units + kThreads - 1) / kThreads;
+        const uint64_t tile = static_cast<uint64_t>(blockIdx.x) * Q;
+        const uint64_t point = tile * kThreads + threadIdx.x;
+        StatRecord* base = partials + static_cast<size_t>(scramble) * tiles * rec;
+        StatRecord* second = tile + 1 < tiles ? base + (tile + 1) * rec : nullptr;
+        lv_tile<E, NP, RQ, CB, Q>(P, g, s_w, s_red, scramble, point, point < P.units, base + tile * rec, mask, err,
+                                  detail, true, s_z, s_zlist, point + kThreads < P.units, second);
+    }
 }
 
 
@@ -153,7 +165,17 @@ cudaError_t launch_lsm_lv_spots(const DevicePlan& P, uint32_t domain, double* sp
     return P.antithetic ? go(lsm_lv_spots_kernel<2>) : go(lsm_lv_spots_kernel<1>);
 }
 
-// Launch helper: picks the instantiation for (evolutions, products).
+// Shared memory of a path-kernel launch with Q paths per thread.
+size_t lv_path_smem(const DevicePlan& P, int Q) {
+    return (2 * static_cast<size_t>(P.nx)) * sizeof(double) +
+           static_cast<size_t>(Q) * P.slot_count * kThreads * sizeof(double) + 4 * kComponents * sizeof(Stat) +
+           static_cast<size_t>(Q == 2 ? z_batch<2>() : z_batch<1>()) * Q * kThreads * sizeof(double) +
+           (kThreads / 32) * 32 * (Q == 2 ? z_batch<2>() : z_batch<1>()) * Q * sizeof(uint16_t);
+}
+
+// Launch helper: picks the instantiation for (evolutions, products).  A whole
+// plan evaluated from unit 0 with one evolution runs two paths per thread;
+// a re-run of one unit (detail) and the multi-evolution kernels one.
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
                            StatRecord* partials, uint32_t mask, ErrorWord* err, int detail,
                            cudaStream_t stream, int& evolutions_out) {
@@ -162,11 +184,15 @@ cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t un
     const int E = pairs * per;
     evolutions_out = E;
     const int np = static_cast<int>(P.product_count);
-    const size_t smem = (2 * static_cast<size_t>(P.nx)) * sizeof(double) +
-                        static_cast<size_t>(P.slot_count) * kThreads * sizeof(double) +
-                        4 * kComponents * sizeof(Stat) + kZBatch * kThreads * sizeof(double) +
-                        (kThreads / 32) * 32 * kZBatch * sizeof(uint16_t);
-    const dim3 grid(static_cast<unsigned>((units + kThreads - 1) / kThreads), scrambles);
+    bool cb = false;
+    for (int k = 0; k < np; ++k) cb |= P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+    // Two paths per thread pay for discrete products (B200: 87.4 -> 75.8 ms on the
+    // 2^24-path local-vol workload); a continuous barrier's bridge state makes
+    // the pair too large (25.0 -> 32.6 ms), so those kernels keep one.
+    const bool two = E == 1 && np <= 2 && !cb && !detail && unit_begin == 0 && units == P.units;
+    const int Q = two ? 2 : 1;
+    const size_t smem = lv_path_smem(P, Q);
+    const dim3 grid(static_cast<unsigned>((units + kThreads * Q - 1) / (kThreads * Q)), scrambles);
     auto go = [&](auto kernel) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(smem));
@@ -174,25 +200,31 @@ cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t un
         kernel<<<grid, kThreads, smem, stream>>>(P, unit_begin, partials, mask, err, detail);
         return cudaGetLastError();
     };
-    bool cb = false;
-    for (int k = 0; k < np; ++k) cb |= P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
     const bool rq = P.engine == MCG_ENGINE_RQMC;
-    // (evolutions, products) x (engine, continuous barrier) instantiations
-#define MCG_LV_PICK(EE, NN)                                                           \
+    // (evolutions, products, paths per thread) x (engine, continuous barrier) instantiations
+#define MCG_LV_PICK(EE, NN, QQ)                                                       \
     do {                                                                              \
-        if (rq && cb) return go(lv_path_kernel<EE, NN, 1, 1>);                        \
-        if (rq) return go(lv_path_kernel<EE, NN, 1, 0>);                              \
-        if (cb) return go(lv_path_kernel<EE, NN, 0, 1>);                              \
-        return go(lv_path_kernel<EE, NN, 0, 0>);                                      \
+        if (rq && cb) return go(lv_path_kernel<EE, NN, 1, 1, QQ>);                    \
+        if (rq) return go(lv_path_kernel<EE, NN, 1, 0, QQ>);                          \
+        if (cb) return go(lv_path_kernel<EE, NN, 0, 1, QQ>);                          \
+        return go(lv_path_kernel<EE, NN, 0, 0, QQ>);                                  \
     } while (0)
-    if (E == 1 && np == 1) MCG_LV_PICK(1, 1);
-    if (E == 1 && np == 2) MCG_LV_PICK(1, 2);
-    if (E == 1 && np <= 4) MCG_LV_PICK(1, 4);
-    if (E == 2 && np == 1) MCG_LV_PICK(2, 1);
-    if (E == 2 && np == 2) MCG_LV_PICK(2, 2);
-    if (E == 3 && np == 1) MCG_LV_PICK(3, 1);
-    if (E == 3 && np == 2) MCG_LV_PICK(3, 2);
-    if (E == 6 && np == 1) MCG_LV_PICK(6, 1);
+    if (two && np == 1) {
+        if (rq) return go(lv_path_kernel<1, 1, 1, 0, 2>);
+        return go(lv_path_kernel<1, 1, 0, 0, 2>);
+    }
+    if (two && np == 2) {
+        if (rq) return go(lv_path_kernel<1, 2, 1, 0, 2>);
+        return go(lv_path_kernel<1, 2, 0, 0, 2>);
+    }
+    if (E == 1 && np == 1) MCG_LV_PICK(1, 1, 1);
+    if (E == 1 && np == 2) MCG_LV_PICK(1, 2, 1);
+    if (E == 1 && np <= 4) MCG_LV_PICK(1, 4, 1);
+    if (E == 2 && np == 1) MCG_LV_PICK(2, 1, 1);
+    if (E == 2 && np == 2) MCG_LV_PICK(2, 2, 1);
+    if (E == 3 && np == 1) MCG_LV_PICK(3, 1, 1);
+    if (E == 3 && np == 2) MCG_LV_PICK(3, 2, 1);
+    if (E == 6 && np == 1) MCG_LV_PICK(6, 1, 1);
 #undef MCG_LV_PICK
     return cudaErrorNotSupported;
 }

@@ -58,44 +58,65 @@ MCG_HD bool monitored(const ProductParams& p, uint32_t obs) {
     return p.weights == nullptr || p.weights[obs] != 0.0;
 }
 
-// Observation update: discrete products (compile.rs:159-202 Asian, :204-403
+// Observation update of one product on N paths with one dispatch on the
+// product's kind: discrete products (compile.rs:159-202 Asian, :204-403
 // discrete barrier, :405-474 lookback, tape.rs:1038-1080 opcode semantics).
-MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
-                                           double spot, double smoothing, bool& failed) {
-    (void)failed;
-    s.terminal = spot;
+template <int N>
+MCG_HD void acc_observe_n(const ProductParams& p, ProductAcc (&s)[N], uint32_t obs, const double (&spot)[N],
+                          double smoothing) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) s[i].terminal = spot[i];
     switch (p.kind) {
-    case MCG_PRODUCT_ASIAN:
-        s.a = s.a + spot * p.weights[obs];
+    case MCG_PRODUCT_ASIAN: {
+        const double w = p.weights[obs];
+#pragma unroll
+        for (int i = 0; i < N; ++i) s[i].a = s[i].a + spot[i] * w;
         break;
+    }
     case MCG_PRODUCT_LOOKBACK:
         if (!monitored(p, obs)) break;
-        if (s.counts == 0u) {
-            s.a = spot;
-            s.counts = 1u;
-        } else if (p.side == MCG_CALL) {
-            if (!(s.a >= spot)) s.a = spot;
-        } else {
-            if (!(s.a <= spot)) s.a = spot;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            if (s[i].counts == 0u) {
+                s[i].a = spot[i];
+                s[i].counts = 1u;
+            } else if (p.side == MCG_CALL) {
+                if (!(s[i].a >= spot[i])) s[i].a = spot[i];
+            } else {
+                if (!(s[i].a <= spot[i])) s[i].a = spot[i];
+            }
         }
         break;
     case MCG_PRODUCT_DISCRETE_BARRIER: {
         if (!monitored(p, obs)) break;
-        const double dist =
-            p.barrier_direction == MCG_BARRIER_UP ? spot - p.barrier : p.barrier - spot;
-        double w;
-        if (smoothing > 0.0) {
-            double comp;
-            w = smooth_indicator(smoothing, dist, comp).value;
-        } else {
-            w = dist >= 0.0 ? 1.0 : 0.0;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const double dist =
+                p.barrier_direction == MCG_BARRIER_UP ? spot[i] - p.barrier : p.barrier - spot[i];
+            double w;
+            if (smoothing > 0.0) {
+                double comp;
+                w = smooth_indicator(smoothing, dist, comp).value;
+            } else {
+                w = dist >= 0.0 ? 1.0 : 0.0;
+            }
+            s[i].a = s[i].a + (1.0 - s[i].a) * w;
         }
-        s.a = s.a + (1.0 - s.a) * w;
         break;
     }
     default:
         break;
     }
+}
+
+// The same update on one path.
+MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
+                                           double spot, double smoothing, bool& failed) {
+    (void)failed;
+    ProductAcc one[1] = {s};
+    const double at[1] = {spot};
+    acc_observe_n<1>(p, one, obs, at, smoothing);
+    s = one[0];
 }
 
 // ---------------------------------------------- continuous barrier bridge

@@ -49,6 +49,21 @@ struct __align__(16) LvStep {
     int32_t obs_next;  // observation index of node s + 1, or -1
 };
 
+// The path tiles' program, one int4 per step: the Brownian-bridge nodes
+// produced just before the step, bridge_nodes[x, x + y), and the slots of the
+// step's two bracketing values W(t_s), W(t_{s+1}) in z, w (-1: the step takes
+// its normal directly, dimension s).  The tiles walk the steps with no
+// per-op dispatch, reading this record before the nodes and the step's
+// constants after them.
+// One Brownian-bridge node of the path tiles: W[out] = wl W[left] + wr W[right]
+// + sd z[rank].  The terminal node is the same form with wl = wr = 0 and both
+// reads from the W(0) slot, which holds 0.0 when the terminal is produced
+// (it is the first node of every program), so it is sd z bit for bit.
+struct __align__(16) BridgeNode {
+    double wl, wr, sd;
+    int32_t out, left, right, rank;
+};
+
 struct ProductParams {
     int32_t kind, side;
     double strike, notional;
@@ -94,6 +109,9 @@ struct DevicePlan {
     const float* ratio_f;        // FP32 bulk: base forward ratios F_{i+1}/F_i (steps)
     const float4* step_f;        // FP32 bulk: per step {dt, sqrt(dt), time weight, 1/sqrt(dt)}
     const LvStep* lv_steps;      // LV: the base runtime's per-step constants, packed
+    const int4* step_prog;       // LV: the path tiles' program, one record per step
+    const BridgeNode* bridge_nodes;  // LV: the bridge nodes of the path tiles, in program order
+    int32_t zero_slot;           // LV bridge: the slot holding W(0) = 0 at the start of a path
 
     // Black--Scholes observation data (observation_count entries)
     const double* obs_time;
@@ -107,6 +125,9 @@ struct DevicePlan {
     const double* grid_x;
     const double* grid_v;
     const double* grid_vol2;     // 2 sqrt(v) of every grid value (local Vega per node adjoint)
+    // Per row t and x cell c: {v[t][c], (v[t][c+1] - v[t][c]) / (x[c+1] - x[c])}, the
+    // path tiles' form of the grid (nt x (nx - 1) entries, read through L1)
+    const double2* grid_cells;
     const float* grid_v_f;
     uint32_t nt, nx;
 
