@@ -130,6 +130,24 @@ typedef struct mcg_local_variance_grid {
     double cap;
 } mcg_local_variance_grid;
 
+/* Discrete dividends of the escrowed affine model, AffineDividendTransform
+ * with the plan's discount and dividend curves as carry curves
+ * (crates/pricing/src/market/dividend.rs:137-520, market/forward.rs:129-160):
+ * ex-dividend times (ACT/365F year fractions, finite, >= 0, strictly
+ * increasing), fixed cash amounts (finite, >= 0) and proportional fractions
+ * (in [0, 1)).  The simulated state f is the canonical continuous martingale
+ * with forward S0 Dq(t)/Dr(t); every observed spot is S = A(t) S0 + B(t) f(t),
+ * A the discounted cash reserve still to be paid and B the proportional
+ * factor, and an observation on an ex-dividend date of a discrete barrier
+ * also checks the spot just before the dividend.  A local-volatility plan adds
+ * the ex-times up to expiry to its time grid.  count = 0: no dividends. */
+typedef struct mcg_dividends {
+    uint32_t count;
+    const double* ex_times;
+    const double* fixed_cash;
+    const double* proportional;
+} mcg_dividends;
+
 /* One product.  All products of one plan observe the same dates
  * (`observation_times` of the plan); the product's own arrays index those. */
 typedef struct mcg_product_desc {
@@ -214,6 +232,12 @@ typedef struct mcg_plan_desc {
     double gamma_bump;                /* relative fraction or absolute amount */
     double smoothing_half_width;      /* PayoffSmoothing::compact_c2; 0 = exact */
     uint32_t checkpoint_interval;     /* LV reverse: steps between stored states */
+    /* Discrete dividends (see mcg_dividends).  With dividends the engine prices
+     * European, Digital, Asian, Lookback and discrete-barrier products:
+     * Black--Scholes with its full pathwise risk, local volatility with price
+     * and CRN Delta/Gamma; continuous barriers, early exercise, local Vega and
+     * node sensitivities, and the FP32 bulk return MCG_ERR_UNSUPPORTED. */
+    mcg_dividends discrete_dividends;
 } mcg_plan_desc;
 
 typedef struct mcg_statistics {

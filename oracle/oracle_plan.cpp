@@ -337,6 +337,119 @@ bool smooth_interval(bool up, double ls, double rs, double lb, double rb, double
     return true;
 }
 
+// ------------------------------------------------------------- dividends
+
+// AffineDividendCoordinate, crates/pricing/src/market/dividend.rs:137-208:
+// the observed spot is a S0 + b f of the canonical state f; spot_scale is its
+// derivative scale under a spot bump with the cash held fixed.
+struct Coord {
+    double a = 0.0, b = 1.0, spot_scale = 1.0;
+    // at_spot, dividend.rs:170-181.
+    Coord at_spot(double original, double spot) const {
+        if (original == spot) return *this;
+        return {a * original / spot, spot_scale - (spot_scale - b) * original / spot, spot_scale};
+    }
+    double spot_of(double s0, double f) const { return a * s0 + b * f; }
+};
+
+struct DividendEvent {
+    double t, cash, alpha, beta;
+};
+
+// AffineDividendTransform::new_with_carry_curves and its coordinates,
+// dividend.rs:283-491 (compile_event :622-642, validation :644-690).
+struct Dividends {
+    std::vector<DividendEvent> ev;
+    double spot = 0.0, reserve = 0.0;
+    const Curve* rc = nullptr;
+    const Curve* qc = nullptr;
+
+    bool compile(const mcg_dividends& d, double s0, const Curve& r, const Curve& q) {
+        ev.clear();
+        spot = s0;
+        rc = &r;
+        qc = &q;
+        for (uint32_t i = 0; i < d.count; ++i) {
+            const double t = d.ex_times[i], cash = d.fixed_cash[i], beta = d.proportional[i];
+            if (!std::isfinite(t) || t < 0.0) return false;
+            if (!(std::isfinite(cash) && cash >= 0.0)) return false;
+            if (!(std::isfinite(beta) && beta >= 0.0 && beta < 1.0)) return false;
+            if (i && !(t > d.ex_times[i - 1])) return false;
+            const double alpha = cash / s0;
+            if (!std::isfinite(alpha)) return false;
+            ev.push_back({t, cash, alpha, beta});
+        }
+        // compile_reserve, dividend.rs:332-354
+        double proportional = 1.0, res = 0.0;
+        for (const auto& e : ev) {
+            proportional *= 1.0 - e.beta;
+            const double discount = std::exp(rc->log_discount(e.t)) / std::exp(qc->log_discount(e.t));
+            res += e.cash / proportional * discount;
+        }
+        const double residual = s0 - res;
+        if (!std::isfinite(res) || !std::isfinite(residual) || residual <= 0.0) return false;
+        reserve = res;
+        return true;
+    }
+    Coord initial() const { return {reserve / spot, (spot - reserve) / spot, 1.0}; }
+    // carry, dividend.rs:366-392
+    Coord carry(Coord c, double start, double end) const {
+        if (c.a == 0.0 || start == end) return c;
+        const double g = qc->log_discount(end) - rc->log_discount(end) - qc->log_discount(start) +
+                         rc->log_discount(start);
+        c.a *= std::exp(g);
+        return c;
+    }
+    // after, dividend.rs:187-208
+    static Coord after(Coord c, const DividendEvent& e) {
+        return {(1.0 - e.beta) * c.a - e.alpha, (1.0 - e.beta) * c.b, (1.0 - e.beta) * c.spot_scale};
+    }
+    // coordinate_after_time, dividend.rs:434-460
+    Coord after_time(double time) const {
+        if (ev.empty()) return Coord{};  // no dividends: the identity
+        Coord c = initial();
+        double prev = 0.0;
+        for (const auto& e : ev) {
+            if (!(e.t <= time)) break;
+            c = carry(c, prev, e.t);
+            c = after(c, e);
+            prev = e.t;
+        }
+        c = carry(c, prev, time);
+        bool settled = true;
+        for (const auto& e : ev) settled = settled && (e.t <= time || e.cash == 0.0);
+        if (settled) c.a = 0.0;
+        return c;
+    }
+    // event_timeline's `before` entry of event i, dividend.rs:492-518
+    Coord before_event(size_t i) const {
+        if (ev.empty()) return Coord{};
+        Coord c = initial();
+        double prev = 0.0;
+        size_t last_cash = ev.size();
+        for (size_t k = ev.size(); k-- > 0;)
+            if (ev[k].cash != 0.0) {
+                last_cash = k;
+                break;
+            }
+        for (size_t k = 0; k < ev.size(); ++k) {
+            const Coord before = carry(c, prev, ev[k].t);
+            if (k == i) return before;
+            Coord aft = after(before, ev[k]);
+            if (last_cash == ev.size() || k >= last_cash) aft.a = 0.0;
+            c = aft;
+            prev = ev[k].t;
+        }
+        return c;
+    }
+    // index of the event at exactly `time`, or -1
+    long event_at(double time) const {
+        for (size_t k = 0; k < ev.size(); ++k)
+            if (bits_of(ev[k].t) == bits_of(time)) return static_cast<long>(k);
+        return -1;
+    }
+};
+
 // ------------------------------------------------------------- the plan
 
 struct Product {
@@ -373,6 +486,16 @@ struct Plan {
     std::vector<Scramble> scr;  // scramble-major, dimension-minor
     uint32_t dimension = 0;
     uint32_t domain = 0;  // RandomDomain of the pseudo stream: Valuation 0, LsmTrain 1
+    // discrete dividends: observation coordinates after (and, on an ex-date,
+    // before) the dividend; local volatility per spot runtime and node, and the
+    // post-dividend spot checks of the ex-date nodes
+    Dividends div;
+    double residual_spot = 0.0;
+    std::vector<Coord> obs_post, obs_pre;
+    std::vector<char> obs_has_pre;
+    std::vector<Coord> node_post[3], node_pre[3];
+    std::vector<char> node_has_pre;
+    std::vector<std::pair<size_t, Coord>> checks[3];
     bool risk_enabled() const { return req_delta || req_gamma || req_vega; }
     bool has_continuous_barrier() const {
         for (const auto& p : products)
@@ -433,6 +556,22 @@ bool build_plan(const mcg_plan_desc* d, Plan& p) {
     p.discount = std::exp(p.rc.log_discount(d->payment_time));
     p.obs_t.assign(d->observation_times, d->observation_times + d->observation_count);
     p.expiry = p.obs_t.back();
+    p.residual_spot = p.spot;
+    if (d->discrete_dividends.count) {
+        if (!p.div.compile(d->discrete_dividends, p.spot, p.rc, p.qc)) return fail("dividends");
+        p.residual_spot = p.spot - p.div.reserve;
+        for (uint32_t i = 0; i < d->product_count; ++i)
+            if (d->products[i].kind == MCG_PRODUCT_CONTINUOUS_BARRIER || d->products[i].kind == MCG_PRODUCT_AMERICAN)
+                return fail("dividends with a continuous barrier or early exercise");
+        if (d->model == MCG_MODEL_LOCAL_VOLATILITY && (d->request_vega || d->request_local_vega_nodes))
+            return fail("local-volatility Vega with dividends");
+    }
+    for (double t : p.obs_t) {
+        p.obs_post.push_back(p.div.after_time(t));
+        const long k = p.div.event_at(t);
+        p.obs_has_pre.push_back(k >= 0);
+        p.obs_pre.push_back(k >= 0 ? p.div.before_event(static_cast<size_t>(k)) : Coord{});
+    }
     for (double t : p.obs_t) p.obs_fwd.push_back(forward_at(p, p.spot, t));
     for (uint32_t i = 0; i < d->product_count; ++i) {
         Product pr;
@@ -450,7 +589,7 @@ bool build_plan(const mcg_plan_desc* d, Plan& p) {
     p.smoothing = d->smoothing_half_width;
     // Validation bumps, crates/pricing/src/engine/compile/simulation.rs:481-502.
     p.gamma_bump = d->gamma_bump_relative ? p.spot * d->gamma_bump : d->gamma_bump;
-    p.spot_bump = p.req_gamma ? p.gamma_bump : std::min(p.spot * 1.0e-4, 0.5 * p.spot);
+    p.spot_bump = p.req_gamma ? p.gamma_bump : std::min(p.spot * 1.0e-4, 0.5 * p.residual_spot);
     if (p.model == MCG_MODEL_BLACK_SCHOLES) {
         p.total_variance = p.vol * p.vol * p.expiry;
         p.vol_bump = p.vol == 0.0 ? 0.0 : std::min(1.0e-4, p.vol * 0.5);
@@ -466,12 +605,37 @@ bool build_plan(const mcg_plan_desc* d, Plan& p) {
             maximum_step = std::max(maximum_step, p.grid.t[i + 1] - p.grid.t[i]);
         std::vector<double> events = p.grid.t;
         events.insert(events.end(), p.obs_t.begin(), p.obs_t.end());
+        // ex-dividend times up to expiry are grid events (compile/local_vol.rs:38-52)
+        for (const auto& e : p.div.ev)
+            if (e.t <= p.expiry) events.push_back(e.t);
         compile_time_grid(events, maximum_step, p.nodes);
         p.bump_spot[0] = p.spot;
         p.bump_spot[1] = p.spot - p.spot_bump;
         p.bump_spot[2] = p.spot + p.spot_bump;
         for (int k = 0; k < 3; ++k)
             for (double t : p.nodes) p.fwd[k].push_back(forward_at(p, p.bump_spot[k], t));
+        // node coordinates of each spot runtime, the transform recompiled at
+        // that spot (local_vol_runtime_for_spot, risk/pathwise_local_vol.rs:51-69)
+        p.node_has_pre.clear();
+        for (double t : p.nodes) p.node_has_pre.push_back(p.div.event_at(t) >= 0);
+        for (int k = 0; k < 3; ++k) {
+            Dividends dk;
+            if (d->discrete_dividends.count &&
+                !dk.compile(d->discrete_dividends, p.bump_spot[k], p.rc, p.qc))
+                return fail("dividends at a bumped spot");
+            for (double t : p.nodes) {
+                p.node_post[k].push_back(dk.after_time(t));
+                const long e = dk.event_at(t);
+                p.node_pre[k].push_back(e >= 0 ? dk.before_event(static_cast<size_t>(e)) : Coord{});
+            }
+            // dividend checkpoints through the horizon (local_vol.rs:326-345)
+            for (const auto& e : dk.ev) {
+                if (!(e.t <= p.nodes.back())) continue;
+                size_t node = 0;
+                while (node < p.nodes.size() && bits_of(p.nodes[node]) != bits_of(e.t)) ++node;
+                p.checks[k].push_back({node, dk.after_time(e.t)});
+            }
+        }
         for (double t : p.obs_t) {
             uint32_t idx = 0;
             for (; idx < p.nodes.size(); ++idx)
@@ -504,7 +668,22 @@ bool build_plan(const mcg_plan_desc* d, Plan& p) {
 
 struct Obs {
     double post_spot, f, w;
+    double pre_spot;   // the ex-date spot before the dividend (has_pre)
+    bool has_pre;
+    Coord post, pre;   // coordinates at the observation's spot runtime
 };
+
+// path_observation, black_scholes.rs:335-354: S = a S0 + b f after (and
+// before) an ex-date's dividend, at the runtime's spot.
+void bs_observe(const Plan& p, size_t i, double f, double w, double spot, Obs& o) {
+    o.f = f;
+    o.w = w;
+    o.post = p.obs_post[i].at_spot(p.spot, spot);
+    o.post_spot = o.post.a * spot + o.post.b * f;
+    o.has_pre = p.obs_has_pre[i] != 0;
+    o.pre = o.has_pre ? p.obs_pre[i].at_spot(p.spot, spot) : o.post;
+    o.pre_spot = o.has_pre ? o.pre.a * spot + o.pre.b * f : o.post_spot;
+}
 
 // path_observations_from_normals, crates/pricing/src/engine/processes/black_scholes.rs:297-331.
 void bs_observations(const Plan& p, const double* z, double spot, double vol, Obs* out) {
@@ -517,7 +696,7 @@ void bs_observations(const Plan& p, const double* z, double spot, double vol, Ob
         const double w = std::sqrt(t) * z[0];
         const double lr = -0.5 * tv + sd * z[0];
         const double f = p.obs_fwd[0] * spot_scale * std::exp(lr);
-        out[0] = {0.0 * spot + 1.0 * f, f, w};
+        bs_observe(p, 0, f, w, spot, out[0]);
         return;
     }
     double prev = 0.0, w = 0.0;
@@ -528,7 +707,7 @@ void bs_observations(const Plan& p, const double* z, double spot, double vol, Ob
         prev = t;
         const double tv = vol * vol * t;
         const double f = p.obs_fwd[i] * spot_scale * std::exp(-0.5 * tv + vol * w);
-        out[i] = {0.0 * spot + 1.0 * f, f, w};
+        bs_observe(p, i, f, w, spot, out[i]);
     }
 }
 
@@ -537,11 +716,19 @@ void bs_observations(const Plan& p, const double* z, double spot, double vol, Ob
 // Hand-lowered payoff graphs of crates/pricing/src/engine/payoff/compile.rs:35-474
 // with the forward/reverse opcode semantics of crates/pricing/src/engine/payoff/tape.rs:594-781,953-1088.
 // `spots` are the observation spots; `adj` (may be null) receives dPayoff/dSpot.
-double payoff_eval(const Product& pr, const double* spots, size_t n, double h, double* adj) {
+// A discrete barrier monitored on an ex-dividend date (has_pre[i]) also sees the
+// spot before the dividend: its distance is the maximum (smoothed: the compact-C2
+// smooth maximum) of the pre- and post-dividend distances
+// (crates/pricing/src/engine/payoff/compile.rs:315-346); pre_adj receives
+// dPayoff/dPreSpot.
+double payoff_eval(const Product& pr, const double* spots, size_t n, double h, double* adj,
+                   const double* pre_spots = nullptr, const char* has_pre = nullptr, double* pre_adj = nullptr) {
     const mcg_product_desc& d = pr.d;
     const bool call = d.side == MCG_CALL;
     if (adj)
         for (size_t i = 0; i < n; ++i) adj[i] = 0.0;
+    if (pre_adj)
+        for (size_t i = 0; i < n; ++i) pre_adj[i] = 0.0;
     switch (d.kind) {
     case MCG_PRODUCT_EUROPEAN: {
         const double s = spots[n - 1];
@@ -613,11 +800,13 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
         const double vanilla = pos * d.notional;
         const bool up = d.barrier_direction == MCG_BARRIER_UP;
         double hit = d.has_initial_state ? d.initial_state : 0.0;  // historical hit, compile.rs:293-297
-        std::vector<double> hist, weights, firsts;
+        std::vector<double> hist, weights, firsts, pre_share, post_share;
         if (adj && h > 0.0) {
             hist.resize(n);
             weights.resize(n);
             firsts.resize(n);
+            pre_share.assign(n, 0.0);
+            post_share.assign(n, 1.0);
         }
         for (size_t i = 0; i < n; ++i) {
             if (!pr.monitored(i)) {
@@ -628,7 +817,20 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
                 }
                 continue;
             }
-            const double dist = up ? spots[i] - d.barrier : d.barrier - spots[i];
+            double dist = up ? spots[i] - d.barrier : d.barrier - spots[i];
+            if (has_pre && has_pre[i]) {
+                const double pre = up ? pre_spots[i] - d.barrier : d.barrier - pre_spots[i];
+                if (h > 0.0) {
+                    const BinaryDeriv m = smooth_maximum(h, pre, dist);
+                    if (adj) {
+                        pre_share[i] = m.left_first;
+                        post_share[i] = m.right_first;
+                    }
+                    dist = m.value;
+                } else {
+                    dist = pre >= dist ? pre : dist;
+                }
+            }
             double wgt;
             if (h > 0.0) {
                 const Deriv dd = indicator(h, dist);
@@ -657,7 +859,9 @@ double payoff_eval(const Product& pr, const double* spots, size_t n, double h, d
                 for (size_t k = n; k-- > 0;) {
                     const double a_w = a_hit * (1.0 - hist[k]);
                     a_hit = a_hit * (1.0 - weights[k]);
-                    adj[k] += (up ? 1.0 : -1.0) * (a_w * firsts[k]);
+                    const double a_dist = a_w * firsts[k];
+                    adj[k] += (up ? 1.0 : -1.0) * (a_dist * post_share[k]);
+                    if (pre_adj && pre_share[k] != 0.0) pre_adj[k] += (up ? 1.0 : -1.0) * (a_dist * pre_share[k]);
                 }
             }
             adj[n - 1] += (in >= 0.0 ? a_vanilla * d.notional : 0.0) * (call ? 1.0 : -1.0);
@@ -875,27 +1079,39 @@ bool bs_pathwise(const Plan& p, const Product& pr, const double* z, double spot,
         const double lr = -0.5 * tv + sd * z[0];
         const double bf = p.obs_fwd[0] * (spot / p.spot);
         const double f = bf * std::exp(lr);
-        const double terminal = 0.0 * spot + 1.0 * f;
+        const Coord c = p.obs_post[0].at_spot(p.spot, spot);
+        const double terminal = c.a * spot + c.b * f;
         double a;
         const double value = payoff_eval(pr, &terminal, 1, p.smoothing, &a);
         out.price = p.discount * value;
-        out.delta = p.discount * a * 1.0 * f / spot;
-        const double tvega = 1.0 * f * (-vol * t + std::sqrt(t) * z[0]);
+        out.delta = p.discount * a * c.spot_scale * f / spot;
+        const double tvega = c.b * f * (-vol * t + std::sqrt(t) * z[0]);
         out.vega = p.discount * a * tvega;
         return true;
     }
     obs.resize(n);
     bs_observations(p, z, spot, vol, obs.data());
-    tmp.resize(2 * n);
+    tmp.resize(4 * n);
     double* spots = tmp.data();
     double* adj = tmp.data() + n;
-    for (size_t i = 0; i < n; ++i) spots[i] = obs[i].post_spot;
-    const double value = payoff_eval(pr, spots, n, p.smoothing, adj);
+    double* pre_spots = tmp.data() + 2 * n;
+    double* pre_adj = tmp.data() + 3 * n;
+    for (size_t i = 0; i < n; ++i) {
+        spots[i] = obs[i].post_spot;
+        pre_spots[i] = obs[i].pre_spot;
+    }
+    const double value = payoff_eval(pr, spots, n, p.smoothing, adj, pre_spots, p.obs_has_pre.data(), pre_adj);
+    // terminal adjoints, then the pre-dividend ones (black_scholes.rs:525-562)
     double delta = 0.0, vega = 0.0;
     for (size_t k = n; k-- > 0;) {
         if (adj[k] == 0.0) continue;
-        delta += adj[k] * 1.0 * obs[k].f / spot;
-        vega += adj[k] * 1.0 * obs[k].f * (-vol * p.obs_t[k] + obs[k].w);
+        delta += adj[k] * obs[k].post.spot_scale * obs[k].f / spot;
+        vega += adj[k] * obs[k].post.b * obs[k].f * (-vol * p.obs_t[k] + obs[k].w);
+    }
+    for (size_t k = n; k-- > 0;) {
+        if (pre_adj[k] == 0.0 || !obs[k].has_pre) continue;
+        delta += pre_adj[k] * obs[k].pre.spot_scale * obs[k].f / spot;
+        vega += pre_adj[k] * obs[k].pre.b * obs[k].f * (-vol * p.obs_t[k] + obs[k].w);
     }
     out.price = p.discount * value;
     out.delta = p.discount * delta;
@@ -953,9 +1169,13 @@ bool bs_unit_product(const Plan& p, const Product& pr, const double* z, double* 
         for (int k = 0; k < 8; ++k) values[10 + k] = base.diag[k];
         return true;
     }
-    tmp.resize(n);
-    for (size_t i = 0; i < n; ++i) tmp[i] = obs[i].post_spot;
-    values[MCG_PRICE] = p.discount * payoff_eval(pr, tmp.data(), n, p.smoothing, nullptr);
+    tmp.resize(2 * n);
+    for (size_t i = 0; i < n; ++i) {
+        tmp[i] = obs[i].post_spot;
+        tmp[n + i] = obs[i].pre_spot;
+    }
+    values[MCG_PRICE] = p.discount * payoff_eval(pr, tmp.data(), n, p.smoothing, nullptr, tmp.data() + n,
+                                                 p.obs_has_pre.data());
     return true;
 }
 
@@ -998,6 +1218,16 @@ bool lv_evolve(const Plan& p, int which, const double* shocks, LvPath& path, Fai
             f = {MCG_ERR_NON_FINITE_STATE, static_cast<uint32_t>(s + 1), state};
             return false;
         }
+        // post-dividend spot of an ex-date node (validate_post_event_f_state,
+        // dividend.rs:557-583, at local_vol.rs:520-545)
+        for (const auto& ck : p.checks[which])
+            if (ck.first == s + 1) {
+                const double post = ck.second.spot_of(p.bump_spot[which], state);
+                if (!std::isfinite(post) || post <= 0.0) {
+                    f = {MCG_ERR_MARKET, static_cast<uint32_t>(s + 1), post};
+                    return false;
+                }
+            }
         path.state[s + 1] = state;
         path.var[s] = in.value;
         path.interp[s] = in;
@@ -1043,9 +1273,16 @@ bool lv_payoff(const Plan& p, const Product& pr, int which, const LvPath& path, 
         if (terms_out) *terms_out = t;
         return true;
     }
-    std::vector<double> spots(n);
-    for (size_t i = 0; i < n; ++i) spots[i] = 0.0 * spot + 1.0 * path.state[p.obs_node[i]];
-    value = p.discount * payoff_eval(pr, spots.data(), n, p.smoothing, nullptr);
+    // local_vol_state_observations, local_vol_valuation.rs:221-247
+    std::vector<double> spots(2 * n);
+    std::vector<char> has_pre(n);
+    for (size_t i = 0; i < n; ++i) {
+        const size_t node = p.obs_node[i];
+        spots[i] = p.node_post[which][node].spot_of(spot, path.state[node]);
+        has_pre[i] = p.node_has_pre[node];
+        spots[n + i] = has_pre[i] ? p.node_pre[which][node].spot_of(spot, path.state[node]) : spots[i];
+    }
+    value = p.discount * payoff_eval(pr, spots.data(), n, p.smoothing, nullptr, spots.data() + n, has_pre.data());
     return true;
 }
 

@@ -21,7 +21,7 @@
 // fourteen evaluations read it back; a smoothed discrete barrier also keeps
 // its hit states, weights and weight slopes there for the reverse sweep, a
 // continuous barrier its observed states and node adjoints.
-#include "mcg_kernels.cuh"
+#include "mcg_bs_tile.cuh"
 
 namespace mcg {
 
@@ -69,17 +69,28 @@ __device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const Produ
     ProductAcc acc;
     acc_init(acc, pp);
     int32_t arg = -1;  // lookback: observation holding the extremum (-1: the seasoned literal)
+    // With dividends a smoothed barrier also keeps, per observation, the shares
+    // of the pre- and post-dividend distances in the smooth maximum.
+    double* share_tape = h_tape + 3 * static_cast<size_t>(n) * stride;
     for (uint32_t k = 0; k < n; ++k) {
         double w;
         const double f = observe(P, T, k, sign, scale, vol, cached, w);
+        double pre[1];
+        bool with_pre;
+        const double sk[1] = {obs_spot(P, k, spot, f, pre[0], with_pre)};
         if (pp.kind == MCG_PRODUCT_LOOKBACK && monitored(pp, k) &&
-            (acc.counts == 0u || (call ? !(acc.a >= f) : !(acc.a <= f))))
+            (acc.counts == 0u || (call ? !(acc.a >= sk[0]) : !(acc.a <= sk[0]))))
             arg = static_cast<int32_t>(k);
         if (smooth_barrier) {
             // hit state before k, hit weight and its slope (compile.rs:204-403)
-            double weight = 0.0, first = 0.0;
+            double weight = 0.0, first = 0.0, pre_share = 0.0, post_share = 1.0;
             if (monitored(pp, k)) {
-                const double dist = pp.barrier_direction == MCG_BARRIER_UP ? f - pp.barrier : pp.barrier - f;
+                const bool upb = pp.barrier_direction == MCG_BARRIER_UP;
+                double dist = upb ? sk[0] - pp.barrier : pp.barrier - sk[0];
+                if (with_pre) {
+                    const double pd = upb ? pre[0] - pp.barrier : pp.barrier - pre[0];
+                    dist = smooth_maximum(h, pd, dist, pre_share, post_share);
+                }
                 double comp;
                 const SmoothD d = smooth_indicator(h, dist, comp);
                 weight = d.value;
@@ -88,8 +99,14 @@ __device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const Produ
             h_tape[(3 * static_cast<size_t>(k) + 0) * stride] = acc.a;
             h_tape[(3 * static_cast<size_t>(k) + 1) * stride] = weight;
             h_tape[(3 * static_cast<size_t>(k) + 2) * stride] = first;
+            if (P.dividends) {
+                share_tape[(2 * static_cast<size_t>(k) + 0) * stride] = pre_share;
+                share_tape[(2 * static_cast<size_t>(k) + 1) * stride] = post_share;
+            }
         }
-        acc_observe(pp, acc, k, f, h, failed);
+        ProductAcc one[1] = {acc};
+        acc_observe_n<1>(pp, one, k, sk, h, pre, with_pre);
+        acc = one[0];
     }
     const double value = acc_payoff(pp, acc, h);
     // d payoff / d observed spot at the terminal observation and, for the
@@ -142,11 +159,12 @@ __device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const Produ
         break;
     }
     // Reverse sweep, last observation first (the order the tape reverse
-    // pushes the terminal adjoints).
-    double delta = 0.0, vega = 0.0;
+    // pushes the terminal adjoints); the pre-dividend adjoints of a barrier's
+    // ex-dates follow them (black_scholes.rs:525-562).
+    double delta = 0.0, vega = 0.0, delta_pre = 0.0, vega_pre = 0.0;
     const double up_sign = pp.barrier_direction == MCG_BARRIER_UP ? 1.0 : -1.0;
     for (int32_t k = static_cast<int32_t>(n) - 1; k >= 0; --k) {
-        double adj = 0.0;
+        double adj = 0.0, pre_adj = 0.0;
         switch (pp.kind) {
         case MCG_PRODUCT_ASIAN:
             adj = g * pp.weights[k];
@@ -161,7 +179,13 @@ __device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const Produ
                 const double first = h_tape[(3 * static_cast<size_t>(k) + 2) * stride];
                 const double a_w = a_hit * (1.0 - hist);
                 a_hit = a_hit * (1.0 - weight);
-                adj += up_sign * (a_w * first);
+                if (P.dividends) {
+                    const double a_dist = a_w * first;
+                    adj += up_sign * (a_dist * share_tape[(2 * static_cast<size_t>(k) + 1) * stride]);
+                    pre_adj = up_sign * (a_dist * share_tape[(2 * static_cast<size_t>(k) + 0) * stride]);
+                } else {
+                    adj += up_sign * (a_w * first);
+                }
             }
             if (k == static_cast<int32_t>(n) - 1) adj += terminal_adj;
             break;
@@ -169,11 +193,23 @@ __device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const Produ
             if (k == static_cast<int32_t>(n) - 1) adj = terminal_adj;
             break;
         }
-        if (adj == 0.0) continue;
+        if (adj == 0.0 && pre_adj == 0.0) continue;
         double w;
         const double f = observe(P, T, static_cast<uint32_t>(k), sign, scale, vol, cached, w);
-        delta += adj * 1.0 * f / spot;
-        vega += adj * 1.0 * f * (-vol * P.obs_time[k] + w);
+        if (adj != 0.0) {
+            const DivCoord c = obs_coord(P, static_cast<uint32_t>(k), spot);
+            delta += adj * c.spot_scale * f / spot;
+            vega += adj * c.b * f * (-vol * P.obs_time[k] + w);
+        }
+        if (pre_adj != 0.0) {
+            const DivCoord c = div_at_spot(P.obs_div_pre[k], P.spot, spot);
+            delta_pre += pre_adj * c.spot_scale * f / spot;
+            vega_pre += pre_adj * c.b * f * (-vol * P.obs_time[k] + w);
+        }
+    }
+    if (P.dividends) {
+        delta += delta_pre;
+        vega += vega_pre;
     }
     PathAad r;
     r.price = P.discount * value;

@@ -48,19 +48,44 @@ __device__ __forceinline__ double terminal_payoff(const ProductParams& p, double
     return (in >= 0.0 ? in : 0.0) * p.notional;
 }
 
+// The coordinate of observation i at a spot runtime: the plan's dividend
+// coordinate refit to `spot` (AffineDividendCoordinate::at_spot), or the
+// identity (a = 0, b = 1) without dividends.
+__device__ __forceinline__ DivCoord obs_coord(const DevicePlan& P, uint32_t i, double spot) {
+    return P.dividends ? div_at_spot(P.obs_div[i], P.spot, spot) : DivCoord{0.0, 1.0, 1.0};
+}
+
+// The observed spot of state f at observation i and, on an ex-date, the spot
+// before the dividend (path_observation, black_scholes.rs:335-354).
+__device__ __forceinline__ double obs_spot(const DevicePlan& P, uint32_t i, double spot, double f, double& pre,
+                                           bool& with_pre) {
+    with_pre = false;
+    pre = f;
+    if (!P.dividends) return f;
+    const DivCoord c = div_at_spot(P.obs_div[i], P.spot, spot);
+    with_pre = P.obs_div[i].w != 0.0;
+    if (with_pre) {
+        const DivCoord b = div_at_spot(P.obs_div_pre[i], P.spot, spot);
+        pre = b.a * spot + b.b * f;
+    }
+    return c.a * spot + c.b * f;
+}
+
 // pathwise_aad_single_terminal with the exponential supplied by the caller.
 __device__ __forceinline__ Aad single_terminal(const DevicePlan& P, const ProductParams& p,
                                                double spot, double vol, double z, double e_lr) {
     const double t = P.expiry;
     const double bf = P.obs_fwd[0] * (spot / P.spot);
     const double f = bf * e_lr;
-    const double terminal = f;  // 0.0 * spot + 1.0 * f for the identity coordinate
+    const DivCoord c = obs_coord(P, 0, spot);
+    // S = a spot + b f (the identity coordinate: f itself)
+    const double terminal = P.dividends ? c.a * spot + c.b * f : f;
     double a;
     const double value = terminal_payoff(p, terminal, P.smoothing, a);
     Aad r;
     r.price = P.discount * value;
-    r.delta = P.discount * a * 1.0 * f / spot;
-    const double tvega = 1.0 * f * (-vol * t + sqrt(t) * z);
+    r.delta = P.discount * a * c.spot_scale * f / spot;
+    const double tvega = c.b * f * (-vol * t + sqrt(t) * z);
     r.vega = P.discount * a * tvega;
     return r;
 }
@@ -141,15 +166,17 @@ __device__ __forceinline__ void bs_terminal_tile(const DevicePlan& P, Stat* s_re
             }
         } else {
             // discounted_payoff_from_normals, black_scholes.rs:41-55
-            double a;
+            double a, pre;
+            bool with_pre;
             const double t = P.expiry;
             const double tv = P.vol * P.vol * t;
             const double sd = sqrt(tv);
-            double price = P.discount * terminal_payoff(pp, P.obs_fwd[0] * 1.0 * exp(-0.5 * tv + sd * z),
-                                                        P.smoothing, a);
+            const double f0 = P.obs_fwd[0] * 1.0 * exp(-0.5 * tv + sd * z);
+            double price = P.discount * terminal_payoff(pp, obs_spot(P, 0, P.spot, f0, pre, with_pre), P.smoothing, a);
             if (P.antithetic) {
-                const double mate = P.discount *
-                    terminal_payoff(pp, P.obs_fwd[0] * 1.0 * exp(-0.5 * tv + sd * -z), P.smoothing, a);
+                const double f1 = P.obs_fwd[0] * 1.0 * exp(-0.5 * tv + sd * -z);
+                const double mate =
+                    P.discount * terminal_payoff(pp, obs_spot(P, 0, P.spot, f1, pre, with_pre), P.smoothing, a);
                 price = (price + mate) * 0.5;
             }
             vals[MCG_PRICE] = price;
@@ -200,14 +227,20 @@ __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, u
             const double ze = e == 0 ? z : -z;
             wsum[e] += P.obs_sqrt_step[i] * ze;
             const double f = P.obs_fwd[i] * 1.0 * exp(-0.5 * tv + P.vol * wsum[e]);
+            double pre[1];
+            bool with_pre;
+            const double spot[1] = {obs_spot(P, i, P.spot, f, pre[0], with_pre)};
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
                 if (k >= static_cast<int>(P.product_count)) continue;
-                if (P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
+                if (P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER) {
                     barrier_interval(P.products[k], acc[e][k], P.smoothing, prev_f[e], f, var, var,
                                      dt, failed);
-                else
-                    acc_observe(P.products[k], acc[e][k], i, f, P.smoothing, failed);
+                } else {
+                    ProductAcc one[1] = {acc[e][k]};
+                    acc_observe_n<1>(P.products[k], one, i, spot, P.smoothing, pre, with_pre);
+                    acc[e][k] = one[0];
+                }
             }
             prev_f[e] = f;
         }

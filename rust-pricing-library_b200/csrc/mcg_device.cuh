@@ -245,6 +245,51 @@ MCG_HD SmoothD smooth_positive_part(double h, double input) {
     return {value, ind.value};
 }
 
+// Smooth maximum of the compact-C2 smoothing, right + positive_part(left -
+// right) (CompactC2Smoothing::maximum, crates/pricing/src/product/smoothing.rs:136-160),
+// with its partial derivatives d/dleft (the indicator) and d/dright (its
+// complement).
+MCG_HD double smooth_maximum(double h, double left, double right, double& d_left, double& d_right) {
+    const double diff = left - right;
+    if (diff >= h) {
+        d_left = 1.0;
+        d_right = 0.0;
+        return left;
+    }
+    if (diff <= -h) {
+        d_left = 0.0;
+        d_right = 1.0;
+        return right;
+    }
+    const double u = transition_coordinate(diff, h);
+    const double u2 = u * u;
+    const double u4 = u2 * u2;
+    double comp;
+    const SmoothD ind = interior_indicator(diff, h, u, comp);
+    const double scaled_u4 = 2.0 * h * u4;
+    const double poly = 2.5 + u * (-3.0 + u);
+    const double value = is_normal(scaled_u4) ? scaled_u4 * poly : (2.0 * u4 * poly) * h;
+    d_left = ind.value;
+    d_right = comp;
+    return right + value;
+}
+
+// ------------------------------------------------------------- dividends
+
+// AffineDividendCoordinate (crates/pricing/src/market/dividend.rs:137-181):
+// the observed spot a S0 + b f of the canonical state f, and the spot-bump
+// derivative scale.  A plan stores each observation's coordinate at its own
+// spot as double4 {a, b, spot_scale, flag}; at_spot refits it to a bumped
+// spot with the cash held fixed.
+struct DivCoord {
+    double a, b, spot_scale;
+};
+
+MCG_HD DivCoord div_at_spot(const double4& c, double original, double spot) {
+    if (original == spot) return {c.x, c.y, c.z};
+    return {c.x * original / spot, c.z - (c.z - c.y) * original / spot, c.z};
+}
+
 // ------------------------------------------------------------ statistics
 
 // One DeterministicStatistics record: NeumaierSum + CenteredMoment,

@@ -29,6 +29,7 @@
 #include "mcg_mlp.cuh"
 #include "mcg_book.cuh"
 #include "mcg_surface.cuh"
+#include "mcg_dividends.h"
 
 namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -367,6 +368,7 @@ struct mcg_plan {
     DeviceArray<double> node_time, dt, sqrt_dt, inv_sqrt_dt, time_weight, fwd, ratio, obs_time,
         obs_fwd, obs_sqrt_step, grid_t, grid_x, grid_v, grid_vol2, weights;
     DeviceArray<int32_t> obs_of_node, time_cell;
+    DeviceArray<double4> obs_div, obs_div_pre, lv_obs_div;
     DeviceArray<LvStep> lv_steps;
     DeviceArray<int4> step_prog;
     DeviceArray<BridgeNode> bridge_nodes;
@@ -407,6 +409,9 @@ struct mcg_plan {
         weights.release();
         obs_of_node.release();
         time_cell.release();
+        obs_div.release();
+        obs_div_pre.release();
+        lv_obs_div.release();
         lv_steps.release();
         step_prog.release();
         bridge_nodes.release();
@@ -555,6 +560,21 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
     const uint32_t n = d->observation_count;
     const double expiry = d->observation_times[n - 1];
     const bool lv = d->model == MCG_MODEL_LOCAL_VOLATILITY;
+    // Discrete dividends: the escrowed affine transform at the plan's spot.
+    HostDividends<HostCurve> divs;
+    const bool dividends = d->discrete_dividends.count > 0;
+    double residual_spot = d->spot;
+    if (dividends) {
+        if (!divs.compile(d->discrete_dividends, d->spot, rc, qc, why)) return fail(MCG_ERR_MARKET, why);
+        residual_spot = d->spot - divs.reserve;
+        for (uint32_t i = 0; i < d->product_count; ++i)
+            if (d->products[i].kind == MCG_PRODUCT_CONTINUOUS_BARRIER || d->products[i].kind == MCG_PRODUCT_AMERICAN)
+                return fail(MCG_ERR_UNSUPPORTED, "discrete dividends with a continuous barrier or early exercise");
+        if (d->precision != MCG_PRECISION_F64)
+            return fail(MCG_ERR_UNSUPPORTED, "discrete dividends in the FP32 path bulk");
+        if (lv && (d->request_vega || d->request_local_vega_nodes))
+            return fail(MCG_ERR_UNSUPPORTED, "local-volatility Vega and node sensitivities with discrete dividends");
+    }
 
     DevicePlan& P = plan.dp;
     P.model = d->model;
@@ -577,9 +597,10 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
     // Bumps, crates/pricing/src/engine/compile/simulation.rs:481-502.
     P.req_gamma = d->request_gamma != 0;
     P.gamma_bump = resolve_gamma_bump(d);
-    if (d->request_gamma && (!std::isfinite(P.gamma_bump) || P.gamma_bump >= d->spot || P.gamma_bump <= 0.0))
-        return fail(MCG_ERR_INVALID_ARGUMENT, "gamma bump must be positive and below spot");
-    P.spot_bump = d->request_gamma ? P.gamma_bump : std::min(d->spot * 1.0e-4, 0.5 * d->spot);
+    // With dividends the bumps stay below the escrowed spot S0 - R (compile/simulation.rs:473-489).
+    if (d->request_gamma && (!std::isfinite(P.gamma_bump) || P.gamma_bump >= residual_spot || P.gamma_bump <= 0.0))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "gamma bump must be positive and below the (escrowed) spot");
+    P.spot_bump = d->request_gamma ? P.gamma_bump : std::min(d->spot * 1.0e-4, 0.5 * residual_spot);
     P.spot_variant[0] = d->spot;
     P.spot_variant[1] = d->spot - P.spot_bump;
     P.spot_variant[2] = d->spot + P.spot_bump;
@@ -610,6 +631,23 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         P.obs_time = plan.obs_time.ptr;
         P.obs_fwd = plan.obs_fwd.ptr;
         P.obs_sqrt_step = plan.obs_sqrt_step.ptr;
+        if (dividends) {
+            // path_observation (black_scholes.rs:335-354): the observations'
+            // coordinates and, on an ex-date, the one before its dividend
+            std::vector<double4> post(n), pre(n);
+            for (uint32_t i = 0; i < n; ++i) {
+                const HostCoord c = divs.after_time(ot[i]);
+                const long e = divs.event_at(ot[i]);
+                const HostCoord b = e >= 0 ? divs.before_event(static_cast<size_t>(e)) : c;
+                post[i] = make_double4(c.a, c.b, c.spot_scale, e >= 0 ? 1.0 : 0.0);
+                pre[i] = make_double4(b.a, b.b, b.spot_scale, 0.0);
+            }
+            MCG_CUDA(plan.obs_div.upload(post));
+            MCG_CUDA(plan.obs_div_pre.upload(pre));
+            P.obs_div = plan.obs_div.ptr;
+            P.obs_div_pre = plan.obs_div_pre.ptr;
+            P.dividends = 1;
+        }
         steps = n;
         P.steps = n;
         P.dimension = n;
@@ -651,6 +689,9 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         for (size_t i = 0; i + 1 < gt.size(); ++i) maximum_step = std::max(maximum_step, gt[i + 1] - gt[i]);
         std::vector<double> events = gt;
         events.insert(events.end(), d->observation_times, d->observation_times + n);
+        // ex-dividend times up to expiry are time-grid events (compile/local_vol.rs:38-52)
+        for (const auto& e : divs.ev)
+            if (e.t <= expiry) events.push_back(e.t);
         std::vector<double> nodes;
         compile_time_grid(events, maximum_step, nodes);
         steps = static_cast<uint32_t>(nodes.size() - 1);
@@ -686,6 +727,40 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
             while (k <= steps && bits_of(nodes[k]) != b) ++k;
             if (k > steps) return fail(MCG_ERR_MARKET, "observation time missing from the time grid");
             oon[k] = static_cast<int32_t>(i);
+        }
+        if (dividends) {
+            // Every spot runtime's transform recompiled at its spot
+            // (local_vol_runtime_for_spot, risk/pathwise_local_vol.rs:51-69); the
+            // observations' node coordinates (local_vol_valuation.rs:221-247).
+            std::vector<double4> lvc(3 * static_cast<size_t>(n)), post(n), pre(n);
+            for (int k = 0; k < 3; ++k) {
+                HostDividends<HostCurve> dk;
+                if (!dk.compile(d->discrete_dividends, P.spot_variant[k], rc, qc, why))
+                    return fail(MCG_ERR_MARKET, why + " (bumped spot)");
+                for (uint32_t i = 0; i < n; ++i) {
+                    const double t = d->observation_times[i];
+                    const HostCoord c = dk.after_time(t);
+                    const long e = dk.event_at(t);
+                    const HostCoord b = e >= 0 ? dk.before_event(static_cast<size_t>(e)) : c;
+                    lvc[k * static_cast<size_t>(n) + i] = make_double4(c.a, c.b, b.a, b.b);
+                    if (k == 0) {
+                        post[i] = make_double4(c.a, c.b, c.spot_scale, e >= 0 ? 1.0 : 0.0);
+                        pre[i] = make_double4(b.a, b.b, b.spot_scale, 0.0);
+                    }
+                }
+                // The post-dividend spot A S + B f of an ex-date node (its check,
+                // dividend.rs:557-583) is positive for every positive f when A >= 0.
+                for (const auto& e : dk.ev)
+                    if (e.t <= expiry && dk.after_time(e.t).a < 0.0)
+                        return fail(MCG_ERR_UNSUPPORTED, "discrete dividends: a negative cash reserve after an ex-date");
+            }
+            MCG_CUDA(plan.lv_obs_div.upload(lvc));
+            MCG_CUDA(plan.obs_div.upload(post));
+            MCG_CUDA(plan.obs_div_pre.upload(pre));
+            P.lv_obs_div = plan.lv_obs_div.ptr;
+            P.obs_div = plan.obs_div.ptr;
+            P.obs_div_pre = plan.obs_div_pre.ptr;
+            P.dividends = 1;
         }
         if (d->precision == MCG_PRECISION_F32_BULK) {
             std::vector<float> inv_f(steps + 1), ra_f(steps);
@@ -898,7 +973,7 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         const bool smooth_barrier =
             plan.products[0].kind == MCG_PRODUCT_DISCRETE_BARRIER && P.smoothing > 0.0;
         const bool continuous = plan.products[0].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
-        P.bs_tape_rows = smooth_barrier ? 5u * P.observation_count
+        P.bs_tape_rows = smooth_barrier ? (P.dividends ? 7u : 5u) * P.observation_count
                                         : (continuous ? 4u * P.observation_count + 1u : 2u * P.observation_count);
         const uint64_t budget = (2048ull << 20) / (sizeof(double) * P.bs_tape_rows * P.scramble_count);
         const uint64_t units_rounded = (P.units + kThreads - 1) / kThreads * kThreads;
@@ -1357,6 +1432,8 @@ mcg_status lsm_price(const mcg_plan_desc* d, const mcg_lsm_desc* l, cudaStream_t
     int devices = 0;
     if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
         return fail(MCG_ERR_CUDA, "no CUDA device is visible");
+    if (d->discrete_dividends.count)
+        return fail(MCG_ERR_UNSUPPORTED, "early exercise with discrete dividends");
     // The path plans of both engines: the American product prices nothing by
     // itself, so each plan carries a European placeholder of the same contract.
     mcg_product_desc placeholder = d->products[0];
@@ -2121,6 +2198,8 @@ mcg_status book_create(const mcg_plan_desc* trades, uint32_t n, const mcg_book_o
     for (uint32_t i = 0; i < n; ++i) {
         const mcg_plan_desc& d = trades[i];
         const std::string who = "trade " + std::to_string(i) + ": ";
+        if (d.discrete_dividends.count)
+            return fail(MCG_ERR_UNSUPPORTED, who + "a book prices trades without discrete dividends");
         if (d.engine != MCG_ENGINE_PSEUDO || d.product_count != 1 || d.request_delta || d.request_gamma ||
             d.request_vega || d.request_local_vega_nodes)
             return fail(MCG_ERR_UNSUPPORTED, who + "a book trade is pseudo-MC, one product, price only");

@@ -155,6 +155,8 @@ extern "C" mcg_status mcg_price_european_noalloc(const mcg_plan_desc* d, void* s
         return noalloc_fail(MCG_ERR_INVALID_ARGUMENT, "product strike/notional must be positive");
     if (pd.has_initial_state)  // as mcg_plan_create: a terminal product has no observation history
         return noalloc_fail(MCG_ERR_UNSUPPORTED, "seasoned state of a product without observation history");
+    if (d->discrete_dividends.count)
+        return noalloc_fail(MCG_ERR_UNSUPPORTED, "the no-allocation entry point prices without discrete dividends");
     if (!(d->smoothing_half_width >= 0.0) || !std::isfinite(d->smoothing_half_width))
         return noalloc_fail(MCG_ERR_INVALID_ARGUMENT, "smoothing_half_width");
     const bool rqmc = d->engine == MCG_ENGINE_RQMC;

@@ -61,9 +61,13 @@ MCG_HD bool monitored(const ProductParams& p, uint32_t obs) {
 // Observation update of one product on N paths with one dispatch on the
 // product's kind: discrete products (compile.rs:159-202 Asian, :204-403
 // discrete barrier, :405-474 lookback, tape.rs:1038-1080 opcode semantics).
+// A discrete barrier monitored on an ex-dividend date also sees the spots just
+// before the dividend, `pre` (with_pre): its distance is the maximum (smoothed:
+// the compact-C2 smooth maximum) of the pre- and post-dividend distances
+// (crates/pricing/src/engine/payoff/compile.rs:315-346).
 template <int N>
 MCG_HD void acc_observe_n(const ProductParams& p, ProductAcc (&s)[N], uint32_t obs, const double (&spot)[N],
-                          double smoothing) {
+                          double smoothing, const double (&pre)[N], bool with_pre) {
 #pragma unroll
     for (int i = 0; i < N; ++i) s[i].terminal = spot[i];
     switch (p.kind) {
@@ -91,8 +95,16 @@ MCG_HD void acc_observe_n(const ProductParams& p, ProductAcc (&s)[N], uint32_t o
         if (!monitored(p, obs)) break;
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-            const double dist =
-                p.barrier_direction == MCG_BARRIER_UP ? spot[i] - p.barrier : p.barrier - spot[i];
+            double dist = p.barrier_direction == MCG_BARRIER_UP ? spot[i] - p.barrier : p.barrier - spot[i];
+            if (with_pre) {
+                const double pd = p.barrier_direction == MCG_BARRIER_UP ? pre[i] - p.barrier : p.barrier - pre[i];
+                if (smoothing > 0.0) {
+                    double dl, dr;
+                    dist = smooth_maximum(smoothing, pd, dist, dl, dr);
+                } else {
+                    dist = pd >= dist ? pd : dist;
+                }
+            }
             double w;
             if (smoothing > 0.0) {
                 double comp;
@@ -115,7 +127,7 @@ MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
     (void)failed;
     ProductAcc one[1] = {s};
     const double at[1] = {spot};
-    acc_observe_n<1>(p, one, obs, at, smoothing);
+    acc_observe_n<1>(p, one, obs, at, smoothing, at, false);
     s = one[0];
 }
 

@@ -144,6 +144,16 @@ struct DevicePlan {
     int32_t lv_bumps;      // LV: CRN delta/gamma evolutions
     double gamma_bump, spot_bump, vol_bump;
     double smoothing;
+    // Discrete dividends (escrowed affine model; null without dividends): per
+    // observation its coordinate {a, b, spot_scale, 1 when the observation is
+    // an ex-date} at the plan's spot and the coordinate just before that
+    // ex-date's dividend {a, b, spot_scale, 0}; local volatility: per spot
+    // runtime (base, down, up) and observation {a, b, pre a, pre b} at the
+    // runtime's spot, observation i of runtime w at lv_obs_div[w * n + i].
+    int32_t dividends;
+    const double4* obs_div;
+    const double4* obs_div_pre;
+    const double4* lv_obs_div;
     // BS pathwise risk of a multi-observation product: per-thread scratch of
     // `bs_tape_units` threads x bs_tape_rows rows ([row][thread]).
     double* bs_tape;

@@ -39,6 +39,10 @@ _dp = C.POINTER(C.c_double)
 _up = C.POINTER(C.c_uint32)
 
 
+class Dividends(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("ex_times", _dp), ("fixed_cash", _dp), ("proportional", _dp)]
+
+
 class Curve(C.Structure):
     _fields_ = [("pillar_count", C.c_uint32), ("times", _dp), ("discount_factors", _dp)]
 
@@ -105,6 +109,7 @@ class PlanDesc(C.Structure):
         ("request_local_vega_nodes", C.c_int32), ("gamma_bump_relative", C.c_int32),
         ("gamma_bump", C.c_double), ("smoothing_half_width", C.c_double),
         ("checkpoint_interval", C.c_uint32),
+        ("discrete_dividends", Dividends),
     ]
 
 

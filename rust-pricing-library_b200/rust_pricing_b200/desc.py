@@ -122,6 +122,8 @@ class PlanSpec:
     gamma_bump: float = 0.01
     smoothing_half_width: float = 0.0
     checkpoint_interval: int = 16
+    # Discrete dividends of the escrowed affine model: (ex-time, fixed cash, proportional fraction)
+    dividends: Sequence[tuple] = ()
     _keep: list = field(default_factory=list, repr=False)
 
     def steps(self) -> int:
@@ -193,6 +195,10 @@ class PlanSpec:
         d.gamma_bump = self.gamma_bump
         d.smoothing_half_width = self.smoothing_half_width
         d.checkpoint_interval = self.checkpoint_interval
+        if self.dividends:
+            ex, cash, beta = (_f64([float(x[i]) for x in self.dividends]) for i in range(3))
+            keep += [ex, cash, beta]
+            d.discrete_dividends = A.Dividends(len(ex), _ptr(ex), _ptr(cash), _ptr(beta))
         keep.append(d)
         return d
 
@@ -201,6 +207,9 @@ class PlanSpec:
         if self.model == A.MODEL_LOCAL_VOLATILITY and self.local_variance is not None:
             union = np.union1d(np.asarray(self.local_variance.time_nodes, dtype=np.float64),
                                np.asarray(self.observation_times, dtype=np.float64))
+            ex = [float(d[0]) for d in self.dividends if float(d[0]) <= float(self.observation_times[-1])]
+            if ex:
+                union = np.union1d(union, np.asarray(ex, dtype=np.float64))
             gaps = np.diff(np.asarray(self.local_variance.time_nodes, dtype=np.float64))
             step = float(gaps.max())
             count = int(np.sum(np.maximum(1, np.ceil(np.diff(np.concatenate([[0.0], union])) / step))))

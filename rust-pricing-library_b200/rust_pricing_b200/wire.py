@@ -104,6 +104,35 @@ class CompiledRequest:
     observation_dates: list = field(default_factory=list)
 
 
+# --------------------------------------------------------------- dividends
+
+def _dividends(events: list) -> list:
+    """market.discrete_dividends (schemas/v3 dividend_event / dividend_quote):
+    (ex_time, fixed cash, proportional fraction) per event, as the plan's
+    escrowed affine dividend schedule (DividendQuote, crates/pricing/src/market/dividend.rs:9-55)."""
+    out = []
+    for i, e in enumerate(events):
+        where = f"market.discrete_dividends[{i}]"
+        t = float(_get(e, "ex_time", where))
+        q = _get(e, "quote", where)
+        kind = _get(q, "type", where + ".quote")
+        if kind == "fixed_cash":
+            cash, beta = float(_get(q, "amount", where + ".quote")), 0.0
+        elif kind == "proportional":
+            cash, beta = 0.0, float(_get(q, "beta", where + ".quote"))
+        elif kind == "fixed_cash_and_proportional":
+            cash, beta = float(_get(q, "fixed_cash", where + ".quote")), float(_get(q, "beta", where + ".quote"))
+        else:
+            raise WireError(f"{where}.quote: unknown type {kind!r}")
+        if not (math.isfinite(t) and t >= 0.0) or not (math.isfinite(cash) and cash >= 0.0) or \
+                not (math.isfinite(beta) and 0.0 <= beta < 1.0):
+            raise WireError(f"{where}: ex_time and cash must be finite and >= 0, beta in [0, 1)")
+        if out and not t > out[-1][0]:
+            raise WireError("market.discrete_dividends must be ordered by strictly increasing ex_time")
+        out.append((t, cash, beta))
+    return out
+
+
 # ------------------------------------------------------------------ engine
 
 def _engine(engine: dict, where: str) -> dict:
@@ -422,8 +451,7 @@ def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledR
     market = _get(doc, "market", "request")
     if _get(market, "type", "market") != "equity":
         raise WireError("market.type must be 'equity'")
-    if market.get("discrete_dividends"):
-        raise UnsupportedRequest("discrete dividends (affine dividend transform) are not on this engine's path")
+    dividends = _dividends(market.get("discrete_dividends") or [])
     spot = _positive(_get(market, "spot", "market"), "market.spot")
     dt, dfs = _curve(_get(market, "discount_curve", "market"), "market.discount_curve")
     qt, qfs = _curve(_get(market, "dividend_curve", "market"), "market.dividend_curve")
@@ -433,7 +461,8 @@ def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledR
     payment_time = year_fraction(valuation, product.payment)
     plan_kw = dict(observation_times=times, products=[product.spec], spot=spot,
                    discount_times=dt, discount_factors=dfs, dividend_times=qt, dividend_factors=qfs,
-                   reduction_block_size=reduction_block_size, payment_time=payment_time, **engine)
+                   reduction_block_size=reduction_block_size, payment_time=payment_time, dividends=dividends,
+                   **engine)
     warnings: list = []
     basis = _model(doc, plan_kw, times[-1], warnings)
     if times[0] == 0.0 and (plan_kw["model"] != A.MODEL_BLACK_SCHOLES or ptype == "american_vanilla"
@@ -473,6 +502,11 @@ def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledR
         vega_kt = {"config": risk["vega_kt"], "reporting_iv_basis": basis,
                    "policy": TERMINAL_REPLICATION if replicable else NODE_ALLOCATION}
 
+    if dividends:
+        if ptype == "american_vanilla" or product.spec.kind == A.PRODUCT_CONTINUOUS_BARRIER:
+            raise UnsupportedRequest("discrete dividends with early exercise or a continuous barrier")
+        if plan_kw.get("model") == A.MODEL_LOCAL_VOLATILITY and (req_vega or vega_kt is not None):
+            raise UnsupportedRequest("local-volatility Vega and VegaKT with discrete dividends")
     plan = PlanSpec(**plan_kw)
     if plan.engine == A.ENGINE_RQMC and plan.scramble_count < 1:
         raise WireError("engine.scramble_count must be positive")

@@ -198,8 +198,11 @@ def test_oracle_honours_seasoned_state_and_flags():
     (lambda d: d.update(document_kind="pricing_result"), wire.WireError),
     (lambda d: d.update(schema_version=2), wire.UnsupportedRequest),
     (lambda d: d["market"].update(discrete_dividends=[{"event_id": 1, "ex_time": 0.5,
-                                                        "quote": {"type": "fixed_cash", "amount": 1.0}}]),
-     wire.UnsupportedRequest),
+                                                        "quote": {"type": "proportional", "beta": 1.0}}]),
+     wire.WireError),
+    (lambda d: d["market"].update(discrete_dividends=[{"event_id": 1, "ex_time": 0.5,
+                                                        "quote": {"type": "stock", "amount": 1.0}}]),
+     wire.WireError),
     (lambda d: d.update(model={"type": "bass_local_volatility", "parameters": {}}), wire.UnsupportedRequest),
     (lambda d: d["risk"].update(payoff_smoothing_width_ladder=[1.0, 2.0]), wire.UnsupportedRequest),  # ladder entry
     (lambda d: d["product"].update(expiry="2026-09-04", payment_date="2026-09-04"), wire.UnsupportedRequest),  # t = 0 only
@@ -298,7 +301,7 @@ def test_facade_compile_and_validation():
     with pytest.raises(ValidationError):
         PricingRequest.from_json("[1, 2")
     bad = copy.deepcopy(case["request"])
-    bad["market"]["discrete_dividends"] = [{"event_id": 1, "ex_time": 0.5, "quote": {"type": "fixed_cash", "amount": 1.0}}]
+    bad["market"]["discrete_dividends"] = [{"event_id": 1, "ex_time": 0.5, "quote": {"type": "fixed_cash", "amount": -1.0}}]
     with pytest.raises(ValidationError):
         PricingPlan.compile(PricingRequest(bad), worker_threads=1)
 
@@ -359,3 +362,23 @@ def test_replicable_vega_kt_is_not_reported_by_node_allocation(case):
     basis = off_basis["model"]["reporting_iv_basis"]
     basis["maturity_nodes"] = [t for t in basis["maturity_nodes"] if t != 1.0] + [1.5]
     assert wire.compile_request(off_basis).vega_kt["policy"] == wire.NODE_ALLOCATION
+
+
+def test_discrete_dividends_compile_to_the_plan_schedule():
+    """market.discrete_dividends (all three quote types) become the plan's
+    escrowed affine schedule; combinations the engine leaves out raise."""
+    doc = _case("digital_exact_price_only")
+    doc["market"]["discrete_dividends"] = [
+        {"event_id": 1, "ex_time": 0.25, "quote": {"type": "fixed_cash", "amount": 1.5}},
+        {"event_id": 2, "ex_time": 0.5, "quote": {"type": "proportional", "beta": 0.02}},
+        {"event_id": 3, "ex_time": 0.75, "quote": {"type": "fixed_cash_and_proportional", "fixed_cash": 1.0,
+                                                  "beta": 0.01}}]
+    req = wire.compile_request(doc)
+    assert list(req.plan.dividends) == [(0.25, 1.5, 0.0), (0.5, 0.0, 0.02), (0.75, 1.0, 0.01)]
+    H.oracle_evaluate(req.plan, threads=2)  # the oracle prices it
+    cont = _case("continuous_barrier_smoothed_full_risk") if any(
+        c["name"] == "continuous_barrier_smoothed_full_risk" for c in WC.path_dependence_cases()) else None
+    if cont is not None:
+        cont["market"]["discrete_dividends"] = doc["market"]["discrete_dividends"]
+        with pytest.raises(wire.UnsupportedRequest):
+            wire.compile_request(cont)
