@@ -543,11 +543,12 @@ def main():
                 "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": achieved / peak.value if peak.value else None,
                 # DRAM bytes of one path-kernel launch, scaled by CTA count from the ncu capture
-                # of the 2^14-point x 16-scramble case (1.771776 MB read + 1.024 KB written over
-                # 2048 CTAs: grid, scramble tables and tile records, in proportion to the CTAs)
-                "traffic": (1.771776e6 + 1.024e3) * (args.points * args.scrambles / 128) / 2048,
+                # of the 2^16-point x 16-scramble case (1.342208 MB read + 256 B written over
+                # 4096 CTAs of two 128-unit tiles: grid, scramble tables and tile records, in
+                # proportion to the CTAs)
+                "traffic": (1.342208e6 + 256.0) * (args.points * args.scrambles / 256) / 4096,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the path kernel on the "
-                                  "2^14-point x 16-scramble case, scaled by CTA count",
+                                  "2^16-point x 16-scramble case, scaled by CTA count",
                 "peak_source": "measured live: mcg_measure_fp64_peak (DFMA chains, this GPU)",
                 "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel_ms": path_ms}
 
