@@ -710,6 +710,91 @@ mcg_status mcg_book_create(const mcg_plan_desc* trades, uint32_t trade_count, co
 mcg_status mcg_book_evaluate(mcg_book* book, void* stream, mcg_estimate* prices, mcg_book_report* report);
 void mcg_book_destroy(mcg_book* book);
 
+/* ---- Correlated multi-asset paths ----
+ *
+ * MultiAssetPricingPlan::compile / evaluate (crates/pricing/src/engine/multi_asset/compile.rs:200-470,
+ * multi_asset/path.rs:24-200, multi_asset/evaluate.rs:92-300) for Black--Scholes
+ * and local-volatility assets on one time grid: the union of the expiry, the
+ * correlation change times, every local-variance grid's time nodes up to the
+ * expiry and the substeps of `maximum_step` (LocalVolTimeGrid::compile).  Per
+ * sampling unit each asset's factor takes its own normals -- Philox
+ * coordinate (unit, dimension) or scrambled Sobol, dimension factor x steps +
+ * step, or step x assets + factor for RQMC with the Brownian bridge (every
+ * factor's terminal bridge normal in the first dimensions) -- optionally
+ * Brownian-bridged per factor, correlated per step by the lower Cholesky
+ * factor of the step's correlation matrix (unpivoted, zero pivots below
+ * 1e-12 allowed: CorrelationFactor::compile, crates/pricing-numerics/src/correlation.rs:61-180),
+ * and evolves its asset: f <- f F_{s+1}/F_s exp(-sigma^2 dt/2 + sigma sqrt(dt) z)
+ * (Black--Scholes) or the Log-Euler step on its grid (local volatility).  The
+ * payoff is a basket option on sum_i w_i S_i(T) / scale_i or a worst-of
+ * option on min_i S_i(T) / reference_i (crates/pricing/src/product/multi_asset.rs:77-246),
+ * exact or compact-C2 smoothed, paid at `payment_time`; statistics as the
+ * single-asset plans (antithetic pairs averaged, RQMC two-pass over scramble
+ * means).  Price only. */
+#define MCG_MAX_ASSETS 8u
+
+typedef enum mcg_multi_product_kind {
+    MCG_MULTI_BASKET = 0,   /* sum_i weights[i] S_i(T) / scales[i] */
+    MCG_MULTI_WORST_OF = 1  /* min_i S_i(T) / scales[i] (the reference levels) */
+} mcg_multi_product_kind;
+
+typedef struct mcg_asset_desc {
+    int32_t model;          /* mcg_model_kind */
+    double spot;
+    mcg_curve dividend_curve;
+    double volatility;      /* Black--Scholes */
+    mcg_local_variance_grid local_variance; /* local volatility */
+} mcg_asset_desc;
+
+typedef struct mcg_multi_asset_desc {
+    uint32_t abi_version;   /* MCG_ABI_VERSION */
+    uint32_t asset_count;   /* 1 .. MCG_MAX_ASSETS */
+    const mcg_asset_desc* assets;
+    mcg_curve discount_curve;
+    /* Correlation term structure: `correlation_count` matrices (asset_count^2,
+     * row-major), matrix k in force from correlation_times[k] (increasing; the
+     * first <= 0) until the next. */
+    uint32_t correlation_count;
+    const double* correlation_times;
+    const double* correlations;
+    double maximum_step;
+    double expiry;
+    double payment_time;
+    /* engine */
+    int32_t engine;         /* mcg_engine_kind */
+    uint64_t master_seed;
+    uint64_t sampling_units;
+    uint32_t scramble_count;
+    int32_t antithetic;
+    int32_t brownian_bridge;
+    uint64_t reduction_block_size;  /* ExecutionPolicy block size of the statistics; 0 = 4096 */
+    uint32_t sobol_dimension_count;
+    const uint32_t* sobol_directions;
+    /* product */
+    int32_t product;        /* mcg_multi_product_kind */
+    int32_t side;           /* mcg_side */
+    double strike;
+    double notional;
+    const double* weights;  /* basket: per asset (ignored by the worst-of) */
+    const double* scales;   /* basket scales / worst-of reference levels, positive */
+    double smoothing_half_width;
+} mcg_multi_asset_desc;
+
+typedef struct mcg_multi_asset_result {
+    mcg_statistics price_statistics;
+    mcg_estimate price;
+    double sampling_variance;
+    uint64_t evaluated_paths;
+    uint64_t independent_sampling_units;
+    uint32_t time_steps;
+    uint32_t dimension;
+    uint32_t kernel_launches;
+    float device_ms;
+    mcg_error_record error;
+} mcg_multi_asset_result;
+
+mcg_status mcg_multi_asset_price(const mcg_multi_asset_desc* desc, void* stream, mcg_multi_asset_result* result);
+
 /* ---- Pricing without device allocation (no counterpart in the reference) ----
  *
  * For callers that must not allocate GPU memory while pricing (a service that

@@ -36,6 +36,7 @@ UNITS = [
     ("mcg_book.cu", ["-fmad=false"]),
     ("mcg_lv32.cu", []),
     ("mcg_vegakt.cu", []),
+    ("mcg_multi.cu", ["-fmad=false"]),
 ]
 
 

@@ -30,6 +30,7 @@
 #include "mcg_book.cuh"
 #include "mcg_surface.cuh"
 #include "mcg_dividends.h"
+#include "mcg_multi.cuh"
 
 namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -328,6 +329,38 @@ bool bridge_program(const std::vector<double>& t, const std::vector<BridgeInstr>
     }
     slot_count = used;
     return used <= static_cast<uint32_t>(kMaxBridgeSlots);
+}
+
+// The path tiles' form of a program: per step, the bridge nodes produced just
+// before it (the terminal as a node with zero weights reading the W(0) slot)
+// and its bracketing slots.  False if the steps are not in order.
+bool step_program(const std::vector<Op>& ops, uint32_t steps, std::vector<int4>& prog,
+                  std::vector<BridgeNode>& bnodes, int32_t& zero_slot) {
+    prog.assign(steps, make_int4(0, 0, -1, -1));
+    bnodes.clear();
+    zero_slot = 0;
+    size_t pending = 0;
+    uint32_t next_step = 0;
+    for (const Op& op : ops) {
+        if (op.kind == kOpZero) {
+            zero_slot = op.out;
+        } else if (op.kind == kOpTerminal) {
+            bnodes.push_back(BridgeNode{0.0, 0.0, op.sd, op.out, zero_slot, zero_slot, op.rank});
+        } else if (op.kind == kOpInterior) {
+            bnodes.push_back(BridgeNode{op.wl, op.wr, op.sd, op.out, op.left, op.right, op.rank});
+        } else {
+            if (op.step != static_cast<int32_t>(next_step) || next_step >= steps) return false;
+            int4& r = prog[next_step++];
+            r.x = static_cast<int32_t>(pending);
+            r.y = static_cast<int32_t>(bnodes.size() - pending);
+            pending = bnodes.size();
+            if (op.kind == kOpStep) {
+                r.z = op.left;
+                r.w = op.right;
+            }
+        }
+    }
+    return next_step == steps && pending == bnodes.size();
 }
 
 template <class T>
@@ -867,35 +900,11 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         P.ops = plan.ops.ptr;
         P.op_count = static_cast<uint32_t>(ops.size());
         {
-            // The path tiles' form of the program: per step, the bridge nodes
-            // produced just before it and its bracketing slots.
-            std::vector<int4> prog(steps, make_int4(0, 0, -1, -1));
+            std::vector<int4> prog;
             std::vector<BridgeNode> bnodes;
             int32_t zero_slot = 0;
-            size_t pending = 0;
-            uint32_t next_step = 0;
-            for (const Op& op : ops) {
-                if (op.kind == kOpZero) {
-                    zero_slot = op.out;
-                } else if (op.kind == kOpTerminal) {
-                    bnodes.push_back(BridgeNode{0.0, 0.0, op.sd, op.out, zero_slot, zero_slot, op.rank});
-                } else if (op.kind == kOpInterior) {
-                    bnodes.push_back(BridgeNode{op.wl, op.wr, op.sd, op.out, op.left, op.right, op.rank});
-                } else {
-                    if (op.step != static_cast<int32_t>(next_step))
-                        return fail(MCG_ERR_BRIDGE, "internal: path program steps out of order");
-                    int4& r = prog[next_step++];
-                    r.x = static_cast<int32_t>(pending);
-                    r.y = static_cast<int32_t>(bnodes.size() - pending);
-                    pending = bnodes.size();
-                    if (op.kind == kOpStep) {
-                        r.z = op.left;
-                        r.w = op.right;
-                    }
-                }
-            }
-            if (next_step != steps || pending != bnodes.size())
-                return fail(MCG_ERR_BRIDGE, "internal: path program does not end with a step");
+            if (!step_program(ops, steps, prog, bnodes, zero_slot))
+                return fail(MCG_ERR_BRIDGE, "internal: path program steps out of order");
             MCG_CUDA(plan.step_prog.upload(prog));
             P.step_prog = plan.step_prog.ptr;
             MCG_CUDA(plan.bridge_nodes.upload(bnodes));
@@ -2372,6 +2381,375 @@ namespace mcg {
 void set_last_error(const std::string& message) { g_last_error = message; }
 }  // namespace mcg
 
+namespace {
+
+// CorrelationFactor::compile (crates/pricing-numerics/src/correlation.rs:61-180)
+// with every tolerance 1e-12: symmetric average, unit diagonal, unpivoted
+// lower Cholesky factor of a positive semi-definite matrix whose zero pivots
+// leave zero columns (residuals checked against the same tolerance).
+bool correlation_lower(const double* raw, uint32_t n, std::vector<double>& lower, std::string& why) {
+    const double tol = 1e-12;
+    std::vector<double> c(raw, raw + static_cast<size_t>(n) * n);
+    for (double v : c)
+        if (!std::isfinite(v)) {
+            why = "correlation: non-finite entry";
+            return false;
+        }
+    for (uint32_t i = 0; i < n; ++i) {
+        if (std::fabs(raw[i * n + i] - 1.0) > tol) {
+            why = "correlation: diagonal must be 1";
+            return false;
+        }
+        c[i * n + i] = 1.0;
+        for (uint32_t j = i + 1; j < n; ++j) {
+            if (std::fabs(raw[i * n + j] - raw[j * n + i]) > tol) {
+                why = "correlation: matrix must be symmetric";
+                return false;
+            }
+            const double avg = (raw[i * n + j] + raw[j * n + i]) * 0.5;
+            if (!(avg >= -1.0 && avg <= 1.0)) {
+                why = "correlation: entries must lie in [-1, 1]";
+                return false;
+            }
+            c[i * n + j] = c[j * n + i] = avg;
+        }
+    }
+    double scale = 1.0;
+    for (uint32_t i = 0; i < n; ++i) {
+        double row = 0.0;
+        for (uint32_t j = 0; j < n; ++j) row = row + std::fabs(c[i * n + j]);
+        scale = std::max(scale, row);
+    }
+    const double threshold = std::max(tol, tol * scale);
+    lower.assign(static_cast<size_t>(n) * n, 0.0);
+    for (uint32_t j = 0; j < n; ++j) {
+        double sum = 0.0;
+        for (uint32_t k = 0; k < j; ++k) sum += lower[j * n + k] * lower[j * n + k];
+        const double pivot = c[j * n + j] - sum;
+        if (!std::isfinite(pivot) || pivot < -threshold) {
+            why = "correlation: matrix is not positive semi-definite";
+            return false;
+        }
+        if (pivot > threshold) lower[j * n + j] = std::sqrt(pivot);
+        for (uint32_t i = j + 1; i < n; ++i) {
+            double s2 = 0.0;
+            for (uint32_t k = 0; k < j; ++k) s2 += lower[i * n + k] * lower[j * n + k];
+            const double residual = c[i * n + j] - s2;
+            if (pivot > threshold) {
+                lower[i * n + j] = residual / lower[j * n + j];
+            } else if (!std::isfinite(residual) || std::fabs(residual) > threshold) {
+                why = "correlation: singular matrix with an inconsistent residual";
+                return false;
+            }
+        }
+    }
+    return true;
+}
+
+// Device arrays of one multi-asset evaluation, released on every exit.
+struct MultiArrays {
+    DeviceArray<double> dt, sqrt_dt, inv_sqrt_dt, lower, ratio, time_weight;
+    DeviceArray<int32_t> step_entry, time_cell;
+    DeviceArray<double2> bounds[kMaxAssets], cells[kMaxAssets];
+    DeviceArray<int4> step_prog;
+    DeviceArray<BridgeNode> bridge_nodes;
+    DeviceArray<uint32_t> directions, scr_dirs, scr_shift, scr_low;
+    DeviceArray<StatRecord> partials, records;
+    DeviceArray<ErrorWord> error;
+    ~MultiArrays() {
+        for (auto* a : {&dt, &sqrt_dt, &inv_sqrt_dt, &lower, &ratio, &time_weight}) a->release();
+        step_entry.release();
+        time_cell.release();
+        for (int i = 0; i < kMaxAssets; ++i) {
+            bounds[i].release();
+            cells[i].release();
+        }
+        step_prog.release();
+        bridge_nodes.release();
+        for (auto* a : {&directions, &scr_dirs, &scr_shift, &scr_low}) a->release();
+        partials.release();
+        records.release();
+        error.release();
+    }
+};
+
+mcg_status multi_asset_price(const mcg_multi_asset_desc* d, cudaStream_t stream, mcg_multi_asset_result* r) {
+    if (!d || !r) return fail(MCG_ERR_INVALID_ARGUMENT, "null descriptor or result");
+    std::memset(r, 0, sizeof(*r));
+    if (d->abi_version != MCG_ABI_VERSION) return fail(MCG_ERR_INVALID_ARGUMENT, "abi_version mismatch");
+    const uint32_t n = d->asset_count;
+    if (n == 0 || n > MCG_MAX_ASSETS || !d->assets) return fail(MCG_ERR_INVALID_ARGUMENT, "asset_count must be 1..8");
+    const double horizon = d->expiry;
+    if (!(horizon > 0.0) || !std::isfinite(horizon)) return fail(MCG_ERR_INVALID_ARGUMENT, "expiry");
+    if (!(d->payment_time >= horizon) || !std::isfinite(d->payment_time))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "payment_time must not precede the expiry");
+    if (!(d->maximum_step > 0.0) || !std::isfinite(d->maximum_step))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "maximum_step");
+    if (!(d->smoothing_half_width >= 0.0) || !std::isfinite(d->smoothing_half_width))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "smoothing_half_width");
+    if (d->product != MCG_MULTI_BASKET && d->product != MCG_MULTI_WORST_OF)
+        return fail(MCG_ERR_UNSUPPORTED, "product");
+    if (!std::isfinite(d->strike) || !(d->notional > 0.0) || !std::isfinite(d->notional) || !d->scales ||
+        (d->product == MCG_MULTI_BASKET && !d->weights))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "strike, notional, weights and scales");
+    for (uint32_t i = 0; i < n; ++i)
+        if (!(d->scales[i] > 0.0) || !std::isfinite(d->scales[i]) ||
+            (d->product == MCG_MULTI_BASKET && !std::isfinite(d->weights[i])))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "basket weights must be finite and scales positive");
+    const bool rqmc = d->engine == MCG_ENGINE_RQMC;
+    if (!rqmc && d->engine != MCG_ENGINE_PSEUDO) return fail(MCG_ERR_UNSUPPORTED, "engine");
+    const uint64_t units = d->sampling_units;
+    const uint32_t scrambles = rqmc ? d->scramble_count : 1;
+    if (units == 0 || (rqmc && (units & (units - 1)) != 0) || units > (1ull << 32))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "sampling_units (RQMC: a power of two)");
+    if ((rqmc ? scrambles : units) < 2)
+        return fail(MCG_ERR_INSUFFICIENT_UNITS, "at least two independent sampling units are required");
+    HostCurve rc;
+    std::string why;
+    if (!load_curve(d->discount_curve, rc, "discount_curve", why)) return fail(MCG_ERR_MARKET, why);
+    // correlation term structure
+    if (d->correlation_count == 0 || !d->correlation_times || !d->correlations)
+        return fail(MCG_ERR_INVALID_ARGUMENT, "correlation term structure is empty");
+    std::vector<double> lower;
+    for (uint32_t k = 0; k < d->correlation_count; ++k) {
+        if (!std::isfinite(d->correlation_times[k]) || (k && !(d->correlation_times[k] > d->correlation_times[k - 1])))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "correlation times must be increasing");
+        std::vector<double> l;
+        if (!correlation_lower(d->correlations + static_cast<size_t>(k) * n * n, n, l, why))
+            return fail(MCG_ERR_INVALID_ARGUMENT, why);
+        lower.insert(lower.end(), l.begin(), l.end());
+    }
+    if (!(d->correlation_times[0] <= 0.0))
+        return fail(MCG_ERR_INVALID_ARGUMENT, "the first correlation matrix must be in force at the valuation date");
+    // time grid: the expiry, correlation changes, the grids' nodes (compile.rs:285-336)
+    std::vector<double> events{horizon};
+    for (uint32_t k = 0; k < d->correlation_count; ++k)
+        if (d->correlation_times[k] > 0.0 && d->correlation_times[k] < horizon) events.push_back(d->correlation_times[k]);
+    for (uint32_t i = 0; i < n; ++i) {
+        const mcg_asset_desc& a = d->assets[i];
+        if (!(a.spot > 0.0) || !std::isfinite(a.spot)) return fail(MCG_ERR_INVALID_ARGUMENT, "asset spot");
+        if (a.model == MCG_MODEL_BLACK_SCHOLES) {
+            if (!(a.volatility >= 0.0) || !std::isfinite(a.volatility))
+                return fail(MCG_ERR_INVALID_ARGUMENT, "asset volatility");
+        } else if (a.model == MCG_MODEL_LOCAL_VOLATILITY) {
+            const mcg_local_variance_grid& g = a.local_variance;
+            if (g.time_count < 2 || g.log_moneyness_count < 2 || !g.time_nodes || !g.log_moneyness_nodes || !g.values)
+                return fail(MCG_ERR_MARKET, "local variance grid needs at least 2x2 nodes");
+            for (uint32_t k = 0; k < g.time_count; ++k)
+                if (!std::isfinite(g.time_nodes[k]) || (k && !(g.time_nodes[k] > g.time_nodes[k - 1])))
+                    return fail(MCG_ERR_MARKET, "grid time nodes must be finite and increasing");
+            if (bits_of(g.time_nodes[0]) != 0 || g.time_nodes[g.time_count - 1] < horizon)
+                return fail(MCG_ERR_MARKET, "local variance grid must cover [0, expiry]");
+            for (uint32_t k = 0; k < g.log_moneyness_count; ++k)
+                if (!std::isfinite(g.log_moneyness_nodes[k]) ||
+                    (k && !(g.log_moneyness_nodes[k] > g.log_moneyness_nodes[k - 1])))
+                    return fail(MCG_ERR_MARKET, "grid log-moneyness nodes must be finite and increasing");
+            for (size_t k = 0; k < static_cast<size_t>(g.time_count) * g.log_moneyness_count; ++k)
+                if (!std::isfinite(g.values[k]) || g.values[k] < g.floor || g.values[k] > g.cap)
+                    return fail(MCG_ERR_MARKET, "grid value outside [floor, cap]");
+            for (uint32_t k = 0; k < g.time_count; ++k)
+                if (g.time_nodes[k] <= horizon) events.push_back(g.time_nodes[k]);
+        } else {
+            return fail(MCG_ERR_UNSUPPORTED, "multi-asset models are Black-Scholes and local volatility");
+        }
+    }
+    std::vector<double> nodes;
+    compile_time_grid(events, d->maximum_step, nodes);
+    const uint32_t steps = static_cast<uint32_t>(nodes.size() - 1);
+    MultiAssetDev M{};
+    M.n = n;
+    M.steps = steps;
+    M.dimension = n * steps;
+    M.engine = d->engine;
+    M.antithetic = d->antithetic != 0;
+    M.bridge = d->brownian_bridge != 0;
+    M.rank_major = rqmc && M.bridge;
+    M.seed = d->master_seed;
+    M.units = units;
+    MultiArrays A;
+    {
+        std::vector<double> dtv(steps), sq(steps), isq(steps);
+        std::vector<int32_t> entry(steps);
+        for (uint32_t s = 0; s < steps; ++s) {
+            dtv[s] = nodes[s + 1] - nodes[s];
+            sq[s] = std::sqrt(dtv[s]);
+            isq[s] = 1.0 / std::sqrt(dtv[s]);
+            uint32_t e = 0;
+            while (e < d->correlation_count && d->correlation_times[e] <= nodes[s]) ++e;
+            entry[s] = static_cast<int32_t>(e) - 1;
+        }
+        MCG_CUDA(A.dt.upload(dtv));
+        MCG_CUDA(A.sqrt_dt.upload(sq));
+        MCG_CUDA(A.inv_sqrt_dt.upload(isq));
+        MCG_CUDA(A.step_entry.upload(entry));
+        MCG_CUDA(A.lower.upload(lower));
+        M.dt = A.dt.ptr;
+        M.sqrt_dt = A.sqrt_dt.ptr;
+        M.inv_sqrt_dt = A.inv_sqrt_dt.ptr;
+        M.step_entry = A.step_entry.ptr;
+        M.lower = A.lower.ptr;
+    }
+    {
+        std::vector<double> ratio(static_cast<size_t>(n) * steps), tw(static_cast<size_t>(n) * steps, 0.0);
+        std::vector<int32_t> tc(static_cast<size_t>(n) * steps, 0);
+        for (uint32_t i = 0; i < n; ++i) {
+            const mcg_asset_desc& a = d->assets[i];
+            HostCurve qc;
+            if (!load_curve(a.dividend_curve, qc, "asset dividend_curve", why)) return fail(MCG_ERR_MARKET, why);
+            std::vector<double> fw(steps + 1);
+            for (uint32_t k = 0; k <= steps; ++k) {
+                fw[k] = a.spot * std::exp(qc.log_discount(nodes[k]) - rc.log_discount(nodes[k]));
+                if (!std::isfinite(fw[k]) || fw[k] <= 0.0) return fail(MCG_ERR_MARKET, "non-finite forward");
+            }
+            for (uint32_t s = 0; s < steps; ++s) ratio[static_cast<size_t>(i) * steps + s] = fw[s + 1] / fw[s];
+            M.model[i] = a.model;
+            M.vol[i] = a.volatility;
+            M.spot[i] = a.spot;
+            M.weights[i] = d->product == MCG_MULTI_BASKET ? d->weights[i] : 0.0;
+            M.scales[i] = d->scales[i];
+            if (a.model == MCG_MODEL_LOCAL_VOLATILITY) {
+                const mcg_local_variance_grid& g = a.local_variance;
+                std::vector<double> gt(g.time_nodes, g.time_nodes + g.time_count);
+                const uint32_t nx = g.log_moneyness_count, ncell = nx - 1;
+                for (uint32_t s = 0; s < steps; ++s) {
+                    const int64_t key = host_total_key(nodes[s]);
+                    const size_t lo = lower_bound_key(gt, key);
+                    size_t c = (lo < gt.size() && host_total_key(gt[lo]) == key) ? lo : (lo == 0 ? 0 : lo - 1);
+                    c = std::min(c, gt.size() - 2);
+                    tc[static_cast<size_t>(i) * steps + s] = static_cast<int32_t>(c);
+                    tw[static_cast<size_t>(i) * steps + s] = (nodes[s] - gt[c]) / (gt[c + 1] - gt[c]);
+                }
+                std::vector<double2> bounds(ncell), cells(static_cast<size_t>(g.time_count) * ncell);
+                for (uint32_t c = 0; c < ncell; ++c)
+                    bounds[c] = make_double2(g.log_moneyness_nodes[c], g.log_moneyness_nodes[c + 1]);
+                for (uint32_t t = 0; t < g.time_count; ++t)
+                    for (uint32_t c = 0; c < ncell; ++c) {
+                        const double* row = g.values + static_cast<size_t>(t) * nx;
+                        const double inv = 1.0 / (g.log_moneyness_nodes[c + 1] - g.log_moneyness_nodes[c]);
+                        cells[static_cast<size_t>(t) * ncell + c] = make_double2(row[c], (row[c + 1] - row[c]) * inv);
+                    }
+                MCG_CUDA(A.bounds[i].upload(bounds));
+                MCG_CUDA(A.cells[i].upload(cells));
+                M.bounds[i] = A.bounds[i].ptr;
+                M.cells[i] = A.cells[i].ptr;
+                M.nx[i] = static_cast<int32_t>(nx);
+                M.x_first[i] = g.log_moneyness_nodes[0];
+                M.x_last[i] = g.log_moneyness_nodes[nx - 1];
+            }
+        }
+        MCG_CUDA(A.ratio.upload(ratio));
+        MCG_CUDA(A.time_cell.upload(tc));
+        MCG_CUDA(A.time_weight.upload(tw));
+        M.ratio = A.ratio.ptr;
+        M.time_cell = A.time_cell.ptr;
+        M.time_weight = A.time_weight.ptr;
+    }
+    if (M.bridge) {
+        std::vector<BridgeInstr> instrs;
+        std::vector<Op> ops;
+        uint32_t slots = 1;
+        if (!compile_bridge(nodes, instrs)) return fail(MCG_ERR_BRIDGE, "invalid bridge grid");
+        if (!bridge_program(nodes, instrs, ops, slots))
+            return fail(MCG_ERR_UNSUPPORTED, "bridge needs more than 32 live values");
+        std::vector<int4> prog;
+        std::vector<BridgeNode> bnodes;
+        int32_t zero_slot = 0;
+        if (!step_program(ops, steps, prog, bnodes, zero_slot))
+            return fail(MCG_ERR_BRIDGE, "internal: path program steps out of order");
+        for (const BridgeNode& b : bnodes)
+            if (b.out < 0 || b.out >= static_cast<int32_t>(slots) || b.left < 0 || b.left >= static_cast<int32_t>(slots) ||
+                b.right < 0 || b.right >= static_cast<int32_t>(slots) || b.rank < 0 || b.rank >= static_cast<int32_t>(steps))
+                return fail(MCG_ERR_BRIDGE, "internal: bridge node index out of range");
+        MCG_CUDA(A.step_prog.upload(prog));
+        MCG_CUDA(A.bridge_nodes.upload(bnodes));
+        M.step_prog = A.step_prog.ptr;
+        M.bridge_nodes = A.bridge_nodes.ptr;
+        M.zero_slot = zero_slot;
+        M.slot_count = slots;
+    }
+    if (rqmc) {
+        if (M.dimension > MCG_MAX_SOBOL_DIMENSION)
+            return fail(MCG_ERR_SOBOL_DIMENSION, "effective Sobol dimension exceeds 21201");
+        if (!d->sobol_directions || d->sobol_dimension_count < M.dimension)
+            return fail(MCG_ERR_SOBOL_DIMENSION, "sobol_directions cover fewer dimensions than the plan needs");
+        std::vector<uint32_t> dirs(d->sobol_directions, d->sobol_directions + static_cast<size_t>(M.dimension) * 32u);
+        MCG_CUDA(A.directions.upload(dirs));
+        const uint32_t rows = scrambles * M.dimension;
+        MCG_CUDA(A.scr_dirs.alloc(static_cast<size_t>(rows) * 32u));
+        MCG_CUDA(A.scr_shift.alloc(rows));
+        MCG_CUDA(A.scr_low.alloc(static_cast<size_t>(rows) * 32u));
+        scramble_table_kernel<<<(rows + 127) / 128, 128, 0, stream>>>(A.directions.ptr, M.dimension, scrambles, 0u,
+                                                                     M.seed, A.scr_dirs.ptr, A.scr_shift.ptr);
+        MCG_CUDA(cudaGetLastError());
+        scramble_low_kernel<<<(rows * 32u + 127) / 128, 128, 0, stream>>>(A.scr_dirs.ptr, rows, A.scr_low.ptr);
+        MCG_CUDA(cudaGetLastError());
+        M.scr_dirs = A.scr_dirs.ptr;
+        M.scr_shift = A.scr_shift.ptr;
+        M.scr_low = A.scr_low.ptr;
+    }
+    M.product = d->product;
+    M.side = d->side;
+    M.strike = d->strike;
+    M.notional = d->notional;
+    M.smoothing = d->smoothing_half_width;
+    M.df = std::exp(rc.log_discount(d->payment_time));
+    if (multi_asset_smem(M) > 200 * 1024) return fail(MCG_ERR_UNSUPPORTED, "bridge slots exceed shared memory");
+    const uint32_t tiles = static_cast<uint32_t>((units + kThreads - 1) / kThreads);
+    MCG_CUDA(A.partials.alloc(static_cast<size_t>(tiles) * scrambles));
+    MCG_CUDA(A.records.alloc(scrambles));
+    MCG_CUDA(A.error.alloc(1));
+    const ErrorWord init{~0ull, 0, 0, 0, 0};
+    MCG_CUDA(cudaMemcpyAsync(A.error.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, stream);
+    cudaError_t e = launch_multi_asset(M, scrambles, A.partials.ptr, A.error.ptr, stream);
+    if (e == cudaSuccess) {
+        reduce_tiles_kernel<<<dim3(1, scrambles), 256, 0, stream>>>(A.partials.ptr, tiles, 1, A.records.ptr);
+        e = cudaGetLastError();
+    }
+    cudaEventRecord(t1, stream);
+    std::vector<StatRecord> rec(scrambles);
+    ErrorWord ew{};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rec.data(), A.records.ptr, scrambles * sizeof(StatRecord),
+                                              cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ew, A.error.ptr, sizeof(ew), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    float ms = 0.0f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
+    r->kernel_launches = 2 + (rqmc ? 2 : 0);
+    r->device_ms = ms;
+    r->time_steps = steps;
+    r->dimension = M.dimension;
+    if (ew.key != ~0ull) {
+        r->error.code = static_cast<int32_t>(ew.key & 0xff);
+        r->error.sampling_unit = ew.key >> 8;
+        return fail(static_cast<mcg_status>(r->error.code),
+                    "sampling unit " + std::to_string(r->error.sampling_unit) + " failed");
+    }
+    HostStat h;
+    if (!rqmc) {
+        h = {rec[0].sum, rec[0].corr, static_cast<uint64_t>(rec[0].count), rec[0].mean, rec[0].m2};
+    } else {
+        std::vector<double> reps(scrambles);
+        for (uint32_t sc = 0; sc < scrambles; ++sc) reps[sc] = (rec[sc].sum + rec[sc].corr) / static_cast<double>(units);
+        h = two_pass(reps);
+    }
+    const uint64_t independent = rqmc ? scrambles : units;
+    r->price_statistics = {h.sum, h.corr, h.count, h.mean, h.m2};
+    r->price = make_estimate(h, independent, 1.0);
+    r->sampling_variance = h.count > 1 ? h.m2 / static_cast<double>(h.count - 1) : 0.0;
+    r->independent_sampling_units = independent;
+    r->evaluated_paths = units * scrambles * (M.antithetic ? 2 : 1);
+    return MCG_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 uint32_t mcg_abi_version(void) { return MCG_ABI_VERSION; }
@@ -2543,6 +2921,10 @@ mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint6
     if (low) cudaFree(low);
     if (e != cudaSuccess) return fail(MCG_ERR_CUDA, cudaGetErrorString(e));
     return MCG_OK;
+}
+
+mcg_status mcg_multi_asset_price(const mcg_multi_asset_desc* desc, void* stream, mcg_multi_asset_result* result) {
+    return multi_asset_price(desc, static_cast<cudaStream_t>(stream), result);
 }
 
 }  // extern "C"

@@ -155,6 +155,40 @@ class Result(C.Structure):
     ]
 
 
+# ---- correlated multi-asset paths ----
+MAX_ASSETS = 8
+MULTI_BASKET, MULTI_WORST_OF = 0, 1
+
+
+class AssetDesc(C.Structure):
+    _fields_ = [
+        ("model", C.c_int32), ("spot", C.c_double), ("dividend_curve", Curve), ("volatility", C.c_double),
+        ("local_variance", LocalVarianceGrid),
+    ]
+
+
+class MultiAssetDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_uint32), ("asset_count", C.c_uint32), ("assets", C.POINTER(AssetDesc)),
+        ("discount_curve", Curve), ("correlation_count", C.c_uint32), ("correlation_times", _dp),
+        ("correlations", _dp), ("maximum_step", C.c_double), ("expiry", C.c_double), ("payment_time", C.c_double),
+        ("engine", C.c_int32), ("master_seed", C.c_uint64), ("sampling_units", C.c_uint64),
+        ("scramble_count", C.c_uint32), ("antithetic", C.c_int32), ("brownian_bridge", C.c_int32),
+        ("reduction_block_size", C.c_uint64), ("sobol_dimension_count", C.c_uint32), ("sobol_directions", _up),
+        ("product", C.c_int32), ("side", C.c_int32), ("strike", C.c_double), ("notional", C.c_double),
+        ("weights", _dp), ("scales", _dp), ("smoothing_half_width", C.c_double),
+    ]
+
+
+class MultiAssetResult(C.Structure):
+    _fields_ = [
+        ("price_statistics", Statistics), ("price", Estimate), ("sampling_variance", C.c_double),
+        ("evaluated_paths", C.c_uint64), ("independent_sampling_units", C.c_uint64),
+        ("time_steps", C.c_uint32), ("dimension", C.c_uint32), ("kernel_launches", C.c_uint32),
+        ("device_ms", C.c_float), ("error", ErrorRecord),
+    ]
+
+
 class ResultBuffers:
     """Caller-owned result storage for `products` products and `nodes` node entries."""
 

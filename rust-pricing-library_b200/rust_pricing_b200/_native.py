@@ -20,7 +20,7 @@ EXPORTS = (
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
     "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient", "mcg_book_create", "mcg_book_evaluate",
     "mcg_book_destroy", "mcg_surface_local_variance_grid", "mcg_surface_total_variance", "mcg_vega_kt_project",
-    "mcg_lsm_dual",
+    "mcg_lsm_dual", "mcg_multi_asset_price",
 )
 
 _lib = None
@@ -94,6 +94,8 @@ def library() -> C.CDLL:
     lib.mcg_book_evaluate.argtypes = [vp, vp, C.POINTER(A.Estimate), C.POINTER(A.BookReport)]
     lib.mcg_book_evaluate.restype = C.c_int
     lib.mcg_book_destroy.argtypes = [vp]
+    lib.mcg_multi_asset_price.argtypes = [C.POINTER(A.MultiAssetDesc), vp, C.POINTER(A.MultiAssetResult)]
+    lib.mcg_multi_asset_price.restype = C.c_int
     if lib.mcg_abi_version() != A.ABI_VERSION:
         raise EngineError(1, "engine library ABI version mismatch")
     _lib = lib
@@ -193,6 +195,15 @@ def lsm_dual(spec, lsm, continuation_inner_paths: int, exercise_inner_paths: int
     status = library().mcg_lsm_dual(C.byref(desc), C.byref(ldesc), C.byref(dual), C.c_void_p(stream),
                                     C.byref(out))
     check(status, out.error)
+    return out
+
+
+def multi_asset_price(spec, stream: int = 0) -> A.MultiAssetResult:
+    """mcg_multi_asset_price: a basket or worst-of option on correlated
+    Black--Scholes / local-volatility assets, on the GPU."""
+    out = A.MultiAssetResult()
+    desc = spec.desc()
+    check(library().mcg_multi_asset_price(C.byref(desc), C.c_void_p(stream), C.byref(out)), out.error)
     return out
 
 

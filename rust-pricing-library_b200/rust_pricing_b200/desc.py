@@ -265,3 +265,111 @@ class LsmSpec:
         d.mlp_seed = self.mlp_seed & 0xFFFFFFFFFFFFFFFF
         self._keep[:] = [d]
         return d
+
+
+@dataclass
+class AssetSpec:
+    """One asset of a multi-asset plan: Black--Scholes (volatility) or local
+    volatility (its own variance grid), its spot and dividend-yield curve."""
+
+    spot: float = 100.0
+    volatility: float = 0.2
+    model: int = A.MODEL_BLACK_SCHOLES
+    local_variance: Optional[LocalVarianceSpec] = None
+    dividend_times: Sequence[float] = (0.0, 1.0)
+    dividend_factors: Sequence[float] = (1.0, 1.0)
+
+
+@dataclass
+class MultiAssetSpec:
+    """mcg_multi_asset_desc: correlated assets, a correlation term structure
+    (matrices in force from their times), the common time grid's maximum step,
+    the engine and a basket or worst-of option."""
+
+    assets: Sequence[AssetSpec]
+    correlations: Sequence  # list of (time, n x n matrix)
+    expiry: float = 1.0
+    payment_time: Optional[float] = None
+    maximum_step: float = 0.25
+    product: int = A.MULTI_BASKET
+    side: int = A.CALL
+    strike: float = 100.0
+    notional: float = 1.0
+    weights: Optional[Sequence[float]] = None
+    scales: Optional[Sequence[float]] = None
+    smoothing_half_width: float = 0.0
+    engine: int = A.ENGINE_PSEUDO
+    master_seed: int = 511
+    sampling_units: int = 4096
+    scramble_count: int = 8
+    antithetic: bool = True
+    brownian_bridge: bool = True
+    reduction_block_size: int = 256
+    discount_times: Sequence[float] = (0.0, 2.0)
+    discount_factors: Sequence[float] = (1.0, float(np.exp(-0.06)))
+    _keep: list = field(default_factory=list, repr=False)
+
+    def desc(self) -> A.MultiAssetDesc:
+        keep = self._keep
+        keep.clear()
+        n = len(self.assets)
+        d = A.MultiAssetDesc()
+        d.abi_version = A.ABI_VERSION
+        d.asset_count = n
+        arr = (A.AssetDesc * n)()
+        for i, a in enumerate(self.assets):
+            q = arr[i]
+            q.model, q.spot, q.volatility = a.model, a.spot, a.volatility
+            t, f = _f64(a.dividend_times), _f64(a.dividend_factors)
+            keep += [t, f]
+            q.dividend_curve = A.Curve(len(t), _ptr(t), _ptr(f))
+            if a.local_variance is not None:
+                g = a.local_variance
+                gt, gx, gv = _f64(g.time_nodes), _f64(g.log_moneyness_nodes), _f64(g.values).ravel()
+                keep += [gt, gx, gv]
+                q.local_variance = A.LocalVarianceGrid(len(gt), len(gx), _ptr(gt), _ptr(gx), _ptr(gv), g.floor, g.cap)
+        keep.append(arr)
+        d.assets = C.cast(arr, C.POINTER(A.AssetDesc))
+        t, f = _f64(self.discount_times), _f64(self.discount_factors)
+        keep += [t, f]
+        d.discount_curve = A.Curve(len(t), _ptr(t), _ptr(f))
+        ct = _f64([c[0] for c in self.correlations])
+        cm = _f64([np.asarray(c[1], dtype=np.float64).ravel() for c in self.correlations]).ravel()
+        keep += [ct, cm]
+        d.correlation_count = len(ct)
+        d.correlation_times = _ptr(ct)
+        d.correlations = _ptr(cm)
+        d.maximum_step = self.maximum_step
+        d.expiry = self.expiry
+        d.payment_time = self.expiry if self.payment_time is None else self.payment_time
+        d.engine = self.engine
+        d.master_seed = self.master_seed & 0xFFFFFFFFFFFFFFFF
+        d.sampling_units = self.sampling_units
+        d.scramble_count = self.scramble_count
+        d.antithetic = int(self.antithetic)
+        d.brownian_bridge = int(self.brownian_bridge)
+        d.reduction_block_size = self.reduction_block_size
+        if self.engine == A.ENGINE_RQMC:
+            dims = min(sobol.DIMENSIONS, n * self.step_hint())
+            words = np.ascontiguousarray(sobol.direction_words(dims))
+            keep.append(words)
+            d.sobol_dimension_count = dims
+            d.sobol_directions = _ptr(words, C.c_uint32)
+        d.product, d.side, d.strike, d.notional = self.product, self.side, self.strike, self.notional
+        w = _f64(self.weights if self.weights is not None else [1.0 / n] * n)
+        sc = _f64(self.scales if self.scales is not None else [1.0] * n)
+        keep += [w, sc]
+        d.weights, d.scales = _ptr(w), _ptr(sc)
+        d.smoothing_half_width = self.smoothing_half_width
+        keep.append(d)
+        return d
+
+    def step_hint(self) -> int:
+        """An upper bound of the common time grid's steps."""
+        events = {0.0, float(self.expiry)}
+        events |= {float(c[0]) for c in self.correlations if 0.0 < float(c[0]) < self.expiry}
+        for a in self.assets:
+            if a.local_variance is not None:
+                events |= {float(t) for t in a.local_variance.time_nodes if float(t) <= self.expiry}
+        ev = sorted(events)
+        return int(sum(max(1, int(np.ceil((b - a) / self.maximum_step))) for a, b in zip(ev, ev[1:]))) + 4

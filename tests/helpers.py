@@ -91,6 +91,8 @@ def oracle():
     lib.oracle_lsm_fit.argtypes = [C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl), u64,
                                    C.POINTER(A.LsmDesc), C.POINTER(A.LsmDateModel)]
     lib.oracle_lsm_fit.restype = C.c_int
+    lib.oracle_multi_asset_price.argtypes = [C.POINTER(A.MultiAssetDesc), C.POINTER(A.MultiAssetResult), C.c_int]
+    lib.oracle_multi_asset_price.restype = C.c_int
     _oracle = lib
     return lib
 
@@ -143,3 +145,13 @@ def dptr(array):
 
 def uptr(array):
     return array.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def oracle_multi(spec, threads: int | None = None):
+    """Run the oracle's multi-asset evaluation; returns the MultiAssetResult."""
+    out = A.MultiAssetResult()
+    desc = spec.desc()
+    rc = oracle().oracle_multi_asset_price(C.byref(desc), C.byref(out), threads or os.cpu_count() or 1)
+    if rc != 0:
+        raise RuntimeError(f"oracle multi-asset status {A.STATUS_NAMES.get(rc, rc)}")
+    return out
