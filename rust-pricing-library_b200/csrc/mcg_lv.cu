@@ -188,8 +188,10 @@ cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t un
     for (int k = 0; k < np; ++k) cb |= P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
     // Two paths per thread pay for discrete products (B200: 87.4 -> 75.8 ms on the
     // 2^24-path local-vol workload); a continuous barrier's bridge state makes
-    // the pair too large (25.0 -> 32.6 ms), so those kernels keep one.
-    const bool two = E == 1 && np <= 2 && !cb && !detail && unit_begin == 0 && units == P.units;
+    // the pair too large (25.0 -> 32.6 ms), so those kernels keep one, and so
+    // do plans with discrete dividends (their observation coordinates are
+    // compiled out of the two-path kernels, which otherwise spill).
+    const bool two = E == 1 && np <= 2 && !cb && !P.dividends && !detail && unit_begin == 0 && units == P.units;
     const int Q = two ? 2 : 1;
     const size_t smem = lv_path_smem(P, Q);
     const dim3 grid(static_cast<unsigned>((units + kThreads * Q - 1) / (kThreads * Q)), scrambles);

@@ -268,29 +268,39 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             }
         }
         if (obs >= 0) {
-            // Observed spots: the state itself, or with discrete dividends the
-            // node coordinate a S + b f of each evolution's spot runtime (and the
-            // pre-dividend one on an ex-date), local_vol_valuation.rs:221-247.
-            double spot[QE], pre[QE];
-            bool with_pre = false;
+            if constexpr (Q == 1) {
+                // Observed spots: the state itself, or with discrete dividends the
+                // node coordinate a S + b f of each evolution's spot runtime (and
+                // the pre-dividend one on an ex-date), local_vol_valuation.rs:221-247.
+                double spot[QE], pre[QE];
+                bool with_pre = false;
 #pragma unroll
-            for (int i = 0; i < QE; ++i) spot[i] = pre[i] = f[i];
-            if (P.dividends) {
-                with_pre = P.obs_div[obs].w != 0.0;
+                for (int i = 0; i < QE; ++i) spot[i] = pre[i] = f[i];
+                if (P.dividends) {
+                    with_pre = P.obs_div[obs].w != 0.0;
 #pragma unroll
-                for (int i = 0; i < QE; ++i) {
-                    const int which = ev_which<E>(i % E);
-                    const double4 c = P.lv_obs_div[static_cast<size_t>(which) * P.observation_count + obs];
-                    const double s0 = P.spot_variant[which];
-                    spot[i] = c.x * s0 + c.y * f[i];
-                    pre[i] = c.z * s0 + c.w * f[i];
+                    for (int i = 0; i < QE; ++i) {
+                        const int which = ev_which<E>(i % E);
+                        const double4 c = P.lv_obs_div[static_cast<size_t>(which) * P.observation_count + obs];
+                        const double s0 = P.spot_variant[which];
+                        spot[i] = c.x * s0 + c.y * f[i];
+                        pre[i] = c.z * s0 + c.w * f[i];
+                    }
                 }
-            }
 #pragma unroll
-            for (int k = 0; k < NP; ++k)
-                if (k < static_cast<int>(P.product_count))
-                    acc_observe_n<QE>(P.products[k], acc[k], static_cast<uint32_t>(obs), spot, P.smoothing, pre,
-                                      with_pre);
+                for (int k = 0; k < NP; ++k)
+                    if (k < static_cast<int>(P.product_count))
+                        acc_observe_n<QE>(P.products[k], acc[k], static_cast<uint32_t>(obs), spot, P.smoothing, pre,
+                                          with_pre);
+            } else {
+                // Two paths per thread: plans without dividends (the launch
+                // helper's choice), so the observed spot is the state.
+#pragma unroll
+                for (int k = 0; k < NP; ++k)
+                    if (k < static_cast<int>(P.product_count))
+                        acc_observe_n<QE, false>(P.products[k], acc[k], static_cast<uint32_t>(obs), f, P.smoothing,
+                                                 f, false);
+            }
         }
     }
     // Close the last bridge interval: the terminal node's variance.

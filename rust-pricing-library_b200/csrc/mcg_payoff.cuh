@@ -65,7 +65,8 @@ MCG_HD bool monitored(const ProductParams& p, uint32_t obs) {
 // before the dividend, `pre` (with_pre): its distance is the maximum (smoothed:
 // the compact-C2 smooth maximum) of the pre- and post-dividend distances
 // (crates/pricing/src/engine/payoff/compile.rs:315-346).
-template <int N>
+// PRE = false compiles the pre-dividend check out (plans without dividends).
+template <int N, bool PRE = true>
 MCG_HD void acc_observe_n(const ProductParams& p, ProductAcc (&s)[N], uint32_t obs, const double (&spot)[N],
                           double smoothing, const double (&pre)[N], bool with_pre) {
 #pragma unroll
@@ -96,7 +97,7 @@ MCG_HD void acc_observe_n(const ProductParams& p, ProductAcc (&s)[N], uint32_t o
 #pragma unroll
         for (int i = 0; i < N; ++i) {
             double dist = p.barrier_direction == MCG_BARRIER_UP ? spot[i] - p.barrier : p.barrier - spot[i];
-            if (with_pre) {
+            if (PRE && with_pre) {
                 const double pd = p.barrier_direction == MCG_BARRIER_UP ? pre[i] - p.barrier : p.barrier - pre[i];
                 if (smoothing > 0.0) {
                     double dl, dr;
