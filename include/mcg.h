@@ -795,6 +795,61 @@ typedef struct mcg_multi_asset_result {
 
 mcg_status mcg_multi_asset_price(const mcg_multi_asset_desc* desc, void* stream, mcg_multi_asset_result* result);
 
+/* ---- Bump-and-revalue on common random numbers ----
+ *
+ * PricingSource::scenarios / bump_cost and CompiledScenarios::compile /
+ * evaluate (crates/pricing/src/engine/risk/bump.rs:362-690): every request
+ * moves one input by a half-width h -- the spot (Delta, Gamma) or the
+ * Black--Scholes volatility (Vega) -- as an absolute amount or relative to the
+ * input's level; requests that move the same input by the same amount share
+ * one up/down pair of scenario sides, in first-use order.  Each side is the
+ * base plan with that input moved, on the base plan's seeds (the same random
+ * coordinates), so the differences are common-random-number differences.  All
+ * sides (and the base plan, when a Gamma is requested) are priced in ONE
+ * launch: a grid of (tile, scramble, side) CTAs, each staging its side's plan
+ * and evaluating a 128-unit tile with the single-plan tile functions.  The
+ * estimates pair the sides unit by unit: Delta/Vega the mean of
+ * (up_u - down_u) / 2h, Gamma the mean of ((up_u - base_u) + (down_u - base_u)) / h^2,
+ * with the standard error of that mean; a unit is a pseudo-random sampling
+ * unit (antithetic pairs averaged) or an RQMC scramble's mean over its points.
+ * The base plan is single-product, price-only, without discrete dividends. */
+typedef enum mcg_bump_measure {
+    MCG_BUMP_SPOT_DELTA = 0,
+    MCG_BUMP_SPOT_GAMMA = 1,
+    MCG_BUMP_VOLATILITY_VEGA = 2  /* Black--Scholes plans */
+} mcg_bump_measure;
+
+typedef struct mcg_bump_request {
+    int32_t measure;   /* mcg_bump_measure */
+    int32_t relative;  /* 1: h = size x the input's level (BumpSize::Relative); 0: h = size */
+    double size;       /* positive */
+} mcg_bump_request;
+
+typedef struct mcg_bump_estimate {
+    int32_t measure;
+    uint32_t scenario;       /* the up/down pair used, in first-use order */
+    double amount;           /* h */
+    double value;
+    double standard_error;   /* of the mean of the paired per-unit differences */
+    uint64_t units;          /* paired sampling units */
+    double up_price, down_price;
+} mcg_bump_estimate;
+
+typedef struct mcg_bump_report {
+    uint32_t scenarios;
+    uint32_t sides;          /* side plans priced by the launch (2 x scenarios, + 1 base for Gamma) */
+    uint64_t evaluations;    /* BumpCost::evaluations: 2 x scenarios + 1 when a Gamma is requested */
+    mcg_estimate base_price; /* the base plan's price (evaluated when a Gamma is requested) */
+    uint64_t path_steps;     /* simulated path-steps of the launch */
+    uint32_t kernel_launches;
+    float device_ms;
+    mcg_error_record error;  /* first failing side: code, the side index in `step`, unit, value */
+} mcg_bump_report;
+
+/* `estimates` receives one entry per request; `report` may be NULL. */
+mcg_status mcg_bump_evaluate(const mcg_plan_desc* base, const mcg_bump_request* requests, uint32_t request_count,
+                             void* stream, mcg_bump_estimate* estimates, mcg_bump_report* report);
+
 /* ---- Pricing without device allocation (no counterpart in the reference) ----
  *
  * For callers that must not allocate GPU memory while pricing (a service that

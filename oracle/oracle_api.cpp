@@ -14,6 +14,8 @@ int evaluate(const mcg_plan_desc* desc, mcg_result* result, int threads);
 const char* last_error();
 int unit_shocks_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out);
 int unit_values_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out);
+int bump_evaluate_api(const mcg_plan_desc* desc, const mcg_bump_request* req, uint32_t count,
+                      mcg_bump_estimate* est, mcg_bump_report* rep, int threads);
 int time_grid_api(const mcg_plan_desc* desc, double* nodes_out, uint32_t capacity, uint32_t* count);
 std::vector<double> pchip_derivatives(const std::vector<double>& t, const std::vector<double>& v);
 int vega_kt_project(const double* times, uint32_t nt, const double* xs, uint32_t nx, const double* nodes,
@@ -131,6 +133,11 @@ int oracle_unit_shocks(const mcg_plan_desc* desc, uint32_t scramble, uint64_t un
 
 int oracle_unit_values(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit, double* out) {
     return oracle::unit_values_api(desc, scramble, unit, out);
+}
+
+int oracle_bump_evaluate(const mcg_plan_desc* desc, const mcg_bump_request* requests, uint32_t count,
+                         mcg_bump_estimate* estimates, mcg_bump_report* report, int threads) {
+    return oracle::bump_evaluate_api(desc, requests, count, estimates, report, threads);
 }
 
 int oracle_time_grid(const mcg_plan_desc* desc, double* nodes, uint32_t capacity,

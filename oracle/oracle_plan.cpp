@@ -1702,6 +1702,125 @@ int unit_values_api(const mcg_plan_desc* desc, uint32_t scramble, uint64_t unit,
     return MCG_OK;
 }
 
+// Bump-and-revalue on common random numbers: PricingSource::scenarios
+// (crates/pricing/src/engine/risk/bump.rs:384-462) for spot and constant-
+// volatility moves, CompiledScenarios::compile / evaluate (:568-690): every
+// side is the plan with one input moved, on the same seeds; its sampling units
+// (units_from_recorded, :490-523) are the unit values (pseudo-MC, antithetic
+// pairs averaged) or the scramble means (RQMC); each estimate is paired(),
+// the ordered two-pass statistics of the per-unit differences (:556-566).
+int bump_evaluate_api(const mcg_plan_desc* desc, const mcg_bump_request* req, uint32_t count,
+                      mcg_bump_estimate* est, mcg_bump_report* rep, int threads) {
+    if (!desc || !req || !est || count == 0) return MCG_ERR_INVALID_ARGUMENT;
+    if (rep) std::memset(rep, 0, sizeof(*rep));
+    if (desc->product_count != 1) return MCG_ERR_UNSUPPORTED;
+    struct Sc {
+        int target;
+        double amount;
+    };
+    std::vector<Sc> sc;
+    std::vector<uint32_t> sc_of(count);
+    bool gamma = false;
+    for (uint32_t i = 0; i < count; ++i) {
+        const int target = req[i].measure == MCG_BUMP_VOLATILITY_VEGA ? 1 : 0;
+        if (!(req[i].size > 0.0)) return MCG_ERR_INVALID_ARGUMENT;
+        if (target == 1 && desc->model != MCG_MODEL_BLACK_SCHOLES) return MCG_ERR_INVALID_ARGUMENT;
+        const double level = target == 0 ? desc->spot : desc->volatility;
+        const double amount = req[i].relative ? req[i].size * level : req[i].size;
+        uint32_t j = 0;
+        while (j < sc.size() && !(sc[j].target == target && sc[j].amount == amount)) ++j;
+        if (j == sc.size()) sc.push_back({target, amount});
+        sc_of[i] = j;
+        gamma |= req[i].measure == MCG_BUMP_SPOT_GAMMA;
+    }
+    const uint32_t ns = static_cast<uint32_t>(sc.size());
+    const uint32_t sides = 2 * ns + (gamma ? 1u : 0u);
+    std::vector<std::vector<double>> units_of(sides);
+    std::vector<double> side_price(sides);
+    uint64_t independent = 0;
+    for (uint32_t k = 0; k < sides; ++k) {
+        mcg_plan_desc s = *desc;
+        if (k < 2 * ns) {
+            const double sign = k % 2 == 0 ? 1.0 : -1.0;
+            if (sc[k / 2].target == 0) s.spot = desc->spot + sign * sc[k / 2].amount;
+            else s.volatility = desc->volatility + sign * sc[k / 2].amount;
+            if (!(s.spot > 0.0) || (sc[k / 2].target == 1 && !(s.volatility > 0.0))) return MCG_ERR_INVALID_ARGUMENT;
+        }
+        Plan p;
+        if (!build_plan(&s, p)) return MCG_ERR_INVALID_ARGUMENT;
+        mcg_error_record err{};
+        if (p.engine == MCG_ENGINE_PSEUDO) {
+            std::vector<Statistics> stats;
+            if (!map_reduce(p, 0, p.units, threads, stats, err)) return err.code;
+            side_price[k] = stats[MCG_PRICE].sum.total() / static_cast<double>(p.units);
+            std::vector<double>& u = units_of[k];
+            u.assign(p.units, 0.0);
+            std::atomic<uint64_t> next{0};
+            std::atomic<int> failed{0};
+            auto worker = [&]() {
+                std::vector<double> vals, nodes;
+                Failure f;
+                for (;;) {
+                    const uint64_t b = next.fetch_add(4096);
+                    if (b >= p.units) break;
+                    for (uint64_t i = b; i < std::min<uint64_t>(p.units, b + 4096); ++i) {
+                        if (!unit_values(p, 0, i, vals, nodes, f)) {
+                            failed = f.code;
+                            return;
+                        }
+                        u[i] = vals[MCG_PRICE];
+                    }
+                }
+            };
+            std::vector<std::thread> pool;
+            for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(worker);
+            for (auto& t : pool) t.join();
+            if (failed) return failed;
+            independent = p.units;
+        } else {
+            std::vector<double>& u = units_of[k];
+            NeumaierSum total;
+            for (uint32_t sidx = 0; sidx < p.scrambles; ++sidx) {
+                std::vector<Statistics> within;
+                if (!map_reduce(p, sidx, p.units, threads, within, err)) return err.code;
+                u.push_back(within[MCG_PRICE].sum.total() / static_cast<double>(p.units));
+                total.add(u.back());
+            }
+            side_price[k] = total.total() / static_cast<double>(p.scrambles);
+            independent = p.scrambles;
+        }
+    }
+    const uint32_t base = 2 * ns;
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t j = sc_of[i];
+        const double h = sc[j].amount;
+        const bool second = req[i].measure == MCG_BUMP_SPOT_GAMMA;
+        const std::vector<double>& up = units_of[2 * j];
+        const std::vector<double>& down = units_of[2 * j + 1];
+        std::vector<double> diff(up.size());
+        for (size_t q = 0; q < up.size(); ++q)
+            diff[q] = second ? ((up[q] - units_of[base][q]) + (down[q] - units_of[base][q])) / (h * h)
+                             : (up[q] - down[q]) / (2.0 * h);
+        if (diff.size() < 2) return MCG_ERR_INVALID_ARGUMENT;
+        NeumaierSum sum;
+        for (double v : diff) sum.add(v);
+        const CenteredMoment m = CenteredMoment::two_pass(diff);
+        const double n = static_cast<double>(diff.size());
+        const double value = sum.total() / n;
+        const double se = std::sqrt(m.second_moment / (n - 1.0) / n);
+        est[i] = mcg_bump_estimate{req[i].measure, j, h, value, se, static_cast<uint64_t>(diff.size()),
+                                   side_price[2 * j], side_price[2 * j + 1]};
+    }
+    if (rep) {
+        rep->scenarios = ns;
+        rep->sides = sides;
+        rep->evaluations = 2ull * ns + (gamma ? 1u : 0u);
+        if (gamma) rep->base_price.value = side_price[base];
+        rep->base_price.effective_sampling_units = independent;
+    }
+    return MCG_OK;
+}
+
 // One Log-Euler path on given nodes, forwards, grid and shocks, and its
 // reverse sweep for given dPayoff/dS_k seeds (the equation-(10) step
 // adjoints of the reference's local-vol fixtures): the path's states and the

@@ -37,6 +37,7 @@ UNITS = [
     ("mcg_lv32.cu", []),
     ("mcg_vegakt.cu", []),
     ("mcg_multi.cu", ["-fmad=false"]),
+    ("mcg_bump.cu", ["-fmad=false"]),
 ]
 
 

@@ -136,9 +136,12 @@ __device__ __forceinline__ void single_terminal_values(const DevicePlan& P, cons
 // One 128-unit tile of the single-terminal path (European/Digital at expiry),
 // price-only or risk: unit `point` of scramble `scramble` per thread, the
 // CTA's statistics records written at tile_out[k * kComponents + c].
+// unit_price (optional): receives the first product's discounted price of
+// each unit (antithetic pairs averaged) at unit_price[point].
 template <bool kRisk>
 __device__ __forceinline__ void bs_terminal_tile(const DevicePlan& P, Stat* s_red, uint32_t scramble, uint64_t point,
-                                                 bool valid, StatRecord* tile_out, uint32_t mask) {
+                                                 bool valid, StatRecord* tile_out, uint32_t mask,
+                                                 double* unit_price = nullptr) {
     const uint64_t unit = valid ? point : 0;
     NormalSource ns;
     ns.rqmc = P.engine == MCG_ENGINE_RQMC;
@@ -181,6 +184,7 @@ __device__ __forceinline__ void bs_terminal_tile(const DevicePlan& P, Stat* s_re
             }
             vals[MCG_PRICE] = price;
         }
+        if (unit_price != nullptr && k == 0 && valid) unit_price[point] = vals[MCG_PRICE];
         cta_reduce_write<kComponents>(vals, valid, mask, tile_out + static_cast<size_t>(k) * kComponents, s_red);
     }
 }
@@ -191,7 +195,7 @@ __device__ __forceinline__ void bs_terminal_tile(const DevicePlan& P, Stat* s_re
 template <int NP>
 __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, uint32_t scramble, uint64_t point,
                                              bool valid, StatRecord* tile_out, uint32_t mask, ErrorWord* err,
-                                             int detail) {
+                                             int detail, double* unit_price = nullptr) {
     const uint64_t unit = valid ? point : 0;
     NormalSource ns;
     ns.rqmc = P.engine == MCG_ENGINE_RQMC;
@@ -272,6 +276,7 @@ __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, u
                 for (int c = 0; c < kComponents; ++c) vals[c] = (vals[c] + comp[c]) * 0.5;
             }
         }
+        if (unit_price != nullptr && k == 0 && valid) unit_price[point] = vals[MCG_PRICE];
         cta_reduce_write<kComponents>(vals, valid, mask, tile_out + static_cast<size_t>(k) * kComponents, s_red);
     }
 }

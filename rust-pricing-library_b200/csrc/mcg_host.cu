@@ -31,6 +31,7 @@
 #include "mcg_surface.cuh"
 #include "mcg_dividends.h"
 #include "mcg_multi.cuh"
+#include "mcg_bump.cuh"
 
 namespace mcg {
 cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -2748,6 +2749,250 @@ mcg_status multi_asset_price(const mcg_multi_asset_desc* d, cudaStream_t stream,
     return MCG_OK;
 }
 
+// ---- bump-and-revalue on common random numbers
+
+// Compiled sides and device arrays of one bump evaluation, released on every exit.
+struct BumpArrays {
+    std::vector<mcg_plan*> plans;
+    DeviceArray<DevicePlan> dplans;
+    DeviceArray<uint32_t> masks;
+    DeviceArray<StatRecord> partials, records, pair_partials, pair_records;
+    DeviceArray<double> unit_prices;
+    DeviceArray<BumpPair> pairs;
+    DeviceArray<ErrorWord> errors;
+    ~BumpArrays() {
+        for (mcg_plan* p : plans) delete p;
+        dplans.release();
+        masks.release();
+        for (auto* a : {&partials, &records, &pair_partials, &pair_records}) a->release();
+        unit_prices.release();
+        pairs.release();
+        errors.release();
+    }
+};
+
+// One scenario: the input a request moves and the half-width
+// (Scenario, crates/pricing/src/engine/risk/bump.rs:35-44).
+struct BumpScenario {
+    int target;  // 0 spot, 1 volatility
+    double amount;
+};
+
+// paired(), bump.rs:556-566: the mean of the ordered per-unit differences and
+// the standard error of that mean.
+mcg_status bump_paired(const HostStat& h, double& value, double& se) {
+    if (h.count < 2) return fail(MCG_ERR_INVALID_ARGUMENT, "a paired standard error needs at least two sampling units");
+    const double n = static_cast<double>(h.count);
+    value = h.total() / n;
+    se = std::sqrt(h.m2 / (n - 1.0) / n);
+    return MCG_OK;
+}
+
+mcg_status bump_evaluate(const mcg_plan_desc* d, const mcg_bump_request* req, uint32_t count, cudaStream_t stream,
+                         mcg_bump_estimate* est, mcg_bump_report* rep) {
+    if (!d || !req || !est) return fail(MCG_ERR_INVALID_ARGUMENT, "null descriptor, requests or estimates");
+    if (rep) std::memset(rep, 0, sizeof(*rep));
+    if (count == 0 || count > 64) return fail(MCG_ERR_INVALID_ARGUMENT, "request_count must be 1..64");
+    if (d->product_count != 1 || d->request_delta || d->request_gamma || d->request_vega ||
+        d->request_local_vega_nodes)
+        return fail(MCG_ERR_UNSUPPORTED, "a bump plan's base is one product, price only");
+    if (d->discrete_dividends.count)
+        return fail(MCG_ERR_UNSUPPORTED, "a bump plan's base has no discrete dividends");
+    if (d->precision != MCG_PRECISION_F64) return fail(MCG_ERR_UNSUPPORTED, "a bump plan runs in FP64");
+    // The distinct scenarios in first-use order (PricingSource::scenarios,
+    // bump.rs:446-462): Delta and Gamma of one size share a pair.
+    std::vector<BumpScenario> sc;
+    std::vector<uint32_t> sc_of(count);
+    bool gamma = false;
+    for (uint32_t i = 0; i < count; ++i) {
+        const mcg_bump_request& q = req[i];
+        if (q.measure < MCG_BUMP_SPOT_DELTA || q.measure > MCG_BUMP_VOLATILITY_VEGA)
+            return fail(MCG_ERR_INVALID_ARGUMENT, "request " + std::to_string(i) + ": unknown measure");
+        if (!(q.size > 0.0) || !std::isfinite(q.size))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "request " + std::to_string(i) + ": bump_size must be positive");
+        const int target = q.measure == MCG_BUMP_VOLATILITY_VEGA ? 1 : 0;
+        if (target == 1 && d->model != MCG_MODEL_BLACK_SCHOLES)
+            return fail(MCG_ERR_INVALID_ARGUMENT,
+                        "a volatility bump needs a constant-volatility (Black-Scholes) model");
+        const double level = target == 0 ? d->spot : d->volatility;
+        const double amount = q.relative ? q.size * level : q.size;  // BumpSize::amount, api/measure.rs:429-436
+        uint32_t j = 0;
+        while (j < sc.size() && !(sc[j].target == target && sc[j].amount == amount)) ++j;
+        if (j == sc.size()) sc.push_back({target, amount});
+        sc_of[i] = j;
+        gamma |= q.measure == MCG_BUMP_SPOT_GAMMA;
+    }
+    // Sides: scenario j up at 2j, down at 2j + 1; the base plan last (Gamma).
+    const uint32_t ns = static_cast<uint32_t>(sc.size());
+    const uint32_t sides = 2 * ns + (gamma ? 1u : 0u);
+    const uint32_t base_side = 2 * ns;
+    BumpArrays A;
+    std::vector<DevicePlan> dp(sides);
+    std::vector<uint32_t> masks(sides);
+    for (uint32_t k = 0; k < sides; ++k) {
+        mcg_plan_desc s = *d;
+        if (k < base_side) {
+            const BumpScenario& c = sc[k / 2];
+            const double sign = (k % 2 == 0) ? 1.0 : -1.0;
+            if (c.target == 0) {
+                s.spot = d->spot + sign * c.amount;
+                if (!(s.spot > 0.0) || !std::isfinite(s.spot))
+                    return fail(MCG_ERR_INVALID_ARGUMENT, "bumped_spot must stay positive");
+            } else {
+                s.volatility = d->volatility + sign * c.amount;
+                if (!(s.volatility > 0.0) || !std::isfinite(s.volatility))
+                    return fail(MCG_ERR_INVALID_ARGUMENT, "the bumped volatility must stay positive");
+            }
+        }
+        auto* plan = new (std::nothrow) mcg_plan();
+        if (!plan) return fail(MCG_ERR_ALLOCATION, "plan allocation");
+        A.plans.push_back(plan);
+        const mcg_status st = build(&s, *plan, false);
+        if (st != MCG_OK) return fail(st, "side " + std::to_string(k) + ": " + g_last_error);
+        dp[k] = plan->dp;
+        masks[k] = plan->mask;
+    }
+    const mcg_plan& first = *A.plans[0];
+    const DevicePlan& P0 = first.dp;
+    const bool lv = P0.model == MCG_MODEL_LOCAL_VOLATILITY;
+    const bool rqmc = P0.engine == MCG_ENGINE_RQMC;
+    const uint64_t units = P0.units;
+    const uint32_t scrambles = P0.scramble_count;
+    const uint32_t tiles = first.tiles;
+    ScenarioLaunch L{};
+    L.sides = sides;
+    L.scrambles = scrambles;
+    L.tiles = tiles;
+    L.path = lv ? kBookLocalVol : (first.single_terminal ? kBookBsTerminal : kBookBsPath);
+    L.evolutions = P0.antithetic ? 2 : 1;
+    L.units = units;
+    L.max_nodes = lv ? P0.nx : 0u;
+    L.max_slots = lv ? std::max(P0.slot_count, 1u) : 0u;
+    const size_t smem = scenario_smem_bytes(L.max_nodes, L.max_slots);
+    if (smem > 200 * 1024) return fail(MCG_ERR_UNSUPPORTED, "bump plan grid too large for shared memory");
+    if (!rqmc && static_cast<double>(sides) * static_cast<double>(units) * 8.0 > 8.0e9)
+        return fail(MCG_ERR_UNSUPPORTED, "bump plan unit prices exceed 8 GB (sides x sampling units)");
+    MCG_CUDA(A.dplans.upload(dp));
+    MCG_CUDA(A.masks.upload(masks));
+    MCG_CUDA(A.partials.alloc(static_cast<size_t>(sides) * scrambles * tiles * kComponents));
+    MCG_CUDA(A.records.alloc(static_cast<size_t>(sides) * scrambles * kComponents));
+    MCG_CUDA(A.errors.alloc(sides));
+    std::vector<BumpPair> pairs(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t j = sc_of[i];
+        pairs[i] = BumpPair{2 * j, 2 * j + 1, base_side, req[i].measure == MCG_BUMP_SPOT_GAMMA ? 1 : 0,
+                            sc[j].amount};
+    }
+    if (!rqmc) {
+        MCG_CUDA(A.unit_prices.alloc(static_cast<size_t>(sides) * units));
+        MCG_CUDA(A.pairs.upload(pairs));
+        MCG_CUDA(A.pair_partials.alloc(static_cast<size_t>(count) * tiles));
+        MCG_CUDA(A.pair_records.alloc(count));
+    }
+    L.plans = A.dplans.ptr;
+    L.masks = A.masks.ptr;
+    L.partials = A.partials.ptr;
+    L.unit_prices = rqmc ? nullptr : A.unit_prices.ptr;
+    L.errors = A.errors.ptr;
+    cudaEvent_t t0, t1;
+    MCG_CUDA(cudaEventCreate(&t0));
+    MCG_CUDA(cudaEventCreate(&t1));
+    MCG_CUDA(cudaMemsetAsync(A.errors.ptr, 0xff, sides * sizeof(ErrorWord), stream));
+    MCG_CUDA(cudaEventRecord(t0, stream));
+    uint32_t launches = 0;
+    cudaError_t e = launch_scenarios(L, smem, stream);
+    if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("scenario kernel: ") + cudaGetErrorString(e));
+    ++launches;
+    reduce_tiles_kernel<<<dim3(1, sides * scrambles), 256, 0, stream>>>(A.partials.ptr, tiles, kComponents,
+                                                                       A.records.ptr);
+    MCG_CUDA(cudaGetLastError());
+    ++launches;
+    if (!rqmc) {
+        e = launch_bump_pairs(A.unit_prices.ptr, units, A.pairs.ptr, count, A.pair_partials.ptr, stream);
+        if (e != cudaSuccess) return fail(MCG_ERR_CUDA, std::string("pair kernel: ") + cudaGetErrorString(e));
+        reduce_tiles_kernel<<<dim3(1, count), 256, 0, stream>>>(A.pair_partials.ptr, tiles, 1, A.pair_records.ptr);
+        MCG_CUDA(cudaGetLastError());
+        launches += 2;
+    }
+    MCG_CUDA(cudaEventRecord(t1, stream));
+    std::vector<StatRecord> rec(static_cast<size_t>(sides) * scrambles * kComponents), prec(rqmc ? 0 : count);
+    std::vector<ErrorWord> ew(sides);
+    MCG_CUDA(cudaMemcpyAsync(rec.data(), A.records.ptr, rec.size() * sizeof(StatRecord), cudaMemcpyDeviceToHost,
+                             stream));
+    if (!rqmc)
+        MCG_CUDA(cudaMemcpyAsync(prec.data(), A.pair_records.ptr, prec.size() * sizeof(StatRecord),
+                                 cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaMemcpyAsync(ew.data(), A.errors.ptr, sides * sizeof(ErrorWord), cudaMemcpyDeviceToHost, stream));
+    MCG_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    for (uint32_t k = 0; k < sides; ++k)
+        if (ew[k].key != ~0ull) {
+            if (rep) {
+                rep->error.code = static_cast<int32_t>(ew[k].key & 0xff);
+                rep->error.step = k;
+                rep->error.sampling_unit = ew[k].key >> 8;
+            }
+            return fail(static_cast<mcg_status>(ew[k].key & 0xff),
+                        "side " + std::to_string(k) + ": sampling unit " + std::to_string(ew[k].key >> 8) + " failed");
+        }
+    // Each side's price (its own plan's estimate) and, for RQMC, its scramble means.
+    std::vector<mcg_estimate> price(sides);
+    std::vector<std::vector<double>> reps(sides);
+    for (uint32_t k = 0; k < sides; ++k) {
+        HostStat h;
+        if (!rqmc) {
+            const StatRecord& x = rec[static_cast<size_t>(k) * kComponents];
+            h = {x.sum, x.corr, static_cast<uint64_t>(x.count), x.mean, x.m2};
+            price[k] = make_estimate(h, units, 1.0);
+        } else {
+            reps[k].resize(scrambles);
+            for (uint32_t s = 0; s < scrambles; ++s) {
+                const StatRecord& x = rec[(static_cast<size_t>(k) * scrambles + s) * kComponents];
+                reps[k][s] = (x.sum + x.corr) / static_cast<double>(units);
+            }
+            h = two_pass(reps[k]);
+            price[k] = make_estimate(h, scrambles, 1.0);
+        }
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        const BumpPair& pr = pairs[i];
+        HostStat h;
+        if (!rqmc) {
+            const StatRecord& x = prec[i];
+            h = {x.sum, x.corr, static_cast<uint64_t>(x.count), x.mean, x.m2};
+        } else {
+            std::vector<double> diff(scrambles);
+            for (uint32_t s = 0; s < scrambles; ++s) {
+                const double up = reps[pr.up][s], down = reps[pr.down][s];
+                diff[s] = pr.second ? ((up - reps[pr.base][s]) + (down - reps[pr.base][s])) / (pr.h * pr.h)
+                                    : (up - down) / (2.0 * pr.h);
+            }
+            h = two_pass(diff);
+        }
+        double value = 0.0, se = 0.0;
+        const mcg_status st = bump_paired(h, value, se);
+        if (st != MCG_OK) return st;
+        if (!std::isfinite(value) || !std::isfinite(se))
+            return fail(MCG_ERR_INVALID_ARGUMENT, "the bump is too small or too large for a finite difference");
+        est[i] = mcg_bump_estimate{req[i].measure, sc_of[i], pr.h, value, se, h.count, price[pr.up].value,
+                                   price[pr.down].value};
+    }
+    if (rep) {
+        rep->scenarios = ns;
+        rep->sides = sides;
+        rep->evaluations = 2ull * ns + (gamma ? 1u : 0u);
+        if (gamma) rep->base_price = price[base_side];
+        const uint64_t steps = lv ? P0.steps : (first.single_terminal ? 1u : P0.observation_count);
+        rep->path_steps = static_cast<uint64_t>(sides) * units * scrambles * steps * (P0.antithetic ? 2u : 1u);
+        rep->kernel_launches = launches;
+        rep->device_ms = ms;
+    }
+    return MCG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2925,6 +3170,11 @@ mcg_status mcg_rqmc_words(const uint32_t* directions, uint32_t dimensions, uint6
 
 mcg_status mcg_multi_asset_price(const mcg_multi_asset_desc* desc, void* stream, mcg_multi_asset_result* result) {
     return multi_asset_price(desc, static_cast<cudaStream_t>(stream), result);
+}
+
+mcg_status mcg_bump_evaluate(const mcg_plan_desc* base, const mcg_bump_request* requests, uint32_t request_count,
+                             void* stream, mcg_bump_estimate* estimates, mcg_bump_report* report) {
+    return bump_evaluate(base, requests, request_count, static_cast<cudaStream_t>(stream), estimates, report);
 }
 
 }  // extern "C"

@@ -117,7 +117,8 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                                         uint32_t scramble, uint64_t point, bool valid, StatRecord* tile_out,
                                         uint32_t mask, ErrorWord* err, int detail, bool warp_sobol = false,
                                         double* s_z = nullptr, uint16_t* s_zlist = nullptr,
-                                        bool valid_second = false, StatRecord* tile_out_second = nullptr) {
+                                        bool valid_second = false, StatRecord* tile_out_second = nullptr,
+                                        double* unit_price = nullptr) {
     static_assert(Q == 1 || (Q == 2 && E == 1), "two paths per thread take one evolution each");
     constexpr int QE = Q * E;
     const bool valid_q[2] = {valid, valid_second};
@@ -383,6 +384,9 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
 #pragma unroll
                 for (int d = 0; d < 8; ++d) vals[10 + d] = diag_src[q][k][d];
             }
+            // unit_price (optional, one path per thread): the first product's
+            // discounted price of each unit, antithetic pairs averaged.
+            if (Q == 1 && unit_price != nullptr && k == 0 && valid_q[q]) unit_price[unit_q[q]] = vals[MCG_PRICE];
             cta_reduce_write<kComponents>(vals, valid_q[q], mask, outs[q] + static_cast<size_t>(k) * kComponents,
                                           s_red);
         }

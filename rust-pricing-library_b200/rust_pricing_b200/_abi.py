@@ -189,6 +189,30 @@ class MultiAssetResult(C.Structure):
     ]
 
 
+# ---- bump-and-revalue on common random numbers ----
+BUMP_SPOT_DELTA, BUMP_SPOT_GAMMA, BUMP_VOLATILITY_VEGA = 0, 1, 2
+
+
+class BumpRequest(C.Structure):
+    _fields_ = [("measure", C.c_int32), ("relative", C.c_int32), ("size", C.c_double)]
+
+
+class BumpEstimate(C.Structure):
+    _fields_ = [
+        ("measure", C.c_int32), ("scenario", C.c_uint32), ("amount", C.c_double), ("value", C.c_double),
+        ("standard_error", C.c_double), ("units", C.c_uint64), ("up_price", C.c_double),
+        ("down_price", C.c_double),
+    ]
+
+
+class BumpReport(C.Structure):
+    _fields_ = [
+        ("scenarios", C.c_uint32), ("sides", C.c_uint32), ("evaluations", C.c_uint64),
+        ("base_price", Estimate), ("path_steps", C.c_uint64), ("kernel_launches", C.c_uint32),
+        ("device_ms", C.c_float), ("error", ErrorRecord),
+    ]
+
+
 class ResultBuffers:
     """Caller-owned result storage for `products` products and `nodes` node entries."""
 

@@ -20,7 +20,7 @@ EXPORTS = (
     "mcg_ssvi_local_variance_grid", "mcg_measure_fp64_peak", "mcg_price_european_noalloc",
     "mcg_lsm_price", "mcg_mlp_forward", "mcg_mlp_gradient", "mcg_book_create", "mcg_book_evaluate",
     "mcg_book_destroy", "mcg_surface_local_variance_grid", "mcg_surface_total_variance", "mcg_vega_kt_project",
-    "mcg_lsm_dual", "mcg_multi_asset_price",
+    "mcg_lsm_dual", "mcg_multi_asset_price", "mcg_bump_evaluate",
 )
 
 _lib = None
@@ -96,6 +96,9 @@ def library() -> C.CDLL:
     lib.mcg_book_destroy.argtypes = [vp]
     lib.mcg_multi_asset_price.argtypes = [C.POINTER(A.MultiAssetDesc), vp, C.POINTER(A.MultiAssetResult)]
     lib.mcg_multi_asset_price.restype = C.c_int
+    lib.mcg_bump_evaluate.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.BumpRequest), u32, vp,
+                                      C.POINTER(A.BumpEstimate), C.POINTER(A.BumpReport)]
+    lib.mcg_bump_evaluate.restype = C.c_int
     if lib.mcg_abi_version() != A.ABI_VERSION:
         raise EngineError(1, "engine library ABI version mismatch")
     _lib = lib
@@ -311,3 +314,16 @@ class Book:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def bump_evaluate(spec, requests, stream: int = 0):
+    """mcg_bump_evaluate: bump-and-revalue of a price-only plan on common random
+    numbers, every scenario side in one launch.  `requests` are
+    (measure, size, relative) triples; returns (estimates, report)."""
+    n = len(requests)
+    req = (A.BumpRequest * n)(*[A.BumpRequest(m, int(rel), size) for m, size, rel in requests])
+    est = (A.BumpEstimate * n)()
+    rep = A.BumpReport()
+    desc = spec.desc()
+    check(library().mcg_bump_evaluate(C.byref(desc), req, n, C.c_void_p(stream), est, C.byref(rep)), rep.error)
+    return list(est), rep

@@ -93,6 +93,9 @@ def oracle():
     lib.oracle_lsm_fit.restype = C.c_int
     lib.oracle_multi_asset_price.argtypes = [C.POINTER(A.MultiAssetDesc), C.POINTER(A.MultiAssetResult), C.c_int]
     lib.oracle_multi_asset_price.restype = C.c_int
+    lib.oracle_bump_evaluate.argtypes = [C.POINTER(A.PlanDesc), C.POINTER(A.BumpRequest), C.c_uint32,
+                                         C.POINTER(A.BumpEstimate), C.POINTER(A.BumpReport), C.c_int]
+    lib.oracle_bump_evaluate.restype = C.c_int
     _oracle = lib
     return lib
 
@@ -155,3 +158,21 @@ def oracle_multi(spec, threads: int | None = None):
     if rc != 0:
         raise RuntimeError(f"oracle multi-asset status {A.STATUS_NAMES.get(rc, rc)}")
     return out
+
+
+def bump_requests(requests):
+    """[(measure, size, relative)] -> a ctypes array of mcg_bump_request."""
+    return (A.BumpRequest * len(requests))(*[A.BumpRequest(m, int(rel), size) for m, size, rel in requests])
+
+
+def oracle_bump(spec, requests, threads: int | None = None):
+    """The oracle's bump-and-revalue: (estimates, report)."""
+    req = bump_requests(requests)
+    est = (A.BumpEstimate * len(requests))()
+    rep = A.BumpReport()
+    desc = spec.desc()
+    rc = oracle().oracle_bump_evaluate(C.byref(desc), req, len(requests), est, C.byref(rep),
+                                       threads or os.cpu_count() or 1)
+    if rc != 0:
+        raise RuntimeError(f"oracle bump status {A.STATUS_NAMES.get(rc, rc)}")
+    return list(est), rep

@@ -49,7 +49,10 @@ STRUCTS = {
     "mcg_lsm_desc": A.LsmDesc, "mcg_lsm_date_model": A.LsmDateModel, "mcg_lsm_result": A.LsmResult,
     "mcg_book_options": A.BookOptions, "mcg_book_report": A.BookReport, "mcg_surface_desc": A.SurfaceDesc,
     "mcg_vega_kt_basis": A.VegaKtBasis, "mcg_vega_kt_projection": A.VegaKtProjection,
-    "mcg_dual_desc": A.DualDesc, "mcg_dual_result": A.DualResult,
+    "mcg_dual_desc": A.DualDesc, "mcg_dual_result": A.DualResult, "mcg_dividends": A.Dividends,
+    "mcg_asset_desc": A.AssetDesc, "mcg_multi_asset_desc": A.MultiAssetDesc,
+    "mcg_multi_asset_result": A.MultiAssetResult, "mcg_bump_request": A.BumpRequest,
+    "mcg_bump_estimate": A.BumpEstimate, "mcg_bump_report": A.BumpReport,
 }
 
 
