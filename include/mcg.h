@@ -668,25 +668,27 @@ mcg_status mcg_mlp_forward(const float* params, const float* x, uint32_t count, 
 mcg_status mcg_mlp_gradient(const float* params, const float* x, const float* y, const uint8_t* mask,
                             uint32_t count, float* grad, float* loss);
 
-/* ---- A book of trades in one launch (no counterpart in the reference) ----
+/* ---- A book of trades in one launch per path family (no counterpart in the reference) ----
  *
  * Thousands of single-product plans -- each with its own model (Black-Scholes
  * or local volatility with its own grid), maturity and step count, strike and
- * product -- priced by one persistent kernel that pulls (trade, tile-range)
- * work items from a queue ordered heaviest first, followed by the per-trade
- * tile reduction.  Each trade's price statistics are bit for bit those of
- * mcg_plan_evaluate on its own plan.  Trades must be pseudo-MC with the same
- * sampling_units, one product, no risk request, and (local volatility) no
- * antithetic pairing.  The launch shape (tiles per work item, resident CTAs
- * per SM) is chosen at creation by timing candidate shapes on a stratified
- * sample of the book (`autotune`), and the evaluation can be captured once in
- * a CUDA graph (`use_graph`) and replayed. */
+ * product -- priced by one persistent kernel per path family (local
+ * volatility with discrete products, two paths per thread; local volatility
+ * with a continuous barrier; Black-Scholes single-terminal; Black-Scholes
+ * multi-observation), each pulling (trade, tile-range) work items from its
+ * own queue ordered heaviest first, followed by the per-trade tile reduction.
+ * Each trade's price statistics are bit for bit those of mcg_plan_evaluate on
+ * its own plan.  Trades must be pseudo-MC with the same sampling_units, one
+ * product, no risk request, FP64, and (local volatility) no antithetic
+ * pairing.  The tiles per work item are chosen at creation by timing
+ * candidates on a stratified sample of the book (`autotune`), and the
+ * evaluation can be captured once in a CUDA graph (`use_graph`) and replayed. */
 typedef struct mcg_book mcg_book;
 
 typedef struct mcg_book_options {
     int32_t autotune;        /* 1: time candidate launch shapes at creation and keep the fastest */
     uint32_t tiles_per_item; /* 128-unit tiles per work item when not autotuned; 0 = 4 */
-    uint32_t ctas_per_sm;    /* resident CTAs per SM when not autotuned; 0 = as many as fit */
+    uint32_t ctas_per_sm;    /* cap on every family's resident CTAs per SM; 0 = as many as fit */
     int32_t use_graph;       /* 1: capture the evaluation in a CUDA graph at creation */
 } mcg_book_options;
 
@@ -694,7 +696,7 @@ typedef struct mcg_book_report {
     uint32_t trade_count;
     uint32_t items;            /* work items of one evaluation */
     uint32_t tiles_per_item;   /* the launch shape in use */
-    uint32_t ctas_per_sm;
+    uint32_t ctas_per_sm;      /* of the heaviest family's kernel */
     uint32_t ctas;
     uint32_t kernel_launches;  /* per evaluation */
     int32_t graph;             /* 1: evaluated by replaying the captured graph */

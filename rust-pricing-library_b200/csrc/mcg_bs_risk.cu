@@ -465,12 +465,246 @@ __global__ void __launch_bounds__(kThreads, kCont ? 4 : 6) bs_path_risk_kernel(c
     cta_reduce_write<kComponents>(vals, valid, mask, tile_out, s_red);
 }
 
+// Single-sweep form of pathwise_values for the products whose adjoint seeds
+// need no reverse pass over the path: European, Digital and an exact discrete
+// barrier seed only the terminal observation, a lookback only the observation
+// holding its extremum, an Asian every observation with weight_k times a
+// factor g that is either 0 or +-notional (in or out of the money at the end).
+// The seven (spot, volatility) evaluations of both antithetic signs therefore
+// run in one forward loop over the observations with no scratch tape: per
+// observation one normal, W_k, the exponential at the plan's volatility per
+// sign (shared by the five spot points, whose observations are
+// F_k (S/S0) e_k as above) and the two volatility-bump exponentials; the
+// Asian adjoint sums carry the seed with g = +-notional and are dropped when
+// g is 0; the lookback keeps the extremum's observation.  Each term is the
+// reference's ((adj spot_scale) f_k) / S and ((adj b) f_k)(-sigma t_k + W_k);
+// only the Asian sums add them in observation order instead of the reverse.
+// Plans without dividends; a smoothed discrete barrier (whose hit weights do
+// need the reverse pass) and a continuous barrier use the tape kernel.
+template <bool kAnti>
+__global__ void __launch_bounds__(kThreads, kAnti ? 2 : 4) bs_path_sweep_kernel(const DevicePlan P, uint64_t unit_begin,
+                                                                  uint64_t unit_end, StatRecord* partials,
+                                                                  uint32_t mask, ErrorWord* err, int detail) {
+    (void)err;
+    (void)detail;
+    __shared__ Stat s_red[4 * kComponents];
+    constexpr int S = kAnti ? 2 : 1;  // path signs: primary and antithetic mate
+    constexpr int N = 7 * S;          // evaluation i of sign s at 7 s + i
+    const uint32_t scramble = blockIdx.y;
+    const uint64_t point = unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    const bool valid = point < unit_end && point < P.units;
+    const uint64_t unit = valid ? point : 0;
+    NormalSource ns;
+    ns.rqmc = P.engine == MCG_ENGINE_RQMC;
+    ns.seed = P.seed;
+    ns.unit = unit;
+    ns.gray = static_cast<uint32_t>(unit ^ (unit >> 1));
+    ns.dirs = P.scr_dirs ? P.scr_dirs + static_cast<size_t>(scramble) * P.dimension * 32u : nullptr;
+    ns.shift = P.scr_shift ? P.scr_shift + static_cast<size_t>(scramble) * P.dimension : nullptr;
+    ns.cached_block = 0xffffffffu;
+    const ProductParams& pp = P.products[0];
+    const uint32_t n = P.observation_count;
+    const double h = P.smoothing;
+    const bool call = pp.side == MCG_CALL;
+    const bool asian = pp.kind == MCG_PRODUCT_ASIAN;
+    const bool lookback = pp.kind == MCG_PRODUCT_LOOKBACK;
+    const double b = P.gamma_bump, sb = P.spot_bump, vb = P.vol_bump;
+    const bool vbump = vb != 0.0;
+    // base, gamma down/up, validation spot down/up, validation volatility down/up
+    const double spots[7] = {P.spot, P.spot - b, P.spot + b, P.spot - sb, P.spot + sb, P.spot, P.spot};
+    const double vols[7] = {P.vol, P.vol, P.vol, P.vol, P.vol, P.vol - vb, P.vol + vb};
+    double scale[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) scale[i] = spots[i] / P.spot;
+    const double gstar = pp.notional * (call ? 1.0 : -1.0);
+    ProductAcc acc[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) acc_init(acc[j], pp);
+    // adjoint sums of the base and gamma points (Asian), the extremum's
+    // observation (lookback: its spot per point, W and time for the base Vega)
+    double ad[3 * S], av[S], fa[3 * S], wa[S], ta[S];
+    bool has_arg[3 * S];
+#pragma unroll
+    for (int j = 0; j < 3 * S; ++j) {
+        ad[j] = 0.0;
+        fa[j] = 0.0;
+        has_arg[j] = false;
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s) av[s] = wa[s] = ta[s] = 0.0;
+    double w = 0.0, wlast[S], sk[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) sk[j] = 0.0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const double z = P.zero_variance ? 0.0 : ns.normal(k);
+        w += P.obs_sqrt_step[k] * z;
+        const double t = P.obs_time[k];
+        const double F = P.obs_fwd[k];
+        const double tv = P.vol * P.vol * t;
+        const bool mon = lookback && monitored(pp, k);
+        const double wg = asian ? pp.weights[k] : 0.0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const double ws = (s == 0 ? 1.0 : -1.0) * w;
+            wlast[s] = ws;
+            const double e = exp(-0.5 * tv + P.vol * ws);
+#pragma unroll
+            for (int i = 0; i < 5; ++i) sk[7 * s + i] = F * scale[i] * e;
+            if (vbump) {
+#pragma unroll
+                for (int i = 5; i < 7; ++i) {
+                    const double tvb = vols[i] * vols[i] * t;
+                    sk[7 * s + i] = F * 1.0 * exp(-0.5 * tvb + vols[i] * ws);
+                }
+            }
+            if (asian) {
+                const double a = (gstar * wg) * 1.0;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) ad[3 * s + i] += a * sk[7 * s + i] / spots[i];
+                av[s] += a * 1.0 * sk[7 * s] * (-P.vol * t + ws);
+            }
+            if (mon) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const ProductAcc& q = acc[7 * s + i];
+                    const double x = sk[7 * s + i];
+                    if (q.counts == 0u || (call ? !(q.a >= x) : !(q.a <= x))) {
+                        fa[3 * s + i] = x;
+                        has_arg[3 * s + i] = true;
+                        if (i == 0) {
+                            wa[s] = ws;
+                            ta[s] = t;
+                        }
+                    }
+                }
+            }
+        }
+        acc_observe_n<N, false>(pp, acc, k, sk, h, sk, false);
+    }
+    const double t_last = n ? P.obs_time[n - 1] : 0.0;
+    double vals[kComponents];
+#pragma unroll
+    for (int c = 0; c < kComponents; ++c) vals[c] = 0.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        PathAad r[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            r[i] = PathAad{0.0, 0.0, 0.0};
+            if ((i == 1 || i == 2) && !P.req_gamma) continue;
+            if (i >= 5 && !vbump) continue;
+            const ProductAcc& q = acc[7 * s + i];
+            const double value = acc_payoff(pp, q, h);
+            double delta = 0.0, vega = 0.0;
+            if (i < 3) {
+                // the seed of this point (discrete_aad's switch) and its pull-back
+                double terminal_adj = 0.0, g = 0.0;
+                const double term = q.terminal;
+                switch (pp.kind) {
+                case MCG_PRODUCT_EUROPEAN: {
+                    const double in = call ? term - pp.strike : pp.strike - term;
+                    terminal_adj = (in >= 0.0 ? pp.notional : 0.0) * (call ? 1.0 : -1.0);
+                    break;
+                }
+                case MCG_PRODUCT_DIGITAL: {
+                    const double dist = call ? term - pp.strike : pp.strike - term;
+                    double ind, first = 0.0;
+                    if (h > 0.0) {
+                        double comp;
+                        const SmoothD dd = smooth_indicator(h, dist, comp);
+                        ind = dd.value;
+                        first = dd.first;
+                    } else {
+                        ind = dist >= 0.0 ? 1.0 : 0.0;
+                    }
+                    const bool asset = pp.digital_payout == MCG_DIGITAL_ASSET;
+                    const double base = asset ? term * pp.payout : pp.payout;
+                    double a = 0.0;
+                    if (asset) a += ind * pp.payout;
+                    if (h > 0.0) a += (call ? 1.0 : -1.0) * (base * first);
+                    terminal_adj = a;
+                    break;
+                }
+                case MCG_PRODUCT_ASIAN:
+                case MCG_PRODUCT_LOOKBACK: {
+                    const double in = call ? q.a - pp.strike : pp.strike - q.a;
+                    g = (in >= 0.0 ? pp.notional : 0.0) * (call ? 1.0 : -1.0);
+                    break;
+                }
+                case MCG_PRODUCT_DISCRETE_BARRIER: {
+                    const double in = call ? term - pp.strike : pp.strike - term;
+                    const double active = pp.barrier_style == MCG_KNOCK_OUT ? 1.0 - q.a : q.a;
+                    terminal_adj = (in >= 0.0 ? active * pp.notional : 0.0) * (call ? 1.0 : -1.0);
+                    break;
+                }
+                default:
+                    break;
+                }
+                if (asian) {
+                    if (g != 0.0) {
+                        delta = ad[3 * s + i];
+                        if (i == 0) vega = av[s];
+                    }
+                } else if (lookback) {
+                    if (g != 0.0 && has_arg[3 * s + i]) {
+                        delta = g * 1.0 * fa[3 * s + i] / spots[i];
+                        if (i == 0) vega = g * 1.0 * fa[3 * s] * (-P.vol * ta[s] + wa[s]);
+                    }
+                } else if (terminal_adj != 0.0 && n > 0) {
+                    delta = terminal_adj * 1.0 * term / spots[i];
+                    if (i == 0) vega = terminal_adj * 1.0 * term * (-P.vol * t_last + wlast[s]);
+                }
+            }
+            r[i] = PathAad{P.discount * value, P.discount * delta, P.discount * vega};
+        }
+        const double gamma = P.req_gamma ? (r[2].delta - r[1].delta) / (2.0 * b) : 0.0;
+        const double bump_delta = (r[4].price - r[3].price) / (2.0 * sb);
+        const double bump_gamma = (r[4].price - 2.0 * r[0].price + r[3].price) / (sb * sb);
+        const double bump_vega = vb != 0.0 ? (r[6].price - r[5].price) / (2.0 * vb) : 0.0;
+        double v[kComponents];
+#pragma unroll
+        for (int c = 0; c < kComponents; ++c) v[c] = 0.0;
+        v[MCG_PRICE] = r[0].price;
+        v[MCG_DELTA] = r[0].delta;
+        v[MCG_VEGA] = r[0].vega;
+        v[MCG_GAMMA] = gamma;
+        v[MCG_BUMP_DELTA] = bump_delta;
+        v[MCG_DELTA_DIFFERENCE] = bump_delta - r[0].delta;
+        v[MCG_BUMP_VEGA] = bump_vega;
+        v[MCG_VEGA_DIFFERENCE] = bump_vega - r[0].vega;
+        v[MCG_BUMP_GAMMA] = bump_gamma;
+        v[MCG_GAMMA_DIFFERENCE] = bump_gamma - gamma;
+        if (s == 0) {
+#pragma unroll
+            for (int c = 0; c < kComponents; ++c) vals[c] = v[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < kComponents; ++c) vals[c] = (vals[c] + v[c]) * 0.5;
+        }
+    }
+    const uint64_t tiles = (P.units + kThreads - 1) / kThreads;
+    const uint64_t tile = (unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads) / kThreads;
+    StatRecord* tile_out = partials + (static_cast<size_t>(scramble) * tiles + tile) * kComponents;
+    cta_reduce_write<kComponents>(vals, valid, mask, tile_out, s_red);
+}
+
 // Units are launched in chunks of at most P.bs_tape_units threads (all
 // scrambles of a chunk in one launch), so the scratch tape stays bounded.
 cudaError_t launch_bs_path_risk(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
                                 StatRecord* partials, uint32_t mask, ErrorWord* err, int detail,
                                 cudaStream_t stream) {
-    if (P.product_count != 1 || !P.bs_tape) return cudaErrorNotSupported;
+    if (P.product_count != 1) return cudaErrorNotSupported;
+    if (P.bs_sweep) {
+        const dim3 grid(static_cast<unsigned>((units + kThreads - 1) / kThreads), scrambles);
+        if (P.antithetic)
+            bs_path_sweep_kernel<true><<<grid, kThreads, 0, stream>>>(P, unit_begin, unit_begin + units, partials,
+                                                                      mask, err, detail);
+        else
+            bs_path_sweep_kernel<false><<<grid, kThreads, 0, stream>>>(P, unit_begin, unit_begin + units, partials,
+                                                                       mask, err, detail);
+        return cudaGetLastError();
+    }
+    if (!P.bs_tape) return cudaErrorNotSupported;
     const bool cont = P.products[0].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
     const uint64_t per_launch = P.bs_tape_units / scrambles / kThreads * kThreads;
     if (per_launch == 0) return cudaErrorInvalidValue;

@@ -88,6 +88,34 @@ __device__ __forceinline__ double as241_central(double centered) {
     return centered * num / den;
 }
 
+// The central branch with each Horner step a fused multiply-add (and a = 0.180625
+// - c^2 as one), for the path kernels' batched normals: within a few ulps of
+// as241_central, whose two-rounding form the exported normals keep bit for bit.
+// The path results are held to 1e-12 of the reference, not to the bit.
+__device__ __forceinline__ double poly8_fma(double x, double c0, double c1, double c2, double c3, double c4,
+                                           double c5, double c6, double c7) {
+    double v = c7;
+    v = fma(v, x, c6);
+    v = fma(v, x, c5);
+    v = fma(v, x, c4);
+    v = fma(v, x, c3);
+    v = fma(v, x, c2);
+    v = fma(v, x, c1);
+    v = fma(v, x, c0);
+    return v;
+}
+
+__device__ __forceinline__ double as241_central_fma(double centered) {
+    const double a = fma(-centered, centered, 0.180625);
+    const double num = poly8_fma(a, 0x1.b18d91e9eef75p+1, 0x1.0a4888b1a436ep+7, 0x1.ece5d2213c0ccp+10,
+                                 0x1.ad1d8cd4ee71dp+13, 0x1.66c3e869b752ap+15, 0x1.06c1c55b78f20p+16,
+                                 0x1.052d26b2e4604p+15, 0x1.39a296f7d925ep+11);
+    const double den = poly8_fma(a, 1.0, 0x1.5281b386e1ab5p+5, 0x1.5797efdc8b3f7p+9,
+                                 0x1.512322e75c89fp+12, 0x1.4b772d5d65266p+14, 0x1.3317caa64f4bep+15,
+                                 0x1.c0e457cb1ae76p+14, 0x1.46a7eca984b6ap+12);
+    return centered * num / den;
+}
+
 __device__ __forceinline__ double as241_tail(double p, double centered) {
     const double tail = centered < 0.0 ? p : 1.0 - p;
     const double r = sqrt(-log(tail));

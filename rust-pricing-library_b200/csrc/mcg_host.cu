@@ -975,7 +975,11 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
     MCG_CUDA(plan.partials.alloc(static_cast<size_t>(P.scramble_count) * plan.tiles * plan.product_count * kComponents));
     MCG_CUDA(plan.records.alloc(static_cast<size_t>(P.scramble_count) * plan.product_count * kComponents));
     MCG_CUDA(plan.error.alloc(1));
-    if (!lv && P.risk && !plan.single_terminal) {
+    const bool sweep = !lv && P.risk && !plan.single_terminal && plan.product_count == 1 && !P.dividends &&
+                       plan.products[0].kind != MCG_PRODUCT_CONTINUOUS_BARRIER &&
+                       !(plan.products[0].kind == MCG_PRODUCT_DISCRETE_BARRIER && P.smoothing > 0.0);
+    P.bs_sweep = sweep ? 1 : 0;
+    if (!lv && P.risk && !plan.single_terminal && !sweep) {
         // Scratch of the path-risk kernel (at most 2 GiB): W_k and the path's
         // exponentials per thread, plus the hit state, weight and slope per
         // observation for a smoothed discrete barrier, or the observed states
@@ -2095,19 +2099,22 @@ mcg_status lsm_dual(const mcg_plan_desc* d, const mcg_lsm_desc* l, const mcg_dua
 
 struct mcg_book {
     std::vector<mcg_plan*> plans;
-    std::vector<BookItem> host_items;
-    std::vector<uint64_t> item_cost;
-    std::vector<uint32_t> trade_path, trade_steps;
+    std::vector<uint32_t> trade_family, trade_path, trade_steps;
+    std::vector<BookItem> host_items[kBookFamilies];
     DeviceArray<DevicePlan> dplans;
     DeviceArray<uint32_t> masks;
-    DeviceArray<BookItem> items;
-    DeviceArray<unsigned int> cursor;
+    DeviceArray<BookItem> items[kBookFamilies];
+    DeviceArray<unsigned int> cursor;  // one per family
     DeviceArray<StatRecord> partials, records;
     DeviceArray<ErrorWord> errors;
-    uint32_t trades = 0, tiles = 0, max_values = 0, max_nodes = 0, max_slots = 1;
-    uint32_t tiles_per_item = 4, ctas_per_sm = 1, ctas = 1;
+    uint32_t trades = 0, tiles = 0;
+    uint32_t max_nodes[kBookFamilies] = {0, 0, 0, 0}, max_slots[kBookFamilies] = {1, 1, 1, 1};
+    size_t smem[kBookFamilies] = {0, 0, 0, 0};
+    int fit[kBookFamilies] = {1, 1, 1, 1};
+    uint32_t ctas[kBookFamilies] = {0, 0, 0, 0};
+    uint64_t family_cost[kBookFamilies] = {0, 0, 0, 0};
+    uint32_t tiles_per_item = 4, ctas_per_sm = 0;  // 0: every family at its own occupancy
     uint64_t units = 0, path_steps = 0;
-    size_t smem = 0;
     int sms = 148;
     float autotune_ms = 0.f;
     cudaStream_t capture_stream = nullptr;
@@ -2120,7 +2127,7 @@ struct mcg_book {
         for (mcg_plan* p : plans) delete p;
         dplans.release();
         masks.release();
-        items.release();
+        for (auto& it : items) it.release();
         cursor.release();
         partials.release();
         records.release();
@@ -2130,48 +2137,64 @@ struct mcg_book {
 
 namespace {
 
-// Work items of `tiles_per_item` tiles, ordered heaviest first (cost = tiles x
-// steps, local volatility weighted 3x for its interpolation and logarithm);
-// ties keep trade order, so the queue is deterministic.
+// Work items of `tiles_per_item` tiles (even in the two-path family, from even
+// first tiles), per family ordered heaviest first (cost = tiles x steps, local
+// volatility weighted 3x for its interpolation); ties keep trade order, so the
+// queues are deterministic.
 void book_items(mcg_book& b, uint32_t tiles_per_item, const std::vector<uint32_t>& trades) {
-    b.host_items.clear();
-    std::vector<std::pair<uint64_t, size_t>> order;
-    for (uint32_t t : trades)
-        for (uint32_t first = 0; first < b.tiles; first += tiles_per_item) {
-            const uint32_t n = std::min(tiles_per_item, b.tiles - first);
-            BookItem it{t, first, n, b.trade_path[t]};
-            const uint64_t cost = static_cast<uint64_t>(n) * b.trade_steps[t] * (it.path == kBookLocalVol ? 3 : 1);
-            order.emplace_back(cost, b.host_items.size());
-            b.host_items.push_back(it);
+    for (uint32_t f = 0; f < kBookFamilies; ++f) {
+        std::vector<std::pair<uint64_t, BookItem>> order;
+        for (uint32_t t : trades) {
+            if (b.trade_family[t] != f) continue;
+            const uint32_t step = f == kFamilyLvDiscrete ? (tiles_per_item + 1) & ~1u : tiles_per_item;
+            for (uint32_t first = 0; first < b.tiles; first += step) {
+                const uint32_t n = std::min(step, b.tiles - first);
+                const BookItem it{t, first, n, b.trade_path[t]};
+                order.emplace_back(static_cast<uint64_t>(n) * b.trade_steps[t] * (it.path == kBookLocalVol ? 3 : 1), it);
+            }
         }
-    std::stable_sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-    std::vector<BookItem> sorted;
-    sorted.reserve(order.size());
-    for (auto& o : order) sorted.push_back(b.host_items[o.second]);
-    b.host_items.swap(sorted);
+        std::stable_sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        b.host_items[f].clear();
+        b.family_cost[f] = 0;
+        for (auto& o : order) {
+            b.host_items[f].push_back(o.second);
+            b.family_cost[f] += o.first;
+        }
+    }
 }
 
-BookLaunch book_launch(mcg_book& b) {
+BookLaunch book_launch(mcg_book& b, uint32_t f) {
     BookLaunch L{};
     L.plans = b.dplans.ptr;
     L.masks = b.masks.ptr;
-    L.items = b.items.ptr;
-    L.item_count = static_cast<uint32_t>(b.host_items.size());
-    L.next = b.cursor.ptr;
+    L.items = b.items[f].ptr;
+    L.item_count = static_cast<uint32_t>(b.host_items[f].size());
+    L.next = b.cursor.ptr + f;
     L.partials = b.partials.ptr;
     L.tiles_per_trade = b.tiles;
     L.errors = b.errors.ptr;
-    L.max_values = b.max_values;
-    L.max_nodes = b.max_nodes;
-    L.max_slots = b.max_slots;
+    L.max_nodes = b.max_nodes[f];
+    L.max_slots = b.max_slots[f];
     return L;
 }
 
-// The evaluation's launches: queue reset, error words, persistent kernel, reduction.
+// The families in launch order: heaviest first.
+std::vector<uint32_t> book_order(const mcg_book& b) {
+    std::vector<uint32_t> order;
+    for (uint32_t f = 0; f < kBookFamilies; ++f)
+        if (!b.host_items[f].empty()) order.push_back(f);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t x, uint32_t y) { return b.family_cost[x] > b.family_cost[y]; });
+    return order;
+}
+
+// The evaluation's launches: queue reset, error words, one persistent kernel
+// per family, the per-trade reduction.
 cudaError_t book_enqueue(mcg_book& b, cudaStream_t stream) {
-    cudaError_t e = cudaMemsetAsync(b.cursor.ptr, 0, sizeof(unsigned int), stream);
+    cudaError_t e = cudaMemsetAsync(b.cursor.ptr, 0, kBookFamilies * sizeof(unsigned int), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.errors.ptr, 0xff, b.trades * sizeof(ErrorWord), stream);
-    if (e == cudaSuccess) e = launch_book(book_launch(b), b.ctas, b.smem, stream);
+    for (uint32_t f : book_order(b))
+        if (e == cudaSuccess) e = launch_book(f, book_launch(b, f), b.ctas[f], b.smem[f], stream);
     if (e == cudaSuccess) {
         reduce_tiles_kernel<<<dim3(kComponents, b.trades), 256, 0, stream>>>(b.partials.ptr, b.tiles, kComponents,
                                                                           b.records.ptr);
@@ -2184,10 +2207,13 @@ mcg_status book_set_shape(mcg_book& b, uint32_t tiles_per_item, uint32_t ctas_pe
                           const std::vector<uint32_t>& trades) {
     b.tiles_per_item = tiles_per_item;
     b.ctas_per_sm = ctas_per_sm;
-    b.ctas = static_cast<uint32_t>(b.sms) * ctas_per_sm;
     book_items(b, tiles_per_item, trades);
-    b.items.release();
-    MCG_CUDA(b.items.upload(b.host_items));
+    for (uint32_t f = 0; f < kBookFamilies; ++f) {
+        const int per_sm = ctas_per_sm ? std::min<int>(static_cast<int>(ctas_per_sm), b.fit[f]) : b.fit[f];
+        b.ctas[f] = static_cast<uint32_t>(b.sms) * static_cast<uint32_t>(std::max(per_sm, 1));
+        b.items[f].release();
+        MCG_CUDA(b.items[f].upload(b.host_items[f]));
+    }
     return MCG_OK;
 }
 
@@ -2217,6 +2243,7 @@ mcg_status book_create(const mcg_plan_desc* trades, uint32_t n, const mcg_book_o
             return fail(MCG_ERR_INVALID_ARGUMENT, who + "every trade of a book has the same sampling_units");
         if (d.model == MCG_MODEL_LOCAL_VOLATILITY && d.antithetic)
             return fail(MCG_ERR_UNSUPPORTED, who + "local-volatility book trades are not antithetic");
+        if (d.precision != MCG_PRECISION_F64) return fail(MCG_ERR_UNSUPPORTED, who + "a book prices in FP64");
         auto* plan = new (std::nothrow) mcg_plan();
         if (!plan) return fail(MCG_ERR_ALLOCATION, "plan allocation");
         b->plans.push_back(plan);
@@ -2225,26 +2252,30 @@ mcg_status book_create(const mcg_plan_desc* trades, uint32_t n, const mcg_book_o
         dp[i] = plan->dp;
         masks[i] = plan->mask;
         const bool lv = d.model == MCG_MODEL_LOCAL_VOLATILITY;
+        const bool cont = d.products[0].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+        const uint32_t family = lv ? (cont ? kFamilyLvBarrier : kFamilyLvDiscrete)
+                                   : (plan->single_terminal ? kFamilyBsTerminal : kFamilyBsPath);
+        b->trade_family.push_back(family);
         b->trade_path.push_back(lv ? kBookLocalVol : (plan->single_terminal ? kBookBsTerminal : kBookBsPath));
         const uint32_t steps = lv ? plan->dp.steps : (plan->single_terminal ? 1u : plan->dp.observation_count);
         b->trade_steps.push_back(steps);
         b->path_steps += b->units * steps * (d.antithetic ? 2u : 1u);
         if (lv) {
-            b->max_values = std::max(b->max_values, plan->dp.nt * plan->dp.nx);
-            b->max_nodes = std::max(b->max_nodes, plan->dp.nx);
-            b->max_slots = std::max(b->max_slots, plan->dp.slot_count);
+            b->max_nodes[family] = std::max(b->max_nodes[family], plan->dp.nx);
+            b->max_slots[family] = std::max(b->max_slots[family], plan->dp.slot_count);
         }
     }
     b->tiles = b->plans[0]->tiles;
-    b->smem = book_smem_bytes(b->max_values, b->max_nodes, b->max_slots);
-    if (b->smem > 200 * 1024) return fail(MCG_ERR_UNSUPPORTED, "book grids too large for shared memory");
-    MCG_CUDA(book_prepare(b->smem));
-    int fit = 1;
-    MCG_CUDA(book_occupancy(b->smem, &fit));
-    fit = std::max(fit, 1);
+    for (uint32_t f = 0; f < kBookFamilies; ++f) {
+        b->smem[f] = book_smem_bytes(f, b->max_nodes[f], b->max_slots[f]);
+        if (b->smem[f] > 200 * 1024) return fail(MCG_ERR_UNSUPPORTED, "book grids too large for shared memory");
+        MCG_CUDA(book_prepare(f, b->smem[f]));
+        MCG_CUDA(book_occupancy(f, b->smem[f], &b->fit[f]));
+        b->fit[f] = std::max(b->fit[f], 1);
+    }
     MCG_CUDA(b->dplans.upload(dp));
     MCG_CUDA(b->masks.upload(masks));
-    MCG_CUDA(b->cursor.alloc(1));
+    MCG_CUDA(b->cursor.alloc(kBookFamilies));
     MCG_CUDA(b->partials.alloc(static_cast<size_t>(n) * b->tiles * kComponents));
     MCG_CUDA(b->records.alloc(static_cast<size_t>(n) * kComponents));
     MCG_CUDA(b->errors.alloc(n));
@@ -2253,11 +2284,11 @@ mcg_status book_create(const mcg_plan_desc* trades, uint32_t n, const mcg_book_o
     mcg_book_options o{};
     if (opt) o = *opt;
     uint32_t tpi = o.tiles_per_item ? o.tiles_per_item : 4u;
-    uint32_t cps = o.ctas_per_sm ? std::min<uint32_t>(o.ctas_per_sm, static_cast<uint32_t>(fit))
-                                 : static_cast<uint32_t>(fit);
+    const uint32_t cps = o.ctas_per_sm;
     if (o.autotune) {
-        // Candidate shapes timed on a stratified sample (every k-th trade of
-        // the book, at most 128 trades), the fastest kept.
+        // Tiles per work item timed on a stratified sample (every k-th trade of
+        // the book, at most 128 trades), the fastest kept; every family runs at
+        // its own occupancy (or the caller's cap).
         const auto t0 = std::chrono::steady_clock::now();
         std::vector<uint32_t> sample;
         const uint32_t stride = std::max(1u, n / 128u);
@@ -2268,40 +2299,30 @@ mcg_status book_create(const mcg_plan_desc* trades, uint32_t n, const mcg_book_o
         MCG_CUDA(cudaEventCreate(&e0));
         MCG_CUDA(cudaEventCreate(&e1));
         float best = 1e30f;
-        uint32_t best_tpi = tpi, best_cps = cps;
-        std::vector<uint32_t> cps_candidates;
-        for (uint32_t c : {2u, 4u})
-            if (c <= static_cast<uint32_t>(fit)) cps_candidates.push_back(c);
-        if (std::find(cps_candidates.begin(), cps_candidates.end(), static_cast<uint32_t>(fit)) == cps_candidates.end())
-            cps_candidates.push_back(static_cast<uint32_t>(fit));
+        uint32_t best_tpi = tpi;
         mcg_status st = MCG_OK;
-        for (uint32_t cand_tpi : {1u, 4u, 16u}) {
-            for (uint32_t cand_cps : cps_candidates) {
-                if ((st = book_set_shape(*b, cand_tpi, cand_cps, sample)) != MCG_OK) break;
-                float ms = 0.f;
-                for (int rep = 0; rep < 2; ++rep) {  // the first run warms the caches
-                    if (cudaEventRecord(e0, s) != cudaSuccess || book_enqueue(*b, s) != cudaSuccess ||
-                        cudaEventRecord(e1, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
-                        st = fail(MCG_ERR_CUDA, "book autotune launch failed");
-                        break;
-                    }
-                    cudaEventElapsedTime(&ms, e0, e1);
+        for (uint32_t cand_tpi : {2u, 4u, 16u}) {
+            if ((st = book_set_shape(*b, cand_tpi, cps, sample)) != MCG_OK) break;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {  // the first run warms the caches
+                if (cudaEventRecord(e0, s) != cudaSuccess || book_enqueue(*b, s) != cudaSuccess ||
+                    cudaEventRecord(e1, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+                    st = fail(MCG_ERR_CUDA, "book autotune launch failed");
+                    break;
                 }
-                if (st != MCG_OK) break;
-                if (ms < best) {
-                    best = ms;
-                    best_tpi = cand_tpi;
-                    best_cps = cand_cps;
-                }
+                cudaEventElapsedTime(&ms, e0, e1);
             }
             if (st != MCG_OK) break;
+            if (ms < best) {
+                best = ms;
+                best_tpi = cand_tpi;
+            }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaStreamDestroy(s);
         if (st != MCG_OK) return st;
         tpi = best_tpi;
-        cps = best_cps;
         b->autotune_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     mcg_status st = book_set_shape(*b, tpi, cps, all);
@@ -2345,12 +2366,15 @@ mcg_status book_evaluate(mcg_book* b, cudaStream_t stream, mcg_estimate* prices,
     cudaEventDestroy(e1);
     if (report) {
         std::memset(report, 0, sizeof(*report));
+        const std::vector<uint32_t> order = book_order(*b);
         report->trade_count = b->trades;
-        report->items = static_cast<uint32_t>(b->host_items.size());
+        for (uint32_t f : order) {
+            report->items += static_cast<uint32_t>(b->host_items[f].size());
+            report->ctas += b->ctas[f];
+        }
         report->tiles_per_item = b->tiles_per_item;
-        report->ctas_per_sm = b->ctas_per_sm;
-        report->ctas = b->ctas;
-        report->kernel_launches = 2;
+        report->ctas_per_sm = order.empty() ? 0u : b->ctas[order[0]] / static_cast<uint32_t>(b->sms);
+        report->kernel_launches = static_cast<uint32_t>(order.size()) + 1u;
         report->graph = b->graph_exec ? 1 : 0;
         report->device_ms = ms;
         report->autotune_ms = b->autotune_ms;

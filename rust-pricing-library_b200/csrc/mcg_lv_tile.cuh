@@ -38,10 +38,12 @@ __device__ __forceinline__ double ev_sign(int e) {
 // Batched normals: z_batch<Q>() normals of the program per path at a time
 // (eight per thread either way), in s_z[(k * Q + q)][thread] for the thread's
 // Q paths.  The warp forms the uniforms, takes AS241's central branch for
-// every lane, and evaluates the tail branch only for the lanes that need it,
-// 32 at a time from a compacted list (s_zlist, 32 * z_batch<Q>() * Q entries
-// per warp); the values are those of as241 bit for bit, without a warp
-// executing the tail branch for each normal that one of its lanes sends there.
+// every lane (its fused multiply-add form), and evaluates the tail branch only
+// for the lanes that need it, 32 at a time from a compacted list (s_zlist,
+// 32 * z_batch<Q>() * Q entries per warp), without a warp executing the tail
+// branch for each normal that one of its lanes sends there.  The branch
+// decision is that of as241 on the same word, the tail values are as241's bit
+// for bit, the central ones within a few ulps.
 template <int Q>
 __host__ __device__ constexpr int z_batch() { return Q == 2 ? 4 : 8; }
 
@@ -74,10 +76,11 @@ __device__ __forceinline__ void fill_normals(const DevicePlan& P, NormalSource (
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const double p = open_unit(words[q]);
+            // (w + 0.5) 2^-32 as one exact fused multiply-add (w 2^-32 + 2^-33 needs 33 bits)
+            const double p = fma(static_cast<double>(words[q]), 0x1p-32, 0x1p-33);
             const double c = p - 0.5;
             const bool tail = !(fabs(c) <= 0.425);
-            const double central = as241_central(c);
+            const double central = as241_central_fma(c);
             const uint32_t slot = k * Q + q;
             s_z[slot * kThreads + threadIdx.x] = tail ? p : central;
             const unsigned m = __ballot_sync(0xffffffffu, tail);

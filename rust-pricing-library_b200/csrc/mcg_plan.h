@@ -157,6 +157,7 @@ struct DevicePlan {
     // BS pathwise risk of a multi-observation product: per-thread scratch of
     // `bs_tape_units` threads x bs_tape_rows rows ([row][thread]).
     double* bs_tape;
+    int32_t bs_sweep;  // 1: the single-sweep kernel (no tape) prices this plan's path risk
     uint64_t bs_tape_units;
     uint32_t bs_tape_rows;
 

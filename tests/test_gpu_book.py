@@ -63,3 +63,16 @@ def test_rejects_what_a_book_cannot_hold(engine):
     with pytest.raises(N.EngineError) as err:
         N.Book(specs)
     assert err.value.name == "unsupported"
+
+
+@pytest.mark.parametrize("tpi", [1, 3])
+def test_ragged_tiles_equal_their_plans_alone(engine, tpi):
+    """An odd tile count with a partial last tile: the two-path family pairs
+    tiles from even first tiles (odd tiles per item are rounded up to even)."""
+    specs = W.batched_book(G.gpu_grid, trades=16, units=1100, seed=3)
+    with N.Book(specs, autotune=False, tiles_per_item=tpi) as book:
+        prices, report = book.evaluate()
+    assert report.kernel_launches >= 2
+    for i, spec in enumerate(specs):
+        want = alone(spec)
+        assert (prices[i].value, prices[i].standard_error) == (want.value, want.standard_error), i
