@@ -383,6 +383,51 @@ def dual_secondary(units: int = 1 << 14, cpu_units: int = 2048):
             "cpu_sample": f"{cpu_units} outer units, training included ({cpu_s:.1f} s)"}
 
 
+def multi_asset_secondary(paths: int = 1 << 20, cpu_units: int = 1 << 14):
+    """Correlated multi-asset paths: a four-asset basket call (two Black--Scholes
+    assets, two local-volatility assets on their own SSVI Dupire grids),
+    weights 0.4/0.3/0.2/0.1, strike 100, a correlation change at half a year,
+    daily steps over one year, `paths` antithetic pseudo units.  The oracle on
+    the host's cores prices `cpu_units` units of the same plan."""
+    import math
+    from rust_pricing_b200 import _abi as A, _native as N, workloads as W
+    from rust_pricing_b200.desc import AssetSpec, MultiAssetSpec
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+
+    def div(q):
+        return dict(dividend_times=(0.0, 2.0), dividend_factors=(1.0, math.exp(-2.0 * q)))
+
+    grids = [W.local_vol_grid(W.SsviSurface(steps=STEPS, expiries=30, rho=rho, eta=eta), gpu_grid)
+             for rho, eta in ((-0.4, 1.0), (-0.3, 0.8))]
+    assets = [AssetSpec(spot=100.0, volatility=0.2, **div(0.01)),
+              AssetSpec(spot=95.0, model=A.MODEL_LOCAL_VOLATILITY, local_variance=grids[0], **div(0.02)),
+              AssetSpec(spot=110.0, volatility=0.25, **div(0.0)),
+              AssetSpec(spot=90.0, model=A.MODEL_LOCAL_VOLATILITY, local_variance=grids[1], **div(0.015))]
+    rho = [[1.0, 0.5, 0.3, 0.1], [0.5, 1.0, 0.4, 0.2], [0.3, 0.4, 1.0, -0.3], [0.1, 0.2, -0.3, 1.0]]
+    half = [[1.0 if i == j else 0.5 * rho[i][j] for j in range(4)] for i in range(4)]
+    spec = MultiAssetSpec(assets=assets, correlations=[(-1.0 / 365, rho), (0.5, half)], strike=100.0,
+                          weights=[0.4, 0.3, 0.2, 0.1], sampling_units=paths, antithetic=True,
+                          brownian_bridge=False, maximum_step=1.0 / STEPS, reduction_block_size=4096,
+                          discount_times=(0.0, 2.0), discount_factors=(1.0, math.exp(-0.06)))
+    N.multi_asset_price(spec)
+    r = min((N.multi_asset_price(spec) for _ in range(3)), key=lambda x: x.device_ms)
+    asset_steps = paths * 2 * r.time_steps * len(assets)
+    spec.sampling_units = cpu_units
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    c = H.oracle_multi(spec, threads)
+    cpu_s = time.perf_counter() - t0
+    return {"workload": f"4-asset basket call (2 BS + 2 SSVI local vol), correlation change at 0.5 y, "
+                        f"{r.time_steps} daily steps, {paths} antithetic pseudo units",
+            "device_ms": r.device_ms, "path_asset_steps_per_s": asset_steps / (r.device_ms * 1e-3),
+            "price": r.price.value, "standard_error": r.price.standard_error,
+            "ms_to_1bp_standard_error": time_to_bp(r.device_ms, r.price.standard_error, r.price.value),
+            "kernel_launches": r.kernel_launches,
+            "cpu_oracle_path_asset_steps_per_s": cpu_units * 2 * c.time_steps * len(assets) / cpu_s,
+            "cpu_threads": threads, "cpu_sample": f"{cpu_units} units ({cpu_s:.1f} s)"}
+
+
 def f32_secondary(points: int, scrambles: int, prices64):
     """The timed workload with the FP32 path bulk: time and the error of each
     price against the FP64 run's."""
@@ -585,7 +630,8 @@ def main():
         "ms_to_1bp_standard_error": [time_to_bp(ms_per_step, m["standard_error"], m["value"])
                                      for m in merged] if merged else None,
     }
-    wanted = {"european", "early_exercise", "book", "f32", "adjoint", "path_risk", "dual"} if args.secondary == "all" else (
+    wanted = {"european", "early_exercise", "book", "f32", "adjoint", "path_risk", "dual",
+              "multi_asset"} if args.secondary == "all" else (
         set() if args.secondary == "none" else set(args.secondary.split(",")))
     if rank == 0 and world == 1 and wanted:
         sec = {}
@@ -606,6 +652,8 @@ def main():
             sec["bs_path_risk"] = path_risk_secondary(args.path_risk_units)
         if "dual" in wanted:
             sec["dual_upper_bound"] = dual_secondary(args.dual_units)
+        if "multi_asset" in wanted:
+            sec["multi_asset"] = multi_asset_secondary()
         line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

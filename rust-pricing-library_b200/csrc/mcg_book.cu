@@ -5,8 +5,9 @@
 // Every trade is a compiled single-product plan (its own model, surface,
 // maturity, step count and product); the kernels run the very per-tile path
 // evaluation of the single-plan kernels (mcg_bs_tile.cuh, mcg_lv_tile.cuh), in
-// the same specialisation the single-plan launch picks for that trade, so each
-// trade's statistics are bit for bit those of evaluating its plan alone.
+// the same specialisation the single-plan launch picks for that trade (batched
+// normals included), so each trade's statistics are bit for bit those of
+// evaluating its plan alone.
 //
 // Families: the trades are split by path kind, and each family has its own
 // persistent kernel, specialised and register-budgeted for it -- local
@@ -52,6 +53,8 @@ __host__ __device__ inline BookSmem book_smem(uint32_t family, uint32_t max_node
         at += static_cast<size_t>(max_nodes) * sizeof(double2);
         m.slots = at;
         at += q * max_slots * kThreads * sizeof(double);
+    }
+    if (family_lv(family) || family == kFamilyBsPath) {
         m.normals = at;
         at += zb * q * kThreads * sizeof(double);
         m.lists = at;
@@ -119,8 +122,10 @@ __global__ void __launch_bounds__(kThreads, family_lv(F) ? 5 : (F == kFamilyBsPa
                 StatRecord* out = base + static_cast<size_t>(tile) * kComponents;
                 if constexpr (F == kFamilyBsTerminal)
                     bs_terminal_tile<false>(P, s_red, 0, point, point < P.units, out, mask);
+                else if (P.antithetic)
+                    bs_path_tile<1, 2>(P, s_red, 0, point, point < P.units, out, mask, err, 0, nullptr, s_z, s_zlist);
                 else
-                    bs_path_tile<1>(P, s_red, 0, point, point < P.units, out, mask, err, 0);
+                    bs_path_tile<1, 1>(P, s_red, 0, point, point < P.units, out, mask, err, 0, nullptr, s_z, s_zlist);
             }
         }
     }

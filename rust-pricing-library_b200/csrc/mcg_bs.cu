@@ -26,17 +26,20 @@ __global__ void __launch_bounds__(kThreads) bs_terminal_kernel(const DevicePlan 
     bs_terminal_tile<kRisk>(P, s_red, scramble, point, valid, tile_out, mask);
 }
 
-// Multi-observation kernel, price and barrier diagnostics (NP products).
-template <int NP>
+// Multi-observation kernel, price and barrier diagnostics (NP products; EV
+// evolutions: 2 with the antithetic mate).
+template <int NP, int EV>
 __global__ void __launch_bounds__(kThreads) bs_path_kernel(const DevicePlan P, uint64_t unit_begin,
                                                            StatRecord* partials, uint32_t mask,
                                                            ErrorWord* err, int detail) {
     __shared__ Stat s_red[4 * kComponents];
+    __shared__ double s_z[z_batch<1>() * kThreads];                 // batched normals [k][thread]
+    __shared__ uint16_t s_zlist[(kThreads / 32) * 32 * z_batch<1>()];  // tail lists, per warp
     const uint32_t scramble = blockIdx.y;
     const uint64_t point = unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
     const bool valid = point < unit_begin + (detail ? 1 : P.units) && point < P.units;
     StatRecord* tile_out = partials + (static_cast<size_t>(scramble) * gridDim.x + blockIdx.x) * P.product_count * kComponents;
-    bs_path_tile<NP>(P, s_red, scramble, point, valid, tile_out, mask, err, detail);
+    bs_path_tile<NP, EV>(P, s_red, scramble, point, valid, tile_out, mask, err, detail, nullptr, s_z, s_zlist);
 }
 
 cudaError_t launch_bs_path_risk(const DevicePlan& P, uint64_t unit_begin, uint64_t units, uint32_t scrambles,
@@ -56,11 +59,15 @@ cudaError_t launch_bs_path(const DevicePlan& P, bool single_terminal, uint64_t u
     }
     if (P.risk) return launch_bs_path_risk(P, unit_begin, units, scrambles, partials, mask, err, detail, stream);
     const int np = static_cast<int>(P.product_count);
-    if (np == 1) bs_path_kernel<1><<<grid, kThreads, 0, stream>>>(P, unit_begin, partials, mask, err, detail);
-    else if (np == 2) bs_path_kernel<2><<<grid, kThreads, 0, stream>>>(P, unit_begin, partials, mask, err, detail);
-    else if (np <= 4) bs_path_kernel<4><<<grid, kThreads, 0, stream>>>(P, unit_begin, partials, mask, err, detail);
-    else return cudaErrorNotSupported;
-    return cudaGetLastError();
+    auto go = [&](auto kernel) {
+        kernel<<<grid, kThreads, 0, stream>>>(P, unit_begin, partials, mask, err, detail);
+        return cudaGetLastError();
+    };
+    const bool anti = P.antithetic != 0;
+    if (np == 1) return anti ? go(bs_path_kernel<1, 2>) : go(bs_path_kernel<1, 1>);
+    if (np == 2) return anti ? go(bs_path_kernel<2, 2>) : go(bs_path_kernel<2, 1>);
+    if (np <= 4) return anti ? go(bs_path_kernel<4, 2>) : go(bs_path_kernel<4, 1>);
+    return cudaErrorNotSupported;
 }
 
 }  // namespace mcg

@@ -191,11 +191,18 @@ __device__ __forceinline__ void bs_terminal_tile(const DevicePlan& P, Stat* s_re
 
 
 // One 128-unit tile of a multi-observation path, price and barrier
-// diagnostics (NP products), records at tile_out[k * kComponents + c].
-template <int NP>
+// diagnostics (NP products), records at tile_out[k * kComponents + c].  With
+// s_z / s_zlist (z_batch<1>() x kThreads doubles, 32 x z_batch<1>() entries
+// per warp) the normals are formed eight at a time per thread with AS241's
+// tail branch compacted across the warp (fill_normals); without them one at a
+// time.  Either way the CTA's threads call it together.  EV: the path's
+// evolutions, 1, or 2 with its antithetic mate (P.antithetic), so the state
+// of both stays in registers.
+template <int NP, int EV>
 __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, uint32_t scramble, uint64_t point,
                                              bool valid, StatRecord* tile_out, uint32_t mask, ErrorWord* err,
-                                             int detail, double* unit_price = nullptr) {
+                                             int detail, double* unit_price = nullptr, double* s_z = nullptr,
+                                             uint16_t* s_zlist = nullptr) {
     const uint64_t unit = valid ? point : 0;
     NormalSource ns;
     ns.rqmc = P.engine == MCG_ENGINE_RQMC;
@@ -205,12 +212,13 @@ __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, u
     ns.dirs = P.scr_dirs ? P.scr_dirs + static_cast<size_t>(scramble) * P.dimension * 32u : nullptr;
     ns.shift = P.scr_shift ? P.scr_shift + static_cast<size_t>(scramble) * P.dimension : nullptr;
     ns.cached_block = 0xffffffffu;
-    const int pairs = P.antithetic ? 2 : 1;
+    constexpr int pairs = EV;
     double wsum[2] = {0.0, 0.0};
     double prev_f[2] = {P.spot, P.spot};
     ProductAcc acc[2][NP];
     bool failed = false;
     const double var = P.vol * P.vol;
+#pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
@@ -221,12 +229,27 @@ __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, u
         }
     double prev_t = 0.0;
     const uint32_t n = P.observation_count;
+    const bool batched = s_z != nullptr && !P.zero_variance;
+    NormalSource nsq[1] = {ns};
+    uint32_t zbase = 0, zend = 0;
     for (uint32_t i = 0; i < n; ++i) {
-        const double z = P.zero_variance ? 0.0 : ns.normal(i);
+        double z;
+        if (batched) {
+            if (i == zend) {
+                zbase = i;
+                const uint32_t cnt = n - i < static_cast<uint32_t>(z_batch<1>()) ? n - i : z_batch<1>();
+                fill_normals<1>(P, nsq, false, i, cnt, s_z, s_zlist, nullptr);
+                zend = i + cnt;
+            }
+            z = s_z[(i - zbase) * kThreads + threadIdx.x];
+        } else {
+            z = P.zero_variance ? 0.0 : ns.normal(i);
+        }
         const double t = P.obs_time[i];
         const double tv = P.vol * P.vol * t;
         const double dt = t - prev_t;
         prev_t = t;
+#pragma unroll
         for (int e = 0; e < pairs; ++e) {
             const double ze = e == 0 ? z : -z;
             wsum[e] += P.obs_sqrt_step[i] * ze;
@@ -255,6 +278,7 @@ __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, u
         double vals[kComponents];
 #pragma unroll
         for (int c = 0; c < kComponents; ++c) vals[c] = 0.0;
+#pragma unroll
         for (int e = 0; e < pairs; ++e) {
             double comp[kComponents];
 #pragma unroll

@@ -49,7 +49,10 @@ __global__ void __launch_bounds__(kThreads) scenario_kernel(const ScenarioLaunch
     } else if constexpr (PATH == kBookBsTerminal) {
         bs_terminal_tile<false>(P, s_red, scramble, point, valid, out, mask, unit_price);
     } else {
-        bs_path_tile<1>(P, s_red, scramble, point, valid, out, mask, err, 0, unit_price);
+        if (P.antithetic)
+            bs_path_tile<1, 2>(P, s_red, scramble, point, valid, out, mask, err, 0, unit_price);
+        else
+            bs_path_tile<1, 1>(P, s_red, scramble, point, valid, out, mask, err, 0, unit_price);
     }
 }
 

@@ -204,4 +204,73 @@ __device__ __forceinline__ void cta_reduce_write(const double (&vals)[NC], bool 
     __syncthreads();
 }
 
+// Batched normals: z_batch<Q>() normals per path at a time -- the ranks
+// ranks[first..first+count) of a local-volatility program, or (ranks null)
+// the dimensions first..first+count of a Black--Scholes path --
+// (eight per thread either way), in s_z[(k * Q + q)][thread] for the thread's
+// Q paths.  The warp forms the uniforms, takes AS241's central branch for
+// every lane (its fused multiply-add form), and evaluates the tail branch only
+// for the lanes that need it, 32 at a time from a compacted list (s_zlist,
+// 32 * z_batch<Q>() * Q entries per warp), without a warp executing the tail
+// branch for each normal that one of its lanes sends there.  The branch
+// decision is that of as241 on the same word, the tail values are as241's bit
+// for bit, the central ones within a few ulps.
+template <int Q>
+__host__ __device__ constexpr int z_batch() { return Q == 2 ? 4 : 8; }
+
+template <int Q>
+__device__ __forceinline__ void fill_normals(const DevicePlan& P, NormalSource (&ns)[Q], bool wsob, uint32_t first,
+                                             uint32_t count, double* s_z, uint16_t* s_zlist, const uint32_t* ranks) {
+    (void)P;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    uint16_t* list = s_zlist + warp * (32u * z_batch<Q>() * Q);
+    uint32_t tails = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t rank = ranks ? __ldg(ranks + first + k) : first + k;
+        uint32_t words[Q];
+        if constexpr (Q == 1) {
+            words[0] = wsob ? ns[0].word_warp(rank) : ns[0].word(rank);
+        } else {
+            // Q paths of one warp lane share the lane part of the Gray code and
+            // the direction row: one load of each, one XOR reduction per path.
+            if (wsob) {
+                const uint32_t v = __ldg(ns[0].dirs + static_cast<size_t>(rank) * 32u + lane);
+                const uint32_t common = __ldg(ns[0].shift + rank) ^
+                                        __ldg(ns[0].low + static_cast<size_t>(rank) * 32u + ns[0].lane_low);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    words[q] = common ^ __reduce_xor_sync(0xffffffffu, (ns[q].high_gray >> lane) & 1u ? v : 0u);
+            } else {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) words[q] = ns[q].word(rank);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            // (w + 0.5) 2^-32 as one exact fused multiply-add (w 2^-32 + 2^-33 needs 33 bits)
+            const double p = fma(static_cast<double>(words[q]), 0x1p-32, 0x1p-33);
+            const double c = p - 0.5;
+            const bool tail = !(fabs(c) <= 0.425);
+            const double central = as241_central_fma(c);
+            const uint32_t slot = k * Q + q;
+            s_z[slot * kThreads + threadIdx.x] = tail ? p : central;
+            const unsigned m = __ballot_sync(0xffffffffu, tail);
+            if (tail) list[tails + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(slot * 32u + lane);
+            tails += static_cast<uint32_t>(__popc(m));
+        }
+    }
+    __syncwarp();
+    for (uint32_t b = 0; b < tails; b += 32u) {
+        const uint32_t i = b + lane;
+        if (i < tails) {
+            const uint32_t idx = list[i];
+            double* at = s_z + (idx >> 5) * kThreads + warp * 32u + (idx & 31u);
+            const double p = *at;
+            *at = as241_tail(p, p - 0.5);
+        }
+    }
+    __syncwarp();
+}
+
 }  // namespace mcg

@@ -22,6 +22,26 @@
 
 namespace mcg {
 
+// exp of a step's increment.  For |x| < 1/8 (every daily step short of an
+// eight-sigma move) the Taylor series of e^x to degree 10 in Horner form with
+// fused multiply-adds: the truncation is below x^11/11! < 2.3e-18 relative,
+// so the value is within an ulp or two of the library exp; larger arguments
+// take the library exp.  The step's result is held to 1e-12 of the reference.
+__device__ __forceinline__ double exp_step(double x) {
+    if (!(fabs(x) < 0.125)) return exp(x);
+    double p = 1.0 / 3628800.0;
+    p = fma(p, x, 1.0 / 362880.0);
+    p = fma(p, x, 1.0 / 40320.0);
+    p = fma(p, x, 1.0 / 5040.0);
+    p = fma(p, x, 1.0 / 720.0);
+    p = fma(p, x, 1.0 / 120.0);
+    p = fma(p, x, 1.0 / 24.0);
+    p = fma(p, x, 1.0 / 6.0);
+    p = fma(p, x, 0.5);
+    p = fma(p, x, 1.0);
+    return fma(p, x, 1.0);
+}
+
 // Evolution e of E: runtime (0 base, 1 down, 2 up) and shock sign.
 template <int E>
 __device__ __forceinline__ int ev_which(int e) {
@@ -33,72 +53,6 @@ __device__ __forceinline__ double ev_sign(int e) {
     if constexpr (E == 2) return e == 0 ? 1.0 : -1.0;
     else if constexpr (E == 6) return e < 3 ? 1.0 : -1.0;
     else return 1.0;
-}
-
-// Batched normals: z_batch<Q>() normals of the program per path at a time
-// (eight per thread either way), in s_z[(k * Q + q)][thread] for the thread's
-// Q paths.  The warp forms the uniforms, takes AS241's central branch for
-// every lane (its fused multiply-add form), and evaluates the tail branch only
-// for the lanes that need it, 32 at a time from a compacted list (s_zlist,
-// 32 * z_batch<Q>() * Q entries per warp), without a warp executing the tail
-// branch for each normal that one of its lanes sends there.  The branch
-// decision is that of as241 on the same word, the tail values are as241's bit
-// for bit, the central ones within a few ulps.
-template <int Q>
-__host__ __device__ constexpr int z_batch() { return Q == 2 ? 4 : 8; }
-
-template <int Q>
-__device__ __forceinline__ void fill_normals(const DevicePlan& P, NormalSource (&ns)[Q], bool wsob, uint32_t first,
-                                             uint32_t count, double* s_z, uint16_t* s_zlist) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = threadIdx.x >> 5;
-    uint16_t* list = s_zlist + warp * (32u * z_batch<Q>() * Q);
-    uint32_t tails = 0;
-    for (uint32_t k = 0; k < count; ++k) {
-        const uint32_t rank = __ldg(P.z_ranks + first + k);
-        uint32_t words[Q];
-        if constexpr (Q == 1) {
-            words[0] = wsob ? ns[0].word_warp(rank) : ns[0].word(rank);
-        } else {
-            // Q paths of one warp lane share the lane part of the Gray code and
-            // the direction row: one load of each, one XOR reduction per path.
-            if (wsob) {
-                const uint32_t v = __ldg(ns[0].dirs + static_cast<size_t>(rank) * 32u + lane);
-                const uint32_t common = __ldg(ns[0].shift + rank) ^
-                                        __ldg(ns[0].low + static_cast<size_t>(rank) * 32u + ns[0].lane_low);
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                    words[q] = common ^ __reduce_xor_sync(0xffffffffu, (ns[q].high_gray >> lane) & 1u ? v : 0u);
-            } else {
-#pragma unroll
-                for (int q = 0; q < Q; ++q) words[q] = ns[q].word(rank);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            // (w + 0.5) 2^-32 as one exact fused multiply-add (w 2^-32 + 2^-33 needs 33 bits)
-            const double p = fma(static_cast<double>(words[q]), 0x1p-32, 0x1p-33);
-            const double c = p - 0.5;
-            const bool tail = !(fabs(c) <= 0.425);
-            const double central = as241_central_fma(c);
-            const uint32_t slot = k * Q + q;
-            s_z[slot * kThreads + threadIdx.x] = tail ? p : central;
-            const unsigned m = __ballot_sync(0xffffffffu, tail);
-            if (tail) list[tails + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(slot * 32u + lane);
-            tails += static_cast<uint32_t>(__popc(m));
-        }
-    }
-    __syncwarp();
-    for (uint32_t b = 0; b < tails; b += 32u) {
-        const uint32_t i = b + lane;
-        if (i < tails) {
-            const uint32_t idx = list[i];
-            double* at = s_z + (idx >> 5) * kThreads + warp * 32u + (idx & 31u);
-            const double p = *at;
-            *at = as241_tail(p, p - 0.5);
-        }
-    }
-    __syncwarp();
 }
 
 // One or two 128-unit tiles of Log-Euler paths.  Thread t evaluates unit
@@ -195,7 +149,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             zbase = zi;
             constexpr uint32_t kBatch = static_cast<uint32_t>(z_batch<Q>());
             const uint32_t n = P.z_count - zi < kBatch ? P.z_count - zi : kBatch;
-            fill_normals<Q>(P, ns, wsob, zi, n, s_z, s_zlist);
+            fill_normals<Q>(P, ns, wsob, zi, n, s_z, s_zlist, P.z_ranks);
             zend = zi + n;
         }
         const uint32_t k = zi++ - zbase;
@@ -258,7 +212,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             const double ratio = which == 0 ? st.ratio : P.ratio[static_cast<size_t>(which) * steps + s];
             // -v dt / 2 + sqrt(v) sqrt(dt) z with the last product and the sum fused
             const double incr = fma(sqrt(v) * sq, z, v * mhdt);
-            const double e_factor = ratio * exp(incr);
+            const double e_factor = ratio * exp_step(incr);
             xs[i] += incr;
             if (CB != 0) {
                 prev_f[i] = f[i];
