@@ -3,8 +3,12 @@
 Same plan, same Sobol words: the local-vol RQMC workload's Asian call and
 discrete down-and-out call (SSVI -> Dupire grid, 252 daily steps, Brownian
 bridge) priced with the state evolved in FP32.  The stated error of the FP32
-bulk is F32_TOL relative to the FP64 price (measured 6e-6 at 2^20 x 16 and
-2^14 x 4 points); its standard errors agree with the FP64 ones to 1 %.
+bulk is F32_TOL relative to the FP64 price (measured 6.0e-6 and 6.8e-6 at
+2^20 x 16 and at 2^14 x 4 points).  At the benchmark's 2^20 x 16 points the
+FP64 standard errors are 5.2e-6 (Asian) and 3.8e-5 (barrier) relative, so
+1e-5 bounds the FP32 bias by about two standard errors there; the measured
+bias is 1.16 and 0.18 of them.  Its standard errors agree with the FP64 ones
+to 1 %.
 """
 import pytest
 
@@ -15,7 +19,7 @@ from rust_pricing_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-F32_TOL = 2e-5
+F32_TOL = 1e-5
 
 
 def run(precision, points=1 << 14, scrambles=4, antithetic=False):
