@@ -587,7 +587,7 @@ def main():
                 # of the 2^16-point x 16-scramble case (1.342208 MB read + 256 B written over
                 # 4096 CTAs of two 128-unit tiles: grid, scramble tables and tile records, in
                 # proportion to the CTAs)
-                "traffic": (1.342208e6 + 256.0) * (args.points * args.scrambles / 256) / 4096,
+                "traffic": (1.337088e6 + 256.0) * (args.points * args.scrambles / 256) / 4096,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the path kernel on the "
                                   "2^16-point x 16-scramble case, scaled by CTA count",
                 "peak_source": "measured live: mcg_measure_fp64_peak (DFMA chains, this GPU)",
