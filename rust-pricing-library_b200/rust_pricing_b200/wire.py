@@ -435,7 +435,7 @@ def compile_request(doc: dict, *, reduction_block_size: int = 4096) -> CompiledR
     if _get(doc, "document_kind", "request") != "pricing_request":
         raise WireError("document_kind must be 'pricing_request'")
     if _get(doc, "schema_version", "request") != SCHEMA_VERSION:
-        raise UnsupportedRequest(f"schema_version {doc['schema_version']} (this engine reads version 3)")
+        doc, _ = migrate_request(doc)
     valuation = parse_date(_get(doc, "valuation_date", "request"))
     product_doc = _get(doc, "product", "request")
     ptype = _get(product_doc, "type", "product")
@@ -601,26 +601,75 @@ def _encode(value, out: bytearray) -> None:
     out += payload
 
 
-def request_fingerprint(doc: dict) -> str:
-    """fingerprint_request (wire.rs:4144-4163): BLAKE3 of "pricing/request\0",
-    the schema version as a big-endian u32 and the canonical encoding."""
+def _fingerprint_value(value, schema_version: int) -> str:
+    """fingerprint_request_value (wire.rs:4158-4163): BLAKE3 of
+    "pricing/request\0", the schema version as a big-endian u32 and the
+    encoding of the value."""
     import struct
     from .blake3 import blake3
-    body = bytearray(b"pricing/request\0" + struct.pack(">I", SCHEMA_VERSION))
-    _encode(_canonical(doc), body)
+    body = bytearray(b"pricing/request\0" + struct.pack(">I", schema_version))
+    _encode(value, body)
     return "blake3-256:" + blake3(bytes(body)).hex()
+
+
+def request_fingerprint(doc: dict) -> str:
+    """fingerprint_request (wire.rs:4144-4163): the fingerprint of the v3
+    request as the reference re-serialises it (the canonical encoding)."""
+    return _fingerprint_value(_canonical(doc), SCHEMA_VERSION)
+
+
+MIGRATION_REQUEST_V1_TO_V2 = "pricing_request/v1-to-v2"
+MIGRATION_REQUEST_V2_TO_V3 = "pricing_request/v2-to-v3"
+
+
+def migrate_request(doc: dict) -> tuple[dict, dict]:
+    """request_from_document's schema migration (crates/pricing/src/wire.rs:4015-4076,
+    RequestV1 -> RequestV2 -> RequestV3 at :1090-1137): a version-1 or -2
+    `pricing_request` carried to version 3 (v1 -> v2: the risk block gains no
+    smoothing-width ladder; v2 -> v3: no LSM block), and the migration
+    provenance the result's replay block records: the source and current
+    versions, the migration ids, the fingerprint of the source document as
+    parsed at its own version and that of the migrated request.  Features the
+    older schemas do not have are refused, as the reference refuses them:
+    graph products, Bass local volatility, a lookback's valuation-date fixing,
+    an LSM block, and (version 1) a smoothing-width ladder."""
+    import copy
+    version = _get(doc, "schema_version", "request")
+    if version == SCHEMA_VERSION:
+        fp = request_fingerprint(doc)
+        return doc, {"original_schema_version": SCHEMA_VERSION, "current_schema_version": SCHEMA_VERSION,
+                     "migration_ids": [], "pre_migration_fingerprint": fp, "post_migration_fingerprint": fp}
+    if version not in (1, 2) or isinstance(version, bool):
+        raise UnsupportedRequest(f"schema_version {version!r} (this engine reads versions 1 to 3)")
+    product, model = doc.get("product") or {}, doc.get("model") or {}
+    if product.get("type") == "graph":
+        raise UnsupportedRequest("graph products require pricing_specification v2")
+    if model.get("type") == "bass_local_volatility":
+        raise UnsupportedRequest(f"Bass local volatility is not in schema version {version}")
+    if "valuation_date_fixing" in product:
+        raise UnsupportedRequest(f"Lookback valuation-date fixing is not in schema version {version}")
+    if "lsm" in doc:
+        raise WireError(f"unknown field `lsm` in a schema-version-{version} request")
+    if version == 1 and "payoff_smoothing_width_ladder" in (doc.get("risk") or {}):
+        raise WireError("unknown field `payoff_smoothing_width_ladder` in a schema-version-1 risk block")
+    pre = _fingerprint_value(doc, version)
+    current = copy.deepcopy(doc)
+    current["schema_version"] = SCHEMA_VERSION
+    post = request_fingerprint(current)
+    ids = [MIGRATION_REQUEST_V1_TO_V2, MIGRATION_REQUEST_V2_TO_V3] if version == 1 else [MIGRATION_REQUEST_V2_TO_V3]
+    return current, {"original_schema_version": version, "current_schema_version": SCHEMA_VERSION,
+                     "migration_ids": ids, "pre_migration_fingerprint": pre, "post_migration_fingerprint": post}
 
 
 def replay_block(doc: dict) -> dict:
     """The result's replay section: this engine's version and platform, the
-    request fingerprint, and an identity migration (v3 requests only)."""
+    (migrated) request's fingerprint and the migration provenance."""
     import platform
     from . import __version__
-    fp = request_fingerprint(doc)
+    _, migration = migrate_request(doc)
     return {"library_version": __version__, "platform": f"{platform.system().lower()}-{platform.machine()}-b200",
-            "request_fingerprint": fp, "schema_version": SCHEMA_VERSION,
-            "migration": {"current_schema_version": SCHEMA_VERSION, "original_schema_version": SCHEMA_VERSION,
-                          "migration_ids": [], "pre_migration_fingerprint": fp, "post_migration_fingerprint": fp}}
+            "request_fingerprint": migration["post_migration_fingerprint"], "schema_version": SCHEMA_VERSION,
+            "migration": migration}
 
 
 # ------------------------------------------------------------------ result

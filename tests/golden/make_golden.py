@@ -33,6 +33,9 @@ which the wire-format tests compile.
   variances, and 100-digit bump references of the grid-value derivatives.
 * wire_v3_documents.json    -- fixtures/v3/*.golden.json: the format goldens of a v3 request and
   result (European and American).
+* wire_migration.json      -- fixtures/v1/pricing_request.golden.json and
+  fixtures/v2/pricing_request.golden.json: the request documents the schema
+  migrations carry to v3 (fixtures/v3/pricing_request.golden.json).
 * early_exercise_cases.json -- fixtures/early-exercise/reference-cases-v0.1.json: the
   decision, monomial-basis, feature-scaling and CPQR cases (decimal strings).
 * early_exercise.json      -- fixtures/replay/early_exercise-windows-x86_64.json:
@@ -219,6 +222,12 @@ def wire_documents():
     json.dump(out, open(os.path.join(OUT, "wire_v3_documents.json"), "w"), indent=1)
 
 
+def wire_migration():
+    out = {f"v{v}": json.load(open(os.path.join(REF, f"fixtures/v{v}/pricing_request.golden.json"))) for v in (1, 2)}
+    out["source"] = "fixtures/v1/pricing_request.golden.json, fixtures/v2/pricing_request.golden.json"
+    json.dump(out, open(os.path.join(OUT, "wire_migration.json"), "w"), indent=1)
+
+
 def early_exercise_cases():
     src = os.path.join(REF, "fixtures/early-exercise/reference-cases-v0.1.json")
     d = json.load(open(src))
@@ -330,5 +339,6 @@ if __name__ == "__main__":
     step_adjoints()
     direct_variance()
     wire_documents()
+    wire_migration()
     surfaces()
     print("golden fixtures written to", OUT)

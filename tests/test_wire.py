@@ -196,7 +196,7 @@ def test_oracle_honours_seasoned_state_and_flags():
 
 @pytest.mark.parametrize("edit, error", [
     (lambda d: d.update(document_kind="pricing_result"), wire.WireError),
-    (lambda d: d.update(schema_version=2), wire.UnsupportedRequest),
+    (lambda d: d.update(schema_version=4), wire.UnsupportedRequest),
     (lambda d: d["market"].update(discrete_dividends=[{"event_id": 1, "ex_time": 0.5,
                                                         "quote": {"type": "proportional", "beta": 1.0}}]),
      wire.WireError),
@@ -382,3 +382,63 @@ def test_discrete_dividends_compile_to_the_plan_schedule():
         cont["market"]["discrete_dividends"] = doc["market"]["discrete_dividends"]
         with pytest.raises(wire.UnsupportedRequest):
             wire.compile_request(cont)
+
+
+# ----------------------------------------------------------------- schema migrations
+
+def _migration_goldens():
+    import json as _json
+    import os as _os
+    return (_json.load(open(_os.path.join(H.GOLDEN, "wire_migration.json"))),
+            _json.load(open(_os.path.join(H.GOLDEN, "wire_v3_documents.json")))["pricing_request"])
+
+
+@pytest.mark.parametrize("version", [1, 2])
+def test_older_schema_documents_migrate_forward(version):
+    """crates/pricing/src/wire/tests.rs:423-450: the v1 (and v2) request goldens
+    migrate to the v3 golden request, with the migration ids of each step, a
+    pre-migration fingerprint (the source document at its own version) that
+    differs from the post-migration one, and the post-migration fingerprint
+    equal to the v3 golden's; the migrated request compiles to the v3 plan and
+    the result's replay block records the provenance."""
+    old, v3 = _migration_goldens()
+    doc = old[f"v{version}"]
+    assert doc["schema_version"] == version
+    migrated, prov = wire.migrate_request(copy.deepcopy(doc))
+    assert migrated == v3
+    assert prov["original_schema_version"] == version and prov["current_schema_version"] == 3
+    want_ids = ["pricing_request/v1-to-v2", "pricing_request/v2-to-v3"][version - 1:]
+    assert prov["migration_ids"] == want_ids
+    assert prov["pre_migration_fingerprint"] != prov["post_migration_fingerprint"]
+    assert prov["post_migration_fingerprint"] == wire.request_fingerprint(v3)
+    a, b = wire.compile_request(copy.deepcopy(doc)), wire.compile_request(copy.deepcopy(v3))
+    same_estimates(H.oracle_evaluate(a.plan, threads=4).products[0], H.oracle_evaluate(b.plan, threads=4).products[0])
+    replay = wire.replay_block(doc)
+    assert replay["migration"] == prov and replay["request_fingerprint"] == prov["post_migration_fingerprint"]
+    assert wire.replay_block(v3)["migration"]["migration_ids"] == []
+
+
+@pytest.mark.parametrize("version", [1, 2])
+@pytest.mark.parametrize("edit, error", [
+    (lambda d: d["product"].update(valuation_date_fixing=100.0), wire.UnsupportedRequest),
+    (lambda d: d.update(model={"type": "bass_local_volatility", "parameters": {}}), wire.UnsupportedRequest),
+    (lambda d: d["product"].update(type="graph"), wire.UnsupportedRequest),
+    (lambda d: d.update(lsm={}), wire.WireError),
+])
+def test_older_schemas_refuse_what_they_do_not_have(version, edit, error):
+    old, _ = _migration_goldens()
+    doc = copy.deepcopy(old[f"v{version}"])
+    edit(doc)
+    with pytest.raises(error):
+        wire.migrate_request(doc)
+
+
+def test_version_one_has_no_width_ladder():
+    old, _ = _migration_goldens()
+    doc = copy.deepcopy(old["v1"])
+    doc["risk"]["payoff_smoothing_width_ladder"] = [0.5, 1.0]
+    with pytest.raises(wire.WireError):
+        wire.migrate_request(doc)
+    doc["schema_version"] = 2
+    migrated, _ = wire.migrate_request(doc)
+    assert migrated["risk"]["payoff_smoothing_width_ladder"] == [0.5, 1.0]
