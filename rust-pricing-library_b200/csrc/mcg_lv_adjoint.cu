@@ -21,6 +21,7 @@
 namespace mcg {
 
 constexpr int kAdjThreads = 128;
+static_assert(kAdjThreads == kThreads, "the batched normals index [k][thread] with kThreads");
 
 struct AdjointArgs {
     int32_t which;          // spot runtime: 0 base, 1 down, 2 up
@@ -153,6 +154,9 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     long long* s_xk = reinterpret_cast<long long*>(s_x + nx);
     double* s_win = reinterpret_cast<double*>(s_xk + nx);
     double* s_w = s_win + 3 * nx;  // bridge slots [slot][thread]
+    // batched normals [k][thread] and their per-warp tail lists (fill_normals)
+    double* s_z = s_w + static_cast<size_t>(P.slot_count) * kAdjThreads;
+    uint16_t* s_zlist = reinterpret_cast<uint16_t*>(s_z + z_batch<1>() * kAdjThreads);
     for (int i = threadIdx.x; i < nx; i += kAdjThreads) {
         s_x[i] = P.grid_x[i];
         s_xk[i] = total_key(P.grid_x[i]);
@@ -200,6 +204,22 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     if (barrier) barrier_begin(pp, acc, h, f, failed);
     if (valid) A.tape_f[local] = f;
     double* w = s_w + threadIdx.x;
+    // The program's normals in order (P.z_ranks), eight at a time with AS241's
+    // tail branch compacted across the warp; every thread of the CTA walks the
+    // same program, so the warp-collective batches line up.
+    NormalSource nsq[1] = {ns};
+    uint32_t zi = 0, zbase = 0, zend = 0;
+    auto next_normal = [&]() -> double {
+        if (zi == zend) {
+            zbase = zi;
+            constexpr uint32_t kBatch = static_cast<uint32_t>(z_batch<1>());
+            const uint32_t n = P.z_count - zi < kBatch ? P.z_count - zi : kBatch;
+            fill_normals<1>(P, nsq, false, zi, n, s_z, s_zlist, P.z_ranks);
+            zend = zi + n;
+        }
+        const uint32_t k = zi++ - zbase;
+        return s_z[k * kAdjThreads + threadIdx.x];
+    };
     for (uint32_t oi = 0; oi < P.op_count; ++oi) {
         const Op op = P.ops[oi];
         if (op.kind == kOpZero) {
@@ -207,11 +227,11 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
             continue;
         }
         if (op.kind == kOpTerminal) {
-            w[op.out * kAdjThreads] = op.sd * ns.normal(op.rank);
+            w[op.out * kAdjThreads] = op.sd * next_normal();
             continue;
         }
         if (op.kind == kOpInterior) {
-            const double z = ns.normal(op.rank);
+            const double z = next_normal();
             w[op.out * kAdjThreads] = op.wl * w[op.left * kAdjThreads] + op.wr * w[op.right * kAdjThreads] + op.sd * z;
             continue;
         }
@@ -220,7 +240,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
         if (op.kind == kOpStep)
             shock = (w[op.right * kAdjThreads] - w[op.left * kAdjThreads]) * P.inv_sqrt_dt[s];
         else
-            shock = ns.normal(op.rank);
+            shock = next_normal();
         const double z = A.sign * shock;
         const double x = log(f / F[s]);
         const double v = interp_variance(g, P.time_cell[s], P.time_weight[s], x, hint);
@@ -542,7 +562,9 @@ __global__ void lv_node_reduce_kernel(const double* node_tiles, uint32_t tiles_p
 
 size_t lv_adjoint_smem(const DevicePlan& P) {
     return (2 * static_cast<size_t>(P.nx) + 3 * P.nx) * sizeof(double) +
-           static_cast<size_t>(P.slot_count) * kAdjThreads * sizeof(double);
+           static_cast<size_t>(P.slot_count) * kAdjThreads * sizeof(double) +
+           static_cast<size_t>(z_batch<1>()) * kAdjThreads * sizeof(double) +
+           (kAdjThreads / 32) * 32 * static_cast<size_t>(z_batch<1>()) * sizeof(uint16_t);
 }
 
 cudaError_t launch_lv_adjoint(const DevicePlan& P, const AdjointArgs& A, ErrorWord* err, cudaStream_t stream) {
