@@ -238,7 +238,7 @@ __device__ __forceinline__ void bs_path_tile(const DevicePlan& P, Stat* s_red, u
             if (i == zend) {
                 zbase = i;
                 const uint32_t cnt = n - i < static_cast<uint32_t>(z_batch<1>()) ? n - i : z_batch<1>();
-                fill_normals<1>(P, nsq, false, i, cnt, s_z, s_zlist, nullptr);
+                fill_normals<1>(nsq, false, i, cnt, s_z, s_zlist, nullptr);
                 zend = i + cnt;
             }
             z = s_z[(i - zbase) * kThreads + threadIdx.x];

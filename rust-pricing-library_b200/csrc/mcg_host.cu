@@ -2478,10 +2478,11 @@ struct MultiArrays {
     DeviceArray<double2> bounds[kMaxAssets], cells[kMaxAssets];
     DeviceArray<int4> step_prog;
     DeviceArray<BridgeNode> bridge_nodes;
-    DeviceArray<uint32_t> directions, scr_dirs, scr_shift, scr_low;
+    DeviceArray<uint32_t> directions, scr_dirs, scr_shift, scr_low, z_dims;
     DeviceArray<StatRecord> partials, records;
     DeviceArray<ErrorWord> error;
     ~MultiArrays() {
+        z_dims.release();
         for (auto* a : {&dt, &sqrt_dt, &inv_sqrt_dt, &lower, &ratio, &time_weight}) a->release();
         step_entry.release();
         time_cell.release();
@@ -2669,6 +2670,8 @@ mcg_status multi_asset_price(const mcg_multi_asset_desc* d, cudaStream_t stream,
         M.time_cell = A.time_cell.ptr;
         M.time_weight = A.time_weight.ptr;
     }
+    std::vector<int4> prog;
+    std::vector<BridgeNode> bnodes;
     if (M.bridge) {
         std::vector<BridgeInstr> instrs;
         std::vector<Op> ops;
@@ -2676,8 +2679,6 @@ mcg_status multi_asset_price(const mcg_multi_asset_desc* d, cudaStream_t stream,
         if (!compile_bridge(nodes, instrs)) return fail(MCG_ERR_BRIDGE, "invalid bridge grid");
         if (!bridge_program(nodes, instrs, ops, slots))
             return fail(MCG_ERR_UNSUPPORTED, "bridge needs more than 32 live values");
-        std::vector<int4> prog;
-        std::vector<BridgeNode> bnodes;
         int32_t zero_slot = 0;
         if (!step_program(ops, steps, prog, bnodes, zero_slot))
             return fail(MCG_ERR_BRIDGE, "internal: path program steps out of order");
@@ -2691,6 +2692,28 @@ mcg_status multi_asset_price(const mcg_multi_asset_desc* d, cudaStream_t stream,
         M.bridge_nodes = A.bridge_nodes.ptr;
         M.zero_slot = zero_slot;
         M.slot_count = slots;
+    }
+    {
+        // The dimensions of a unit's normals in the order the kernel consumes
+        // them: per step, each bridge node's rank for every factor, or the
+        // step for every factor; dimension factor x steps + rank, or rank x
+        // assets + factor when rank-major (path.rs:24-75).
+        std::vector<uint32_t> zd;
+        auto dim = [&](uint32_t f, uint32_t r) { return M.rank_major ? r * n + f : f * steps + r; };
+        for (uint32_t st = 0; st < steps; ++st) {
+            if (M.bridge) {
+                for (int32_t j = 0; j < prog[st].y; ++j)
+                    for (uint32_t q = 0; q < n; ++q)
+                        zd.push_back(dim(q, static_cast<uint32_t>(bnodes[static_cast<size_t>(prog[st].x) + j].rank)));
+            } else {
+                for (uint32_t q = 0; q < n; ++q) zd.push_back(dim(q, st));
+            }
+        }
+        for (uint32_t v : zd)
+            if (v >= M.dimension) return fail(MCG_ERR_BRIDGE, "internal: normal dimension out of range");
+        MCG_CUDA(A.z_dims.upload(zd));
+        M.z_dims = A.z_dims.ptr;
+        M.z_count = static_cast<uint32_t>(zd.size());
     }
     if (rqmc) {
         if (M.dimension > MCG_MAX_SOBOL_DIMENSION)

@@ -219,9 +219,8 @@ template <int Q>
 __host__ __device__ constexpr int z_batch() { return Q == 2 ? 4 : 8; }
 
 template <int Q>
-__device__ __forceinline__ void fill_normals(const DevicePlan& P, NormalSource (&ns)[Q], bool wsob, uint32_t first,
-                                             uint32_t count, double* s_z, uint16_t* s_zlist, const uint32_t* ranks) {
-    (void)P;
+__device__ __forceinline__ void fill_normals(NormalSource (&ns)[Q], bool wsob, uint32_t first, uint32_t count,
+                                             double* s_z, uint16_t* s_zlist, const uint32_t* ranks) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
     uint16_t* list = s_zlist + warp * (32u * z_batch<Q>() * Q);

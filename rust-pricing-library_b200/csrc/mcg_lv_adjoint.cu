@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
             zbase = zi;
             constexpr uint32_t kBatch = static_cast<uint32_t>(z_batch<1>());
             const uint32_t n = P.z_count - zi < kBatch ? P.z_count - zi : kBatch;
-            fill_normals<1>(P, nsq, false, zi, n, s_z, s_zlist, P.z_ranks);
+            fill_normals<1>(nsq, false, zi, n, s_z, s_zlist, P.z_ranks);
             zend = zi + n;
         }
         const uint32_t k = zi++ - zbase;

@@ -149,7 +149,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             zbase = zi;
             constexpr uint32_t kBatch = static_cast<uint32_t>(z_batch<Q>());
             const uint32_t n = P.z_count - zi < kBatch ? P.z_count - zi : kBatch;
-            fill_normals<Q>(P, ns, wsob, zi, n, s_z, s_zlist, P.z_ranks);
+            fill_normals<Q>(ns, wsob, zi, n, s_z, s_zlist, P.z_ranks);
             zend = zi + n;
         }
         const uint32_t k = zi++ - zbase;

@@ -21,13 +21,6 @@ namespace mcg {
 
 namespace {
 
-// Normal of (factor f, rank r): the reference's dimension layout.
-__device__ __forceinline__ double multi_normal(const MultiAssetDev& M, NormalSource& ns, uint32_t f, uint32_t r) {
-    const uint32_t dim = M.rank_major ? r * M.n + f : f * M.steps + r;
-    if (M.engine == MCG_ENGINE_RQMC) return ns.normal_warp(dim);
-    return ns.normal(dim);
-}
-
 // The basket's value (sum of weighted, scaled terminal spots) or the
 // worst-of's (the smallest scaled spot), then the option on it.
 template <int NA>
@@ -70,7 +63,9 @@ __global__ void __launch_bounds__(kThreads) multi_asset_kernel(const MultiAssetD
                                                                ErrorWord* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Stat* s_red = reinterpret_cast<Stat*>(smem_raw);
-    double* s_w = reinterpret_cast<double*>(s_red + 4);  // bridge slots [factor][slot][thread]
+    double* s_z = reinterpret_cast<double*>(s_red + 4);                                 // batched normals [k][thread]
+    uint16_t* s_zlist = reinterpret_cast<uint16_t*>(s_z + z_batch<1>() * kThreads);      // tail lists, per warp
+    double* s_w = reinterpret_cast<double*>(s_zlist + (kThreads / 32) * 32 * z_batch<1>());  // bridge slots
     const uint32_t scramble = blockIdx.y;
     const uint64_t point = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
     const bool valid = point < M.units;
@@ -106,6 +101,22 @@ __global__ void __launch_bounds__(kThreads) multi_asset_kernel(const MultiAssetD
     uint32_t bad_step = 0;
     double bad_value = 0.0;
     double* w = s_w + threadIdx.x;
+    // The unit's normals in consumption order (M.z_dims), eight at a time with
+    // AS241's tail branch compacted across the warp (fill_normals); every
+    // thread walks the same program, so the warp-collective batches line up.
+    NormalSource nsq[1] = {ns};
+    uint32_t zi = 0, zbase = 0, zend = 0;
+    auto next_normal = [&]() -> double {
+        if (zi == zend) {
+            zbase = zi;
+            constexpr uint32_t kBatch = static_cast<uint32_t>(z_batch<1>());
+            const uint32_t cnt = M.z_count - zi < kBatch ? M.z_count - zi : kBatch;
+            fill_normals<1>(nsq, ns.rqmc, zi, cnt, s_z, s_zlist, M.z_dims);
+            zend = zi + cnt;
+        }
+        const uint32_t k = zi++ - zbase;
+        return s_z[k * kThreads + threadIdx.x];
+    };
     const size_t fstride = static_cast<size_t>(M.slot_count) * kThreads;  // factor f's slots: w + f * fstride
     if (M.bridge)
         for (uint32_t q = 0; q < n; ++q) w[q * fstride + M.zero_slot * kThreads] = 0.0;
@@ -117,7 +128,7 @@ __global__ void __launch_bounds__(kThreads) multi_asset_kernel(const MultiAssetD
                 const BridgeNode nd = M.bridge_nodes[prog.x + j];
                 for (uint32_t q = 0; q < n; ++q) {
                     double* wq = w + q * fstride;
-                    const double z = multi_normal(M, ns, q, static_cast<uint32_t>(nd.rank));
+                    const double z = next_normal();
                     wq[nd.out * kThreads] = nd.wl * wq[nd.left * kThreads] + nd.wr * wq[nd.right * kThreads] + nd.sd * z;
                 }
             }
@@ -128,7 +139,7 @@ __global__ void __launch_bounds__(kThreads) multi_asset_kernel(const MultiAssetD
                              : 0.0;
         } else {
 #pragma unroll
-            for (int q = 0; q < NA; ++q) ind[q] = q < static_cast<int>(n) ? multi_normal(M, ns, q, s) : 0.0;
+            for (int q = 0; q < NA; ++q) ind[q] = q < static_cast<int>(n) ? next_normal() : 0.0;
         }
         // correlated shocks, path.rs:76-96
         const double* l = M.lower + static_cast<size_t>(M.step_entry[s]) * n * n;
@@ -182,7 +193,9 @@ __global__ void __launch_bounds__(kThreads) multi_asset_kernel(const MultiAssetD
 }  // namespace
 
 size_t multi_asset_smem(const MultiAssetDev& M) {
-    return 4 * sizeof(Stat) + (M.bridge ? static_cast<size_t>(M.n) * M.slot_count * kThreads * sizeof(double) : 0);
+    return 4 * sizeof(Stat) + static_cast<size_t>(z_batch<1>()) * kThreads * sizeof(double) +
+           (kThreads / 32) * 32 * static_cast<size_t>(z_batch<1>()) * sizeof(uint16_t) +
+           (M.bridge ? static_cast<size_t>(M.n) * M.slot_count * kThreads * sizeof(double) : 0);
 }
 
 cudaError_t launch_multi_asset(const MultiAssetDev& M, uint32_t scrambles, StatRecord* partials, ErrorWord* err,

@@ -29,6 +29,10 @@ struct MultiAssetDev {
     const double2* bounds[kMaxAssets];  // local volatility: cell bounds {x[c], x[c+1]}
     const double2* cells[kMaxAssets];   // local volatility: {v[t][c], slope} per row and cell
     double x_first[kMaxAssets], x_last[kMaxAssets];
+    // the dimensions of the unit's normals in the order the kernel consumes
+    // them (per step: the bridge nodes' ranks x factors, or the step x factors)
+    const uint32_t* z_dims;
+    uint32_t z_count;
     // the one-factor bridge program of the common grid
     const int4* step_prog;
     const BridgeNode* bridge_nodes;
