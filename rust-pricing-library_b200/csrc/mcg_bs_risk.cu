@@ -424,6 +424,8 @@ __global__ void __launch_bounds__(kThreads, kCont ? 4 : 6) bs_path_risk_kernel(c
                                                                 uint64_t unit_end, StatRecord* partials,
                                                                 uint32_t mask, ErrorWord* err, int detail) {
     __shared__ Stat s_red[4 * kComponents];
+    __shared__ double s_z[z_batch<1>() * kThreads];                    // batched normals [k][thread]
+    __shared__ uint16_t s_zlist[(kThreads / 32) * 32 * z_batch<1>()];  // tail lists, per warp
     const uint32_t scramble = blockIdx.y;
     const uint64_t point = unit_begin + static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
     const bool valid = point < unit_end && point < P.units;
@@ -441,10 +443,26 @@ __global__ void __launch_bounds__(kThreads, kCont ? 4 : 6) bs_path_risk_kernel(c
     ns.dirs = P.scr_dirs ? P.scr_dirs + static_cast<size_t>(scramble) * P.dimension * 32u : nullptr;
     ns.shift = P.scr_shift ? P.scr_shift + static_cast<size_t>(scramble) * P.dimension : nullptr;
     ns.cached_block = 0xffffffffu;
+    // The path's normals, dimension k at observation k, eight at a time with
+    // AS241's tail branch compacted across the warp (fill_normals); every
+    // thread of the CTA walks the same observations.
+    NormalSource nsq[1] = {ns};
+    uint32_t zbase = 0, zend = 0, zi = 0;
+    auto next_normal = [&]() -> double {
+        if (zi == zend) {
+            zbase = zi;
+            constexpr uint32_t kBatch = static_cast<uint32_t>(z_batch<1>());
+            const uint32_t cnt = P.observation_count - zi < kBatch ? P.observation_count - zi : kBatch;
+            fill_normals<1>(nsq, false, zi, cnt, s_z, s_zlist, nullptr);
+            zend = zi + cnt;
+        }
+        const uint32_t kk = zi++ - zbase;
+        return s_z[kk * kThreads + threadIdx.x];
+    };
     // W_k of the primary path (path_observations_from_normals, :297-331)
     double w = 0.0;
     for (uint32_t k = 0; k < P.observation_count; ++k) {
-        const double z = P.zero_variance ? 0.0 : ns.normal(k);
+        const double z = P.zero_variance ? 0.0 : next_normal();
         w += P.obs_sqrt_step[k] * z;
         w_tape[static_cast<size_t>(k) * stride] = w;
     }
@@ -488,6 +506,8 @@ __global__ void __launch_bounds__(kThreads, kAnti ? 2 : 4) bs_path_sweep_kernel(
     (void)err;
     (void)detail;
     __shared__ Stat s_red[4 * kComponents];
+    __shared__ double s_z[z_batch<1>() * kThreads];                    // batched normals [k][thread]
+    __shared__ uint16_t s_zlist[(kThreads / 32) * 32 * z_batch<1>()];  // tail lists, per warp
     constexpr int S = kAnti ? 2 : 1;  // path signs: primary and antithetic mate
     constexpr int N = 7 * S;          // evaluation i of sign s at 7 s + i
     const uint32_t scramble = blockIdx.y;
@@ -532,11 +552,27 @@ __global__ void __launch_bounds__(kThreads, kAnti ? 2 : 4) bs_path_sweep_kernel(
     }
 #pragma unroll
     for (int s = 0; s < S; ++s) av[s] = wa[s] = ta[s] = 0.0;
+    // The path's normals, dimension k at observation k, eight at a time with
+    // AS241's tail branch compacted across the warp (fill_normals); every
+    // thread of the CTA walks the same observations.
+    NormalSource nsq[1] = {ns};
+    uint32_t zbase = 0, zend = 0, zi = 0;
+    auto next_normal = [&]() -> double {
+        if (zi == zend) {
+            zbase = zi;
+            constexpr uint32_t kBatch = static_cast<uint32_t>(z_batch<1>());
+            const uint32_t cnt = P.observation_count - zi < kBatch ? P.observation_count - zi : kBatch;
+            fill_normals<1>(nsq, false, zi, cnt, s_z, s_zlist, nullptr);
+            zend = zi + cnt;
+        }
+        const uint32_t kk = zi++ - zbase;
+        return s_z[kk * kThreads + threadIdx.x];
+    };
     double w = 0.0, wlast[S], sk[N];
 #pragma unroll
     for (int j = 0; j < N; ++j) sk[j] = 0.0;
     for (uint32_t k = 0; k < n; ++k) {
-        const double z = P.zero_variance ? 0.0 : ns.normal(k);
+        const double z = P.zero_variance ? 0.0 : next_normal();
         w += P.obs_sqrt_step[k] * z;
         const double t = P.obs_time[k];
         const double F = P.obs_fwd[k];
