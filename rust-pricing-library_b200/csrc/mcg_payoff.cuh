@@ -27,6 +27,12 @@ struct ProductAcc {
     uint32_t counts2;
     int32_t touched; // exact continuous barrier: an endpoint touched
     int32_t initial_touched;
+    // Continuous barrier: the next interval's left-endpoint quantities, carried
+    // from this interval's right endpoint (the same values a fresh evaluation
+    // of the same state gives): exact -- ln(state) and ln(log-distance);
+    // smoothed -- the effective log-distance and its ln.
+    double c_end, c_logd;
+    uint32_t c_valid;  // bit 0: c_end, bit 1: c_logd
 };
 
 MCG_HD void acc_init(ProductAcc& s) {
@@ -39,6 +45,9 @@ MCG_HD void acc_init(ProductAcc& s) {
     s.counts2 = 0;
     s.touched = 0;
     s.initial_touched = 0;
+    s.c_end = 0.0;
+    s.c_logd = 0.0;
+    s.c_valid = 0u;
 }
 
 // Initial state of a product: the seasoned literals of compile.rs:162-176
@@ -247,23 +256,113 @@ MCG_HD void count_status(ProductAcc& s, int status) {
 // One bridge interval of a continuous barrier (exact or smoothed).  Smoothed
 // endpoints are recomputed for each interval, as the reference does; the
 // smoothed right endpoint's safety weight is a hit factor.
+// One interval of a path whose intervals follow one another: the left
+// endpoint `ls` is the previous call's right endpoint, whose logarithms (and,
+// smoothed, effective log-distance) the accumulator carries, so each interval
+// evaluates its right endpoint only.  The arithmetic is exact_interval's and
+// smooth_endpoint / smooth_interval's, value for value.
 MCG_HD void barrier_interval(const ProductParams& p, ProductAcc& s,
                                                  double h, double ls, double rs, double lv,
                                                  double rv, double dt, bool& failed) {
     const bool up = p.barrier_direction == MCG_BARRIER_UP;
+    const uint32_t carried = s.c_valid;
+    s.c_valid = 0u;  // the endpoint quantities are set below
     if (!(dt > 0.0)) return;
     double log_surv;
     int status;
     if (h > 0.0) {
         double lsafe, rsafe, ld, rd;
-        smooth_endpoint(up, ls, p.barrier, h, lsafe, ld, failed);
+        if (carried & 1u) ld = s.c_end;
+        else smooth_endpoint(up, ls, p.barrier, h, lsafe, ld, failed);
         smooth_endpoint(up, rs, p.barrier, h, rsafe, rd, failed);
-        status = smooth_interval(ld, rd, lv, rv, dt, log_surv, failed);
+        s.c_end = rd;
+        s.c_valid |= 1u;
+        // smooth_interval with ln(ld) carried and ln(rd) kept for the next interval
+        if (!(lv >= 0.0) || !isfinite(lv) || !(rv >= 0.0) || !isfinite(rv)) {
+            failed = true;
+            log_surv = 0.0;
+            status = 1;
+        } else if (ld == 0.0 || rd == 0.0) {
+            log_surv = -INFINITY;
+            status = 1;
+        } else {
+            const double integrated = (0.5 * lv + 0.5 * rv) * dt;
+            if (!isfinite(integrated)) {
+                failed = true;
+                log_surv = 0.0;
+                status = 1;
+            } else if (integrated == 0.0) {
+                log_surv = 0.0;
+                status = 2;
+            } else {
+                const double lld = (carried & 2u) ? s.c_logd : log(ld);
+                const double lrd = log(rd);
+                s.c_logd = lrd;
+                s.c_valid |= 2u;
+                const double le = kLn2 + lld + lrd - log(integrated);
+                if (le >= kLogMaxExpArgument) {
+                    log_surv = 0.0;
+                    status = 4;
+                } else if (le <= kLogMinPositive) {
+                    log_surv = le;
+                    status = 3;
+                } else {
+                    const double e = exp(le);
+                    log_surv = log(-expm1(-e));
+                    status = 0;
+                }
+            }
+        }
         s.hit_log = s.hit_log + log(rsafe);
         s.hit_prod = s.hit_prod * rsafe;
     } else {
         if (s.initial_touched) return;
-        status = exact_interval(up, ls, rs, p.barrier, lv, rv, dt, log_surv, failed);
+        // exact_interval with ln(ls) and ln(ld) carried
+        if (!(ls > 0.0) || !isfinite(ls) || !(rs > 0.0) || !isfinite(rs) || !(lv >= 0.0) || !isfinite(lv) ||
+            !(rv >= 0.0) || !isfinite(rv)) {
+            failed = true;
+            log_surv = 0.0;
+            status = 1;
+        } else {
+            const double lb = log(p.barrier);
+            const double lls = (carried & 1u) ? s.c_end : log(ls);
+            const double lrs = log(rs);
+            s.c_end = lrs;
+            s.c_valid |= 1u;
+            const double ld = up ? lb - lls : lls - lb;
+            const double rd = up ? lb - lrs : lrs - lb;
+            if (ld <= 0.0 || rd <= 0.0) {
+                log_surv = -INFINITY;
+                status = 1;  // touched
+            } else {
+                const double integrated = (0.5 * lv + 0.5 * rv) * dt;
+                if (!isfinite(integrated)) {
+                    failed = true;
+                    log_surv = 0.0;
+                    status = 1;
+                } else if (integrated == 0.0) {
+                    log_surv = 0.0;
+                    status = 2;
+                } else {
+                    const double lld = (carried & 2u) ? s.c_logd : log(ld);
+                    const double lrd = log(rd);
+                    s.c_logd = lrd;
+                    s.c_valid |= 2u;
+                    const double le = kLn2 + lld + lrd - log(integrated);
+                    if (le >= kLogMaxExpArgument) {
+                        log_surv = 0.0;
+                        status = 4;
+                    } else if (le <= kLogMinPositive) {
+                        log_surv = le;
+                        status = 3;
+                    } else {
+                        const double e = exp(le);
+                        log_surv = log(-expm1(-e));
+                        status = 0;
+                    }
+                }
+            }
+        }
         if (status == 1) s.touched = 1;
     }
     s.log_sum += log_surv;

@@ -27,7 +27,9 @@ def hm():
     if not os.path.exists(nvcc):
         pytest.skip("nvcc not available")
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    if not os.path.exists(OUT) or os.path.getmtime(OUT) < os.path.getmtime(SRC):
+    csrc = os.path.join(H.ROOT, "rust-pricing-library_b200", "csrc")
+    deps = [SRC] + [os.path.join(csrc, f) for f in os.listdir(csrc) if f.endswith((".cuh", ".h"))]
+    if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(d) for d in deps):
         subprocess.run([nvcc, "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-shared", SRC, "-o", OUT],
                        check=True, capture_output=True)
     lib = C.CDLL(OUT)
