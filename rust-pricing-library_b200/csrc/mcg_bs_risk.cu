@@ -238,10 +238,11 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
     double* sa_tape = f_tape + static_cast<size_t>(n) * stride;
     ProductAcc acc;
     acc_init(acc, pp);
-    double ld = 0.0;  // smoothed: effective log distance of the interval's left endpoint
+    double ld = 0.0, lld = 0.0;  // smoothed: the left endpoint's effective log distance and its log
     if (h > 0.0) {
         double safety;
         smooth_endpoint(up, spot, B, h, safety, ld, failed);
+        lld = log(ld);
         acc.hit_log = 0.0 + log(safety);
         acc.hit_prod = 1.0 * safety;
     } else {
@@ -258,14 +259,18 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
             // barrier_interval with the left endpoint carried over
             double rsafe, rd, log_surv;
             smooth_endpoint(up, f, B, h, rsafe, rd, failed);
+            const double lrd = log(rd);
             if (dt > 0.0) {
-                const int status = smooth_interval(ld, rd, var, var, dt, log_surv, failed);
-                acc.hit_log = acc.hit_log + log(rsafe);
-                acc.hit_prod = acc.hit_prod * rsafe;
+                const int status = smooth_interval(ld, rd, lld, lrd, var, var, dt, log_surv, failed);
+                if (rsafe != 1.0) {  // log(1) = +0 leaves the hit factor unchanged
+                    acc.hit_log = acc.hit_log + log(rsafe);
+                    acc.hit_prod = acc.hit_prod * rsafe;
+                }
                 acc.log_sum += log_surv;
                 count_status(acc, status);
             }
             ld = rd;
+            lld = lrd;
         } else {
             barrier_interval(pp, acc, h, prev_f, f, var, var, dt, failed);
         }
@@ -298,40 +303,27 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
     double var_adj = 0.0;
     double carry = n == 0 ? 0.0 + td * 1.0 : 0.0;  // sa of the next node before its left part
     if (flows) {
-        SmoothEndpointFull el{1.0, 1.0, 0.0, 0.0};
-        if (h > 0.0) el = smooth_endpoint_full(up, spot, B, h);
+        // Each node's bridge quantities are computed once and carried into the next interval.
+        const double lb = h > 0.0 ? 0.0 : log(B);
+        BarrierEndpoint nl = barrier_endpoint(up, B, lb, h, spot);
         prev_f = spot;
         prev_t = 0.0;
         for (uint32_t k = 0; k < n; ++k) {
             const double fk = f_tape[static_cast<size_t>(k) * stride];
             const double t = P.obs_time[k];
             const double dt = t - prev_t;
-            double left = 0.0, right = 0.0, hit = 0.0;
-            SmoothEndpointFull er{1.0, 1.0, 0.0, 0.0};
-            if (h > 0.0) {
-                er = smooth_endpoint_full(up, fk, B, h);
-                if (dt > 0.0) {
-                    const SmoothIntervalDerivs d = smooth_interval_derivs(el.eld, er.eld, var, var, dt);
-                    left = 0.0 * el.hit_d_state + (lsa * d.d_left_distance) * el.eld_d_state;
-                    right = 0.0 * er.hit_d_state + (lsa * d.d_right_distance) * er.eld_d_state;
-                    var_adj += (lsa * d.d_left_var) + (lsa * d.d_right_var);
-                }
-                hit = el.safety == 0.0 ? 0.0 : -lsa * el.hit_d_state / el.safety;
-            } else {
-                const IntervalAdjoint ia = barrier_interval_adjoint(up, B, h, lsa, prev_f, fk, var, var, dt);
-                left = ia.left_state;
-                right = ia.right_state;
-                var_adj += ia.left_var + ia.right_var;
-            }
-            double sa = carry + left;
-            if (h > 0.0) sa += hit;
+            const BarrierEndpoint nr = barrier_endpoint(up, B, lb, h, fk);
+            const IntervalAdjoint ia = bridge_interval_adjoint(up, h, lsa, nl, nr, prev_f, fk, var, var, dt);
+            var_adj += ia.left_var + ia.right_var;
+            double sa = carry + ia.left_state;
+            if (h > 0.0) sa += hit_factor_adjoint(nl, lsa);
             sa_tape[static_cast<size_t>(k) * stride] = sa;
-            carry = (k + 1 == n) ? (0.0 + td * 1.0) + right : 0.0 + right;
-            el = er;
+            carry = (k + 1 == n) ? (0.0 + td * 1.0) + ia.right_state : 0.0 + ia.right_state;
+            nl = nr;
             prev_f = fk;
             prev_t = t;
         }
-        if (h > 0.0) carry += el.safety == 0.0 ? 0.0 : -lsa * el.hit_d_state / el.safety;
+        if (h > 0.0) carry += hit_factor_adjoint(nl, lsa);
     } else {
         for (uint32_t k = 0; k < n; ++k) sa_tape[static_cast<size_t>(k) * stride] = 0.0;
         carry = 0.0 + td * 1.0;

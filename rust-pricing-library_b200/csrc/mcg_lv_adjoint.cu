@@ -375,9 +375,14 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     if (!barrier && !fixed &&
         (pp.kind == MCG_PRODUCT_EUROPEAN || pp.kind == MCG_PRODUCT_DIGITAL || pp.kind == MCG_PRODUCT_DISCRETE_BARRIER))
         sa_next += terminal_adj;
+    // The bridge quantities of node s + 1, carried down from the previous step.
+    const bool endpoints = bridge_adjoint || (barrier && h > 0.0);
+    const double lb = endpoints && !(h > 0.0) ? log(pp.barrier) : 0.0;
+    BarrierEndpoint node_next{};
+    if (endpoints) node_next = barrier_endpoint(up, pp.barrier, lb, h, f);
     if (barrier) {
         sa_next += terminal_adj;
-        if (h > 0.0) sa_next += hit_factor_adjoint(up, pp.barrier, h, lsa, f);
+        if (h > 0.0) sa_next += hit_factor_adjoint(node_next, lsa);
     }
     double vs_next = 0.0;
     for (int s = static_cast<int>(steps) - 1; s >= 0; --s) {
@@ -393,15 +398,18 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
         const InterpFull in_s = interp_full(g, tc, P.time_weight[s], log(fs / F[s]), hint);
         double sa_cur = obs_seed(static_cast<uint32_t>(s));
         double vs_cur = 0.0;
+        BarrierEndpoint node_s{};
+        if (endpoints) node_s = barrier_endpoint(up, pp.barrier, lb, h, fs);
         if (bridge_adjoint) {
-            const IntervalAdjoint ia = barrier_interval_adjoint(up, pp.barrier, h, lsa, fs, f_next,
-                                                                in_s.value, in_next.value, P.dt[s]);
+            const IntervalAdjoint ia = bridge_interval_adjoint(up, h, lsa, node_s, node_next, fs, f_next, in_s.value,
+                                                               in_next.value, P.dt[s]);
             sa_next += ia.right_state;
             vs_next += ia.right_var;
             sa_cur += ia.left_state;
             vs_cur += ia.left_var;
         }
-        if (barrier && h > 0.0) sa_cur += hit_factor_adjoint(up, pp.barrier, h, lsa, fs);
+        if (barrier && h > 0.0) sa_cur += hit_factor_adjoint(node_s, lsa);
+        node_next = node_s;
         // finalise node s + 1: its direct variance seed
         if (vs_next != 0.0) {
             sa_next += vs_next * in_next.dvdx / f_next;

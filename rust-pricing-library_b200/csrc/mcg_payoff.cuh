@@ -143,6 +143,10 @@ MCG_HD void acc_observe(const ProductParams& p, ProductAcc& s, uint32_t obs,
 
 // ---------------------------------------------- continuous barrier bridge
 
+// log(-expm1(-exp(le))), the ordinary branch's log survival
+// (barrier_bridge.rs:341-345, :493-497).
+MCG_HD double interval_log_survival(double le) { return log(-expm1(-exp(le))); }
+
 // BarrierBridgeInterval::evaluate (exact), barrier_bridge.rs:446-528, with a
 // constant barrier; returns the status and log survival only.
 MCG_HD int exact_interval(bool up, double ls, double rs, double barrier,
@@ -180,8 +184,7 @@ MCG_HD int exact_interval(bool up, double ls, double rs, double barrier,
         log_surv = le;
         return 3;
     }
-    const double e = exp(le);
-    log_surv = log(-expm1(-e));
+    log_surv = interval_log_survival(le);
     return 0;
 }
 
@@ -209,9 +212,11 @@ MCG_HD void smooth_endpoint(bool up, double state, double barrier, double h,
     eld = up ? -log1p(-safe.value / spot_barrier) : log1p(safe.value / spot_barrier);
 }
 
-// SmoothedBarrierBridgeInterval::evaluate, barrier_bridge.rs:276-357.
-MCG_HD int smooth_interval(double ld, double rd, double lv, double rv,
-                                               double dt, double& log_surv, bool& failed) {
+// SmoothedBarrierBridgeInterval::evaluate, barrier_bridge.rs:276-357, given
+// lld = log(ld) and lrd = log(rd) (a path's consecutive intervals share an
+// endpoint and pass its logarithm on); they are read only when ld, rd != 0.
+MCG_HD int smooth_interval(double ld, double rd, double lld, double lrd, double lv, double rv,
+                           double dt, double& log_surv, bool& failed) {
     if (!(lv >= 0.0) || !isfinite(lv) || !(rv >= 0.0) || !isfinite(rv)) {
         failed = true;
         log_surv = 0.0;
@@ -231,7 +236,7 @@ MCG_HD int smooth_interval(double ld, double rd, double lv, double rv,
         log_surv = 0.0;
         return 2;
     }
-    const double le = kLn2 + log(ld) + log(rd) - log(integrated);
+    const double le = kLn2 + lld + lrd - log(integrated);
     if (le >= kLogMaxExpArgument) {
         log_surv = 0.0;
         return 4;
@@ -240,8 +245,7 @@ MCG_HD int smooth_interval(double ld, double rd, double lv, double rv,
         log_surv = le;
         return 3;
     }
-    const double e = exp(le);
-    log_surv = log(-expm1(-e));
+    log_surv = interval_log_survival(le);
     return 0;
 }
 
@@ -307,8 +311,7 @@ MCG_HD void barrier_interval(const ProductParams& p, ProductAcc& s,
                     log_surv = le;
                     status = 3;
                 } else {
-                    const double e = exp(le);
-                    log_surv = log(-expm1(-e));
+                    log_surv = interval_log_survival(le);
                     status = 0;
                 }
             }
@@ -356,8 +359,7 @@ MCG_HD void barrier_interval(const ProductParams& p, ProductAcc& s,
                         log_surv = le;
                         status = 3;
                     } else {
-                        const double e = exp(le);
-                        log_surv = log(-expm1(-e));
+                        log_surv = interval_log_survival(le);
                         status = 0;
                     }
                 }
@@ -477,17 +479,17 @@ struct ExactIntervalDerivs {
     double d_left_state, d_right_state, d_left_var, d_right_var;
 };
 
-MCG_HD ExactIntervalDerivs exact_interval_derivs(bool up, double ls, double rs, double barrier,
-                                                 double lv, double rv, double dt) {
+// ld, rd: the endpoints' signed log distances to the barrier (log(B) - log(state)
+// up, log(state) - log(B) down); lld, lrd: their logarithms, read only when
+// ld, rd > 0.
+MCG_HD ExactIntervalDerivs exact_interval_derivs(bool up, double ls, double rs, double ld, double rd, double lld,
+                                                 double lrd, double lv, double rv, double dt) {
     ExactIntervalDerivs d{0.0, 0.0, 0.0, 0.0};
-    const double lb = log(barrier);
-    const double ld = up ? lb - log(ls) : log(ls) - lb;
-    const double rd = up ? lb - log(rs) : log(rs) - lb;
     if (ld <= 0.0 || rd <= 0.0) return d;
     const double average = 0.5 * lv + 0.5 * rv;
     const double integrated = average * dt;
     if (!isfinite(integrated) || integrated == 0.0) return d;
-    const double le = kLn2 + log(ld) + log(rd) - log(integrated);
+    const double le = kLn2 + lld + lrd - log(integrated);
     if (le >= kLogMaxExpArgument) return d;
     double led;
     if (le <= kLogMinPositive) {
@@ -535,19 +537,20 @@ MCG_HD SmoothEndpointFull smooth_endpoint_full(bool up, double state, double bar
 }
 
 // Log-survival derivatives of one smoothed interval with respect to the two
-// effective log distances and the two local variances (barrier_bridge.rs:276-357).
+// effective log distances and the two local variances (barrier_bridge.rs:276-357),
+// given lld = log(ld) and lrd = log(rd).
 struct SmoothIntervalDerivs {
     double d_left_distance, d_right_distance, d_left_var, d_right_var;
 };
 
-MCG_HD SmoothIntervalDerivs smooth_interval_derivs(double ld, double rd, double lv, double rv,
-                                                   double dt) {
+MCG_HD SmoothIntervalDerivs smooth_interval_derivs(double ld, double rd, double lld, double lrd, double lv,
+                                                   double rv, double dt) {
     SmoothIntervalDerivs d{0.0, 0.0, 0.0, 0.0};
     if (ld == 0.0 || rd == 0.0) return d;
     const double average = 0.5 * lv + 0.5 * rv;
     const double integrated = average * dt;
     if (!isfinite(integrated) || integrated == 0.0) return d;
-    const double le = kLn2 + log(ld) + log(rd) - log(integrated);
+    const double le = kLn2 + lld + lrd - log(integrated);
     if (le >= kLogMaxExpArgument) return d;
     double led;
     if (le <= kLogMinPositive) {
@@ -565,6 +568,32 @@ MCG_HD SmoothIntervalDerivs smooth_interval_derivs(double ld, double rd, double 
     return d;
 }
 
+// One observation node of a continuous-barrier path as the bridge adjoint
+// reads it: computed once per node and shared by the two intervals that meet
+// there (and by the node's smoothed hit factor).
+struct BarrierEndpoint {
+    double d;      // smoothed: effective log distance; exact: signed log distance to the barrier
+    double log_d;  // log(d)
+    double d_state, hit_d_state, safety;  // smoothed: d(d)/d(state), d(hit weight)/d(state), safety weight
+};
+
+// lb = log(barrier).
+MCG_HD BarrierEndpoint barrier_endpoint(bool up, double barrier, double lb, double h, double state) {
+    BarrierEndpoint n{1.0, 0.0, 0.0, 0.0, 1.0};
+    if (h > 0.0) {
+        const SmoothEndpointFull e = smooth_endpoint_full(up, state, barrier, h);
+        n.d = e.eld;
+        n.d_state = e.eld_d_state;
+        n.hit_d_state = e.hit_d_state;
+        n.safety = e.safety;
+    } else {
+        const double ls = log(state);
+        n.d = up ? lb - ls : ls - lb;
+    }
+    n.log_d = log(n.d);
+    return n;
+}
+
 // Adjoint of the continuous-barrier bridge for one interval [k-1, k]:
 // contributions to the state seeds and the direct variance seeds of both
 // nodes, given the log-survival adjoint lsa
@@ -573,22 +602,21 @@ struct IntervalAdjoint {
     double left_state, right_state, left_var, right_var;
 };
 
-MCG_HD IntervalAdjoint barrier_interval_adjoint(bool up, double barrier, double h, double lsa,
-                                                double ls, double rs, double lv, double rv,
-                                                double dt) {
+MCG_HD IntervalAdjoint bridge_interval_adjoint(bool up, double h, double lsa, const BarrierEndpoint& L,
+                                               const BarrierEndpoint& R, double ls, double rs, double lv, double rv,
+                                               double dt) {
     IntervalAdjoint a{0.0, 0.0, 0.0, 0.0};
     if (!(dt > 0.0)) return a;
     if (h > 0.0) {
-        const SmoothEndpointFull le = smooth_endpoint_full(up, ls, barrier, h);
-        const SmoothEndpointFull re = smooth_endpoint_full(up, rs, barrier, h);
-        const SmoothIntervalDerivs d = smooth_interval_derivs(le.eld, re.eld, lv, rv, dt);
-        a.left_state = 0.0 * le.hit_d_state + (lsa * d.d_left_distance) * le.eld_d_state;
-        a.right_state = 0.0 * re.hit_d_state + (lsa * d.d_right_distance) * re.eld_d_state;
+        const SmoothIntervalDerivs d = smooth_interval_derivs(L.d, R.d, L.log_d, R.log_d, lv, rv, dt);
+        a.left_state = 0.0 * L.hit_d_state + (lsa * d.d_left_distance) * L.d_state;
+        a.right_state = 0.0 * R.hit_d_state + (lsa * d.d_right_distance) * R.d_state;
         a.left_var = lsa * d.d_left_var;
         a.right_var = lsa * d.d_right_var;
         return a;
     }
-    const ExactIntervalDerivs d = exact_interval_derivs(up, ls, rs, barrier, lv, rv, dt);
+    const ExactIntervalDerivs d =
+        exact_interval_derivs(up, ls, rs, L.d, R.d, L.log_d, R.log_d, lv, rv, dt);
     a.left_state = lsa * d.d_left_state;
     a.right_state = lsa * d.d_right_state;
     a.left_var = lsa * d.d_left_var;
@@ -596,7 +624,22 @@ MCG_HD IntervalAdjoint barrier_interval_adjoint(bool up, double barrier, double 
     return a;
 }
 
+// The same for a lone interval.
+MCG_HD IntervalAdjoint barrier_interval_adjoint(bool up, double barrier, double h, double lsa,
+                                                double ls, double rs, double lv, double rv,
+                                                double dt) {
+    if (!(dt > 0.0)) return IntervalAdjoint{0.0, 0.0, 0.0, 0.0};
+    const double lb = log(barrier);
+    const BarrierEndpoint L = barrier_endpoint(up, barrier, lb, h, ls);
+    const BarrierEndpoint R = barrier_endpoint(up, barrier, lb, h, rs);
+    return bridge_interval_adjoint(up, h, lsa, L, R, ls, rs, lv, rv, dt);
+}
+
 // Adjoint of a smoothed hit factor at one node: -lsa * d(hit)/d(state) / safety.
+MCG_HD double hit_factor_adjoint(const BarrierEndpoint& n, double lsa) {
+    return n.safety == 0.0 ? 0.0 : -lsa * n.hit_d_state / n.safety;
+}
+
 MCG_HD double hit_factor_adjoint(bool up, double barrier, double h, double lsa, double state) {
     const SmoothEndpointFull e = smooth_endpoint_full(up, state, barrier, h);
     return e.safety == 0.0 ? 0.0 : -lsa * e.hit_d_state / e.safety;
