@@ -316,7 +316,7 @@ def european_secondary(paths: int = 1 << 20, cpu_units: int = 1 << 24):
     r = 3 %, q = 1 %, sigma = 20 %, T = 1, one exact lognormal step, `paths`
     pseudo paths (seed 0x0123456789abcdef), FP64, price with pathwise Delta and
     Vega and Gamma by a 1 % relative bump (which also fills the CRN validation
-    components: 7 evaluations of every path), judged by the closed form.  The
+    components: 7 evaluations of every path), checked against the closed form.  The
     oracle on the host's cores prices `cpu_units` paths of the same plan."""
     from rust_pricing_b200 import _native as N, workloads as W
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -336,7 +336,7 @@ def european_secondary(paths: int = 1 << 20, cpu_units: int = 1 << 24):
     H.oracle_evaluate(spec, threads)
     cpu_s = time.perf_counter() - t0
     out = {"workload": f"European BS call, {paths} pseudo paths, 1 exact step, FP64, price + pathwise Delta/Vega "
-                       "+ 1 % relative Gamma bump (7 path evaluations per unit); judge: closed form",
+                       "+ 1 % relative Gamma bump (7 path evaluations per unit); checked against the closed form",
            "device_ms": ms, "path_steps_per_s": paths / (ms * 1e-3),
            "path_evaluations_per_s": 7 * paths / (ms * 1e-3), "kernel_launches": r.result.kernel_launches,
            "ms_to_1bp_standard_error": time_to_bp(ms, p.price.standard_error, p.price.value),
@@ -372,7 +372,7 @@ def dual_secondary(units: int = 1 << 14, cpu_units: int = 2048):
     c = H.oracle_lsm_dual(spec, lsm, n2, n3, seed, threads=os.cpu_count() or 1)
     cpu_s = time.perf_counter() - t0
     return {"workload": f"Andersen-Broadie dual, American put, 50 dates, {units} x 2 outer paths, "
-                        f"N2 = {n2}, N3 = {n3} inner paths; judge: 5000-step Bermudan tree",
+                        f"N2 = {n2}, N3 = {n3} inner paths; checked against a 5000-step Bermudan tree",
             "tree": tree, "device_ms": r.device_ms, "nested_ms": r.nested_ms,
             "lower_bound": r.lower_bound.value, "lower_se": r.lower_bound.standard_error,
             "upper_bound": r.upper_bound.value, "upper_se": r.upper_bound.standard_error,
@@ -454,7 +454,7 @@ def lsm_secondary(units: int = 1 << 20):
     from bermudan_tree import bermudan_equally_spaced
     from rust_pricing_b200 import _abi as A, _native as N, workloads as W
     tree = bermudan_equally_spaced(100.0, 100.0, 0.05, 0.0, 0.25, 1.0, 50, steps=5000)
-    out = {"workload": f"American put by LSM, 50 dates, {units} + {units} paths, cubic basis; judge: 5000-step "
+    out = {"workload": f"American put by LSM, 50 dates, {units} + {units} paths, cubic basis; checked against a 5000-step "
                        "Bermudan binomial tree", "tree": tree}
     for name, kind in (("plain", A.CONTINUATION_POLYNOMIAL), ("learned", A.CONTINUATION_MLP)):
         spec, lsm = W.american_bs(dates=50, units=units)

@@ -77,7 +77,7 @@ typedef enum mcg_status {
     MCG_ERR_MARKET = 11,               /* MarketError (curve, surface, grid) */
     MCG_ERR_LSM = 12,                  /* LsmNumericalError */
     MCG_ERR_TIMEOUT = 13,              /* a bounded device wait ran out */
-    MCG_ERR_NOT_BUILT = 14             /* a kernel variant is missing from this build */
+    MCG_ERR_NOT_BUILT = 14             /* a kernel variant is missing from the compiled library */
 } mcg_status;
 
 typedef enum mcg_model_kind {

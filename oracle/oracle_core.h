@@ -1,6 +1,6 @@
 // oracle_core.h -- CPU restatement of the reference's Monte Carlo hot path.
 //
-// TEST INFRASTRUCTURE ONLY.  This code is the checker the CUDA engine is
+// TEST INFRASTRUCTURE ONLY.  This code is the oracle the CUDA engine is
 // compared against: only tests/, __graft_entry__.smoke() and bench.py's CPU
 // baseline leg may load it.  It is never linked into the engine.
 //

@@ -1,6 +1,6 @@
 // oracle_lsm.cpp -- Longstaff--Schwartz early exercise of the CPU oracle.
 //
-// TEST INFRASTRUCTURE ONLY: the checker the CUDA engine is compared against,
+// TEST INFRASTRUCTURE ONLY: the oracle the CUDA engine is compared against,
 // never linked into the engine.  Restates, from msfmfjt/rust-pricing-library
 // (paths relative to that project):
 //   FeatureScaling::fit                 crates/pricing/src/engine/mc/lsm.rs:537-574

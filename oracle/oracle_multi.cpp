@@ -1,6 +1,6 @@
 // oracle_multi.cpp -- correlated multi-asset Monte Carlo of the CPU oracle.
 //
-// TEST INFRASTRUCTURE ONLY: the checker the CUDA engine is compared against.
+// TEST INFRASTRUCTURE ONLY: the oracle the CUDA engine is compared against.
 // It restates MultiAssetPricingPlan (msfmfjt/rust-pricing-library, paths
 // relative to that project) for Black--Scholes and local-volatility assets:
 //   compile        crates/pricing/src/engine/multi_asset/compile.rs:200-470

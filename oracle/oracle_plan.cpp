@@ -1,6 +1,6 @@
 // oracle_plan.cpp -- plan compile and execute of the CPU oracle.
 //
-// TEST INFRASTRUCTURE ONLY: the checker the CUDA engine is compared against.
+// TEST INFRASTRUCTURE ONLY: the oracle the CUDA engine is compared against.
 // It restates SimulationPlan::execute and the per-unit closures of
 // msfmfjt/rust-pricing-library (paths relative to that project) and evaluates
 // the same `mcg_plan_desc` the engine takes.  Fixed reduction blocks are run on

@@ -1,6 +1,6 @@
 """Cox--Ross--Rubinstein binomial tree for Bermudan and American options.
 
-The independent judge of the early-exercise prices: a recombining tree with
+The independent benchmark of the early-exercise prices: a recombining tree with
 `steps` steps over the horizon, exercise allowed at the tree steps that fall
 on the exercise dates (every steps / dates steps for equally spaced dates).
 Backward induction in numpy, O(steps^2) node updates (25e6 for 5000 steps).

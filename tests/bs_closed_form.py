@@ -1,4 +1,4 @@
-"""Closed-form Black--Scholes with continuous yields: the analytic judge.
+"""Closed-form Black--Scholes with continuous yields: the analytic benchmark.
 
 Restates the forward Black--Scholes formula of
 crates/pricing/src/engine/analytic/closed_form.rs:191-223 (price, spot Delta,

@@ -1,4 +1,4 @@
-"""Bump-and-revalue cases and their judges.
+"""Bump-and-revalue cases and their acceptance checks.
 
 The reference's own acceptance of its bump plans
 (crates/pricing/src/engine/risk/bump.rs:936-1012,

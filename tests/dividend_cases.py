@@ -1,7 +1,7 @@
-"""Discrete-dividend plans of the escrowed affine model and their judges.
+"""Discrete-dividend plans of the escrowed affine model and their acceptance checks.
 
 The cases restate the reference's own acceptance of the affine dividend model
-(crates/pricing/tests/affine_oracles.rs:131-230), whose judges need no
+(crates/pricing/tests/affine_oracles.rs:131-230), whose checks need no
 simulation:
 
 * with zero volatility and zero rates a cash dividend, a proportional one or

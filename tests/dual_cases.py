@@ -39,7 +39,7 @@ def case(side=A.PUT, strike=100.0, vol=0.2, dividend=0.0, dates=DATES, units=256
 
 
 def tree_price(side=A.PUT, strike=100.0, dividend=0.0, vol=0.2, steps_per_day=4):
-    """The Bermudan binomial judge on the exercise dates (day counts x steps per day)."""
+    """The Bermudan binomial benchmark on the exercise dates (day counts x steps per day)."""
     from bermudan_tree import bermudan_binomial
     days = [(d - VALUATION).days for d in DATES]
     steps = days[-1] * steps_per_day

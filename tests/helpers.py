@@ -1,6 +1,6 @@
 """Shared test helpers: paths, the oracle loader and descriptor utilities.
 
-The oracle (oracle/_build/liboracle.so) is the checker; the engine under test is
+The oracle (oracle/_build/liboracle.so) is the reference restatement; the engine under test is
 loaded through rust_pricing_b200._native.
 """
 from __future__ import annotations

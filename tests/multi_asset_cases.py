@@ -1,4 +1,4 @@
-"""Multi-asset plans and their judges, after the reference's own acceptance
+"""Multi-asset plans and their acceptance checks, after the reference's own acceptance
 (crates/pricing/tests/multi_asset.rs:157-246): one-asset basket = the
 Black--Scholes closed form; two perfectly correlated copies of an asset = the
 one asset; an exchange option (basket [1, -1], strike 0) under a correlation

@@ -1,4 +1,4 @@
-"""The binomial judge: converges to Black--Scholes for a European and bounds
+"""The binomial benchmark: converges to Black--Scholes for a European and bounds
 the early-exercise premium of the Bermudan put from above by the American."""
 from bermudan_tree import bermudan_binomial, bermudan_equally_spaced
 from bs_closed_form import black_scholes

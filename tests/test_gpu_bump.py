@@ -5,7 +5,7 @@
   1e-12 -- Black--Scholes single-terminal and path (Asian) plans, local
   volatility pseudo-MC (with and without antithetic pairs) and RQMC with the
   bridge, spot and volatility scenarios, shared pairs.
-* The reference's judge (crates/pricing/src/engine/risk/bump.rs:986-1012): the
+* The reference's acceptance check (crates/pricing/src/engine/risk/bump.rs:986-1012): the
   local-volatility bump Delta at relative size 1e-6 agrees with the native
   Delta within the combined standard errors.
 * At the native CRN half-width the bump Delta and Gamma equal the engine's own

@@ -1,6 +1,6 @@
 """Discrete dividends (escrowed affine model) on the GPU.
 
-* The reference's own judges (crates/pricing/tests/affine_oracles.rs:131-230):
+* The reference's own acceptance checks (crates/pricing/tests/affine_oracles.rs:131-230):
   zero-volatility terminal spots exactly, and the escrowed-spot closed form for
   a cash-and-proportional dividend (price, Delta, Vega, Gamma within 4.5 SE).
 * Engine vs oracle on identical draws, within the parity tolerances

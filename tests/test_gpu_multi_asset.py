@@ -1,6 +1,6 @@
 """Correlated multi-asset paths on the GPU (mcg_multi_asset_price).
 
-* The reference's judges (crates/pricing/tests/multi_asset.rs:157-246), as for
+* The reference's acceptance checks (crates/pricing/tests/multi_asset.rs:157-246), as for
   the oracle: a one-asset basket is Black--Scholes, two perfectly correlated
   copies are the one asset to 1e-12, and an exchange option under a
   correlation change is Margrabe with the time-averaged correlation.

@@ -1,5 +1,5 @@
 """Engine vs oracle parity on identical draws (small sizes), plus the
-reference's own replay values and the analytic judge.
+reference's own replay values and the analytic benchmark.
 
 Tolerances are in gpu_common: 1e-12 of the component's scale for estimates,
 1e-8 for CRN bump-validation components (they divide last-ulp libm
@@ -136,7 +136,7 @@ def test_local_vol_short_grid_with_substeps(engine, grid):
 
 
 def test_european_statistical_acceptance_full_size(engine):
-    """2^20 paths: estimates within 4 SE of the closed form (the reference's judge)."""
+    """2^20 paths: estimates within 4 SE of the closed form (the reference's acceptance check)."""
     spec = W.european_bs(paths=1 << 20)
     p = G.run_engine(spec).products[0]
     cf = black_scholes(True, 100.0, 100.0, 1.0, W.RATE, W.DIVIDEND, 0.2)

@@ -1,4 +1,4 @@
-"""The oracle's bump-and-revalue restatement against the reference's judges.
+"""The oracle's bump-and-revalue restatement against the reference's acceptance checks.
 
 * crates/pricing/src/engine/risk/bump.rs:986-1012: under local volatility a
   spot-Delta bump of relative size 1e-6 agrees with the native Delta within the

@@ -1,5 +1,5 @@
 """The oracle's escrowed affine dividend model against the reference's own
-judges (crates/pricing/tests/affine_oracles.rs:131-230): deterministic
+acceptance checks (crates/pricing/tests/affine_oracles.rs:131-230): deterministic
 terminal spots under zero volatility, and the escrowed-spot Black--Scholes
 closed form for a cash-and-proportional dividend (price, Delta, Vega)."""
 import pytest

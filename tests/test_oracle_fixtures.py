@@ -9,7 +9,7 @@
 * Local volatility: the pseudo-MC and RQMC cases of
   fixtures/replay/local_volatility-*.json (3 x 5 grid, price-only and
   Delta/Gamma/Vega) reproduce price, standard error and variance bits.
-* Analytic: the closed-form judge reproduces fixtures/acceptance/european_bs_analytical.csv.
+* Analytic: the closed-form benchmark reproduces fixtures/acceptance/european_bs_analytical.csv.
 """
 import ctypes as C
 import json
@@ -173,7 +173,7 @@ def test_replay_independent_of_thread_count():
         assert getattr(a, f).value == getattr(b, f).value
 
 
-def test_closed_form_judge_matches_analytical_grid():
+def test_closed_form_benchmark_matches_analytical_grid():
     rows = json.load(open(os.path.join(GOLDEN, "bs_analytical.json")))["rows"]
     for row in rows:
         spot, t = 100.0, float(row["time"])

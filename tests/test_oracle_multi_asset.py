@@ -1,4 +1,4 @@
-"""The oracle's correlated multi-asset paths against the reference's judges
+"""The oracle's correlated multi-asset paths against the reference's acceptance checks
 (crates/pricing/tests/multi_asset.rs:157-246), each within 7 standard errors
 plus the reference's floor: a one-asset basket is Black--Scholes, two
 perfectly correlated copies equal the one asset to 1e-12 (the bridged terminal
