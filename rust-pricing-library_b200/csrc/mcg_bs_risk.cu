@@ -223,6 +223,7 @@ __device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const Produ
 // 10..17 of the evaluation.  Scratch rows: f_k at [0, n) of `f_tape` and
 // the node state adjoints sa_0..sa_n at [n, 2n + 1).  Each smoothed endpoint
 // is evaluated once per sweep and shared by the two intervals that meet there.
+template <bool kSmooth>
 __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
                                                   double sign, double spot, double vol, bool cached, double* diag,
                                                   bool& failed) {
@@ -231,7 +232,10 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
     const size_t stride = T.stride;
     const double* w_tape = T.w;
     const double scale = spot / P.spot;
-    const double h = P.smoothing;
+    // The launch picks the instantiation by the plan's smoothing width (> 0:
+    // smoothed, 0: exact), so each compiles one form of the bridge.
+    const double h = kSmooth ? P.smoothing : 0.0;
+    if constexpr (kSmooth) __builtin_assume(h > 0.0);
     const double var = vol * vol;
     const bool up = pp.barrier_direction == MCG_BARRIER_UP;
     const double B = pp.barrier;
@@ -345,12 +349,13 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
     return r;
 }
 
-template <bool kCont>
+// kCont: 0 no continuous barrier, 1 exact continuous barrier, 2 smoothed.
+template <int kCont>
 __device__ __forceinline__ PathAad path_aad(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
                                             double sign, double spot, double vol, bool cached, double* diag,
                                             bool& failed) {
-    if constexpr (kCont)
-        return continuous_aad(P, pp, T, sign, spot, vol, cached, diag, failed);
+    if constexpr (kCont != 0)
+        return continuous_aad<kCont == 2>(P, pp, T, sign, spot, vol, cached, diag, failed);
     else
         return discrete_aad(P, pp, T, sign, spot, vol, cached, failed);
 }
@@ -358,7 +363,7 @@ __device__ __forceinline__ PathAad path_aad(const DevicePlan& P, const ProductPa
 // The components of one primary or mate path (pathwise_values, :417-472).
 // The seven evaluations run in one loop over (spot, volatility) points, so the
 // evaluation body is instantiated once.
-template <bool kCont>
+template <int kCont>
 __device__ __forceinline__ void path_values(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
                                             double sign, double* v, bool& failed) {
     // the exponentials of this path at the plan's volatility
@@ -411,7 +416,7 @@ __device__ __forceinline__ void path_values(const DevicePlan& P, const ProductPa
 
 // One thread per unit of [unit_begin, unit_end); CTA records of tile
 // unit/128 of scramble blockIdx.y.
-template <bool kCont>
+template <int kCont>
 __global__ void __launch_bounds__(kThreads, kCont ? 4 : 6) bs_path_risk_kernel(const DevicePlan P, uint64_t unit_begin,
                                                                 uint64_t unit_end, StatRecord* partials,
                                                                 uint32_t mask, ErrorWord* err, int detail) {
@@ -740,10 +745,12 @@ cudaError_t launch_bs_path_risk(const DevicePlan& P, uint64_t unit_begin, uint64
     for (uint64_t begin = unit_begin; begin < end; begin += per_launch) {
         const uint64_t n = end - begin < per_launch ? end - begin : per_launch;
         const dim3 grid(static_cast<unsigned>((n + kThreads - 1) / kThreads), scrambles);
-        if (cont)
-            bs_path_risk_kernel<true><<<grid, kThreads, 0, stream>>>(P, begin, begin + n, partials, mask, err, detail);
+        if (cont && P.smoothing > 0.0)
+            bs_path_risk_kernel<2><<<grid, kThreads, 0, stream>>>(P, begin, begin + n, partials, mask, err, detail);
+        else if (cont)
+            bs_path_risk_kernel<1><<<grid, kThreads, 0, stream>>>(P, begin, begin + n, partials, mask, err, detail);
         else
-            bs_path_risk_kernel<false><<<grid, kThreads, 0, stream>>>(P, begin, begin + n, partials, mask, err, detail);
+            bs_path_risk_kernel<0><<<grid, kThreads, 0, stream>>>(P, begin, begin + n, partials, mask, err, detail);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
