@@ -142,7 +142,10 @@ __device__ __forceinline__ void flush_rows(double* window, int lo, int hi, int n
 
 // The grid values and their 2 sqrt(v) are read through L1 (shared memory
 // holds the x nodes, the node window and the bridge slots), which lets 5 CTAs
-// share an SM.
+// share an SM.  kBridge: the product's continuous-barrier bridge, 0 none
+// (another product), 1 exact, 2 smoothed; the launch picks it from the
+// product and the smoothing width, so each instantiation holds one form.
+template <int kBridge>
 __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const DevicePlan P, AdjointArgs A,
                                                                     ErrorWord* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -174,9 +177,10 @@ __global__ void __launch_bounds__(kAdjThreads, 5) lv_adjoint_kernel(const Device
     const double* F = P.fwd + static_cast<size_t>(which) * (steps + 1);
     const double* ratio = P.ratio + static_cast<size_t>(which) * steps;
     const ProductParams& pp = P.products[0];
-    const bool barrier = pp.kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
+    constexpr bool barrier = kBridge != 0;
     const bool up = pp.barrier_direction == MCG_BARRIER_UP;
-    const double h = P.smoothing;
+    const double h = kBridge == 1 ? 0.0 : P.smoothing;
+    if constexpr (kBridge == 2) __builtin_assume(h > 0.0);
     const bool call = pp.side == MCG_CALL;
 
     NormalSource ns;
@@ -577,12 +581,17 @@ size_t lv_adjoint_smem(const DevicePlan& P) {
 
 cudaError_t launch_lv_adjoint(const DevicePlan& P, const AdjointArgs& A, ErrorWord* err, cudaStream_t stream) {
     const size_t smem = lv_adjoint_smem(P);
-    cudaError_t e = cudaFuncSetAttribute(lv_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
     const unsigned blocks = static_cast<unsigned>((A.units + kAdjThreads - 1) / kAdjThreads);
-    lv_adjoint_kernel<<<blocks, kAdjThreads, smem, stream>>>(P, A, err);
-    return cudaGetLastError();
+    auto go = [&](auto kernel) -> cudaError_t {
+        const cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        kernel<<<blocks, kAdjThreads, smem, stream>>>(P, A, err);
+        return cudaGetLastError();
+    };
+    if (P.products[0].kind != MCG_PRODUCT_CONTINUOUS_BARRIER) return go(lv_adjoint_kernel<0>);
+    if (P.smoothing > 0.0) return go(lv_adjoint_kernel<2>);
+    return go(lv_adjoint_kernel<1>);
 }
 
 cudaError_t launch_lv_adjoint_combine(const double* vega, const double* delta, uint64_t units, int pairs,
