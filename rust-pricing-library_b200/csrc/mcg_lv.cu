@@ -203,11 +203,15 @@ cudaError_t launch_lv_path(const DevicePlan& P, uint64_t unit_begin, uint64_t un
         return cudaGetLastError();
     };
     const bool rq = P.engine == MCG_ENGINE_RQMC;
-    // (evolutions, products, paths per thread) x (engine, continuous barrier) instantiations
+    const bool smooth = cb && P.smoothing > 0.0;
+    // (evolutions, products, paths per thread) x (engine, continuous barrier:
+    // none, exact or smoothed) instantiations
 #define MCG_LV_PICK(EE, NN, QQ)                                                       \
     do {                                                                              \
+        if (rq && smooth) return go(lv_path_kernel<EE, NN, 1, 2, QQ>);                \
         if (rq && cb) return go(lv_path_kernel<EE, NN, 1, 1, QQ>);                    \
         if (rq) return go(lv_path_kernel<EE, NN, 1, 0, QQ>);                          \
+        if (smooth) return go(lv_path_kernel<EE, NN, 0, 2, QQ>);                      \
         if (cb) return go(lv_path_kernel<EE, NN, 0, 1, QQ>);                          \
         return go(lv_path_kernel<EE, NN, 0, 0, QQ>);                                  \
     } while (0)
