@@ -80,8 +80,13 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                                         double* unit_price = nullptr) {
     static_assert(Q == 1 || (Q == 2 && E == 1), "two paths per thread take one evolution each");
     constexpr int QE = Q * E;
-    const double smoothing = P.smoothing;
-    if constexpr (CB == 2) __builtin_assume(smoothing > 0.0);
+    // The plan's smoothing width, read where it is used (a kernel parameter,
+    // so no register holds it); positive under CB = 2.
+    auto smoothing_width = [&]() -> double {
+        const double h = P.smoothing;
+        if constexpr (CB == 2) __builtin_assume(h > 0.0);
+        return h;
+    };
     const bool valid_q[2] = {valid, valid_second};
     uint64_t unit_q[Q];
     NormalSource ns[Q];
@@ -135,7 +140,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
             acc_init(acc[k][i], P.products[k]);
             if (CB != 0 && k < static_cast<int>(P.product_count) &&
                 P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
-                barrier_begin(P.products[k], acc[k][i], smoothing, f[i], failed[i / E]);
+                barrier_begin(P.products[k], acc[k][i], smoothing_width(), f[i], failed[i / E]);
         }
     }
     double* w = s_w + threadIdx.x;
@@ -210,7 +215,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                 for (int k = 0; k < NP; ++k)
                     if (k < static_cast<int>(P.product_count) &&
                         P.products[k].kind == MCG_PRODUCT_CONTINUOUS_BARRIER)
-                        barrier_interval(P.products[k], acc[k][i], smoothing, prev_f[i], f[i],
+                        barrier_interval(P.products[k], acc[k][i], smoothing_width(), prev_f[i], f[i],
                                          prev_v[i], v, P.dt[s - 1], failed[q]);
             }
             const double ratio = which == 0 ? st.ratio : P.ratio[static_cast<size_t>(which) * steps + s];
@@ -252,16 +257,16 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
 #pragma unroll
                 for (int k = 0; k < NP; ++k)
                     if (k < static_cast<int>(P.product_count))
-                        acc_observe_n<QE>(P.products[k], acc[k], static_cast<uint32_t>(obs), spot, smoothing, pre,
-                                          with_pre);
+                        acc_observe_n<QE>(P.products[k], acc[k], static_cast<uint32_t>(obs), spot,
+                                          smoothing_width(), pre, with_pre);
             } else {
                 // Two paths per thread: plans without dividends (the launch
                 // helper's choice), so the observed spot is the state.
 #pragma unroll
                 for (int k = 0; k < NP; ++k)
                     if (k < static_cast<int>(P.product_count))
-                        acc_observe_n<QE, false>(P.products[k], acc[k], static_cast<uint32_t>(obs), f, smoothing,
-                                                 f, false);
+                        acc_observe_n<QE, false>(P.products[k], acc[k], static_cast<uint32_t>(obs), f,
+                                                 smoothing_width(), f, false);
             }
         }
     }
@@ -281,10 +286,10 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                 const double* F = P.fwd + static_cast<size_t>(which) * (steps + 1);
                 const double x = log(f[i] / F[steps]);
                 const double v = interp_variance_walk(g, static_cast<int>(P.nt) - 2, 1.0, x, hint[i]);
-                barrier_interval(pp, acc[k][i], smoothing, prev_f[i], f[i], prev_v[i], v,
+                barrier_interval(pp, acc[k][i], smoothing_width(), prev_f[i], f[i], prev_v[i], v,
                                  P.dt[steps - 1], failed[q]);
                 double diag[8];
-                const double surv = barrier_finish(acc[k][i], smoothing, steps, diag);
+                const double surv = barrier_finish(acc[k][i], smoothing_width(), steps, diag);
                 price[i][k] = P.discount * barrier_value(pp, f[i], surv);
                 if (which == 0 && ev_sign<E>(e) > 0.0) {
 #pragma unroll
@@ -294,7 +299,7 @@ __device__ __forceinline__ void lv_tile(const DevicePlan& P, const GridView& g, 
                     for (int d = 0; d < 8; ++d) diag_src[q][k][d] = (diag_src[q][k][d] + diag[d]) * 0.5;
                 }
             } else {
-                price[i][k] = P.discount * acc_payoff(pp, acc[k][i], smoothing);
+                price[i][k] = P.discount * acc_payoff(pp, acc[k][i], smoothing_width());
             }
         }
     }
