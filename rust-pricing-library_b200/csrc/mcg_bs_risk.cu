@@ -239,7 +239,6 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
     const double var = vol * vol;
     const bool up = pp.barrier_direction == MCG_BARRIER_UP;
     const double B = pp.barrier;
-    double* sa_tape = f_tape + static_cast<size_t>(n) * stride;
     ProductAcc acc;
     acc_init(acc, pp);
     double ld = 0.0, lld = 0.0;  // smoothed: the left endpoint's effective log distance and its log
@@ -252,10 +251,11 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
     } else {
         barrier_begin(pp, acc, h, spot, failed);
     }
-    double prev_f = spot, prev_t = 0.0, f = spot;
+    double prev_f = spot, prev_t = 0.0, f = spot, w_last = 0.0;
     for (uint32_t k = 0; k < n; ++k) {
         double w;
         f = observe(P, T, k, sign, scale, vol, cached, w);
+        w_last = w;
         f_tape[static_cast<size_t>(k) * stride] = f;
         const double t = P.obs_time[k];
         const double dt = t - prev_t;
@@ -304,16 +304,24 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
     // One sweep over the intervals: the variance adjoint in interval order and
     // sa_k = ((0 + right part of interval k-1) + left part of interval k)
     // + the smoothed hit factor at k; the terminal seed enters sa_n first.
+    // Each sa_k is final when its interval is done, so the sweep also takes the
+    // state adjoint's Delta term sa_k f_{k-1} / S and Vega term
+    // sa_k f_{k-1} (-sigma t_{k-1} + W_{k-1}) of the node before it (delta
+    // starts from sa_0); the Vega terms are summed apart from the variance
+    // adjoint's 2 sigma var_adj, which is complete only after the sweep.
     double var_adj = 0.0;
-    double carry = n == 0 ? 0.0 + td * 1.0 : 0.0;  // sa of the next node before its left part
+    double delta = 0.0, vega_terms = 0.0;
     if (flows) {
+        double carry = n == 0 ? 0.0 + td * 1.0 : 0.0;  // sa of the next node before its left part
         // Each node's bridge quantities are computed once and carried into the next interval.
         const double lb = h > 0.0 ? 0.0 : log(B);
         BarrierEndpoint nl = barrier_endpoint(up, B, lb, h, spot);
         prev_f = spot;
         prev_t = 0.0;
+        double prev_w = 0.0;
         for (uint32_t k = 0; k < n; ++k) {
             const double fk = f_tape[static_cast<size_t>(k) * stride];
+            const double wk = sign * w_tape[static_cast<size_t>(k) * stride];
             const double t = P.obs_time[k];
             const double dt = t - prev_t;
             const BarrierEndpoint nr = barrier_endpoint(up, B, lb, h, fk);
@@ -321,27 +329,36 @@ __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const Pro
             var_adj += ia.left_var + ia.right_var;
             double sa = carry + ia.left_state;
             if (h > 0.0) sa += hit_factor_adjoint(nl, lsa);
-            sa_tape[static_cast<size_t>(k) * stride] = sa;
+            if (k == 0) {
+                delta = sa;
+            } else {
+                delta += sa * prev_f / spot;
+                vega_terms += sa * prev_f * (-vol * prev_t + prev_w);
+            }
             carry = (k + 1 == n) ? (0.0 + td * 1.0) + ia.right_state : 0.0 + ia.right_state;
             nl = nr;
             prev_f = fk;
+            prev_w = wk;
             prev_t = t;
         }
         if (h > 0.0) carry += hit_factor_adjoint(nl, lsa);
+        if (n == 0) {
+            delta = carry;
+        } else {
+            delta += carry * prev_f / spot;
+            vega_terms += carry * prev_f * (-vol * prev_t + prev_w);
+        }
     } else {
-        for (uint32_t k = 0; k < n; ++k) sa_tape[static_cast<size_t>(k) * stride] = 0.0;
-        carry = 0.0 + td * 1.0;
+        // No flow through the bridge: every sa_k is 0 but the terminal's.
+        const double carry = 0.0 + td * 1.0;
+        if (n == 0) {
+            delta = carry;
+        } else {
+            delta = carry * f / spot;
+            vega_terms = carry * f * (-vol * P.obs_time[n - 1] + w_last);
+        }
     }
-    sa_tape[static_cast<size_t>(n) * stride] = carry;
-    double delta = sa_tape[0];
-    double vega = 2.0 * vol * var_adj;
-    for (uint32_t k = 0; k < n; ++k) {
-        const double s = sa_tape[static_cast<size_t>(k + 1) * stride];
-        const double fk = f_tape[static_cast<size_t>(k) * stride];
-        const double wk = sign * w_tape[static_cast<size_t>(k) * stride];
-        delta += s * fk / spot;
-        vega += s * fk * (-vol * P.obs_time[k] + wk);
-    }
+    const double vega = 2.0 * vol * var_adj + vega_terms;
     PathAad r;
     r.price = P.discount * value;
     r.delta = P.discount * delta;
