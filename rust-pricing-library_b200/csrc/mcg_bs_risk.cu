@@ -20,7 +20,7 @@
 // once into the per-thread scratch tape ([k][thread], coalesced) and all
 // fourteen evaluations read it back; a smoothed discrete barrier also keeps
 // its hit states, weights and weight slopes there for the reverse sweep, a
-// continuous barrier its observed states and node adjoints.
+// continuous barrier its observed states.
 #include "mcg_bs_tile.cuh"
 
 namespace mcg {
@@ -220,9 +220,9 @@ __device__ __forceinline__ PathAad discrete_aad(const DevicePlan& P, const Produ
 
 // pathwise_aad of a continuous barrier: the bridge over [0, t_1], ..., and
 // its adjoint (black_scholes.rs:94-293, 648-753); diag receives components
-// 10..17 of the evaluation.  Scratch rows: f_k at [0, n) of `f_tape` and
-// the node state adjoints sa_0..sa_n at [n, 2n + 1).  Each smoothed endpoint
-// is evaluated once per sweep and shared by the two intervals that meet there.
+// 10..17 of the evaluation.  Scratch rows: f_k at [0, n) of `f_tape`.  Each
+// node's bridge endpoint is evaluated once per sweep and shared by the two
+// intervals that meet there.
 template <bool kSmooth>
 __device__ __forceinline__ PathAad continuous_aad(const DevicePlan& P, const ProductParams& pp, const Scratch& T,
                                                   double sign, double spot, double vol, bool cached, double* diag,

@@ -983,12 +983,12 @@ mcg_status build(const mcg_plan_desc* d, mcg_plan& plan, bool reduction_buffers 
         // Scratch of the path-risk kernel (at most 2 GiB): W_k and the path's
         // exponentials per thread, plus the hit state, weight and slope per
         // observation for a smoothed discrete barrier, or the observed states
-        // and n + 1 node adjoints for a continuous barrier.
+        // for a continuous barrier.
         const bool smooth_barrier =
             plan.products[0].kind == MCG_PRODUCT_DISCRETE_BARRIER && P.smoothing > 0.0;
         const bool continuous = plan.products[0].kind == MCG_PRODUCT_CONTINUOUS_BARRIER;
         P.bs_tape_rows = smooth_barrier ? (P.dividends ? 7u : 5u) * P.observation_count
-                                        : (continuous ? 4u * P.observation_count + 1u : 2u * P.observation_count);
+                                        : (continuous ? 3u : 2u) * P.observation_count;
         const uint64_t budget = (2048ull << 20) / (sizeof(double) * P.bs_tape_rows * P.scramble_count);
         const uint64_t units_rounded = (P.units + kThreads - 1) / kThreads * kThreads;
         const uint64_t per_scramble =
