@@ -20,11 +20,14 @@ namespace mcg {
 // and the per-step record, grid rows, product dispatch and Sobol direction
 // rows shared) at 5 CTAs of 128 threads per SM (96 registers); one path per
 // thread runs 7 CTAs, 5 with a continuous barrier; the multi-evolution
-// (antithetic, CRN) kernels already carry several chains per thread.  The grid values are read through L1 (24.8 KB for
-// 31 x 100), so shared memory holds only the x nodes, the bridge slots and the
-// batched normals.
+// (antithetic, CRN) and four-product kernels are held to 5 CTAs as well
+// (96 registers, some spilled to L1): left free they took 150-240 registers
+// and 1-3 CTAs, and ran 1.1-1.6x slower (CRN Delta/Gamma under a smoothed
+// continuous barrier, 2^20 x 252: 86.2 -> 54.0 ms).  The grid values are
+// read through L1 (24.8 KB for 31 x 100), so shared memory holds only the x
+// nodes, the bridge slots and the batched normals.
 template <int E, int NP, int RQ, int CB, int Q>
-__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (Q == 2 ? 5 : (CB == 0 ? 7 : 5)) : 1)
+__global__ void __launch_bounds__(kThreads, (E == 1 && NP <= 2) ? (Q == 2 ? 5 : (CB == 0 ? 7 : 5)) : 5)
     lv_path_kernel(const DevicePlan P, uint64_t unit_begin, StatRecord* partials, uint32_t mask, ErrorWord* err,
                    int detail) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
