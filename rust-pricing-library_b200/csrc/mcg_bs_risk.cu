@@ -432,9 +432,11 @@ __device__ __forceinline__ void path_values(const DevicePlan& P, const ProductPa
 }  // namespace
 
 // One thread per unit of [unit_begin, unit_end); CTA records of tile
-// unit/128 of scramble blockIdx.y.
+// unit/128 of scramble blockIdx.y.  The continuous-barrier forms run 5 CTAs
+// per SM (96 registers; at 4 CTAs and 125 registers the smoothed barrier took
+// 204 against 184 ms at 2^20 paths).
 template <int kCont>
-__global__ void __launch_bounds__(kThreads, kCont ? 4 : 6) bs_path_risk_kernel(const DevicePlan P, uint64_t unit_begin,
+__global__ void __launch_bounds__(kThreads, kCont ? 5 : 6) bs_path_risk_kernel(const DevicePlan P, uint64_t unit_begin,
                                                                 uint64_t unit_end, StatRecord* partials,
                                                                 uint32_t mask, ErrorWord* err, int detail) {
     __shared__ Stat s_red[4 * kComponents];

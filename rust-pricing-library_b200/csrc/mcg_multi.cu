@@ -58,8 +58,10 @@ __device__ __forceinline__ double multi_payoff(const MultiAssetDev& M, const dou
     return 0.0 + (M.notional * positive) * M.df;
 }
 
+// 5 CTAs per SM (96 registers; left free it took 128 and 4 CTAs, 24.66 against 23.64 ms for the
+// four-asset basket at 2^20 antithetic units).
 template <int NA>
-__global__ void __launch_bounds__(kThreads) multi_asset_kernel(const MultiAssetDev M, StatRecord* partials,
+__global__ void __launch_bounds__(kThreads, 5) multi_asset_kernel(const MultiAssetDev M, StatRecord* partials,
                                                                ErrorWord* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Stat* s_red = reinterpret_cast<Stat*>(smem_raw);
