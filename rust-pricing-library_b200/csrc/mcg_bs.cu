@@ -27,9 +27,11 @@ __global__ void __launch_bounds__(kThreads) bs_terminal_kernel(const DevicePlan 
 }
 
 // Multi-observation kernel, price and barrier diagnostics (NP products; EV
-// evolutions: 2 with the antithetic mate).
+// evolutions: 2 with the antithetic mate).  Several products or evolutions
+// run at 5 CTAs per SM (96 registers; left free they took 118-248 registers:
+// four antithetic products at 2^20 x 252 ran 13.0 against 10.8 ms).
 template <int NP, int EV>
-__global__ void __launch_bounds__(kThreads) bs_path_kernel(const DevicePlan P, uint64_t unit_begin,
+__global__ void __launch_bounds__(kThreads, (NP == 1 && EV == 1) ? 1 : 5) bs_path_kernel(const DevicePlan P, uint64_t unit_begin,
                                                            StatRecord* partials, uint32_t mask,
                                                            ErrorWord* err, int detail) {
     __shared__ Stat s_red[4 * kComponents];
